@@ -1,0 +1,305 @@
+"""Seeded synthetic beds written in the reference's input formats.
+
+The reference's own scenario (input/input.txt) is not shipped, so every
+run uses one of these generators.  Two families:
+
+* ``spouted_bed`` -- the geometry the reference hard-wires: a 12.5 mm
+  cylinder over a truncated cone (functions_DEM_BC.cuh:254-257, 4237-4243),
+  an inlet pipe below z = L2 and an outlet slab above z = L3
+  (functions_NNPS.cuh:2-5), gas (argon) properties, dx = h/1.6.  Runs with
+  the reference-compat preset and is the case the reference kernels can
+  run unmodified.
+* ``box_bed`` -- the 3-D fluidized bed of the benchmark: a 0.1 x 0.02 x
+  0.4 m box, water-like fluid on a dx = 1.25 mm lattice (first N sites in
+  z-major order), Wendland C2 with h = 1.3 dx, DEM spheres of 2 mm +/-5 %
+  at density 2500 on random FCC sites in the lower 0.1 m, inlet at the
+  bottom, heat transfer on.
+
+Lattice positions get seeded uniform jitter of +/-0.01 dx so that no pair
+sits exactly on a kernel-support boundary.
+"""
+import os
+
+import numpy as np
+
+from .params import reference_params
+
+INPUT_LABELS = [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35]
+_LABEL_FIELD = {1: "x", 2: "y", 3: "z", 4: "ux", 5: "uy", 6: "uz", 7: "m", 8: "p_type", 9: "h", 10: "temp",
+                11: "pres", 12: "rho", 26: "flt_s", 27: "rad", 28: "ri", 29: "dem_idx", 30: "wx", 31: "wy",
+                32: "wz", 33: "temp1", 34: "temp2", 35: "temp3"}
+
+
+def _fcc_sites(lo, hi, spacing):
+    a = spacing * np.sqrt(2.0)
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) * a
+    n = np.floor((np.asarray(hi) - np.asarray(lo)) / a).astype(int) + 1
+    g = np.stack(np.meshgrid(np.arange(n[0]), np.arange(n[1]), np.arange(n[2]), indexing="ij"), -1).reshape(-1, 3) * a
+    pts = (g[:, None, :] + base[None, :, :]).reshape(-1, 3) + np.asarray(lo)
+    keep = np.all((pts >= lo) & (pts <= hi), axis=1)
+    return pts[keep]
+
+
+def _dem_arrays(pos, rad, rho_s, h, temp, first_id=1):
+    nd = len(pos)
+    m = rho_s * 4.0 / 3.0 * np.pi * rad ** 3
+    return dict(
+        x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(),
+        ux=np.zeros(nd), uy=np.zeros(nd), uz=np.zeros(nd),
+        wx=np.zeros(nd), wy=np.zeros(nd), wz=np.zeros(nd),
+        m=m, rho=np.full(nd, rho_s), rad=rad, ri=0.4 * m * rad ** 2,
+        h=np.full(nd, h), temp=np.full(nd, temp), temp1=np.full(nd, temp), temp2=np.full(nd, temp),
+        temp3=np.full(nd, temp), pres=np.zeros(nd), flt_s=np.zeros(nd),
+        p_type=np.full(nd, 1001, dtype=np.int32), dem_idx=np.arange(first_id, first_id + nd, dtype=np.int32),
+    )
+
+
+def spouted_bed(dx=0.5e-3, n_dem=4580, r_dem=0.5e-3, seed=0, t_gas=823.0, t_dem=300.0, dem_top=-0.002,
+                spacing=2.1, u_dem=0.0):
+    """Reference-compat spouted bed.  Returns (params, sph, dem).
+
+    DEM spheres sit on random sites of an FCC lattice whose nearest spacing
+    is ``spacing`` x the largest radius (below 2 the neighbours start in
+    contact); ``u_dem`` is the amplitude of a seeded uniform initial
+    velocity of the spheres."""
+    rng = np.random.default_rng(seed)
+    p = reference_params()
+    h = 1.6 * dx
+    R_cyl, r2, h_cone = p.cyl_r, p.cone_r2, p.cone_h
+    wall = 3 * dx
+    xs = np.arange(-(R_cyl + wall), R_cyl + wall + 1e-12, dx)
+    zs = np.arange(-0.02275, 0.01375 + 1e-12, dx)
+    X, Y, Z = np.meshgrid(xs, xs, zs, indexing="ij")
+    X, Y, Z = X.ravel(), Y.ravel(), Z.ravel()
+    r = np.hypot(X, Y)
+    # radius of the fluid region at height z: pipe, cone, cylinder
+    rz = np.where(Z >= 0.0, R_cyl, np.where(Z >= -h_cone, r2 + (Z + h_cone) * (R_cyl - r2) / h_cone, r2))
+    fluid = r < rz
+    solid = (~fluid) & (r < rz + wall)
+    keep = fluid | solid
+    X, Y, Z, fl = X[keep], Y[keep], Z[keep], fluid[keep]
+    n = len(X)
+    jit = rng.uniform(-0.01 * dx, 0.01 * dx, size=(n, 3))
+    X, Y, Z = X + jit[:, 0], Y + jit[:, 1], Z + jit[:, 2]
+    ptype = np.where(fl, 1, 0).astype(np.int32)
+    vol = (h / p.h_over_dx) ** 3
+    sph = dict(x=X, y=Y, z=Z, ux=np.zeros(n), uy=np.zeros(n), uz=np.zeros(n),
+               m=np.full(n, p.rho_gas * vol), rho=np.full(n, p.rho_gas), pres=np.zeros(n),
+               temp=np.full(n, t_gas), h=np.full(n, h), flt_s=np.ones(n), p_type=ptype,
+               rad=np.zeros(n), ri=np.zeros(n))
+    # DEM spheres on random FCC sites inside the cone/cylinder, below dem_top
+    rmax = 1.05 * r_dem
+    sites = _fcc_sites([-R_cyl, -R_cyl, -h_cone], [R_cyl, R_cyl, dem_top], spacing * rmax)
+    sr = np.hypot(sites[:, 0], sites[:, 1])
+    zz = sites[:, 2]
+    rz_s = np.where(zz >= 0.0, R_cyl, r2 + (zz + h_cone) * (R_cyl - r2) / h_cone)
+    # clearance from the cone wall measured along the wall normal
+    cosang = h_cone / np.hypot(R_cyl - r2, h_cone)
+    ok = (sr + 1.3 * rmax / cosang < rz_s) & (zz > -h_cone + 1.3 * rmax)
+    sites = sites[ok]
+    if len(sites) < n_dem:
+        n_dem = len(sites)
+    pick = rng.choice(len(sites), size=n_dem, replace=False)
+    pos = sites[np.sort(pick)]
+    rad = r_dem * rng.uniform(0.95, 1.05, size=n_dem)
+    dem = _dem_arrays(pos, rad, 2500.0, h, t_dem)
+    if u_dem > 0:
+        for f in ("ux", "uy", "uz"):
+            dem[f] = rng.uniform(-u_dem, u_dem, size=n_dem)
+    return p, sph, dem
+
+
+def box_bed(n_fluid=200_000, n_dem=20_000, dx=1.25e-3, seed=0, u_in=0.15, t_fluid=300.0, t_dem=350.0,
+            lx=0.1, ly=0.02, lz=0.4, dem_height=0.1, d_dem=2.0e-3):
+    """Benchmark bed (0.1 x 0.02 x 0.4 m).  Returns (params, sph, dem)."""
+    rng = np.random.default_rng(seed)
+    p = reference_params()
+    h = 1.3 * dx
+    p.kernel_type = 3            # Wendland C2
+    p.h_over_dx = 1.3
+    p.rho_gas = 1000.0           # the p_type 1 fluid: water-like
+    p.mu_gas = 1.0e-3
+    p.nu_gas = 1.0e-6
+    p.dem_shear_modulus = 1.0e7 / (2.0 * 1.3)   # E = 1e7, nu = 0.3
+    p.dem_poisson = 0.3
+    p.dem_friction_ratio = 0.3
+    p.g_sph = 9.81
+    p.g_dem = 9.81
+    p.con_solve = 1
+    p.dt = 1.0e-5
+    p.inlet_uz_mirror = u_in
+    p.inlet_temp = t_fluid
+    p.dem_wall_mask = 2          # box walls only
+    nx, ny = int(round(lx / dx)), int(round(ly / dx))
+    per_layer = nx * ny
+    nz_full = n_fluid // per_layer + (1 if n_fluid % per_layer else 0)
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    ii, jj = ii.T.ravel(), jj.T.ravel()        # x fastest, then y
+    layers = []
+    for k in range(-3, nz_full):               # three inlet layers below z = 0
+        z = (k + 0.5) * dx
+        layers.append(np.stack([(ii + 0.5) * dx, (jj + 0.5) * dx, np.full(per_layer, z)], 1))
+    lat = np.concatenate(layers)
+    inlet = lat[: 3 * per_layer]
+    fluid = lat[3 * per_layer: 3 * per_layer + n_fluid]
+    ztop = fluid[:, 2].max() + 0.5 * dx
+    # three wall layers around the sides, from the inlet bottom to the fluid top
+    wx = np.arange(-3, nx + 3)
+    wy = np.arange(-3, ny + 3)
+    wz = np.arange(-3, int(np.ceil(ztop / dx)))
+    WI, WJ, WK = np.meshgrid(wx, wy, wz, indexing="ij")
+    side = (WI < 0) | (WI >= nx) | (WJ < 0) | (WJ >= ny)
+    walls = np.stack([(WI[side] + 0.5) * dx, (WJ[side] + 0.5) * dx, (WK[side] + 0.5) * dx], 1)
+    pos = np.concatenate([fluid, inlet, walls])
+    ptype = np.concatenate([np.ones(len(fluid) + len(inlet), np.int32), np.zeros(len(walls), np.int32)])
+    n = len(pos)
+    pos = pos + rng.uniform(-0.01 * dx, 0.01 * dx, size=(n, 3))
+    vol = (h / p.h_over_dx) ** 3
+    uz = np.where(pos[:, 2] < 0, u_in, 0.0) * (ptype == 1)
+    sph = dict(x=pos[:, 0], y=pos[:, 1], z=pos[:, 2], ux=np.zeros(n), uy=np.zeros(n), uz=uz,
+               m=np.full(n, p.rho_gas * vol), rho=np.full(n, p.rho_gas), pres=np.zeros(n),
+               temp=np.full(n, t_fluid), h=np.full(n, h), flt_s=np.ones(n), p_type=ptype,
+               rad=np.zeros(n), ri=np.zeros(n))
+    # open-boundary slabs: inlet below z = 0, outlet in the top three fluid layers
+    p.obc_L1 = -1.0
+    p.obc_L2 = 0.0
+    p.obc_L3 = ztop - 3 * dx
+    p.obc_L4 = ztop + 1.0
+    # DEM on random FCC sites with nearest spacing 2.1 mm in the lower dem_height
+    rmax = 0.5 * d_dem * 1.05
+    sites = _fcc_sites([rmax * 1.2, rmax * 1.2, rmax * 1.2],
+                       [lx - rmax * 1.2, ly - rmax * 1.2, dem_height - rmax], 2.1e-3 * max(1.0, d_dem / 2.0e-3))
+    if len(sites) < n_dem:
+        n_dem = len(sites)
+    pick = rng.choice(len(sites), size=n_dem, replace=False)
+    dpos = sites[np.sort(pick)]
+    rad = 0.5 * d_dem * rng.uniform(0.95, 1.05, size=n_dem)
+    dem = _dem_arrays(dpos, rad, 2500.0, h, t_dem)
+    p.box_c[:] = [0.5 * lx, 0.5 * ly, 0.5 * lz]
+    p.box_L[:] = [lx, ly, lz]
+    return p, sph, dem
+
+
+def scaled_box_bed(n_fluid=2_000_000, n_dem=200_000, seed=0):
+    """The same bed with the x extent scaled by 10 (1.0 x 0.02 x 0.4 m)."""
+    return box_bed(n_fluid=n_fluid, n_dem=n_dem, seed=seed, lx=1.0)
+
+
+# ---------------------------------------------------------------------------
+# reference input formats
+# ---------------------------------------------------------------------------
+def write_input_txt(path, sph, dem):
+    """input.txt: tab-separated labels, then one row per particle
+    (function_init.cuh:743-891).  SPH rows first, then DEM rows."""
+    rows = []
+    for d in (sph, dem):
+        if not d:
+            continue
+        n = len(d["x"])
+        cols = []
+        for lbl in INPUT_LABELS:
+            f = _LABEL_FIELD[lbl]
+            v = d.get(f)
+            cols.append(np.zeros(n) if v is None else np.asarray(v, dtype=np.float64))
+        rows.append(np.stack(cols, 1))
+    data = np.concatenate(rows)
+    with open(path, "w") as fh:
+        fh.write("\t".join(str(l) for l in INPUT_LABELS) + "\n")
+        int_cols = {INPUT_LABELS.index(8), INPUT_LABELS.index(29)}
+        for r in data:
+            fh.write("\t".join(str(int(v)) if k in int_cols else repr(float(v)) for k, v in enumerate(r)) + "\n")
+
+
+_KERNEL_NAME = {0: "Gaussian", 1: "Quintic", 2: "Quartic", 3: "Wendland2", 4: "Wendland4", 5: "Wendland6"}
+
+
+def write_solv_txt(path, p):
+    """solv.txt in the layout of the reference's input/solv.txt."""
+    yn = lambda v: "YES" if v else "NO"
+    lines = [
+        "# SOPHIA Input: Solver Setup\t// standard input",
+        "solver_type (WCSPH/ISPH/DFSPH):\t" + {0: "WCSPH", 1: "ISPH", 2: "DFSPH"}[p.solver_type],
+        "dimension(1/2/3): \t%d" % p.dim,
+        "property_table(YES/NO):\t" + yn(p.prop_table),
+        "kernel type (Gaussian/Quartic/Quintic/Wendland[2/4/6]):\t" + _KERNEL_NAME[p.kernel_type],
+        "filter type (Shepard/MLS): \tShepard",
+        "density calculation (Direct/Continuity): \t" + ("Continuity" if p.rho_type == 1 else "Direct"),
+        "time integration (Euler/Predictor_Corrector): \t" + ("Predictor_Corrector" if p.time_type else "Euler"),
+        "fluid type (Liquid/Gas): \tLiquid",
+        "simulation type (Single_Phase/Two_Phase):\tSingle_Phase",
+        "pressure-force solve(YES/NO): \t" + yn(p.fp_solve),
+        "viscous-force solve(YES/NO): \t" + yn(p.fv_solve),
+        "turbulence-model (Laminar/k-lm/k-e/SPS/HB): Laminar",
+        "artificial-viscous-force solve(YES/NO): \t" + yn(p.fva_solve),
+        "gravitational-force solve(YES/NO): \t" + yn(p.fg_solve),
+        "surface-tension-force solve(YES/NO): \t" + yn(p.fs_solve),
+        "surface-tension-model (Potential/Curvature)\tPotential",
+        "interface-sharpness-force solve(YES/NO):\t" + yn(p.interface_solve),
+        "boundary-force solve(YES/NO):\t" + yn(p.fb_solve),
+        "Conduction(YES/NO):\t" + yn(p.con_solve),
+        "Boussinesq-natural-convection solve(YES/NO):\tNO",
+        "Concentration-diffusion(YES/NO):\tNO",
+        "XSPH solve(YES/NO): \t" + yn(p.xsph_solve),
+        "kernel-gradient-correction solve(NO/KGC/FPM/DFPM/KGF):\t" + ("KGC" if p.kgc_solve == 1 else "NO"),
+        "delta-SPH solve(NO/Molteni/Antuono):\t" + {0: "NO", 1: "Molteni", 2: "Antuono"}[p.delSPH_solve],
+        "particle-shifting solve(YES/NO):\tNO",
+        "penetration_box solve(YES/NO):           NO",
+        "noslip_boundary (YES/NO):                NO",
+        "open boundary (OPEN/PERIODIC/NO):\t" + {0: "NO", 1: "OPEN", 2: "PERIODIC"}[p.open_boundary],
+        "switch_ptype (YES/NO):          NO",
+        "reference-pressure (Pa): \t%r" % p.p_ref,
+        "sound-speed:  %r" % p.soundspeed,
+        "reference-density-eos: %r" % p.rho0_eos,
+        "gamma (for EOS): \t%r" % p.gamma,
+        "kappa: \t%r" % p.kappa,
+        "XSPH-coefficient:\t%r" % p.c_xsph,
+        "Boundary-coefficient:\t%r" % p.c_repulsive,
+        "minimum-iteration:\t%d" % p.min_iteration,
+        "maximum-iteration:\t%d" % p.max_iteration,
+        "pressure-convergence criterion\t%r" % p.dp_th,
+        "density-convergence criterion\t%r" % p.drho_th,
+        "pressure-relaxation factor\t%r" % p.p_relaxation,
+        "time-step (sec): \t%r" % p.dt,
+        "start-time (sec):\t%r" % p.time,
+        "end-time (sec):\t%r" % p.time_end,
+        "cell-initialization frequency: \t%d" % p.freq_cell,
+        "z-indexing (YES/NO)\t" + yn(p.flag_z_index),
+        "timestep update (YES/NO)\tNO",
+        "neighbor cell type (3X3/5X5)\t3X3",
+        "filtering frequency: \t%d" % p.freq_filt,
+        "density-renormalization frequency: \t%d" % p.freq_mass_sum,
+        "temperature-filtering frequency:\t%d" % p.freq_temp,
+        "plot-output frequency:\t%d" % p.freq_output,
+        "plot-variables:                         3 rho pres p_type",
+        "velocity-limit (m/s): \t%r" % p.u_limit,
+        "Xmargin(-): \t%r" % p.margin[0],
+        "Xmargin(+): \t%r" % p.margin[1],
+        "Ymargin(-): \t%r" % p.margin[2],
+        "Ymargin(+): \t%r" % p.margin[3],
+        "Zmargin(-): \t%r" % p.margin[4],
+        "Zmargin(+): \t%r" % p.margin[5],
+        "decouple-stride:  %d" % p.decouple_stride,
+    ]
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+
+
+DATA_TXT = """#p_type 0
+//T
+10, 100, 200, 300, 400
+//h
+0, 1000, 2000, 3000, 4000
+//k
+1, 1, 1, 1, 1
+//mu
+1e-3, 1e-3, 1e-3, 1e-3, 1e-3
+#end
+"""
+
+
+def write_input_dir(path, p, sph, dem):
+    os.makedirs(path, exist_ok=True)
+    write_solv_txt(os.path.join(path, "solv.txt"), p)
+    write_input_txt(os.path.join(path, "input.txt"), sph, dem)
+    with open(os.path.join(path, "data.txt"), "w") as fh:
+        fh.write(DATA_TXT)

@@ -1,0 +1,262 @@
+// device_common.cuh -- device-side helpers shared by the step kernels.
+//
+// Smoothing kernels, cell hashing and the FP64 pair-distance test.  The
+// distance and cell arithmetic are written with explicit round-to-nearest
+// intrinsics so that no FMA contraction happens: neighbour sets and cell
+// indices then agree bit for bit with a plain IEEE evaluation of
+//   sqrt((xi-xj)*(xi-xj)+(yi-yj)*(yi-yj)+(zi-zj)*(zi-zj))
+//   min(floor((x-xmin)/(xmax-xmin)*NI), NI-1), clamped at 0
+// (functions_NNPS.cuh:774-784, e.g. functions_PPE2.cuh:629).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SPHDEM_NSLOT 16
+
+namespace sphdem {
+
+// Constants that travel with every launch.  Copied from SphdemParams plus
+// the grid computed at commit time.
+struct DevParams {
+    int kernel_type, dim, kgc, delsph, fp, fv, fva, fg, con, xsph, open_bc, rho_type;
+    int NI, NJ, NK, num_cells;
+    int ns, nd, nb_cap;
+    int nwall, nbuf;          // static counts of wall (p_type<=0) and open-boundary buffer particles
+    int wall_mask;
+    int sph_lagrangian;
+    double kappa, dt, sdt, soundspeed, u_limit, c_xsph;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double rho_gas, rho_liquid, mu_gas, mu_liquid, nu_gas, g_sph, g_dem, h_over_dx;
+    double k_sph, cp_sph, k_dem, cp_dem;
+    double G, nu_p, damp, fric, r_contact, r_search;
+    double inlet_uz, inlet_temp, L2, L3, ball_vel;
+    double cyl_cx, cyl_cy, cyl_r;
+    double box_c[3], box_L[3];
+    double cone_c[3], cone_r1, cone_r2, cone_h;
+    double rest_n, rest_s, mu_s, mu_rs;
+};
+
+// ---- cell index ---------------------------------------------------------
+__device__ __forceinline__ int cell_coord(double v, double vmin, double vmax, int N) {
+    if (vmax == vmin) return 0;
+    double f = floor(__dmul_rn(__ddiv_rn(__dsub_rn(v, vmin), __dsub_rn(vmax, vmin)), (double)N));
+    double r = (f < (double)(N - 1)) ? f : (double)(N - 1);
+    int c = (int)r;
+    return c < 0 ? 0 : c;
+}
+
+__device__ __forceinline__ void cell_ijk(const DevParams& P, double x, double y, double z, int& ic, int& jc, int& kc) {
+    ic = cell_coord(x, P.xmin, P.xmax, P.NI);
+    jc = cell_coord(y, P.ymin, P.ymax, P.NJ);
+    kc = cell_coord(z, P.zmin, P.zmax, P.NK);
+}
+
+// reference predicate distance, no contraction
+__device__ __forceinline__ double pair_dist(double xi, double yi, double zi, double xj, double yj, double zj) {
+    double dx = __dsub_rn(xi, xj), dy = __dsub_rn(yi, yj), dz = __dsub_rn(zi, zj);
+    double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return __dsqrt_rn(d2);
+}
+
+// ---- smoothing kernels (functions_KNL.cuh:2-144) -----------------------
+// Wendland normalisations use the literal constants of the reference.
+template <typename R>
+__device__ __forceinline__ R knl_tmpA(int kt, int dim, R tH) {
+    const R PI_REF = (R)3.141592653;
+    if (dim == 3) {
+        switch (kt) {
+        case 0: return (R)1.0 / (pow(PI_REF, (R)1.5) * tH * tH * tH);
+        case 1: return (R)3.0 / ((R)359.0 * PI_REF * tH * tH * tH);
+        case 2: return (R)315.0 / ((R)208.0 * PI_REF * tH * tH * tH);
+        case 3: return (R)3.342253804929802 / ((R)8 * tH * tH * tH);
+        case 4: return (R)4.923856051905513 / ((R)8 * tH * tH * tH);
+        case 5: return (R)6.788953041263660 / ((R)8 * tH * tH * tH);
+        }
+    } else {
+        switch (kt) {
+        case 0: return (R)1.0 / (PI_REF * tH * tH);
+        case 1: return (R)7.0 / ((R)478.0 * PI_REF * tH * tH);
+        case 2: return (R)15.0 / ((R)7.0 * PI_REF * tH * tH);
+        case 3: return (R)2.228169203286535 / ((R)4 * tH * tH);
+        case 4: return (R)2.864788975654116 / ((R)4 * tH * tH);
+        case 5: return (R)3.546881588905096 / ((R)4 * tH * tH);
+        }
+    }
+    return (R)0;
+}
+
+template <typename R>
+__device__ __forceinline__ R ipow(R b, int e) {
+    R r = (R)1;
+    for (int k = 0; k < e; k++) r *= b;
+    return r;
+}
+
+template <typename R>
+__device__ __forceinline__ R knl_w(int kt, R tA, R tH, R rr) {
+    R tR;
+    switch (kt) {
+    case 5: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR, a2 = a * a, a4 = a2 * a2;
+        return tA * a4 * a4 * ((R)1 + (R)8 * tR + (R)25 * tR * tR + (R)32 * tR * tR * tR);
+    }
+    case 3: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR, a2 = a * a;
+        return tA * a2 * a2 * ((R)1 + (R)4 * tR);
+    }
+    case 4: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR, a3 = a * a * a;
+        return tA * a3 * a3 * ((R)1 + (R)6 * tR + (R)11.666666666666666 * tR * tR);
+    }
+    case 0:
+        tR = rr / tH;
+        return tA * exp(-tR * tR);
+    case 1:
+        tR = rr / tH;
+        if (tR < (R)1) return tA * (ipow((R)3 - tR, 5) - (R)6 * ipow((R)2 - tR, 5) + (R)15 * ipow((R)1 - tR, 5));
+        if (tR < (R)2) return tA * (ipow((R)3 - tR, 5) - (R)6 * ipow((R)2 - tR, 5));
+        if (tR < (R)3) return tA * ipow((R)3 - tR, 5);
+        return (R)0;
+    case 2:
+        tR = rr / tH;
+        if (!(tR < (R)2)) return (R)0;
+        return tA * ((R)2 / (R)3 - (R)9 / (R)8 * tR * tR + (R)19 / (R)24 * tR * tR * tR - (R)5 / (R)32 * tR * tR * tR * tR);
+    }
+    return (R)0;
+}
+
+// dW/dr
+template <typename R>
+__device__ __forceinline__ R knl_dw(int kt, R tA, R tH, R rr) {
+    R tR;
+    switch (kt) {
+    case 5: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR, a2 = a * a, a4 = a2 * a2;
+        return ((R)1 / ((R)2 * tH)) * tA * ((R)-22 * tR * a4 * a2 * a * ((R)16 * tR * tR + (R)7 * tR + (R)1));
+    }
+    case 3: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR;
+        return ((R)1 / ((R)2 * tH)) * tA * ((R)-20 * tR * a * a * a);
+    }
+    case 4: {
+        tR = rr / tH * (R)0.5;
+        if (!(tR < (R)1)) return (R)0;
+        R a = (R)1 - tR, a2 = a * a;
+        return ((R)1 / ((R)2 * tH)) * tA * ((R)-18.666666666666668 * tR * a2 * a2 * a * ((R)5 * tR + (R)1));
+    }
+    case 0:
+        tR = rr / tH;
+        return ((R)1 / tH) * tA * (R)-2 * tR * exp(-tR * tR);
+    case 1:
+        tR = rr / tH;
+        if (tR < (R)1) return ((R)1 / tH) * tA * (ipow((R)3 - tR, 5) + (R)30 * ipow((R)2 - tR, 4) - (R)75 * ipow((R)1 - tR, 4));
+        if (tR < (R)2) return ((R)1 / tH) * tA * ((R)-5 * ipow((R)3 - tR, 4) + (R)30 * ipow((R)2 - tR, 4));
+        if (tR < (R)3) return ((R)1 / tH) * tA * ((R)-5 * ipow((R)3 - tR, 4));
+        return (R)0;
+    case 2:
+        tR = rr / tH;
+        if (!(tR < (R)2)) return (R)0;
+        return ((R)1 / tH) * tA * ((R)-9 / (R)8 * (R)2 * tR + (R)19 / (R)24 * (R)3 * tR * tR - (R)5 / (R)32 * (R)4 * tR * tR * tR);
+    }
+    return (R)0;
+}
+
+// ---- pair test with FP32 prefilter -------------------------------------
+// inside == (sqrt(dx^2+dy^2+dz^2) + add < Rr) evaluated exactly in FP64.
+// The FP32 build first compares the squared distance formed from the
+// float-rounded differences against Rr^2 (1 -/+ 1e-6); the relative error
+// of that square is below 3e-7, so only pairs inside that band need the
+// exact FP64 evaluation.  r is the pair distance in field precision.
+template <typename R>
+struct PairT {
+    R dx, dy, dz, r;
+    bool in;
+};
+
+template <typename R>
+__device__ __forceinline__ PairT<R> pair_test(double xi, double yi, double zi, double xj, double yj, double zj,
+                                              double Rr, double add, float r2lo, float r2hi);
+
+template <>
+__device__ __forceinline__ PairT<float> pair_test<float>(double xi, double yi, double zi, double xj, double yj,
+                                                         double zj, double Rr, double add, float r2lo, float r2hi) {
+    PairT<float> g;
+    g.dx = (float)(xi - xj);
+    g.dy = (float)(yi - yj);
+    g.dz = (float)(zi - zj);
+    float d2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+    if (d2 < r2lo) g.in = true;
+    else if (d2 > r2hi) g.in = false;
+    else g.in = __dadd_rn(pair_dist(xi, yi, zi, xj, yj, zj), add) < Rr;
+    g.r = sqrtf(d2);
+    return g;
+}
+
+template <>
+__device__ __forceinline__ PairT<double> pair_test<double>(double xi, double yi, double zi, double xj, double yj,
+                                                           double zj, double Rr, double add, float, float) {
+    PairT<double> g;
+    g.dx = xi - xj;
+    g.dy = yi - yj;
+    g.dz = zi - zj;
+    g.r = pair_dist(xi, yi, zi, xj, yj, zj);
+    g.in = __dadd_rn(g.r, add) < Rr;
+    return g;
+}
+
+__device__ __forceinline__ float r2_lo(double Rr) { return (float)(Rr * Rr * (1.0 - 1e-6)); }
+__device__ __forceinline__ float r2_hi(double Rr) { return (float)(Rr * Rr * (1.0 + 1e-6)); }
+
+// ---- stencil as 9 contiguous slot ranges --------------------------------
+// The three cells (ix-1..ix+1, jy, kz) have consecutive keys, so their
+// particles form one contiguous range of the cell-sorted arrays.  Visiting
+// the 9 (z,y) rows in order with ascending slots inside each row is the
+// reference's 27-cell visit order.
+template <typename F>
+__device__ __forceinline__ void for_stencil_rows(const DevParams& P, int ic, int jc, int kc, const int* __restrict__ gs,
+                                                 const int* __restrict__ ge, F f) {
+    int x0 = ic > 0 ? ic - 1 : 0, x1 = ic < P.NI - 1 ? ic + 1 : P.NI - 1;
+    for (int z = -1; z <= 1; z++) {
+        int kz = kc + z;
+        if (kz < 0 || kz > P.NK - 1) continue;
+        for (int y = -1; y <= 1; y++) {
+            int jy = jc + y;
+            if (jy < 0 || jy > P.NJ - 1) continue;
+            int base = P.NI * jy + P.NI * P.NJ * kz;
+            int lo = -1, hi = -1;
+            for (int ix = x0; ix <= x1; ix++) {
+                int s = gs[base + ix];
+                if (s == -1) continue;
+                if (lo < 0) lo = s;
+                hi = ge[base + ix];
+            }
+            if (lo >= 0) f(lo, hi);
+        }
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// one grid-stride-free 1-D launch helper
+__host__ __device__ inline int nblocks(int n, int t) { return n <= 0 ? 1 : (n + t - 1) / t; }
+
+}  // namespace sphdem

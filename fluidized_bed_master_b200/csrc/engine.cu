@@ -1,0 +1,991 @@
+// engine.cu -- host side of the B200 SPH-DEM step engine and its C ABI.
+//
+// The time loop of the reference (ISPH_Calc_seperate.cuh:905-975) calls
+// SOPHIA_single_ISPH once per step; sphdem_step does the same work as one
+// CUDA graph per step (captured once per step variant and replayed).
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "handle.h"
+#include "step_kernels.cuh"
+
+using namespace sphdem;
+
+#define CK(call)                                     \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return SPHDEM_E_CUDA; \
+    } while (0)
+
+static const int TPB = 128;
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Alloc {
+    std::vector<void*> ptrs;
+    bool ok = true;
+    template <typename T>
+    T* get(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+            ok = false;
+            return nullptr;
+        }
+        cudaMemset(p, 0, sizeof(T) * (n ? n : 1));
+        ptrs.push_back(p);
+        return (T*)p;
+    }
+};
+
+template <typename R>
+struct EngineHost {
+    Engine<R> E;
+    Alloc A;
+    int nb_cap = 0;
+    size_t list_elems = 0;
+};
+
+template <typename R>
+void alloc_sph_state(Alloc& A, SphState<R>& S, int n) {
+    S.x = A.get<double>(n); S.y = A.get<double>(n); S.z = A.get<double>(n); S.h = A.get<double>(n);
+    S.ux = A.get<R>(n); S.uy = A.get<R>(n); S.uz = A.get<R>(n);
+    S.m = A.get<R>(n); S.rho = A.get<R>(n); S.pres = A.get<R>(n); S.temp = A.get<R>(n);
+    S.dDEMpor = A.get<R>(n); S.flt_s = A.get<R>(n);
+    S.ptype = A.get<int>(n); S.btype = A.get<int>(n); S.itype = A.get<int>(n); S.pid = A.get<int>(n);
+}
+
+template <typename R>
+void alloc_dem_state(Alloc& A, DemState<R>& D, int n) {
+    D.x = A.get<double>(n); D.y = A.get<double>(n); D.z = A.get<double>(n); D.h = A.get<double>(n);
+    D.rad = A.get<double>(n);
+    D.ux = A.get<R>(n); D.uy = A.get<R>(n); D.uz = A.get<R>(n);
+    D.wx = A.get<R>(n); D.wy = A.get<R>(n); D.wz = A.get<R>(n);
+    D.m = A.get<R>(n); D.rho = A.get<R>(n); D.ri = A.get<R>(n);
+    D.temp = A.get<R>(n); D.temp1 = A.get<R>(n); D.temp2 = A.get<R>(n); D.temp3 = A.get<R>(n);
+    D.Fdx_df = A.get<R>(n); D.Fdy_df = A.get<R>(n); D.Fdz_df = A.get<R>(n); D.Q_sd = A.get<R>(n);
+    D.ptype = A.get<int>(n); D.btype = A.get<int>(n); D.itype = A.get<int>(n); D.pid = A.get<int>(n);
+    D.dem_idx = A.get<int>(n);
+    D.hid = A.get<int>((size_t)n * SPHDEM_NSLOT);
+    D.hds = A.get<double>((size_t)n * SPHDEM_NSLOT * 3);
+}
+
+template <typename R>
+void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int ncells) {
+    W.m_new = A.get<R>(ns); W.rho_new = A.get<R>(ns); W.rho_ref = A.get<R>(ns); W.DEMpor = A.get<R>(ns);
+    W.dDEMpor_prev = A.get<R>(ns);
+    W.Cm = A.get<R>((size_t)ns * 9);
+    W.ftx = A.get<R>(ns); W.fty = A.get<R>(ns); W.ftz = A.get<R>(ns); W.ftot = A.get<R>(ns);
+    W.fpx = A.get<R>(ns); W.fpy = A.get<R>(ns); W.fpz = A.get<R>(ns);
+    W.pgfx = A.get<R>(ns); W.pgfy = A.get<R>(ns); W.pgfz = A.get<R>(ns);
+    W.dtemp = A.get<R>(ns); W.temp0 = A.get<R>(ns);
+    W.ux0 = A.get<R>(ns); W.uy0 = A.get<R>(ns); W.uz0 = A.get<R>(ns);
+    W.p_new = A.get<R>(ns);
+    W.u_tmpx = A.get<R>(ns); W.u_tmpy = A.get<R>(ns); W.u_tmpz = A.get<R>(ns); W.temp_tmp = A.get<R>(ns);
+    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
+    W.g_str = A.get<int>(ncells + 1); W.g_end = A.get<int>(ncells + 1);
+    W.ncnt = A.get<int>(ns);
+    W.wall_idx = A.get<int>(ns); W.buf_idx = A.get<int>(ns); W.counters = A.get<int>(4);
+    W.nbr = nullptr;
+    DW.flt_s = A.get<R>(nd); DW.flt_sd = A.get<R>(nd); DW.flt_sd2 = A.get<R>(nd); DW.DEMpor = A.get<R>(nd);
+    DW.ftx = A.get<R>(nd); DW.fty = A.get<R>(nd); DW.ftz = A.get<R>(nd);
+    DW.tqx = A.get<R>(nd); DW.tqy = A.get<R>(nd); DW.tqz = A.get<R>(nd);
+    DW.dtemp = A.get<R>(nd); DW.dtemp1 = A.get<R>(nd); DW.dtemp2 = A.get<R>(nd); DW.dtemp3 = A.get<R>(nd);
+    DW.Fdx_b = A.get<R>(nd); DW.Fdy_b = A.get<R>(nd); DW.Fdz_b = A.get<R>(nd);
+    DW.Fdx_da = A.get<R>(nd); DW.Fdy_da = A.get<R>(nd); DW.Fdz_da = A.get<R>(nd);
+    DW.ux0 = A.get<R>(nd); DW.uy0 = A.get<R>(nd); DW.uz0 = A.get<R>(nd); DW.temp0 = A.get<R>(nd);
+    DW.magf = A.get<R>(nd);
+    DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = A.get<int>(nd); DW.val_out = A.get<int>(nd);
+    DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
+}
+
+int key_bits(int num_cells) {
+    int b = 1;
+    while ((1ll << b) <= (long long)num_cells) b++;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device field transfer (conversion R <-> double on the host)
+// ---------------------------------------------------------------------------
+template <typename R>
+int upload_real(R* dst, const double* src, int n, cudaStream_t s) {
+    std::vector<R> tmp(n);
+    for (int i = 0; i < n; i++) tmp[i] = (R)src[i];
+    CK(cudaMemcpyAsync(dst, tmp.data(), sizeof(R) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return SPHDEM_OK;
+}
+template <typename R>
+int download_real(double* dst, const R* src, int n, cudaStream_t s) {
+    std::vector<R> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), src, sizeof(R) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; i++) dst[i] = (double)tmp[i];
+    return SPHDEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// NNPS for one set; writes the sorted state into dst.
+// ---------------------------------------------------------------------------
+template <typename R>
+int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) {
+    Engine<R>& E = EH->E;
+    DevParams& P = E.P;
+    SphWork<R>& W = E.sw;
+    cudaStream_t st = H->stream;
+    int n = P.ns;
+    if (n == 0) return SPHDEM_OK;
+    SphState<R>& S = E.S[src];
+    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    size_t bytes = E.sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
+                                       key_bits(P.num_cells), st));
+    CK(cudaMemsetAsync(W.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
+    CK(cudaMemsetAsync(W.counters, 0, sizeof(int) * 4, st));
+    SphGatherSrc<R> g;
+    if (P.xsph) { g.ux = W.u_tmpx; g.uy = W.u_tmpy; g.uz = W.u_tmpz; g.temp = W.temp_tmp; }
+    else { g.ux = S.ux; g.uy = S.uy; g.uz = S.uz; g.temp = S.temp; }
+    g.m = W.m_new; g.rho = W.rho_new; g.pres = W.p_new;
+    k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.key_out, W.val_out, W.g_str, W.g_end,
+                                                            W.wall_idx, W.buf_idx, W.counters);
+    *nl += 3;
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+template <typename R>
+int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) {
+    Engine<R>& E = EH->E;
+    DevParams& P = E.P;
+    DemWork<R>& DW = E.dw;
+    cudaStream_t st = H->stream;
+    int n = P.nd;
+    CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
+    if (n == 0) return SPHDEM_OK;
+    DemState<R>& D = E.D[src];
+    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, DW.val_in);
+    size_t bytes = E.sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, DW.key_in, DW.key_out, DW.val_in, DW.val_out, n, 0,
+                                       key_bits(P.num_cells), st));
+    k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str, DW.g_end);
+    *nl += 3;
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one step (SOPHIA_single_ISPH order).  flags: bit1 count==0, bit2 filter
+// step, bit3 time==0.
+// ---------------------------------------------------------------------------
+enum { F_COUNT0 = 2, F_FILT = 4, F_TIME0 = 8 };
+
+template <typename R>
+int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
+    Engine<R>& E = EH->E;
+    DevParams& P = E.P;
+    SphWork<R>& W = E.sw;
+    DemWork<R>& DW = E.dw;
+    cudaStream_t st = H->stream;
+    int ns = P.ns, nd = P.nd;
+    int so = E.cur_s, sn = 1 - E.cur_s, dox = E.cur_d, dn = 1 - E.cur_d;
+    int r;
+    if ((r = nnps_sph<R>(H, EH, so, sn, nl))) return r;
+    if ((r = nnps_dem<R>(H, EH, dox, dn, nl))) return r;
+    SphState<R>& S = E.S[sn];
+    DemState<R>& D = E.D[dn];
+    int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
+    int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
+    if (ns > 0) {
+        k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.g_str, W.g_end, W.nbr, W.ncnt, E.flags);
+        k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.g_str, DW.g_end);
+        *nl += 2;
+    }
+    if (nd > 0) {
+        k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, D, DW, W.g_str, W.g_end, DW.g_str, DW.g_end);
+        *nl += 1;
+    }
+    if (ns > 0) {
+        k_passB<R><<<bs, TPB, 0, st>>>(P, S, W, (flags & F_FILT) ? 1 : 0);
+        *nl += 1;
+    }
+    if (nd > 0) {
+        k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.g_str, DW.g_end, E.flags);
+        k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.g_str, W.g_end);
+        *nl += 2;
+    }
+    if (ns > 0) {
+        k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.g_str, DW.g_end, (flags & F_TIME0) ? 1 : 0);
+        if (flags & F_COUNT0) {
+            k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.g_str, W.g_end);
+            *nl += 1;
+        }
+        k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W);
+        k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.g_str, W.g_end);
+        k_passC<R><<<bs, TPB, 0, st>>>(P, S, W);
+        *nl += 4;
+    }
+    if (nd > 0) {
+        k_dem_update<R><<<bd, TPB, 0, st>>>(P, D, DW);
+        *nl += 1;
+    }
+    if (ns > 0) {
+        if (P.open_bc > 0) {
+            k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.g_str, W.g_end);
+            *nl += 1;
+        }
+        if (P.xsph) {
+            k_xsph<R><<<bs, TPB, 0, st>>>(P, S, W);
+            *nl += 1;
+        }
+    }
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+template <typename R>
+int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
+    Engine<R>& E = EH->E;
+    int flags = 0;
+    if (H->count == 0) flags |= F_COUNT0;
+    if (H->count % (H->p.freq_filt * H->p.decouple_stride) == 0) flags |= F_FILT;
+    if (H->time == 0.0) flags |= F_TIME0;
+    int key = flags | (E.cur_s << 8) | (E.cur_d << 9);
+    int64_t n = 0;
+    if (H->use_graphs) {
+        auto it = H->graphs.find(key);
+        if (it == H->graphs.end()) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
+            int r = enqueue_step<R>(H, EH, flags, &n);
+            cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
+            if (r) return r;
+            if (ce != cudaSuccess) return SPHDEM_E_CUDA;
+            cudaGraphExec_t ge;
+            CK(cudaGraphInstantiate(&ge, g, 0));
+            cudaGraphDestroy(g);
+            H->graphs[key] = ge;
+            H->graph_launches[key] = n;
+            it = H->graphs.find(key);
+        }
+        n = H->graph_launches[key];
+        CK(cudaGraphLaunch(it->second, H->stream));
+    } else {
+        int r = enqueue_step<R>(H, EH, flags, &n);
+        if (r) return r;
+    }
+    *nl += n;
+    E.cur_s ^= 1;
+    E.cur_d ^= 1;
+    return SPHDEM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// commit: domain, grid, buffer tags, upload, list capacity
+// ---------------------------------------------------------------------------
+template <typename R>
+static int commit_t(SphdemHandle* H) {
+    const SphdemParams& p = H->p;
+    int ns = H->ns, nd = H->nd;
+    // bounding box: find_minmax (function_init.cuh:913-950) over the rows in
+    // file order, stopping one row short (the reference loop bound)
+    std::vector<double> fx, fy, fz;
+    double h0;
+    if (H->have_file_order) {
+        fx = H->file_x; fy = H->file_y; fz = H->file_z; h0 = H->file_h0;
+    } else {
+        auto& sx = H->stage_d[0][SPHDEM_F_X];
+        auto& sy = H->stage_d[0][SPHDEM_F_Y];
+        auto& sz = H->stage_d[0][SPHDEM_F_Z];
+        auto& dx = H->stage_d[1][SPHDEM_F_X];
+        auto& dy = H->stage_d[1][SPHDEM_F_Y];
+        auto& dz = H->stage_d[1][SPHDEM_F_Z];
+        fx = sx; fx.insert(fx.end(), dx.begin(), dx.end());
+        fy = sy; fy.insert(fy.end(), dy.begin(), dy.end());
+        fz = sz; fz.insert(fz.end(), dz.begin(), dz.end());
+        h0 = ns > 0 ? H->stage_d[0][SPHDEM_F_H][0] : H->stage_d[1][SPHDEM_F_H][0];
+    }
+    int n = (int)fx.size();
+    double mnx = fx[0], mxx = fx[0], mny = fy[0], mxy = fy[0], mnz = fz[0], mxz = fz[0];
+    for (int k = 0; k < n - 1; k++) {
+        mnx = std::min(mnx, fx[k]); mxx = std::max(mxx, fx[k]);
+        mny = std::min(mny, fy[k]); mxy = std::max(mxy, fy[k]);
+        mnz = std::min(mnz, fz[k]); mxz = std::max(mxz, fz[k]);
+    }
+    mnx -= (mxx - mnx) * p.margin[0]; mxx += (mxx - mnx) * p.margin[1];
+    mny -= (mxy - mny) * p.margin[2]; mxy += (mxy - mny) * p.margin[3];
+    mnz -= (mxz - mnz) * p.margin[4]; mxz += (mxz - mnz) * p.margin[5];
+    double dcell = 1.1 * p.kappa * h0;
+    int NI = (int)((mxx - mnx) / dcell) + 1, NJ = (int)((mxy - mny) / dcell) + 1, NK = (int)((mxz - mnz) / dcell) + 1;
+    if (!(dcell > 0) || NI <= 0 || NJ <= 0 || NK <= 0 || (double)NI * NJ * NK > 2.0e9) return SPHDEM_E_INPUT;
+    H->bbox[0] = mnx; H->bbox[1] = mxx; H->bbox[2] = mny; H->bbox[3] = mxy; H->bbox[4] = mnz; H->bbox[5] = mxz;
+    H->nijk[0] = NI; H->nijk[1] = NJ; H->nijk[2] = NK;
+    H->dcell = dcell;
+    int num_cells = NI * NJ * NK + 1;
+
+    EngineHost<R>* EH = new EngineHost<R>();
+    H->eng = EH;
+    Engine<R>& E = EH->E;
+    DevParams& P = E.P;
+    std::memset(&P, 0, sizeof(P));
+    P.kernel_type = p.kernel_type; P.dim = p.dim; P.kgc = p.kgc_solve; P.delsph = p.delSPH_solve;
+    P.fp = p.fp_solve; P.fv = p.fv_solve; P.fva = p.fva_solve; P.fg = p.fg_solve; P.con = p.con_solve;
+    P.xsph = p.xsph_solve; P.open_bc = p.open_boundary; P.rho_type = p.rho_type;
+    P.NI = NI; P.NJ = NJ; P.NK = NK; P.num_cells = num_cells;
+    P.ns = ns; P.nd = nd;
+    P.wall_mask = p.dem_wall_mask;
+    P.sph_lagrangian = 0;   // KERNEL_set_alpha_sph: SPH particles are Eulerian (functions_ALE.cuh:26-47)
+    P.kappa = p.kappa; P.dt = p.dt; P.sdt = p.decouple_stride * p.dt; P.soundspeed = p.soundspeed;
+    P.u_limit = p.u_limit; P.c_xsph = p.c_xsph;
+    P.xmin = mnx; P.xmax = mxx; P.ymin = mny; P.ymax = mxy; P.zmin = mnz; P.zmax = mxz;
+    P.rho_gas = p.rho_gas; P.rho_liquid = p.rho_liquid; P.mu_gas = p.mu_gas; P.mu_liquid = p.mu_liquid;
+    P.nu_gas = p.nu_gas; P.g_sph = p.g_sph; P.g_dem = p.g_dem; P.h_over_dx = p.h_over_dx;
+    P.k_sph = p.k_sph; P.cp_sph = p.cp_sph; P.k_dem = p.k_dem; P.cp_dem = p.cp_dem;
+    P.G = p.dem_shear_modulus; P.nu_p = p.dem_poisson; P.damp = p.dem_damp_coef; P.fric = p.dem_friction_ratio;
+    P.r_contact = p.dem_contact_range; P.r_search = p.dem_search_range;
+    P.inlet_uz = p.inlet_uz_mirror; P.inlet_temp = p.inlet_temp; P.L2 = p.obc_L2; P.L3 = p.obc_L3;
+    P.ball_vel = p.ball_vel;
+    P.cyl_cx = p.cyl_cx; P.cyl_cy = p.cyl_cy; P.cyl_r = p.cyl_r;
+    for (int k = 0; k < 3; k++) { P.box_c[k] = p.box_c[k]; P.box_L[k] = p.box_L[k]; P.cone_c[k] = p.cone_c[k]; }
+    P.cone_r1 = p.cone_r1; P.cone_r2 = p.cone_r2; P.cone_h = p.cone_h;
+    P.rest_n = p.wall_rest_n; P.rest_s = p.wall_rest_s; P.mu_s = p.wall_mu_s; P.mu_rs = p.wall_mu_rs;
+
+    Alloc& A = EH->A;
+    alloc_sph_state<R>(A, E.S[0], ns); alloc_sph_state<R>(A, E.S[1], ns);
+    alloc_dem_state<R>(A, E.D[0], nd); alloc_dem_state<R>(A, E.D[1], nd);
+    alloc_work<R>(A, E.sw, E.dw, ns, nd, num_cells);
+    E.flags = A.get<DevFlags>(1);
+    E.red_buf = A.get<double>(8);
+    if (!A.ok) return SPHDEM_E_NOMEM;
+    E.cur_s = 0; E.cur_d = 0;
+    // CUB temporary storage, sized for the larger set
+    {
+        size_t b1 = 0, b2 = 0;
+        int nmax = std::max(ns, nd);
+        cub::DeviceRadixSort::SortPairs(nullptr, b1, E.sw.key_in, E.sw.key_out, E.sw.val_in, E.sw.val_out,
+                                        std::max(nmax, 1), 0, key_bits(num_cells), H->stream);
+        (void)b2;
+        E.sort_tmp_bytes = b1;
+        E.sort_tmp = A.get<char>(b1);
+        if (!A.ok) return SPHDEM_E_NOMEM;
+    }
+    // buffer tags (c_initial_inner_outer_particle_single_{sph,dem}, functions_NNPS.cuh:60-200)
+    for (int q = 0; q < 2; q++) {
+        int nq = q ? nd : ns;
+        std::vector<int> itype(nq, 1), btype(nq, 0), pid(nq);
+        auto& pt = H->stage_i[q][SPHDEM_F_PTYPE];
+        auto& zz = H->stage_d[q][SPHDEM_F_Z];
+        for (int i = 0; i < nq; i++) {
+            pid[i] = i;
+            if (p.open_boundary > 0 && pt[i] < 1000 && pt[i] >= 1) {
+                if (zz[i] >= (p.obc_L1 - 1e-6) && (zz[i] < p.obc_L2 - 1e-6)) { btype[i] = 1; itype[i] = 2; }
+                if (zz[i] >= (p.obc_L3 - 1e-6) && (zz[i] < p.obc_L4 - 1e-6)) { btype[i] = 2; itype[i] = 2; }
+            }
+        }
+        H->stage_i[q][SPHDEM_F_ITYPE] = itype;
+        H->stage_i[q][SPHDEM_F_BUFFER_TYPE] = btype;
+        H->stage_i[q][SPHDEM_F_PID] = pid;
+    }
+    {
+        auto& pt = H->stage_i[0][SPHDEM_F_PTYPE];
+        auto& bt = H->stage_i[0][SPHDEM_F_BUFFER_TYPE];
+        int nw = 0, nb = 0;
+        for (int i = 0; i < ns; i++) {
+            if (pt[i] <= 0) nw++;
+            if (bt[i] > 0 && pt[i] < 1000) nb++;
+        }
+        P.nwall = nw;
+        P.nbuf = nb;
+    }
+    // DEM ids must be unique and >= 1: the contact history stores partner
+    // ids and treats id < 1 as a free slot (functions_DEM_INTERACTION2.cuh:1326)
+    if (nd > 0) {
+        auto& id = H->stage_i[1][SPHDEM_F_DEM_IDX];
+        std::set<int> seen;
+        for (int v : id) {
+            if (v < 1 || !seen.insert(v).second) return SPHDEM_E_INPUT;
+        }
+    }
+    cudaStream_t st = H->stream;
+    auto up_d = [&](double* dst, int q, int f, int nq) -> int {
+        auto& v = H->stage_d[q][f];
+        if ((int)v.size() != nq) v.assign(nq, 0.0);
+        if (nq) CK(cudaMemcpyAsync(dst, v.data(), sizeof(double) * nq, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return SPHDEM_OK;
+    };
+    auto up_r = [&](R* dst, int q, int f, int nq) -> int {
+        auto& v = H->stage_d[q][f];
+        if ((int)v.size() != nq) v.assign(nq, 0.0);
+        return nq ? upload_real<R>(dst, v.data(), nq, st) : SPHDEM_OK;
+    };
+    auto up_i = [&](int* dst, int q, int f, int nq) -> int {
+        auto& v = H->stage_i[q][f];
+        if ((int)v.size() != nq) v.assign(nq, 0);
+        if (nq) CK(cudaMemcpyAsync(dst, v.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return SPHDEM_OK;
+    };
+    int r = 0;
+    SphState<R>& S = E.S[0];
+    SphWork<R>& W = E.sw;
+    r |= up_d(S.x, 0, SPHDEM_F_X, ns); r |= up_d(S.y, 0, SPHDEM_F_Y, ns); r |= up_d(S.z, 0, SPHDEM_F_Z, ns);
+    r |= up_d(S.h, 0, SPHDEM_F_H, ns);
+    r |= up_r(S.ux, 0, SPHDEM_F_UX, ns); r |= up_r(S.uy, 0, SPHDEM_F_UY, ns); r |= up_r(S.uz, 0, SPHDEM_F_UZ, ns);
+    r |= up_r(S.m, 0, SPHDEM_F_M, ns); r |= up_r(S.rho, 0, SPHDEM_F_RHO, ns); r |= up_r(S.pres, 0, SPHDEM_F_PRES, ns);
+    r |= up_r(S.temp, 0, SPHDEM_F_TEMP, ns); r |= up_r(S.flt_s, 0, SPHDEM_F_FLT_S, ns);
+    r |= up_r(S.dDEMpor, 0, SPHDEM_F_DDEMPOR, ns);
+    r |= up_i(S.ptype, 0, SPHDEM_F_PTYPE, ns); r |= up_i(S.btype, 0, SPHDEM_F_BUFFER_TYPE, ns);
+    r |= up_i(S.itype, 0, SPHDEM_F_ITYPE, ns); r |= up_i(S.pid, 0, SPHDEM_F_PID, ns);
+    // end-of-step copies the reorder reads from
+    r |= up_r(W.m_new, 0, SPHDEM_F_M, ns); r |= up_r(W.rho_new, 0, SPHDEM_F_RHO, ns);
+    r |= up_r(W.p_new, 0, SPHDEM_F_PRES, ns);
+    r |= up_r(W.u_tmpx, 0, SPHDEM_F_UX, ns); r |= up_r(W.u_tmpy, 0, SPHDEM_F_UY, ns);
+    r |= up_r(W.u_tmpz, 0, SPHDEM_F_UZ, ns); r |= up_r(W.temp_tmp, 0, SPHDEM_F_TEMP, ns);
+    DemState<R>& D = E.D[0];
+    r |= up_d(D.x, 1, SPHDEM_F_X, nd); r |= up_d(D.y, 1, SPHDEM_F_Y, nd); r |= up_d(D.z, 1, SPHDEM_F_Z, nd);
+    r |= up_d(D.h, 1, SPHDEM_F_H, nd); r |= up_d(D.rad, 1, SPHDEM_F_RAD, nd);
+    r |= up_r(D.ux, 1, SPHDEM_F_UX, nd); r |= up_r(D.uy, 1, SPHDEM_F_UY, nd); r |= up_r(D.uz, 1, SPHDEM_F_UZ, nd);
+    r |= up_r(D.wx, 1, SPHDEM_F_WX, nd); r |= up_r(D.wy, 1, SPHDEM_F_WY, nd); r |= up_r(D.wz, 1, SPHDEM_F_WZ, nd);
+    r |= up_r(D.m, 1, SPHDEM_F_M, nd); r |= up_r(D.rho, 1, SPHDEM_F_RHO, nd); r |= up_r(D.ri, 1, SPHDEM_F_RI, nd);
+    r |= up_r(D.temp, 1, SPHDEM_F_TEMP, nd); r |= up_r(D.temp1, 1, SPHDEM_F_TEMP1, nd);
+    r |= up_r(D.temp2, 1, SPHDEM_F_TEMP2, nd); r |= up_r(D.temp3, 1, SPHDEM_F_TEMP3, nd);
+    r |= up_r(D.Fdx_df, 1, SPHDEM_F_FDX_DF, nd); r |= up_r(D.Fdy_df, 1, SPHDEM_F_FDY_DF, nd);
+    r |= up_r(D.Fdz_df, 1, SPHDEM_F_FDZ_DF, nd); r |= up_r(D.Q_sd, 1, SPHDEM_F_Q_SD, nd);
+    r |= up_i(D.ptype, 1, SPHDEM_F_PTYPE, nd); r |= up_i(D.btype, 1, SPHDEM_F_BUFFER_TYPE, nd);
+    r |= up_i(D.itype, 1, SPHDEM_F_ITYPE, nd); r |= up_i(D.pid, 1, SPHDEM_F_PID, nd);
+    r |= up_i(D.dem_idx, 1, SPHDEM_F_DEM_IDX, nd);
+    if (r) return SPHDEM_E_CUDA;
+    // neighbour-list capacity from an exact count on the sorted input
+    if (ns > 0) {
+        int64_t nl = 0;
+        P.nb_cap = 0;
+        if ((r = nnps_sph<R>(H, EH, 0, 1, &nl))) return r;
+        k_build_list<R><<<nblocks(ns, TPB), TPB, 0, st>>>(P, E.S[1], W.g_str, W.g_end, nullptr, W.ncnt, E.flags);
+        CK(cudaGetLastError());
+        DevFlags f;
+        CK(cudaMemcpyAsync(&f, E.flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int cap = std::max(32, ((int)(f.max_ncnt * 1.25) + 16 + 7) / 8 * 8);
+        P.nb_cap = cap;
+        EH->nb_cap = cap;
+        W.nbr = A.get<int>((size_t)cap * ns);
+        if (!A.ok) return SPHDEM_E_NOMEM;
+        CK(cudaMemsetAsync(E.flags, 0, sizeof(DevFlags), st));
+        CK(cudaStreamSynchronize(st));
+    }
+    H->committed = true;
+    return SPHDEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// field access
+// ---------------------------------------------------------------------------
+template <typename R>
+static int field_ptr(SphdemHandle* H, int which, int field, const void** ptr, int* kind) {
+    // kind: 0 double, 1 R, 2 int
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    Engine<R>& E = EH->E;
+    const DevParams& P = E.P;
+    if (which == SPHDEM_SPH) {
+        SphState<R>& S = E.S[E.cur_s];
+        SphWork<R>& W = E.sw;
+        bool xs = P.xsph;
+        switch (field) {
+        case SPHDEM_F_X: *ptr = S.x; *kind = 0; return 0;
+        case SPHDEM_F_Y: *ptr = S.y; *kind = 0; return 0;
+        case SPHDEM_F_Z: *ptr = S.z; *kind = 0; return 0;
+        case SPHDEM_F_H: *ptr = S.h; *kind = 0; return 0;
+        case SPHDEM_F_UX: *ptr = xs ? W.u_tmpx : S.ux; *kind = 1; return 0;
+        case SPHDEM_F_UY: *ptr = xs ? W.u_tmpy : S.uy; *kind = 1; return 0;
+        case SPHDEM_F_UZ: *ptr = xs ? W.u_tmpz : S.uz; *kind = 1; return 0;
+        case SPHDEM_F_TEMP: *ptr = xs ? W.temp_tmp : S.temp; *kind = 1; return 0;
+        case SPHDEM_F_M: *ptr = W.m_new; *kind = 1; return 0;
+        case SPHDEM_F_RHO: *ptr = W.rho_new; *kind = 1; return 0;
+        case SPHDEM_F_PRES: *ptr = W.p_new; *kind = 1; return 0;
+        case SPHDEM_F_DEMPOR: *ptr = W.DEMpor; *kind = 1; return 0;
+        case SPHDEM_F_DDEMPOR: *ptr = S.dDEMpor; *kind = 1; return 0;
+        case SPHDEM_F_FLT_S: *ptr = S.flt_s; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALX: *ptr = W.ftx; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALY: *ptr = W.fty; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALZ: *ptr = W.ftz; *kind = 1; return 0;
+        case SPHDEM_F_FPX: *ptr = W.fpx; *kind = 1; return 0;
+        case SPHDEM_F_FPY: *ptr = W.fpy; *kind = 1; return 0;
+        case SPHDEM_F_FPZ: *ptr = W.fpz; *kind = 1; return 0;
+        case SPHDEM_F_PGFX: *ptr = W.pgfx; *kind = 1; return 0;
+        case SPHDEM_F_PGFY: *ptr = W.pgfy; *kind = 1; return 0;
+        case SPHDEM_F_PGFZ: *ptr = W.pgfz; *kind = 1; return 0;
+        case SPHDEM_F_RHO_REF: *ptr = W.rho_ref; *kind = 1; return 0;
+        case SPHDEM_F_DTEMP: *ptr = W.dtemp; *kind = 1; return 0;
+        case SPHDEM_F_PTYPE: *ptr = S.ptype; *kind = 2; return 0;
+        case SPHDEM_F_ITYPE: *ptr = S.itype; *kind = 2; return 0;
+        case SPHDEM_F_BUFFER_TYPE: *ptr = S.btype; *kind = 2; return 0;
+        case SPHDEM_F_PID: *ptr = S.pid; *kind = 2; return 0;
+        case SPHDEM_F_CELL: *ptr = W.key_out; *kind = 2; return 0;
+        }
+    } else {
+        DemState<R>& D = E.D[E.cur_d];
+        DemWork<R>& DW = E.dw;
+        switch (field) {
+        case SPHDEM_F_X: *ptr = D.x; *kind = 0; return 0;
+        case SPHDEM_F_Y: *ptr = D.y; *kind = 0; return 0;
+        case SPHDEM_F_Z: *ptr = D.z; *kind = 0; return 0;
+        case SPHDEM_F_H: *ptr = D.h; *kind = 0; return 0;
+        case SPHDEM_F_RAD: *ptr = D.rad; *kind = 0; return 0;
+        case SPHDEM_F_UX: *ptr = D.ux; *kind = 1; return 0;
+        case SPHDEM_F_UY: *ptr = D.uy; *kind = 1; return 0;
+        case SPHDEM_F_UZ: *ptr = D.uz; *kind = 1; return 0;
+        case SPHDEM_F_WX: *ptr = D.wx; *kind = 1; return 0;
+        case SPHDEM_F_WY: *ptr = D.wy; *kind = 1; return 0;
+        case SPHDEM_F_WZ: *ptr = D.wz; *kind = 1; return 0;
+        case SPHDEM_F_M: *ptr = D.m; *kind = 1; return 0;
+        case SPHDEM_F_RHO: *ptr = D.rho; *kind = 1; return 0;
+        case SPHDEM_F_RI: *ptr = D.ri; *kind = 1; return 0;
+        case SPHDEM_F_TEMP: *ptr = D.temp; *kind = 1; return 0;
+        case SPHDEM_F_TEMP1: *ptr = D.temp1; *kind = 1; return 0;
+        case SPHDEM_F_TEMP2: *ptr = D.temp2; *kind = 1; return 0;
+        case SPHDEM_F_TEMP3: *ptr = D.temp3; *kind = 1; return 0;
+        case SPHDEM_F_FDX_DF: *ptr = D.Fdx_df; *kind = 1; return 0;
+        case SPHDEM_F_FDY_DF: *ptr = D.Fdy_df; *kind = 1; return 0;
+        case SPHDEM_F_FDZ_DF: *ptr = D.Fdz_df; *kind = 1; return 0;
+        case SPHDEM_F_Q_SD: *ptr = D.Q_sd; *kind = 1; return 0;
+        case SPHDEM_F_DEMPOR: *ptr = DW.DEMpor; *kind = 1; return 0;
+        case SPHDEM_F_FLT_S: *ptr = DW.flt_s; *kind = 1; return 0;
+        case SPHDEM_F_FLT_SD: *ptr = DW.flt_sd; *kind = 1; return 0;
+        case SPHDEM_F_FLT_SD2: *ptr = DW.flt_sd2; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALX: *ptr = DW.ftx; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALY: *ptr = DW.fty; *kind = 1; return 0;
+        case SPHDEM_F_FTOTALZ: *ptr = DW.ftz; *kind = 1; return 0;
+        case SPHDEM_F_TORQX: *ptr = DW.tqx; *kind = 1; return 0;
+        case SPHDEM_F_TORQY: *ptr = DW.tqy; *kind = 1; return 0;
+        case SPHDEM_F_TORQZ: *ptr = DW.tqz; *kind = 1; return 0;
+        case SPHDEM_F_DTEMP: *ptr = DW.dtemp; *kind = 1; return 0;
+        case SPHDEM_F_PTYPE: *ptr = D.ptype; *kind = 2; return 0;
+        case SPHDEM_F_ITYPE: *ptr = D.itype; *kind = 2; return 0;
+        case SPHDEM_F_BUFFER_TYPE: *ptr = D.btype; *kind = 2; return 0;
+        case SPHDEM_F_PID: *ptr = D.pid; *kind = 2; return 0;
+        case SPHDEM_F_DEM_IDX: *ptr = D.dem_idx; *kind = 2; return 0;
+        case SPHDEM_F_CELL: *ptr = DW.key_out; *kind = 2; return 0;
+        }
+    }
+    return SPHDEM_E_ARG;
+}
+
+template <typename R>
+static int get_field_t(SphdemHandle* H, int which, int field, void* dst, int n) {
+    const void* ptr;
+    int kind;
+    if (field_ptr<R>(H, which, field, &ptr, &kind)) return SPHDEM_E_ARG;
+    if (n == 0) return SPHDEM_OK;
+    CK(cudaStreamSynchronize(H->stream));
+    if (kind == 0) {
+        CK(cudaMemcpy(dst, ptr, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    } else if (kind == 1) {
+        return download_real<R>((double*)dst, (const R*)ptr, n, H->stream);
+    } else {
+        CK(cudaMemcpy(dst, ptr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int stats_t(SphdemHandle* H, SphdemStats* out) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    Engine<R>& E = EH->E;
+    const DevParams& P = E.P;
+    std::memset(out, 0, sizeof(*out));
+    cudaStream_t st = H->stream;
+    SphState<R>& S = E.S[E.cur_s];
+    SphWork<R>& W = E.sw;
+    DemState<R>& D = E.D[E.cur_d];
+    double hb[8] = {0};
+    if (P.ns > 0) {
+        k_stats<R><<<1, 256, 0, st>>>(P.ns, W.rho_new, P.xsph ? W.u_tmpx : S.ux, P.xsph ? W.u_tmpy : S.uy,
+                                      P.xsph ? W.u_tmpz : S.uz, W.ftot, S.ptype, S.itype, E.red_buf, E.flags);
+        CK(cudaMemcpyAsync(hb, E.red_buf, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out->rho_max_sph = hb[0]; out->u_max_sph = hb[1]; out->ftotal_max_sph = hb[2];
+    }
+    if (P.nd > 0) {
+        k_stats<R><<<1, 256, 0, st>>>(P.nd, D.rho, D.ux, D.uy, D.uz, (const R*)nullptr, D.ptype, D.itype, E.red_buf,
+                                      E.flags);
+        CK(cudaMemcpyAsync(hb, E.red_buf, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out->rho_max_dem = hb[0]; out->u_max_dem = hb[1]; out->ftotal_max_dem = hb[2];
+    }
+    DevFlags f;
+    CK(cudaMemcpyAsync(&f, E.flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    out->count = H->count;
+    out->time = H->time;
+    out->ppe_iters = H->ppe_iters;
+    out->ppe_rel_residual = H->ppe_res;
+    out->ppe_ms = H->ppe_ms;
+    out->overflow_flags = f.overflow;
+    out->nan_flag = f.nan;
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static void destroy_t(SphdemHandle* H) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    if (!EH) return;
+    for (void* p : EH->A.ptrs) cudaFree(p);
+    delete EH;
+    H->eng = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+static bool is_real_field(int f) { return f >= SPHDEM_F_X && f <= SPHDEM_F_Q_SD; }
+static bool is_int_field(int f) { return f >= SPHDEM_F_PTYPE && f <= SPHDEM_F_CELL; }
+
+static int check_supported(const SphdemParams* p) {
+    if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
+    if (p->dim != 3) return SPHDEM_E_UNSUPPORTED;
+    if (p->prop_table || p->fs_solve || p->fb_solve || p->interface_solve || p->boussinesq_solve ||
+        p->concn_solve || p->pst_solve || p->turbulence_model != 0 || p->penetration_solve || p->noslip_bc)
+        return SPHDEM_E_UNSUPPORTED;
+    if (p->kgc_solve != 0 && p->kgc_solve != 1) return SPHDEM_E_UNSUPPORTED;
+    if (p->time_type != 1) return SPHDEM_E_UNSUPPORTED;
+    if (p->decouple_stride != 1) return SPHDEM_E_UNSUPPORTED;
+    if (p->flag_z_index) return SPHDEM_E_UNSUPPORTED;
+    if (p->open_boundary == 2) return SPHDEM_E_UNSUPPORTED;
+    if (p->ppe_mode != SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
+    if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
+    if (!(p->dt > 0) || !(p->kappa > 0) || p->freq_filt <= 0) return SPHDEM_E_ARG;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem, SphdemHandle** out) {
+    if (!p || !out || n_sph < 0 || n_dem < 0 || n_sph + n_dem == 0) return SPHDEM_E_ARG;
+    *out = nullptr;
+    int r = check_supported(p);
+    if (r) return r;
+    SphdemHandle* h = new SphdemHandle();
+    h->p = *p;
+    h->ns = n_sph;
+    h->nd = n_dem;
+    h->prec = p->precision == SPHDEM_PREC_FP64 ? SPHDEM_PREC_FP64 : SPHDEM_PREC_FP32;
+    h->time = p->time;
+    h->count = (int)std::floor(p->time / p->dt + 0.5);  // ISPH_Calc_seperate.cuh:522
+    if (cudaGetDevice(&h->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return SPHDEM_E_CUDA;
+    }
+    *out = h;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, SphdemHandle** out) {
+    if (!dir || !out) return SPHDEM_E_ARG;
+    *out = nullptr;
+    SphdemParams p;
+    sphdem_io_params_default(&p);
+    std::string d(dir);
+    int r = sphdem_read_solv((d + "/solv.txt").c_str(), &p);
+    if (r) return r;
+    if (ov) {
+        p.precision = ov->precision;
+        p.ppe_mode = ov->ppe_mode;
+        p.warm_start = ov->warm_start;
+        p.ppe_tol = ov->ppe_tol;
+        p.ppe_max_iter = ov->ppe_max_iter;
+    }
+    if ((r = sphdem_io_check_table((d + "/data.txt").c_str()))) return r;
+    SphdemHandle tmp;
+    if ((r = sphdem_io_read_input_txt((d + "/input.txt").c_str(), &tmp, &p))) return r;
+    SphdemHandle* h = nullptr;
+    if ((r = sphdem_create(&p, tmp.ns, tmp.nd, &h))) return r;
+    h->stage_d[0] = tmp.stage_d[0]; h->stage_d[1] = tmp.stage_d[1];
+    h->stage_i[0] = tmp.stage_i[0]; h->stage_i[1] = tmp.stage_i[1];
+    h->file_x = tmp.file_x; h->file_y = tmp.file_y; h->file_z = tmp.file_z;
+    h->file_h0 = tmp.file_h0;
+    h->have_file_order = true;
+    if ((r = sphdem_commit_particles(h))) {
+        sphdem_destroy(h);
+        return r;
+    }
+    *out = h;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const void* src, size_t bytes) {
+    if (!h || !src || (which != 0 && which != 1) || h->committed) return SPHDEM_E_ARG;
+    int n = which ? h->nd : h->ns;
+    if (is_real_field(field)) {
+        if (bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
+        const double* s = (const double*)src;
+        h->stage_d[which][field].assign(s, s + n);
+        return SPHDEM_OK;
+    }
+    if (is_int_field(field) && field != SPHDEM_F_CELL && field != SPHDEM_F_PID && field != SPHDEM_F_ITYPE &&
+        field != SPHDEM_F_BUFFER_TYPE) {
+        if (bytes != sizeof(int) * (size_t)n) return SPHDEM_E_ARG;
+        const int* s = (const int*)src;
+        h->stage_i[which][field].assign(s, s + n);
+        return SPHDEM_OK;
+    }
+    return SPHDEM_E_ARG;
+}
+
+extern "C" int sphdem_commit_particles(SphdemHandle* h) {
+    if (!h || h->committed) return SPHDEM_E_ARG;
+    for (int q = 0; q < 2; q++) {
+        int nq = q ? h->nd : h->ns;
+        if (nq == 0) continue;
+        for (int f : {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_H})
+            if ((int)h->stage_d[q][f].size() != nq) return SPHDEM_E_INPUT;
+        if ((int)h->stage_i[q][SPHDEM_F_PTYPE].size() != nq) return SPHDEM_E_INPUT;
+        for (int i = 0; i < nq; i++) {
+            int pt = h->stage_i[q][SPHDEM_F_PTYPE][i];
+            if ((q == 0 && pt > 1000) || (q == 1 && pt <= 1000)) return SPHDEM_E_INPUT;
+            if (!(h->stage_d[q][SPHDEM_F_H][i] > 0)) return SPHDEM_E_INPUT;
+        }
+        if (q == 1) {
+            if ((int)h->stage_d[1][SPHDEM_F_RAD].size() != nq) return SPHDEM_E_INPUT;
+            if ((int)h->stage_i[1][SPHDEM_F_DEM_IDX].size() != nq) return SPHDEM_E_INPUT;
+        }
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) return SPHDEM_E_CUDA;
+    int r = h->prec == SPHDEM_PREC_FP64 ? commit_t<double>(h) : commit_t<float>(h);
+    if (r) {
+        if (h->eng) {
+            if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
+        }
+        return r;
+    }
+    for (int q = 0; q < 2; q++) { h->stage_d[q].clear(); h->stage_i[q].clear(); }
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_step(SphdemHandle* h, int32_t nsteps) {
+    if (!h || !h->committed || nsteps < 0) return SPHDEM_E_ARG;
+    int64_t nl = 0;
+    for (int k = 0; k < nsteps; k++) {
+        int r = h->prec == SPHDEM_PREC_FP64 ? run_step<double>(h, (EngineHost<double>*)h->eng, &nl)
+                                            : run_step<float>(h, (EngineHost<float>*)h->eng, &nl);
+        if (r) return r;
+        h->time += h->p.dt;   // ISPH_Calc_seperate.cuh:924-925
+        h->count++;
+    }
+    h->last_launches = nl;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_field(SphdemHandle* h, int which, int field, void* dst, size_t bytes) {
+    if (!h || !dst || (which != 0 && which != 1)) return SPHDEM_E_ARG;
+    int n = which ? h->nd : h->ns;
+    if (!h->committed) {
+        if (is_real_field(field)) {
+            auto it = h->stage_d[which].find(field);
+            if (it == h->stage_d[which].end() || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
+            std::memcpy(dst, it->second.data(), bytes);
+            return SPHDEM_OK;
+        }
+        return SPHDEM_E_ARG;
+    }
+    size_t need = (is_int_field(field) ? sizeof(int) : sizeof(double)) * (size_t)n;
+    if (bytes != need) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64 ? get_field_t<double>(h, which, field, dst, n)
+                                       : get_field_t<float>(h, which, field, dst, n);
+}
+
+extern "C" int sphdem_get_stats(SphdemHandle* h, SphdemStats* out) {
+    if (!h || !out || !h->committed) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64 ? stats_t<double>(h, out) : stats_t<float>(h, out);
+}
+
+extern "C" int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* dst, int32_t cap) {
+    if (!h || !counts || !h->committed || cap < 0) return SPHDEM_E_ARG;
+    int ns = h->ns;
+    const int* ncnt;
+    const int* nbr;
+    int ncap;
+    if (h->prec == SPHDEM_PREC_FP64) {
+        auto* EH = (EngineHost<double>*)h->eng;
+        ncnt = EH->E.sw.ncnt; nbr = EH->E.sw.nbr; ncap = EH->nb_cap;
+    } else {
+        auto* EH = (EngineHost<float>*)h->eng;
+        ncnt = EH->E.sw.ncnt; nbr = EH->E.sw.nbr; ncap = EH->nb_cap;
+    }
+    if (ns == 0) return SPHDEM_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(counts, ncnt, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+    if (!dst || cap == 0) return SPHDEM_OK;
+    std::vector<int> colmajor((size_t)ncap * ns);
+    CK(cudaMemcpy(colmajor.data(), nbr, sizeof(int) * colmajor.size(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ns; i++) {
+        int c = std::min(std::min(counts[i], cap), ncap);
+        for (int k = 0; k < c; k++) dst[(size_t)i * cap + k] = colmajor[(size_t)k * ns + i];
+    }
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int history_t(SphdemHandle* H, int32_t* ids, double* sp) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    DemState<R>& D = EH->E.D[EH->E.cur_d];
+    int n = H->nd;
+    if (n == 0) return SPHDEM_OK;
+    std::vector<int> hid((size_t)n * SPHDEM_NSLOT);
+    std::vector<double> hds((size_t)n * SPHDEM_NSLOT * 3);
+    CK(cudaStreamSynchronize(H->stream));
+    CK(cudaMemcpy(hid.data(), D.hid, sizeof(int) * hid.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(hds.data(), D.hds, sizeof(double) * hds.size(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++)
+        for (int s = 0; s < SPHDEM_NSLOT; s++) {
+            ids[(size_t)i * SPHDEM_NSLOT + s] = hid[(size_t)s * n + i];
+            for (int c = 0; c < 3; c++) sp[((size_t)i * SPHDEM_NSLOT + s) * 3 + c] = hds[(size_t)(s * 3 + c) * n + i];
+        }
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs) {
+    if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, ids, springs) : history_t<float>(h, ids, springs);
+}
+
+extern "C" int sphdem_write_vtk_dem(SphdemHandle* h, const char* path) {
+    if (!h || !path || !h->committed) return SPHDEM_E_ARG;
+    int n = h->nd;
+    std::vector<double> x(n), y(n), z(n), magf(n), eliz(n, 1.0), por(n), uz(n), qsd(n), ftz(n), temp(n), rad(n), dtemp(n);
+    std::vector<int> itype(n), ptype(n), idx(n);
+    int r = 0;
+    size_t bd = sizeof(double) * n, bi = sizeof(int) * n;
+    r |= sphdem_get_field(h, 1, SPHDEM_F_X, x.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_Y, y.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_Z, z.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_DEMPOR, por.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_UZ, uz.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_Q_SD, qsd.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_FTOTALZ, ftz.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_TEMP, temp.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_RAD, rad.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_DTEMP, dtemp.data(), bd);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_ITYPE, itype.data(), bi);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_PTYPE, ptype.data(), bi);
+    r |= sphdem_get_field(h, 1, SPHDEM_F_DEM_IDX, idx.data(), bi);
+    if (r) return SPHDEM_E_CUDA;
+    if (n > 0) {
+        if (h->prec == SPHDEM_PREC_FP64) {
+            auto* EH = (EngineHost<double>*)h->eng;
+            if (download_real<double>(magf.data(), EH->E.dw.magf, n, h->stream)) return SPHDEM_E_CUDA;
+        } else {
+            auto* EH = (EngineHost<float>*)h->eng;
+            if (download_real<float>(magf.data(), EH->E.dw.magf, n, h->stream)) return SPHDEM_E_CUDA;
+        }
+    }
+    return sphdem_io_write_vtk_dem(path, n, x.data(), y.data(), z.data(), itype.data(), ptype.data(), idx.data(),
+                                   magf.data(), eliz.data(), por.data(), uz.data(), qsd.data(), ftz.data(),
+                                   temp.data(), rad.data(), dtemp.data());
+}
+
+extern "C" int sphdem_write_restart(SphdemHandle* h, const char* path) {
+    if (!h || !path || !h->committed) return SPHDEM_E_ARG;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return SPHDEM_E_INPUT;
+    // every column the reader understands, tab-separated labels
+    const int lbl[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35};
+    const int fld[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_UX, SPHDEM_F_UY, SPHDEM_F_UZ, SPHDEM_F_M,
+                       SPHDEM_F_PTYPE, SPHDEM_F_H, SPHDEM_F_TEMP, SPHDEM_F_PRES, SPHDEM_F_RHO, SPHDEM_F_FLT_S,
+                       SPHDEM_F_RAD, SPHDEM_F_RI, SPHDEM_F_DEM_IDX, SPHDEM_F_WX, SPHDEM_F_WY, SPHDEM_F_WZ,
+                       SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3};
+    const int nc = sizeof(lbl) / sizeof(lbl[0]);
+    for (int c = 0; c < nc; c++) std::fprintf(f, c ? "\t%d" : "%d", lbl[c]);
+    std::fprintf(f, "\n");
+    for (int q = 0; q < 2; q++) {
+        int n = q ? h->nd : h->ns;
+        if (n == 0) continue;
+        std::vector<std::vector<double>> cols(nc, std::vector<double>(n, 0.0));
+        for (int c = 0; c < nc; c++) {
+            int fd = fld[c];
+            if (is_int_field(fd)) {
+                if (q == 0 && fd == SPHDEM_F_DEM_IDX) continue;
+                std::vector<int> v(n);
+                if (sphdem_get_field(h, q, fd, v.data(), sizeof(int) * n) == 0)
+                    for (int i = 0; i < n; i++) cols[c][i] = v[i];
+            } else {
+                std::vector<double> v(n);
+                if (sphdem_get_field(h, q, fd, v.data(), sizeof(double) * n) == 0) cols[c] = v;
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            for (int c = 0; c < nc; c++) {
+                if (fld[c] == SPHDEM_F_PTYPE || fld[c] == SPHDEM_F_DEM_IDX)
+                    std::fprintf(f, c ? "\t%d" : "%d", (int)cols[c][i]);
+                else
+                    std::fprintf(f, c ? "\t%.17g" : "%.17g", cols[c][i]);
+            }
+            std::fprintf(f, "\n");
+        }
+    }
+    std::fclose(f);
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_time(SphdemHandle* h, double* time, int32_t* count) {
+    if (!h || !time || !count) return SPHDEM_E_ARG;
+    *time = h->time;
+    *count = h->count;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_counts(SphdemHandle* h, int32_t* ns, int32_t* nd) {
+    if (!h || !ns || !nd) return SPHDEM_E_ARG;
+    *ns = h->ns;
+    *nd = h->nd;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_stream(SphdemHandle* h, void** stream) {
+    if (!h || !stream) return SPHDEM_E_ARG;
+    *stream = (void*)h->stream;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_launch_count(SphdemHandle* h, int64_t* launches) {
+    if (!h || !launches) return SPHDEM_E_ARG;
+    *launches = h->last_launches;
+    return SPHDEM_OK;
+}
+
+extern "C" void sphdem_destroy(SphdemHandle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    if (h->eng) {
+        if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+extern "C" const char* sphdem_strerror(int s) {
+    switch (s) {
+    case SPHDEM_OK: return "ok";
+    case SPHDEM_E_ARG: return "invalid argument";
+    case SPHDEM_E_CUDA: return "CUDA runtime error";
+    case SPHDEM_E_INPUT: return "malformed input";
+    case SPHDEM_E_OVERFLOW: return "neighbour list or contact history overflow";
+    case SPHDEM_E_NAN: return "non-finite value in the particle state";
+    case SPHDEM_E_TIMEOUT: return "bounded device wait timed out";
+    case SPHDEM_E_UNSUPPORTED: return "switch combination not supported";
+    case SPHDEM_E_NOMEM: return "out of memory or size above limit";
+    }
+    return "unknown status";
+}
+
+extern "C" int sphdem_params_size(void) { return (int)sizeof(SphdemParams); }

@@ -1,0 +1,84 @@
+// engine.cuh -- device state of one SPH-DEM engine handle.
+//
+// Layout in HBM (structure of arrays, one array per field, cell-sorted):
+//   positions, smoothing length and DEM radius: double
+//   every other field: R (float in the FP32 build, double in the FP64 one)
+//   DEM contact history: SPHDEM_NSLOT slot-major planes, partner id int32
+//     and tangential spring double[3]  (slot s of particle i at s*n+i)
+// Persistent fields live in two copies (A/B) that the per-step reorder
+// gathers between; work arrays are single copies overwritten each step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "device_common.cuh"
+
+namespace sphdem {
+
+template <typename R>
+struct SphState {
+    double *x, *y, *z, *h;
+    R *ux, *uy, *uz, *m, *rho, *pres, *temp, *dDEMpor, *flt_s;
+    int *ptype, *btype, *itype, *pid;
+};
+
+template <typename R>
+struct DemState {
+    double *x, *y, *z, *h, *rad;
+    R *ux, *uy, *uz, *wx, *wy, *wz, *m, *rho, *ri, *temp, *temp1, *temp2, *temp3;
+    R *Fdx_df, *Fdy_df, *Fdz_df, *Q_sd;
+    int *ptype, *btype, *itype, *pid, *dem_idx;
+    int* hid;      // NSLOT*n
+    double* hds;   // NSLOT*3*n
+};
+
+template <typename R>
+struct SphWork {
+    R *m_new, *rho_new, *rho_ref, *DEMpor, *dDEMpor_prev;
+    R* Cm;                       // 9*n, row-major per particle plane: Cm[k*n+i]
+    R *ftx, *fty, *ftz, *ftot;
+    R *fpx, *fpy, *fpz;
+    R *pgfx, *pgfy, *pgfz;
+    R *dtemp, *temp0;
+    R *ux0, *uy0, *uz0;
+    R *p_new;
+    R *u_tmpx, *u_tmpy, *u_tmpz, *temp_tmp;
+    int *key_in, *key_out, *val_in, *val_out;
+    int *g_str, *g_end;
+    int *nbr, *ncnt;
+    int *wall_idx, *buf_idx, *counters;   // per-step compacted wall / buffer slots
+};
+
+template <typename R>
+struct DemWork {
+    R *flt_s, *flt_sd, *flt_sd2, *DEMpor;
+    R *ftx, *fty, *ftz, *tqx, *tqy, *tqz;
+    R *dtemp, *dtemp1, *dtemp2, *dtemp3;
+    R *Fdx_b, *Fdy_b, *Fdz_b, *Fdx_da, *Fdy_da, *Fdz_da;
+    R *ux0, *uy0, *uz0, *temp0;
+    R *magf;                     // |u_f - u_a| of the drag closure (VTK mag_uijf)
+    int *key_in, *key_out, *val_in, *val_out;
+    int *g_str, *g_end;
+};
+
+// device-side status words (checked by the host at sync points)
+struct DevFlags {
+    int overflow;   // bit0 SPH neighbour list, bit1 DEM contact history
+    int nan;
+    int max_ncnt;
+};
+
+template <typename R>
+struct Engine {
+    DevParams P;
+    SphState<R> S[2];    // ping-pong; cur = S[cur_s]
+    DemState<R> D[2];
+    int cur_s, cur_d;
+    SphWork<R> sw;
+    DemWork<R> dw;
+    DevFlags* flags;
+    void* sort_tmp;
+    size_t sort_tmp_bytes;
+    double* red_buf;     // reductions for stats
+};
+
+}  // namespace sphdem

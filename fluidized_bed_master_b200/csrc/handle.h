@@ -1,0 +1,46 @@
+// handle.h -- host-side state of an engine handle (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <map>
+#include <string>
+#include <vector>
+#include "../../include/sphdem.h"
+
+struct SphdemHandle {
+    SphdemParams p;
+    int ns = 0, nd = 0;
+    int device = 0;
+    int prec = SPHDEM_PREC_FP32;
+    cudaStream_t stream = nullptr;
+    bool committed = false;
+    // staged host input (input order) until commit
+    std::map<int, std::vector<double>> stage_d[2];
+    std::map<int, std::vector<int>> stage_i[2];
+    // rows in file order for the bounding box (SPH then DEM if set
+    // programmatically; input.txt order if read from a directory)
+    std::vector<double> file_x, file_y, file_z;
+    double file_h0 = 0.0;
+    bool have_file_order = false;
+    double time = 0.0;
+    int count = 0;
+    double bbox[6] = {0, 0, 0, 0, 0, 0};
+    int nijk[3] = {0, 0, 0};
+    double dcell = 0.0;
+    void* eng = nullptr;     // sphdem::Engine<float|double>*
+    std::map<int, cudaGraphExec_t> graphs;
+    std::map<int, int64_t> graph_launches;
+    int use_graphs = 1;
+    int64_t last_launches = 0;
+    int ppe_iters = 0;
+    double ppe_res = 0.0;
+    double ppe_ms = 0.0;
+};
+
+// io.cpp
+int sphdem_io_read_input_txt(const char* path, SphdemHandle* h, const SphdemParams* p);
+int sphdem_io_check_table(const char* path);
+void sphdem_io_params_default(SphdemParams* p);
+int sphdem_io_write_vtk_dem(const char* path, int n, const double* x, const double* y, const double* z,
+                            const int* itype, const int* ptype, const int* dem_idx, const double* magf,
+                            const double* eliz, const double* por, const double* uz, const double* qsd,
+                            const double* ftz, const double* temp, const double* rad, const double* dtemp);

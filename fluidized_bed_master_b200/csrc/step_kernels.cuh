@@ -1,0 +1,1310 @@
+// step_kernels.cuh -- the kernels of one ISPH-DEM step.
+//
+// One kernel per fused pass, launched in the order of SOPHIA_single_ISPH
+// (ISPH_Calc_seperate.cuh:13-503):
+//
+//   k_hash_* / sort / k_cells_gather_*   NNPS: cell key, stable sort by cell,
+//                                        cell start/end + SoA permutation
+//   k_build_list                         SPH neighbour list (kappa*h_i)
+//   k_passA          mass_init + KGC + SPH porosity + prep_sph
+//   k_dem_prep       DEM filters and porosity
+//   k_passB          prep3D filter + advection forces
+//   k_dem_contact    Hertz-Mindlin contact with tangential history
+//   k_dem_coupling   Di Felice drag + pressure-gradient force + DEM predictor
+//   k_sph_coupling   reaction force + SPH predictor
+//   k_neumann        wall pressure/density/temperature extrapolation
+//   k_ppe            one Jacobi sweep of the pressure Poisson equation
+//   k_passC          pressure force + SPH corrector
+//   k_dem_update     DEM corrector + cylinder/box/cone walls
+//   k_open_bc        inlet/outlet ghost extrapolation
+//   k_xsph           XSPH velocity/temperature smoothing
+//
+// Each kernel cites the reference kernels it replaces.  R is the field
+// precision (float or double); positions, h and radii are always double.
+#pragma once
+#include "engine.cuh"
+
+namespace sphdem {
+
+// pair geometry in field precision from double positions
+template <typename R>
+struct Pair {
+    R dx, dy, dz, r2, r;
+};
+
+template <typename R>
+__device__ __forceinline__ Pair<R> make_pair(double xi, double yi, double zi, double xj, double yj, double zj) {
+    Pair<R> g;
+    g.dx = (R)(xi - xj);
+    g.dy = (R)(yi - yj);
+    g.dz = (R)(zi - zj);
+    g.r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+    g.r = sqrt(g.r2);
+    return g;
+}
+
+template <typename R>
+__device__ __forceinline__ void kgc3(const R* __restrict__ Cm, int n, int i, int on, R& ax, R& ay, R& az) {
+    if (!on) return;
+    R a = ax, b = ay, c = az;
+    ax = Cm[0 * n + i] * a + Cm[1 * n + i] * b + Cm[2 * n + i] * c;
+    ay = Cm[3 * n + i] * a + Cm[4 * n + i] * b + Cm[5 * n + i] * c;
+    az = Cm[6 * n + i] * a + Cm[7 * n + i] * b + Cm[8 * n + i] * c;
+}
+
+// 27-cell stencil in the reference order (z,y,x), calling f(j) for every
+// slot j of every non-empty cell.
+template <typename F>
+__device__ __forceinline__ void for_stencil(const DevParams& P, int ic, int jc, int kc, const int* __restrict__ gs,
+                                            const int* __restrict__ ge, F f) {
+    for (int z = -1; z <= 1; z++) {
+        int kz = kc + z;
+        if (kz < 0 || kz > P.NK - 1) continue;
+        for (int y = -1; y <= 1; y++) {
+            int jy = jc + y;
+            if (jy < 0 || jy > P.NJ - 1) continue;
+            for (int x = -1; x <= 1; x++) {
+                int ix = ic + x;
+                if (ix < 0 || ix > P.NI - 1) continue;
+                int c = ix + P.NI * jy + P.NI * P.NJ * kz;
+                int s = gs[c];
+                if (s == -1) continue;
+                int e = ge[c];
+                for (int j = s; j < e; j++) f(j);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// NNPS
+// ---------------------------------------------------------------------------
+// KERNEL_index_particle_to_cell_{sph,dem}: functions_NNPS.cuh:762-821
+__global__ void k_hash(DevParams P, int n, const double* __restrict__ x, const double* __restrict__ y,
+                       const double* __restrict__ z, const int* __restrict__ itype, int* key, int* val) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int k;
+    if (itype[i] == 3) k = P.num_cells;
+    else {
+        int ic, jc, kc;
+        cell_ijk(P, x[i], y[i], z[i], ic, jc, kc);
+        k = ic + P.NI * jc + P.NI * P.NJ * kc;
+    }
+    key[i] = k;
+    val[i] = i;
+}
+
+// cell start/end of KERNEL_reorder_{sph,dem} (functions_NNPS.cuh:670-730)
+__device__ __forceinline__ void cell_bounds(const DevParams& P, int i, int n, const int* __restrict__ key, int* gs, int* ge) {
+    int k = key[i];
+    if (i == 0 || k != key[i - 1]) {
+        if (k < P.num_cells) gs[k] = i;
+        if (i > 0 && key[i - 1] < P.num_cells) ge[key[i - 1]] = i;
+    }
+    if (i == n - 1 && k < P.num_cells) ge[k] = n;
+}
+
+// reorder of every persistent SPH field, source of m/rho/pres/u/temp is
+// the array that held the end-of-step value
+template <typename R>
+struct SphGatherSrc {
+    const R *ux, *uy, *uz, *m, *rho, *pres, *temp;
+};
+
+template <typename R>
+__global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R> gsrc, SphState<R> dst,
+                                   const int* __restrict__ key, const int* __restrict__ perm, int* gs, int* ge,
+                                   int* wall_idx, int* buf_idx, int* counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    cell_bounds(P, i, n, key, gs, ge);
+    int p = perm[i];
+    dst.x[i] = src.x[p];
+    dst.y[i] = src.y[p];
+    dst.z[i] = src.z[p];
+    dst.h[i] = src.h[p];
+    dst.ux[i] = gsrc.ux[p];
+    dst.uy[i] = gsrc.uy[p];
+    dst.uz[i] = gsrc.uz[p];
+    dst.m[i] = gsrc.m[p];
+    dst.rho[i] = gsrc.rho[p];
+    dst.pres[i] = gsrc.pres[p];
+    dst.temp[i] = gsrc.temp[p];
+    dst.dDEMpor[i] = src.dDEMpor[p];
+    dst.flt_s[i] = src.flt_s[p];
+    int pt = src.ptype[p], bt = src.btype[p];
+    dst.ptype[i] = pt;
+    dst.btype[i] = bt;
+    dst.itype[i] = src.itype[p];
+    dst.pid[i] = src.pid[p];
+    if (pt <= 0) wall_idx[atomicAdd(&counters[0], 1)] = i;
+    if (bt > 0 && pt < 1000) buf_idx[atomicAdd(&counters[1], 1)] = i;
+}
+
+template <typename R>
+__global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst, const int* __restrict__ key,
+                                   const int* __restrict__ perm, int* gs, int* ge) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.nd;
+    if (i >= n) return;
+    cell_bounds(P, i, n, key, gs, ge);
+    int p = perm[i];
+    dst.x[i] = src.x[p]; dst.y[i] = src.y[p]; dst.z[i] = src.z[p];
+    dst.h[i] = src.h[p]; dst.rad[i] = src.rad[p];
+    dst.ux[i] = src.ux[p]; dst.uy[i] = src.uy[p]; dst.uz[i] = src.uz[p];
+    dst.wx[i] = src.wx[p]; dst.wy[i] = src.wy[p]; dst.wz[i] = src.wz[p];
+    dst.m[i] = src.m[p]; dst.rho[i] = src.rho[p]; dst.ri[i] = src.ri[p];
+    dst.temp[i] = src.temp[p]; dst.temp1[i] = src.temp1[p]; dst.temp2[i] = src.temp2[p]; dst.temp3[i] = src.temp3[p];
+    dst.Fdx_df[i] = src.Fdx_df[p]; dst.Fdy_df[i] = src.Fdy_df[p]; dst.Fdz_df[i] = src.Fdz_df[p];
+    dst.Q_sd[i] = src.Q_sd[p];
+    dst.ptype[i] = src.ptype[p]; dst.btype[i] = src.btype[p]; dst.itype[i] = src.itype[p];
+    dst.pid[i] = src.pid[p]; dst.dem_idx[i] = src.dem_idx[p];
+#pragma unroll
+    for (int s = 0; s < SPHDEM_NSLOT; s++) {
+        dst.hid[s * n + i] = src.hid[s * n + p];
+        dst.hds[(s * 3 + 0) * n + i] = src.hds[(s * 3 + 0) * n + p];
+        dst.hds[(s * 3 + 1) * n + i] = src.hds[(s * 3 + 1) * n + p];
+        dst.hds[(s * 3 + 2) * n + i] = src.hds[(s * 3 + 2) * n + p];
+    }
+}
+
+// SPH neighbour list: the candidate set and predicate of every SPH gather
+// kernel (e.g. functions_PPE2.cuh:609-638): 27-cell stencil and
+// sqrt(dx^2+dy^2+dz^2) + 1e-20 < kappa*h_i, decided exactly in FP64 (see
+// pair_test).  Rows come out in ascending slot order, which is the
+// reference's z,y,x cell visit order.  Column-major rows.
+template <typename R>
+__global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, const int* __restrict__ gs,
+                                                    const int* __restrict__ ge, int* __restrict__ nbr,
+                                                    int* __restrict__ ncnt, DevFlags* F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.ns) return;
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
+    double Rr = __dmul_rn(P.kappa, S.h[i]);
+    float lo = r2_lo(Rr), hi = r2_hi(Rr);
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    int c = 0, cap = P.nb_cap, n = P.ns;
+    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
+        for (int j = a; j < b; j++) {
+            if (pair_test<float>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 1e-20, lo, hi).in) {
+                if (c < cap) nbr[(size_t)c * n + i] = j;
+                c++;
+            }
+        }
+    });
+    ncnt[i] = c;
+    if (c > cap) atomicOr(&F->overflow, 1);
+    atomicMax(&F->max_ncnt, c);
+}
+
+// ---------------------------------------------------------------------------
+// pass A: KERNEL_clc_mass_init_sph (functions_MASS.cuh:24-43),
+// KERNEL_clc_correction_KGC_3D_sph (functions_PREP2.cuh:452-568),
+// KERNEL_clc_prep3D_coupling_sph (functions_PREP2.cuh:3190-3364),
+// KERNEL_clc_prep3D_prep_sph (functions_PREP2.cuh:1623-1679).
+// Neighbours read the start-of-step m, rho; the new m, rho go to m_new,
+// rho_new so that no thread sees a half-updated neighbour.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+                                               const int* __restrict__ dgs, const int* __restrict__ dge) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i];
+    R mo = S.m[i], ro = S.rho[i];
+    if (it > 2) {
+        W.m_new[i] = mo;
+        W.rho_new[i] = ro;
+        return;
+    }
+    R dprev = S.dDEMpor[i];
+    W.dDEMpor_prev[i] = dprev;
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
+    R th = (R)hi;
+    R tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    int cnt = min(W.ncnt[i], P.nb_cap);
+    R txx = 0, tyy = 0, tzz = 0, txy = 0, tyz = 0, tzx = 0, sflt = 0;
+    const int* __restrict__ nb = W.nbr;
+    for (int k = 0; k < cnt; k++) {
+        int j = nb[(size_t)k * n + i];
+        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
+        R mj = S.m[j], rj = S.rho[j];
+        int ptj = S.ptype[j];
+        R r = g.r + (R)1e-20;
+        R w = knl_w<R>(P.kernel_type, tA, th, r);
+        if (ptj <= 1000) sflt += mj / rj * w * (R)(ptj == 1);
+        if (P.kgc == 1 && g.r2 > (R)0 && ptj <= 1000) {
+            R dw = knl_dw<R>(P.kernel_type, tA, th, g.r);
+            R mtd = mj * dw, rtd = (R)1 / (rj * g.r), t;
+            t = -mtd * g.dx * g.dx; t *= rtd; txx += t;
+            t = -mtd * g.dy * g.dx; t *= rtd; txy += t;
+            t = -mtd * g.dy * g.dy; t *= rtd; tyy += t;
+            t = -mtd * g.dx * g.dz; t *= rtd; tzx += t;
+            t = -mtd * g.dy * g.dz; t *= rtd; tyz += t;
+            t = -mtd * g.dz * g.dz; t *= rtd; tzz += t;
+        }
+    }
+    if (P.kgc == 1) {
+        R det = txx * (tyy * tzz - tyz * tyz);
+        det -= txy * (txy * tzz - tyz * tzx);
+        det += tzx * (txy * tyz - tyy * tzx);
+        R C[9];
+        if (fabs(det) > (R)1e-4) {
+            R rr = (R)1 / det;
+            C[0] = (tyy * tzz - tyz * tyz) * rr;
+            C[1] = (tzx * tyz - txy * tzz) * rr;
+            C[2] = (txy * tyz - tzx * tyy) * rr;
+            C[3] = (tzx * tyz - txy * tzz) * rr;
+            C[4] = (txx * tzz - tzx * tzx) * rr;
+            C[5] = (tzx * txy - txx * tyz) * rr;
+            C[6] = (txy * tyz - tzx * tyy) * rr;
+            C[7] = (tzx * txy - txx * tyz) * rr;
+            C[8] = (txx * tyy - txy * txy) * rr;
+        } else {
+            C[0] = 1; C[1] = 0; C[2] = 0; C[3] = 0; C[4] = 1; C[5] = 0; C[6] = 0; C[7] = 0; C[8] = 1;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) W.Cm[(size_t)q * n + i] = C[q];
+    }
+    // SPH-DEM porosity
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    double Rr = P.kappa * hi;
+    R por = 0, dfx = 0, dfy = 0, dfz = 0;
+    if (P.nd > 0) {
+        for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
+            double d = pair_dist(xi, yi, zi, D.x[j], D.y[j], D.z[j]) + 1e-20;
+            if (d < Rr && D.ptype[j] > 1000) {
+                Pair<R> g = make_pair<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j]);
+                R r = (R)d;
+                R w = knl_w<R>(P.kernel_type, tA, th, r);
+                R dw = knl_dw<R>(P.kernel_type, tA, th, r);
+                R rj = (R)D.rad[j];
+                R v = (R)4.18879 * rj * rj * rj;
+                por += w * v;
+                dfx += dw * g.dx / r * (R)D.ux[j] * v;
+                dfy += dw * g.dy / r * (R)D.uy[j] * v;
+                dfz += dw * g.dz / r * (R)D.uz[j] * v;
+            }
+        });
+    }
+    R pori = (R)1 - (por / (sflt + (R)1e-20));
+    W.DEMpor[i] = pori;
+    S.dDEMpor[i] = (dfx + dfy + dfz) / (sflt + (R)1e-20);
+    // prep_sph
+    R hd = (R)P.h_over_dx;
+    R v = (th / hd) * (th / hd) * (th / hd);
+    R mref;
+    if (pt == 9) mref = (R)P.rho_liquid * v * pori;
+    else if (pt == -3 || pt == 0 || pt == 3 || pt == 1) mref = (R)P.rho_gas * v * pori;
+    else mref = (R)P.rho_liquid * v * pori;
+    if (pt == 9 && zi < 0.05) mref = (R)P.rho_gas * v * pori;
+    R rref = (P.dim == 2) ? mref / ((th / hd) * (th / hd)) : mref / v;
+    W.rho_ref[i] = rref;
+    if (P.rho_type == 1) {
+        W.rho_new[i] = mref / v;
+        W.m_new[i] = mref;
+    } else {
+        W.rho_new[i] = ro;
+        W.m_new[i] = mo;
+    }
+}
+
+// KERNEL_clc_prep3D_coupling_dem: functions_PREP2.cuh:3367-3523.
+// One warp per DEM sphere; lanes stride over the candidate rows.
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, DemState<R> D, DemWork<R> DW,
+                                                  const int* __restrict__ sgs, const int* __restrict__ sge,
+                                                  const int* __restrict__ dgs, const int* __restrict__ dge) {
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= P.nd) return;
+    if (D.itype[i] > 2) return;
+    int pti = D.ptype[i];
+    double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
+    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    double Rr = P.kappa * hi;
+    float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    R f1 = 0, f3 = 0, por = 0;
+    for_stencil_rows(P, ic, jc, kc, sgs, sge, [&](int a, int b) {
+        for (int j = a + lane; j < b; j += 32) {
+            int ptj = S.ptype[j];
+            if (ptj != 1 && ptj != 3) continue;
+            PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
+            if (!g.in) continue;
+            R w = knl_w<R>(P.kernel_type, tA, th, g.r);
+            R c = S.m[j] / S.rho[j] * w;
+            if (ptj == 1) f1 += c;
+            else f3 += c;
+        }
+    });
+    for_stencil_rows(P, ic, jc, kc, dgs, dge, [&](int a, int b) {
+        for (int j = a + lane; j < b; j += 32) {
+            if (D.ptype[j] <= 1000) continue;
+            PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
+            if (!g.in) continue;
+            R w = knl_w<R>(P.kernel_type, tA, th, g.r);
+            R rj = (R)D.rad[j];
+            por += w * (R)4.18879 * rj * rj * rj;
+        }
+    });
+    f1 = warp_sum(f1);
+    f3 = warp_sum(f3);
+    por = warp_sum(por);
+    if (lane == 0 && pti > 1000) {
+        DW.flt_s[i] = f3;
+        DW.flt_sd[i] = f1;
+        DW.flt_sd2[i] = f1;
+        DW.DEMpor[i] = (R)1 - (por / (f3 + f1 + (R)1.0e-20));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass B: KERNEL_clc_prep3D_sph (functions_PREP2.cuh:1985-2227, Shepard
+// filter) + KERNEL_advection_force3D_sph (functions_PPE2.cuh:1251-1607).
+// The delta-SPH density gradient of prep3D is not formed: no kernel of the
+// ISPH step reads it.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, int filt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
+    W.ftx[i] = 0; W.fty[i] = 0; W.ftz[i] = 0; W.ftot[i] = 0;
+    W.pgfx[i] = 0; W.pgfy[i] = 0; W.pgfz[i] = 0;
+    W.dtemp[i] = 0;
+    if (it > 2 || pt > 1000) return;
+    bool adv = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
+    if (!filt && !adv) return;
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
+    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i];
+    R tempi = S.temp[i], pi = S.pres[i], rhoi = W.rho_new[i];
+    R pori = W.DEMpor[i];
+    R vis = (R)P.mu_gas, vis_h = (vis * vis) / (vis + vis);
+    R kc = (R)P.k_sph, kc_h = (kc * kc) / (kc + kc);
+    R eli = P.sph_lagrangian ? (R)1 : (R)0;
+    int cnt = min(W.ncnt[i], P.nb_cap);
+    R flt = 0, tx = 0, ty = 0, tz = 0, px = 0, py = 0, pz = 0, Rc = 0, ex = 0, ey = 0, ez = 0, et = 0;
+    const int* __restrict__ nb = W.nbr;
+    for (int k = 0; k < cnt; k++) {
+        int j = nb[(size_t)k * n + i];
+        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
+        R r = g.r + (R)1e-20;
+        R mj = W.m_new[j], rhoj = W.rho_new[j];
+        if (filt) flt += mj / rhoj * knl_w<R>(P.kernel_type, tA, th, r);
+        if (!adv || S.ptype[j] >= 1000) continue;
+        R dw = knl_dw<R>(P.kernel_type, tA, th, r);
+        R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
+        kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
+        R uxj = S.ux[j], uyj = S.uy[j], uzj = S.uz[j], pj = S.pres[j], tj = S.temp[j];
+        if (P.fp) {
+            R Cp = -pori * (mj) * (pi + pj) / (rhoi * rhoj);
+            R s = rhoi / pori * Cp;
+            px += s * gx;
+            py += s * gy;
+            pz += s * gz;
+        }
+        if (P.fv) {
+            R Cv = g.dx * gx + g.dy * gy + g.dz * gz;
+            Cv *= vis_h;
+            Cv *= (R)4 * pori * (mj / (rhoi * rhoj));
+            Cv /= r;
+            Cv /= r;
+            tx += Cv * (uxi - uxj);
+            ty += Cv * (uyi - uyj);
+            tz += Cv * (uzi - uzj);
+        }
+        if (P.fva) {
+            R uij = (uxi - uxj) * g.dx + (uyi - uyj) * g.dy + (uzi - uzj) * g.dz;
+            if (uij < (R)0) {
+                R hij = (th + th) * (R)0.5;
+                R phi = hij * uij / (r * r + (R)0.01 * hij * hij);
+                R Pij = W.m_new[i] * phi * ((R)-0.1 * (R)P.soundspeed + (R)0.02 * phi) / (rhoi + rhoj) * (R)0.5;
+                tx += -Pij * gx;
+                ty += -Pij * gy;
+                tz += -Pij * gz;
+            }
+        }
+        if (eli < (R)1) {
+            R mr = mj / rhoj * ((R)1 - eli);
+            ex += (uxi * (uxj - uxi) * gx + uyi * (uxj - uxi) * gy + uzi * (uxj - uxi) * gz) * mr;
+            ey += (uxi * (uyj - uyi) * gx + uyi * (uyj - uyi) * gy + uzi * (uyj - uyi) * gz) * mr;
+            ez += (uxi * (uzj - uzi) * gx + uyi * (uzj - uzi) * gy + uzi * (uzj - uzi) * gz) * mr;
+            if (P.con) et += (uxi * (tj - tempi) * gx + uyi * (tj - tempi) * gy + uzi * (tj - tempi) * gz) * mr;
+        }
+        if (P.con) {
+            R h = (R)4 * pori * mj * kc * kc * (tempi - tj) * dw;
+            h /= (r + (R)1e-10) * rhoi * rhoj * (kc + kc);
+            Rc += h;
+        }
+        (void)kc_h;
+    }
+    if (filt) S.flt_s[i] = flt;
+    if (!adv) return;
+    if (P.fg) tz += -(R)P.g_sph;
+    W.ftx[i] = tx - ex;
+    W.fty[i] = ty - ey;
+    W.ftz[i] = tz - ez;
+    W.ftot[i] = sqrt(tx * tx + ty * ty + tz * tz);
+    W.pgfx[i] = px;
+    W.pgfy[i] = py;
+    W.pgfz[i] = pz;
+    if (P.con) W.dtemp[i] = Rc / (R)P.cp_sph * (R)(pt != -1) - et;
+}
+
+// ---------------------------------------------------------------------------
+// DEM contact: KERNEL_DEM_interaction3D_dem (functions_DEM_INTERACTION2.cuh:
+// 888-1766).  The history lookup compares against the start-of-step slot
+// ids held in registers; inserts pick the first slot that was free at the
+// start of the step (so two new partners in one step share a slot, as in
+// the reference).  Spring increments and overlap are FP64.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D, DemWork<R> DW,
+                                                     const int* __restrict__ dgs, const int* __restrict__ dge,
+                                                     DevFlags* F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.nd;
+    if (i >= n) return;
+    DW.ftx[i] = 0; DW.fty[i] = 0; DW.ftz[i] = 0;
+    DW.tqx[i] = 0; DW.tqy[i] = 0; DW.tqz[i] = 0;
+    DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
+    if (D.itype[i] != 1 || D.ptype[i] <= 1000) return;
+    double xi = D.x[i], yi = D.y[i], zi = D.z[i], radi = D.rad[i];
+    R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
+    R mi = D.m[i], rii = D.ri[i], rhoi = D.rho[i], tempi = D.temp[i];
+    R pri = (R)P.nu_p, Gi = (R)P.G, ymi = Gi * ((R)2 * ((R)1 + pri));
+    R ymij = (R)1 / ((((R)1 - pri * pri) / ymi) + (((R)1 - pri * pri) / ymi));
+    R Gij = (R)1 / ((((R)2 - pri) / Gi) + (((R)2 - pri) / Gi));
+    R cdamp = sqrt((R)3.333333333) * (R)P.damp;
+    R kci = (R)P.k_dem, cpi = (R)P.cp_dem;
+    R emi = (tempi >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tempi - (R)5.228643e-7 * tempi * tempi +
+                                 (R)1.10479e-10 * tempi * tempi * tempi)
+                              : (R)0.842337;
+    R radiR = (R)radi;
+    R dr2 = ((R)1 / (R)6) * radiR;
+    R volm = ((R)4 / (R)3) * (R)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
+    int oid[SPHDEM_NSLOT];
+#pragma unroll
+    for (int s = 0; s < SPHDEM_NSLOT; s++) oid[s] = D.hid[s * n + i];
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    R tx = 0, ty = 0, tz = 0, tqx = 0, tqy = 0, tqz = 0, dtr = 0, dtc = 0;
+    const double kdt = P.dt;
+    bool ovf = false;
+    for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
+        if (D.ptype[j] <= 1000) return;
+        double xj = D.x[j], yj = D.y[j], zj = D.z[j], radj = D.rad[j];
+        double td = pair_dist(xi, yi, zi, xj, yj, zj);
+        if (!(td < P.r_search * radi && td > 0.0)) return;
+        double ovlp = radi + radj - td;
+        int demj = D.dem_idx[j];
+        R radjR = (R)radj;
+        R radij = (R)1 / ((R)1 / radiR + (R)1 / radjR);
+        R tdR = (R)td;
+        if (P.con) {
+            R tempj = D.temp[j];
+            R emj = (tempj >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tempj - (R)5.228643e-7 * tempj * tempj +
+                                         (R)1.10479e-10 * tempj * tempj * tempj)
+                                      : (R)0.842337;
+            R ai = radiR / tdR, aj = radjR / tdR, dij = aj - ai;
+            R dc_r = (R)0.56 * ((R)2 * radij);
+            R dc_ar = (R)3.14159 * dc_r * dc_r;
+            R dmax = (R)0.5 * (sqrt((R)1 + (R)4 * dc_ar / ((R)3.14159 * tdR * tdR * ((R)1 - dij * dij))) - dij);
+            R ci = ((R)1 - dij * dij) / ((R)2 * dmax) - dij;
+            R cj = ((R)1 - dij * dij) / ((R)2 * (dmax + dij)) + dij;
+            R si = sqrt((R)1 - ci * ci), sj = sqrt((R)1 - cj * cj);
+            R ri_cr = radiR * si, rj_cr = radjR * sj;
+            R td_cr = tdR - radiR * ci - radjR * cj;
+            R z_cr = (R)1 + ((R)4 * rj_cr * rj_cr + td_cr * td_cr) / (ri_cr * ri_cr);
+            R F_cr = (R)0.5 * (z_cr - sqrt(z_cr * z_cr - (R)4 * rj_cr * rj_cr / (ri_cr * ri_cr)));
+            R F_ij = ((R)1 + ci) * F_cr * (R)0.5;
+            R ar_i = (R)2 * (R)3.14159 * radiR * radiR * ((R)1 - ci);
+            R ar_j = (R)2 * (R)3.14159 * radjR * radjR * ((R)1 - cj);
+            R arr = ar_j / ar_i;
+            R Y = F_ij + ((R)1 - F_ij) * (arr / ((R)1 + arr));
+            R einv = ((R)1 - emi) / (emi * ar_i) + ((R)1 - emj) / (emj * ar_j) + (R)1 / (Y * ar_i);
+            dtr += -(R)5.6704e-8 * (tempi * tempi * tempi * tempi - tempj * tempj * tempj * tempj) /
+                   (einv * (rhoi * volm) * cpi);
+        }
+        if (!(td < P.r_contact * radi)) return;
+        if (td > 0 && ovlp > 0) {
+            R tov = (R)ovlp;
+            if (P.con) {
+                R kij = (R)1 / ((R)1 / kci + (R)1 / kci);
+                dtc += -(R)4 * kij * sqrt(((R)2 * tov) * (radij - (R)0.5 * tov)) * (tempi - D.temp[j]) /
+                       ((rhoi * volm) * cpi);
+            }
+            int slot = -1;
+#pragma unroll
+            for (int s = 0; s < SPHDEM_NSLOT; s++)
+                if (slot < 0 && oid[s] == demj) slot = s;
+            double dsx = 0, dsy = 0, dsz = 0;
+            if (slot >= 0) {
+                dsx = D.hds[(slot * 3 + 0) * n + i];
+                dsy = D.hds[(slot * 3 + 1) * n + i];
+                dsz = D.hds[(slot * 3 + 2) * n + i];
+            } else {
+#pragma unroll
+                for (int s = 0; s < SPHDEM_NSLOT; s++)
+                    if (slot < 0 && oid[s] < 1) slot = s;
+                if (slot < 0) { ovf = true; slot = 0; }
+            }
+            R mj = D.m[j];
+            R nx = (R)((xj - xi) / td), ny = (R)((yj - yi) / td), nz = (R)((zj - zi) / td);
+            R li = radiR - (R)0.5 * tov, lj = radjR - (R)0.5 * tov;
+            R rcxi = li * nx, rcyi = li * ny, rczi = li * nz;
+            R rcxj = -lj * nx, rcyj = -lj * ny, rczj = -lj * nz;
+            R wxj = D.wx[j], wyj = D.wy[j], wzj = D.wz[j];
+            R urxi = wyi * rczi - wzi * rcyi, uryi = wzi * rcxi - wxi * rczi, urzi = wxi * rcyi - wyi * rcxi;
+            R urxj = wyj * rczj - wzj * rcyj, uryj = wzj * rcxj - wxj * rczj, urzj = wxj * rcyj - wyj * rcxj;
+            R urx = (D.ux[j] + urxj) - (uxi + urxi);
+            R ury = (D.uy[j] + uryj) - (uyi + uryi);
+            R urz = (D.uz[j] + urzj) - (uzi + urzi);
+            R unm = nx * urx + ny * ury + nz * urz;
+            R unx = unm * nx, uny = unm * ny, unz = unm * nz;
+            R usx = urx - unx, usy = ury - uny, usz = urz - unz;
+            dsx += (double)usx * kdt;
+            dsy += (double)usy * kdt;
+            dsz += (double)usz * kdt;
+            R usm = sqrt(usx * usx + usy * usy + usz * usz) + (R)1e-20;
+            R sx = usx / usm, sy = usy / usm, sz = usz / usm;
+            R mij = (R)1 / ((R)1 / mi + (R)1 / mj);
+            R sq = sqrt(radij * tov);
+            R Cspr = (R)1.33333 * ymij * sqrt(radij) * sqrt(tov) * tov / mi;
+            R Cspr_s = (R)8 * Gij * sq / mi;
+            R Kn = (R)2 * ymij * sq;
+            R Cd = cdamp * sqrt(mij * Kn) / mi;
+            R Cds = cdamp * sqrt(mij * Cspr_s * mi) / mi;
+            tx += Cspr * (R)((xi - xj) / td);
+            ty += Cspr * (R)((yi - yj) / td);
+            tz += Cspr * (R)((zi - zj) / td);
+            tx += Cd * unx;
+            ty += Cd * uny;
+            tz += Cd * unz;
+            R fssx = Cspr_s * (R)dsx + Cds * usx;
+            R fssy = Cspr_s * (R)dsy + Cds * usy;
+            R fssz = Cspr_s * (R)dsz + Cds * usz;
+            R sgx = (fssx >= (R)0) ? (R)1 : (R)-1;
+            R sgy = (fssy >= (R)0) ? (R)1 : (R)-1;
+            R sgz = (fssz >= (R)0) ? (R)1 : (R)-1;
+            R mfss = sqrt(fssx * fssx + fssy * fssy + fssz * fssz);
+            R fr = (R)P.fric * Cspr;
+            R ffx = fr * sx, ffy = fr * sy, ffz = fr * sz;
+            R mfsf = sqrt(ffx * ffx + ffy * ffy + ffz * ffz);
+            bool stick = mfss < mfsf;
+            R fsx = stick ? fssx : sgx * fabs(ffx);
+            R fsy = stick ? fssy : sgy * fabs(ffy);
+            R fsz = stick ? fssz : sgz * fabs(ffz);
+            tx += fsx;
+            ty += fsy;
+            tz += fsz;
+            tqx += mi * (rcyi * fsz - rczi * fsy);
+            tqy += mi * (rczi * fsx - rcxi * fsz);
+            tqz += mi * (rcxi * fsy - rcyi * fsx);
+            D.hid[slot * n + i] = demj;
+            D.hds[(slot * 3 + 0) * n + i] = dsx;
+            D.hds[(slot * 3 + 1) * n + i] = dsy;
+            D.hds[(slot * 3 + 2) * n + i] = dsz;
+        } else {
+            int slot = -1;
+#pragma unroll
+            for (int s = 0; s < SPHDEM_NSLOT; s++)
+                if (slot < 0 && oid[s] == demj) slot = s;
+            if (slot >= 0) {
+                D.hds[(slot * 3 + 0) * n + i] = 0.0;
+                D.hds[(slot * 3 + 1) * n + i] = 0.0;
+                D.hds[(slot * 3 + 2) * n + i] = 0.0;
+                D.hid[slot * n + i] = 0;
+            }
+        }
+    });
+    if (ovf) atomicOr(&F->overflow, 2);
+    if (P.fg) tz += -(R)P.g_dem;
+    if (P.con) {
+        R temp1i = D.temp1[i], temp2i = D.temp2[i], temp3i = D.temp3[i];
+        R a0 = kci / (rhoi * cpi);
+        R dr1 = ((R)5 / (R)6) * radiR / (R)3;
+        R A = ((R)2 * kci / dr1) / ((R)2 * kci / dr1 + kci / dr2), B = (R)1 - A;
+        R ts = A * temp1i + B * tempi;
+        R d0 = (R)2 * (a0 / radiR) * (tempi - ts) / ((R)2 * dr2) + a0 * (tempi - (R)2 * tempi + ts) / (dr2 * dr2);
+        R d1 = ((R)2 * a0 / ((R)2.5 * dr1)) * ((R)2 * ts - temp1i - temp2i) / ((R)2 * dr1) +
+               a0 * ((R)2 * ts - (R)3 * temp1i + temp2i) / (dr1 * dr1);
+        R d2 = (R)2 * (a0 / ((R)1.5 * dr1)) * (temp1i - temp3i) / ((R)2 * dr1) +
+               a0 * (temp1i - (R)2 * temp2i + temp3i) / (dr1 * dr1);
+        R d3 = (R)2 * (a0 / ((R)0.5 * dr1)) * ((temp2i - temp3i) / ((R)2 * dr1)) + a0 * (temp2i - temp3i) / (dr1 * dr1);
+        DW.dtemp[i] = d0 + dtr + dtc;
+        DW.dtemp1[i] = d1;
+        DW.dtemp2[i] = d2;
+        DW.dtemp3[i] = d3;
+    }
+    DW.ftx[i] = tx;
+    DW.fty[i] = ty;
+    DW.ftz[i] = tz;
+    DW.tqx[i] = tqx / rii;
+    DW.tqy[i] = tqy / rii;
+    DW.tqz[i] = tqz / rii;
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_DEM_coupling3D_dem (functions_SPH_DEM_COUPLING2.cuh:627-1129) with
+// KERNEL_clc_projection_dem (functions_TIME_ISPH2.cuh:206-308) fused into its
+// epilogue (the predictor only needs this particle's force).  One warp per
+// DEM sphere; lanes stride over the SPH candidate rows and the partial
+// Shepard sums are reduced with shuffles.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+                                                      DemWork<R> DW, const int* __restrict__ sgs,
+                                                      const int* __restrict__ sge) {
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= P.nd) return;
+    int it = D.itype[i], pt = D.ptype[i];
+    if (it > 2) return;
+    R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i];
+    R ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
+    if (it == 1 && pt > 1000) {
+        double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
+        R radi = (R)D.rad[i], di = (R)2 * radi, voli = ((R)4 / (R)3) * (R)3.14159 * radi * radi * radi;
+        R mi = D.m[i], rhoi = D.rho[i], tempi = D.temp[i];
+        R fa = DW.flt_s[i], ff = DW.flt_sd[i];
+        R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+        double Rr = P.kappa * hi;
+        float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+        int ic, jc, kc;
+        cell_ijk(P, xi, yi, zi, ic, jc, kc);
+        R tx = 0, ty = 0, tz = 0, ufx = 0, ufy = 0, ufz = 0, uax = 0, uay = 0, uaz = 0, por = 0, ttf = 0, tta = 0;
+        int has_f = 0, has_a = 0;
+        R pgc = voli / (mi * ff + (R)1.0e-15);
+        for_stencil_rows(P, ic, jc, kc, sgs, sge, [&](int a, int b) {
+            for (int j = a + lane; j < b; j += 32) {
+                int ptj = S.ptype[j];
+                if (ptj > 1000) continue;
+                R porj = W.DEMpor[j];
+                if (!(porj < (R)1)) continue;
+                PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 0.0, r2l, r2h);
+                if (!g.in) continue;
+                R w = knl_w<R>(P.kernel_type, tA, th, g.r);
+                R mj = W.m_new[j], rhoj = W.rho_new[j], c = mj * w / rhoj;
+                if (ptj == 1 && ff > (R)0.000001) {
+                    has_f = 1;
+                    ufx += S.ux[j] * c; ufy += S.uy[j] * c; ufz += S.uz[j] * c;
+                    por += porj * c;
+                    ttf += S.temp[j] * c;
+                }
+                if (ptj == 3 && fa > (R)0.000001) {
+                    has_a = 1;
+                    uax += S.ux[j] * c; uay += S.uy[j] * c; uaz += S.uz[j] * c;
+                    por += porj * c;
+                    tta += S.temp[j] * c;
+                }
+                if (ptj != 0 && ptj != 9 && ptj != -3 && ptj != 3 && ff > (R)0.01) {
+                    R q = (mj / rhoj) * w * pgc;
+                    tx += W.pgfx[j] * q;
+                    ty += W.pgfy[j] * q;
+                    tz += W.pgfz[j] * q;
+                }
+            }
+        });
+        tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
+        ufx = warp_sum(ufx); ufy = warp_sum(ufy); ufz = warp_sum(ufz);
+        uax = warp_sum(uax); uay = warp_sum(uay); uaz = warp_sum(uaz);
+        por = warp_sum(por); ttf = warp_sum(ttf); tta = warp_sum(tta);
+        has_f = __any_sync(0xffffffffu, has_f);
+        has_a = __any_sync(0xffffffffu, has_a);
+        if (lane != 0) return;
+        R rho_f = has_f ? (R)P.rho_gas : (R)0, rho_a = has_a ? (R)P.rho_gas : (R)0;
+        R ki = (radi < (R)0.0012) ? (R)55.0 : (R)0.84;
+        R ali = (radi < (R)0.0012) ? (R)1.77e-5 : (R)2.5e-6;
+        R cpi = ki / (ali * rhoi);
+        R eps = (R)1.0e-15;
+        R pori = por / (ff + eps);
+        R ux_f = ufx / (ff + eps) - uxi, uy_f = ufy / (ff + eps) - uyi, uz_f = ufz / (ff + eps) - uzi;
+        R tf = ttf / (ff + eps) - tempi;
+        R ux_a = uax / (fa + eps) - uxi, uy_a = uay / (fa + eps) - uyi, uz_a = uaz / (fa + eps) - uzi;
+        R ta = tta / (fa + eps) - tempi;
+        R ux_fa = (ufx + uax) / (ff + fa + eps) - uxi, uy_fa = (ufy + uay) / (ff + fa + eps) - uyi,
+          uz_fa = (ufz + uaz) / (ff + fa + eps) - uzi;
+        R tfa = (ttf + tta) / (ff + fa + eps) - tempi;
+        R f_fluid = ff / (ff + fa + eps), f_air = fa / (ff + fa + eps);
+        R mf = sqrt(ux_f * ux_f + uy_f * uy_f + uz_f * uz_f);
+        DW.magf[i] = mf;
+        R ma = sqrt(ux_a * ux_a + uy_a * uy_a + uz_a * uz_a);
+        R mfa = sqrt(ux_fa * ux_fa + uy_fa * uy_fa + uz_fa * uz_fa);
+        R dfx = 0, dfy = 0, dfz = 0, dax = 0, day = 0, daz = 0, dq = 0;
+        R a_ht = (R)6 / di;
+        R nu = (R)P.nu_gas;
+        DW.DEMpor[i] = pori;
+        if (mf > (R)1.0e-8 && (ff + fa) > (R)0.00001 && f_fluid > (R)0.65) {
+            R Re = di * mf * pori / (nu + eps);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R Cdf = q * q;
+            R lr = (R)1.5 - log10(Re);
+            R bf = (R)3.7 - (R)0.65 * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * Cdf * rho_f * (R)3.14159 * di * di * mf * pow(pori, (R)2 - bf) / mi;
+            dfx = c * ux_f; dfy = c * uy_f; dfz = c * uz_f;
+            dq = ((R)2 + (R)0.6 * sqrt(Re)) * (R)0.0518 / di * a_ht * tf;
+            D.Fdx_df[i] = dfx;
+            D.Fdy_df[i] = dfy;
+            D.Fdz_df[i] = dfz;
+        }
+        if (ma > (R)1.0e-8 && (ff + fa) > (R)0.00001 && f_air > (R)0.65) {
+            R Re = di * pori * ma / (nu + eps);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R lr = (R)1.5 - log10(Re);
+            R b = (R)2.65 * ((R)1 + pori) - ((R)5.3 - (R)3.5 * pori) * pori * pori * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * q * q * rho_a * (R)3.14159 * di * di * ma * pow(pori, (R)-1 - b) / mi;
+            dax = c * ux_a; day = c * uy_a; daz = c * uz_a;
+            dq = ((R)2 + (R)0.6 * sqrt(Re)) * ki / di * a_ht * ta;
+        }
+        if ((ma > (R)1.0e-8 || mf > (R)1.0e-8) && (ff + fa) > (R)0.00001 && f_air <= (R)0.65 && f_fluid <= (R)0.65) {
+            R rfa = (R)P.rho_gas * f_air + (R)P.rho_liquid * f_fluid;
+            R vfa = (R)P.mu_gas * f_air + (R)P.mu_liquid * f_fluid;
+            R vk = vfa / (rfa + eps);
+            R Re = di * pori * mfa / (vk + eps);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R lr = (R)1.5 - log10(Re);
+            R b = (R)2.65 * ((R)1 + pori) - ((R)5.3 - (R)3.5 * pori) * pori * pori * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * q * q * rfa * (R)3.14159 * di * di * mfa * pow(pori, (R)-1 - b) / mi;
+            dax = c * ux_fa; day = c * uy_fa; daz = c * uz_fa;
+            dq = ((R)2 + (R)0.6 * sqrt(Re)) * ki / di * a_ht * tfa;
+        }
+        ftx = ftx + dfx / pori + tx;
+        fty = fty + dfy / pori + ty;
+        ftz = ftz + dfz / pori + tz;
+        DW.ftx[i] = ftx;
+        DW.fty[i] = fty;
+        DW.ftz[i] = ftz;
+        if (P.con) {
+            DW.dtemp[i] = dq / (rhoi * cpi);
+            D.Q_sd[i] = dq * mi / rhoi;
+        }
+        DW.Fdx_da[i] = dax; DW.Fdy_da[i] = day; DW.Fdz_da[i] = daz;
+        DW.Fdx_b[i] = tx; DW.Fdy_b[i] = ty; DW.Fdz_b[i] = tz;
+    }
+    if (lane != 0) return;
+    // predictor (DEM): u* = u + f dt
+    DW.ux0[i] = uxi; DW.uy0[i] = uyi; DW.uz0[i] = uzi;
+    if (pt == 9) {
+        D.ux[i] = (R)P.ball_vel; D.uy[i] = (R)0; D.uz[i] = (R)0;
+        DW.ux0[i] = (R)P.ball_vel; DW.uy0[i] = (R)0; DW.uz0[i] = (R)0;
+    } else if (pt >= 0) {
+        R b = (R)(D.btype[i] == 0);
+        R dt = (R)P.dt;
+        D.ux[i] = uxi + ftx * b * dt;
+        D.uy[i] = uyi + fty * b * dt;
+        D.uz[i] = uzi + ftz * b * dt;
+    }
+    if (P.con && pt > 0) DW.temp0[i] = D.temp[i];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_SPH_coupling3D_sph (functions_SPH_DEM_COUPLING2.cuh:1815-2019) +
+// KERNEL_clc_projection_sph (functions_TIME_ISPH2.cuh:104-204).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+                                                      DemWork<R> DW, const int* __restrict__ dgs,
+                                                      const int* __restrict__ dge, int time_zero) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i];
+    if (it > 2) return;
+    R ftx = W.ftx[i], fty = W.fty[i], ftz = W.ftz[i];
+    if (it == 1 && pt <= 1000) {
+        double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
+        R rhoi = W.rho_new[i], tempi = S.temp[i];
+        // heat_capacity(ptypei, tempi): the reference passes the arguments
+        // swapped (functions_SPH_DEM_COUPLING2.cuh:1860)
+        R cpi = (abs((int)tempi) > 1000) ? (R)P.cp_dem : (R)P.cp_sph;
+        R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+        double Rr = P.kappa * hi;
+        R tx = 0, ty = 0, tz = 0, tt = 0;
+        if (P.nd > 0 && (pt == 1 || pt == 3)) {
+            int ic, jc, kc;
+            cell_ijk(P, xi, yi, zi, ic, jc, kc);
+            for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
+                if (D.ptype[j] <= 1000) return;
+                double d = pair_dist(xi, yi, zi, D.x[j], D.y[j], D.z[j]);
+                if (!(d < Rr)) return;
+                R ffj = DW.flt_sd2[j] + DW.flt_s[j];
+                if (!(ffj > (R)0)) return;
+                R w = knl_w<R>(P.kernel_type, tA, th, (R)d);
+                R c = w / (ffj + (R)1.0e-20);
+                R mr = D.m[j] / rhoi;
+                tx += -mr * D.Fdx_df[j] * c;
+                ty += -mr * D.Fdy_df[j] * c;
+                tz += -mr * D.Fdz_df[j] * c;
+                tt += -D.Q_sd[j] / (rhoi * cpi) * c;
+            });
+        }
+        ftx += tx;
+        fty += ty;
+        ftz += tz;
+        W.ftx[i] = ftx;
+        W.fty[i] = fty;
+        W.ftz[i] = ftz;
+        W.ftot[i] = sqrt(ftx * ftx + fty * fty + ftz * ftz);
+        if (P.con) W.dtemp[i] += tt;
+    }
+    // predictor (SPH), KERNEL_clc_projection_sph
+    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i];
+    W.ux0[i] = uxi; W.uy0[i] = uyi; W.uz0[i] = uzi;
+    if (pt == 9) {
+        S.ux[i] = (R)P.ball_vel; S.uy[i] = (R)0; S.uz[i] = (R)0;
+        W.ux0[i] = (R)P.ball_vel; W.uy0[i] = (R)0; W.uz0[i] = (R)0;
+    } else if (pt >= 0) {
+        R b = (R)(S.btype[i] == 0);
+        R dt = (R)P.sdt;
+        S.ux[i] = uxi + ftx * b * dt;
+        S.uy[i] = uyi + fty * b * dt;
+        S.uz[i] = uzi + ftz * b * dt;
+    }
+    if (time_zero) W.rho_ref[i] = W.rho_new[i];
+    if (P.con && pt > 0) W.temp0[i] = S.temp[i];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_Neumann_boundary3D_sph (functions_BC.cuh:139-274): wall particles
+// take the Shepard average over fluid within 2*kappa*h (W evaluated with
+// 2h) inside the 27-cell stencil.  pres is the array the walls write into.
+// One warp per wall particle (W.wall_idx lists the walls of this step).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, SphWork<R> W, R* pres,
+                                                 const int* __restrict__ gs, const int* __restrict__ ge) {
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= P.nwall) return;
+    int i = W.wall_idx[w];
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
+    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th), th2 = (R)2 * th;
+    double R2 = 2.0 * (P.kappa * hi);
+    float r2l = r2_lo(R2), r2h = r2_hi(R2);
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    R tp = 0, flt = 0, tt = 0, tr = 0;
+    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
+        for (int j = a + lane; j < b; j += 32) {
+            int ptj = S.ptype[j];
+            if (ptj < 1 || ptj >= 1000) continue;
+            PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], R2, 1e-20, r2l, r2h);
+            if (!g.in) continue;
+            R wk = knl_w<R>(P.kernel_type, tA, th2, g.r);
+            R mj = W.m_new[j], rj = W.rho_new[j];
+            R mr = mj / rj * wk;
+            tp += mr * pres[j];
+            flt += mr;
+            tt += mr * S.temp[j];
+            tr += rj / W.DEMpor[j] * wk * mj / rj;
+        }
+    });
+    tp = warp_sum(tp);
+    flt = warp_sum(flt);
+    tt = warp_sum(tt);
+    tr = warp_sum(tr);
+    if (lane != 0) return;
+    if (flt < (R)1e-6) {
+        W.rho_new[i] = W.rho_ref[i];
+        pres[i] = (R)0;
+    } else {
+        pres[i] = tp / flt;
+        S.temp[i] = tt / flt;
+        W.rho_new[i] = W.DEMpor[i] * tr / flt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_PPE3D_sph + KERNEL_PPE3D_calc_sph (functions_PPE2.cuh:542-698,
+// 868-878): one Jacobi sweep; p_new = (b + sum A_ij p_j) / sum A_ij for
+// fluid, every other particle keeps its pressure.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork<R> W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
+    R pcur = S.pres[i];
+    bool solve = it <= 2 && !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
+    if (!solve) {
+        W.p_new[i] = pcur;
+        return;
+    }
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
+    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i], rhoi = W.rho_new[i];
+    R pori = W.DEMpor[i];
+    int cnt = min(W.ncnt[i], P.nb_cap);
+    R bx = 0, by = 0, bz = 0, A = 0, AP = 0;
+    const int* __restrict__ nb = W.nbr;
+    for (int k = 0; k < cnt; k++) {
+        int j = nb[(size_t)k * n + i];
+        if (S.ptype[j] >= 1000 || S.itype[j] == 4) continue;
+        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
+        R r = g.r + (R)1e-20;
+        R mj = W.m_new[j], rhoj = W.rho_new[j], porj = W.DEMpor[j], pj = S.pres[j];
+        R dw = knl_dw<R>(P.kernel_type, tA, th, r);
+        R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
+        kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
+        R mr = mj / rhoj;
+        bx += mr * (pori * uxi - porj * S.ux[j]) * gx;
+        by += mr * (pori * uyi - porj * S.uy[j]) * gy;
+        bz += mr * (pori * uzi - porj * S.uz[j]) * gz;
+        R c = -(g.dx * gx + g.dy * gy + g.dz * gz) / r / r;
+        R a = mj * ((pori * rhoi + porj * rhoj) / (rhoj * rhoi)) * c;
+        A += a;
+        AP += a * pj;
+    }
+    R b = (R)P.rho_gas * (bx + by + bz + (R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
+    W.p_new[i] = (b + AP) / A;
+}
+
+// ---------------------------------------------------------------------------
+// pass C: KERNEL_pressureforce3D_sph (functions_PPE2.cuh:2154-2335) and
+// KERNEL_time_update_projection_sph (functions_TIME_ISPH2.cuh:467-620).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWork<R> W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
+    W.fpx[i] = 0; W.fpy[i] = 0; W.fpz[i] = 0;
+    if (it > 2) return;
+    R fx = 0, fy = 0, fz = 0;
+    bool pf = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
+    if (pf && P.fp) {
+        double xi = S.x[i], yi = S.y[i], zi = S.z[i];
+        R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+        R pi = W.p_new[i], rhoi = W.rho_new[i], pori = W.DEMpor[i];
+        int cnt = min(W.ncnt[i], P.nb_cap);
+        const int* __restrict__ nb = W.nbr;
+        for (int k = 0; k < cnt; k++) {
+            int j = nb[(size_t)k * n + i];
+            if (S.ptype[j] >= 1000) continue;
+            Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
+            R r = g.r + (R)1e-20;
+            R dw = knl_dw<R>(P.kernel_type, tA, th, r);
+            R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
+            kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
+            R Cp = -pori * W.m_new[j] * (pi + W.p_new[j]) / (rhoi * W.rho_new[j]);
+            fx += Cp * gx;
+            fy += Cp * gy;
+            fz += Cp * gz;
+        }
+        W.fpx[i] = fx; W.fpy[i] = fy; W.fpz[i] = fz;
+    }
+    if (pt == 9) return;
+    R ux0, uy0, uz0, ax, ay, az;
+    if (pt > 0) {
+        ux0 = S.ux[i]; uy0 = S.uy[i]; uz0 = S.uz[i];
+        R b = (R)(bt == 0);
+        ax = fx * b; ay = fy * b; az = fz * b;
+    } else {
+        ux0 = W.ux0[i]; uy0 = W.uy0[i]; uz0 = W.uz0[i];
+        ax = ay = az = (R)0;
+    }
+    R dt = (R)P.sdt;
+    R uxc = ux0 + ax * dt, uyc = uy0 + ay * dt, uzc = uz0 + az * dt;
+    R lim = (R)P.u_limit;
+    if ((uxc * uxc + uyc * uyc + uzc * uzc) >= lim * lim) {
+        uxc = ux0; uyc = uy0; uzc = uz0;
+    }
+    if (!P.xsph && P.sph_lagrangian && pt > 0) {
+        S.x[i] += ((double)W.ux0[i] + (double)uxc) / 2.0 * P.sdt;
+        S.y[i] += ((double)W.uy0[i] + (double)uyc) / 2.0 * P.sdt;
+        S.z[i] += ((double)W.uz0[i] + (double)uzc) / 2.0 * P.sdt;
+    }
+    S.ux[i] = uxc; S.uy[i] = uyc; S.uz[i] = uzc;
+    if (P.con && pt > 0) S.temp[i] = W.temp0[i] + W.dtemp[i] * dt * (R)(pt != -1);
+}
+
+// ---------------------------------------------------------------------------
+// DEM corrector (KERNEL_time_update_projection_dem, functions_TIME_ISPH2.cuh:
+// 622-776) followed by KERNEL_treat_DEM_{cylinder_z,box_z,truncated_cone_z}_dem
+// (functions_DEM_BC.cuh:491-718, 1770-2027, 4485-4722) on the same particle.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void dem_wall_response(const DevParams& P, DemState<R>& D, DemWork<R>& DW, int i, R nx, R ny, R nz) {
+    R kdt = (R)P.dt;
+    R ux = D.ux[i], uy = D.uy[i], uz = D.uz[i], wx = D.wx[i], wy = D.wy[i], wz = D.wz[i];
+    R m = D.m[i], ri = D.ri[i], rad = (R)D.rad[i];
+    R ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
+    R ucx = ux - rad * (wy * nz - wz * ny), ucy = uy - rad * (wz * nx - wx * nz), ucz = uz - rad * (wx * ny - wy * nx);
+    R cwx = -rad * (wy * nz - wz * ny), cwy = -rad * (wz * nx - wx * nz), cwz = -rad * (wx * ny - wy * nx);
+    R unm = ux * nx + uy * ny + uz * nz;
+    R ucn = ucx * nx + ucy * ny + ucz * nz, cwn = cwx * nx + cwy * ny + cwz * nz;
+    R usx = ucx - ucn * nx, usy = ucy - ucn * ny, usz = ucz - ucn * nz;
+    R uwx = cwx - cwn * nx, uwy = cwy - cwn * ny, uwz = cwz - cwn * nz;
+    const R tiny = (R)1e-10;
+    if (fabs(usx) < tiny) usx = 0;
+    if (fabs(usy) < tiny) usy = 0;
+    if (fabs(usz) < tiny) usz = 0;
+    if (fabs(uwx) < tiny) uwx = 0;
+    if (fabs(uwy) < tiny) uwy = 0;
+    if (fabs(uwz) < tiny) uwz = 0;
+    R usm = sqrt(usx * usx + usy * usy + usz * usz), uwm = sqrt(uwx * uwx + uwy * uwy + uwz * uwz);
+    R sx = usx / (usm + (R)1e-20), sy = usy / (usm + (R)1e-20), sz = usz / (usm + (R)1e-20);
+    R swx = uwx / (uwm + (R)1e-20), swy = uwy / (uwm + (R)1e-20), swz = uwz / (uwm + (R)1e-20);
+    if (fabs(unm) < (R)50 * kdt) {
+        R fn = ftx * nx + fty * ny + ftz * nz;
+        R a = (R)P.mu_s * m * fn, b = (R)P.mu_rs * m * fn;
+        R ffx = a * sx, ffy = a * sy, ffz = a * sz, frx = b * swx, fry = b * swy, frz = b * swz;
+        if (fn > (R)0) { ffx = ffy = ffz = frx = fry = frz = 0; }
+        DW.ftx[i] = ftx + ffx / m;
+        DW.fty[i] = fty + ffy / m;
+        DW.ftz[i] = ftz + ffz / m;
+        R q = rad / ri;
+        DW.tqx[i] += -q * (ny * (ffz + frz) - nz * (ffy + fry));
+        DW.tqy[i] += -q * (nz * (ffx + frx) - nx * (ffz + frz));
+        DW.tqz[i] += -q * (nx * (ffy + fry) - ny * (ffx + frx));
+        R uxc = ux + (ffx / m) * kdt, uyc = uy + (ffy / m) * kdt, uzc = uz + (ffz / m) * kdt;
+        R ucn2 = uxc * nx + uyc * ny + uzc * nz;
+        D.ux[i] = uxc - ucn2 * nx;
+        D.uy[i] = uyc - ucn2 * ny;
+        D.uz[i] = uzc - ucn2 * nz;
+        D.wx[i] = wx - q * (ny * (ffz + frz) - nz * (ffy + fry)) * kdt;
+        D.wy[i] = wy - q * (nz * (ffx + frx) - nx * (ffz + frz)) * kdt;
+        D.wz[i] = wz - q * (nx * (ffy + fry) - ny * (ffx + frx)) * kdt;
+    } else {
+        R cn = -m * ((R)1 + (R)P.rest_n) * ucn;
+        R cs = -(R)1 / (((R)1 / m) + (rad * rad / ri)) * ((R)1 + (R)P.rest_s) * usm;
+        R Jx = cn * nx + cs * sx, Jy = cn * ny + cs * sy, Jz = cn * nz + cs * sz;
+        R q = rad / ri;
+        D.ux[i] = ux + ((R)1 / m) * Jx;
+        D.uy[i] = uy + ((R)1 / m) * Jy;
+        D.uz[i] = uz + ((R)1 / m) * Jz;
+        D.wx[i] = wx - q * (ny * Jz - nz * Jy);
+        D.wy[i] = wy - q * (nz * Jx - nx * Jz);
+        D.wz[i] = wz - q * (nx * Jy - ny * Jx);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, DemWork<R> DW) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nd) return;
+    int it = D.itype[i], pt = D.ptype[i];
+    if (it > 2) return;
+    if (pt != 9) {
+        R ux0, uy0, uz0;
+        if (pt > 0) { ux0 = D.ux[i]; uy0 = D.uy[i]; uz0 = D.uz[i]; }
+        else { ux0 = DW.ux0[i]; uy0 = DW.uy0[i]; uz0 = DW.uz0[i]; }
+        // fp and fb are zero for DEM particles: the corrector keeps u*
+        R lim = (R)P.u_limit;
+        R uxc = ux0, uyc = uy0, uzc = uz0;
+        if ((uxc * uxc + uyc * uyc + uzc * uzc) >= lim * lim) { uxc = ux0; uyc = uy0; uzc = uz0; }
+        if (pt > 0) {
+            D.x[i] += ((double)DW.ux0[i] + (double)uxc) / 2.0 * P.dt;
+            D.y[i] += ((double)DW.uy0[i] + (double)uyc) / 2.0 * P.dt;
+            D.z[i] += ((double)DW.uz0[i] + (double)uzc) / 2.0 * P.dt;
+        }
+        D.ux[i] = uxc; D.uy[i] = uyc; D.uz[i] = uzc;
+    }
+    if (P.con && pt > 0) D.temp[i] = DW.temp0[i] + DW.dtemp[i] * (R)P.dt * (R)(pt != -1);
+    if (it != 1 || pt <= 1000) return;
+    // cylinder_z
+    if (P.wall_mask & 1) {
+        double xc = P.cyl_cx, yc = P.cyl_cy, Rc = P.cyl_r;
+        double x = D.x[i], y = D.y[i], z = D.z[i], rad = D.rad[i];
+        double F = (x - xc) * (x - xc) + (y - yc) * (y - yc) - (Rc - rad) * (Rc - rad);
+        if (F > 0) {
+            double rr = sqrt((x - xc) * (x - xc) + (y - yc) * (y - yc));
+            double cpx = xc + (Rc - rad) * (x - xc) / rr, cpy = yc + (Rc - rad) * (y - yc) / rr;
+            D.x[i] = cpx; D.y[i] = cpy; D.z[i] = z;
+            double nx = -(cpx - xc) / (Rc - rad), ny = -(cpy - yc) / (Rc - rad);
+            if (!(sqrt(nx * nx + ny * ny) < 0.5)) dem_wall_response<R>(P, D, DW, i, (R)nx, (R)ny, (R)0);
+        }
+    }
+    // box_z
+    if (P.wall_mask & 2) {
+        double xc = P.box_c[0], yc = P.box_c[1], zc = P.box_c[2];
+        double hx = 0.5 * P.box_L[0], hy = 0.5 * P.box_L[1], hz = 0.5 * P.box_L[2];
+        double x = D.x[i], y = D.y[i], z = D.z[i], rad = D.rad[i];
+        double F = fmax(fmax(fabs(x - xc) - (hx - rad), fabs(y - yc) - (hy - rad)), fabs(z - zc) - (hz - rad));
+        if (F > 0) {
+            double cpx = xc + fmin(hx - rad, fmax(-(hx - rad), x - xc));
+            double cpy = yc + fmin(hy - rad, fmax(-(hy - rad), y - yc));
+            double cpz = zc + fmin(hz - rad, fmax(-(hz - rad), z - zc));
+            D.x[i] = cpx; D.y[i] = cpy; D.z[i] = cpz;
+            double sgx = (cpx - x) / (fabs(cpx - x) + 1e-20);
+            double sgy = (cpy - y) / (fabs(cpy - y) + 1e-20);
+            double sgz = (cpz - z) / (fabs(cpz - z) + 1e-20);
+            if (fabs(cpy - y) < 1e-12) sgy = 0.0;
+            if (fabs(cpy - x) < 1e-12) sgx = 0.0;  // the reference tests cpy-x here (functions_DEM_BC.cuh:1846)
+            if (fabs(cpz - z) < 1e-12) sgz = 0.0;
+            double nn = sqrt(sgx * sgx + sgy * sgy + sgz * sgz) + 1e-20;
+            double nx = sgx / nn, ny = sgy / nn, nz = sgz / nn;
+            if (!(sqrt(nx * nx + ny * ny + nz * nz) < 0.5)) dem_wall_response<R>(P, D, DW, i, (R)nx, (R)ny, (R)nz);
+        }
+    }
+    // truncated_cone_z
+    if (P.wall_mask & 4) {
+        double xc = P.cone_c[0], yc = P.cone_c[1], r1 = P.cone_r1, r2 = P.cone_r2, hc = P.cone_h;
+        double x = D.x[i], y = D.y[i], z = D.z[i], rad = D.rad[i];
+        if (!(z <= -hc + rad)) {
+            double L = sqrt((r1 - r2) * (r1 - r2) + hc * hc);
+            double st = hc / L, ct = fabs(r1 - r2) / L, tt = st / ct;
+            double rr = r2 + (hc + z) / tt - rad / st;
+            double rxy = sqrt((x - xc) * (x - xc) + (y - yc) * (y - yc));
+            double F = (x - xc) * (x - xc) + (y - yc) * (y - yc) - rr * rr;
+            if (F > 0) {
+                double cpz = tt * (rxy + rad / st - r2) - hc;
+                D.z[i] = cpz;
+                double nx = -st * (x - xc) / rxy, ny = -st * (y - yc) / rxy, nz = ct;
+                dem_wall_response<R>(P, D, DW, i, (R)nx, (R)ny, (R)nz);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_open_boundary_extrapolation3D_1{,_calc}_sph (functions_BC.cuh:
+// 787-984, 1204-1218): buffer particles take Shepard averages of the fluid
+// around their mirror point.  Only non-buffer fluid is read, so the update
+// is done in place.  One warp per buffer particle (W.buf_idx).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int* __restrict__ gs,
+                                                 const int* __restrict__ ge) {
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= P.nbuf) return;
+    int i = W.buf_idx[w];
+    int bt = S.btype[i];
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
+    double zg = zi;
+    if (bt == 1) zg = 2 * P.L2 - zi;
+    else if (bt == 2) zg = 2 * P.L3 - zi;
+    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    double Rr = P.kappa * hi;
+    float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+    int ic, jc, kc;
+    cell_ijk(P, xi, yi, zg, ic, jc, kc);
+    R hd = (R)P.h_over_dx;
+    R trho = 0, tp = 0, tux = 0, tuy = 0, tuz = 0, tt = 0, flt = 0;
+    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
+        for (int j = a + lane; j < b; j += 32) {
+            if (S.ptype[j] != 1 || S.btype[j] != 0) continue;
+            PairT<R> g = pair_test<R>(xi, yi, zg, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
+            if (!g.in) continue;
+            R wk = knl_w<R>(P.kernel_type, tA, th, g.r);
+            R hj = (R)S.h[j];
+            R volj = (hj / hd) * (hj / hd) * (hj / hd);
+            R vw = volj * wk;
+            trho += W.rho_new[j] / W.DEMpor[j] * wk * volj;
+            tp += vw * W.p_new[j];
+            tuz += vw * S.uz[j];
+            tux += vw * S.ux[j];
+            tuy += vw * S.uy[j];
+            tt += vw * S.temp[j];
+            flt += vw;
+        }
+    });
+    trho = warp_sum(trho); tp = warp_sum(tp); tux = warp_sum(tux); tuy = warp_sum(tuy);
+    tuz = warp_sum(tuz); tt = warp_sum(tt); flt = warp_sum(flt);
+    if (lane != 0 || P.open_bc != 1) return;
+    R pori = W.DEMpor[i];
+    R vol0 = (th / hd) * (th / hd) * (th / hd);
+    R rho_old = W.rho_new[i];
+    if (bt == 1) {
+        W.p_new[i] = tp / flt;
+        W.rho_new[i] = pori * (R)P.rho_gas;
+        W.m_new[i] = rho_old * vol0;
+        S.uz[i] = (R)P.inlet_uz * (R)2 - tuz / flt;
+        S.ux[i] = (R)0 - tux / flt;
+        S.uy[i] = (R)0 - tuy / flt;
+        S.temp[i] = (R)P.inlet_temp;
+    } else {
+        W.p_new[i] = (R)0;
+        W.rho_new[i] = pori * (trho / flt);
+        W.m_new[i] = rho_old * vol0;
+        S.uz[i] = tuz / flt;
+        S.ux[i] = tux / flt;
+        S.uy[i] = tuy / flt;
+        S.temp[i] = tt / flt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_xsph3D_sph + KERNEL_xsph3D_calc_sph (functions_TIME.cuh:1735-1997).
+// Writes the smoothed velocity/temperature of every particle (or a copy)
+// into u_tmp/temp_tmp; the next reorder reads them.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWork<R> W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    int it = S.itype[i], pt = S.ptype[i];
+    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i], ti = S.temp[i];
+    if (it != 1 || pt > 1000 || pt == 0 || pt == 9) {
+        W.u_tmpx[i] = uxi; W.u_tmpy[i] = uyi; W.u_tmpz[i] = uzi; W.temp_tmp[i] = ti;
+        return;
+    }
+    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
+    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R c = (R)P.c_xsph;
+    int cnt = min(W.ncnt[i], P.nb_cap);
+    R tx = 0, ty = 0, tz = 0, tt = 0, flt = 0;
+    const int* __restrict__ nb = W.nbr;
+    for (int k = 0; k < cnt; k++) {
+        int j = nb[(size_t)k * n + i];
+        int ptj = S.ptype[j];
+        if (ptj != 1 && ptj != 3) continue;
+        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
+        R w = knl_w<R>(P.kernel_type, tA, th, g.r);
+        R mr = W.m_new[j] / W.rho_new[j] * w;
+        tx += c * mr * (S.ux[j] - uxi);
+        ty += c * mr * (S.uy[j] - uyi);
+        tz += c * mr * (S.uz[j] - uzi);
+        tt += (R)0.01 * c * mr * (S.temp[j] - ti);
+        flt += mr;
+    }
+    R on = (R)(pt > 0);
+    W.u_tmpx[i] = (uxi + tx / flt) * on;
+    W.u_tmpy[i] = (uyi + ty / flt) * on;
+    W.u_tmpz[i] = (uzi + tz / flt) * on;
+    W.temp_tmp[i] = (ti + tt / flt) * on;
+}
+
+// ---------------------------------------------------------------------------
+// printed maxima (kernel_copy_max_*, functions_OUTPUT.cuh:19-65 + cub max)
+// out[0..2] = rho, |u|, ftotal over p_type!=0 && i_type<2.
+// One block, grid-stride; used off the timed path.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_stats(int n, const R* __restrict__ rho, const R* __restrict__ ux, const R* __restrict__ uy,
+                        const R* __restrict__ uz, const R* __restrict__ ft, const int* __restrict__ ptype,
+                        const int* __restrict__ itype, double* out, DevFlags* F) {
+    __shared__ double sm[3][256];
+    double a = 0, b = 0, c = 0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double u = sqrt((double)ux[i] * ux[i] + (double)uy[i] * uy[i] + (double)uz[i] * uz[i]);
+        if (!isfinite(u) || !isfinite((double)rho[i])) bad = 1;
+        if (ptype[i] == 0 || itype[i] >= 2) continue;
+        a = fmax(a, (double)rho[i]);
+        b = fmax(b, u);
+        c = fmax(c, ft ? (double)ft[i] : 0.0);
+    }
+    sm[0][threadIdx.x] = a; sm[1][threadIdx.x] = b; sm[2][threadIdx.x] = c;
+    if (bad) atomicOr(&F->nan, 1);
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 3; q++) sm[q][threadIdx.x] = fmax(sm[q][threadIdx.x], sm[q][threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) out[q] = sm[q][0];
+}
+
+}  // namespace sphdem

@@ -1,0 +1,212 @@
+"""Python binding of the C ABI in include/sphdem.h (libsphdem.so).
+
+Mirrors the reference's per-step operator: ``Engine.step(n)`` advances n
+calls of SOPHIA_single_ISPH (ISPH_Calc_seperate.cuh:13-503) plus the host
+loop's ``time += dt; count++`` (ISPH_Calc_seperate.cuh:924-925).  There is
+no CPU fallback: if the CUDA library is missing or a call fails, an
+exception is raised.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .params import DEM, F, INT_FIELDS, SPH, STATUS, SphdemParams, SphdemStats
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsphdem.so")
+_lib = None
+
+
+class SphdemError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+def lib():
+    """Load libsphdem.so (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: the CUDA extension is not built")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp = C.c_void_p
+    L.sphdem_params_default.argtypes = [P(SphdemParams)]
+    L.sphdem_read_solv.argtypes = [C.c_char_p, P(SphdemParams)]
+    L.sphdem_create.argtypes = [P(SphdemParams), C.c_int32, C.c_int32, P(vp)]
+    L.sphdem_create_from_dir.argtypes = [C.c_char_p, P(SphdemParams), P(vp)]
+    L.sphdem_set_field.argtypes = [vp, C.c_int, C.c_int, vp, C.c_size_t]
+    L.sphdem_commit_particles.argtypes = [vp]
+    L.sphdem_step.argtypes = [vp, C.c_int32]
+    L.sphdem_get_field.argtypes = [vp, C.c_int, C.c_int, vp, C.c_size_t]
+    L.sphdem_get_stats.argtypes = [vp, P(SphdemStats)]
+    L.sphdem_get_neighbors.argtypes = [vp, P(C.c_int32), P(C.c_int32), C.c_int32]
+    L.sphdem_get_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
+    L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
+    L.sphdem_input_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
+    L.sphdem_input_column.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, C.c_size_t]
+    L.sphdem_write_restart.argtypes = [vp, C.c_char_p]
+    L.sphdem_get_time.argtypes = [vp, P(C.c_double), P(C.c_int32)]
+    L.sphdem_get_counts.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
+    L.sphdem_get_stream.argtypes = [vp, P(vp)]
+    L.sphdem_get_launch_count.argtypes = [vp, P(C.c_int64)]
+    L.sphdem_destroy.argtypes = [vp]
+    L.sphdem_destroy.restype = None
+    L.sphdem_strerror.argtypes = [C.c_int]
+    L.sphdem_strerror.restype = C.c_char_p
+    L.sphdem_params_size.argtypes = []
+    if L.sphdem_params_size() != C.sizeof(SphdemParams):
+        raise RuntimeError("SphdemParams layout mismatch between params.py and libsphdem.so")
+    _lib = L
+    return L
+
+
+def _chk(status, what):
+    if status != 0:
+        raise SphdemError(status, what)
+
+
+def default_params():
+    p = SphdemParams()
+    _chk(lib().sphdem_params_default(C.byref(p)), "sphdem_params_default")
+    return p
+
+
+def read_solv(path, params=None):
+    p = params.copy() if params is not None else default_params()
+    _chk(lib().sphdem_read_solv(os.fsencode(path), C.byref(p)), "sphdem_read_solv")
+    return p
+
+
+class Engine:
+    """One engine handle on the current CUDA device."""
+
+    def __init__(self, params, sph, dem):
+        """params: SphdemParams; sph/dem: dict field-name -> array in input order."""
+        L = lib()
+        ns = len(sph["x"]) if sph else 0
+        nd = len(dem["x"]) if dem else 0
+        self._h = C.c_void_p()
+        _chk(L.sphdem_create(C.byref(params), ns, nd, C.byref(self._h)), "sphdem_create")
+        self.params = params.copy()
+        self.ns, self.nd = ns, nd
+        try:
+            for which, d in ((SPH, sph), (DEM, dem)):
+                for name, arr in (d or {}).items():
+                    self._set(which, name, arr)
+            _chk(L.sphdem_commit_particles(self._h), "sphdem_commit_particles")
+        except Exception:
+            self.close()
+            raise
+
+    @classmethod
+    def from_dir(cls, path, precision=0):
+        self = cls.__new__(cls)
+        L = lib()
+        ov = default_params()
+        ov.precision = precision
+        self._h = C.c_void_p()
+        _chk(L.sphdem_create_from_dir(os.fsencode(path), C.byref(ov), C.byref(self._h)), "sphdem_create_from_dir")
+        ns, nd = C.c_int32(), C.c_int32()
+        L.sphdem_get_counts(self._h, C.byref(ns), C.byref(nd))
+        self.ns, self.nd = ns.value, nd.value
+        self.params = read_solv(os.path.join(path, "solv.txt"))
+        return self
+
+    def _set(self, which, name, arr):
+        fid = F[name]
+        if name in INT_FIELDS:
+            a = np.ascontiguousarray(arr, dtype=np.int32)
+        else:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+        _chk(lib().sphdem_set_field(self._h, which, fid, a.ctypes.data, a.nbytes), f"sphdem_set_field({name})")
+
+    def step(self, n=1):
+        _chk(lib().sphdem_step(self._h, int(n)), "sphdem_step")
+
+    def get(self, which, name):
+        n = self.nd if which == DEM else self.ns
+        if name in INT_FIELDS:
+            a = np.empty(n, dtype=np.int32)
+        else:
+            a = np.empty(n, dtype=np.float64)
+        _chk(lib().sphdem_get_field(self._h, which, F[name], a.ctypes.data, a.nbytes), f"sphdem_get_field({name})")
+        return a
+
+    def stats(self):
+        s = SphdemStats()
+        _chk(lib().sphdem_get_stats(self._h, C.byref(s)), "sphdem_get_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def neighbors(self, cap=512):
+        counts = np.zeros(self.ns, dtype=np.int32)
+        lst = np.full((self.ns, cap), -1, dtype=np.int32)
+        _chk(lib().sphdem_get_neighbors(self._h, counts.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        lst.ctypes.data_as(C.POINTER(C.c_int32)), cap), "sphdem_get_neighbors")
+        return counts, lst
+
+    def history(self):
+        ids = np.zeros((self.nd, 16), dtype=np.int32)
+        sp = np.zeros((self.nd, 16, 3), dtype=np.float64)
+        _chk(lib().sphdem_get_history(self._h, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      sp.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_get_history")
+        return ids, sp
+
+    def time(self):
+        t, c = C.c_double(), C.c_int32()
+        lib().sphdem_get_time(self._h, C.byref(t), C.byref(c))
+        return t.value, c.value
+
+    def stream_ptr(self):
+        s = C.c_void_p()
+        lib().sphdem_get_stream(self._h, C.byref(s))
+        return s.value or 0
+
+    def launches(self):
+        n = C.c_int64()
+        lib().sphdem_get_launch_count(self._h, C.byref(n))
+        return n.value
+
+    def write_vtk_dem(self, path):
+        _chk(lib().sphdem_write_vtk_dem(self._h, os.fsencode(path)), "sphdem_write_vtk_dem")
+
+    def write_restart(self, path):
+        _chk(lib().sphdem_write_restart(self._h, os.fsencode(path)), "sphdem_write_restart")
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().sphdem_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def read_input_txt(path):
+    """Host-only read of an input.txt: returns (sph, dem) dicts of arrays."""
+    L = lib()
+    ns, nd = C.c_int32(), C.c_int32()
+    _chk(L.sphdem_input_counts(os.fsencode(path), C.byref(ns), C.byref(nd)), "sphdem_input_counts")
+    out = []
+    for which, n in ((SPH, ns.value), (DEM, nd.value)):
+        d = {}
+        for name in ("x", "y", "z", "ux", "uy", "uz", "m", "h", "temp", "pres", "rho", "flt_s", "rad", "ri",
+                     "wx", "wy", "wz", "temp1", "temp2", "temp3", "p_type", "dem_idx"):
+            a = np.zeros(n, dtype=np.int32 if name in INT_FIELDS else np.float64)
+            _chk(L.sphdem_input_column(os.fsencode(path), which, F[name], a.ctypes.data, a.nbytes),
+                 f"sphdem_input_column({name})")
+            d[name] = a
+        out.append(d)
+    return out[0], out[1]

@@ -1,0 +1,305 @@
+/*
+ * sphdem.h -- C ABI of the B200 SPH-DEM step engine.
+ *
+ * The engine replaces the per-step kernel sequence that SOPHIA_gpu's time
+ * loop calls once per iteration:
+ *   SOPHIA_single_ISPH(...)   ISPH_Calc_seperate.cuh:13-503  (ISPH + DEM)
+ * driven by the host loop at ISPH_Calc_seperate.cuh:905-975 (time += dt,
+ * count++ after every step).  The reference passes ~40 raw device pointers
+ * and reads solver switches from __constant__ k_vii/k_vif
+ * (SOPHIA_gpu.cu:47-56, function_init.cuh:1-213).  Here the same switches
+ * travel in SphdemParams and the particle state lives behind an opaque
+ * handle; every entry point returns an int status (0 = ok, <0 = error) and
+ * never exits the process (the reference's CUDA_CHECK calls exit(),
+ * ISPH.cuh:1-8).
+ *
+ * Threading: one handle per device and host thread (the reference runs one
+ * pthread per GPU, ISPH.cuh:178-181).  A handle must not be used from two
+ * host threads at the same time.  Steps run asynchronously on the handle's
+ * CUDA stream; sphdem_get_* synchronise.
+ */
+#ifndef SPHDEM_H
+#define SPHDEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define SPHDEM_OK              0
+#define SPHDEM_E_ARG          -1   /* bad argument / null pointer            */
+#define SPHDEM_E_CUDA         -2   /* a CUDA runtime call failed             */
+#define SPHDEM_E_INPUT        -3   /* malformed solv.txt / input.txt / data  */
+#define SPHDEM_E_OVERFLOW     -4   /* neighbour list or contact history full */
+#define SPHDEM_E_NAN          -5   /* non-finite value detected in the state */
+#define SPHDEM_E_TIMEOUT      -6   /* a bounded device wait gave up          */
+#define SPHDEM_E_UNSUPPORTED  -7   /* switch combination not implemented     */
+#define SPHDEM_E_NOMEM        -8   /* allocation failed / size above limit   */
+
+/* ---- solver switches (values of solv.txt, function_init.cuh:216-615) -- */
+#define SPHDEM_WCSPH 0
+#define SPHDEM_ISPH  1
+#define SPHDEM_DFSPH 2
+
+/* kernel_type (Parameters.cuh) */
+#define SPHDEM_KERNEL_GAUSSIAN  0
+#define SPHDEM_KERNEL_QUINTIC   1
+#define SPHDEM_KERNEL_QUARTIC   2
+#define SPHDEM_KERNEL_WENDLAND2 3
+#define SPHDEM_KERNEL_WENDLAND4 4
+#define SPHDEM_KERNEL_WENDLAND6 5
+
+/* PPE solution method.  REFERENCE = one Jacobi sweep per step with the
+ * previous pressure as iterate (functions_PPE2.cuh:542-698, 868-878).
+ * KRYLOV = matrix-free Jacobi-preconditioned BiCGStab on the same operator
+ * to a relative residual ppe_tol (no reference counterpart). */
+#define SPHDEM_PPE_REFERENCE 0
+#define SPHDEM_PPE_KRYLOV    1
+
+/* Warm start for the KRYLOV mode: previous pressure or the learned MLP. */
+#define SPHDEM_WARM_PREVIOUS 0
+#define SPHDEM_WARM_MLP      1
+
+/* Precision of the non-position fields inside the engine. */
+#define SPHDEM_PREC_FP32 0
+#define SPHDEM_PREC_FP64 1
+
+typedef struct SphdemParams {
+    /* -- integer switches: vii[] of function_init.cuh:2-58 -- */
+    int32_t solver_type;        /* vii[0]  */
+    int32_t dim;                /* vii[1]  */
+    int32_t prop_table;         /* vii[2]  */
+    int32_t kernel_type;        /* vii[3]  */
+    int32_t flt_type;           /* vii[4]  */
+    int32_t rho_type;           /* vii[5]  0 Direct, 1 Continuity */
+    int32_t time_type;          /* vii[6]  0 Euler, 1 Predictor_Corrector */
+    int32_t fluid_type;         /* vii[7]  */
+    int32_t open_boundary;      /* vii[8]  0 NO, 1 OPEN, 2 PERIODIC */
+    int32_t simulation_type;    /* vii[9]  */
+    int32_t freq_cell;          /* vii[10] */
+    int32_t flag_z_index;       /* vii[11] */
+    int32_t flag_timestep_update; /* vii[12] */
+    int32_t nb_cell_type;       /* vii[13] */
+    int32_t freq_filt;          /* vii[14] */
+    int32_t freq_mass_sum;      /* vii[15] */
+    int32_t freq_temp;          /* vii[16] */
+    int32_t freq_output;        /* vii[17] */
+    int32_t fp_solve;           /* vii[18] */
+    int32_t fv_solve;           /* vii[19] */
+    int32_t fva_solve;          /* vii[20] */
+    int32_t fg_solve;           /* vii[21] */
+    int32_t fs_solve;           /* vii[22] */
+    int32_t fb_solve;           /* vii[23] */
+    int32_t con_solve;          /* vii[24] */
+    int32_t boussinesq_solve;   /* vii[25] */
+    int32_t interface_solve;    /* vii[26] */
+    int32_t surf_model;         /* vii[27] */
+    int32_t xsph_solve;         /* vii[28] */
+    int32_t kgc_solve;          /* vii[29] 0 NO, 1 KGC */
+    int32_t delSPH_solve;       /* vii[30] 0 NO, 1 Molteni, 2 Antuono */
+    int32_t delSPH_model;       /* vii[31] */
+    int32_t pst_solve;          /* vii[32] */
+    int32_t turbulence_model;   /* vii[33] */
+    int32_t concn_solve;        /* vii[34] */
+    int32_t min_iteration;      /* vii[35] */
+    int32_t max_iteration;      /* vii[36] */
+    int32_t penetration_solve;  /* vii[49] */
+    int32_t switch_ptype;       /* vii[50] */
+    int32_t noslip_bc;          /* vii[51] */
+    int32_t decouple_stride;    /* vii[57] */
+    int32_t ppe_mode;           /* SPHDEM_PPE_*  (engine extension)      */
+    int32_t warm_start;         /* SPHDEM_WARM_* (engine extension)      */
+    int32_t ppe_max_iter;       /* KRYLOV iteration cap                  */
+    int32_t precision;          /* SPHDEM_PREC_* (engine extension)      */
+    int32_t dem_wall_mask;      /* bit0 cylinder_z, bit1 box_z, bit2 truncated_cone_z */
+    int32_t reserved_i[6];
+
+    /* -- real switches: vif[] of function_init.cuh:59-100 -- */
+    double kappa;               /* vif[0]  */
+    double p_ref;               /* vif[1]  */
+    double gamma;               /* vif[2]  */
+    double dt;                  /* vif[3]  */
+    double time;                /* vif[4]  start time */
+    double time_end;            /* vif[5]  */
+    double margin[6];           /* vif[6..11] X-,X+,Y-,Y+,Z-,Z+ */
+    double u_limit;             /* vif[12] */
+    double c_xsph;              /* vif[13] */
+    double c_repulsive;         /* vif[14] */
+    double drho_th;             /* vif[15] */
+    double dp_th;               /* vif[16] */
+    double p_relaxation;        /* vif[17] */
+    double soundspeed;          /* vif[25] */
+    double rho0_eos;            /* vif[26] */
+    double ball_vel;            /* vif[30] */
+    double ppe_tol;             /* KRYLOV relative residual target */
+
+    /* -- constants the reference hard-wires with #define; the
+     *    reference-compat preset reproduces them exactly. -- */
+    double rho_gas;             /* DENSITY_AIR 1.784 (Parameters.cuh:59) */
+    double rho_liquid;          /* DENSITY_WATER 1000 (Parameters.cuh:58) */
+    double mu_gas;              /* VISCOSITY_AIR 2e-5 (Parameters.cuh:62) */
+    double mu_liquid;           /* VISCOSITY_WATER 1e-3 (Parameters.cuh:61) */
+    double g_sph;               /* Gravitational_CONST 9.8 (Parameters.cuh:81) */
+    double g_dem;               /* 9.8 (functions_DEM_INTERACTION2.cuh:1702) */
+    double h_over_dx;           /* 1.6 (functions_MASS.cuh:33) */
+    double k_sph;               /* SPH conductivity 0.0518 (functions_PROP.cuh:271) */
+    double cp_sph;              /* SPH heat capacity 1006.4 (functions_PROP.cuh:409) */
+    double k_dem;               /* DEM conductivity 2.5 (functions_PROP.cuh:258-268) */
+    double cp_dem;              /* DEM heat capacity 1068 (functions_PROP.cuh:401) */
+    double dem_shear_modulus;   /* 8.3e8 (functions_PROP.cuh:507) */
+    double dem_poisson;         /* 0.23 (functions_PROP.cuh:491) */
+    double dem_damp_coef;       /* 0.0535184 (e=0.9) (functions_DEM_INTERACTION2.cuh:1471) */
+    double dem_friction_ratio;  /* 0.5 (functions_DEM_INTERACTION2.cuh:1528-1530) */
+    double dem_contact_range;   /* 2.01 x radius (functions_DEM_INTERACTION2.cuh:1083) */
+    double dem_search_range;    /* 3.5 x radius (functions_DEM_INTERACTION2.cuh:1038) */
+    double nu_gas;              /* mu/rho used by the drag Reynolds number */
+    double inlet_uz_mirror;     /* 24.045 (functions_BC.cuh:962) */
+    double inlet_temp;          /* 823 (functions_BC.cuh:966) */
+    double obc_L1, obc_L2, obc_L3, obc_L4;  /* functions_NNPS.cuh:2-5 */
+    double cyl_cx, cyl_cy, cyl_r;           /* functions_DEM_BC.cuh:254-257 */
+    double box_c[3], box_L[3];              /* functions_DEM_BC.cuh:1503-1509 */
+    double cone_c[3], cone_r1, cone_r2, cone_h; /* functions_DEM_BC.cuh:723-725,4237-4243 */
+    double wall_rest_n, wall_rest_s, wall_mu_s, wall_mu_rs; /* functions_DEM_BC.cuh:1-5 */
+    double reserved_d[8];
+} SphdemParams;
+
+/* Particle fields addressable through get/set.  Values cross the ABI as
+ * double (or int32 for the integer fields), in the engine's current
+ * (cell-sorted) order; SPHDEM_F_PID gives the input row of each slot. */
+typedef enum SphdemField {
+    SPHDEM_F_X = 0, SPHDEM_F_Y, SPHDEM_F_Z,
+    SPHDEM_F_UX, SPHDEM_F_UY, SPHDEM_F_UZ,
+    SPHDEM_F_WX, SPHDEM_F_WY, SPHDEM_F_WZ,
+    SPHDEM_F_M, SPHDEM_F_RHO, SPHDEM_F_PRES, SPHDEM_F_TEMP,
+    SPHDEM_F_H, SPHDEM_F_RAD, SPHDEM_F_RI,
+    SPHDEM_F_DEMPOR, SPHDEM_F_DDEMPOR, SPHDEM_F_FLT_S,
+    SPHDEM_F_FLT_SD, SPHDEM_F_FLT_SD2,
+    SPHDEM_F_FTOTALX, SPHDEM_F_FTOTALY, SPHDEM_F_FTOTALZ,
+    SPHDEM_F_FPX, SPHDEM_F_FPY, SPHDEM_F_FPZ,
+    SPHDEM_F_PGFX, SPHDEM_F_PGFY, SPHDEM_F_PGFZ,
+    SPHDEM_F_FDX_DF, SPHDEM_F_FDY_DF, SPHDEM_F_FDZ_DF,
+    SPHDEM_F_TORQX, SPHDEM_F_TORQY, SPHDEM_F_TORQZ,
+    SPHDEM_F_RHO_REF, SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3,
+    SPHDEM_F_DTEMP, SPHDEM_F_Q_SD,
+    /* integer fields (int32 buffers) */
+    SPHDEM_F_PTYPE = 64, SPHDEM_F_ITYPE, SPHDEM_F_BUFFER_TYPE,
+    SPHDEM_F_DEM_IDX, SPHDEM_F_PID, SPHDEM_F_CELL
+} SphdemField;
+
+#define SPHDEM_SPH 0
+#define SPHDEM_DEM 1
+
+typedef struct SphdemStats {
+    double rho_max_sph, u_max_sph, ftotal_max_sph;   /* ISPH_Calc_seperate.cuh:928-968 */
+    double rho_max_dem, u_max_dem, ftotal_max_dem;
+    int32_t count;              /* step counter (vii[43])                 */
+    int32_t ppe_iters;          /* iterations of the last PPE solve       */
+    double  time;               /* simulated time (vif[4])                */
+    double  ppe_rel_residual;   /* last PPE relative residual (KRYLOV)    */
+    double  ppe_ms;             /* device time of the last PPE solve      */
+    int32_t overflow_flags;     /* bit0 SPH list, bit1 DEM history        */
+    int32_t nan_flag;
+} SphdemStats;
+
+typedef struct SphdemHandle SphdemHandle;
+
+/* Reference-compat preset: the switches of the reference's own
+ * input/solv.txt and every hard-wired constant listed above. */
+int sphdem_params_default(SphdemParams* p);
+
+/* Keyword parser for solv.txt (function_init.cuh:216-615).  Fields not
+ * named in the file keep the values already in *p. */
+int sphdem_read_solv(const char* path, SphdemParams* p);
+
+/* Host-only reader of input.txt (function_init.cuh:743-891): particle
+ * counts after the SPH/DEM split (p_type <= 1000 is SPH), then one column
+ * per call in input order within the set.  No GPU is touched. */
+int sphdem_input_counts(const char* input_txt, int32_t* n_sph, int32_t* n_dem);
+int sphdem_input_column(const char* input_txt, int which, int field,
+                        void* host_dst, size_t bytes);
+
+/* Create an engine for n_sph SPH and n_dem DEM particles on the current
+ * CUDA device.  Particle data is then uploaded with sphdem_set_field and
+ * sphdem_commit_particles. */
+int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem,
+                  SphdemHandle** out);
+
+/* Read input_dir/solv.txt, input_dir/data.txt and input_dir/input.txt
+ * (function_init.cuh:216-1182, ISPH.cuh:55-113) and create an engine.
+ * ov may be NULL; when given, its non-switch engine extensions
+ * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter) override the
+ * defaults. */
+int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
+                           SphdemHandle** out);
+
+/* Upload one field for the SPH (which=0) or DEM (which=1) set from host
+ * memory, in input order.  bytes = n * 8 (real fields) or n * 4 (int). */
+int sphdem_set_field(SphdemHandle* h, int which, int field,
+                     const void* host_src, size_t bytes);
+
+/* Finish the particle upload: bounding box, cell grid, buffer tags
+ * (ISPH.cuh:104-113, functions_NNPS.cuh:60-200).  Must be called once
+ * after the last sphdem_set_field and before the first step. */
+int sphdem_commit_particles(SphdemHandle* h);
+
+/* Advance nsteps time steps (one SOPHIA_single_ISPH + time/count update
+ * each).  Asynchronous on the handle's stream. */
+int sphdem_step(SphdemHandle* h, int32_t nsteps);
+
+/* Copy a field back to host memory (synchronises). */
+int sphdem_get_field(SphdemHandle* h, int which, int field,
+                     void* host_dst, size_t bytes);
+
+/* Maxima printed by the reference every freq_output/10 steps, plus PPE
+ * statistics (synchronises). */
+int sphdem_get_stats(SphdemHandle* h, SphdemStats* out);
+
+/* Cell-sorted neighbour list of the SPH set as built for the current
+ * step: counts[n_sph] and, for each particle, its neighbours within
+ * kappa*h in the reference's visit order (27 cells z,y,x; ascending
+ * slot), as slot indices.  cap = row capacity of dst (ints per row). */
+int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* dst,
+                         int32_t cap);
+
+/* Tangential contact history of the DEM set (16 slots per sphere,
+ * class_Cuda_Particle_Array2.cuh:57-58): partner dem_idx (0 = free) as
+ * ids[n*16] and spring vectors as springs[n*16*3], particle-major, in the
+ * current sorted order. */
+int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs);
+
+/* Binary legacy-VTK POLYDATA of the DEM set, the format of
+ * save_plot_fluid_vtk_bin_solid_dem (functions_OUTPUT.cuh:1135-1446). */
+int sphdem_write_vtk_dem(SphdemHandle* h, const char* path);
+
+/* Restart file in input.txt format: tab-separated column labels then one
+ * row per particle with all columns (fixes save_restart,
+ * functions_OUTPUT.cuh:1926-1955). */
+int sphdem_write_restart(SphdemHandle* h, const char* path);
+
+/* Simulated time and step count of the handle. */
+int sphdem_get_time(SphdemHandle* h, double* time, int32_t* count);
+
+/* Static particle counts of the handle. */
+int sphdem_get_counts(SphdemHandle* h, int32_t* n_sph, int32_t* n_dem);
+
+/* The CUDA stream the handle launches on (as an opaque pointer). */
+int sphdem_get_stream(SphdemHandle* h, void** stream);
+
+/* Number of engine kernels launched by the last sphdem_step call. */
+int sphdem_get_launch_count(SphdemHandle* h, int64_t* launches);
+
+/* sizeof(SphdemParams) as compiled into the library (binding check). */
+int sphdem_params_size(void);
+
+void sphdem_destroy(SphdemHandle* h);
+
+/* Human-readable text of a status code. */
+const char* sphdem_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHDEM_H */

@@ -1,0 +1,132 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Runs on a machine with a B200 and the reference harness built
+(``make -C oracle ref`` -> oracle/_ref/libsophia_ref.so, compiled from
+the unmodified reference sources).  For every case it writes the
+synthetic bed in the reference's input formats, lets the reference's own
+SOPHIA_single_ISPH advance it, and stores inputs plus the read-back state
+after each checkpoint in tests/golden/<case>.npz.
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py --case contact
+
+Each case runs in its own process because the reference keeps its state
+in globals and changes the working directory.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from fluidized_bed_master_b200.beds import spouted_bed, write_input_dir  # noqa: E402
+
+SPH_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor", "dDEMpor", "flt_s",
+              "pgfx", "pgfy", "pgfz", "rho_ref", "ftotalx", "ftotaly", "ftotalz", "fpx", "fpy", "fpz",
+              "p_type", "i_type", "buffer_type", "pid"]
+DEM_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "DEMpor", "flt_s", "flt_sd", "flt_sd2",
+              "Fdx_df", "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz", "dtemp",
+              "dem_idx"]
+
+# name -> (generator kwargs, param overrides, checkpoints)
+CASES = {
+    # reference-compat bed, spheres starting in contact (Hertz-Mindlin,
+    # tangential history insert/lookup/release), drag from moving spheres
+    "contact": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=11, spacing=1.9, u_dem=0.05),
+                dict(), [1, 8]),
+    # same bed with heat transfer on (SPH conduction, DEM shells,
+    # radiation, contact conduction, convective exchange)
+    "heat": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=12, spacing=1.9, u_dem=0.05),
+             dict(con_solve=1), [1, 8]),
+}
+
+
+def case_inputs(name):
+    gen, over, cps = CASES[name]
+    p, sph, dem = spouted_bed(**gen)
+    for k, v in over.items():
+        setattr(p, k, v)
+    p.freq_output = 1000000   # VTK only at step 0
+    return p, sph, dem, cps
+
+
+def worker(name, out):
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libsophia_ref.so")
+    L = C.CDLL(lib_path)
+    L.ref_load.argtypes = [C.c_char_p]
+    L.ref_run.argtypes = [C.c_int]
+    L.ref_get.argtypes = [C.c_int, C.c_char_p, C.POINTER(C.c_double)]
+    L.ref_counts.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.ref_last_ms.restype = C.c_double
+    p, sph, dem, cps = case_inputs(name)
+    work = tempfile.mkdtemp(prefix="golden_")
+    write_input_dir(os.path.join(work, "input"), p, sph, dem)
+    os.makedirs(os.path.join(work, "plotdata"), exist_ok=True)
+    rc = L.ref_load(work.encode())
+    if rc != 0:
+        raise SystemExit(f"ref_load failed: {rc}")
+    ns, nd = C.c_int(), C.c_int()
+    nijk = (C.c_int * 3)()
+    L.ref_counts(C.byref(ns), C.byref(nd), nijk)
+    blob = {"params": np.frombuffer(bytes(p), dtype=np.uint8), "nijk": np.array(list(nijk))}
+    for k, v in sph.items():
+        blob["in_sph_" + k] = np.asarray(v)
+    for k, v in dem.items():
+        blob["in_dem_" + k] = np.asarray(v)
+    done = 0
+    for cp in cps:
+        rc = L.ref_run(cp - done)
+        if rc != 0:
+            raise SystemExit(f"ref_run failed: {rc}")
+        done = cp
+        for which, fields, n in ((0, SPH_FIELDS, ns.value), (1, DEM_FIELDS, nd.value)):
+            for f in fields:
+                a = np.zeros(n)
+                if L.ref_get(which, f.encode(), a.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+                    raise SystemExit(f"ref_get {f}")
+                blob[f"s{cp}_{'sph' if which == 0 else 'dem'}_{f}"] = a
+            if which == 1:
+                for s in range(16):
+                    a = np.zeros(n)
+                    L.ref_get(1, f"ct_idx{s}".encode(), a.ctypes.data_as(C.POINTER(C.c_double)))
+                    blob[f"s{cp}_dem_ct_idx{s}"] = a
+                    for c in range(3):
+                        b = np.zeros(n)
+                        L.ref_get(1, f"del_s{s}_{c}".encode(), b.ctypes.data_as(C.POINTER(C.c_double)))
+                        blob[f"s{cp}_dem_del_s{s}_{c}"] = b
+    vtk = os.path.join(work, "plotdata")
+    vtks = sorted(os.listdir(vtk))
+    if vtks:
+        with open(os.path.join(vtk, vtks[0]), "rb") as fh:
+            blob["vtk_step0"] = np.frombuffer(fh.read(), dtype=np.uint8)
+    blob["checkpoints"] = np.array(cps)
+    blob["meta"] = np.frombuffer(json.dumps({"case": name, "ns": ns.value, "nd": nd.value}).encode(), dtype=np.uint8)
+    np.savez_compressed(out, **blob)
+    print(f"{name}: ns={ns.value} nd={nd.value} grid={list(nijk)} -> {out}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default=None)
+    ap.add_argument("--worker", nargs=2, metavar=("CASE", "OUT"))
+    ap.add_argument("--outdir", default=HERE)
+    a = ap.parse_args()
+    if a.worker:
+        worker(*a.worker)
+        return
+    names = [a.case] if a.case else list(CASES)
+    for n in names:
+        out = os.path.abspath(os.path.join(a.outdir, f"{n}.npz"))
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--worker", n, out], check=True)
+
+
+if __name__ == "__main__":
+    main()

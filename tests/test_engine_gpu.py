@@ -1,0 +1,218 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Bar (written into each assert):
+* integer and index work bit-exact: cell keys, sort order, neighbour
+  lists, particle types, contact-history partner ids;
+* FP64 build vs oracle: rel. L2 <= 1e-9 per field (rounding and FMA only);
+* FP32 build vs oracle: rel. L2 <= 1e-5 per field after 100 steps on a
+  bed without initial contacts, the tolerance of the specification for
+  the FP32 paths.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from fluidized_bed_master_b200.beds import spouted_bed, write_input_dir
+from fluidized_bed_master_b200.params import DEM, SPH
+from oracle import Oracle
+from tests.helpers import by_id, history_map, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SPH_REAL = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor", "dDEMpor", "flt_s",
+            "ftotalx", "ftotaly", "ftotalz", "fpx", "fpy", "fpz", "pgfx", "pgfy", "pgfz", "rho_ref"]
+DEM_REAL = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "DEMpor", "flt_s", "flt_sd", "flt_sd2",
+            "Fdx_df", "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz"]
+
+
+def _engine(p, sph, dem, prec):
+    from fluidized_bed_master_b200.engine import Engine
+
+    q = p.copy()
+    q.precision = prec
+    return Engine(q, sph, dem)
+
+
+def _ids(src, which):
+    return src.get(which, "pid") if which == SPH else src.get(which, "dem_idx")
+
+
+def _compare(eng, orc, fields_s, fields_d, tol, label):
+    bad = []
+    for which, fields in ((SPH, fields_s), (DEM, fields_d)):
+        n = eng.nd if which == DEM else eng.ns
+        if n == 0:
+            continue
+        ie, io = _ids(eng, which), _ids(orc, which)
+        for f in fields:
+            a = by_id(ie, eng.get(which, f))
+            b = by_id(io, orc.get(which, f))
+            e = rel_l2(a, b)
+            if not (e <= tol):
+                bad.append((label, "dem" if which else "sph", f, e))
+    return bad
+
+
+@pytest.fixture(scope="module")
+def contact_bed():
+    return spouted_bed(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=21, spacing=1.9, u_dem=0.05)
+
+
+@pytest.fixture(scope="module")
+def calm_bed():
+    return spouted_bed(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=22, spacing=2.1)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_cells_sort_and_neighbor_lists_bit_exact(contact_bed, prec):
+    p, sph, dem = contact_bed
+    eng = _engine(p, sph, dem, prec)
+    orc = Oracle(p, sph, dem, threads=8)
+    for k in range(3):
+        eng.step(1)
+        orc.step(1)
+        for which in (SPH, DEM):
+            assert np.array_equal(_ids(eng, which), _ids(orc, which)), "sorted order differs"
+            assert np.array_equal(eng.get(which, "cell"), orc.get(which, "cell")), "cell keys differ"
+        ce, le = eng.neighbors()
+        co, lo = orc.neighbors()
+        assert np.array_equal(ce, co), "neighbour counts differ"
+        assert ce.max() <= le.shape[1]
+        for i in range(eng.ns):
+            assert np.array_equal(le[i, : ce[i]], lo[i, : co[i]]), f"neighbour list of slot {i} differs"
+
+
+def test_fp64_matches_oracle_contact_bed(contact_bed):
+    """FP64 build vs oracle: rel. L2 <= 1e-9 per field after 1 and 8 steps."""
+    p, sph, dem = contact_bed
+    eng = _engine(p, sph, dem, 1)
+    orc = Oracle(p, sph, dem, threads=8)
+    bad = []
+    done = 0
+    for cp in (1, 8):
+        eng.step(cp - done)
+        orc.step(cp - done)
+        done = cp
+        bad += _compare(eng, orc, SPH_REAL, DEM_REAL, 1e-9, f"step{cp}")
+        for f in ("p_type", "i_type", "buffer_type"):
+            assert np.array_equal(by_id(_ids(eng, SPH), eng.get(SPH, f)), by_id(_ids(orc, SPH), orc.get(SPH, f)))
+        ie, se = eng.history()
+        io_, so = orc.history()
+        me = history_map(ie.astype(float), se)
+        mo = history_map(io_, so)
+        ide = _ids(eng, DEM)
+        ido = _ids(orc, DEM)
+        he = {int(ide[i]): me[i] for i in range(eng.nd)}
+        ho = {int(ido[i]): mo[i] for i in range(orc.nd)}
+        for k in ho:
+            assert set(he[k]) == set(ho[k]), f"contact partners of sphere {k} differ"
+            for j in ho[k]:
+                assert np.allclose(he[k][j], ho[k][j], rtol=1e-9, atol=1e-18)
+        assert sum(len(v) for v in ho.values()) > 0, "the bed has no contacts: the test would be vacuous"
+    assert not bad, bad
+
+
+def test_fp64_matches_oracle_heat(contact_bed):
+    p, sph, dem = contact_bed
+    q = p.copy()
+    q.con_solve = 1
+    eng = _engine(q, sph, dem, 1)
+    orc = Oracle(q, sph, dem, threads=8)
+    eng.step(5)
+    orc.step(5)
+    bad = _compare(eng, orc, SPH_REAL + ["dtemp"], DEM_REAL + ["dtemp"], 1e-9, "heat")
+    assert not bad, bad
+
+
+def test_fp32_within_1e5_after_100_steps(calm_bed):
+    """FP32 build vs the FP64 oracle: rel. L2 <= 1e-5 after 100 steps."""
+    p, sph, dem = calm_bed
+    eng = _engine(p, sph, dem, 0)
+    orc = Oracle(p, sph, dem, threads=8)
+    eng.step(100)
+    orc.step(100)
+    fs = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor"]
+    fd = ["x", "y", "z", "ux", "uy", "uz", "temp", "DEMpor"]
+    bad = _compare(eng, orc, fs, fd, 1e-5, "fp32-100")
+    assert not bad, bad
+
+
+def test_fp32_vs_fp64_engine_builds(calm_bed):
+    """Every field of the FP32 build against the FP64 build of the same kernels."""
+    p, sph, dem = calm_bed
+    e32 = _engine(p, sph, dem, 0)
+    e64 = _engine(p, sph, dem, 1)
+    e32.step(10)
+    e64.step(10)
+    report = {}
+    for which, fields in ((SPH, SPH_REAL), (DEM, DEM_REAL)):
+        for f in fields:
+            report[("dem" if which else "sph", f)] = rel_l2(by_id(_ids(e32, which), e32.get(which, f)),
+                                                           by_id(_ids(e64, which), e64.get(which, f)))
+    worst = max(report.values())
+    assert worst < 1e-3, sorted(report.items(), key=lambda kv: -kv[1])[:5]
+
+
+def test_stats_and_time(calm_bed):
+    p, sph, dem = calm_bed
+    eng = _engine(p, sph, dem, 0)
+    eng.step(3)
+    t, c = eng.time()
+    assert c == 3 and abs(t - 3 * p.dt) < 1e-15
+    s = eng.stats()
+    assert s["count"] == 3 and s["overflow_flags"] == 0 and s["nan_flag"] == 0
+    orc = Oracle(p, sph, dem, threads=8)
+    orc.step(3)
+    m = (orc.get(SPH, "p_type") != 0) & (orc.get(SPH, "i_type") < 2)
+    assert abs(s["rho_max_sph"] - orc.get(SPH, "rho")[m].max()) <= 1e-5 * orc.get(SPH, "rho")[m].max()
+    assert eng.launches() > 0
+
+
+def test_from_dir_equals_arrays(calm_bed):
+    from fluidized_bed_master_b200.engine import Engine
+
+    p, sph, dem = calm_bed
+    with tempfile.TemporaryDirectory() as d:
+        write_input_dir(d, p, sph, dem)
+        e1 = Engine.from_dir(d, precision=1)
+        e2 = _engine(p, sph, dem, 1)
+        e1.step(2)
+        e2.step(2)
+        for f in ("pres", "uz", "rho"):
+            assert rel_l2(by_id(_ids(e1, SPH), e1.get(SPH, f)), by_id(_ids(e2, SPH), e2.get(SPH, f))) < 1e-12
+
+
+def test_restart_roundtrip(calm_bed):
+    from fluidized_bed_master_b200.engine import Engine, read_input_txt
+
+    p, sph, dem = calm_bed
+    e = _engine(p, sph, dem, 1)
+    e.step(2)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "input.txt")
+        e.write_restart(path)
+        s2, d2 = read_input_txt(path)
+        assert len(s2["x"]) == e.ns and len(d2["x"]) == e.nd
+        assert np.allclose(s2["uz"], e.get(SPH, "uz"), rtol=0, atol=1e-12)
+        assert np.array_equal(d2["dem_idx"], e.get(DEM, "dem_idx"))
+
+
+def test_vtk_dem_layout(calm_bed):
+    p, sph, dem = calm_bed
+    e = _engine(p, sph, dem, 0)
+    e.step(1)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "dem.vtk")
+        e.write_vtk_dem(path)
+        raw = open(path, "rb").read()
+    assert raw.startswith(b"# vtk DataFile Version 3.0\nPrint out results in vtk format\nBINARY\nDATASET POLYDATA\n")
+    n = e.nd
+    head = f"POINTS\t{n}\tfloat\n".encode()
+    k = raw.index(head) + len(head)
+    xyz = np.frombuffer(raw[k:k + 12 * n], dtype=">f4").reshape(n, 3)
+    assert np.allclose(xyz[:, 2], e.get(DEM, "z").astype(np.float32))
+    for name in (b"itype", b"mag_uijf", b"Euler", b"porosity", b"uz", b"Q_sd", b"ftotal_z",
+                 b"temperature_surface", b"rad", b"dtemp_dt"):
+        assert name + f"\t1\t{n}\tfloat\n".encode() in raw
