@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""SPH-DEM particle-updates/s of one ISPH-DEM step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Workload: the 3-D SPH-DEM fluidized bed (0.1 x 0.02 x 0.4 m box,
+200,000 fluid SPH particles on a dx = 1.25 mm lattice plus inlet and wall
+particles, 20,000 DEM spheres of 2 mm, Wendland C2, h = 1.3 dx, heat
+transfer on), generated from a seed: synthetic data of the benchmark's
+shape.  A step is one call of the engine's step (the reference's
+SOPHIA_single_ISPH + time/count update).  value = (N_sph + N_dem) x K x
+ranks / max-over-ranks device time of the K timed steps; L2 is flushed
+(a 256 MB write) before every timed step and each step is timed with CUDA
+events on the engine's stream.
+
+--gpus N (torchrun, one process per GPU): every rank steps its own,
+independently seeded bed -- the reference's ISPH-DEM path runs on one GPU
+(ISPH_Calc_seperate.cuh:907), so ranks are replicas and scaling is weak.
+
+--impl reference: the reference arm, timed on the host CPU: the oracle
+port of the reference step (all host threads) on a bounded sample of the
+same bed (a quarter-height slice with the same lattice and sphere density).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(n_fluid=200_000, n_dem=20_000, dx=1.25e-3)
+SAMPLE = dict(n_fluid=50_000, n_dem=5_000, dx=1.25e-3, dem_height=0.025)
+SPH_STATE = ["ux", "uy", "uz", "m", "rho", "pres", "temp", "dDEMpor", "flt_s"]
+DEM_STATE = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "Fdx_df", "Fdy_df", "Fdz_df", "Q_sd"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl"
+        import torch
+
+        if not torch.cuda.is_available():
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch (field manifest of each kernel, SoA precision)
+# ---------------------------------------------------------------------------
+def manifest_bytes(kernel, ns, nd, nwall, nbuf, avg_nb, r):
+    """Bytes each pass must move: every particle's own fields once (read +
+    write), neighbour fields counted once per particle (perfect reuse), and
+    the neighbour list it streams (4 B per entry)."""
+    L = 4 * avg_nb + 4
+    pos = 32  # x, y, z, h (double)
+    per = {
+        "build_list": ns * (pos + L),
+        "passA": ns * (pos + 8 + L + 3 * r + 15 * r),
+        "passB": ns * (pos + 12 + L + 17 * r + 8 * r),
+        "ppe": ns * (pos + 12 + L + 18 * r + r),
+        "passC": ns * (pos + 12 + L + 19 * r + 6 * r),
+        "xsph": ns * (pos + 8 + L + 7 * r + 4 * r),
+        "neumann": nwall * (pos + 4 * r),
+        "open_bc": nbuf * (pos + 8 * r),
+        "sph_coupling": ns * (pos + 12 * r),
+        "dem_contact": nd * (5 * 8 + 12 * r + 16 * 28),
+        "dem_coupling": nd * (5 * 8 + 20 * r),
+        "dem_prep": nd * (5 * 8 + 6 * r),
+        "dem_update": nd * (3 * 8 + 20 * r),
+        "cells_gather_sph": ns * 2 * (pos + 9 * r + 16) + ns * 8,
+        "cells_gather_dem": nd * 2 * (5 * 8 + 17 * r + 20 + 16 * 28) + nd * 8,
+        "hash_sph": ns * (24 + 4 + 8),
+        "hash_dem": nd * (24 + 4 + 8),
+    }
+    return per.get(kernel)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle port of the reference step)
+# ---------------------------------------------------------------------------
+def cpu_reference(seconds=None, warmup=1, steps=None):
+    from fluidized_bed_master_b200.beds import box_bed
+    from oracle import Oracle
+
+    p, sph, dem = box_bed(**SAMPLE)
+    threads = os.cpu_count() or 1
+    orc = Oracle(p, sph, dem, threads=threads)
+    n = orc.ns + orc.nd
+    orc.step(warmup)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        orc.step(1)
+        k += 1
+        el = time.perf_counter() - t0
+        if steps is not None and k >= steps:
+            break
+        if steps is None and (el >= seconds or k >= 200):
+            break
+    el = time.perf_counter() - t0
+    sample = (f"box bed slice: {orc.ns} SPH + {orc.nd} DEM (n_fluid=50000, n_dem=5000, same dx and sphere "
+              f"density), {k} steps after {warmup} warm-up")
+    return n * k / el, threads, sample, el / k
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    val, cores, sample, s_per_step = cpu_reference(warmup=args.warmup, steps=args.steps)
+    unit = "particle-updates/s"
+    line = {
+        "metric": "SPH-DEM particle-updates/s on 1 B200 (3-D fluidized bed, ISPH-DEM step)",
+        "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded box bed slice)",
+        "config": {"workload": "3-D SPH-DEM fluidized bed 0.1x0.02x0.4 m, dx=1.25 mm, bounded CPU sample",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# engine arm
+# ---------------------------------------------------------------------------
+def run_engine(args, world, rank, local, pg):
+    import torch
+
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import DEM, SPH
+
+    torch.cuda.set_device(local)
+    p, sph, dem = box_bed(seed=rank, **WORKLOAD)
+    p.precision = 1 if args.precision == "fp64" else 0
+    eng = Engine(p, sph, dem)
+    n_part = eng.ns + eng.nd
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    eng.set_timing(True)
+    eng.step(2)          # capture both graph parities with timing events, outside the timed region
+    eng.collect_timing()
+    counts, _ = eng.neighbors(cap=1)
+    avg_nb = float(counts.mean()) if eng.ns else 0.0
+    base = eng.timing()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
+    sampler = ClockSampler(int(vis) if vis.isdigit() else local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms = 0.0
+    launches0 = 0
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        eng.step(1)
+        launches0 += eng.launches()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        eng.collect_timing()  # synchronises the engine stream
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    t_max = total_ms
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = n_part * args.steps * world / (t_max / 1e3)
+    ms_per_step = t_max / args.steps
+
+    # dominant kernel and its roofline
+    tim = eng.timing()
+    per_kernel = {k: (v[0] - base.get(k, (0, 0))[0], v[1] - base.get(k, (0, 0))[1]) for k, v in tim.items()}
+    dom = max(per_kernel.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom[0], dom[1]
+    r = 8 if args.precision == "fp64" else 4
+    nwall = int((sph["p_type"] <= 0).sum())
+    nbuf = int(((sph["p_type"] == 1) & ((sph["z"] < p.obc_L2 - 1e-6) | (sph["z"] >= p.obc_L3 - 1e-6))).sum())
+    bytes_dom = manifest_bytes(dom_name, eng.ns, eng.nd, nwall, nbuf, avg_nb, r)
+    peak, peak_kind = load_peaks()
+    achieved = bytes_dom / (dom_ms / max(dom_n, 1) / 1e3) / 1e9 if (bytes_dom and dom_n) else None
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            traffic = json.load(open(tr_path)).get(dom_name)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "bytes_per_launch": bytes_dom, "launch_ms": dom_ms / max(dom_n, 1), "peak_source": peak_kind,
+                "share_of_step": dom_ms / max(sum(v[0] for v in per_kernel.values()), 1e-12)}
+
+    # end to end through the C ABI with host buffers: each step uploads the
+    # mutable particle state from pinned host arrays, steps, reads it back
+    e2e = None
+    if not args.no_e2e:
+        def pinned(n, dt):
+            return torch.empty(n, dtype=dt, pin_memory=True).numpy()
+        hs = {f: pinned(eng.ns, torch.float64) for f in SPH_STATE}
+        hd = {f: pinned(eng.nd, torch.float64) for f in DEM_STATE}
+        for f in SPH_STATE:
+            hs[f][:] = eng.get(SPH, f)
+        for f in DEM_STATE:
+            hd[f][:] = eng.get(DEM, f)
+        hid, hsp = eng.history()
+        hb = sum(a.nbytes for a in hs.values()) + sum(a.nbytes for a in hd.values()) + hid.nbytes + hsp.nbytes
+        eng.set_timing(False)
+        ke = max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            for f in SPH_STATE:
+                eng.set(SPH, f, hs[f])
+            for f in DEM_STATE:
+                eng.set(DEM, f, hd[f])
+            eng.set_history(hid, hsp)
+            eng.step(1)
+            for f in SPH_STATE:
+                hs[f][:] = eng.get(SPH, f)
+            for f in DEM_STATE:
+                hd[f][:] = eng.get(DEM, f)
+            hid, hsp = eng.history()
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([te], dtype=torch.float64, device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": n_part * ke * world / te, "unit": "particle-updates/s", "h2d_bytes_per_step": hb,
+               "d2h_bytes_per_step": hb, "ms_per_step": te / ke * 1e3,
+               "how": "per step: sphdem_set_field/set_history of the mutable state from pinned host arrays, "
+                      "sphdem_step, sphdem_get_field/get_history back"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample, _ = cpu_reference(seconds=args.cpu_seconds)
+        cpu = {"value": v, "unit": "particle-updates/s", "cores": cores, "kind": "port", "sample": sample}
+
+    stats = eng.stats()
+    line = {
+        "metric": "SPH-DEM particle-updates/s on 1 B200 (3-D fluidized bed, ISPH-DEM step)",
+        "value": value, "unit": "particle-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if r == 4 else "f64",
+        "data": "synthetic (seeded box bed; reference input.txt not shipped)",
+        "config": {"workload": "3-D SPH-DEM fluidized bed 0.1x0.02x0.4 m: 200,000 fluid SPH on dx=1.25 mm "
+                               "(+inlet/wall particles) and 20,000 DEM spheres d=2 mm, Wendland C2, "
+                               "h=1.3dx, heat transfer, ISPH-DEM step (reference PPE sweep)",
+                   "n_sph": eng.ns, "n_dem": eng.nd, "avg_neighbours": avg_nb,
+                   "l2": "256 MB buffer written before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "positions": "f64", "fields": "f32" if r == 4 else "f64"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches0),
+        "clocks": clocks,
+        "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "u_max_dem", "overflow_flags", "nan_flag")},
+        "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_engine(args, world, rank, local, pg)
+    finally:
+        if pg:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

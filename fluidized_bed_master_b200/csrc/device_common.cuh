@@ -21,7 +21,8 @@ struct DevParams {
     int kernel_type, dim, kgc, delsph, fp, fv, fva, fg, con, xsph, open_bc, rho_type;
     int NI, NJ, NK, num_cells;
     int ns, nd, nb_cap;
-    int nwall, nbuf;          // static counts of wall (p_type<=0) and open-boundary buffer particles
+    int nwall, nbuf;
+    int filt_period;          // freq_filt * decouple_stride          // static counts of wall (p_type<=0) and open-boundary buffer particles
     int wall_mask;
     int sph_lagrangian;
     double kappa, dt, sdt, soundspeed, u_limit, c_xsph;

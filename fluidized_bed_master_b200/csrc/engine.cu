@@ -26,6 +26,42 @@ using namespace sphdem;
 
 static const int TPB = 128;
 
+// kernel slots for per-kernel timing
+enum {
+    KT_HASH_S, KT_SORT_S, KT_GATHER_S, KT_HASH_D, KT_SORT_D, KT_GATHER_D, KT_LIST, KT_PASSA, KT_DEMPREP, KT_PASSB,
+    KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
+    KT_OPENBC, KT_XSPH, KT_COUNT
+};
+static const char* KT_NAMES[KT_COUNT] = {
+    "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
+    "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
+    "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph"};
+
+// Event records inside a captured step graph must be external event
+// nodes (cudaEventRecordExternal); a plain record during capture only
+// marks a dependency point.
+static void record_event(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
+
+struct KTimer {
+    SphdemHandle* H;
+    int k;
+    KTimer(SphdemHandle* h, int kk) : H(h), k(kk) {
+        if (H->timing) {
+            record_event(H->ev_beg[k], H->stream);
+            H->ev_used[k] = 1;
+        }
+    }
+    ~KTimer() {
+        if (H->timing) record_event(H->ev_end[k], H->stream);
+    }
+};
+#define KTIME(k) KTimer kt_##__LINE__(H, k)
+
 // ---------------------------------------------------------------------------
 // allocation
 // ---------------------------------------------------------------------------
@@ -146,18 +182,27 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     int n = P.ns;
     if (n == 0) return SPHDEM_OK;
     SphState<R>& S = E.S[src];
-    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    {
+        KTIME(KT_HASH_S);
+        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    }
     size_t bytes = E.sort_tmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
-                                       key_bits(P.num_cells), st));
+    {
+        KTIME(KT_SORT_S);
+        CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
+                                           key_bits(P.num_cells), st));
+    }
     CK(cudaMemsetAsync(W.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
     CK(cudaMemsetAsync(W.counters, 0, sizeof(int) * 4, st));
     SphGatherSrc<R> g;
     if (P.xsph) { g.ux = W.u_tmpx; g.uy = W.u_tmpy; g.uz = W.u_tmpz; g.temp = W.temp_tmp; }
     else { g.ux = S.ux; g.uy = S.uy; g.uz = S.uz; g.temp = S.temp; }
     g.m = W.m_new; g.rho = W.rho_new; g.pres = W.p_new;
-    k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.key_out, W.val_out, W.g_str, W.g_end,
-                                                            W.wall_idx, W.buf_idx, W.counters);
+    {
+        KTIME(KT_GATHER_S);
+        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.key_out, W.val_out, W.g_str,
+                                                                W.g_end, W.wall_idx, W.buf_idx, W.counters);
+    }
     *nl += 3;
     CK(cudaGetLastError());
     return SPHDEM_OK;
@@ -173,11 +218,21 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
     if (n == 0) return SPHDEM_OK;
     DemState<R>& D = E.D[src];
-    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, DW.val_in);
+    {
+        KTIME(KT_HASH_D);
+        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, DW.val_in);
+    }
     size_t bytes = E.sort_tmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, DW.key_in, DW.key_out, DW.val_in, DW.val_out, n, 0,
-                                       key_bits(P.num_cells), st));
-    k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str, DW.g_end);
+    {
+        KTIME(KT_SORT_D);
+        CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, DW.key_in, DW.key_out, DW.val_in, DW.val_out, n, 0,
+                                           key_bits(P.num_cells), st));
+    }
+    {
+        KTIME(KT_GATHER_D);
+        k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str,
+                                                                DW.g_end);
+    }
     *nl += 3;
     CK(cudaGetLastError());
     return SPHDEM_OK;
@@ -206,48 +261,53 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
     if (ns > 0) {
-        k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.g_str, W.g_end, W.nbr, W.ncnt, E.flags);
-        k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.g_str, DW.g_end);
+        { KTIME(KT_LIST); k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.g_str, W.g_end, W.nbr, W.ncnt, E.flags); }
+        { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.g_str, DW.g_end); }
         *nl += 2;
     }
     if (nd > 0) {
-        k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, D, DW, W.g_str, W.g_end, DW.g_str, DW.g_end);
+        { KTIME(KT_DEMPREP); k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, D, DW, W.g_str, W.g_end, DW.g_str, DW.g_end); }
         *nl += 1;
     }
     if (ns > 0) {
-        k_passB<R><<<bs, TPB, 0, st>>>(P, S, W, (flags & F_FILT) ? 1 : 0);
+        { KTIME(KT_PASSB); k_passB<R><<<bs, TPB, 0, st>>>(P, S, W, E.flags); }
         *nl += 1;
     }
     if (nd > 0) {
-        k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.g_str, DW.g_end, E.flags);
-        k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.g_str, W.g_end);
+        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.g_str, DW.g_end, E.flags); }
+        { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.g_str, W.g_end); }
         *nl += 2;
     }
     if (ns > 0) {
-        k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.g_str, DW.g_end, (flags & F_TIME0) ? 1 : 0);
+        { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.g_str, DW.g_end, (flags & F_TIME0) ? 1 : 0); }
         if (flags & F_COUNT0) {
+            KTIME(KT_NEUMANN0);
             k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.g_str, W.g_end);
             *nl += 1;
         }
-        k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W);
-        k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.g_str, W.g_end);
-        k_passC<R><<<bs, TPB, 0, st>>>(P, S, W);
+        { KTIME(KT_PPE); k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W); }
+        { KTIME(KT_NEUMANN); k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.g_str, W.g_end); }
+        { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
         *nl += 4;
     }
     if (nd > 0) {
-        k_dem_update<R><<<bd, TPB, 0, st>>>(P, D, DW);
+        { KTIME(KT_DEMUPDATE); k_dem_update<R><<<bd, TPB, 0, st>>>(P, D, DW); }
         *nl += 1;
     }
     if (ns > 0) {
         if (P.open_bc > 0) {
+            KTIME(KT_OPENBC);
             k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.g_str, W.g_end);
             *nl += 1;
         }
         if (P.xsph) {
+            KTIME(KT_XSPH);
             k_xsph<R><<<bs, TPB, 0, st>>>(P, S, W);
             *nl += 1;
         }
     }
+    k_tick<<<1, 1, 0, st>>>(E.flags);
+    *nl += 1;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -257,7 +317,6 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
     Engine<R>& E = EH->E;
     int flags = 0;
     if (H->count == 0) flags |= F_COUNT0;
-    if (H->count % (H->p.freq_filt * H->p.decouple_stride) == 0) flags |= F_FILT;
     if (H->time == 0.0) flags |= F_TIME0;
     int key = flags | (E.cur_s << 8) | (E.cur_d << 9);
     int64_t n = 0;
@@ -265,6 +324,7 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
         auto it = H->graphs.find(key);
         if (it == H->graphs.end()) {
             cudaGraph_t g;
+            if (H->timing) std::fill(H->ev_used.begin(), H->ev_used.end(), 0);
             CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
             int r = enqueue_step<R>(H, EH, flags, &n);
             cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
@@ -275,9 +335,11 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
             cudaGraphDestroy(g);
             H->graphs[key] = ge;
             H->graph_launches[key] = n;
+            H->graph_kused[key] = H->ev_used;
             it = H->graphs.find(key);
         }
         n = H->graph_launches[key];
+        if (H->timing) H->ev_used = H->graph_kused[key];
         CK(cudaGraphLaunch(it->second, H->stream));
     } else {
         int r = enqueue_step<R>(H, EH, flags, &n);
@@ -344,6 +406,7 @@ static int commit_t(SphdemHandle* H) {
     P.xsph = p.xsph_solve; P.open_bc = p.open_boundary; P.rho_type = p.rho_type;
     P.NI = NI; P.NJ = NJ; P.NK = NK; P.num_cells = num_cells;
     P.ns = ns; P.nd = nd;
+    P.filt_period = p.freq_filt * p.decouple_stride;
     P.wall_mask = p.dem_wall_mask;
     P.sph_lagrangian = 0;   // KERNEL_set_alpha_sph: SPH particles are Eulerian (functions_ALE.cuh:26-47)
     P.kappa = p.kappa; P.dt = p.dt; P.sdt = p.decouple_stride * p.dt; P.soundspeed = p.soundspeed;
@@ -484,6 +547,12 @@ static int commit_t(SphdemHandle* H) {
         if (!A.ok) return SPHDEM_E_NOMEM;
         CK(cudaMemsetAsync(E.flags, 0, sizeof(DevFlags), st));
         CK(cudaStreamSynchronize(st));
+    }
+    {
+        DevFlags f0;
+        std::memset(&f0, 0, sizeof(f0));
+        f0.step_count = H->count;
+        CK(cudaMemcpy(E.flags, &f0, sizeof(f0), cudaMemcpyHostToDevice));
     }
     H->committed = true;
     return SPHDEM_OK;
@@ -722,8 +791,35 @@ extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, S
     return SPHDEM_OK;
 }
 
+template <typename R>
+static int set_state_t(SphdemHandle* H, int which, int field, const void* src, int n) {
+    static const int allowed[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_UX, SPHDEM_F_UY, SPHDEM_F_UZ,
+                                  SPHDEM_F_WX, SPHDEM_F_WY, SPHDEM_F_WZ, SPHDEM_F_M, SPHDEM_F_RHO, SPHDEM_F_PRES,
+                                  SPHDEM_F_TEMP, SPHDEM_F_DDEMPOR, SPHDEM_F_FLT_S, SPHDEM_F_FDX_DF, SPHDEM_F_FDY_DF,
+                                  SPHDEM_F_FDZ_DF, SPHDEM_F_Q_SD, SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3};
+    bool ok = false;
+    for (int f : allowed) ok |= (f == field);
+    if (!ok) return SPHDEM_E_ARG;
+    const void* ptr;
+    int kind;
+    if (field_ptr<R>(H, which, field, &ptr, &kind)) return SPHDEM_E_ARG;
+    if (n == 0) return SPHDEM_OK;
+    CK(cudaStreamSynchronize(H->stream));
+    if (kind == 0) {
+        CK(cudaMemcpy((void*)ptr, src, sizeof(double) * n, cudaMemcpyHostToDevice));
+        return SPHDEM_OK;
+    }
+    return upload_real<R>((R*)ptr, (const double*)src, n, H->stream);
+}
+
 extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const void* src, size_t bytes) {
-    if (!h || !src || (which != 0 && which != 1) || h->committed) return SPHDEM_E_ARG;
+    if (!h || !src || (which != 0 && which != 1)) return SPHDEM_E_ARG;
+    if (h->committed) {
+        int n = which ? h->nd : h->ns;
+        if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
+        return h->prec == SPHDEM_PREC_FP64 ? set_state_t<double>(h, which, field, src, n)
+                                           : set_state_t<float>(h, which, field, src, n);
+    }
     int n = which ? h->nd : h->ns;
     if (is_real_field(field)) {
         if (bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
@@ -858,6 +954,82 @@ extern "C" int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs
     return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, ids, springs) : history_t<float>(h, ids, springs);
 }
 
+template <typename R>
+static int set_history_t(SphdemHandle* H, const int32_t* ids, const double* sp) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    DemState<R>& D = EH->E.D[EH->E.cur_d];
+    int n = H->nd;
+    if (n == 0) return SPHDEM_OK;
+    std::vector<int> hid((size_t)n * SPHDEM_NSLOT);
+    std::vector<double> hds((size_t)n * SPHDEM_NSLOT * 3);
+    for (int i = 0; i < n; i++)
+        for (int s = 0; s < SPHDEM_NSLOT; s++) {
+            hid[(size_t)s * n + i] = ids[(size_t)i * SPHDEM_NSLOT + s];
+            for (int c = 0; c < 3; c++) hds[(size_t)(s * 3 + c) * n + i] = sp[((size_t)i * SPHDEM_NSLOT + s) * 3 + c];
+        }
+    CK(cudaStreamSynchronize(H->stream));
+    CK(cudaMemcpy(D.hid, hid.data(), sizeof(int) * hid.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(D.hds, hds.data(), sizeof(double) * hds.size(), cudaMemcpyHostToDevice));
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* springs) {
+    if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64 ? set_history_t<double>(h, ids, springs) : set_history_t<float>(h, ids, springs);
+}
+
+extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
+    if (!h) return SPHDEM_E_ARG;
+    if (h->ev_beg.empty()) {
+        h->ev_beg.resize(KT_COUNT);
+        h->ev_end.resize(KT_COUNT);
+        for (int k = 0; k < KT_COUNT; k++) {
+            CK(cudaEventCreate(&h->ev_beg[k]));
+            CK(cudaEventCreate(&h->ev_end[k]));
+        }
+        h->ev_used.assign(KT_COUNT, 0);
+        h->kern_ms.assign(KT_COUNT, 0.0);
+        h->kern_n.assign(KT_COUNT, 0);
+    }
+    if ((on != 0) != (h->timing != 0)) {
+        // captured graphs embed (or omit) the event records: recapture
+        CK(cudaStreamSynchronize(h->stream));
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+        h->graphs.clear();
+        h->graph_launches.clear();
+        h->graph_kused.clear();
+    }
+    h->timing = on ? 1 : 0;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_collect_timing(SphdemHandle* h) {
+    if (!h || h->ev_beg.empty()) return SPHDEM_E_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < KT_COUNT; k++) {
+        if (!h->ev_used[k]) continue;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->ev_beg[k], h->ev_end[k]) == cudaSuccess) {
+            h->kern_ms[k] += ms;
+            h->kern_n[k] += 1;
+        }
+        h->ev_used[k] = 0;
+    }
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_timing(SphdemHandle* h, int k, char* name, int name_cap, double* total_ms, int64_t* launches) {
+    if (!h || k < 0) return SPHDEM_E_ARG;
+    if (k >= KT_COUNT) return SPHDEM_E_ARG;
+    if (name && name_cap > 0) {
+        std::strncpy(name, KT_NAMES[k], name_cap - 1);
+        name[name_cap - 1] = 0;
+    }
+    if (total_ms) *total_ms = h->kern_ms.empty() ? 0.0 : h->kern_ms[k];
+    if (launches) *launches = h->kern_n.empty() ? 0 : h->kern_n[k];
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_write_vtk_dem(SphdemHandle* h, const char* path) {
     if (!h || !path || !h->committed) return SPHDEM_E_ARG;
     int n = h->nd;
@@ -966,6 +1138,8 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    for (cudaEvent_t e : h->ev_beg) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->ev_end) cudaEventDestroy(e);
     if (h->eng) {
         if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
     }

@@ -65,6 +65,7 @@ struct DevFlags {
     int overflow;   // bit0 SPH neighbour list, bit1 DEM contact history
     int nan;
     int max_ncnt;
+    int step_count; // the reference's count (vii[43]), advanced by k_tick at the end of a step
 };
 
 template <typename R>

@@ -29,8 +29,15 @@ struct SphdemHandle {
     void* eng = nullptr;     // sphdem::Engine<float|double>*
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int64_t> graph_launches;
+    std::map<int, std::vector<int>> graph_kused;
     int use_graphs = 1;
     int64_t last_launches = 0;
+    // per-kernel timing (events recorded inside the step graph)
+    int timing = 0;
+    std::vector<cudaEvent_t> ev_beg, ev_end;
+    std::vector<int> ev_used;
+    std::vector<double> kern_ms;
+    std::vector<int64_t> kern_n;
     int ppe_iters = 0;
     double ppe_res = 0.0;
     double ppe_ms = 0.0;

@@ -371,10 +371,12 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, De
 // ISPH step reads it.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, int filt) {
+__global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    // Shepard filter every freq_filt*decouple_stride steps (functions_PREP2.cuh:2120)
+    const int filt = (F->step_count % P.filt_period) == 0;
     int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
     W.ftx[i] = 0; W.fty[i] = 0; W.ftz[i] = 0; W.ftot[i] = 0;
     W.pgfx[i] = 0; W.pgfy[i] = 0; W.pgfz[i] = 0;
@@ -1274,6 +1276,9 @@ __global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWor
     W.u_tmpz[i] = (uzi + tz / flt) * on;
     W.temp_tmp[i] = (ti + tt / flt) * on;
 }
+
+// end of a step: the host loop's count++ (ISPH_Calc_seperate.cuh:925)
+__global__ void k_tick(DevFlags* F) { F->step_count += 1; }
 
 // ---------------------------------------------------------------------------
 // printed maxima (kernel_copy_max_*, functions_OUTPUT.cuh:19-65 + cub max)

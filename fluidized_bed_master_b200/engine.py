@@ -46,6 +46,10 @@ def lib():
     L.sphdem_get_neighbors.argtypes = [vp, P(C.c_int32), P(C.c_int32), C.c_int32]
     L.sphdem_get_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
+    L.sphdem_set_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
+    L.sphdem_set_timing.argtypes = [vp, C.c_int]
+    L.sphdem_collect_timing.argtypes = [vp]
+    L.sphdem_get_timing.argtypes = [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_double), P(C.c_int64)]
     L.sphdem_input_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
     L.sphdem_input_column.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, C.c_size_t]
     L.sphdem_write_restart.argtypes = [vp, C.c_char_p]
@@ -154,6 +158,35 @@ class Engine:
         _chk(lib().sphdem_get_history(self._h, ids.ctypes.data_as(C.POINTER(C.c_int32)),
                                       sp.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_get_history")
         return ids, sp
+
+    def set(self, which, name, arr):
+        """Upload a state field after commit, in the current slot order."""
+        self._set(which, name, arr)
+
+    def set_history(self, ids, springs):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        sp = np.ascontiguousarray(springs, dtype=np.float64)
+        _chk(lib().sphdem_set_history(self._h, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      sp.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_set_history")
+
+    def set_timing(self, on):
+        _chk(lib().sphdem_set_timing(self._h, int(bool(on))), "sphdem_set_timing")
+
+    def collect_timing(self):
+        _chk(lib().sphdem_collect_timing(self._h), "sphdem_collect_timing")
+
+    def timing(self):
+        """{kernel name: (total ms, launches)} accumulated by collect_timing."""
+        out = {}
+        k = 0
+        name = C.create_string_buffer(64)
+        while True:
+            ms, n = C.c_double(), C.c_int64()
+            if lib().sphdem_get_timing(self._h, k, name, 64, C.byref(ms), C.byref(n)) != 0:
+                break
+            out[name.value.decode()] = (ms.value, n.value)
+            k += 1
+        return out
 
     def time(self):
         t, c = C.c_double(), C.c_int32()

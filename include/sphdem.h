@@ -236,7 +236,11 @@ int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
                            SphdemHandle** out);
 
 /* Upload one field for the SPH (which=0) or DEM (which=1) set from host
- * memory, in input order.  bytes = n * 8 (real fields) or n * 4 (int). */
+ * memory.  Before sphdem_commit_particles: input order, any field.  After
+ * it: the engine's current slot order (the order sphdem_get_field
+ * returns), state fields only (positions, velocities, m, rho, pres, temp,
+ * dDEMpor, flt_s, Fd*_df, Q_sd, temp1-3).  bytes = n * 8 (real fields) or
+ * n * 4 (int). */
 int sphdem_set_field(SphdemHandle* h, int which, int field,
                      const void* host_src, size_t bytes);
 
@@ -269,6 +273,19 @@ int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* dst,
  * ids[n*16] and spring vectors as springs[n*16*3], particle-major, in the
  * current sorted order. */
 int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs);
+
+/* Upload a contact history in the layout of sphdem_get_history. */
+int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* springs);
+
+/* Per-kernel device timing.  While enabled, every step records a CUDA
+ * event pair around each engine kernel on the handle's stream (inside the
+ * captured step graph); sphdem_collect_timing synchronises and adds the
+ * elapsed times of the last step to per-kernel totals, which
+ * sphdem_get_timing reports (kernel k = 0..n-1, name, total ms, count). */
+int sphdem_set_timing(SphdemHandle* h, int on);
+int sphdem_collect_timing(SphdemHandle* h);
+int sphdem_get_timing(SphdemHandle* h, int k, char* name, int name_cap,
+                      double* total_ms, int64_t* launches);
 
 /* Binary legacy-VTK POLYDATA of the DEM set, the format of
  * save_plot_fluid_vtk_bin_solid_dem (functions_OUTPUT.cuh:1135-1446). */

@@ -216,3 +216,20 @@ def test_vtk_dem_layout(calm_bed):
     for name in (b"itype", b"mag_uijf", b"Euler", b"porosity", b"uz", b"Q_sd", b"ftotal_z",
                  b"temperature_surface", b"rad", b"dtemp_dt"):
         assert name + f"\t1\t{n}\tfloat\n".encode() in raw
+
+
+def test_kernel_timing_mode(calm_bed):
+    """In-graph event timing: every engine kernel of the step reports a time."""
+    p, sph, dem = calm_bed
+    e = _engine(p, sph, dem, 0)
+    e.step(1)
+    e.set_timing(True)
+    for _ in range(3):
+        e.step(1)
+        e.collect_timing()
+    t = e.timing()
+    for k in ("build_list", "passA", "passB", "ppe", "passC", "dem_contact", "dem_coupling", "xsph"):
+        ms, n = t[k]
+        assert n == 3 and ms > 0, (k, ms, n)
+    e.set_timing(False)
+    e.step(2)
