@@ -311,6 +311,31 @@ int sphdem_get_launch_count(SphdemHandle* h, int64_t* launches);
 /* sizeof(SphdemParams) as compiled into the library (binding check). */
 int sphdem_params_size(void);
 
+/* Allocation-free cell sort.  No counterpart in the reference: an extra
+ * entry point for callers that cannot allocate device memory once their
+ * time loop runs (a host code capturing its step into a CUDA graph, where
+ * cudaMalloc is not allowed during capture, or an application that hands
+ * out all device memory from its own pool).  It does the engine's NNPS
+ * step on caller-owned device arrays: cell key of every particle
+ * (functions_NNPS.cuh:762-821), stable sort by cell, cell start/end
+ * (functions_NNPS.cuh:670-730).  Inputs: x, y, z (n doubles, device), the
+ * grid bbox[6] = xmin,xmax,ymin,ymax,zmin,zmax and nijk[3] = NI,NJ,NK on the
+ * host.  Outputs (device, caller-allocated): perm[n] (input index of each
+ * sorted slot), cell_key[n] (sorted cell keys), cell_start/cell_end
+ * [NI*NJ*NK] (-1 start for an empty cell).  Work is enqueued on stream.
+ * Its scratch is a file-scope __device__ array of
+ * SPHDEM_STATIC_SCRATCH_BYTES that every GPU loading the library keeps
+ * until exit; n above SPHDEM_STATIC_MAX_PARTICLES returns SPHDEM_E_NOMEM.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race. */
+#define SPHDEM_STATIC_MAX_PARTICLES (1 << 18)
+#define SPHDEM_STATIC_SCRATCH_BYTES (8u << 20)
+int sphdem_sort_cells_static(const double* x, const double* y, const double* z, int32_t n,
+                             const double* bbox, const int32_t* nijk, int32_t* perm,
+                             int32_t* cell_key, int32_t* cell_start, int32_t* cell_end,
+                             void* stream);
+
 void sphdem_destroy(SphdemHandle* h);
 
 /* Human-readable text of a status code. */
