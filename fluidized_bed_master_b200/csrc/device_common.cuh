@@ -22,7 +22,7 @@ struct DevParams {
     int NI, NJ, NK, num_cells;
     int ns, nd, nb_cap;
     int nwall, nbuf;
-    int filt_period;          // freq_filt * decouple_stride          // static counts of wall (p_type<=0) and open-boundary buffer particles
+    int filt_period;          // freq_filt * decouple_stride
     int wall_mask;
     int sph_lagrangian;
     double kappa, dt, sdt, soundspeed, u_limit, c_xsph;
@@ -35,6 +35,11 @@ struct DevParams {
     double box_c[3], box_L[3];
     double cone_c[3], cone_r1, cone_r2, cone_h;
     double rest_n, rest_s, mu_s, mu_rs;
+    // fixed-point positions of the FP32 build (records.cuh): origin, 1/step
+    // and step per axis; q_abs = 8 x the largest step, which sets the width
+    // of the band a prefilter leaves to the exact FP64 test.
+    double q_org[3], q_inv[3], q_abs;
+    float q_step[3];
 };
 
 // ---- cell index ---------------------------------------------------------
@@ -218,32 +223,83 @@ __device__ __forceinline__ PairT<double> pair_test<double>(double xi, double yi,
 __device__ __forceinline__ float r2_lo(double Rr) { return (float)(Rr * Rr * (1.0 - 1e-6)); }
 __device__ __forceinline__ float r2_hi(double Rr) { return (float)(Rr * Rr * (1.0 + 1e-6)); }
 
-// ---- stencil as 9 contiguous slot ranges --------------------------------
+// ---- stencil rows from a per-cell row table ------------------------------
 // The three cells (ix-1..ix+1, jy, kz) have consecutive keys, so their
-// particles form one contiguous range of the cell-sorted arrays.  Visiting
-// the 9 (z,y) rows in order with ascending slots inside each row is the
-// reference's 27-cell visit order.
+// particles are one contiguous slot range of the cell-sorted arrays, and
+// visiting the 9 (z,y) rows in order with ascending slots inside each row
+// is the reference's 27-cell (z,y,x) visit order.  rows[c] = {first, end}
+// of that range around cell c (clamped to the grid), built once per step
+// after the cell sort; {0, 0} when the row is empty.  A 27-cell scan is
+// then 9 table loads.
+__device__ __forceinline__ int2 row_range(const int* __restrict__ gs, const int* __restrict__ ge, int NI, int base,
+                                          int ic) {
+    int x0 = ic > 0 ? ic - 1 : 0, x1 = ic < NI - 1 ? ic + 1 : NI - 1;
+    int lo = -1, hi = 0;
+    for (int ix = x0; ix <= x1; ix++) {
+        int s = gs[base + ix];
+        if (s == -1) continue;
+        if (lo < 0) lo = s;
+        hi = ge[base + ix];
+    }
+    return lo < 0 ? make_int2(0, 0) : make_int2(lo, hi);
+}
+
 template <typename F>
-__device__ __forceinline__ void for_stencil_rows(const DevParams& P, int ic, int jc, int kc, const int* __restrict__ gs,
-                                                 const int* __restrict__ ge, F f) {
-    int x0 = ic > 0 ? ic - 1 : 0, x1 = ic < P.NI - 1 ? ic + 1 : P.NI - 1;
+__device__ __forceinline__ void for_rows(const DevParams& P, int ic, int jc, int kc, const int2* __restrict__ rows,
+                                         F f) {
     for (int z = -1; z <= 1; z++) {
         int kz = kc + z;
         if (kz < 0 || kz > P.NK - 1) continue;
         for (int y = -1; y <= 1; y++) {
             int jy = jc + y;
             if (jy < 0 || jy > P.NJ - 1) continue;
-            int base = P.NI * jy + P.NI * P.NJ * kz;
-            int lo = -1, hi = -1;
-            for (int ix = x0; ix <= x1; ix++) {
-                int s = gs[base + ix];
-                if (s == -1) continue;
-                if (lo < 0) lo = s;
-                hi = ge[base + ix];
-            }
-            if (lo >= 0) f(lo, hi);
+            int2 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
+            if (r.x < r.y) f(r.x, r.y);
         }
     }
+}
+
+// One warp scanning the 27-cell stencil of one particle: the 9 row ranges
+// are concatenated and lane l takes candidates l, l+32, ... of the
+// concatenation, so no lane idles at the end of each row.  sm is 20 ints
+// of shared memory owned by the warp (row offsets and starts).  The order
+// in which a lane visits its candidates is ascending slot order.
+template <typename F>
+__device__ __forceinline__ void for_rows_warp(const DevParams& P, int ic, int jc, int kc, const int2* __restrict__ rows,
+                                              int* sm, int lane, F f) {
+    int len = 0, lo = 0;
+    if (lane < 9) {
+        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
+        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
+            int2 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
+            lo = r.x;
+            len = r.y - r.x;
+        }
+    }
+    // inclusive prefix over lanes 0..8
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < 9) {
+        sm[lane + 1] = inc;
+        sm[10 + lane] = lo;
+    }
+    if (lane == 0) sm[0] = 0;
+    int tot = __shfl_sync(0xffffffffu, inc, 8);
+    __syncwarp();
+    int r = 0, nxt = sm[1], base = sm[10];
+    for (int t = lane; t < tot; t += 32) {
+        while (t >= nxt) {
+            r++;
+            nxt = sm[r + 1];
+            base = sm[10 + r] - sm[r];
+        }
+        f(base + t);
+    }
+    __syncwarp();
 }
 
 __device__ __forceinline__ float warp_sum(float v) {

@@ -30,12 +30,12 @@ static const int TPB = 128;
 enum {
     KT_HASH_S, KT_SORT_S, KT_GATHER_S, KT_HASH_D, KT_SORT_D, KT_GATHER_D, KT_LIST, KT_PASSA, KT_DEMPREP, KT_PASSB,
     KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
-    KT_OPENBC, KT_XSPH, KT_COUNT
+    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_COUNT
 };
 static const char* KT_NAMES[KT_COUNT] = {
     "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
-    "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph"};
+    "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem"};
 
 // Event records inside a captured step graph must be external event
 // nodes (cudaEventRecordExternal); a plain record during capture only
@@ -129,9 +129,15 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     W.u_tmpx = A.get<R>(ns); W.u_tmpy = A.get<R>(ns); W.u_tmpz = A.get<R>(ns); W.temp_tmp = A.get<R>(ns);
     W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
     W.g_str = A.get<int>(ncells + 1); W.g_end = A.get<int>(ncells + 1);
+    W.rows = A.get<int2>(ncells);
     W.ncnt = A.get<int>(ns);
     W.wall_idx = A.get<int>(ns); W.buf_idx = A.get<int>(ns); W.counters = A.get<int>(4);
     W.nbr = nullptr;
+    W.rec.pos = A.get<PosRec<R>>(ns);
+    W.rec.mr0 = A.get<V2<R>>(ns);
+    W.rec.f1 = A.get<V4<R>>(ns);
+    W.rec.up = A.get<V4<R>>(ns);
+    W.rec.ut = A.get<V4<R>>(ns);
     DW.flt_s = A.get<R>(nd); DW.flt_sd = A.get<R>(nd); DW.flt_sd2 = A.get<R>(nd); DW.DEMpor = A.get<R>(nd);
     DW.ftx = A.get<R>(nd); DW.fty = A.get<R>(nd); DW.ftz = A.get<R>(nd);
     DW.tqx = A.get<R>(nd); DW.tqy = A.get<R>(nd); DW.tqz = A.get<R>(nd);
@@ -142,6 +148,7 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     DW.magf = A.get<R>(nd);
     DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = A.get<int>(nd); DW.val_out = A.get<int>(nd);
     DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
+    DW.rows = A.get<int2>(ncells);
 }
 
 int key_bits(int num_cells) {
@@ -200,10 +207,14 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     g.m = W.m_new; g.rho = W.rho_new; g.pres = W.p_new;
     {
         KTIME(KT_GATHER_S);
-        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.key_out, W.val_out, W.g_str,
+        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.rec, W.key_out, W.val_out, W.g_str,
                                                                 W.g_end, W.wall_idx, W.buf_idx, W.counters);
     }
-    *nl += 3;
+    {
+        KTIME(KT_ROWS_S);
+        k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, W.g_str, W.g_end, W.rows);
+    }
+    *nl += 4;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -216,7 +227,10 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     cudaStream_t st = H->stream;
     int n = P.nd;
     CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
-    if (n == 0) return SPHDEM_OK;
+    if (n == 0) {
+        CK(cudaMemsetAsync(DW.rows, 0, sizeof(int2) * P.NI * P.NJ * P.NK, st));
+        return SPHDEM_OK;
+    }
     DemState<R>& D = E.D[src];
     {
         KTIME(KT_HASH_D);
@@ -233,7 +247,11 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
         k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str,
                                                                 DW.g_end);
     }
-    *nl += 3;
+    {
+        KTIME(KT_ROWS_D);
+        k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, DW.g_str, DW.g_end, DW.rows);
+    }
+    *nl += 4;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -261,12 +279,12 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
     if (ns > 0) {
-        { KTIME(KT_LIST); k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.g_str, W.g_end, W.nbr, W.ncnt, E.flags); }
-        { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.g_str, DW.g_end); }
+        { KTIME(KT_LIST); k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags); }
+        { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
         *nl += 2;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMPREP); k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, D, DW, W.g_str, W.g_end, DW.g_str, DW.g_end); }
+        { KTIME(KT_DEMPREP); k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
         *nl += 1;
     }
     if (ns > 0) {
@@ -274,19 +292,19 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 1;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.g_str, DW.g_end, E.flags); }
-        { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.g_str, W.g_end); }
+        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
+        { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows); }
         *nl += 2;
     }
     if (ns > 0) {
-        { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.g_str, DW.g_end, (flags & F_TIME0) ? 1 : 0); }
+        { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0); }
         if (flags & F_COUNT0) {
             KTIME(KT_NEUMANN0);
-            k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.g_str, W.g_end);
+            k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.rows, 1);
             *nl += 1;
         }
         { KTIME(KT_PPE); k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W); }
-        { KTIME(KT_NEUMANN); k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.g_str, W.g_end); }
+        { KTIME(KT_NEUMANN); k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0); }
         { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
         *nl += 4;
     }
@@ -297,7 +315,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if (ns > 0) {
         if (P.open_bc > 0) {
             KTIME(KT_OPENBC);
-            k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.g_str, W.g_end);
+            k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.rows);
             *nl += 1;
         }
         if (P.xsph) {
@@ -423,6 +441,22 @@ static int commit_t(SphdemHandle* H) {
     for (int k = 0; k < 3; k++) { P.box_c[k] = p.box_c[k]; P.box_L[k] = p.box_L[k]; P.cone_c[k] = p.cone_c[k]; }
     P.cone_r1 = p.cone_r1; P.cone_r2 = p.cone_r2; P.cone_h = p.cone_h;
     P.rest_n = p.wall_rest_n; P.rest_s = p.wall_rest_s; P.mu_s = p.wall_mu_s; P.mu_rs = p.wall_mu_rs;
+    // fixed-point position grid of the FP32 records: origin at the box
+    // centre, 2^30 steps per box extent (records.cuh)
+    {
+        const double lo[3] = {mnx, mny, mnz}, hi[3] = {mxx, mxy, mxz};
+        double smax = 0;
+        for (int k = 0; k < 3; k++) {
+            double e = hi[k] - lo[k];
+            if (!(e > 0)) e = 1.0;
+            double step = e / 1073741824.0;
+            P.q_org[k] = 0.5 * (lo[k] + hi[k]);
+            P.q_inv[k] = 1.0 / step;
+            P.q_step[k] = (float)step;
+            smax = std::max(smax, step);
+        }
+        P.q_abs = 8.0 * smax;
+    }
 
     Alloc& A = EH->A;
     alloc_sph_state<R>(A, E.S[0], ns); alloc_sph_state<R>(A, E.S[1], ns);
@@ -464,6 +498,9 @@ static int commit_t(SphdemHandle* H) {
         auto& pt = H->stage_i[0][SPHDEM_F_PTYPE];
         auto& bt = H->stage_i[0][SPHDEM_F_BUFFER_TYPE];
         int nw = 0, nb = 0;
+        // the position records carry p_type in 16 bits
+        for (int i = 0; i < ns; i++)
+            if (pt[i] < -32768 || pt[i] > 32767) return SPHDEM_E_UNSUPPORTED;
         for (int i = 0; i < ns; i++) {
             if (pt[i] <= 0) nw++;
             if (bt[i] > 0 && pt[i] < 1000) nb++;
@@ -535,7 +572,7 @@ static int commit_t(SphdemHandle* H) {
         int64_t nl = 0;
         P.nb_cap = 0;
         if ((r = nnps_sph<R>(H, EH, 0, 1, &nl))) return r;
-        k_build_list<R><<<nblocks(ns, TPB), TPB, 0, st>>>(P, E.S[1], W.g_str, W.g_end, nullptr, W.ncnt, E.flags);
+        k_build_list<R><<<nblocks(ns, TPB), TPB, 0, st>>>(P, E.S[1], W.rec, W.rows, nullptr, W.ncnt, E.flags);
         CK(cudaGetLastError());
         DevFlags f;
         CK(cudaMemcpyAsync(&f, E.flags, sizeof(f), cudaMemcpyDeviceToHost, st));
@@ -680,14 +717,16 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
     DemState<R>& D = E.D[E.cur_d];
     double hb[8] = {0};
     if (P.ns > 0) {
-        k_stats<R><<<1, 256, 0, st>>>(P.ns, W.rho_new, P.xsph ? W.u_tmpx : S.ux, P.xsph ? W.u_tmpy : S.uy,
+        CK(cudaMemsetAsync(E.red_buf, 0, sizeof(double) * 3, st));
+        k_stats<R><<<std::min(nblocks(P.ns, 256), 592), 256, 0, st>>>(P.ns, W.rho_new, P.xsph ? W.u_tmpx : S.ux, P.xsph ? W.u_tmpy : S.uy,
                                       P.xsph ? W.u_tmpz : S.uz, W.ftot, S.ptype, S.itype, E.red_buf, E.flags);
         CK(cudaMemcpyAsync(hb, E.red_buf, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         out->rho_max_sph = hb[0]; out->u_max_sph = hb[1]; out->ftotal_max_sph = hb[2];
     }
     if (P.nd > 0) {
-        k_stats<R><<<1, 256, 0, st>>>(P.nd, D.rho, D.ux, D.uy, D.uz, (const R*)nullptr, D.ptype, D.itype, E.red_buf,
+        CK(cudaMemsetAsync(E.red_buf, 0, sizeof(double) * 3, st));
+        k_stats<R><<<std::min(nblocks(P.nd, 256), 592), 256, 0, st>>>(P.nd, D.rho, D.ux, D.uy, D.uz, (const R*)nullptr, D.ptype, D.itype, E.red_buf,
                                       E.flags);
         CK(cudaMemcpyAsync(hb, E.red_buf, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

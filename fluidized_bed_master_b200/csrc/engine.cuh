@@ -5,12 +5,15 @@
 //   every other field: R (float in the FP32 build, double in the FP64 one)
 //   DEM contact history: SPHDEM_NSLOT slot-major planes, partner id int32
 //     and tangential spring double[3]  (slot s of particle i at s*n+i)
+//   packed records of what the neighbour passes read of a neighbour
+//     (records.cuh): position + tag, {m,rho}, {m',rho',T,eps}, {u,p}, {u,T}
 // Persistent fields live in two copies (A/B) that the per-step reorder
 // gathers between; work arrays are single copies overwritten each step.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "device_common.cuh"
+#include "records.cuh"
 
 namespace sphdem {
 
@@ -31,6 +34,16 @@ struct DemState {
     double* hds;   // NSLOT*3*n
 };
 
+// packed neighbour records (records.cuh), indexed by the current slot
+template <typename R>
+struct SphRec {
+    PosRec<R>* pos;
+    V2<R>* mr0;
+    V4<R>* f1;
+    V4<R>* up;
+    V4<R>* ut;
+};
+
 template <typename R>
 struct SphWork {
     R *m_new, *rho_new, *rho_ref, *DEMpor, *dDEMpor_prev;
@@ -44,8 +57,10 @@ struct SphWork {
     R *u_tmpx, *u_tmpy, *u_tmpz, *temp_tmp;
     int *key_in, *key_out, *val_in, *val_out;
     int *g_str, *g_end;
+    int2* rows;                  // per-cell stencil rows (for_rows)
     int *nbr, *ncnt;
     int *wall_idx, *buf_idx, *counters;   // per-step compacted wall / buffer slots
+    SphRec<R> rec;
 };
 
 template <typename R>
@@ -58,6 +73,7 @@ struct DemWork {
     R *magf;                     // |u_f - u_a| of the drag closure (VTK mag_uijf)
     int *key_in, *key_out, *val_in, *val_out;
     int *g_str, *g_end;
+    int2* rows;
 };
 
 // device-side status words (checked by the host at sync points)

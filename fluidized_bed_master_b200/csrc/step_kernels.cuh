@@ -53,27 +53,14 @@ __device__ __forceinline__ void kgc3(const R* __restrict__ Cm, int n, int i, int
 }
 
 // 27-cell stencil in the reference order (z,y,x), calling f(j) for every
-// slot j of every non-empty cell.
+// slot j of every non-empty cell: the 9 rows in order, ascending slots
+// inside a row.
 template <typename F>
-__device__ __forceinline__ void for_stencil(const DevParams& P, int ic, int jc, int kc, const int* __restrict__ gs,
-                                            const int* __restrict__ ge, F f) {
-    for (int z = -1; z <= 1; z++) {
-        int kz = kc + z;
-        if (kz < 0 || kz > P.NK - 1) continue;
-        for (int y = -1; y <= 1; y++) {
-            int jy = jc + y;
-            if (jy < 0 || jy > P.NJ - 1) continue;
-            for (int x = -1; x <= 1; x++) {
-                int ix = ic + x;
-                if (ix < 0 || ix > P.NI - 1) continue;
-                int c = ix + P.NI * jy + P.NI * P.NJ * kz;
-                int s = gs[c];
-                if (s == -1) continue;
-                int e = ge[c];
-                for (int j = s; j < e; j++) f(j);
-            }
-        }
-    }
+__device__ __forceinline__ void for_stencil_j(const DevParams& P, int ic, int jc, int kc,
+                                              const int2* __restrict__ rows, F f) {
+    for_rows(P, ic, jc, kc, rows, [&](int a, int b) {
+        for (int j = a; j < b; j++) f(j);
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -105,6 +92,15 @@ __device__ __forceinline__ void cell_bounds(const DevParams& P, int i, int n, co
     if (i == n - 1 && k < P.num_cells) ge[k] = n;
 }
 
+// per-cell stencil row table (for_rows), one thread per cell
+__global__ void k_rows(DevParams P, const int* __restrict__ gs, const int* __restrict__ ge, int2* rows) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int nc = P.NI * P.NJ * P.NK;
+    if (c >= nc) return;
+    int ic = c % P.NI, base = c - ic;
+    rows[c] = row_range(gs, ge, P.NI, base, ic);
+}
+
 // reorder of every persistent SPH field, source of m/rho/pres/u/temp is
 // the array that held the end-of-step value
 template <typename R>
@@ -114,31 +110,36 @@ struct SphGatherSrc {
 
 template <typename R>
 __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R> gsrc, SphState<R> dst,
-                                   const int* __restrict__ key, const int* __restrict__ perm, int* gs, int* ge,
-                                   int* wall_idx, int* buf_idx, int* counters) {
+                                   SphRec<R> rec, const int* __restrict__ key, const int* __restrict__ perm, int* gs,
+                                   int* ge, int* wall_idx, int* buf_idx, int* counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
     cell_bounds(P, i, n, key, gs, ge);
     int p = perm[i];
-    dst.x[i] = src.x[p];
-    dst.y[i] = src.y[p];
-    dst.z[i] = src.z[p];
+    double x = src.x[p], y = src.y[p], z = src.z[p];
+    dst.x[i] = x;
+    dst.y[i] = y;
+    dst.z[i] = z;
     dst.h[i] = src.h[p];
-    dst.ux[i] = gsrc.ux[p];
-    dst.uy[i] = gsrc.uy[p];
-    dst.uz[i] = gsrc.uz[p];
-    dst.m[i] = gsrc.m[p];
-    dst.rho[i] = gsrc.rho[p];
-    dst.pres[i] = gsrc.pres[p];
+    R ux = gsrc.ux[p], uy = gsrc.uy[p], uz = gsrc.uz[p], m = gsrc.m[p], rho = gsrc.rho[p], pr = gsrc.pres[p];
+    dst.ux[i] = ux;
+    dst.uy[i] = uy;
+    dst.uz[i] = uz;
+    dst.m[i] = m;
+    dst.rho[i] = rho;
+    dst.pres[i] = pr;
     dst.temp[i] = gsrc.temp[p];
     dst.dDEMpor[i] = src.dDEMpor[p];
     dst.flt_s[i] = src.flt_s[p];
-    int pt = src.ptype[p], bt = src.btype[p];
+    int pt = src.ptype[p], bt = src.btype[p], it = src.itype[p];
     dst.ptype[i] = pt;
     dst.btype[i] = bt;
-    dst.itype[i] = src.itype[p];
+    dst.itype[i] = it;
     dst.pid[i] = src.pid[p];
+    store_pos(rec.pos, i, make_pos<R>(P, x, y, z, pt, bt, it));
+    rec.mr0[i] = mk2<R>(m, rho);
+    rec.up[i] = mk4<R>(ux, uy, uz, pr);
     if (pt <= 0) wall_idx[atomicAdd(&counters[0], 1)] = i;
     if (bt > 0 && pt < 1000) buf_idx[atomicAdd(&counters[1], 1)] = i;
 }
@@ -173,24 +174,30 @@ __global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst
 // SPH neighbour list: the candidate set and predicate of every SPH gather
 // kernel (e.g. functions_PPE2.cuh:609-638): 27-cell stencil and
 // sqrt(dx^2+dy^2+dz^2) + 1e-20 < kappa*h_i, decided exactly in FP64 (see
-// pair_test).  Rows come out in ascending slot order, which is the
-// reference's z,y,x cell visit order.  Column-major rows.
+// test_pair).  Rows come out in ascending slot order, which is the
+// reference's z,y,x cell visit order.  Column-major rows.  Threads of a
+// warp are consecutive slots, mostly of one cell, so they walk the same
+// candidate rows and their position-record loads coalesce.
 template <typename R>
-__global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, const int* __restrict__ gs,
-                                                    const int* __restrict__ ge, int* __restrict__ nbr,
-                                                    int* __restrict__ ncnt, DevFlags* F) {
+__global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, SphRec<R> rec,
+                                                    const int2* __restrict__ rows,
+                                                    int* __restrict__ nbr, int* __restrict__ ncnt, DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.ns) return;
     double xi = S.x[i], yi = S.y[i], zi = S.z[i];
     double Rr = __dmul_rn(P.kappa, S.h[i]);
-    float lo = r2_lo(Rr), hi = r2_hi(Rr);
+    Band bd = make_band(P, Rr);
+    PosRec<R> qi = ldr(rec.pos + i);
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     int c = 0, cap = P.nb_cap, n = P.ns;
-    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
+    for_rows(P, ic, jc, kc, rows, [&](int a, int b) {
         for (int j = a; j < b; j++) {
-            if (pair_test<float>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 1e-20, lo, hi).in) {
-                if (c < cap) nbr[(size_t)c * n + i] = j;
+            PosRec<R> qj = ldr(rec.pos + j);
+            Disp<R> d;
+            R r2;
+            if (test_pair(P, qi, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) {
+                if (nbr && c < cap) nbr[(size_t)c * n + i] = j;
                 c++;
             }
         }
@@ -210,45 +217,57 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                               const int* __restrict__ dgs, const int* __restrict__ dge) {
+                                               const int2* __restrict__ drows) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    const SphRec<R> rec = W.rec;
     int it = S.itype[i], pt = S.ptype[i];
     R mo = S.m[i], ro = S.rho[i];
     if (it > 2) {
         W.m_new[i] = mo;
         W.rho_new[i] = ro;
+        rec.f1[i] = mk4<R>(mo, ro, S.temp[i], W.DEMpor[i]);
         return;
     }
     R dprev = S.dDEMpor[i];
     W.dDEMpor_prev[i] = dprev;
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
     R th = (R)hi;
-    R tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    Knl<R> K = knl_make<R>(P, th);
+    PosRec<R> qi = ldr(rec.pos + i);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R txx = 0, tyy = 0, tzz = 0, txy = 0, tyz = 0, tzx = 0, sflt = 0;
     const int* __restrict__ nb = W.nbr;
-    for (int k = 0; k < cnt; k++) {
-        int j = nb[(size_t)k * n + i];
-        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
-        R mj = S.m[j], rj = S.rho[j];
-        int ptj = S.ptype[j];
-        R r = g.r + (R)1e-20;
-        R w = knl_w<R>(P.kernel_type, tA, th, r);
-        if (ptj <= 1000) sflt += mj / rj * w * (R)(ptj == 1);
-        if (P.kgc == 1 && g.r2 > (R)0 && ptj <= 1000) {
-            R dw = knl_dw<R>(P.kernel_type, tA, th, g.r);
-            R mtd = mj * dw, rtd = (R)1 / (rj * g.r), t;
-            t = -mtd * g.dx * g.dx; t *= rtd; txx += t;
-            t = -mtd * g.dy * g.dx; t *= rtd; txy += t;
-            t = -mtd * g.dy * g.dy; t *= rtd; tyy += t;
-            t = -mtd * g.dx * g.dz; t *= rtd; tzx += t;
-            t = -mtd * g.dy * g.dz; t *= rtd; tyz += t;
-            t = -mtd * g.dz * g.dz; t *= rtd; tzz += t;
-        }
-    }
-    if (P.kgc == 1) {
+    const bool kgc = P.kgc == 1;
+    nb_walk<4, NbQ2<R>>(
+        cnt, nb, n, i,
+        [&](int j) {
+            NbQ2<R> t;
+            t.q = ldr(rec.pos + j);
+            t.a = ldr(rec.mr0 + j);
+            return t;
+        },
+        [&](int j, const NbQ2<R>& t) {
+            int ptj = tag_ptype(t.q.w);
+            if (ptj > 1000) return;
+            Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+            R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+            rdist(r2, r, rinv);
+            R irj = rcp(t.a.y);
+            if (ptj == 1) sflt += t.a.x * irj * kw(K, r);
+            if (kgc && r2 > (R)0) {
+                R dw = kdw(K, r);
+                R c = -t.a.x * dw * irj * rinv;
+                txx += c * g.dx * g.dx;
+                txy += c * g.dy * g.dx;
+                tyy += c * g.dy * g.dy;
+                tzx += c * g.dx * g.dz;
+                tyz += c * g.dy * g.dz;
+                tzz += c * g.dz * g.dz;
+            }
+        });
+    if (kgc) {
         R det = txx * (tyy * tzz - tyz * tyz);
         det -= txy * (txy * tzz - tyz * tzx);
         det += tzx * (txy * tyz - tyy * tzx);
@@ -270,31 +289,32 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
 #pragma unroll
         for (int q = 0; q < 9; q++) W.Cm[(size_t)q * n + i] = C[q];
     }
-    // SPH-DEM porosity
+    // SPH-DEM porosity (DEM arrays are small and L2-resident: plain loads)
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     double Rr = P.kappa * hi;
     R por = 0, dfx = 0, dfy = 0, dfz = 0;
     if (P.nd > 0) {
-        for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
-            double d = pair_dist(xi, yi, zi, D.x[j], D.y[j], D.z[j]) + 1e-20;
-            if (d < Rr && D.ptype[j] > 1000) {
-                Pair<R> g = make_pair<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j]);
-                R r = (R)d;
-                R w = knl_w<R>(P.kernel_type, tA, th, r);
-                R dw = knl_dw<R>(P.kernel_type, tA, th, r);
-                R rj = (R)D.rad[j];
-                R v = (R)4.18879 * rj * rj * rj;
-                por += w * v;
-                dfx += dw * g.dx / r * (R)D.ux[j] * v;
-                dfy += dw * g.dy / r * (R)D.uy[j] * v;
-                dfz += dw * g.dz / r * (R)D.uz[j] * v;
-            }
+        float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+        for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
+            if (D.ptype[j] <= 1000) return;
+            PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
+            if (!g.in) return;
+            R r = g.r + (R)1e-20, ir = rcp(r);
+            R w = kw(K, r);
+            R dw = kdw(K, r);
+            R rj = (R)D.rad[j];
+            R v = (R)4.18879 * rj * rj * rj;
+            por += w * v;
+            dfx += dw * g.dx * ir * (R)D.ux[j] * v;
+            dfy += dw * g.dy * ir * (R)D.uy[j] * v;
+            dfz += dw * g.dz * ir * (R)D.uz[j] * v;
         });
     }
-    R pori = (R)1 - (por / (sflt + (R)1e-20));
+    R isf = rcp(sflt + (R)1e-20);
+    R pori = (R)1 - por * isf;
     W.DEMpor[i] = pori;
-    S.dDEMpor[i] = (dfx + dfy + dfz) / (sflt + (R)1e-20);
+    S.dDEMpor[i] = (dfx + dfy + dfz) * isf;
     // prep_sph
     R hd = (R)P.h_over_dx;
     R v = (th / hd) * (th / hd) * (th / hd);
@@ -305,53 +325,58 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
     if (pt == 9 && zi < 0.05) mref = (R)P.rho_gas * v * pori;
     R rref = (P.dim == 2) ? mref / ((th / hd) * (th / hd)) : mref / v;
     W.rho_ref[i] = rref;
+    R mn = mo, rn = ro;
     if (P.rho_type == 1) {
-        W.rho_new[i] = mref / v;
-        W.m_new[i] = mref;
-    } else {
-        W.rho_new[i] = ro;
-        W.m_new[i] = mo;
+        rn = mref / v;
+        mn = mref;
     }
+    W.rho_new[i] = rn;
+    W.m_new[i] = mn;
+    rec.f1[i] = mk4<R>(mn, rn, S.temp[i], pori);
 }
 
 // KERNEL_clc_prep3D_coupling_dem: functions_PREP2.cuh:3367-3523.
 // One warp per DEM sphere; lanes stride over the candidate rows.
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, DemState<R> D, DemWork<R> DW,
-                                                  const int* __restrict__ sgs, const int* __restrict__ sge,
-                                                  const int* __restrict__ dgs, const int* __restrict__ dge) {
+__global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<R> D,
+                                                  DemWork<R> DW, const int2* __restrict__ srows, const int2* __restrict__ drows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
+    int* sm = s_rows[threadIdx.x >> 5];
     if (i >= P.nd) return;
     if (D.itype[i] > 2) return;
     int pti = D.ptype[i];
     double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
-    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R th = (R)hi;
+    Knl<R> K = knl_make<R>(P, th);
     double Rr = P.kappa * hi;
+    Band bd = make_band(P, Rr);
     float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+    PosRec<R> qp = make_pos<R>(P, xi, yi, zi, 0, 0, 0);
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R f1 = 0, f3 = 0, por = 0;
-    for_stencil_rows(P, ic, jc, kc, sgs, sge, [&](int a, int b) {
-        for (int j = a + lane; j < b; j += 32) {
-            int ptj = S.ptype[j];
-            if (ptj != 1 && ptj != 3) continue;
-            PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
-            if (!g.in) continue;
-            R w = knl_w<R>(P.kernel_type, tA, th, g.r);
-            R c = S.m[j] / S.rho[j] * w;
-            if (ptj == 1) f1 += c;
-            else f3 += c;
-        }
+    for_rows_warp(P, ic, jc, kc, srows, sm, lane, [&](int j) {
+        PosRec<R> qj = ldr(rec.pos + j);
+        int ptj = tag_ptype(qj.w);
+        if (ptj != 1 && ptj != 3) return;
+        Disp<R> d;
+        R r2;
+        if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) return;
+        R r, rinv;
+        rdist(r2, r, rinv);
+        V2<R> mr = ldr(rec.mr0 + j);
+        R c = mr.x * rcp(mr.y) * kw(K, r);
+        if (ptj == 1) f1 += c;
+        else f3 += c;
     });
-    for_stencil_rows(P, ic, jc, kc, dgs, dge, [&](int a, int b) {
-        for (int j = a + lane; j < b; j += 32) {
-            if (D.ptype[j] <= 1000) continue;
-            PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
-            if (!g.in) continue;
-            R w = knl_w<R>(P.kernel_type, tA, th, g.r);
-            R rj = (R)D.rad[j];
-            por += w * (R)4.18879 * rj * rj * rj;
-        }
+    for_rows_warp(P, ic, jc, kc, drows, sm, lane, [&](int j) {
+        if (D.ptype[j] <= 1000) return;
+        PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
+        if (!g.in) return;
+        R w = kw(K, g.r);
+        R rj = (R)D.rad[j];
+        por += w * (R)4.18879 * rj * rj * rj;
     });
     f1 = warp_sum(f1);
     f3 = warp_sum(f3);
@@ -375,6 +400,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    const SphRec<R> rec = W.rec;
     // Shepard filter every freq_filt*decouple_stride steps (functions_PREP2.cuh:2120)
     const int filt = (F->step_count % P.filt_period) == 0;
     int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
@@ -384,70 +410,81 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     if (it > 2 || pt > 1000) return;
     bool adv = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
     if (!filt && !adv) return;
-    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
-    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
-    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i];
-    R tempi = S.temp[i], pi = S.pres[i], rhoi = W.rho_new[i];
-    R pori = W.DEMpor[i];
+    R th = (R)S.h[i];
+    Knl<R> K = knl_make<R>(P, th);
+    PosRec<R> qi = ldr(rec.pos + i);
+    V4<R> upi = rec.up[i];
+    V4<R> fi = rec.f1[i];
+    R uxi = upi.x, uyi = upi.y, uzi = upi.z, pi = upi.w;
+    R rhoi = fi.y, tempi = fi.z, pori = fi.w, mi = fi.x;
+    R irhoi = rcp(rhoi);
+    const bool kgc = P.kgc == 1;
+    Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
     R vis = (R)P.mu_gas, vis_h = (vis * vis) / (vis + vis);
-    R kc = (R)P.k_sph, kc_h = (kc * kc) / (kc + kc);
+    R kc = (R)P.k_sph;
     R eli = P.sph_lagrangian ? (R)1 : (R)0;
+    // per-particle factors of the pair terms
+    R cp_i = -pori * irhoi * (rhoi / pori);      // rho_i/eps_i * (-eps_i / rho_i)
+    R cv_i = vis_h * (R)4 * pori * irhoi;
+    R ch_i = (R)4 * pori * kc * kc * irhoi / (kc + kc);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R flt = 0, tx = 0, ty = 0, tz = 0, px = 0, py = 0, pz = 0, Rc = 0, ex = 0, ey = 0, ez = 0, et = 0;
     const int* __restrict__ nb = W.nbr;
-    for (int k = 0; k < cnt; k++) {
-        int j = nb[(size_t)k * n + i];
-        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
-        R r = g.r + (R)1e-20;
-        R mj = W.m_new[j], rhoj = W.rho_new[j];
-        if (filt) flt += mj / rhoj * knl_w<R>(P.kernel_type, tA, th, r);
-        if (!adv || S.ptype[j] >= 1000) continue;
-        R dw = knl_dw<R>(P.kernel_type, tA, th, r);
-        R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
-        kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
-        R uxj = S.ux[j], uyj = S.uy[j], uzj = S.uz[j], pj = S.pres[j], tj = S.temp[j];
-        if (P.fp) {
-            R Cp = -pori * (mj) * (pi + pj) / (rhoi * rhoj);
-            R s = rhoi / pori * Cp;
-            px += s * gx;
-            py += s * gy;
-            pz += s * gz;
-        }
-        if (P.fv) {
-            R Cv = g.dx * gx + g.dy * gy + g.dz * gz;
-            Cv *= vis_h;
-            Cv *= (R)4 * pori * (mj / (rhoi * rhoj));
-            Cv /= r;
-            Cv /= r;
-            tx += Cv * (uxi - uxj);
-            ty += Cv * (uyi - uyj);
-            tz += Cv * (uzi - uzj);
-        }
-        if (P.fva) {
-            R uij = (uxi - uxj) * g.dx + (uyi - uyj) * g.dy + (uzi - uzj) * g.dz;
-            if (uij < (R)0) {
-                R hij = (th + th) * (R)0.5;
-                R phi = hij * uij / (r * r + (R)0.01 * hij * hij);
-                R Pij = W.m_new[i] * phi * ((R)-0.1 * (R)P.soundspeed + (R)0.02 * phi) / (rhoi + rhoj) * (R)0.5;
-                tx += -Pij * gx;
-                ty += -Pij * gy;
-                tz += -Pij * gz;
+    nb_walk<2, NbQ44<R>>(
+        cnt, nb, n, i,
+        [&](int j) {
+            NbQ44<R> t;
+            t.q = ldr(rec.pos + j);
+            t.a = ldr(rec.f1 + j);
+            t.b = ldr(rec.up + j);
+            return t;
+        },
+        [&](int j, const NbQ44<R>& t) {
+            const V4<R>& fj = t.a;
+            const V4<R>& uj = t.b;
+            Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+            R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+            rdist(r2, r, rinv);
+            R mj = fj.x, irj = rcp(fj.y);
+            if (filt) flt += mj * irj * kw(K, r);
+            if (!adv || tag_ptype(t.q.w) >= 1000) return;
+            R dw = kdw(K, r);
+            R gx = dw * g.dx * rinv, gy = dw * g.dy * rinv, gz = dw * g.dz * rinv;
+            cm_apply(Cm, kgc, gx, gy, gz);
+            R tj = fj.z;
+            if (P.fp) {
+                R s = cp_i * mj * (pi + uj.w) * irj;
+                px += s * gx;
+                py += s * gy;
+                pz += s * gz;
             }
-        }
-        if (eli < (R)1) {
-            R mr = mj / rhoj * ((R)1 - eli);
-            ex += (uxi * (uxj - uxi) * gx + uyi * (uxj - uxi) * gy + uzi * (uxj - uxi) * gz) * mr;
-            ey += (uxi * (uyj - uyi) * gx + uyi * (uyj - uyi) * gy + uzi * (uyj - uyi) * gz) * mr;
-            ez += (uxi * (uzj - uzi) * gx + uyi * (uzj - uzi) * gy + uzi * (uzj - uzi) * gz) * mr;
-            if (P.con) et += (uxi * (tj - tempi) * gx + uyi * (tj - tempi) * gy + uzi * (tj - tempi) * gz) * mr;
-        }
-        if (P.con) {
-            R h = (R)4 * pori * mj * kc * kc * (tempi - tj) * dw;
-            h /= (r + (R)1e-10) * rhoi * rhoj * (kc + kc);
-            Rc += h;
-        }
-        (void)kc_h;
-    }
+            if (P.fv) {
+                R Cv = (g.dx * gx + g.dy * gy + g.dz * gz) * cv_i * mj * irj * rinv * rinv;
+                tx += Cv * (uxi - uj.x);
+                ty += Cv * (uyi - uj.y);
+                tz += Cv * (uzi - uj.z);
+            }
+            if (P.fva) {
+                R uij = (uxi - uj.x) * g.dx + (uyi - uj.y) * g.dy + (uzi - uj.z) * g.dz;
+                if (uij < (R)0) {
+                    R hij = (th + th) * (R)0.5;
+                    R phi = hij * uij / (r * r + (R)0.01 * hij * hij);
+                    R Pij = mi * phi * ((R)-0.1 * (R)P.soundspeed + (R)0.02 * phi) / (rhoi + fj.y) * (R)0.5;
+                    tx += -Pij * gx;
+                    ty += -Pij * gy;
+                    tz += -Pij * gz;
+                }
+            }
+            if (eli < (R)1) {
+                R mr = mj * irj * ((R)1 - eli);
+                R ug = uxi * gx + uyi * gy + uzi * gz;
+                ex += (uj.x - uxi) * ug * mr;
+                ey += (uj.y - uyi) * ug * mr;
+                ez += (uj.z - uzi) * ug * mr;
+                if (P.con) et += (tj - tempi) * ug * mr;
+            }
+            if (P.con) Rc += ch_i * mj * (tempi - tj) * dw * irj * rcp(r + (R)1e-10);
+        });
     if (filt) S.flt_s[i] = flt;
     if (!adv) return;
     if (P.fg) tz += -(R)P.g_sph;
@@ -470,7 +507,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D, DemWork<R> DW,
-                                                     const int* __restrict__ dgs, const int* __restrict__ dge,
+                                                     const int2* __restrict__ drows,
                                                      DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.nd;
@@ -501,7 +538,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     R tx = 0, ty = 0, tz = 0, tqx = 0, tqy = 0, tqz = 0, dtr = 0, dtc = 0;
     const double kdt = P.dt;
     bool ovf = false;
-    for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
+    for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
         if (D.ptype[j] <= 1000) return;
         double xj = D.x[j], yj = D.y[j], zj = D.z[j], radj = D.rad[j];
         double td = pair_dist(xi, yi, zi, xj, yj, zj);
@@ -664,55 +701,63 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int* __restrict__ sgs,
-                                                      const int* __restrict__ sge) {
+                                                      DemWork<R> DW, const int2* __restrict__ srows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
+    int* sm = s_rows[threadIdx.x >> 5];
     if (i >= P.nd) return;
     int it = D.itype[i], pt = D.ptype[i];
     if (it > 2) return;
     R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i];
     R ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
     if (it == 1 && pt > 1000) {
+        const SphRec<R> rec = W.rec;
         double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
         R radi = (R)D.rad[i], di = (R)2 * radi, voli = ((R)4 / (R)3) * (R)3.14159 * radi * radi * radi;
         R mi = D.m[i], rhoi = D.rho[i], tempi = D.temp[i];
         R fa = DW.flt_s[i], ff = DW.flt_sd[i];
-        R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+        R th = (R)hi;
+        Knl<R> K = knl_make<R>(P, th);
         double Rr = P.kappa * hi;
-        float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+        Band bd = make_band(P, Rr);
+        PosRec<R> qp = make_pos<R>(P, xi, yi, zi, 0, 0, 0);
         int ic, jc, kc;
         cell_ijk(P, xi, yi, zi, ic, jc, kc);
         R tx = 0, ty = 0, tz = 0, ufx = 0, ufy = 0, ufz = 0, uax = 0, uay = 0, uaz = 0, por = 0, ttf = 0, tta = 0;
         int has_f = 0, has_a = 0;
         R pgc = voli / (mi * ff + (R)1.0e-15);
-        for_stencil_rows(P, ic, jc, kc, sgs, sge, [&](int a, int b) {
-            for (int j = a + lane; j < b; j += 32) {
-                int ptj = S.ptype[j];
-                if (ptj > 1000) continue;
-                R porj = W.DEMpor[j];
-                if (!(porj < (R)1)) continue;
-                PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], Rr, 0.0, r2l, r2h);
-                if (!g.in) continue;
-                R w = knl_w<R>(P.kernel_type, tA, th, g.r);
-                R mj = W.m_new[j], rhoj = W.rho_new[j], c = mj * w / rhoj;
-                if (ptj == 1 && ff > (R)0.000001) {
+        for_rows_warp(P, ic, jc, kc, srows, sm, lane, [&](int j) {
+            PosRec<R> qj = ldr(rec.pos + j);
+            int ptj = tag_ptype(qj.w);
+            if (ptj > 1000) return;
+            V4<R> fj = ldr(rec.f1 + j);
+            R porj = fj.w;
+            if (!(porj < (R)1)) return;
+            Disp<R> d;
+            R r2;
+            if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 0.0, bd, d, r2)) return;
+            R r, rinv;
+            rdist(r2, r, rinv);
+            R w = kw(K, r);
+            R mj = fj.x, rhoj = fj.y, c = mj * w * rcp(rhoj);
+            if ((ptj == 1 && ff > (R)0.000001) || (ptj == 3 && fa > (R)0.000001)) {
+                V4<R> uj = ldr(rec.up + j);
+                if (ptj == 1) {
                     has_f = 1;
-                    ufx += S.ux[j] * c; ufy += S.uy[j] * c; ufz += S.uz[j] * c;
-                    por += porj * c;
-                    ttf += S.temp[j] * c;
-                }
-                if (ptj == 3 && fa > (R)0.000001) {
+                    ufx += uj.x * c; ufy += uj.y * c; ufz += uj.z * c;
+                    ttf += fj.z * c;
+                } else {
                     has_a = 1;
-                    uax += S.ux[j] * c; uay += S.uy[j] * c; uaz += S.uz[j] * c;
-                    por += porj * c;
-                    tta += S.temp[j] * c;
+                    uax += uj.x * c; uay += uj.y * c; uaz += uj.z * c;
+                    tta += fj.z * c;
                 }
-                if (ptj != 0 && ptj != 9 && ptj != -3 && ptj != 3 && ff > (R)0.01) {
-                    R q = (mj / rhoj) * w * pgc;
-                    tx += W.pgfx[j] * q;
-                    ty += W.pgfy[j] * q;
-                    tz += W.pgfz[j] * q;
-                }
+                por += porj * c;
+            }
+            if (ptj != 0 && ptj != 9 && ptj != -3 && ptj != 3 && ff > (R)0.01) {
+                R q = c * pgc;
+                tx += W.pgfx[j] * q;
+                ty += W.pgfy[j] * q;
+                tz += W.pgfz[j] * q;
             }
         });
         tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
@@ -813,8 +858,7 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int* __restrict__ dgs,
-                                                      const int* __restrict__ dge, int time_zero) {
+                                                      DemWork<R> DW, const int2* __restrict__ drows, int time_zero) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -827,19 +871,21 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
         // heat_capacity(ptypei, tempi): the reference passes the arguments
         // swapped (functions_SPH_DEM_COUPLING2.cuh:1860)
         R cpi = (abs((int)tempi) > 1000) ? (R)P.cp_dem : (R)P.cp_sph;
-        R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+        R th = (R)hi;
+        Knl<R> K = knl_make<R>(P, th);
         double Rr = P.kappa * hi;
         R tx = 0, ty = 0, tz = 0, tt = 0;
         if (P.nd > 0 && (pt == 1 || pt == 3)) {
             int ic, jc, kc;
             cell_ijk(P, xi, yi, zi, ic, jc, kc);
-            for_stencil(P, ic, jc, kc, dgs, dge, [&](int j) {
+            float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+            for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
                 if (D.ptype[j] <= 1000) return;
-                double d = pair_dist(xi, yi, zi, D.x[j], D.y[j], D.z[j]);
-                if (!(d < Rr)) return;
+                PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 0.0, r2l, r2h);
+                if (!g.in) return;
                 R ffj = DW.flt_sd2[j] + DW.flt_s[j];
                 if (!(ffj > (R)0)) return;
-                R w = knl_w<R>(P.kernel_type, tA, th, (R)d);
+                R w = kw(K, g.r);
                 R c = w / (ffj + (R)1.0e-20);
                 R mr = D.m[j] / rhoi;
                 tx += -mr * D.Fdx_df[j] * c;
@@ -857,19 +903,23 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
         W.ftot[i] = sqrt(ftx * ftx + fty * fty + ftz * ftz);
         if (P.con) W.dtemp[i] += tt;
     }
-    // predictor (SPH), KERNEL_clc_projection_sph
+    // predictor (SPH), KERNEL_clc_projection_sph; u* also goes to the
+    // {u, p} record the PPE reads
     R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i];
     W.ux0[i] = uxi; W.uy0[i] = uyi; W.uz0[i] = uzi;
+    R usx = uxi, usy = uyi, usz = uzi;
     if (pt == 9) {
-        S.ux[i] = (R)P.ball_vel; S.uy[i] = (R)0; S.uz[i] = (R)0;
+        usx = (R)P.ball_vel; usy = (R)0; usz = (R)0;
         W.ux0[i] = (R)P.ball_vel; W.uy0[i] = (R)0; W.uz0[i] = (R)0;
     } else if (pt >= 0) {
         R b = (R)(S.btype[i] == 0);
         R dt = (R)P.sdt;
-        S.ux[i] = uxi + ftx * b * dt;
-        S.uy[i] = uyi + fty * b * dt;
-        S.uz[i] = uzi + ftz * b * dt;
+        usx = uxi + ftx * b * dt;
+        usy = uyi + fty * b * dt;
+        usz = uzi + ftz * b * dt;
     }
+    S.ux[i] = usx; S.uy[i] = usy; S.uz[i] = usz;
+    W.rec.up[i] = mk4<R>(usx, usy, usz, S.pres[i]);
     if (time_zero) W.rho_ref[i] = W.rho_new[i];
     if (P.con && pt > 0) W.temp0[i] = S.temp[i];
 }
@@ -882,45 +932,61 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, SphWork<R> W, R* pres,
-                                                 const int* __restrict__ gs, const int* __restrict__ ge) {
+                                                 const int2* __restrict__ rows,
+                                                 int patch_up) {
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
+    int* sm = s_rows[threadIdx.x >> 5];
     if (w >= P.nwall) return;
+    const SphRec<R> rec = W.rec;
     int i = W.wall_idx[w];
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
-    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th), th2 = (R)2 * th;
+    R th2 = (R)2 * (R)hi;
+    Knl<R> K = knl_make<R>(P, (R)hi);
+    K.ih = rcp(th2);
+    K.th = th2;
     double R2 = 2.0 * (P.kappa * hi);
-    float r2l = r2_lo(R2), r2h = r2_hi(R2);
+    Band bd = make_band(P, R2);
+    PosRec<R> qi = ldr(rec.pos + i);
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R tp = 0, flt = 0, tt = 0, tr = 0;
-    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
-        for (int j = a + lane; j < b; j += 32) {
-            int ptj = S.ptype[j];
-            if (ptj < 1 || ptj >= 1000) continue;
-            PairT<R> g = pair_test<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j], R2, 1e-20, r2l, r2h);
-            if (!g.in) continue;
-            R wk = knl_w<R>(P.kernel_type, tA, th2, g.r);
-            R mj = W.m_new[j], rj = W.rho_new[j];
-            R mr = mj / rj * wk;
-            tp += mr * pres[j];
-            flt += mr;
-            tt += mr * S.temp[j];
-            tr += rj / W.DEMpor[j] * wk * mj / rj;
-        }
+    for_rows_warp(P, ic, jc, kc, rows, sm, lane, [&](int j) {
+        PosRec<R> qj = ldr(rec.pos + j);
+        int ptj = tag_ptype(qj.w);
+        if (ptj < 1 || ptj >= 1000) return;
+        Disp<R> d;
+        R r2;
+        if (!test_pair(P, qi, qj, xi, yi, zi, S.x, S.y, S.z, j, R2, 1e-20, bd, d, r2)) return;
+        R r, rinv;
+        rdist(r2, r, rinv);
+        R wk = kw(K, r);
+        V4<R> fj = ldr(rec.f1 + j);
+        R mj = fj.x, rj = fj.y;
+        R mr = mj * rcp(rj) * wk;
+        tp += mr * pres[j];
+        flt += mr;
+        tt += mr * fj.z;
+        tr += rj * rcp(fj.w) * wk * mj * rcp(rj);
     });
     tp = warp_sum(tp);
     flt = warp_sum(flt);
     tt = warp_sum(tt);
     tr = warp_sum(tr);
     if (lane != 0) return;
+    R pw, rw;
     if (flt < (R)1e-6) {
-        W.rho_new[i] = W.rho_ref[i];
-        pres[i] = (R)0;
+        rw = W.rho_ref[i];
+        pw = (R)0;
     } else {
-        pres[i] = tp / flt;
+        pw = tp / flt;
         S.temp[i] = tt / flt;
-        W.rho_new[i] = W.DEMpor[i] * tr / flt;
+        rw = rec.f1[i].w * tr / flt;
     }
+    pres[i] = pw;
+    W.rho_new[i] = rw;
+    *comp<R>(rec.f1, i, 1) = rw;
+    if (patch_up) *comp<R>(rec.up, i, 3) = pw;
 }
 
 // ---------------------------------------------------------------------------
@@ -933,38 +999,56 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    const SphRec<R> rec = W.rec;
     int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
-    R pcur = S.pres[i];
+    V4<R> upi = rec.up[i];
     bool solve = it <= 2 && !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
     if (!solve) {
-        W.p_new[i] = pcur;
+        W.p_new[i] = upi.w;
         return;
     }
-    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
-    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
-    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i], rhoi = W.rho_new[i];
-    R pori = W.DEMpor[i];
+    R th = (R)S.h[i];
+    Knl<R> K = knl_make<R>(P, th);
+    PosRec<R> qi = ldr(rec.pos + i);
+    V4<R> fi = rec.f1[i];
+    R uxi = upi.x, uyi = upi.y, uzi = upi.z, rhoi = fi.y, pori = fi.w;
+    R irhoi = rcp(rhoi), prhoi = pori * rhoi;
+    R pux = pori * uxi, puy = pori * uyi, puz = pori * uzi;
+    const bool kgc = P.kgc == 1;
+    Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R bx = 0, by = 0, bz = 0, A = 0, AP = 0;
     const int* __restrict__ nb = W.nbr;
-    for (int k = 0; k < cnt; k++) {
-        int j = nb[(size_t)k * n + i];
-        if (S.ptype[j] >= 1000 || S.itype[j] == 4) continue;
-        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
-        R r = g.r + (R)1e-20;
-        R mj = W.m_new[j], rhoj = W.rho_new[j], porj = W.DEMpor[j], pj = S.pres[j];
-        R dw = knl_dw<R>(P.kernel_type, tA, th, r);
-        R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
-        kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
-        R mr = mj / rhoj;
-        bx += mr * (pori * uxi - porj * S.ux[j]) * gx;
-        by += mr * (pori * uyi - porj * S.uy[j]) * gy;
-        bz += mr * (pori * uzi - porj * S.uz[j]) * gz;
-        R c = -(g.dx * gx + g.dy * gy + g.dz * gz) / r / r;
-        R a = mj * ((pori * rhoi + porj * rhoj) / (rhoj * rhoi)) * c;
-        A += a;
-        AP += a * pj;
-    }
+    nb_walk<2, NbQ44<R>>(
+        cnt, nb, n, i,
+        [&](int j) {
+            NbQ44<R> t;
+            t.q = ldr(rec.pos + j);
+            t.a = ldr(rec.f1 + j);
+            t.b = ldr(rec.up + j);
+            return t;
+        },
+        [&](int j, const NbQ44<R>& t) {
+            int tj = t.q.w;
+            if (tag_ptype(tj) >= 1000 || tag_itype(tj) == 4) return;
+            const V4<R>& fj = t.a;
+            const V4<R>& uj = t.b;
+            Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+            R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+            rdist(r2, r, rinv);
+            R mj = fj.x, rhoj = fj.y, porj = fj.w, irj = rcp(rhoj);
+            R dw = kdw(K, r);
+            R gx = dw * g.dx * rinv, gy = dw * g.dy * rinv, gz = dw * g.dz * rinv;
+            cm_apply(Cm, kgc, gx, gy, gz);
+            R mr = mj * irj;
+            bx += mr * (pux - porj * uj.x) * gx;
+            by += mr * (puy - porj * uj.y) * gy;
+            bz += mr * (puz - porj * uj.z) * gz;
+            R c = -(g.dx * gx + g.dy * gy + g.dz * gz) * rinv * rinv;
+            R a = mj * ((prhoi + porj * rhoj) * irj * irhoi) * c;
+            A += a;
+            AP += a * uj.w;
+        });
     R b = (R)P.rho_gas * (bx + by + bz + (R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
     W.p_new[i] = (b + AP) / A;
 }
@@ -978,33 +1062,54 @@ __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWo
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    const SphRec<R> rec = W.rec;
     int it = S.itype[i], pt = S.ptype[i], bt = S.btype[i];
     W.fpx[i] = 0; W.fpy[i] = 0; W.fpz[i] = 0;
-    if (it > 2) return;
+    if (it > 2) {
+        rec.ut[i] = mk4<R>(S.ux[i], S.uy[i], S.uz[i], S.temp[i]);
+        return;
+    }
     R fx = 0, fy = 0, fz = 0;
     bool pf = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
     if (pf && P.fp) {
-        double xi = S.x[i], yi = S.y[i], zi = S.z[i];
-        R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
-        R pi = W.p_new[i], rhoi = W.rho_new[i], pori = W.DEMpor[i];
+        R th = (R)S.h[i];
+        Knl<R> K = knl_make<R>(P, th);
+        PosRec<R> qi = ldr(rec.pos + i);
+        R pi = W.p_new[i], rhoi = W.rho_new[i], pori = rec.f1[i].w;
+        R cpi = -pori * rcp(rhoi);
+        const bool kgc = P.kgc == 1;
+        Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
         int cnt = min(W.ncnt[i], P.nb_cap);
         const int* __restrict__ nb = W.nbr;
-        for (int k = 0; k < cnt; k++) {
-            int j = nb[(size_t)k * n + i];
-            if (S.ptype[j] >= 1000) continue;
-            Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
-            R r = g.r + (R)1e-20;
-            R dw = knl_dw<R>(P.kernel_type, tA, th, r);
-            R gx = dw * g.dx / r, gy = dw * g.dy / r, gz = dw * g.dz / r;
-            kgc3(W.Cm, n, i, P.kgc == 1, gx, gy, gz);
-            R Cp = -pori * W.m_new[j] * (pi + W.p_new[j]) / (rhoi * W.rho_new[j]);
-            fx += Cp * gx;
-            fy += Cp * gy;
-            fz += Cp * gz;
-        }
+        const R* __restrict__ pn = W.p_new;
+        nb_walk<4, NbQ2S<R>>(
+            cnt, nb, n, i,
+            [&](int j) {
+                NbQ2S<R> t;
+                t.q = ldr(rec.pos + j);
+                t.a = ldr(reinterpret_cast<const V2<R>*>(rec.f1 + j));
+                t.s = __ldg(pn + j);
+                return t;
+            },
+            [&](int j, const NbQ2S<R>& t) {
+                if (tag_ptype(t.q.w) >= 1000) return;
+                Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+                R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+                rdist(r2, r, rinv);
+                R dw = kdw(K, r);
+                R gx = dw * g.dx * rinv, gy = dw * g.dy * rinv, gz = dw * g.dz * rinv;
+                cm_apply(Cm, kgc, gx, gy, gz);
+                R Cp = cpi * t.a.x * (pi + t.s) * rcp(t.a.y);
+                fx += Cp * gx;
+                fy += Cp * gy;
+                fz += Cp * gz;
+            });
         W.fpx[i] = fx; W.fpy[i] = fy; W.fpz[i] = fz;
     }
-    if (pt == 9) return;
+    if (pt == 9) {
+        rec.ut[i] = mk4<R>(S.ux[i], S.uy[i], S.uz[i], S.temp[i]);
+        return;
+    }
     R ux0, uy0, uz0, ax, ay, az;
     if (pt > 0) {
         ux0 = S.ux[i]; uy0 = S.uy[i]; uz0 = S.uz[i];
@@ -1026,7 +1131,12 @@ __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWo
         S.z[i] += ((double)W.uz0[i] + (double)uzc) / 2.0 * P.sdt;
     }
     S.ux[i] = uxc; S.uy[i] = uyc; S.uz[i] = uzc;
-    if (P.con && pt > 0) S.temp[i] = W.temp0[i] + W.dtemp[i] * dt * (R)(pt != -1);
+    R tn = S.temp[i];
+    if (P.con && pt > 0) {
+        tn = W.temp0[i] + W.dtemp[i] * dt * (R)(pt != -1);
+        S.temp[i] = tn;
+    }
+    rec.ut[i] = mk4<R>(uxc, uyc, uzc, tn);
 }
 
 // ---------------------------------------------------------------------------
@@ -1175,9 +1285,10 @@ __global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, 
 // is done in place.  One warp per buffer particle (W.buf_idx).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int* __restrict__ gs,
-                                                 const int* __restrict__ ge) {
+__global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int2* __restrict__ rows) {
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
+    int* sm = s_rows[threadIdx.x >> 5];
     if (w >= P.nbuf) return;
     int i = W.buf_idx[w];
     int bt = S.btype[i];
@@ -1185,30 +1296,29 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     double zg = zi;
     if (bt == 1) zg = 2 * P.L2 - zi;
     else if (bt == 2) zg = 2 * P.L3 - zi;
-    R th = (R)hi, tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R th = (R)hi;
+    Knl<R> K = knl_make<R>(P, th);
     double Rr = P.kappa * hi;
     float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zg, ic, jc, kc);
     R hd = (R)P.h_over_dx;
     R trho = 0, tp = 0, tux = 0, tuy = 0, tuz = 0, tt = 0, flt = 0;
-    for_stencil_rows(P, ic, jc, kc, gs, ge, [&](int a, int b) {
-        for (int j = a + lane; j < b; j += 32) {
-            if (S.ptype[j] != 1 || S.btype[j] != 0) continue;
-            PairT<R> g = pair_test<R>(xi, yi, zg, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
-            if (!g.in) continue;
-            R wk = knl_w<R>(P.kernel_type, tA, th, g.r);
-            R hj = (R)S.h[j];
-            R volj = (hj / hd) * (hj / hd) * (hj / hd);
-            R vw = volj * wk;
-            trho += W.rho_new[j] / W.DEMpor[j] * wk * volj;
-            tp += vw * W.p_new[j];
-            tuz += vw * S.uz[j];
-            tux += vw * S.ux[j];
-            tuy += vw * S.uy[j];
-            tt += vw * S.temp[j];
-            flt += vw;
-        }
+    for_rows_warp(P, ic, jc, kc, rows, sm, lane, [&](int j) {
+        if (S.ptype[j] != 1 || S.btype[j] != 0) return;
+        PairT<R> g = pair_test<R>(xi, yi, zg, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
+        if (!g.in) return;
+        R wk = kw(K, g.r);
+        R hj = (R)S.h[j];
+        R volj = (hj / hd) * (hj / hd) * (hj / hd);
+        R vw = volj * wk;
+        trho += W.rho_new[j] / W.DEMpor[j] * wk * volj;
+        tp += vw * W.p_new[j];
+        tuz += vw * S.uz[j];
+        tux += vw * S.ux[j];
+        tuy += vw * S.uy[j];
+        tt += vw * S.temp[j];
+        flt += vw;
     });
     trho = warp_sum(trho); tp = warp_sum(tp); tux = warp_sum(tux); tuy = warp_sum(tuy);
     tuz = warp_sum(tuz); tt = warp_sum(tt); flt = warp_sum(flt);
@@ -1216,23 +1326,32 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     R pori = W.DEMpor[i];
     R vol0 = (th / hd) * (th / hd) * (th / hd);
     R rho_old = W.rho_new[i];
+    R pn, rn, ux, uy, uz, tn;
     if (bt == 1) {
-        W.p_new[i] = tp / flt;
-        W.rho_new[i] = pori * (R)P.rho_gas;
-        W.m_new[i] = rho_old * vol0;
-        S.uz[i] = (R)P.inlet_uz * (R)2 - tuz / flt;
-        S.ux[i] = (R)0 - tux / flt;
-        S.uy[i] = (R)0 - tuy / flt;
-        S.temp[i] = (R)P.inlet_temp;
+        pn = tp / flt;
+        rn = pori * (R)P.rho_gas;
+        uz = (R)P.inlet_uz * (R)2 - tuz / flt;
+        ux = (R)0 - tux / flt;
+        uy = (R)0 - tuy / flt;
+        tn = (R)P.inlet_temp;
     } else {
-        W.p_new[i] = (R)0;
-        W.rho_new[i] = pori * (trho / flt);
-        W.m_new[i] = rho_old * vol0;
-        S.uz[i] = tuz / flt;
-        S.ux[i] = tux / flt;
-        S.uy[i] = tuy / flt;
-        S.temp[i] = tt / flt;
+        pn = (R)0;
+        rn = pori * (trho / flt);
+        uz = tuz / flt;
+        ux = tux / flt;
+        uy = tuy / flt;
+        tn = tt / flt;
     }
+    R mn = rho_old * vol0;
+    W.p_new[i] = pn;
+    W.rho_new[i] = rn;
+    W.m_new[i] = mn;
+    S.ux[i] = ux; S.uy[i] = uy; S.uz[i] = uz;
+    S.temp[i] = tn;
+    // the XSPH pass reads buffer particles through the records
+    *comp<R>(W.rec.f1, i, 0) = mn;
+    *comp<R>(W.rec.f1, i, 1) = rn;
+    W.rec.ut[i] = mk4<R>(ux, uy, uz, tn);
 }
 
 // ---------------------------------------------------------------------------
@@ -1245,36 +1364,51 @@ __global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWor
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
+    const SphRec<R> rec = W.rec;
     int it = S.itype[i], pt = S.ptype[i];
-    R uxi = S.ux[i], uyi = S.uy[i], uzi = S.uz[i], ti = S.temp[i];
+    V4<R> ui = rec.ut[i];
+    R uxi = ui.x, uyi = ui.y, uzi = ui.z, ti = ui.w;
     if (it != 1 || pt > 1000 || pt == 0 || pt == 9) {
         W.u_tmpx[i] = uxi; W.u_tmpy[i] = uyi; W.u_tmpz[i] = uzi; W.temp_tmp[i] = ti;
         return;
     }
-    double xi = S.x[i], yi = S.y[i], zi = S.z[i];
-    R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
+    R th = (R)S.h[i];
+    Knl<R> K = knl_make<R>(P, th);
+    PosRec<R> qi = ldr(rec.pos + i);
     R c = (R)P.c_xsph;
     int cnt = min(W.ncnt[i], P.nb_cap);
     R tx = 0, ty = 0, tz = 0, tt = 0, flt = 0;
     const int* __restrict__ nb = W.nbr;
-    for (int k = 0; k < cnt; k++) {
-        int j = nb[(size_t)k * n + i];
-        int ptj = S.ptype[j];
-        if (ptj != 1 && ptj != 3) continue;
-        Pair<R> g = make_pair<R>(xi, yi, zi, S.x[j], S.y[j], S.z[j]);
-        R w = knl_w<R>(P.kernel_type, tA, th, g.r);
-        R mr = W.m_new[j] / W.rho_new[j] * w;
-        tx += c * mr * (S.ux[j] - uxi);
-        ty += c * mr * (S.uy[j] - uyi);
-        tz += c * mr * (S.uz[j] - uzi);
-        tt += (R)0.01 * c * mr * (S.temp[j] - ti);
-        flt += mr;
-    }
+    nb_walk<4, NbQ24<R>>(
+        cnt, nb, n, i,
+        [&](int j) {
+            NbQ24<R> t;
+            t.q = ldr(rec.pos + j);
+            t.a = ldr(reinterpret_cast<const V2<R>*>(rec.f1 + j));
+            t.b = ldr(rec.ut + j);
+            return t;
+        },
+        [&](int j, const NbQ24<R>& t) {
+            int ptj = tag_ptype(t.q.w);
+            if (ptj != 1 && ptj != 3) return;
+            Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+            R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+            rdist(r2, r, rinv);
+            R w = kw(K, r);
+            R m = t.a.x * rcp(t.a.y) * w;
+            R cm = c * m;
+            tx += cm * (t.b.x - uxi);
+            ty += cm * (t.b.y - uyi);
+            tz += cm * (t.b.z - uzi);
+            tt += (R)0.01 * cm * (t.b.w - ti);
+            flt += m;
+        });
     R on = (R)(pt > 0);
-    W.u_tmpx[i] = (uxi + tx / flt) * on;
-    W.u_tmpy[i] = (uyi + ty / flt) * on;
-    W.u_tmpz[i] = (uzi + tz / flt) * on;
-    W.temp_tmp[i] = (ti + tt / flt) * on;
+    R iflt = rcp(flt);
+    W.u_tmpx[i] = (uxi + tx * iflt) * on;
+    W.u_tmpy[i] = (uyi + ty * iflt) * on;
+    W.u_tmpz[i] = (uzi + tz * iflt) * on;
+    W.temp_tmp[i] = (ti + tt * iflt) * on;
 }
 
 // end of a step: the host loop's count++ (ISPH_Calc_seperate.cuh:925)
@@ -1282,17 +1416,19 @@ __global__ void k_tick(DevFlags* F) { F->step_count += 1; }
 
 // ---------------------------------------------------------------------------
 // printed maxima (kernel_copy_max_*, functions_OUTPUT.cuh:19-65 + cub max)
-// out[0..2] = rho, |u|, ftotal over p_type!=0 && i_type<2.
-// One block, grid-stride; used off the timed path.
+// out[0..2] = rho, |u|, ftotal over p_type!=0 && i_type<2 (zeroed by the
+// caller).  Grid-stride blocks; block maxima are combined with an integer
+// atomicMax on the bit patterns, which orders non-negative doubles.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void k_stats(int n, const R* __restrict__ rho, const R* __restrict__ ux, const R* __restrict__ uy,
-                        const R* __restrict__ uz, const R* __restrict__ ft, const int* __restrict__ ptype,
-                        const int* __restrict__ itype, double* out, DevFlags* F) {
+__global__ void __launch_bounds__(256) k_stats(int n, const R* __restrict__ rho, const R* __restrict__ ux,
+                                               const R* __restrict__ uy, const R* __restrict__ uz,
+                                               const R* __restrict__ ft, const int* __restrict__ ptype,
+                                               const int* __restrict__ itype, double* out, DevFlags* F) {
     __shared__ double sm[3][256];
     double a = 0, b = 0, c = 0;
     int bad = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double u = sqrt((double)ux[i] * ux[i] + (double)uy[i] * uy[i] + (double)uz[i] * uz[i]);
         if (!isfinite(u) || !isfinite((double)rho[i])) bad = 1;
         if (ptype[i] == 0 || itype[i] >= 2) continue;
@@ -1309,7 +1445,8 @@ __global__ void k_stats(int n, const R* __restrict__ rho, const R* __restrict__ 
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int q = 0; q < 3; q++) out[q] = sm[q][0];
+        for (int q = 0; q < 3; q++)
+            atomicMax(reinterpret_cast<unsigned long long*>(out + q), (unsigned long long)__double_as_longlong(sm[q][0]));
 }
 
 }  // namespace sphdem
