@@ -307,24 +307,22 @@ def run_engine(args, world, rank, local, pg):
             hs[f][:] = eng.get(SPH, f)
         for f in DEM_STATE:
             hd[f][:] = eng.get(DEM, f)
-        hid, hsp = eng.history()
+        hid = pinned(eng.nd * 16, torch.int32).reshape(eng.nd, 16)
+        hsp = pinned(eng.nd * 48, torch.float64).reshape(eng.nd, 16, 3)
+        eng.history(out=(hid, hsp))
         hb = sum(a.nbytes for a in hs.values()) + sum(a.nbytes for a in hd.values()) + hid.nbytes + hsp.nbytes
         eng.set_timing(False)
         ke = max(3, min(args.steps, 10))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(ke):
-            for f in SPH_STATE:
-                eng.set(SPH, f, hs[f])
-            for f in DEM_STATE:
-                eng.set(DEM, f, hd[f])
+            eng.set_fields(SPH, hs)
+            eng.set_fields(DEM, hd)
             eng.set_history(hid, hsp)
             eng.step(1)
-            for f in SPH_STATE:
-                hs[f][:] = eng.get(SPH, f)
-            for f in DEM_STATE:
-                hd[f][:] = eng.get(DEM, f)
-            hid, hsp = eng.history()
+            eng.get_fields(SPH, hs)
+            eng.get_fields(DEM, hd)
+            eng.history(out=(hid, hsp))
         torch.cuda.synchronize()
         te = time.perf_counter() - t0
         if pg:
@@ -333,8 +331,8 @@ def run_engine(args, world, rank, local, pg):
             te = float(t.item())
         e2e = {"value": n_part * ke * world / te, "unit": "particle-updates/s", "h2d_bytes_per_step": hb,
                "d2h_bytes_per_step": hb, "ms_per_step": te / ke * 1e3,
-               "how": "per step: sphdem_set_field/set_history of the mutable state from pinned host arrays, "
-                      "sphdem_step, sphdem_get_field/get_history back"}
+               "how": "per step: sphdem_set_fields/set_history of the mutable state from pinned host arrays, "
+                      "sphdem_step, sphdem_get_fields/get_history back into them"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

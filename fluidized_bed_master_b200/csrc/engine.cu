@@ -851,6 +851,113 @@ static int set_state_t(SphdemHandle* H, int which, int field, const void* src, i
     return upload_real<R>((R*)ptr, (const double*)src, n, H->stream);
 }
 
+// ---------------------------------------------------------------------------
+// bulk field transfer: raw doubles cross the host link into (or out of) one
+// device staging buffer, and one kernel converts between the staging
+// buffer and the engine's fields; one stream synchronisation per call.
+// ---------------------------------------------------------------------------
+namespace {
+struct XTab {
+    void* p[SPHDEM_BULK_MAX_FIELDS];
+    unsigned dbl;   // bit f set: field f is stored as double
+};
+
+template <typename R>
+__global__ void k_unstage(int n, int nf, const double* __restrict__ st, XTab t) {
+    long long tot = (long long)n * nf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int f = (int)(q / n), i = (int)(q - (long long)f * n);
+        double v = st[q];
+        if ((t.dbl >> f) & 1u) ((double*)t.p[f])[i] = v;
+        else ((R*)t.p[f])[i] = (R)v;
+    }
+}
+
+template <typename R>
+__global__ void k_stage(int n, int nf, double* __restrict__ st, XTab t) {
+    long long tot = (long long)n * nf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int f = (int)(q / n), i = (int)(q - (long long)f * n);
+        st[q] = ((t.dbl >> f) & 1u) ? ((const double*)t.p[f])[i] : (double)((const R*)t.p[f])[i];
+    }
+}
+}  // namespace
+
+static int ensure_xfer(SphdemHandle* H, size_t elems) {
+    if (elems <= H->xfer_elems) return SPHDEM_OK;
+    if (H->xfer) CK(cudaFree(H->xfer));
+    H->xfer = nullptr;
+    H->xfer_elems = 0;
+    if (cudaMalloc(&H->xfer, sizeof(double) * elems) != cudaSuccess) return SPHDEM_E_NOMEM;
+    H->xfer_elems = elems;
+    return SPHDEM_OK;
+}
+
+static bool is_settable_state(int f) {
+    static const int allowed[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_UX, SPHDEM_F_UY, SPHDEM_F_UZ,
+                                  SPHDEM_F_WX, SPHDEM_F_WY, SPHDEM_F_WZ, SPHDEM_F_M, SPHDEM_F_RHO, SPHDEM_F_PRES,
+                                  SPHDEM_F_TEMP, SPHDEM_F_DDEMPOR, SPHDEM_F_FLT_S, SPHDEM_F_FDX_DF, SPHDEM_F_FDY_DF,
+                                  SPHDEM_F_FDZ_DF, SPHDEM_F_Q_SD, SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3};
+    for (int a : allowed)
+        if (a == f) return true;
+    return false;
+}
+
+template <typename R>
+static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, void* const* host, bool set) {
+    int n = which ? H->nd : H->ns;
+    XTab t;
+    t.dbl = 0;
+    for (int k = 0; k < nf; k++) {
+        if (!host[k]) return SPHDEM_E_ARG;
+        if (set ? !is_settable_state(fields[k]) : !is_real_field(fields[k])) return SPHDEM_E_ARG;
+        const void* ptr;
+        int kind;
+        if (field_ptr<R>(H, which, fields[k], &ptr, &kind) || kind == 2) return SPHDEM_E_ARG;
+        t.p[k] = (void*)ptr;
+        if (kind == 0) t.dbl |= 1u << k;
+    }
+    if (n == 0 || nf == 0) return SPHDEM_OK;
+    size_t need = (size_t)n * nf;
+    int r = ensure_xfer(H, need);
+    if (r) return r;
+    cudaStream_t st = H->stream;
+    int blocks = (int)std::min<long long>(((long long)need + 255) / 256, 148 * 8);
+    if (set) {
+        for (int k = 0; k < nf; k++)
+            CK(cudaMemcpyAsync(H->xfer + (size_t)k * n, host[k], sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        k_unstage<R><<<blocks, 256, 0, st>>>(n, nf, H->xfer, t);
+        CK(cudaGetLastError());
+    } else {
+        k_stage<R><<<blocks, 256, 0, st>>>(n, nf, H->xfer, t);
+        CK(cudaGetLastError());
+        for (int k = 0; k < nf; k++)
+            CK(cudaMemcpyAsync(host[k], H->xfer + (size_t)k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
+                                 const double* const* host_src) {
+    if (!h || !h->committed || !fields || !host_src || (which != 0 && which != 1) || nfields < 0 ||
+        nfields > SPHDEM_BULK_MAX_FIELDS)
+        return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64
+               ? bulk_t<double>(h, which, nfields, fields, (void* const*)host_src, true)
+               : bulk_t<float>(h, which, nfields, fields, (void* const*)host_src, true);
+}
+
+extern "C" int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
+                                 double* const* host_dst) {
+    if (!h || !h->committed || !fields || !host_dst || (which != 0 && which != 1) || nfields < 0 ||
+        nfields > SPHDEM_BULK_MAX_FIELDS)
+        return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64
+               ? bulk_t<double>(h, which, nfields, fields, (void* const*)host_dst, false)
+               : bulk_t<float>(h, which, nfields, fields, (void* const*)host_dst, false);
+}
+
 extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const void* src, size_t bytes) {
     if (!h || !src || (which != 0 && which != 1)) return SPHDEM_E_ARG;
     if (h->committed) {
@@ -969,52 +1076,63 @@ extern "C" int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* d
     return SPHDEM_OK;
 }
 
+// history planes (slot-major on the device) <-> particle-major host
+// arrays: the transpose runs on the GPU into the bulk staging buffer, and
+// the host link sees two contiguous copies.
+__global__ void k_hist_out(int n, const int* __restrict__ hid, const double* __restrict__ hds, int* ids,
+                           double* sp) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * SPHDEM_NSLOT) return;
+    int i = q / SPHDEM_NSLOT, s = q - i * SPHDEM_NSLOT;
+    ids[q] = hid[(size_t)s * n + i];
+    for (int c = 0; c < 3; c++) sp[(size_t)q * 3 + c] = hds[(size_t)(s * 3 + c) * n + i];
+}
+__global__ void k_hist_in(int n, const int* __restrict__ ids, const double* __restrict__ sp, int* hid, double* hds) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * SPHDEM_NSLOT) return;
+    int i = q / SPHDEM_NSLOT, s = q - i * SPHDEM_NSLOT;
+    hid[(size_t)s * n + i] = ids[q];
+    for (int c = 0; c < 3; c++) hds[(size_t)(s * 3 + c) * n + i] = sp[(size_t)q * 3 + c];
+}
+
 template <typename R>
-static int history_t(SphdemHandle* H, int32_t* ids, double* sp) {
+static int history_t(SphdemHandle* H, int32_t* ids, double* sp, bool set) {
     EngineHost<R>* EH = (EngineHost<R>*)H->eng;
     DemState<R>& D = EH->E.D[EH->E.cur_d];
     int n = H->nd;
     if (n == 0) return SPHDEM_OK;
-    std::vector<int> hid((size_t)n * SPHDEM_NSLOT);
-    std::vector<double> hds((size_t)n * SPHDEM_NSLOT * 3);
-    CK(cudaStreamSynchronize(H->stream));
-    CK(cudaMemcpy(hid.data(), D.hid, sizeof(int) * hid.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(hds.data(), D.hds, sizeof(double) * hds.size(), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; i++)
-        for (int s = 0; s < SPHDEM_NSLOT; s++) {
-            ids[(size_t)i * SPHDEM_NSLOT + s] = hid[(size_t)s * n + i];
-            for (int c = 0; c < 3; c++) sp[((size_t)i * SPHDEM_NSLOT + s) * 3 + c] = hds[(size_t)(s * 3 + c) * n + i];
-        }
+    size_t m = (size_t)n * SPHDEM_NSLOT;
+    int r = ensure_xfer(H, m * 3 + (m + 1) / 2);
+    if (r) return r;
+    double* dsp = H->xfer;
+    int* dids = (int*)(H->xfer + m * 3);
+    cudaStream_t st = H->stream;
+    int blocks = (int)((m + 255) / 256);
+    if (set) {
+        CK(cudaMemcpyAsync(dids, ids, sizeof(int) * m, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dsp, sp, sizeof(double) * m * 3, cudaMemcpyHostToDevice, st));
+        k_hist_in<<<blocks, 256, 0, st>>>(n, dids, dsp, D.hid, D.hds);
+        CK(cudaGetLastError());
+    } else {
+        k_hist_out<<<blocks, 256, 0, st>>>(n, D.hid, D.hds, dids, dsp);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(ids, dids, sizeof(int) * m, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sp, dsp, sizeof(double) * m * 3, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
     return SPHDEM_OK;
 }
 
 extern "C" int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs) {
     if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
-    return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, ids, springs) : history_t<float>(h, ids, springs);
-}
-
-template <typename R>
-static int set_history_t(SphdemHandle* H, const int32_t* ids, const double* sp) {
-    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
-    DemState<R>& D = EH->E.D[EH->E.cur_d];
-    int n = H->nd;
-    if (n == 0) return SPHDEM_OK;
-    std::vector<int> hid((size_t)n * SPHDEM_NSLOT);
-    std::vector<double> hds((size_t)n * SPHDEM_NSLOT * 3);
-    for (int i = 0; i < n; i++)
-        for (int s = 0; s < SPHDEM_NSLOT; s++) {
-            hid[(size_t)s * n + i] = ids[(size_t)i * SPHDEM_NSLOT + s];
-            for (int c = 0; c < 3; c++) hds[(size_t)(s * 3 + c) * n + i] = sp[((size_t)i * SPHDEM_NSLOT + s) * 3 + c];
-        }
-    CK(cudaStreamSynchronize(H->stream));
-    CK(cudaMemcpy(D.hid, hid.data(), sizeof(int) * hid.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(D.hds, hds.data(), sizeof(double) * hds.size(), cudaMemcpyHostToDevice));
-    return SPHDEM_OK;
+    return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, ids, springs, false)
+                                       : history_t<float>(h, ids, springs, false);
 }
 
 extern "C" int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* springs) {
     if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
-    return h->prec == SPHDEM_PREC_FP64 ? set_history_t<double>(h, ids, springs) : set_history_t<float>(h, ids, springs);
+    return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, (int32_t*)ids, (double*)springs, true)
+                                       : history_t<float>(h, (int32_t*)ids, (double*)springs, true);
 }
 
 extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
@@ -1182,6 +1300,7 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     if (h->eng) {
         if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
     }
+    if (h->xfer) cudaFree(h->xfer);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

@@ -38,6 +38,9 @@ struct SphdemHandle {
     std::vector<int> ev_used;
     std::vector<double> kern_ms;
     std::vector<int64_t> kern_n;
+    // device staging buffer of the bulk field transfers (doubles)
+    double* xfer = nullptr;
+    size_t xfer_elems = 0;
     int ppe_iters = 0;
     double ppe_res = 0.0;
     double ppe_ms = 0.0;

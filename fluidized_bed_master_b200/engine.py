@@ -57,6 +57,8 @@ def lib():
     L.sphdem_get_counts.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
     L.sphdem_get_stream.argtypes = [vp, P(vp)]
     L.sphdem_get_launch_count.argtypes = [vp, P(C.c_int64)]
+    L.sphdem_set_fields.argtypes = [vp, C.c_int, C.c_int32, P(C.c_int32), P(P(C.c_double))]
+    L.sphdem_get_fields.argtypes = [vp, C.c_int, C.c_int32, P(C.c_int32), P(P(C.c_double))]
     L.sphdem_destroy.argtypes = [vp]
     L.sphdem_destroy.restype = None
     L.sphdem_strerror.argtypes = [C.c_int]
@@ -152,9 +154,17 @@ class Engine:
                                         lst.ctypes.data_as(C.POINTER(C.c_int32)), cap), "sphdem_get_neighbors")
         return counts, lst
 
-    def history(self):
-        ids = np.zeros((self.nd, 16), dtype=np.int32)
-        sp = np.zeros((self.nd, 16, 3), dtype=np.float64)
+    def history(self, out=None):
+        """Contact history (ids (nd, 16) int32, springs (nd, 16, 3) float64);
+        out=(ids, springs) fills preallocated arrays."""
+        if out is None:
+            ids = np.zeros((self.nd, 16), dtype=np.int32)
+            sp = np.zeros((self.nd, 16, 3), dtype=np.float64)
+        else:
+            ids, sp = out
+            if (ids.dtype != np.int32 or sp.dtype != np.float64 or not ids.flags["C_CONTIGUOUS"]
+                    or not sp.flags["C_CONTIGUOUS"] or ids.size != self.nd * 16 or sp.size != self.nd * 48):
+                raise ValueError("history out: contiguous int32 (nd,16) and float64 (nd,16,3) arrays")
         _chk(lib().sphdem_get_history(self._h, ids.ctypes.data_as(C.POINTER(C.c_int32)),
                                       sp.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_get_history")
         return ids, sp
@@ -162,6 +172,28 @@ class Engine:
     def set(self, which, name, arr):
         """Upload a state field after commit, in the current slot order."""
         self._set(which, name, arr)
+
+    def _bulk(self, fn, which, arrays, what):
+        names = list(arrays)
+        n = self.nd if which == DEM else self.ns
+        ids = (C.c_int32 * len(names))(*[F[k] for k in names])
+        ptrs = (C.POINTER(C.c_double) * len(names))()
+        for k, name in enumerate(names):
+            a = arrays[name]
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.shape != (n,):
+                raise ValueError(f"{name}: need a contiguous float64 array of {n}")
+            ptrs[k] = a.ctypes.data_as(C.POINTER(C.c_double))
+        _chk(fn(self._h, which, len(names), ids, ptrs), what)
+
+    def set_fields(self, which, arrays):
+        """Upload several state fields at once ({name: float64 array}) after
+        commit, in the current slot order (sphdem_set_fields)."""
+        self._bulk(lib().sphdem_set_fields, which, arrays, "sphdem_set_fields")
+
+    def get_fields(self, which, arrays):
+        """Fill {name: float64 array} with the current values of several
+        real fields at once (sphdem_get_fields)."""
+        self._bulk(lib().sphdem_get_fields, which, arrays, "sphdem_get_fields")
 
     def set_history(self, ids, springs):
         ids = np.ascontiguousarray(ids, dtype=np.int32)

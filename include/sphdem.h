@@ -244,6 +244,21 @@ int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
 int sphdem_set_field(SphdemHandle* h, int which, int field,
                      const void* host_src, size_t bytes);
 
+/* Bulk transfer of up to SPHDEM_BULK_MAX_FIELDS real fields of one set
+ * after sphdem_commit_particles, in the current slot order: host_src[k]
+ * (host_dst[k]) holds n doubles of field fields[k].  The doubles are
+ * staged through one device buffer and converted on the GPU; the call
+ * returns after one stream synchronisation, so pinned host buffers reach
+ * full link bandwidth.  set: the state fields sphdem_set_field accepts
+ * after commit; get: any real field.  These are the per-step calls of a
+ * host that owns the particle state (the copies SOPHIA_gpu makes around
+ * its output, ISPH_Calc_seperate.cuh:928-968, for every field). */
+#define SPHDEM_BULK_MAX_FIELDS 32
+int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields,
+                      const int32_t* fields, const double* const* host_src);
+int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields,
+                      const int32_t* fields, double* const* host_dst);
+
 /* Finish the particle upload: bounding box, cell grid, buffer tags
  * (ISPH.cuh:104-113, functions_NNPS.cuh:60-200).  Must be called once
  * after the last sphdem_set_field and before the first step. */

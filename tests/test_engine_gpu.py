@@ -233,3 +233,49 @@ def test_kernel_timing_mode(calm_bed):
         assert n == 3 and ms > 0, (k, ms, n)
     e.set_timing(False)
     e.step(2)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_bulk_field_transfer(calm_bed, prec):
+    """sphdem_get_fields equals per-field reads; sphdem_set_fields writes what
+    sphdem_set_field writes (both convert to the field precision)."""
+    p, sph, dem = calm_bed
+    e = _engine(p, sph, dem, prec)
+    e.step(2)
+    for which, names in ((SPH, ["x", "uz", "m", "rho", "pres", "temp", "flt_s"]),
+                         (DEM, ["x", "ux", "wz", "temp", "Q_sd", "ftotalz"])):
+        n = e.nd if which == DEM else e.ns
+        bulk = {f: np.empty(n) for f in names}
+        e.get_fields(which, bulk)
+        for f in names:
+            assert np.array_equal(bulk[f], e.get(which, f)), f
+        settable = [f for f in names if f != "ftotalz"]
+        rng = np.random.default_rng(5)
+        new = {f: bulk[f] * (1.0 + 1e-3 * rng.standard_normal(n)) for f in settable}
+        e.set_fields(which, new)
+        for f in settable:
+            ref = new[f].astype(np.float32).astype(np.float64) if (prec == 0 and f != "x") else new[f]
+            assert np.array_equal(e.get(which, f), ref), f
+    with pytest.raises(Exception):
+        e.set_fields(SPH, {"ftotalx": np.zeros(e.ns)})
+
+
+def test_history_roundtrip_keeps_the_run(contact_bed):
+    """get_history -> set_history is the identity, and a run continued after
+    a round trip of the whole state equals the uninterrupted run."""
+    p, sph, dem = contact_bed
+    a = _engine(p, sph, dem, 1)
+    b = _engine(p, sph, dem, 1)
+    a.step(3)
+    b.step(3)
+    ids, sp = b.history()
+    assert (ids > 0).sum() > 0
+    b.set_history(np.zeros_like(ids), np.zeros_like(sp))
+    assert (b.history()[0] > 0).sum() == 0
+    b.set_history(ids, sp)
+    i2, s2 = b.history()
+    assert np.array_equal(ids, i2) and np.array_equal(sp, s2)
+    a.step(3)
+    b.step(3)
+    for f in ("x", "uz", "wx"):
+        assert np.array_equal(a.get(DEM, f), b.get(DEM, f)), f
