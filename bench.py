@@ -73,6 +73,30 @@ def dist_setup():
     return world, rank, local, pg
 
 
+def reduce_over_ranks(pg, value, op, device="cpu"):
+    """value reduced over all ranks (op: "max" or "sum"); value itself when
+    there is no process group.  Every rank must call it at the same point."""
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX if op == "max" else pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+WORKLOAD_TEXT = ("3-D SPH-DEM fluidized bed 0.1x0.02x0.4 m: 200,000 fluid SPH on dx=1.25 mm (+inlet/wall "
+                 "particles) and 20,000 DEM spheres d=2 mm, Wendland C2, h=1.3dx, heat transfer, ISPH-DEM step "
+                 "(reference PPE sweep)")
+
+
+def bench_config(n_sph, n_dem, world, fields):
+    return {"workload": WORKLOAD_TEXT, "n_sph": n_sph, "n_dem": n_dem,
+            "l2": "256 MB buffer written before every timed step",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "positions": "f64", "fields": fields}
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -158,6 +182,24 @@ def manifest_bytes(kernel, ns, nd, nwall, nbuf, avg_nb, r):
     return per.get(kernel)
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of `kernel` on this workload, from the ncu summaries in profiles/
+    (a line 'traffic_bytes_per_launch: <kernel> <bytes>'), or None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith(".md"):
+            continue
+        with open(os.path.join(d, fn)) as fh:
+            for ln in fh:
+                parts = ln.split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch:" and parts[1] == kernel:
+                    return float(parts[2])
+    return None
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -199,15 +241,18 @@ def cpu_reference(seconds=None, warmup=1, steps=None):
 def run_reference(args, world, rank):
     if rank != 0:
         return
+    from fluidized_bed_master_b200.beds import box_bed
+
+    _, sph_full, dem_full = box_bed(seed=0, **WORKLOAD)
+    config = bench_config(len(sph_full["x"]), len(dem_full["x"]), world, "f64")
     val, cores, sample, s_per_step = cpu_reference(warmup=args.warmup, steps=args.steps)
     unit = "particle-updates/s"
     line = {
         "metric": "SPH-DEM particle-updates/s on 1 B200 (3-D fluidized bed, ISPH-DEM step)",
         "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded box bed slice)",
-        "config": {"workload": "3-D SPH-DEM fluidized bed 0.1x0.02x0.4 m, dx=1.25 mm, bounded CPU sample",
-                   "parallelism": "host threads"},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded box bed; bounded slice per step)",
+        "config": config,
         "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -264,12 +309,9 @@ def run_engine(args, world, rank, local, pg):
     if pg:
         pg.barrier()
     clocks = sampler.stop()
-    t_max = total_ms
-    if pg:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = n_part * args.steps * world / (t_max / 1e3)
+    t_max = reduce_over_ranks(pg, total_ms, "max", "cuda")
+    n_all = reduce_over_ranks(pg, n_part, "sum", "cuda")
+    value = n_all * args.steps / (t_max / 1e3)
     ms_per_step = t_max / args.steps
 
     # dominant kernel and its roofline
@@ -283,13 +325,7 @@ def run_engine(args, world, rank, local, pg):
     bytes_dom = manifest_bytes(dom_name, eng.ns, eng.nd, nwall, nbuf, avg_nb, r)
     peak, peak_kind = load_peaks()
     achieved = bytes_dom / (dom_ms / max(dom_n, 1) / 1e3) / 1e9 if (bytes_dom and dom_n) else None
-    traffic = None
-    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr_path):
-        try:
-            traffic = json.load(open(tr_path)).get(dom_name)
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(dom_name) if args.precision == "fp32" else None
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "bytes_per_launch": bytes_dom, "launch_ms": dom_ms / max(dom_n, 1), "peak_source": peak_kind,
@@ -324,12 +360,8 @@ def run_engine(args, world, rank, local, pg):
             eng.get_fields(DEM, hd)
             eng.history(out=(hid, hsp))
         torch.cuda.synchronize()
-        te = time.perf_counter() - t0
-        if pg:
-            t = torch.tensor([te], dtype=torch.float64, device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            te = float(t.item())
-        e2e = {"value": n_part * ke * world / te, "unit": "particle-updates/s", "h2d_bytes_per_step": hb,
+        te = reduce_over_ranks(pg, time.perf_counter() - t0, "max", "cuda")
+        e2e = {"value": n_all * ke / te, "unit": "particle-updates/s", "h2d_bytes_per_step": hb,
                "d2h_bytes_per_step": hb, "ms_per_step": te / ke * 1e3,
                "how": "per step: sphdem_set_fields/set_history of the mutable state from pinned host arrays, "
                       "sphdem_step, sphdem_get_fields/get_history back into them"}
@@ -346,13 +378,8 @@ def run_engine(args, world, rank, local, pg):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if r == 4 else "f64",
         "data": "synthetic (seeded box bed; reference input.txt not shipped)",
-        "config": {"workload": "3-D SPH-DEM fluidized bed 0.1x0.02x0.4 m: 200,000 fluid SPH on dx=1.25 mm "
-                               "(+inlet/wall particles) and 20,000 DEM spheres d=2 mm, Wendland C2, "
-                               "h=1.3dx, heat transfer, ISPH-DEM step (reference PPE sweep)",
-                   "n_sph": eng.ns, "n_dem": eng.nd, "avg_neighbours": avg_nb,
-                   "l2": "256 MB buffer written before every timed step",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "positions": "f64", "fields": "f32" if r == 4 else "f64"},
+        "config": bench_config(eng.ns, eng.nd, world, "f32" if r == 4 else "f64"),
+        "avg_neighbours": avg_nb,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
