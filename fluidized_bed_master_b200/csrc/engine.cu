@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "handle.h"
-#include "step_kernels.cuh"
+#include "ppe_krylov.cuh"
 
 using namespace sphdem;
 
@@ -86,6 +86,7 @@ struct Alloc {
 template <typename R>
 struct EngineHost {
     Engine<R> E;
+    KryWork<R> K{};          // PPE solver state (allocated for the Krylov modes)
     Alloc A;
     int nb_cap = 0;
     size_t list_elems = 0;
@@ -257,6 +258,89 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
 }
 
 // ---------------------------------------------------------------------------
+// PPE to a relative residual (ppe_krylov.cuh).  Assembly and the initial
+// residual are plain kernels; the iterations are the body of a conditional
+// while node of the step graph (captured on a side stream into the node's
+// body graph).  Without a graph the host drives the same body.
+// ---------------------------------------------------------------------------
+template <typename R>
+static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cudaGraphConditionalHandle hnd,
+                        int in_graph) {
+    KryWork<R>& K = EH->K;
+    const DevParams& P = EH->E.P;
+    const int* nb = EH->E.sw.nbr;
+    int n = P.ns;
+    if (H->p.ppe_mode == SPHDEM_PPE_PCG) {
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.p, K.v, K.p, KP_PQ, nullptr, 0, 0);
+        k_cg_x<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.p, K.v, K.x, K.r, K.z, K.part, K.sc);
+        k_cg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.z, K.p, K.part, K.sc);
+        k_kry_check<<<1, KRY_T, 0, st>>>(K.part, K.sc, hnd, in_graph, 1);
+    } else {
+        k_bicg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.r, K.p, K.v, K.y, K.part, K.sc);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.y, K.v, K.rh, KP_RHV, nullptr, 0, 0);
+        k_bicg_s<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.r, K.v, K.y, K.x, K.s, K.z, K.part, K.sc);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.z, K.t, K.s, KP_TS, nullptr, KP_TT, 1);
+        k_bicg_x<<<KRY_G, KRY_T, 0, st>>>(n, K.s, K.t, K.z, K.rh, K.x, K.r, K.part, K.sc);
+        k_kry_check<<<1, KRY_T, 0, st>>>(K.part, K.sc, hnd, in_graph, 0);
+    }
+}
+
+template <typename R>
+static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, SphWork<R>& W) {
+    KryWork<R>& K = EH->K;
+    const DevParams& P = EH->E.P;
+    cudaStream_t st = H->stream;
+    int n = P.ns;
+    int cg = H->p.ppe_mode == SPHDEM_PPE_PCG;
+    CK(cudaMemsetAsync(K.sc + KS_DONE, 0, sizeof(double), st));
+    k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, (const R*)nullptr);
+    k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
+    k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
+    k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);
+    CK(cudaGetLastError());
+    if (H->capturing) {
+        cudaStreamCaptureStatus cs;
+        unsigned long long id = 0;
+        cudaGraph_t cgraph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(st, &cs, &id, &cgraph, &deps, &ndeps));
+        if (cs != cudaStreamCaptureStatusActive) return SPHDEM_E_CUDA;
+        cudaGraphConditionalHandle hnd;
+        CK(cudaGraphConditionalHandleCreate(&hnd, cgraph, 1, cudaGraphCondAssignDefault));
+        // (the union inside cudaGraphNodeParams has no default constructor)
+        alignas(cudaGraphNodeParams) unsigned char cp_buf[sizeof(cudaGraphNodeParams)];
+        std::memset(cp_buf, 0, sizeof(cp_buf));
+        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_buf);
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, cgraph, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+        if (!H->side) CK(cudaStreamCreateWithFlags(&H->side, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCaptureToGraph(H->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        krylov_body<R>(H, EH, H->side, hnd, 1);
+        cudaGraph_t out = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(H->side, &out);
+        if (ce != cudaSuccess) return SPHDEM_E_CUDA;
+    } else {
+        double done = 0;
+        for (int it = 0; it < std::max(H->p.ppe_max_iter, 1); it++) {
+            krylov_body<R>(H, EH, st, 0, 0);
+            CK(cudaMemcpyAsync(&done, K.sc + KS_DONE, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (done != 0.0) break;
+        }
+    }
+    k_kry_final<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K);
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // one step (SOPHIA_single_ISPH order).  flags: bit1 count==0, bit2 filter
 // step, bit3 time==0.
 // ---------------------------------------------------------------------------
@@ -303,7 +387,11 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.rows, 1);
             *nl += 1;
         }
-        { KTIME(KT_PPE); k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W); }
+        {
+            KTIME(KT_PPE);
+            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W);
+            else if ((r = enqueue_krylov<R>(H, EH, S, W))) return r;
+        }
         { KTIME(KT_NEUMANN); k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0); }
         { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
         *nl += 4;
@@ -344,7 +432,9 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
             cudaGraph_t g;
             if (H->timing) std::fill(H->ev_used.begin(), H->ev_used.end(), 0);
             CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
+            H->capturing = true;
             int r = enqueue_step<R>(H, EH, flags, &n);
+            H->capturing = false;
             cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
             if (r) return r;
             if (ce != cudaSuccess) return SPHDEM_E_CUDA;
@@ -582,6 +672,16 @@ static int commit_t(SphdemHandle* H) {
         EH->nb_cap = cap;
         W.nbr = A.get<int>((size_t)cap * ns);
         if (!A.ok) return SPHDEM_E_NOMEM;
+        if (p.ppe_mode != SPHDEM_PPE_REFERENCE) {
+            KryWork<R>& K = EH->K;
+            K.a = A.get<R>((size_t)cap * ns);
+            K.kcnt = A.get<int>(ns);
+            double** vecs[] = {&K.d, &K.b, &K.x, &K.r, &K.rh, &K.p, &K.v, &K.s, &K.t, &K.y, &K.z};
+            for (double** v : vecs) *v = A.get<double>(ns);
+            K.part = A.get<double>((size_t)KRY_NPART * KRY_G);
+            K.sc = A.get<double>(KS_COUNT);
+            if (!A.ok) return SPHDEM_E_NOMEM;
+        }
         CK(cudaMemsetAsync(E.flags, 0, sizeof(DevFlags), st));
         CK(cudaStreamSynchronize(st));
     }
@@ -737,8 +837,16 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
     CK(cudaStreamSynchronize(st));
     out->count = H->count;
     out->time = H->time;
-    out->ppe_iters = H->ppe_iters;
-    out->ppe_rel_residual = H->ppe_res;
+    out->ppe_iters = 1;               // the reference's single sweep
+    out->ppe_rel_residual = 0.0;      // not formed by the reference sweep
+    if (H->p.ppe_mode != SPHDEM_PPE_REFERENCE && EH->K.sc) {
+        double sc[KS_COUNT];
+        CK(cudaMemcpyAsync(sc, EH->K.sc, sizeof(sc), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out->ppe_iters = (int32_t)sc[KS_ITER];
+        out->ppe_rel_residual = sc[KS_RES];
+        out->ppe_status = (int32_t)sc[KS_STATUS];
+    }
     out->ppe_ms = H->ppe_ms;
     out->overflow_flags = f.overflow;
     out->nan_flag = f.nan;
@@ -771,7 +879,9 @@ static int check_supported(const SphdemParams* p) {
     if (p->decouple_stride != 1) return SPHDEM_E_UNSUPPORTED;
     if (p->flag_z_index) return SPHDEM_E_UNSUPPORTED;
     if (p->open_boundary == 2) return SPHDEM_E_UNSUPPORTED;
-    if (p->ppe_mode != SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
+    if (p->ppe_mode != SPHDEM_PPE_REFERENCE && p->ppe_mode != SPHDEM_PPE_KRYLOV && p->ppe_mode != SPHDEM_PPE_PCG)
+        return SPHDEM_E_UNSUPPORTED;
+    if (p->ppe_mode != SPHDEM_PPE_REFERENCE && !(p->ppe_tol > 0)) return SPHDEM_E_ARG;
     if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
     if (!(p->dt > 0) || !(p->kappa > 0) || p->freq_filt <= 0) return SPHDEM_E_ARG;
     return SPHDEM_OK;
@@ -1301,6 +1411,7 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
         if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
     }
     if (h->xfer) cudaFree(h->xfer);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

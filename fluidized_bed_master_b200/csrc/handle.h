@@ -31,6 +31,8 @@ struct SphdemHandle {
     std::map<int, int64_t> graph_launches;
     std::map<int, std::vector<int>> graph_kused;
     int use_graphs = 1;
+    bool capturing = false;              // inside the capture of a step graph
+    cudaStream_t side = nullptr;         // captures the body of the PPE while node
     int64_t last_launches = 0;
     // per-kernel timing (events recorded inside the step graph)
     int timing = 0;

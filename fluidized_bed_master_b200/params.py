@@ -65,7 +65,13 @@ class SphdemStats(C.Structure):
         ("count", C.c_int32), ("ppe_iters", C.c_int32), ("time", C.c_double),
         ("ppe_rel_residual", C.c_double), ("ppe_ms", C.c_double),
         ("overflow_flags", C.c_int32), ("nan_flag", C.c_int32),
+        ("ppe_status", C.c_int32), ("reserved_stats", C.c_int32),
     ]
+
+
+# PPE modes and warm starts (SPHDEM_PPE_*, SPHDEM_WARM_*)
+PPE_REFERENCE, PPE_KRYLOV, PPE_PCG = 0, 1, 2
+WARM_PREVIOUS, WARM_MLP = 0, 1
 
 
 # field ids (enum SphdemField)

@@ -54,10 +54,14 @@ extern "C" {
 
 /* PPE solution method.  REFERENCE = one Jacobi sweep per step with the
  * previous pressure as iterate (functions_PPE2.cuh:542-698, 868-878).
- * KRYLOV = matrix-free Jacobi-preconditioned BiCGStab on the same operator
- * to a relative residual ppe_tol (no reference counterpart). */
+ * KRYLOV = Jacobi-preconditioned BiCGStab on the same operator to a
+ * relative residual ppe_tol; PCG = Jacobi-preconditioned conjugate
+ * gradients (for symmetric operators: no gradient correction, equal
+ * masses).  Neither has a reference counterpart; one Jacobi sweep of
+ * either operator from the previous pressure is the reference update. */
 #define SPHDEM_PPE_REFERENCE 0
 #define SPHDEM_PPE_KRYLOV    1
+#define SPHDEM_PPE_PCG       2
 
 /* Warm start for the KRYLOV mode: previous pressure or the learned MLP. */
 #define SPHDEM_WARM_PREVIOUS 0
@@ -202,6 +206,8 @@ typedef struct SphdemStats {
     double  ppe_ms;             /* device time of the last PPE solve      */
     int32_t overflow_flags;     /* bit0 SPH list, bit1 DEM history        */
     int32_t nan_flag;
+    int32_t ppe_status;         /* 0 converged, 1 iteration cap, 2 breakdown */
+    int32_t reserved_stats;
 } SphdemStats;
 
 typedef struct SphdemHandle SphdemHandle;

@@ -45,6 +45,7 @@ def lib():
     L.oracle_get_history.argtypes = [vp, P(C.c_double), P(C.c_double), C.c_int]
     L.oracle_set_history.argtypes = [vp, P(C.c_double), P(C.c_double), C.c_int]
     L.oracle_set_threads.argtypes = [vp, C.c_int]
+    L.oracle_get_ppe.argtypes = [vp, P(C.c_int), P(C.c_double), P(C.c_int)]
     _lib = L
     return L
 
@@ -109,6 +110,12 @@ class Oracle:
         lib().oracle_get_history(self._h, ct.ctypes.data_as(C.POINTER(C.c_double)),
                                  ds.ctypes.data_as(C.POINTER(C.c_double)), self.nd)
         return ct, ds
+
+    def ppe(self):
+        """(iterations, relative residual, status) of the last Krylov PPE solve."""
+        it, res, st = C.c_int(), C.c_double(), C.c_int()
+        lib().oracle_get_ppe(self._h, C.byref(it), C.byref(res), C.byref(st))
+        return it.value, res.value, st.value
 
     def close(self):
         if getattr(self, "_h", None):

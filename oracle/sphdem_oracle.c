@@ -73,6 +73,9 @@ struct OracleState {
     int* nb_cnt;           /* SPH neighbour list of the last step */
     int* nb_list;
     int nb_cap;
+    int ppe_iters;         /* last PPE solve (Krylov modes) */
+    double ppe_res;
+    int ppe_status;
 };
 
 static void* xcalloc(size_t n, size_t sz) {
@@ -1179,6 +1182,193 @@ static void k_neumann(OracleState* S) {
     }
 }
 
+/* ---------------------------------------------------------------------- */
+/* PPE solved to a relative residual (engine extension, no reference       */
+/* counterpart).  Row i of a solved particle (the rows the reference sweep */
+/* updates): d_i p_i - sum_{j solved} a_ij p_j = b_i + sum_{j fixed} a_ij p_j */
+/* with a_ij and b_i the terms of KERNEL_PPE3D_sph and d_i = sum_j a_ij, so */
+/* one Jacobi sweep from the current pressure is the reference update.    */
+/* Jacobi-preconditioned BiCGStab (KRYLOV) or CG (PCG), FP64, stopping at  */
+/* ||r||/||b|| <= ppe_tol or ppe_max_iter iterations.                      */
+/* ---------------------------------------------------------------------- */
+static int ppe_solved_row(const SphdemParams* P, const OSet* o, int i) {
+    return o->i_type[i] <= 2 && !(P->open_boundary > 0 && o->buffer_type[i] > 0) && o->p_type[i] < 1000 &&
+           o->p_type[i] > 0;
+}
+
+typedef struct {
+    int n;
+    int* rp;        /* row pointers (solved neighbours only) */
+    int* cj;
+    double* av;
+    double *d, *b;
+} PpeSys;
+
+static void ppe_matvec(const PpeSys* A, const int* solved, const double* x, double* y, int nthreads) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int i = 0; i < A->n; i++) {
+        if (!solved[i]) {
+            y[i] = 0;
+            continue;
+        }
+        double acc = 0;
+        for (int k = A->rp[i]; k < A->rp[i + 1]; k++) acc += A->av[k] * x[A->cj[k]];
+        y[i] = A->d[i] * x[i] - acc;
+    }
+}
+static double ppe_dot(int n, const double* a, const double* b) {
+    double s = 0;
+    for (int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+static void ppe_krylov(OracleState* S, double tdt) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    int n = o->n;
+    (void)tdt;
+    int* solved = (int*)xcalloc(n, sizeof(int));
+    int* cnt = (int*)xcalloc(n, sizeof(int));
+    for (int i = 0; i < n; i++) solved[i] = ppe_solved_row(P, o, i);
+    /* pass 1: solved-neighbour counts; pass 2: coefficients */
+    PpeSys A;
+    A.n = n;
+    A.rp = (int*)xcalloc(n + 1, sizeof(int));
+    A.d = (double*)xcalloc(n, sizeof(double));
+    A.b = (double*)xcalloc(n, sizeof(double));
+    for (int pass = 0; pass < 2; pass++) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+        for (int i = 0; i < n; i++) {
+            if (!solved[i]) continue;
+            double hi = o->h[i], tA = knl_tmpA(P->kernel_type, P->dim, hi), R = P->kappa * hi;
+            double xi = o->x[i], yi = o->y[i], zi = o->z[i], rhoi = o->rho[i], pori = o->DEMpor[i];
+            const double* Cm = o->Cm + (size_t)i * 9;
+            int ic, jc, kc;
+            cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+            int c = 0, k0 = pass ? A.rp[i] : 0;
+            double dsum = 0, bfix = 0;
+            FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+                if (o->p_type[j] < 1000 && o->i_type[j] != 4) {
+                    double xj = o->x[j], yj = o->y[j], zj = o->z[j];
+                    double td = dist3(xi, yi, zi, xj, yj, zj) + 1e-20;
+                    if (td < R) {
+                        if (!pass) {
+                            if (solved[j]) c++;
+                            continue;
+                        }
+                        double mj = o->m[j], rhoj = o->rho[j], porj = o->DEMpor[j];
+                        double dw = knl_dw(P->kernel_type, tA, hi, td);
+                        double tdwx = dw * (xi - xj) / td, tdwy = dw * (yi - yj) / td, tdwz = dw * (zi - zj) / td;
+                        kgc_apply(P, Cm, &tdwx, &tdwy, &tdwz);
+                        double cc = -((xi - xj) * tdwx + (yi - yj) * tdwy + (zi - zj) * tdwz) / td / td;
+                        double a = mj * ((pori * rhoi + porj * rhoj) / (rhoj * rhoi)) * cc;
+                        dsum += a;
+                        if (solved[j]) {
+                            A.cj[k0 + c] = j;
+                            A.av[k0 + c] = a;
+                            c++;
+                        } else {
+                            bfix += a * o->pres[j];
+                        }
+                    }
+                }
+            }
+            if (!pass) cnt[i] = c;
+            else {
+                A.d[i] = dsum;
+                A.b[i] = o->PPE3[i] + bfix;
+            }
+        }
+        if (!pass) {
+            for (int i = 0; i < n; i++) A.rp[i + 1] = A.rp[i] + cnt[i];
+            A.cj = (int*)xcalloc(A.rp[n], sizeof(int));
+            A.av = (double*)xcalloc(A.rp[n], sizeof(double));
+        }
+    }
+    double *x = (double*)xcalloc(n, sizeof(double)), *r = (double*)xcalloc(n, sizeof(double));
+    double *rh = (double*)xcalloc(n, sizeof(double)), *pp = (double*)xcalloc(n, sizeof(double));
+    double *v = (double*)xcalloc(n, sizeof(double)), *ss = (double*)xcalloc(n, sizeof(double));
+    double *t = (double*)xcalloc(n, sizeof(double)), *y = (double*)xcalloc(n, sizeof(double));
+    double *z = (double*)xcalloc(n, sizeof(double));
+    for (int i = 0; i < n; i++) x[i] = solved[i] ? o->pres[i] : 0.0;
+    ppe_matvec(&A, solved, x, y, S->nthreads);
+    int cg = P->ppe_mode == SPHDEM_PPE_PCG;
+    for (int i = 0; i < n; i++) {
+        double bi = solved[i] ? A.b[i] : 0.0;
+        A.b[i] = bi;
+        r[i] = bi - y[i];
+        if (cg) {
+            z[i] = r[i] / (solved[i] ? A.d[i] : 1.0);
+            pp[i] = z[i];
+        } else {
+            rh[i] = r[i];
+        }
+    }
+    double bn = sqrt(ppe_dot(n, A.b, A.b));
+    double res = bn > 0 ? sqrt(ppe_dot(n, r, r)) / bn : 0.0;
+    int it = 0, status = 0;
+    double tol = P->ppe_tol;
+    if (cg) {
+        double rz = ppe_dot(n, r, z);
+        while (bn > 0 && res > tol && it < P->ppe_max_iter) {
+            ppe_matvec(&A, solved, pp, v, S->nthreads);
+            double pq = ppe_dot(n, pp, v);
+            if (!(pq != 0.0) || !isfinite(pq)) { status = 2; break; }
+            double alpha = rz / pq;
+            for (int i = 0; i < n; i++) {
+                x[i] += alpha * pp[i];
+                r[i] -= alpha * v[i];
+                z[i] = r[i] / (solved[i] ? A.d[i] : 1.0);
+            }
+            double rz_new = ppe_dot(n, r, z);
+            double beta = rz_new / rz;
+            for (int i = 0; i < n; i++) pp[i] = z[i] + beta * pp[i];
+            rz = rz_new;
+            it++;
+            res = sqrt(ppe_dot(n, r, r)) / bn;
+            if (!isfinite(res)) { status = 2; break; }
+        }
+    } else {
+        double rho = 1, alpha = 1, om = 1;
+        while (bn > 0 && res > tol && it < P->ppe_max_iter) {
+            double rho_new = ppe_dot(n, rh, r);
+            double beta = (rho_new / rho) * (alpha / om);
+            for (int i = 0; i < n; i++) {
+                pp[i] = r[i] + beta * (pp[i] - om * v[i]);
+                y[i] = pp[i] / (solved[i] ? A.d[i] : 1.0);
+            }
+            ppe_matvec(&A, solved, y, v, S->nthreads);
+            double rv = ppe_dot(n, rh, v);
+            if (!(rv != 0.0) || !isfinite(rv)) { status = 2; break; }
+            alpha = rho_new / rv;
+            for (int i = 0; i < n; i++) {
+                ss[i] = r[i] - alpha * v[i];
+                x[i] += alpha * y[i];
+                z[i] = ss[i] / (solved[i] ? A.d[i] : 1.0);
+            }
+            ppe_matvec(&A, solved, z, t, S->nthreads);
+            double ts = ppe_dot(n, t, ss), tt = ppe_dot(n, t, t);
+            om = tt > 0 ? ts / tt : 0.0;
+            for (int i = 0; i < n; i++) {
+                x[i] += om * z[i];
+                r[i] = ss[i] - om * t[i];
+            }
+            rho = rho_new;
+            it++;
+            res = sqrt(ppe_dot(n, r, r)) / bn;
+            if (!isfinite(res) || om == 0.0) { status = 2; break; }
+        }
+    }
+    if (status == 0 && res > tol) status = 1;
+    for (int i = 0; i < n; i++)
+        if (solved[i]) o->pres[i] = x[i];
+    S->ppe_iters = it;
+    S->ppe_res = res;
+    S->ppe_status = status;
+    free(x); free(r); free(rh); free(pp); free(v); free(ss); free(t); free(y); free(z);
+    free(A.rp); free(A.cj); free(A.av); free(A.d); free(A.b); free(solved); free(cnt);
+}
+
 /* KERNEL_PPE3D_sph + KERNEL_PPE3D_calc_sph: functions_PPE2.cuh:542-698, 868-878 */
 static void k_ppe(OracleState* S, double tdt) {
     OSet* o = &S->s;
@@ -1219,6 +1409,10 @@ static void k_ppe(OracleState* S, double tdt) {
         o->PPE4[i] = AP;
         o->PPE1[i] = rhoi * (bx + by + bz) / tdt;
         o->PPE2[i] = A;
+    }
+    if (P->ppe_mode != SPHDEM_PPE_REFERENCE) {
+        ppe_krylov(S, tdt);
+        return;
     }
     for (int i = 0; i < o->n; i++) {
         if (o->i_type[i] > 2) continue;
@@ -1773,6 +1967,14 @@ int oracle_set_history(OracleState* s, const double* ct, const double* ds, int n
     if (n != s->d.n) return SPHDEM_E_ARG;
     memcpy(s->d.ct_idx, ct, sizeof(double) * (size_t)n * NSLOT);
     memcpy(s->d.del_s, ds, sizeof(double) * (size_t)n * NSLOT * 3);
+    return 0;
+}
+
+int oracle_get_ppe(OracleState* s, int* iters, double* rel_res, int* status) {
+    if (!s) return -1;
+    if (iters) *iters = s->ppe_iters;
+    if (rel_res) *rel_res = s->ppe_res;
+    if (status) *status = s->ppe_status;
     return 0;
 }
 

@@ -57,6 +57,10 @@ int oracle_set_history(OracleState* s, const double* ct_idx, const double* del_s
  * returns W (deriv=0) or dW/dr (deriv=1) at distance r, 3-D. */
 double oracle_kernel(int kernel_type, int dim, double h, double r, int deriv);
 
+/* Iterations, relative residual and status (0 converged, 1 iteration
+ * cap, 2 breakdown) of the last PPE solve in the Krylov modes. */
+int oracle_get_ppe(OracleState* s, int* iters, double* rel_res, int* status);
+
 /* Number of OpenMP threads used by the step loops (1 = serial). */
 int oracle_set_threads(OracleState* s, int nthreads);
 

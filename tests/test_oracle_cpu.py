@@ -103,3 +103,25 @@ def test_two_sphere_head_on_restitution():
     e = (u[1] - u[0]) / (2 * v)
     assert contact_seen
     assert 0.8 < e < 0.98, e
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_oracle_krylov_ppe_converges(mode):
+    """The oracle's Krylov PPE (BiCGStab / PCG, FP64) reaches ppe_tol within
+    the iteration cap on a small bed, and differs from the one-sweep
+    reference pressure only on solved rows."""
+    from fluidized_bed_master_b200.beds import spouted_bed
+    from fluidized_bed_master_b200.params import SPH
+
+    p, sph, dem = spouted_bed(dx=2.5e-3, n_dem=200, r_dem=1.0e-3, seed=43)
+    p.ppe_mode = mode
+    p.ppe_tol = 1e-8
+    p.ppe_max_iter = 2000
+    if mode == 2:
+        p.kgc_solve = 0
+    o = Oracle(p, sph, dem, threads=4)
+    for _ in range(2):
+        o.step(1)
+        it, res, st = o.ppe()
+        assert st == 0 and res <= 1e-8 and it >= 1, (it, res, st)
+    assert np.isfinite(o.get(SPH, "pres")).all()

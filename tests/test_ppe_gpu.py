@@ -1,0 +1,101 @@
+"""The PPE solved to a relative residual (ppe_mode KRYLOV / PCG) on the GPU.
+
+Bar (written into each assert):
+* FP64 build vs the FP64 oracle running the same Jacobi-preconditioned
+  BiCGStab / CG: the same iteration count per step and rel. L2 <= 1e-7 per
+  field after 3 steps (the Krylov recurrences amplify rounding slightly
+  beyond the 1e-9 of the sweep);
+* FP32 build: its own FP64 residual norm reaches ppe_tol every step, and
+  the pressure agrees with the FP64 oracle to rel. L2 <= 1e-3 (the FP32
+  operator coefficients perturb the system at 1e-7 relative, amplified by
+  its condition number).
+"""
+import numpy as np
+import pytest
+
+from fluidized_bed_master_b200.beds import spouted_bed
+from fluidized_bed_master_b200.params import DEM, PPE_KRYLOV, PPE_PCG, SPH
+from oracle import Oracle
+from tests.helpers import by_id, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS_S = ["x", "y", "z", "ux", "uy", "uz", "rho", "pres", "temp", "m"]
+FIELDS_D = ["x", "y", "z", "ux", "uy", "uz", "temp"]
+
+
+def _bed(mode, seed=44):
+    p, sph, dem = spouted_bed(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=seed, spacing=2.1)
+    p.ppe_mode = mode
+    p.ppe_tol = 1e-6
+    p.ppe_max_iter = 1000
+    if mode == PPE_PCG:
+        p.kgc_solve = 0
+    return p, sph, dem
+
+
+def _engine(p, sph, dem, prec):
+    from fluidized_bed_master_b200.engine import Engine
+
+    q = p.copy()
+    q.precision = prec
+    return Engine(q, sph, dem)
+
+
+def _ids(src, which):
+    return src.get(which, "pid") if which == SPH else src.get(which, "dem_idx")
+
+
+@pytest.mark.parametrize("mode", [PPE_KRYLOV, PPE_PCG])
+def test_fp64_krylov_matches_oracle(mode):
+    p, sph, dem = _bed(mode)
+    eng = _engine(p, sph, dem, 1)
+    orc = Oracle(p, sph, dem, threads=8)
+    for step in range(3):
+        eng.step(1)
+        orc.step(1)
+        st = eng.stats()
+        it, res, status = orc.ppe()
+        assert status == 0 and st["ppe_status"] == 0
+        assert st["ppe_iters"] == it, (step, st["ppe_iters"], it)
+        assert st["ppe_rel_residual"] <= 1e-6
+    bad = []
+    for which, fields in ((SPH, FIELDS_S), (DEM, FIELDS_D)):
+        ie, io = _ids(eng, which), _ids(orc, which)
+        for f in fields:
+            e = rel_l2(by_id(ie, eng.get(which, f)), by_id(io, orc.get(which, f)))
+            if not e <= 1e-7:
+                bad.append((which, f, e))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("mode", [PPE_KRYLOV, PPE_PCG])
+def test_fp32_krylov_converges_and_tracks_fp64(mode):
+    p, sph, dem = _bed(mode, seed=45)
+    eng = _engine(p, sph, dem, 0)
+    orc = Oracle(p, sph, dem, threads=8)
+    for _ in range(3):
+        eng.step(1)
+        orc.step(1)
+        st = eng.stats()
+        assert st["ppe_status"] == 0 and st["ppe_rel_residual"] <= 1e-6, st
+    e = rel_l2(by_id(_ids(eng, SPH), eng.get(SPH, "pres")), by_id(_ids(orc, SPH), orc.get(SPH, "pres")))
+    assert e <= 1e-3, e
+
+
+def test_krylov_reaches_tolerance_where_the_sweep_does_not():
+    """After a step, the one-sweep reference pressure and the converged
+    pressure differ, and the converged one is what the Krylov modes return
+    for every tolerance tightening (fewer than ppe_max_iter iterations)."""
+    p, sph, dem = _bed(PPE_KRYLOV, seed=46)
+    q = p.copy()
+    q.ppe_mode = 0
+    a = _engine(p, sph, dem, 1)
+    b = _engine(q, sph, dem, 1)
+    a.step(1)
+    b.step(1)
+    pa = by_id(_ids(a, SPH), a.get(SPH, "pres"))
+    pb = by_id(_ids(b, SPH), b.get(SPH, "pres"))
+    assert rel_l2(pa, pb) > 1e-4
+    assert 1 < a.stats()["ppe_iters"] < p.ppe_max_iter
+    assert b.stats()["ppe_iters"] == 1
