@@ -1,0 +1,153 @@
+// mlp.cu -- host side of the learned PPE warm start network
+// (mlp_tcgen05.cuh): device buffers, launches, and the C-ABI entry points
+// that run the network on caller-owned device arrays.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/sphdem.h"
+#include "mlp.h"
+#include "mlp_tcgen05.cuh"
+
+namespace sphdem {
+
+static int num_sms() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(n, 1);
+}
+
+int mlp_alloc(MlpNet& m) {
+    std::memset(&m, 0, sizeof(m));
+    m.nparts = num_sms();
+    auto al = [&](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess; };
+    bool ok = al((void**)&m.W1, sizeof(__nv_bfloat16) * MLP_H * MLP_IN) &&
+              al((void**)&m.W2, sizeof(__nv_bfloat16) * MLP_H * MLP_H) &&
+              al((void**)&m.W2T, sizeof(__nv_bfloat16) * MLP_H * MLP_H) &&
+              al((void**)&m.b1, sizeof(float) * MLP_H) && al((void**)&m.b2, sizeof(float) * MLP_H) &&
+              al((void**)&m.w3, sizeof(float) * MLP_H) && al((void**)&m.b3, sizeof(float)) &&
+              al((void**)&m.master, sizeof(float) * MLP_NPARAM) && al((void**)&m.mom, sizeof(float) * MLP_NPARAM) &&
+              al((void**)&m.vel, sizeof(float) * MLP_NPARAM) &&
+              al((void**)&m.part, sizeof(float) * MLP_PART * (size_t)m.nparts) &&
+              al((void**)&m.loss, sizeof(float) * 2) && al((void**)&m.err, sizeof(int));
+    if (!ok) {
+        mlp_free(m);
+        return SPHDEM_E_NOMEM;
+    }
+    cudaMemset(m.mom, 0, sizeof(float) * MLP_NPARAM);
+    cudaMemset(m.vel, 0, sizeof(float) * MLP_NPARAM);
+    cudaMemset(m.err, 0, sizeof(int));
+    cudaMemset(m.loss, 0, sizeof(float) * 2);
+    if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_TRAIN_END + SM_ALIGN) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_INFER_END + SM_ALIGN) !=
+            cudaSuccess)
+        return SPHDEM_E_CUDA;
+    return SPHDEM_OK;
+}
+
+void mlp_free(MlpNet& m) {
+    void* ps[] = {m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3, m.master, m.mom, m.vel, m.part, m.loss, m.err};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    std::memset(&m, 0, sizeof(m));
+}
+
+static MlpDev dev_view(const MlpNet& m) { return MlpDev{m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3}; }
+static MlpOpt opt_view(const MlpNet& m) {
+    return MlpOpt{m.master, m.mom, m.vel, m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3, m.loss};
+}
+
+// master <- params (device FP32, MLP_NPARAM), refresh the BF16 copies
+int mlp_set_params(MlpNet& m, const float* params_dev, cudaStream_t st) {
+    if (cudaMemcpyAsync(m.master, params_dev, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToDevice, st) !=
+        cudaSuccess)
+        return SPHDEM_E_CUDA;
+    k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(0, m.part, opt_view(m), 0.f, 0.f, 0.f, 0.f, 1, 0);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st) {
+    if (n <= 0) return SPHDEM_OK;
+    int tiles = (n + MLP_TILE - 1) / MLP_TILE;
+    int grid = std::min(tiles, m.nparts);
+    k_mlp_infer<<<grid, 128, SM_INFER_END + SM_ALIGN, st>>>(n, (const __nv_bfloat16*)feat, dev_view(m), out, m.err);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+// partial gradients of the weighted MSE into m.part (one row per CTA; rows
+// of CTAs that did not run are zeroed so the sum stays over m.nparts rows)
+int mlp_grad(const MlpNet& m, const void* feat, const float* target, const float* weight, int n, float inv_wsum,
+             cudaStream_t st) {
+    if (cudaMemsetAsync(m.part, 0, sizeof(float) * MLP_PART * (size_t)m.nparts, st) != cudaSuccess)
+        return SPHDEM_E_CUDA;
+    if (n <= 0) return SPHDEM_OK;
+    int tiles = (n + MLP_TILE - 1) / MLP_TILE;
+    int grid = std::min(tiles, m.nparts);
+    k_mlp_grad<<<grid, 128, SM_TRAIN_END + SM_ALIGN, st>>>(n, (const __nv_bfloat16*)feat, target, weight, inv_wsum,
+                                                            dev_view(m), m.part, m.err);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+// one Adam step with the gradient in m.part (t = step number from 1)
+int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st) {
+    k_mlp_adam<<<(MLP_NPARAM + 2 + 255) / 256, 256, 0, st>>>(m.nparts, m.part, opt_view(m), lr, 0.9f, 0.999f, 1e-8f,
+                                                            t, 1);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+// gradient sum (MLP_NPARAM) + [sum w e^2, sum w] into out (device)
+__global__ void k_mlp_sum(int nparts, const float* __restrict__ part, float* out) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < MLP_NPARAM + 2; p += gridDim.x * blockDim.x) {
+        float g = 0.f;
+        for (int c = 0; c < nparts; c++) g += part[(size_t)c * MLP_PART + p];
+        out[p] = g;
+    }
+}
+
+}  // namespace sphdem
+
+using namespace sphdem;
+
+static int mlp_oneshot(const float* params, void* stream, MlpNet& m) {
+    int r = mlp_alloc(m);
+    if (r) return r;
+    return mlp_set_params(m, params, (cudaStream_t)stream);
+}
+
+extern "C" int sphdem_mlp_forward(const void* feat, int32_t n, const float* params, float* out, void* stream) {
+    if (!feat || !params || !out || n < 0) return SPHDEM_E_ARG;
+    MlpNet m;
+    cudaStream_t st = (cudaStream_t)stream;
+    int r = mlp_oneshot(params, stream, m);
+    if (!r) r = mlp_forward(m, feat, n, out, st);
+    int err = 0;
+    if (!r && cudaMemcpyAsync(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) r = SPHDEM_E_CUDA;
+    if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = SPHDEM_E_CUDA;
+    if (!r && err) r = SPHDEM_E_TIMEOUT;
+    mlp_free(m);
+    return r;
+}
+
+extern "C" int sphdem_mlp_grad(const void* feat, const float* target, const float* weight, int32_t n,
+                               const float* params, double weight_sum, float* grad, void* stream) {
+    if (!feat || !target || !weight || !params || !grad || n < 0 || !(weight_sum > 0)) return SPHDEM_E_ARG;
+    MlpNet m;
+    cudaStream_t st = (cudaStream_t)stream;
+    int r = mlp_oneshot(params, stream, m);
+    if (!r) r = mlp_grad(m, feat, target, weight, n, (float)(1.0 / weight_sum), st);
+    if (!r) {
+        k_mlp_sum<<<(MLP_NPARAM + 2 + 255) / 256, 256, 0, st>>>(m.nparts, m.part, grad);
+        if (cudaGetLastError() != cudaSuccess) r = SPHDEM_E_CUDA;
+    }
+    int err = 0;
+    if (!r && cudaMemcpyAsync(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) r = SPHDEM_E_CUDA;
+    if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = SPHDEM_E_CUDA;
+    if (!r && err) r = SPHDEM_E_TIMEOUT;
+    mlp_free(m);
+    return r;
+}
+
+extern "C" int32_t sphdem_mlp_param_count(void) { return MLP_NPARAM; }

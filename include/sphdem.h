@@ -265,6 +265,24 @@ int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields,
 int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields,
                       const int32_t* fields, double* const* host_dst);
 
+/* Learned PPE warm start network (engine extension; no reference
+ * counterpart): 16 -> 64 -> 64 -> 1 per-particle MLP with ReLU, BF16
+ * weights and activations, FP32 accumulation, on tcgen05 tensor cores.
+ * Parameters are one flattened FP32 vector of sphdem_mlp_param_count()
+ * values: W1[64][16] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3.
+ * These two entries run the network on caller-owned DEVICE arrays (rows
+ * of 16 BF16 features, row-major) on the given stream and synchronise it:
+ *   forward: out[i] = MLP(feat[i]);
+ *   grad:    grad[0..P) = dL/dparams of L = sum_i w_i (y_i - t_i)^2 /
+ *            weight_sum, grad[P] = sum_i w_i (y_i - t_i)^2, grad[P+1] =
+ *            sum_i w_i. */
+int32_t sphdem_mlp_param_count(void);
+int sphdem_mlp_forward(const void* feat_bf16, int32_t n, const float* params,
+                       float* out, void* stream);
+int sphdem_mlp_grad(const void* feat_bf16, const float* target,
+                    const float* weight, int32_t n, const float* params,
+                    double weight_sum, float* grad, void* stream);
+
 /* Finish the particle upload: bounding box, cell grid, buffer tags
  * (ISPH.cuh:104-113, functions_NNPS.cuh:60-200).  Must be called once
  * after the last sphdem_set_field and before the first step. */

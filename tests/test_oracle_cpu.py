@@ -125,3 +125,31 @@ def test_oracle_krylov_ppe_converges(mode):
         it, res, st = o.ppe()
         assert st == 0 and res <= 1e-8 and it >= 1, (it, res, st)
     assert np.isfinite(o.get(SPH, "pres")).all()
+
+
+def test_mlp_oracle_gradient_by_finite_differences():
+    """The FP64 oracle's backward pass (without BF16 rounding) against
+    central differences of its own loss, every parameter block."""
+    from oracle import mlp_oracle as MO
+
+    rng = np.random.default_rng(3)
+    p = MO.init_params(3)
+    p[MO.OFF_B1:MO.OFF_W2] = 0.1 * rng.standard_normal(MO.N_H)
+    x = rng.standard_normal((64, MO.N_IN))
+    t = rng.standard_normal(64)
+    w = rng.uniform(0.5, 1.0, size=64)
+    ws = w.sum()
+
+    def loss(q):
+        y, _ = MO.forward(q, x, rounding=False)
+        return float((w * (y - t) ** 2).sum() / ws)
+
+    g, _, _ = MO.grad(p, x, t, w, ws, rounding=False)
+    idx = np.concatenate([rng.choice(np.arange(a, b), size=min(8, b - a), replace=False)
+                          for a, b in ((MO.OFF_W1, MO.OFF_B1), (MO.OFF_B1, MO.OFF_W2), (MO.OFF_W2, MO.OFF_B2),
+                                       (MO.OFF_B2, MO.OFF_W3), (MO.OFF_W3, MO.OFF_B3), (MO.OFF_B3, MO.N_PARAM))])
+    for k in idx:
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        fd = (loss(p + e) - loss(p - e)) / 2e-6
+        assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(fd)), (k, fd, g[k])
