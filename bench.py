@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ppe", action="store_true", help="skip the PPE solver comparison")
+    ap.add_argument("--ppe-train", type=int, default=200, help="training steps of the learned warm start")
     return ap.parse_args()
 
 
@@ -372,6 +374,10 @@ def run_engine(args, world, rank, local, pg):
         cpu = {"value": v, "unit": "particle-updates/s", "cores": cores, "kind": "port", "sample": sample}
 
     stats = eng.stats()
+    eng.close()
+    ppe = None
+    if rank == 0 and world == 1 and not args.no_ppe:
+        ppe = ppe_comparison(args)
     line = {
         "metric": "SPH-DEM particle-updates/s on 1 B200 (3-D fluidized bed, ISPH-DEM step)",
         "value": value, "unit": "particle-updates/s", "n_gpus": world, "steps": args.steps,
@@ -387,10 +393,53 @@ def run_engine(args, world, rank, local, pg):
         "clocks": clocks,
         "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "u_max_dem", "overflow_flags", "nan_flag")},
         "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
+        "ppe": ppe,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
+
+
+def ppe_comparison(args):
+    """PPE ms/step and iterations at a relative residual of 1e-6 on the same
+    bed: Jacobi-PCG from the previous pressure (plain), from the previous
+    pressure plus its last change (extrapolated), and from the learned MLP
+    warm start after args.ppe_train training steps.  Times are the in-graph
+    event times of the whole PPE (assembly, features and network included),
+    averaged over 50 steps after the training."""
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import PPE_PCG, WARM_EXTRAPOLATE, WARM_MLP
+
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    out = {"solver": "Jacobi-PCG (FP64 vectors and dots, FP32 operator)", "tol": 1e-6, "kgc": 0,
+           "train_steps": args.ppe_train, "measured_steps": 50}
+    for name, warm in (("plain", 0), ("extrapolated", WARM_EXTRAPOLATE), ("learned", WARM_MLP)):
+        q = p.copy()
+        q.precision = 0
+        q.ppe_mode = PPE_PCG
+        q.kgc_solve = 0
+        q.ppe_tol = 1e-6
+        q.ppe_max_iter = 2000
+        q.warm_start = warm
+        q.mlp_train_steps = args.ppe_train
+        eng = Engine(q, sph, dem)
+        eng.step(args.ppe_train)
+        eng.set_timing(True)
+        its, st = [], 0
+        for _ in range(50):
+            eng.step(1)
+            eng.collect_timing()
+            s = eng.stats()
+            its.append(s["ppe_iters"])
+            st = max(st, s["ppe_status"])
+        t = eng.timing()["ppe"]
+        out[name] = {"ppe_ms_per_step": t[0] / max(t[1], 1), "iters_per_step": float(np.mean(its)),
+                     "converged": st == 0}
+        if warm == WARM_MLP:
+            out[name]["train_loss"] = s["mlp_loss"]
+        eng.close()
+    out["learned_speedup_vs_plain"] = out["plain"]["ppe_ms_per_step"] / out["learned"]["ppe_ms_per_step"]
+    return out
 
 
 def main():

@@ -15,6 +15,7 @@
 
 #include "handle.h"
 #include "ppe_krylov.cuh"
+#include "mlp.h"
 
 using namespace sphdem;
 
@@ -87,6 +88,9 @@ template <typename R>
 struct EngineHost {
     Engine<R> E;
     KryWork<R> K{};          // PPE solver state (allocated for the Krylov modes)
+    MlpNet net{};            // learned warm start (warm_start = WARM_MLP)
+    bool has_mlp = false;
+    int mlp_trained = 0;     // training steps taken
     Alloc A;
     int nb_cap = 0;
     size_t list_elems = 0;
@@ -97,7 +101,7 @@ void alloc_sph_state(Alloc& A, SphState<R>& S, int n) {
     S.x = A.get<double>(n); S.y = A.get<double>(n); S.z = A.get<double>(n); S.h = A.get<double>(n);
     S.ux = A.get<R>(n); S.uy = A.get<R>(n); S.uz = A.get<R>(n);
     S.m = A.get<R>(n); S.rho = A.get<R>(n); S.pres = A.get<R>(n); S.temp = A.get<R>(n);
-    S.dDEMpor = A.get<R>(n); S.flt_s = A.get<R>(n);
+    S.dDEMpor = A.get<R>(n); S.flt_s = A.get<R>(n); S.dpres = A.get<R>(n);
     S.ptype = A.get<int>(n); S.btype = A.get<int>(n); S.itype = A.get<int>(n); S.pid = A.get<int>(n);
 }
 
@@ -285,6 +289,47 @@ static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cud
     }
 }
 
+// learned warm start, before the solve: statistics (training steps),
+// normalised features, and in use the network's initial iterate
+template <typename R>
+static int mlp_before_solve(SphdemHandle* H, EngineHost<R>* EH, int phase) {
+    KryWork<R>& K = EH->K;
+    int n = EH->E.P.ns;
+    cudaStream_t st = H->stream;
+    if (phase == 1) {
+        k_mlp_stats<R><<<KRY_G, KRY_T, 0, st>>>(n, K, 0);
+        k_mlp_stats_final<R><<<1, KRY_T, 0, st>>>(KRY_G, K, 0);
+    }
+    k_mlp_norm<R><<<nblocks(n * MLP_FEAT, 256), 256, 0, st>>>(n, K);
+    if (phase == 2) {
+        int r = mlp_forward(EH->net, K.feat, n, K.yp, st);
+        if (r) return r;
+        k_mlp_x0<R><<<nblocks(n, 256), 256, 0, st>>>(n, K);
+    }
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+// learned warm start, after the solve (training steps): pressure scale,
+// targets = scaled pressure change, mlp_updates Adam steps
+template <typename R>
+static int mlp_after_solve(SphdemHandle* H, EngineHost<R>* EH) {
+    KryWork<R>& K = EH->K;
+    int n = EH->E.P.ns;
+    cudaStream_t st = H->stream;
+    k_mlp_stats<R><<<KRY_G, KRY_T, 0, st>>>(n, K, 1);
+    k_mlp_stats_final<R><<<1, KRY_T, 0, st>>>(KRY_G, K, 1);
+    k_mlp_targets<R><<<nblocks(n, 256), 256, 0, st>>>(n, K);
+    CK(cudaGetLastError());
+    for (int u = 0; u < std::max(H->p.mlp_updates, 1); u++) {
+        int r = mlp_grad(EH->net, K.feat, K.target, K.weight, n, 1.0f, st);
+        if (r) return r;
+        k_mlp_tick<<<1, 1, 0, st>>>(K.mstat);
+        if ((r = mlp_adam(EH->net, (float)H->p.mlp_lr, 1, st, K.mstat + MS_T))) return r;
+    }
+    return SPHDEM_OK;
+}
+
 template <typename R>
 static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, SphWork<R>& W) {
     KryWork<R>& K = EH->K;
@@ -292,8 +337,13 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
     cudaStream_t st = H->stream;
     int n = P.ns;
     int cg = H->p.ppe_mode == SPHDEM_PPE_PCG;
+    int phase = H->mlp_phase;
     CK(cudaMemsetAsync(K.sc + KS_DONE, 0, sizeof(double), st));
-    k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, (const R*)nullptr);
+    k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, H->p.warm_start == SPHDEM_WARM_EXTRAPOLATE);
+    if (phase) {
+        int r = mlp_before_solve<R>(H, EH, phase);
+        if (r) return r;
+    }
     k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
     k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
     k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);
@@ -334,6 +384,10 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
             CK(cudaStreamSynchronize(st));
             if (done != 0.0) break;
         }
+    }
+    if (phase == 1) {
+        int r = mlp_after_solve<R>(H, EH);
+        if (r) return r;
     }
     k_kry_final<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K);
     CK(cudaGetLastError());
@@ -424,7 +478,8 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
     int flags = 0;
     if (H->count == 0) flags |= F_COUNT0;
     if (H->time == 0.0) flags |= F_TIME0;
-    int key = flags | (E.cur_s << 8) | (E.cur_d << 9);
+    H->mlp_phase = EH->has_mlp ? (EH->mlp_trained < H->p.mlp_train_steps ? 1 : 2) : 0;
+    int key = flags | (E.cur_s << 8) | (E.cur_d << 9) | (H->mlp_phase << 10);
     int64_t n = 0;
     if (H->use_graphs) {
         auto it = H->graphs.find(key);
@@ -456,6 +511,7 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
     *nl += n;
     E.cur_s ^= 1;
     E.cur_d ^= 1;
+    if (H->mlp_phase == 1) EH->mlp_trained++;
     return SPHDEM_OK;
 }
 
@@ -681,6 +737,20 @@ static int commit_t(SphdemHandle* H) {
             K.part = A.get<double>((size_t)KRY_NPART * KRY_G);
             K.sc = A.get<double>(KS_COUNT);
             if (!A.ok) return SPHDEM_E_NOMEM;
+            if (p.warm_start == SPHDEM_WARM_MLP) {
+                K.fraw = A.get<float>((size_t)ns * MLP_FEAT);
+                K.feat = A.get<__nv_bfloat16>((size_t)ns * MLP_FEAT);
+                K.pprev = A.get<double>(ns);
+                K.yp = A.get<float>(ns);
+                K.target = A.get<float>(ns);
+                K.weight = A.get<float>(ns);
+                K.mpart = A.get<double>((size_t)KRY_G * MPART_W);
+                K.mstat = A.get<double>(MS_COUNT);
+                if (!A.ok) return SPHDEM_E_NOMEM;
+                if ((r = mlp_alloc(EH->net))) return r;
+                if ((r = mlp_init_params(EH->net, (unsigned)p.mlp_seed, st))) return r;
+                EH->has_mlp = true;
+            }
         }
         CK(cudaMemsetAsync(E.flags, 0, sizeof(DevFlags), st));
         CK(cudaStreamSynchronize(st));
@@ -846,6 +916,14 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
         out->ppe_iters = (int32_t)sc[KS_ITER];
         out->ppe_rel_residual = sc[KS_RES];
         out->ppe_status = (int32_t)sc[KS_STATUS];
+        out->ppe_initial_residual = sc[KS_RES0];
+    }
+    if (EH->has_mlp) {
+        float loss[2] = {0, 0};
+        CK(cudaMemcpy(loss, EH->net.loss, sizeof(loss), cudaMemcpyDeviceToHost));
+        out->mlp_loss = loss[1] > 0 ? loss[0] / loss[1] : loss[0];
+        out->mlp_phase = EH->mlp_trained < H->p.mlp_train_steps ? 1 : 2;
+        out->mlp_trained_steps = EH->mlp_trained;
     }
     out->ppe_ms = H->ppe_ms;
     out->overflow_flags = f.overflow;
@@ -858,6 +936,7 @@ static void destroy_t(SphdemHandle* H) {
     EngineHost<R>* EH = (EngineHost<R>*)H->eng;
     if (!EH) return;
     for (void* p : EH->A.ptrs) cudaFree(p);
+    if (EH->has_mlp) mlp_free(EH->net);
     delete EH;
     H->eng = nullptr;
 }
@@ -882,6 +961,12 @@ static int check_supported(const SphdemParams* p) {
     if (p->ppe_mode != SPHDEM_PPE_REFERENCE && p->ppe_mode != SPHDEM_PPE_KRYLOV && p->ppe_mode != SPHDEM_PPE_PCG)
         return SPHDEM_E_UNSUPPORTED;
     if (p->ppe_mode != SPHDEM_PPE_REFERENCE && !(p->ppe_tol > 0)) return SPHDEM_E_ARG;
+    // the reference sweep always starts from the previous pressure
+    if (p->warm_start == SPHDEM_WARM_MLP && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
+    if (p->warm_start != SPHDEM_WARM_PREVIOUS && p->warm_start != SPHDEM_WARM_MLP &&
+        p->warm_start != SPHDEM_WARM_EXTRAPOLATE)
+        return SPHDEM_E_ARG;
+    if (p->warm_start == SPHDEM_WARM_EXTRAPOLATE && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
     if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
     if (!(p->dt > 0) || !(p->kappa > 0) || p->freq_filt <= 0) return SPHDEM_E_ARG;
     return SPHDEM_OK;
@@ -1231,6 +1316,42 @@ static int history_t(SphdemHandle* H, int32_t* ids, double* sp, bool set) {
     }
     CK(cudaStreamSynchronize(st));
     return SPHDEM_OK;
+}
+
+template <typename R>
+static int mlp_state_t(SphdemHandle* H, float* params, double* stats, int32_t* trained, const float* pin,
+                       const double* sin, int32_t tin, bool set) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    if (!EH->has_mlp) return SPHDEM_E_ARG;
+    CK(cudaStreamSynchronize(H->stream));
+    if (set) {
+        int r = mlp_put_params(EH->net, pin, H->stream);
+        if (r) return r;
+        CK(cudaMemcpy(EH->K.mstat, sin, sizeof(double) * MS_COUNT, cudaMemcpyHostToDevice));
+        EH->mlp_trained = tin;
+        CK(cudaStreamSynchronize(H->stream));
+    } else {
+        int r = mlp_get_params(EH->net, params);
+        if (r) return r;
+        CK(cudaMemcpy(stats, EH->K.mstat, sizeof(double) * MS_COUNT, cudaMemcpyDeviceToHost));
+        *trained = EH->mlp_trained;
+    }
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_mlp_state(SphdemHandle* h, float* params, double* stats, int32_t* trained_steps) {
+    if (!h || !h->committed || !params || !stats || !trained_steps) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64
+               ? mlp_state_t<double>(h, params, stats, trained_steps, nullptr, nullptr, 0, false)
+               : mlp_state_t<float>(h, params, stats, trained_steps, nullptr, nullptr, 0, false);
+}
+
+extern "C" int sphdem_set_mlp_state(SphdemHandle* h, const float* params, const double* stats,
+                                    int32_t trained_steps) {
+    if (!h || !h->committed || !params || !stats || trained_steps < 0) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64
+               ? mlp_state_t<double>(h, nullptr, nullptr, nullptr, params, stats, trained_steps, true)
+               : mlp_state_t<float>(h, nullptr, nullptr, nullptr, params, stats, trained_steps, true);
 }
 
 extern "C" int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs) {

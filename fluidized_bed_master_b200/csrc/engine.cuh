@@ -21,6 +21,7 @@ template <typename R>
 struct SphState {
     double *x, *y, *z, *h;
     R *ux, *uy, *uz, *m, *rho, *pres, *temp, *dDEMpor, *flt_s;
+    R* dpres;    // pressure change of the last PPE solve (learned warm start feature)
     int *ptype, *btype, *itype, *pid;
 };
 

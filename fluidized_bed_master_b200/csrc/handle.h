@@ -32,6 +32,7 @@ struct SphdemHandle {
     std::map<int, std::vector<int>> graph_kused;
     int use_graphs = 1;
     bool capturing = false;              // inside the capture of a step graph
+    int mlp_phase = 0;                   // learned warm start of the step being built: 0 off, 1 train, 2 use
     cudaStream_t side = nullptr;         // captures the body of the PPE while node
     int64_t last_launches = 0;
     // per-kernel timing (events recorded inside the step graph)

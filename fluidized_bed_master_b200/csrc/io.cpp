@@ -61,6 +61,10 @@ void sphdem_io_params_default(SphdemParams* p) {
     p->ppe_mode = SPHDEM_PPE_REFERENCE;
     p->warm_start = SPHDEM_WARM_PREVIOUS;
     p->ppe_max_iter = 500;
+    p->mlp_train_steps = 500;
+    p->mlp_updates = 4;
+    p->mlp_seed = 0;
+    p->mlp_lr = 3e-4;
     p->precision = SPHDEM_PREC_FP32;
     p->dem_wall_mask = 7;
     p->kappa = 2.0;

@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -56,8 +57,8 @@ void mlp_free(MlpNet& m) {
 }
 
 static MlpDev dev_view(const MlpNet& m) { return MlpDev{m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3}; }
-static MlpOpt opt_view(const MlpNet& m) {
-    return MlpOpt{m.master, m.mom, m.vel, m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3, m.loss};
+static MlpOpt opt_view(const MlpNet& m, const double* tstep = nullptr) {
+    return MlpOpt{m.master, m.mom, m.vel, m.W1, m.W2, m.W2T, m.b1, m.b2, m.w3, m.b3, m.loss, tstep};
 }
 
 // master <- params (device FP32, MLP_NPARAM), refresh the BF16 copies
@@ -72,7 +73,7 @@ int mlp_set_params(MlpNet& m, const float* params_dev, cudaStream_t st) {
 int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st) {
     if (n <= 0) return SPHDEM_OK;
     int tiles = (n + MLP_TILE - 1) / MLP_TILE;
-    int grid = std::min(tiles, m.nparts);
+    int grid = std::min(tiles, 2 * m.nparts);   // two CTAs per SM overlap their MMA waits
     k_mlp_infer<<<grid, 128, SM_INFER_END + SM_ALIGN, st>>>(n, (const __nv_bfloat16*)feat, dev_view(m), out, m.err);
     return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
 }
@@ -91,10 +92,49 @@ int mlp_grad(const MlpNet& m, const void* feat, const float* target, const float
     return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
 }
 
-// one Adam step with the gradient in m.part (t = step number from 1)
-int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st) {
-    k_mlp_adam<<<(MLP_NPARAM + 2 + 255) / 256, 256, 0, st>>>(m.nparts, m.part, opt_view(m), lr, 0.9f, 0.999f, 1e-8f,
-                                                            t, 1);
+// one Adam step with the gradient in m.part (step number t from 1, or read
+// from the device when tstep is given)
+int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st, const double* tstep) {
+    k_mlp_adam<<<(MLP_NPARAM + 2 + 255) / 256, 256, 0, st>>>(m.nparts, m.part, opt_view(m, tstep), lr, 0.9f, 0.999f,
+                                                            1e-8f, t, 1);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+int mlp_get_params(const MlpNet& m, float* host) {
+    return cudaMemcpy(host, m.master, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost) == cudaSuccess
+               ? SPHDEM_OK
+               : SPHDEM_E_CUDA;
+}
+
+// He initialisation: W ~ N(0, 2/fan_in) for the hidden layers, N(0, 1/64)
+// for the output, biases zero; normals from splitmix64 + Box-Muller
+int mlp_init_params(MlpNet& m, unsigned seed, cudaStream_t st) {
+    std::vector<float> p(MLP_NPARAM, 0.f);
+    uint64_t s = 0x9E3779B97F4A7C15ull * (uint64_t)(seed + 1);
+    auto next = [&]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    };
+    auto normal = [&]() { return std::sqrt(-2.0 * std::log(next())) * std::cos(6.283185307179586 * next()); };
+    for (int q = 0; q < MLP_H * MLP_IN; q++) p[MLP_OFF_W1 + q] = (float)(normal() * std::sqrt(2.0 / MLP_IN));
+    for (int q = 0; q < MLP_H * MLP_H; q++) p[MLP_OFF_W2 + q] = (float)(normal() * std::sqrt(2.0 / MLP_H));
+    for (int q = 0; q < MLP_H; q++) p[MLP_OFF_W3 + q] = (float)(normal() * std::sqrt(1.0 / MLP_H));
+    if (cudaMemcpy(m.master, p.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) != cudaSuccess)
+        return SPHDEM_E_CUDA;
+    cudaMemset(m.mom, 0, sizeof(float) * MLP_NPARAM);
+    cudaMemset(m.vel, 0, sizeof(float) * MLP_NPARAM);
+    k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(0, m.part, opt_view(m), 0.f, 0.f, 0.f, 0.f, 1, 0);
+    return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
+}
+
+// master <- host values, BF16 copies refreshed
+int mlp_put_params(MlpNet& m, const float* host, cudaStream_t st) {
+    if (cudaMemcpy(m.master, host, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) != cudaSuccess)
+        return SPHDEM_E_CUDA;
+    k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(0, m.part, opt_view(m), 0.f, 0.f, 0.f, 0.f, 1, 0);
     return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
 }
 

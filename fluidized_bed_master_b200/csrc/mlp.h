@@ -22,6 +22,9 @@ int mlp_set_params(MlpNet& m, const float* params_dev, cudaStream_t st);
 int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st);
 int mlp_grad(const MlpNet& m, const void* feat, const float* target, const float* weight, int n, float inv_wsum,
              cudaStream_t st);
-int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st);
+int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st, const double* tstep = nullptr);
+int mlp_get_params(const MlpNet& m, float* host);
+int mlp_init_params(MlpNet& m, unsigned seed, cudaStream_t st);
+int mlp_put_params(MlpNet& m, const float* host, cudaStream_t st);
 
 }  // namespace sphdem

@@ -553,7 +553,8 @@ struct MlpOpt {
     float *master, *m, *v;     // MLP_NPARAM each
     __nv_bfloat16 *W1, *W2, *W2T;
     float *b1, *b2, *w3, *b3;
-    float* loss;               // [0] weighted MSE of the last gradient pass
+    float* loss;               // [sum w e^2, sum w] of the last gradient pass
+    const double* tstep;       // Adam step number on the device (nullptr: the argument t)
 };
 
 __global__ void k_mlp_adam(int nparts, const float* __restrict__ part, MlpOpt o, float lr, float beta1,
@@ -572,7 +573,8 @@ __global__ void k_mlp_adam(int nparts, const float* __restrict__ part, MlpOpt o,
             float v = beta2 * o.v[p] + (1.f - beta2) * g * g;
             o.m[p] = m;
             o.v[p] = v;
-            float mh = m / (1.f - powf(beta1, (float)t)), vh = v / (1.f - powf(beta2, (float)t));
+            float tt = o.tstep ? (float)o.tstep[0] : (float)t;
+            float mh = m / (1.f - powf(beta1, tt)), vh = v / (1.f - powf(beta2, tt));
             w -= lr * mh / (sqrtf(vh) + eps);
             o.master[p] = w;
         }

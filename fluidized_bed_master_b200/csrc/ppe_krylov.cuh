@@ -34,7 +34,7 @@ constexpr int KRY_NPART = 8;
 // scalar slots
 enum {
     KS_RHO = 0, KS_RHO_NEW, KS_ALPHA, KS_OMEGA, KS_BNORM, KS_RES, KS_DONE, KS_ITER, KS_RZ, KS_RZ_NEW,
-    KS_TOL, KS_MAXIT, KS_STATUS, KS_COUNT = 16
+    KS_TOL, KS_MAXIT, KS_STATUS, KS_RES0, KS_COUNT = 16
 };
 // partial-sum slots
 enum { KP_RHR = 0, KP_RR, KP_RHV, KP_SS, KP_TS, KP_TT, KP_BB, KP_PQ };
@@ -46,7 +46,19 @@ struct KryWork {
     double *d, *b, *x, *r, *rh, *p, *v, *s, *t, *y, *z;
     double* part;  // KRY_NPART * KRY_G block partials
     double* sc;    // KS_COUNT scalars
+    // learned warm start (nullptr when it is off)
+    float* fraw;           // [n][16] raw features (0 on rows that are not solved)
+    __nv_bfloat16* feat;   // [n][16] normalised features, the network's input
+    double* pprev;         // previous pressure of every row
+    float *yp, *target, *weight;
+    double* mpart;         // block partials of the feature statistics (33 per block)
+    double* mstat;         // mean[16] | var[16] | pressure scale | rows | samples seen | Adam step
 };
+
+// learned warm start statistics slots
+enum { MS_MEAN = 0, MS_VAR = 16, MS_PS = 32, MS_ROWS = 33, MS_SEEN = 34, MS_T = 35, MS_COUNT = 40 };
+constexpr int MLP_FEAT = 16;
+constexpr int MPART_W = 2 * MLP_FEAT + 2;   // sum f | sum f^2 | rows | sum dp^2
 
 // ---- reductions ----------------------------------------------------------
 __device__ __forceinline__ double block_sum(double v, double* sm) {
@@ -82,11 +94,12 @@ __device__ __forceinline__ bool kry_solve_row(const DevParams& P, int it, int pt
 }
 
 // ---- assembly: coefficients, diagonal, right-hand side, initial iterate --
-// Same neighbour terms and source as k_ppe.  x0: the warm start (previous
-// pressure, or the learned prediction when x0 != nullptr).
+// Same neighbour terms and source as k_ppe.  Initial iterate: the previous
+// pressure, plus its last change when extrapolate is set (the learned
+// warm start overwrites it later).
 template <typename R>
 __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S, SphWork<R> W, KryWork<R> K,
-                                                      const R* __restrict__ x0) {
+                                                      int extrapolate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -98,6 +111,12 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
         K.d[i] = 1.0;
         K.b[i] = 0.0;
         K.x[i] = 0.0;
+        if (K.fraw) {
+            float* f = K.fraw + (size_t)i * MLP_FEAT;
+#pragma unroll
+            for (int q = 0; q < MLP_FEAT; q++) f[q] = 0.f;
+            K.pprev[i] = (double)upi.w;
+        }
         return;
     }
     R th = (R)S.h[i];
@@ -112,6 +131,9 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
     int cnt = min(W.ncnt[i], P.nb_cap);
     R bx = 0, by = 0, bz = 0;
     double dsum = 0, bfix = 0;
+    // learned warm start: sum a_ij p_j over all neighbours, neighbour pressures
+    double apsum = 0, pmean = 0, pmin = 1e300, pmax = -1e300;
+    int np = 0;
     const int* __restrict__ nb = W.nbr;
     int k = 0;
     nb_walk<2, NbQ44<R>>(
@@ -145,15 +167,53 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
                 dsum += (double)a;
                 if (kry_solve_row(P, tag_itype(tj), tag_ptype(tj), tag_btype(tj))) acoef = a;
                 else bfix += (double)a * (double)uj.w;
+                double pj = (double)uj.w;
+                apsum += (double)a * pj;
+                pmean += pj;
+                pmin = fmin(pmin, pj);
+                pmax = fmax(pmax, pj);
+                np++;
             }
             K.a[(size_t)k * n + i] = acoef;
             k++;
         });
+    R bdiv = (R)P.rho_gas * (bx + by + bz) / (R)P.sdt;
+    R bpor = (R)P.rho_gas * ((R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
     R bsrc = (R)P.rho_gas * (bx + by + bz + (R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
     K.kcnt[i] = cnt;
     K.d[i] = dsum;
     K.b[i] = (double)bsrc + bfix;
-    K.x[i] = x0 ? (double)x0[i] : (double)upi.w;
+    K.x[i] = (double)upi.w + (extrapolate ? (double)S.dpres[i] : 0.0);
+    if (K.fraw) {
+        // features of the learned warm start: the previous pressure, the
+        // reference's one-sweep update (b_i + sum_j a_ij p_j)/d_i and its
+        // increment, neighbour pressure statistics, the terms of the
+        // right-hand side, density deviation, porosity, neighbour count,
+        // height, the pressure change of the previous solve, wall coupling
+        // and the diagonal's magnitude
+        double pi = (double)upi.w, idg = dsum > 0 ? 1.0 / dsum : 0.0;
+        double jac = dsum > 0 ? ((double)bsrc + apsum) * idg : pi;
+        pmean = np ? pmean / np : pi;
+        if (np == 0) pmin = pmax = pi;
+        float* f = K.fraw + (size_t)i * MLP_FEAT;
+        f[0] = (float)pi;
+        f[1] = (float)jac;
+        f[2] = (float)(jac - pi);
+        f[3] = (float)(pmean - pi);
+        f[4] = (float)(pmin - pi);
+        f[5] = (float)(pmax - pi);
+        f[6] = (float)((double)bsrc * idg);
+        f[7] = (float)((double)bdiv * idg);
+        f[8] = (float)((fi.y - W.rho_ref[i]) / W.rho_ref[i]);
+        f[9] = (float)pori;
+        f[10] = (float)cnt;
+        f[11] = (float)((double)bpor * idg);
+        f[12] = (float)S.z[i];
+        f[13] = (float)S.dpres[i];   // pressure change of the previous solve
+        f[14] = (float)(bfix * idg);
+        f[15] = (float)log10(fmax(dsum, 1e-30));
+        K.pprev[i] = pi;
+    }
 }
 
 // y = A x over the stored coefficients; optional fused dots
@@ -238,6 +298,7 @@ __global__ void __launch_bounds__(KRY_T) k_kry_init_scalars(double* part, double
     sc[KS_RZ] = rhr;
     double res = bn > 0 ? sqrt(rr) / bn : 0.0;
     sc[KS_RES] = res;
+    sc[KS_RES0] = res;
     sc[KS_DONE] = (bn == 0.0 || res <= tol || maxit <= 0) ? 1.0 : 0.0;
     (void)cg;
 }
@@ -373,13 +434,112 @@ __global__ void __launch_bounds__(KRY_T) k_kry_check(double* part, double* sc, c
     if (in_graph) cudaGraphSetConditional(h, done ? 0u : 1u);
 }
 
+// ---- learned warm start: statistics, normalisation, targets ---------------
+// Block partials over the solved rows (kcnt > 0): mode 0 sums the raw
+// features and their squares; mode 1 sums (x - p_prev)^2 of the solution.
+template <typename R>
+__global__ void __launch_bounds__(KRY_T) k_mlp_stats(int n, KryWork<R> K, int mode) {
+    __shared__ double sm[32];
+    double acc[MPART_W];
+#pragma unroll
+    for (int q = 0; q < MPART_W; q++) acc[q] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (K.kcnt[i] == 0) continue;
+        acc[2 * MLP_FEAT] += 1.0;
+        if (mode == 0) {
+            const float* f = K.fraw + (size_t)i * MLP_FEAT;
+#pragma unroll
+            for (int q = 0; q < MLP_FEAT; q++) {
+                double v = f[q];
+                acc[q] += v;
+                acc[MLP_FEAT + q] += v * v;
+            }
+        } else {
+            double dp = K.x[i] - K.pprev[i];
+            acc[2 * MLP_FEAT + 1] += dp * dp;
+        }
+    }
+    for (int q = 0; q < MPART_W; q++) {
+        double t = block_sum(acc[q], sm);
+        if (threadIdx.x == 0) K.mpart[(size_t)blockIdx.x * MPART_W + q] = t;
+    }
+}
+
+// one block: totals in block order, then the running statistics.  Feature
+// mean/variance and the pressure scale are exponential averages (0.9) over
+// training steps; the first training step sets them.
+template <typename R>
+__global__ void __launch_bounds__(KRY_T) k_mlp_stats_final(int nblocks, KryWork<R> K, int mode) {
+    __shared__ double tot[MPART_W];
+    int q = threadIdx.x;
+    if (q < MPART_W) {
+        double t = 0;
+        for (int b = 0; b < nblocks; b++) t += K.mpart[(size_t)b * MPART_W + q];
+        tot[q] = t;
+    }
+    __syncthreads();
+    double rows = tot[2 * MLP_FEAT];
+    double* M = K.mstat;
+    if (q == 0) M[MS_ROWS] = rows;
+    if (rows <= 0) return;
+    if (mode == 0 && q < MLP_FEAT) {
+        double mu = tot[q] / rows, var = fmax(tot[MLP_FEAT + q] / rows - mu * mu, 0.0);
+        bool first = M[MS_SEEN] == 0.0;
+        M[MS_MEAN + q] = first ? mu : 0.9 * M[MS_MEAN + q] + 0.1 * mu;
+        M[MS_VAR + q] = first ? var : 0.9 * M[MS_VAR + q] + 0.1 * var;
+    }
+    if (mode == 1 && q == 0) {
+        double ps = sqrt(tot[2 * MLP_FEAT + 1] / rows);
+        if (!(ps > 0)) ps = 1.0;
+        M[MS_PS] = M[MS_SEEN] == 0.0 ? ps : 0.9 * M[MS_PS] + 0.1 * ps;
+        M[MS_SEEN] += 1.0;
+    }
+}
+
+// normalised BF16 features of every row (zero on rows that are not solved)
+template <typename R>
+__global__ void k_mlp_norm(int n, KryWork<R> K) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * MLP_FEAT) return;
+    int i = q / MLP_FEAT, c = q - i * MLP_FEAT;
+    float v = 0.f;
+    if (K.kcnt[i] > 0) {
+        double sd = sqrt(K.mstat[MS_VAR + c]);
+        v = (float)((K.fraw[q] - K.mstat[MS_MEAN + c]) / (sd > 1e-30 ? sd : 1.0));
+    }
+    K.feat[q] = __float2bfloat16_rn(v);
+}
+
+// initial iterate from the network: p_prev + scale * y on solved rows
+template <typename R>
+__global__ void k_mlp_x0(int n, KryWork<R> K) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || K.kcnt[i] == 0) return;
+    K.x[i] = K.pprev[i] + K.mstat[MS_PS] * (double)K.yp[i];
+}
+
+// training pairs: target = (x - p_prev) / scale, weight = 1 / rows on solved rows
+template <typename R>
+__global__ void k_mlp_targets(int n, KryWork<R> K) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool on = K.kcnt[i] > 0;
+    double rows = K.mstat[MS_ROWS];
+    K.target[i] = on ? (float)((K.x[i] - K.pprev[i]) / K.mstat[MS_PS]) : 0.f;
+    K.weight[i] = (on && rows > 0) ? (float)(1.0 / rows) : 0.f;
+}
+
+__global__ void k_mlp_tick(double* mstat) { mstat[MS_T] += 1.0; }
+
 // p_new = x on solved rows, the current pressure elsewhere
 template <typename R>
 __global__ void __launch_bounds__(128) k_kry_final(DevParams P, SphState<R> S, SphWork<R> W, KryWork<R> K) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.ns) return;
     bool solve = kry_solve_row(P, S.itype[i], S.ptype[i], S.btype[i]);
-    W.p_new[i] = solve ? (R)K.x[i] : W.rec.up[i].w;
+    R pold = W.rec.up[i].w;
+    W.p_new[i] = solve ? (R)K.x[i] : pold;
+    S.dpres[i] = solve ? (R)(K.x[i] - (double)pold) : (R)0;
 }
 
 }  // namespace sphdem

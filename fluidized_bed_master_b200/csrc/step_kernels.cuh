@@ -132,6 +132,7 @@ __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R>
     dst.temp[i] = gsrc.temp[p];
     dst.dDEMpor[i] = src.dDEMpor[p];
     dst.flt_s[i] = src.flt_s[p];
+    dst.dpres[i] = src.dpres[p];
     int pt = src.ptype[p], bt = src.btype[p], it = src.itype[p];
     dst.ptype[i] = pt;
     dst.btype[i] = bt;

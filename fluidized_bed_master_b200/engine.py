@@ -59,6 +59,9 @@ def lib():
     L.sphdem_get_launch_count.argtypes = [vp, P(C.c_int64)]
     L.sphdem_set_fields.argtypes = [vp, C.c_int, C.c_int32, P(C.c_int32), P(P(C.c_double))]
     L.sphdem_get_fields.argtypes = [vp, C.c_int, C.c_int32, P(C.c_int32), P(P(C.c_double))]
+    L.sphdem_get_mlp_state.argtypes = [vp, P(C.c_float), P(C.c_double), P(C.c_int32)]
+    L.sphdem_set_mlp_state.argtypes = [vp, P(C.c_float), P(C.c_double), C.c_int32]
+    L.sphdem_mlp_param_count.restype = C.c_int32
     L.sphdem_destroy.argtypes = [vp]
     L.sphdem_destroy.restype = None
     L.sphdem_strerror.argtypes = [C.c_int]
@@ -194,6 +197,23 @@ class Engine:
         """Fill {name: float64 array} with the current values of several
         real fields at once (sphdem_get_fields)."""
         self._bulk(lib().sphdem_get_fields, which, arrays, "sphdem_get_fields")
+
+    def mlp_state(self):
+        """(params float32, stats float64, trained steps) of the learned warm start."""
+        L = lib()
+        p = np.zeros(L.sphdem_mlp_param_count(), dtype=np.float32)
+        st = np.zeros(40, dtype=np.float64)
+        t = C.c_int32()
+        _chk(L.sphdem_get_mlp_state(self._h, p.ctypes.data_as(C.POINTER(C.c_float)),
+                                    st.ctypes.data_as(C.POINTER(C.c_double)), C.byref(t)), "sphdem_get_mlp_state")
+        return p, st, t.value
+
+    def set_mlp_state(self, params, stats, trained_steps):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        st = np.ascontiguousarray(stats, dtype=np.float64)
+        _chk(lib().sphdem_set_mlp_state(self._h, p.ctypes.data_as(C.POINTER(C.c_float)),
+                                        st.ctypes.data_as(C.POINTER(C.c_double)), int(trained_steps)),
+             "sphdem_set_mlp_state")
 
     def set_history(self, ids, springs):
         ids = np.ascontiguousarray(ids, dtype=np.int32)

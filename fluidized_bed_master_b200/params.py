@@ -17,6 +17,7 @@ _I32 = [
     "turbulence_model", "concn_solve", "min_iteration", "max_iteration",
     "penetration_solve", "switch_ptype", "noslip_bc", "decouple_stride",
     "ppe_mode", "warm_start", "ppe_max_iter", "precision", "dem_wall_mask",
+    "mlp_train_steps", "mlp_updates", "mlp_seed",
 ]
 _F64_A = [
     "kappa", "p_ref", "gamma", "dt", "time", "time_end",
@@ -33,13 +34,13 @@ _F64_B = [
 _F64_C = ["cone_r1", "cone_r2", "cone_h", "wall_rest_n", "wall_rest_s", "wall_mu_s", "wall_mu_rs"]
 
 _fields = [(n, C.c_int32) for n in _I32]
-_fields += [("reserved_i", C.c_int32 * 6)]
+_fields += [("reserved_i", C.c_int32 * 3)]
 _fields += [(n, C.c_double) for n in _F64_A]
 _fields += [("margin", C.c_double * 6)]
 _fields += [(n, C.c_double) for n in _F64_B]
 _fields += [("box_c", C.c_double * 3), ("box_L", C.c_double * 3), ("cone_c", C.c_double * 3)]
 _fields += [(n, C.c_double) for n in _F64_C]
-_fields += [("reserved_d", C.c_double * 8)]
+_fields += [("mlp_lr", C.c_double), ("reserved_d", C.c_double * 7)]
 
 
 class SphdemParams(C.Structure):
@@ -65,13 +66,15 @@ class SphdemStats(C.Structure):
         ("count", C.c_int32), ("ppe_iters", C.c_int32), ("time", C.c_double),
         ("ppe_rel_residual", C.c_double), ("ppe_ms", C.c_double),
         ("overflow_flags", C.c_int32), ("nan_flag", C.c_int32),
-        ("ppe_status", C.c_int32), ("reserved_stats", C.c_int32),
+        ("ppe_status", C.c_int32), ("mlp_phase", C.c_int32), ("mlp_loss", C.c_double),
+        ("mlp_trained_steps", C.c_int32), ("reserved_stats", C.c_int32),
+        ("ppe_initial_residual", C.c_double),
     ]
 
 
 # PPE modes and warm starts (SPHDEM_PPE_*, SPHDEM_WARM_*)
 PPE_REFERENCE, PPE_KRYLOV, PPE_PCG = 0, 1, 2
-WARM_PREVIOUS, WARM_MLP = 0, 1
+WARM_PREVIOUS, WARM_MLP, WARM_EXTRAPOLATE = 0, 1, 2
 
 
 # field ids (enum SphdemField)
@@ -122,6 +125,9 @@ def reference_params():
     p.max_iteration = 10
     p.decouple_stride = 1
     p.ppe_max_iter = 500
+    p.mlp_train_steps = 500
+    p.mlp_updates = 4
+    p.mlp_lr = 3e-4
     p.dem_wall_mask = 7
     p.kappa = 2.0
     p.gamma = 1.0

@@ -63,9 +63,14 @@ extern "C" {
 #define SPHDEM_PPE_KRYLOV    1
 #define SPHDEM_PPE_PCG       2
 
-/* Warm start for the KRYLOV mode: previous pressure or the learned MLP. */
-#define SPHDEM_WARM_PREVIOUS 0
-#define SPHDEM_WARM_MLP      1
+/* Initial iterate of the KRYLOV/PCG modes: the previous pressure, or the
+ * learned MLP (trained on the solver's own solutions during the first
+ * mlp_train_steps steps, which start from the previous pressure; after
+ * that the network predicts the pressure change and the solver still
+ * converges to ppe_tol, so results do not depend on the prediction). */
+#define SPHDEM_WARM_PREVIOUS    0
+#define SPHDEM_WARM_MLP         1
+#define SPHDEM_WARM_EXTRAPOLATE 2   /* previous pressure + its last change */
 
 /* Precision of the non-position fields inside the engine. */
 #define SPHDEM_PREC_FP32 0
@@ -119,7 +124,10 @@ typedef struct SphdemParams {
     int32_t ppe_max_iter;       /* KRYLOV iteration cap                  */
     int32_t precision;          /* SPHDEM_PREC_* (engine extension)      */
     int32_t dem_wall_mask;      /* bit0 cylinder_z, bit1 box_z, bit2 truncated_cone_z */
-    int32_t reserved_i[6];
+    int32_t mlp_train_steps;    /* WARM_MLP: steps that train the network (plain warm start) */
+    int32_t mlp_updates;        /* WARM_MLP: Adam steps per training step */
+    int32_t mlp_seed;           /* WARM_MLP: initialisation seed */
+    int32_t reserved_i[3];
 
     /* -- real switches: vif[] of function_init.cuh:59-100 -- */
     double kappa;               /* vif[0]  */
@@ -167,7 +175,8 @@ typedef struct SphdemParams {
     double box_c[3], box_L[3];              /* functions_DEM_BC.cuh:1503-1509 */
     double cone_c[3], cone_r1, cone_r2, cone_h; /* functions_DEM_BC.cuh:723-725,4237-4243 */
     double wall_rest_n, wall_rest_s, wall_mu_s, wall_mu_rs; /* functions_DEM_BC.cuh:1-5 */
-    double reserved_d[8];
+    double mlp_lr;              /* WARM_MLP: Adam learning rate */
+    double reserved_d[7];
 } SphdemParams;
 
 /* Particle fields addressable through get/set.  Values cross the ABI as
@@ -207,7 +216,11 @@ typedef struct SphdemStats {
     int32_t overflow_flags;     /* bit0 SPH list, bit1 DEM history        */
     int32_t nan_flag;
     int32_t ppe_status;         /* 0 converged, 1 iteration cap, 2 breakdown */
+    int32_t mlp_phase;          /* learned warm start: 0 off, 1 training, 2 in use */
+    double  mlp_loss;           /* MSE of the last training pass (scaled pressure change) */
+    int32_t mlp_trained_steps;  /* training steps taken */
     int32_t reserved_stats;
+    double  ppe_initial_residual;  /* ||b - A x0|| / ||b|| of the last solve's initial iterate */
 } SphdemStats;
 
 typedef struct SphdemHandle SphdemHandle;
@@ -282,6 +295,17 @@ int sphdem_mlp_forward(const void* feat_bf16, int32_t n, const float* params,
 int sphdem_mlp_grad(const void* feat_bf16, const float* target,
                     const float* weight, int32_t n, const float* params,
                     double weight_sum, float* grad, void* stream);
+
+/* State of the learned warm start of a handle (warm_start = WARM_MLP):
+ * the flattened FP32 parameters (sphdem_mlp_param_count() values), the
+ * feature statistics (SPHDEM_MLP_STATS doubles: feature means[16] and
+ * variances[16], pressure scale, rows, training steps seen, Adam step,
+ * reserved) and the number of training steps taken.  Setting them lets a
+ * trained network move between handles or runs; set trained_steps >=
+ * mlp_train_steps to skip training. */
+#define SPHDEM_MLP_STATS 40
+int sphdem_get_mlp_state(SphdemHandle* h, float* params, double* stats, int32_t* trained_steps);
+int sphdem_set_mlp_state(SphdemHandle* h, const float* params, const double* stats, int32_t trained_steps);
 
 /* Finish the particle upload: bounding box, cell grid, buffer tags
  * (ISPH.cuh:104-113, functions_NNPS.cuh:60-200).  Must be called once

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from fluidized_bed_master_b200.beds import spouted_bed
-from fluidized_bed_master_b200.params import DEM, PPE_KRYLOV, PPE_PCG, SPH
+from fluidized_bed_master_b200.params import DEM, PPE_KRYLOV, PPE_PCG, SPH, WARM_EXTRAPOLATE, WARM_MLP
 from oracle import Oracle
 from tests.helpers import by_id, rel_l2
 
@@ -99,3 +99,78 @@ def test_krylov_reaches_tolerance_where_the_sweep_does_not():
     assert rel_l2(pa, pb) > 1e-4
     assert 1 < a.stats()["ppe_iters"] < p.ppe_max_iter
     assert b.stats()["ppe_iters"] == 1
+
+
+def _box(mode, warm, train=30):
+    from fluidized_bed_master_b200.beds import box_bed
+
+    p, sph, dem = box_bed(n_fluid=30000, n_dem=3000, seed=5)
+    p.ppe_mode = mode
+    p.kgc_solve = 0
+    p.ppe_tol = 1e-6
+    p.ppe_max_iter = 2000
+    p.warm_start = warm
+    p.mlp_train_steps = train
+    p.mlp_updates = 4
+    return p, sph, dem
+
+
+@pytest.mark.parametrize("warm", [WARM_MLP, WARM_EXTRAPOLATE])
+def test_warm_starts_converge_to_the_same_pressure(warm):
+    """Every warm start reaches ppe_tol each step, and the pressure after the
+    run agrees with the plain (previous-pressure) start to the accuracy the
+    tolerance allows (rel. L2 <= 1e-3 after 40 steps)."""
+    p, sph, dem = _box(PPE_PCG, warm)
+    q = p.copy()
+    q.warm_start = 0
+    a = _engine(p, sph, dem, 0)
+    b = _engine(q, sph, dem, 0)
+    phases = set()
+    for _ in range(40):
+        a.step(1)
+        b.step(1)
+        s = a.stats()
+        assert s["ppe_status"] == 0 and s["ppe_rel_residual"] <= 1e-6, s
+        phases.add(s["mlp_phase"])
+    if warm == WARM_MLP:
+        assert phases == {1, 2}, phases
+    e = rel_l2(by_id(_ids(a, SPH), a.get(SPH, "pres")), by_id(_ids(b, SPH), b.get(SPH, "pres")))
+    assert e <= 1e-3, e
+
+
+def test_learned_warm_start_training_and_gain():
+    """Training lowers the network's loss; then, on one and the same state,
+    the learned initial iterate has a smaller initial residual than the
+    previous pressure (the gain the network brings).  Two handles train
+    identically (the run is deterministic); one is then sent back to the
+    training phase, whose initial iterate is the previous pressure."""
+    p, sph, dem = _box(PPE_PCG, WARM_MLP, train=40)
+    a = _engine(p, sph, dem, 0)
+    b = _engine(p, sph, dem, 0)
+    losses = []
+    for _ in range(40):
+        a.step(1)
+        b.step(1)
+        losses.append(a.stats()["mlp_loss"])
+    assert a.stats()["mlp_trained_steps"] == 40
+    assert min(losses[-10:]) < 0.5 * losses[0], losses
+    assert np.array_equal(a.get(SPH, "pres"), b.get(SPH, "pres"))
+    params, stats, trained = b.mlp_state()
+    b.set_mlp_state(params, stats, 0)
+    a.step(1)
+    b.step(1)
+    sa, sb = a.stats(), b.stats()
+    assert sa["mlp_phase"] == 2 and sa["ppe_status"] == 0 and sb["ppe_status"] == 0
+    assert sa["ppe_initial_residual"] < sb["ppe_initial_residual"], (sa, sb)
+
+
+def test_mlp_state_roundtrip():
+    p, sph, dem = _box(PPE_PCG, WARM_MLP, train=5)
+    a = _engine(p, sph, dem, 0)
+    a.step(5)
+    params, stats, trained = a.mlp_state()
+    assert trained == 5 and np.isfinite(params).all() and stats[32] > 0
+    b = _engine(p, sph, dem, 0)
+    b.set_mlp_state(params, stats, trained)
+    p2, s2, t2 = b.mlp_state()
+    assert np.array_equal(p2, params) and np.array_equal(s2, stats) and t2 == trained
