@@ -31,12 +31,13 @@ static const int TPB = 128;
 enum {
     KT_HASH_S, KT_SORT_S, KT_GATHER_S, KT_HASH_D, KT_SORT_D, KT_GATHER_D, KT_LIST, KT_PASSA, KT_DEMPREP, KT_PASSB,
     KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
-    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_COUNT
+    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN, KT_COUNT
 };
 static const char* KT_NAMES[KT_COUNT] = {
     "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
-    "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem"};
+    "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem",
+    "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training"};
 
 // Event records inside a captured step graph must be external event
 // nodes (cudaEventRecordExternal); a plain record during capture only
@@ -57,9 +58,12 @@ struct KTimer {
             H->ev_used[k] = 1;
         }
     }
-    ~KTimer() {
-        if (H->timing) record_event(H->ev_end[k], H->stream);
+    void stop() {
+        if (H->timing && !stopped) record_event(H->ev_end[k], H->stream);
+        stopped = true;
     }
+    ~KTimer() { stop(); }
+    bool stopped = false;
 };
 #define KTIME(k) KTimer kt_##__LINE__(H, k)
 
@@ -304,7 +308,17 @@ static int mlp_before_solve(SphdemHandle* H, EngineHost<R>* EH, int phase) {
     if (phase == 2) {
         int r = mlp_forward(EH->net, K.feat, n, K.yp, st);
         if (r) return r;
-        k_mlp_x0<R><<<nblocks(n, 256), 256, 0, st>>>(n, K);
+        // x0 = p_prev + sum_k c_k d_k, c from the minimal-residual fit
+        // (directions in p, s, t; their images under A in v, rh, z)
+        const int* nb = EH->E.sw.nbr;
+        k_blend_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, EH->E.S[1 - EH->E.cur_s].dpres, K.p, K.s, K.t);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.pprev, K.y, K.pprev, KP_SS, nullptr, 0, 0);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.p, K.v, K.p, KP_SS, nullptr, 0, 0);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.s, K.rh, K.s, KP_SS, nullptr, 0, 0);
+        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.t, K.z, K.t, KP_SS, nullptr, 0, 0);
+        k_blend_dots<<<KRY_G, KRY_T, 0, st>>>(n, K.b, K.y, K.v, K.rh, K.z, K.part);
+        k_blend_solve<<<1, KRY_T, 0, st>>>(K.part, K.sc);
+        k_blend_apply<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, K.p, K.s, K.t);
     }
     CK(cudaGetLastError());
     return SPHDEM_OK;
@@ -339,11 +353,16 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
     int cg = H->p.ppe_mode == SPHDEM_PPE_PCG;
     int phase = H->mlp_phase;
     CK(cudaMemsetAsync(K.sc + KS_DONE, 0, sizeof(double), st));
-    k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, H->p.warm_start == SPHDEM_WARM_EXTRAPOLATE);
+    {
+        KTIME(KT_PPE_ASM);
+        k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, H->p.warm_start == SPHDEM_WARM_EXTRAPOLATE);
+    }
     if (phase) {
+        KTIME(KT_PPE_WARM);
         int r = mlp_before_solve<R>(H, EH, phase);
         if (r) return r;
     }
+    KTimer kt_solve(H, KT_PPE_SOLVE);
     k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
     k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
     k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);
@@ -385,7 +404,9 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
             if (done != 0.0) break;
         }
     }
+    kt_solve.stop();
     if (phase == 1) {
+        KTIME(KT_PPE_TRAIN);
         int r = mlp_after_solve<R>(H, EH);
         if (r) return r;
     }

@@ -29,12 +29,12 @@ namespace sphdem {
 
 constexpr int KRY_G = 592;   // blocks of the vector kernels (4 per SM)
 constexpr int KRY_T = 256;
-constexpr int KRY_NPART = 8;
+constexpr int KRY_NPART = 10;
 
 // scalar slots
 enum {
     KS_RHO = 0, KS_RHO_NEW, KS_ALPHA, KS_OMEGA, KS_BNORM, KS_RES, KS_DONE, KS_ITER, KS_RZ, KS_RZ_NEW,
-    KS_TOL, KS_MAXIT, KS_STATUS, KS_RES0, KS_COUNT = 16
+    KS_TOL, KS_MAXIT, KS_STATUS, KS_RES0, KS_C0, KS_C1, KS_C2, KS_COUNT = 24
 };
 // partial-sum slots
 enum { KP_RHR = 0, KP_RR, KP_RHV, KP_SS, KP_TS, KP_TT, KP_BB, KP_PQ };
@@ -530,6 +530,87 @@ __global__ void k_mlp_targets(int n, KryWork<R> K) {
 }
 
 __global__ void k_mlp_tick(double* mstat) { mstat[MS_T] += 1.0; }
+
+// ---- minimal-residual blend of the initial iterate ---------------------------
+// x0 = p_prev + sum_k c_k d_k with the directions d0 = the network's
+// predicted change (scale * y), d1 = the last pressure change, d2 = the
+// one-sweep increment; c minimises ||r0 - sum_k c_k A d_k|| with
+// r0 = b - A p_prev, so x0 is never worse (in residual) than p_prev.
+constexpr int BLEND_N = 3;
+template <typename R>
+__global__ void k_blend_dirs(int n, KryWork<R> K, const R* __restrict__ dpres, double* d0, double* d1, double* d2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool on = K.kcnt[i] > 0;
+    d0[i] = on ? K.mstat[MS_PS] * (double)K.yp[i] : 0.0;
+    d1[i] = on ? (double)dpres[i] : 0.0;
+    d2[i] = on ? (double)K.fraw[(size_t)i * MLP_FEAT + 2] : 0.0;
+}
+// r0 = b - A p_prev (A p_prev in y); block partials of (Ad_k, Ad_l), (Ad_k, r0)
+__global__ void __launch_bounds__(KRY_T) k_blend_dots(int n, const double* __restrict__ b, const double* __restrict__ y,
+                                                      const double* __restrict__ a0, const double* __restrict__ a1,
+                                                      const double* __restrict__ a2, double* part) {
+    __shared__ double sm[32];
+    double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double r0 = b[i] - y[i], u0 = a0[i], u1 = a1[i], u2 = a2[i];
+        g[0] += u0 * u0; g[1] += u0 * u1; g[2] += u0 * u2;
+        g[3] += u1 * u1; g[4] += u1 * u2; g[5] += u2 * u2;
+        g[6] += u0 * r0; g[7] += u1 * r0; g[8] += u2 * r0;
+    }
+    for (int q = 0; q < 9; q++) {
+        double t = block_sum(g[q], sm);
+        if (threadIdx.x == 0) part[q * KRY_G + blockIdx.x] = t;
+    }
+}
+// one block: totals, then the 3x3 least-squares solve (Gaussian elimination
+// with a relative Tikhonov floor on the diagonal); c = 0 for a degenerate set
+__global__ void __launch_bounds__(KRY_T) k_blend_solve(const double* part, double* sc) {
+    __shared__ double sm[32];
+    __shared__ double g[9];
+    for (int q = 0; q < 9; q++) {
+        double t = part_total(part, q, sm);
+        if (threadIdx.x == 0) g[q] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double A[3][4] = {{g[0], g[1], g[2], g[6]}, {g[1], g[3], g[4], g[7]}, {g[2], g[4], g[5], g[8]}};
+    double tr = g[0] + g[3] + g[5];
+    double c[3] = {0, 0, 0};
+    if (tr > 0 && isfinite(tr)) {
+        for (int k = 0; k < 3; k++) A[k][k] += 1e-12 * tr;
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; k++) {
+            int piv = k;
+            for (int r = k + 1; r < 3; r++)
+                if (fabs(A[r][k]) > fabs(A[piv][k])) piv = r;
+            if (!(fabs(A[piv][k]) > 0)) { ok = false; break; }
+            for (int q = 0; q < 4; q++) { double t = A[k][q]; A[k][q] = A[piv][q]; A[piv][q] = t; }
+            for (int r = k + 1; r < 3; r++) {
+                double f = A[r][k] / A[k][k];
+                for (int q = k; q < 4; q++) A[r][q] -= f * A[k][q];
+            }
+        }
+        if (ok) {
+            for (int k = 2; k >= 0; k--) {
+                double t = A[k][3];
+                for (int q = k + 1; q < 3; q++) t -= A[k][q] * c[q];
+                c[k] = t / A[k][k];
+            }
+            if (!(isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2]))) c[0] = c[1] = c[2] = 0;
+        }
+    }
+    sc[KS_C0] = c[0];
+    sc[KS_C1] = c[1];
+    sc[KS_C2] = c[2];
+}
+template <typename R>
+__global__ void k_blend_apply(int n, KryWork<R> K, const double* __restrict__ d0, const double* __restrict__ d1,
+                              const double* __restrict__ d2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || K.kcnt[i] == 0) return;
+    K.x[i] = K.pprev[i] + K.sc[KS_C0] * d0[i] + K.sc[KS_C1] * d1[i] + K.sc[KS_C2] * d2[i];
+}
 
 // p_new = x on solved rows, the current pressure elsewhere
 template <typename R>
