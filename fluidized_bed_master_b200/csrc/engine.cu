@@ -255,12 +255,14 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
         KTIME(KT_GATHER_D);
         k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str,
                                                                 DW.g_end);
+        k_gather_history<<<nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st>>>(n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
+                                                                         E.D[dst].hds);
     }
     {
         KTIME(KT_ROWS_D);
         k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, DW.g_str, DW.g_end, DW.rows);
     }
-    *nl += 4;
+    *nl += 5;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -451,7 +453,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 1;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bd, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
+        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
         { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows); }
         *nl += 2;
     }

@@ -163,13 +163,6 @@ __global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst
     dst.Q_sd[i] = src.Q_sd[p];
     dst.ptype[i] = src.ptype[p]; dst.btype[i] = src.btype[p]; dst.itype[i] = src.itype[p];
     dst.pid[i] = src.pid[p]; dst.dem_idx[i] = src.dem_idx[p];
-#pragma unroll
-    for (int s = 0; s < SPHDEM_NSLOT; s++) {
-        dst.hid[s * n + i] = src.hid[s * n + p];
-        dst.hds[(s * 3 + 0) * n + i] = src.hds[(s * 3 + 0) * n + p];
-        dst.hds[(s * 3 + 1) * n + i] = src.hds[(s * 3 + 1) * n + p];
-        dst.hds[(s * 3 + 2) * n + i] = src.hds[(s * 3 + 2) * n + p];
-    }
 }
 
 // SPH neighbour list: the candidate set and predicate of every SPH gather
@@ -334,6 +327,19 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
     W.rho_new[i] = rn;
     W.m_new[i] = mn;
     rec.f1[i] = mk4<R>(mn, rn, S.temp[i], pori);
+}
+
+// contact history permutation, one thread per (slot, sphere): the writes of
+// a slot plane are coalesced
+__global__ void k_gather_history(int n, const int* __restrict__ perm, const int* __restrict__ hid_src,
+                                 const double* __restrict__ hds_src, int* hid_dst, double* hds_dst) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * SPHDEM_NSLOT) return;
+    int s = q / n, i = q - s * n;
+    int p = perm[i];
+    hid_dst[(size_t)s * n + i] = hid_src[(size_t)s * n + p];
+#pragma unroll
+    for (int c = 0; c < 3; c++) hds_dst[(size_t)(s * 3 + c) * n + i] = hds_src[(size_t)(s * 3 + c) * n + p];
 }
 
 // KERNEL_clc_prep3D_coupling_dem: functions_PREP2.cuh:3367-3523.
@@ -510,12 +516,22 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D, DemWork<R> DW,
                                                      const int2* __restrict__ drows,
                                                      DevFlags* F) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.nd;
+    // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
+    // in visit order (for_rows_warp) and the pair terms are reduced with
+    // shuffles.  History writes keep the sequential semantics: lookups use
+    // the start-of-step ids, a release clears only the partner's own slot,
+    // and every new contact targets the first slot free at the start of the
+    // step, so the new contact visited last wins that slot.
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];
+    int* sm = s_rows[threadIdx.x >> 5];
+    const int n = P.nd;
     if (i >= n) return;
-    DW.ftx[i] = 0; DW.fty[i] = 0; DW.ftz[i] = 0;
-    DW.tqx[i] = 0; DW.tqy[i] = 0; DW.tqz[i] = 0;
-    DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
+    if (lane == 0) {
+        DW.ftx[i] = 0; DW.fty[i] = 0; DW.ftz[i] = 0;
+        DW.tqx[i] = 0; DW.tqy[i] = 0; DW.tqz[i] = 0;
+        DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
+    }
     if (D.itype[i] != 1 || D.ptype[i] <= 1000) return;
     double xi = D.x[i], yi = D.y[i], zi = D.z[i], radi = D.rad[i];
     R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
@@ -532,14 +548,22 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     R dr2 = ((R)1 / (R)6) * radiR;
     R volm = ((R)4 / (R)3) * (R)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
     int oid[SPHDEM_NSLOT];
+    int free_slot = -1;
 #pragma unroll
-    for (int s = 0; s < SPHDEM_NSLOT; s++) oid[s] = D.hid[s * n + i];
+    for (int s = 0; s < SPHDEM_NSLOT; s++) {
+        oid[s] = D.hid[s * n + i];
+        if (free_slot < 0 && oid[s] < 1) free_slot = s;
+    }
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R tx = 0, ty = 0, tz = 0, tqx = 0, tqy = 0, tqz = 0, dtr = 0, dtc = 0;
     const double kdt = P.dt;
-    bool ovf = false;
-    for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
+    // this lane's last new contact (visit order t) and its spring
+    int new_t = -1, new_id = 0;
+    double new_dx = 0, new_dy = 0, new_dz = 0;
+    int t_visit = lane - 32;
+    for_rows_warp(P, ic, jc, kc, drows, sm, lane, [&](int j) {
+        t_visit += 32;
         if (D.ptype[j] <= 1000) return;
         double xj = D.x[j], yj = D.y[j], zj = D.z[j], radj = D.rad[j];
         double td = pair_dist(xi, yi, zi, xj, yj, zj);
@@ -575,6 +599,10 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
                    (einv * (rhoi * volm) * cpi);
         }
         if (!(td < P.r_contact * radi)) return;
+        int slot = -1;
+#pragma unroll
+        for (int s = 0; s < SPHDEM_NSLOT; s++)
+            if (slot < 0 && oid[s] == demj) slot = s;
         if (td > 0 && ovlp > 0) {
             R tov = (R)ovlp;
             if (P.con) {
@@ -582,20 +610,11 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
                 dtc += -(R)4 * kij * sqrt(((R)2 * tov) * (radij - (R)0.5 * tov)) * (tempi - D.temp[j]) /
                        ((rhoi * volm) * cpi);
             }
-            int slot = -1;
-#pragma unroll
-            for (int s = 0; s < SPHDEM_NSLOT; s++)
-                if (slot < 0 && oid[s] == demj) slot = s;
             double dsx = 0, dsy = 0, dsz = 0;
             if (slot >= 0) {
                 dsx = D.hds[(slot * 3 + 0) * n + i];
                 dsy = D.hds[(slot * 3 + 1) * n + i];
                 dsz = D.hds[(slot * 3 + 2) * n + i];
-            } else {
-#pragma unroll
-                for (int s = 0; s < SPHDEM_NSLOT; s++)
-                    if (slot < 0 && oid[s] < 1) slot = s;
-                if (slot < 0) { ovf = true; slot = 0; }
             }
             R mj = D.m[j];
             R nx = (R)((xj - xi) / td), ny = (R)((yj - yi) / td), nz = (R)((zj - zi) / td);
@@ -649,24 +668,45 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
             tqx += mi * (rcyi * fsz - rczi * fsy);
             tqy += mi * (rczi * fsx - rcxi * fsz);
             tqz += mi * (rcxi * fsy - rcyi * fsx);
-            D.hid[slot * n + i] = demj;
-            D.hds[(slot * 3 + 0) * n + i] = dsx;
-            D.hds[(slot * 3 + 1) * n + i] = dsy;
-            D.hds[(slot * 3 + 2) * n + i] = dsz;
-        } else {
-            int slot = -1;
-#pragma unroll
-            for (int s = 0; s < SPHDEM_NSLOT; s++)
-                if (slot < 0 && oid[s] == demj) slot = s;
             if (slot >= 0) {
-                D.hds[(slot * 3 + 0) * n + i] = 0.0;
-                D.hds[(slot * 3 + 1) * n + i] = 0.0;
-                D.hds[(slot * 3 + 2) * n + i] = 0.0;
-                D.hid[slot * n + i] = 0;
+                // existing partner: its own slot, no other pair touches it
+                D.hid[slot * n + i] = demj;
+                D.hds[(slot * 3 + 0) * n + i] = dsx;
+                D.hds[(slot * 3 + 1) * n + i] = dsy;
+                D.hds[(slot * 3 + 2) * n + i] = dsz;
+            } else {
+                new_t = t_visit;
+                new_id = demj;
+                new_dx = dsx;
+                new_dy = dsy;
+                new_dz = dsz;
             }
+        } else if (slot >= 0) {
+            D.hds[(slot * 3 + 0) * n + i] = 0.0;
+            D.hds[(slot * 3 + 1) * n + i] = 0.0;
+            D.hds[(slot * 3 + 2) * n + i] = 0.0;
+            D.hid[slot * n + i] = 0;
         }
     });
-    if (ovf) atomicOr(&F->overflow, 2);
+    // the new contact visited last takes the first slot free at the start
+    int last_t = new_t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) last_t = max(last_t, __shfl_xor_sync(0xffffffffu, last_t, o));
+    if (last_t >= 0 && new_t == last_t) {
+        int slot = free_slot;
+        if (slot < 0) {
+            atomicOr(&F->overflow, 2);
+            slot = 0;
+        }
+        D.hid[slot * n + i] = new_id;
+        D.hds[(slot * 3 + 0) * n + i] = new_dx;
+        D.hds[(slot * 3 + 1) * n + i] = new_dy;
+        D.hds[(slot * 3 + 2) * n + i] = new_dz;
+    }
+    tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
+    tqx = warp_sum(tqx); tqy = warp_sum(tqy); tqz = warp_sum(tqz);
+    dtr = warp_sum(dtr); dtc = warp_sum(dtc);
+    if (lane != 0) return;
     if (P.fg) tz += -(R)P.g_dem;
     if (P.con) {
         R temp1i = D.temp1[i], temp2i = D.temp2[i], temp3i = D.temp3[i];
