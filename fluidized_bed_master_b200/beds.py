@@ -185,6 +185,66 @@ def scaled_box_bed(n_fluid=2_000_000, n_dem=200_000, seed=0):
     return box_bed(n_fluid=n_fluid, n_dem=n_dem, seed=seed, lx=1.0)
 
 
+def dam_break_2d(dx=5.0e-3, seed=0, tank=(1.6, 1.0), column=(0.4, 0.8), rho0=1000.0, alpha=0.02, g=9.81,
+                 mu=1.0e-3, cfl=0.2, reference_compat=False):
+    """2-D WCSPH dam break: a 0.4 x 0.8 m water column at the left of a
+    1.6 x 1.0 m tank (12,800 fluid particles at dx = 5 mm), three layers of
+    fixed wall particles (p_type 0) under and beside the tank, Wendland C2
+    with h = 1.3 dx, Tait EOS with gamma 7 and c0 = 10 sqrt(2 g H),
+    artificial viscosity, gravity along -y, dt = cfl h / c0.  Continuity
+    density, predictor-corrector; no KGC, delta-SPH or XSPH (switch them on
+    in the returned params).
+
+    Masses are rho0 (h/1.6)^2, the volume the reference's 2-D reference
+    density assumes (rho_ref = m / (h/1.6)^2, functions_PREP2.cuh:1392), so
+    that rho_ref = rho0.  ``reference_compat`` uses the constants the
+    reference hard-wires instead of alpha, g and mu (artificial viscosity
+    0.1, gravity 9.8, viscosity 2e-5 for every p_type).
+    Returns (params, sph, {})."""
+    rng = np.random.default_rng(seed)
+    p = reference_params()
+    p.solver_type = 0
+    p.dim = 2
+    p.open_boundary = 0
+    p.kernel_type = 3
+    p.h_over_dx = 1.3
+    p.kgc_solve = 0
+    p.delSPH_solve = 0
+    p.xsph_solve = 0
+    p.fva_solve = 1
+    p.gamma = 7.0
+    H = column[1]
+    if reference_compat:
+        alpha, g, mu = 0.1, 9.8, 2.0e-5
+    p.soundspeed = 10.0 * np.sqrt(2.0 * g * H)
+    p.rho0_eos = rho0
+    p.rho_gas = rho0
+    p.mu_gas = mu
+    p.g_sph = g
+    p.g_dem = g
+    p.art_visc_alpha = alpha
+    h = 1.3 * dx
+    p.dt = float(cfl * h / p.soundspeed)
+    p.u_limit = 20.0 * p.soundspeed
+    p.freq_filt = 20
+    nfx, nfy = int(round(column[0] / dx)), int(round(column[1] / dx))
+    ntx, nty = int(round(tank[0] / dx)), int(round(tank[1] / dx))
+    ii, jj = np.meshgrid(np.arange(nfx), np.arange(nfy), indexing="ij")
+    fluid = np.stack([(ii.T.ravel() + 0.5) * dx, (jj.T.ravel() + 0.5) * dx], 1)   # x fastest
+    wi, wj = np.meshgrid(np.arange(-3, ntx + 3), np.arange(-3, nty), indexing="ij")
+    wall = (wi < 0) | (wi >= ntx) | (wj < 0)
+    walls = np.stack([(wi.T[wall.T] + 0.5) * dx, (wj.T[wall.T] + 0.5) * dx], 1)
+    pos = np.concatenate([fluid, walls])
+    n = len(pos)
+    pos = pos + rng.uniform(-0.01 * dx, 0.01 * dx, size=(n, 2))
+    ptype = np.concatenate([np.ones(len(fluid), np.int32), np.zeros(len(walls), np.int32)])
+    m = rho0 * (h / 1.6) ** 2
+    sph = dict(x=pos[:, 0], y=pos[:, 1], z=np.zeros(n), ux=np.zeros(n), uy=np.zeros(n), uz=np.zeros(n),
+               m=np.full(n, m), rho=np.full(n, rho0), pres=np.zeros(n), temp=np.full(n, 300.0),
+               h=np.full(n, h), flt_s=np.ones(n), p_type=ptype, rad=np.zeros(n), ri=np.zeros(n))
+    return p, sph, {}
+
+
 # ---------------------------------------------------------------------------
 # reference input formats
 # ---------------------------------------------------------------------------

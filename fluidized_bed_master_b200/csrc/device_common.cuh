@@ -227,12 +227,21 @@ __device__ __forceinline__ float r2_hi(double Rr) { return (float)(Rr * Rr * (1.
 // The three cells (ix-1..ix+1, jy, kz) have consecutive keys, so their
 // particles are one contiguous slot range of the cell-sorted arrays, and
 // visiting the 9 (z,y) rows in order with ascending slots inside each row
-// is the reference's 27-cell (z,y,x) visit order.  rows[c] = {first, end}
-// of that range around cell c (clamped to the grid), built once per step
-// after the cell sort; {0, 0} when the row is empty.  A 27-cell scan is
-// then 9 table loads.
-__device__ __forceinline__ int2 row_range(const int* __restrict__ gs, const int* __restrict__ ge, int NI, int base,
-                                          int ic) {
+// is the reference's 27-cell (z,y,x) visit order.  rows[c] holds the cell
+// boundaries of the row around cell c (clamped to the grid):
+//   [x: first slot of cell ix-1, y: first of ix, z: first of ix+1, w: end),
+// built once per step after the cell sort (empty cells have zero width).
+//
+// Scans skip cells whose box lies farther than the search radius from the
+// particle (rows whose y-z distance already exceeds it, and the end cells
+// of a row whose x distance does).  Cell boxes follow the hash
+// (vmin + c (vmax - vmin)/N); the edge cells of an axis hold every clamped
+// particle, so they extend to infinity.  The skip threshold is the radius
+// squared times (1 + 1e-8), far above the rounding of the box bounds, so a
+// skipped cell cannot hold a particle inside the radius: neighbour sets
+// are unchanged, only candidates that fail the test are not visited.
+__device__ __forceinline__ int4 row_bounds(const int* __restrict__ gs, const int* __restrict__ ge, int NI, int base,
+                                           int ic) {
     int x0 = ic > 0 ? ic - 1 : 0, x1 = ic < NI - 1 ? ic + 1 : NI - 1;
     int lo = -1, hi = 0;
     for (int ix = x0; ix <= x1; ix++) {
@@ -241,39 +250,86 @@ __device__ __forceinline__ int2 row_range(const int* __restrict__ gs, const int*
         if (lo < 0) lo = s;
         hi = ge[base + ix];
     }
-    return lo < 0 ? make_int2(0, 0) : make_int2(lo, hi);
+    if (lo < 0) return make_int4(0, 0, 0, 0);
+    int b1 = lo, b2 = hi;
+    if (ic > 0 && gs[base + ic - 1] != -1) b1 = ge[base + ic - 1];
+    if (ic < NI - 1 && gs[base + ic + 1] != -1) b2 = gs[base + ic + 1];
+    return make_int4(lo, b1, b2, hi);
+}
+
+// distance from v to the slab of cell c on an axis of N cells
+__device__ __forceinline__ double axis_gap(double v, int c, int N, double vmin, double w) {
+    double lo = vmin + c * w, hi = vmin + (c + 1) * w;
+    double g = 0.0;
+    if (c > 0 && v < lo) g = lo - v;
+    if (c < N - 1 && v > hi) g = v - hi;
+    return g;
+}
+
+struct Cull {
+    double x, y, z, thr2;   // particle (or point) and (radius)^2 (1 + 1e-8)
+};
+__device__ __forceinline__ Cull make_cull(double x, double y, double z, double radius) {
+    return Cull{x, y, z, radius * radius * (1.0 + 1e-8)};
+}
+
+// trimmed slot range of row (jy, kz) around cell ic; false if the row is skipped
+__device__ __forceinline__ bool row_range_cull(const DevParams& P, const int4* __restrict__ rows, int ic, int jy,
+                                               int kz, const Cull& C, double gxm2, double gxp2, int& a, int& b) {
+    double wy = (P.ymax - P.ymin) / P.NJ, wz = (P.zmax - P.zmin) / P.NK;
+    double gy = axis_gap(C.y, jy, P.NJ, P.ymin, wy), gz = axis_gap(C.z, kz, P.NK, P.zmin, wz);
+    double dyz = gy * gy + gz * gz;
+    if (dyz > C.thr2) return false;
+    int4 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
+    a = (gxm2 + dyz > C.thr2) ? r.y : r.x;
+    b = (gxp2 + dyz > C.thr2) ? r.z : r.w;
+    return a < b;
+}
+
+__device__ __forceinline__ void x_gaps(const DevParams& P, int ic, const Cull& C, double& gxm2, double& gxp2) {
+    double wx = (P.xmax - P.xmin) / P.NI;
+    double gm = ic > 0 ? axis_gap(C.x, ic - 1, P.NI, P.xmin, wx) : 0.0;
+    double gp = ic < P.NI - 1 ? axis_gap(C.x, ic + 1, P.NI, P.xmin, wx) : 0.0;
+    gxm2 = gm * gm;
+    gxp2 = gp * gp;
 }
 
 template <typename F>
-__device__ __forceinline__ void for_rows(const DevParams& P, int ic, int jc, int kc, const int2* __restrict__ rows,
-                                         F f) {
+__device__ __forceinline__ void for_rows(const DevParams& P, int ic, int jc, int kc, const int4* __restrict__ rows,
+                                         const Cull& C, F f) {
+    double gxm2, gxp2;
+    x_gaps(P, ic, C, gxm2, gxp2);
     for (int z = -1; z <= 1; z++) {
         int kz = kc + z;
         if (kz < 0 || kz > P.NK - 1) continue;
         for (int y = -1; y <= 1; y++) {
             int jy = jc + y;
             if (jy < 0 || jy > P.NJ - 1) continue;
-            int2 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
-            if (r.x < r.y) f(r.x, r.y);
+            int a, b;
+            if (row_range_cull(P, rows, ic, jy, kz, C, gxm2, gxp2, a, b)) f(a, b);
         }
     }
 }
 
-// One warp scanning the 27-cell stencil of one particle: the 9 row ranges
-// are concatenated and lane l takes candidates l, l+32, ... of the
-// concatenation, so no lane idles at the end of each row.  sm is 20 ints
-// of shared memory owned by the warp (row offsets and starts).  The order
-// in which a lane visits its candidates is ascending slot order.
+// One warp scanning the 27-cell stencil of one particle: the 9 (trimmed)
+// row ranges are concatenated and lane l takes candidates l, l+32, ... of
+// the concatenation, so no lane idles at the end of each row.  sm is 20
+// ints of shared memory owned by the warp (row offsets and starts).  Each
+// lane visits its candidates in ascending slot order.
 template <typename F>
-__device__ __forceinline__ void for_rows_warp(const DevParams& P, int ic, int jc, int kc, const int2* __restrict__ rows,
-                                              int* sm, int lane, F f) {
+__device__ __forceinline__ void for_rows_warp(const DevParams& P, int ic, int jc, int kc, const int4* __restrict__ rows,
+                                              const Cull& C, int* sm, int lane, F f) {
     int len = 0, lo = 0;
     if (lane < 9) {
         int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
         if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
-            int2 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
-            lo = r.x;
-            len = r.y - r.x;
+            double gxm2, gxp2;
+            x_gaps(P, ic, C, gxm2, gxp2);
+            int a, b;
+            if (row_range_cull(P, rows, ic, jy, kz, C, gxm2, gxp2, a, b)) {
+                lo = a;
+                len = b - a;
+            }
         }
     }
     // inclusive prefix over lanes 0..8

@@ -16,6 +16,7 @@
 #include "handle.h"
 #include "ppe_krylov.cuh"
 #include "mlp.h"
+#include "wcsph2d.cuh"
 
 using namespace sphdem;
 
@@ -138,7 +139,7 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     W.u_tmpx = A.get<R>(ns); W.u_tmpy = A.get<R>(ns); W.u_tmpz = A.get<R>(ns); W.temp_tmp = A.get<R>(ns);
     W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
     W.g_str = A.get<int>(ncells + 1); W.g_end = A.get<int>(ncells + 1);
-    W.rows = A.get<int2>(ncells);
+    W.rows = A.get<int4>(ncells);
     W.ncnt = A.get<int>(ns);
     W.wall_idx = A.get<int>(ns); W.buf_idx = A.get<int>(ns); W.counters = A.get<int>(4);
     W.nbr = nullptr;
@@ -157,7 +158,7 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     DW.magf = A.get<R>(nd);
     DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = A.get<int>(nd); DW.val_out = A.get<int>(nd);
     DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
-    DW.rows = A.get<int2>(ncells);
+    DW.rows = A.get<int4>(ncells);
 }
 
 int key_bits(int num_cells) {
@@ -237,7 +238,7 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     int n = P.nd;
     CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
     if (n == 0) {
-        CK(cudaMemsetAsync(DW.rows, 0, sizeof(int2) * P.NI * P.NJ * P.NK, st));
+        CK(cudaMemsetAsync(DW.rows, 0, sizeof(int4) * P.NI * P.NJ * P.NK, st));
         return SPHDEM_OK;
     }
     DemState<R>& D = E.D[src];
@@ -965,12 +966,346 @@ static void destroy_t(SphdemHandle* H) {
 }
 
 // ---------------------------------------------------------------------------
+// 2-D WCSPH (solver_type WCSPH, dim 2): wcsph2d.cuh.  Its own state and
+// work arrays behind the same handle (H->kind == 1).
+// ---------------------------------------------------------------------------
+template <typename R>
+struct WEngineHost {
+    DevParams P;
+    WParams Q;
+    WState<R> S[2];
+    int cur = 0;
+    WWork<R> W;
+    DevFlags* flags = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int nb_cap = 0;
+    Alloc A;
+};
+
+template <typename R>
+static void w_alloc_state(Alloc& A, WState<R>& S, int n) {
+    S.x = A.get<double>(n); S.y = A.get<double>(n); S.z = A.get<double>(n); S.h = A.get<double>(n);
+    S.m = A.get<double>(n); S.rho = A.get<double>(n);
+    S.ux = A.get<R>(n); S.uy = A.get<R>(n); S.pres = A.get<R>(n); S.temp = A.get<R>(n); S.flt_s = A.get<R>(n);
+    S.x0 = A.get<double>(n); S.y0 = A.get<double>(n); S.rho0 = A.get<double>(n);
+    S.ux0 = A.get<R>(n); S.uy0 = A.get<R>(n);
+    S.ptype = A.get<int>(n); S.btype = A.get<int>(n); S.itype = A.get<int>(n); S.pid = A.get<int>(n);
+}
+
+// NNPS of the WCSPH state: S[src] -> S[dst] in cell order
+template <typename R>
+static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst) {
+    const DevParams& P = EH->P;
+    WWork<R>& W = EH->W;
+    cudaStream_t st = H->stream;
+    int n = P.ns;
+    WState<R>& S = EH->S[src];
+    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    size_t bytes = EH->sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(EH->sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
+                                       key_bits(P.num_cells), st));
+    CK(cudaMemsetAsync(W.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
+    k_w_gather<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, EH->S[dst], W.key_out, W.val_out, W.g_str, W.g_end);
+    k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, W.g_str, W.g_end, W.rows);
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+// one step of WCSPH_Calc.cuh:15-340 (Lagrangian variant)
+template <typename R>
+static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH) {
+    const DevParams& P = EH->P;
+    const WParams& Q = EH->Q;
+    WWork<R>& W = EH->W;
+    cudaStream_t st = H->stream;
+    int n = P.ns, so = EH->cur, sn = 1 - EH->cur;
+    int bs = nblocks(n, TPB);
+    k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W);
+    int r = w_nnps<R>(H, EH, so, sn);
+    if (r) return r;
+    WState<R>& S = EH->S[sn];
+    k_w_list<R><<<bs, TPB, 0, st>>>(P, S, W.rows, W.nbr, W.ncnt, EH->flags);
+    // gradient_correction() runs for kgc_solve > 0 or Antuono, but only the
+    // KGC case fills Cm, and only KGC reads it (apply_gradient_correction_2D)
+    if (P.kgc == 1) k_w_kgc<R><<<bs, TPB, 0, st>>>(P, S, W);
+    k_w_prep<R><<<bs, TPB, 0, st>>>(P, Q, S, W, EH->flags);
+    k_w_continuity<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
+    k_w_eos<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
+    k_w_interaction<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
+    k_w_corrector<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
+    if (P.xsph) k_w_xsph<R><<<bs, TPB, 0, st>>>(P, S, W);
+    k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W);
+    k_tick<<<1, 1, 0, st>>>(EH->flags);
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int w_run_step(SphdemHandle* H, WEngineHost<R>* EH) {
+    int key = (1 << 16) | EH->cur;
+    if (H->use_graphs) {
+        auto it = H->graphs.find(key);
+        if (it == H->graphs.end()) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
+            H->capturing = true;
+            int r = w_enqueue<R>(H, EH);
+            H->capturing = false;
+            cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
+            if (r) return r;
+            if (ce != cudaSuccess) return SPHDEM_E_CUDA;
+            cudaGraphExec_t ge;
+            CK(cudaGraphInstantiate(&ge, g, 0));
+            cudaGraphDestroy(g);
+            H->graphs[key] = ge;
+            it = H->graphs.find(key);
+        }
+        CK(cudaGraphLaunch(it->second, H->stream));
+    } else {
+        int r = w_enqueue<R>(H, EH);
+        if (r) return r;
+    }
+    EH->cur ^= 1;
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int w_commit_t(SphdemHandle* H) {
+    const SphdemParams& p = H->p;
+    int ns = H->ns;
+    // bounding box and grid as the ISPH engine (function_init.cuh:913-950)
+    std::vector<double> fx = H->have_file_order ? H->file_x : H->stage_d[0][SPHDEM_F_X];
+    std::vector<double> fy = H->have_file_order ? H->file_y : H->stage_d[0][SPHDEM_F_Y];
+    std::vector<double> fz = H->have_file_order ? H->file_z : H->stage_d[0][SPHDEM_F_Z];
+    double h0 = H->have_file_order ? H->file_h0 : H->stage_d[0][SPHDEM_F_H][0];
+    int n = (int)fx.size();
+    if (fz.size() != fx.size()) fz.assign(fx.size(), 0.0);
+    for (double z : fz)
+        if (z != fz[0]) return SPHDEM_E_INPUT;   // 2-D: one z for every particle
+    double mnx = fx[0], mxx = fx[0], mny = fy[0], mxy = fy[0];
+    for (int k = 0; k < n - 1; k++) {
+        mnx = std::min(mnx, fx[k]); mxx = std::max(mxx, fx[k]);
+        mny = std::min(mny, fy[k]); mxy = std::max(mxy, fy[k]);
+    }
+    mnx -= (mxx - mnx) * p.margin[0]; mxx += (mxx - mnx) * p.margin[1];
+    mny -= (mxy - mny) * p.margin[2]; mxy += (mxy - mny) * p.margin[3];
+    double dcell = 1.1 * p.kappa * h0;
+    int NI = (int)((mxx - mnx) / dcell) + 1, NJ = (int)((mxy - mny) / dcell) + 1, NK = 1;
+    if (!(dcell > 0) || (double)NI * NJ > 2.0e9) return SPHDEM_E_INPUT;
+    H->bbox[0] = mnx; H->bbox[1] = mxx; H->bbox[2] = mny; H->bbox[3] = mxy; H->bbox[4] = fz[0]; H->bbox[5] = fz[0];
+    H->nijk[0] = NI; H->nijk[1] = NJ; H->nijk[2] = NK;
+    H->dcell = dcell;
+    auto* EH = new WEngineHost<R>();
+    H->eng = EH;
+    H->kind = 1;
+    DevParams& P = EH->P;
+    std::memset(&P, 0, sizeof(P));
+    P.kernel_type = p.kernel_type; P.dim = 2; P.kgc = p.kgc_solve;
+    P.fp = p.fp_solve; P.fv = p.fv_solve; P.fva = p.fva_solve; P.fg = p.fg_solve; P.xsph = p.xsph_solve;
+    P.NI = NI; P.NJ = NJ; P.NK = NK; P.num_cells = NI * NJ * NK + 1;
+    P.ns = ns;
+    P.kappa = p.kappa; P.dt = p.dt; P.sdt = p.dt; P.soundspeed = p.soundspeed; P.u_limit = p.u_limit;
+    P.c_xsph = p.c_xsph;
+    P.xmin = mnx; P.xmax = mxx; P.ymin = mny; P.ymax = mxy; P.zmin = fz[0]; P.zmax = fz[0];
+    P.mu_gas = p.mu_gas; P.g_sph = p.g_sph;
+    WParams& Q = EH->Q;
+    Q.alpha = p.art_visc_alpha; Q.beta = p.art_visc_beta; Q.delta = p.delta_sph;
+    Q.freq_filt = p.freq_filt; Q.delsph = p.delSPH_solve; Q.rho_cont = p.rho_type == 1;
+    Q.gamma = p.gamma; Q.eos_B = p.soundspeed * p.soundspeed * 1.186 / p.gamma;
+    Alloc& A = EH->A;
+    w_alloc_state<R>(A, EH->S[0], ns);
+    w_alloc_state<R>(A, EH->S[1], ns);
+    WWork<R>& W = EH->W;
+    W.ftx = A.get<R>(ns); W.fty = A.get<R>(ns); W.ftot = A.get<R>(ns); W.drho = A.get<R>(ns);
+    W.rho_ref = A.get<double>(ns); W.grx = A.get<R>(ns); W.gry = A.get<R>(ns); W.pgfx = A.get<R>(ns);
+    W.pgfy = A.get<R>(ns); W.Cm = A.get<R>((size_t)ns * 4);
+    W.xn = A.get<double>(ns); W.yn = A.get<double>(ns); W.rhon = A.get<double>(ns);
+    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
+    W.g_str = A.get<int>(P.num_cells + 1); W.g_end = A.get<int>(P.num_cells + 1);
+    W.rows = A.get<int4>(NI * NJ * NK);
+    W.ncnt = A.get<int>(ns);
+    W.nbr = nullptr;
+    EH->flags = A.get<DevFlags>(1);
+    if (!A.ok) return SPHDEM_E_NOMEM;
+    {
+        size_t b = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b, W.key_in, W.key_out, W.val_in, W.val_out, std::max(ns, 1), 0,
+                                        key_bits(P.num_cells), H->stream);
+        EH->sort_tmp_bytes = b;
+        EH->sort_tmp = A.get<char>(b);
+        if (!A.ok) return SPHDEM_E_NOMEM;
+    }
+    cudaStream_t st = H->stream;
+    auto& pt = H->stage_i[0][SPHDEM_F_PTYPE];
+    for (int v : pt)
+        if (v == 9 || v > 1000) return SPHDEM_E_UNSUPPORTED;   // moving plates, DEM
+    std::vector<int> itype(ns, 1), btype(ns, 0), pid(ns);
+    for (int i = 0; i < ns; i++) pid[i] = i;
+    H->stage_i[0][SPHDEM_F_ITYPE] = itype;
+    H->stage_i[0][SPHDEM_F_BUFFER_TYPE] = btype;
+    H->stage_i[0][SPHDEM_F_PID] = pid;
+    WState<R>& S = EH->S[0];
+    auto up_d = [&](double* dst, int f) -> int {
+        auto& v = H->stage_d[0][f];
+        if ((int)v.size() != ns) v.assign(ns, 0.0);
+        CK(cudaMemcpy(dst, v.data(), sizeof(double) * ns, cudaMemcpyHostToDevice));
+        return SPHDEM_OK;
+    };
+    auto up_r = [&](R* dst, int f) -> int {
+        auto& v = H->stage_d[0][f];
+        if ((int)v.size() != ns) v.assign(ns, 0.0);
+        return upload_real<R>(dst, v.data(), ns, st);
+    };
+    auto up_i = [&](int* dst, int f) -> int {
+        auto& v = H->stage_i[0][f];
+        if ((int)v.size() != ns) v.assign(ns, 0);
+        CK(cudaMemcpy(dst, v.data(), sizeof(int) * ns, cudaMemcpyHostToDevice));
+        return SPHDEM_OK;
+    };
+    int r = 0;
+    r |= up_d(S.x, SPHDEM_F_X); r |= up_d(S.y, SPHDEM_F_Y); r |= up_d(S.z, SPHDEM_F_Z); r |= up_d(S.h, SPHDEM_F_H);
+    r |= up_r(S.ux, SPHDEM_F_UX); r |= up_r(S.uy, SPHDEM_F_UY); r |= up_d(S.m, SPHDEM_F_M);
+    r |= up_d(S.rho, SPHDEM_F_RHO); r |= up_r(S.pres, SPHDEM_F_PRES); r |= up_r(S.temp, SPHDEM_F_TEMP);
+    r |= up_r(S.flt_s, SPHDEM_F_FLT_S);
+    r |= up_i(S.ptype, SPHDEM_F_PTYPE); r |= up_i(S.btype, SPHDEM_F_BUFFER_TYPE); r |= up_i(S.itype, SPHDEM_F_ITYPE);
+    r |= up_i(S.pid, SPHDEM_F_PID);
+    if (r) return SPHDEM_E_CUDA;
+    // neighbour-list capacity from an exact count on the sorted input
+    if ((r = w_nnps<R>(H, EH, 0, 1))) return r;
+    k_w_list<R><<<nblocks(ns, TPB), TPB, 0, st>>>(P, EH->S[1], W.rows, nullptr, W.ncnt, EH->flags);
+    CK(cudaGetLastError());
+    DevFlags f;
+    CK(cudaMemcpyAsync(&f, EH->flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int cap = std::max(32, ((int)(f.max_ncnt * 1.25) + 16 + 7) / 8 * 8);
+    P.nb_cap = cap;
+    EH->nb_cap = cap;
+    W.nbr = A.get<int>((size_t)cap * ns);
+    if (!A.ok) return SPHDEM_E_NOMEM;
+    DevFlags f0;
+    std::memset(&f0, 0, sizeof(f0));
+    f0.step_count = H->count;
+    CK(cudaMemcpy(EH->flags, &f0, sizeof(f0), cudaMemcpyHostToDevice));
+    H->committed = true;
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int w_field_ptr(SphdemHandle* H, int field, const void** ptr, int* kind) {
+    auto* EH = (WEngineHost<R>*)H->eng;
+    WState<R>& S = EH->S[EH->cur];
+    WWork<R>& W = EH->W;
+    switch (field) {
+    case SPHDEM_F_X: *ptr = S.x; *kind = 0; return 0;
+    case SPHDEM_F_Y: *ptr = S.y; *kind = 0; return 0;
+    case SPHDEM_F_Z: *ptr = S.z; *kind = 0; return 0;
+    case SPHDEM_F_H: *ptr = S.h; *kind = 0; return 0;
+    case SPHDEM_F_UX: *ptr = S.ux; *kind = 1; return 0;
+    case SPHDEM_F_UY: *ptr = S.uy; *kind = 1; return 0;
+    case SPHDEM_F_M: *ptr = S.m; *kind = 0; return 0;
+    case SPHDEM_F_RHO: *ptr = S.rho; *kind = 0; return 0;
+    case SPHDEM_F_PRES: *ptr = S.pres; *kind = 1; return 0;
+    case SPHDEM_F_TEMP: *ptr = S.temp; *kind = 1; return 0;
+    case SPHDEM_F_FLT_S: *ptr = S.flt_s; *kind = 1; return 0;
+    case SPHDEM_F_FTOTALX: *ptr = W.ftx; *kind = 1; return 0;
+    case SPHDEM_F_FTOTALY: *ptr = W.fty; *kind = 1; return 0;
+    case SPHDEM_F_PGFX: *ptr = W.pgfx; *kind = 1; return 0;
+    case SPHDEM_F_PGFY: *ptr = W.pgfy; *kind = 1; return 0;
+    case SPHDEM_F_RHO_REF: *ptr = W.rho_ref; *kind = 0; return 0;
+    case SPHDEM_F_FTOTAL: *ptr = W.ftot; *kind = 1; return 0;
+    case SPHDEM_F_DRHO: *ptr = W.drho; *kind = 1; return 0;
+    case SPHDEM_F_GRAD_RHOX: *ptr = W.grx; *kind = 1; return 0;
+    case SPHDEM_F_GRAD_RHOY: *ptr = W.gry; *kind = 1; return 0;
+    case SPHDEM_F_PTYPE: *ptr = S.ptype; *kind = 2; return 0;
+    case SPHDEM_F_ITYPE: *ptr = S.itype; *kind = 2; return 0;
+    case SPHDEM_F_BUFFER_TYPE: *ptr = S.btype; *kind = 2; return 0;
+    case SPHDEM_F_PID: *ptr = S.pid; *kind = 2; return 0;
+    case SPHDEM_F_CELL: *ptr = W.key_out; *kind = 2; return 0;
+    }
+    return -1;
+}
+
+template <typename R>
+static int w_get_field_t(SphdemHandle* H, int field, void* dst, int n) {
+    const void* ptr;
+    int kind;
+    if (w_field_ptr<R>(H, field, &ptr, &kind)) return SPHDEM_E_ARG;
+    if (n == 0) return SPHDEM_OK;
+    CK(cudaStreamSynchronize(H->stream));
+    if (kind == 0) CK(cudaMemcpy(dst, ptr, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    else if (kind == 1) return download_real<R>((double*)dst, (const R*)ptr, n, H->stream);
+    else CK(cudaMemcpy(dst, ptr, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static int w_stats_t(SphdemHandle* H, SphdemStats* out) {
+    auto* EH = (WEngineHost<R>*)H->eng;
+    std::memset(out, 0, sizeof(*out));
+    cudaStream_t st = H->stream;
+    WState<R>& S = EH->S[EH->cur];
+    double* buf = nullptr;
+    CK(cudaMalloc(&buf, sizeof(double) * 4));
+    CK(cudaMemsetAsync(buf, 0, sizeof(double) * 3, st));
+    k_stats<R, double><<<std::min(nblocks(EH->P.ns, 256), 592), 256, 0, st>>>(EH->P.ns, S.rho, S.ux, S.uy, nullptr, EH->W.ftot,
+                                                                     S.ptype, S.itype, buf, EH->flags);
+    double hb[3];
+    CK(cudaMemcpyAsync(hb, buf, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    DevFlags f;
+    CK(cudaMemcpyAsync(&f, EH->flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(buf);
+    out->rho_max_sph = hb[0];
+    out->u_max_sph = hb[1];
+    out->ftotal_max_sph = hb[2];
+    out->count = H->count;
+    out->time = H->time;
+    out->ppe_iters = 0;
+    out->overflow_flags = f.overflow;
+    out->nan_flag = f.nan;
+    return SPHDEM_OK;
+}
+
+template <typename R>
+static void w_destroy_t(SphdemHandle* H) {
+    auto* EH = (WEngineHost<R>*)H->eng;
+    if (!EH) return;
+    for (void* q : EH->A.ptrs) cudaFree(q);
+    delete EH;
+    H->eng = nullptr;
+}
+
+static void engine_destroy(SphdemHandle* h) {
+    if (h->kind == 1) {
+        if (h->prec == SPHDEM_PREC_FP64) w_destroy_t<double>(h); else w_destroy_t<float>(h);
+    } else {
+        if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-static bool is_real_field(int f) { return f >= SPHDEM_F_X && f <= SPHDEM_F_Q_SD; }
+static bool is_real_field(int f) { return f >= SPHDEM_F_X && f <= SPHDEM_F_GRAD_RHOY; }
 static bool is_int_field(int f) { return f >= SPHDEM_F_PTYPE && f <= SPHDEM_F_CELL; }
 
 static int check_supported(const SphdemParams* p) {
+    if (p->solver_type == SPHDEM_WCSPH) {
+        // 2-D WCSPH (SOPHIA_single, WCSPH_Calc.cuh:15-340), Lagrangian variant
+        if (p->dim != 2) return SPHDEM_E_UNSUPPORTED;
+        if (p->prop_table || p->fs_solve || p->fb_solve || p->interface_solve || p->boussinesq_solve ||
+            p->concn_solve || p->pst_solve || p->turbulence_model != 0 || p->penetration_solve || p->noslip_bc ||
+            p->con_solve || p->open_boundary || p->switch_ptype)
+            return SPHDEM_E_UNSUPPORTED;
+        if (p->kgc_solve != 0 && p->kgc_solve != 1) return SPHDEM_E_UNSUPPORTED;
+        if (p->time_type != 1 || p->rho_type != 1) return SPHDEM_E_UNSUPPORTED;   // predictor-corrector, continuity
+        if (p->delSPH_solve < 0 || p->delSPH_solve > 2) return SPHDEM_E_UNSUPPORTED;
+        if (p->ppe_mode != SPHDEM_PPE_REFERENCE || p->warm_start != SPHDEM_WARM_PREVIOUS) return SPHDEM_E_ARG;
+        if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
+        if (!(p->dt > 0) || !(p->kappa > 0) || p->freq_filt <= 0 || !(p->gamma > 0)) return SPHDEM_E_ARG;
+        return SPHDEM_OK;
+    }
     if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
     if (p->dim != 3) return SPHDEM_E_UNSUPPORTED;
     if (p->prop_table || p->fs_solve || p->fb_solve || p->interface_solve || p->boussinesq_solve ||
@@ -1000,6 +1335,7 @@ extern "C" int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem
     *out = nullptr;
     int r = check_supported(p);
     if (r) return r;
+    if (p->solver_type == SPHDEM_WCSPH && (n_dem != 0 || n_sph == 0)) return SPHDEM_E_UNSUPPORTED;
     SphdemHandle* h = new SphdemHandle();
     h->p = *p;
     h->ns = n_sph;
@@ -1158,6 +1494,7 @@ static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, voi
 
 extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
                                  const double* const* host_src) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !fields || !host_src || (which != 0 && which != 1) || nfields < 0 ||
         nfields > SPHDEM_BULK_MAX_FIELDS)
         return SPHDEM_E_ARG;
@@ -1168,6 +1505,7 @@ extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, co
 
 extern "C" int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
                                  double* const* host_dst) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !fields || !host_dst || (which != 0 && which != 1) || nfields < 0 ||
         nfields > SPHDEM_BULK_MAX_FIELDS)
         return SPHDEM_E_ARG;
@@ -1179,6 +1517,7 @@ extern "C" int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields, co
 extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const void* src, size_t bytes) {
     if (!h || !src || (which != 0 && which != 1)) return SPHDEM_E_ARG;
     if (h->committed) {
+        if (h->kind == 1) return SPHDEM_E_UNSUPPORTED;
         int n = which ? h->nd : h->ns;
         if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
         return h->prec == SPHDEM_PREC_FP64 ? set_state_t<double>(h, which, field, src, n)
@@ -1220,11 +1559,11 @@ extern "C" int sphdem_commit_particles(SphdemHandle* h) {
         }
     }
     if (cudaSetDevice(h->device) != cudaSuccess) return SPHDEM_E_CUDA;
-    int r = h->prec == SPHDEM_PREC_FP64 ? commit_t<double>(h) : commit_t<float>(h);
+    const bool w = h->p.solver_type == SPHDEM_WCSPH;
+    int r = w ? (h->prec == SPHDEM_PREC_FP64 ? w_commit_t<double>(h) : w_commit_t<float>(h))
+              : (h->prec == SPHDEM_PREC_FP64 ? commit_t<double>(h) : commit_t<float>(h));
     if (r) {
-        if (h->eng) {
-            if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
-        }
+        if (h->eng) engine_destroy(h);
         return r;
     }
     for (int q = 0; q < 2; q++) { h->stage_d[q].clear(); h->stage_i[q].clear(); }
@@ -1235,7 +1574,12 @@ extern "C" int sphdem_step(SphdemHandle* h, int32_t nsteps) {
     if (!h || !h->committed || nsteps < 0) return SPHDEM_E_ARG;
     int64_t nl = 0;
     for (int k = 0; k < nsteps; k++) {
-        int r = h->prec == SPHDEM_PREC_FP64 ? run_step<double>(h, (EngineHost<double>*)h->eng, &nl)
+        int r;
+        if (h->kind == 1)
+            r = h->prec == SPHDEM_PREC_FP64 ? w_run_step<double>(h, (WEngineHost<double>*)h->eng)
+                                            : w_run_step<float>(h, (WEngineHost<float>*)h->eng);
+        else
+            r = h->prec == SPHDEM_PREC_FP64 ? run_step<double>(h, (EngineHost<double>*)h->eng, &nl)
                                             : run_step<float>(h, (EngineHost<float>*)h->eng, &nl);
         if (r) return r;
         h->time += h->p.dt;   // ISPH_Calc_seperate.cuh:924-925
@@ -1259,12 +1603,17 @@ extern "C" int sphdem_get_field(SphdemHandle* h, int which, int field, void* dst
     }
     size_t need = (is_int_field(field) ? sizeof(int) : sizeof(double)) * (size_t)n;
     if (bytes != need) return SPHDEM_E_ARG;
+    if (h->kind == 1)
+        return which ? SPHDEM_E_ARG
+                     : (h->prec == SPHDEM_PREC_FP64 ? w_get_field_t<double>(h, field, dst, n)
+                                                    : w_get_field_t<float>(h, field, dst, n));
     return h->prec == SPHDEM_PREC_FP64 ? get_field_t<double>(h, which, field, dst, n)
                                        : get_field_t<float>(h, which, field, dst, n);
 }
 
 extern "C" int sphdem_get_stats(SphdemHandle* h, SphdemStats* out) {
     if (!h || !out || !h->committed) return SPHDEM_E_ARG;
+    if (h->kind == 1) return h->prec == SPHDEM_PREC_FP64 ? w_stats_t<double>(h, out) : w_stats_t<float>(h, out);
     return h->prec == SPHDEM_PREC_FP64 ? stats_t<double>(h, out) : stats_t<float>(h, out);
 }
 
@@ -1274,7 +1623,15 @@ extern "C" int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* d
     const int* ncnt;
     const int* nbr;
     int ncap;
-    if (h->prec == SPHDEM_PREC_FP64) {
+    if (h->kind == 1) {
+        if (h->prec == SPHDEM_PREC_FP64) {
+            auto* EH = (WEngineHost<double>*)h->eng;
+            ncnt = EH->W.ncnt; nbr = EH->W.nbr; ncap = EH->nb_cap;
+        } else {
+            auto* EH = (WEngineHost<float>*)h->eng;
+            ncnt = EH->W.ncnt; nbr = EH->W.nbr; ncap = EH->nb_cap;
+        }
+    } else if (h->prec == SPHDEM_PREC_FP64) {
         auto* EH = (EngineHost<double>*)h->eng;
         ncnt = EH->E.sw.ncnt; nbr = EH->E.sw.nbr; ncap = EH->nb_cap;
     } else {
@@ -1363,6 +1720,7 @@ static int mlp_state_t(SphdemHandle* H, float* params, double* stats, int32_t* t
 }
 
 extern "C" int sphdem_get_mlp_state(SphdemHandle* h, float* params, double* stats, int32_t* trained_steps) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !params || !stats || !trained_steps) return SPHDEM_E_ARG;
     return h->prec == SPHDEM_PREC_FP64
                ? mlp_state_t<double>(h, params, stats, trained_steps, nullptr, nullptr, 0, false)
@@ -1371,6 +1729,7 @@ extern "C" int sphdem_get_mlp_state(SphdemHandle* h, float* params, double* stat
 
 extern "C" int sphdem_set_mlp_state(SphdemHandle* h, const float* params, const double* stats,
                                     int32_t trained_steps) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !params || !stats || trained_steps < 0) return SPHDEM_E_ARG;
     return h->prec == SPHDEM_PREC_FP64
                ? mlp_state_t<double>(h, nullptr, nullptr, nullptr, params, stats, trained_steps, true)
@@ -1378,18 +1737,21 @@ extern "C" int sphdem_set_mlp_state(SphdemHandle* h, const float* params, const 
 }
 
 extern "C" int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
     return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, ids, springs, false)
                                        : history_t<float>(h, ids, springs, false);
 }
 
 extern "C" int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* springs) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
     return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, (int32_t*)ids, (double*)springs, true)
                                        : history_t<float>(h, (int32_t*)ids, (double*)springs, true);
 }
 
 extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h) return SPHDEM_E_ARG;
     if (h->ev_beg.empty()) {
         h->ev_beg.resize(KT_COUNT);
@@ -1442,6 +1804,7 @@ extern "C" int sphdem_get_timing(SphdemHandle* h, int k, char* name, int name_ca
 }
 
 extern "C" int sphdem_write_vtk_dem(SphdemHandle* h, const char* path) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !path || !h->committed) return SPHDEM_E_ARG;
     int n = h->nd;
     std::vector<double> x(n), y(n), z(n), magf(n), eliz(n, 1.0), por(n), uz(n), qsd(n), ftz(n), temp(n), rad(n), dtemp(n);
@@ -1477,6 +1840,7 @@ extern "C" int sphdem_write_vtk_dem(SphdemHandle* h, const char* path) {
 }
 
 extern "C" int sphdem_write_restart(SphdemHandle* h, const char* path) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !path || !h->committed) return SPHDEM_E_ARG;
     FILE* f = std::fopen(path, "w");
     if (!f) return SPHDEM_E_INPUT;
@@ -1551,9 +1915,7 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
     for (cudaEvent_t e : h->ev_beg) cudaEventDestroy(e);
     for (cudaEvent_t e : h->ev_end) cudaEventDestroy(e);
-    if (h->eng) {
-        if (h->prec == SPHDEM_PREC_FP64) destroy_t<double>(h); else destroy_t<float>(h);
-    }
+    if (h->eng) engine_destroy(h);
     if (h->xfer) cudaFree(h->xfer);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -58,7 +58,7 @@ struct SphWork {
     R *u_tmpx, *u_tmpy, *u_tmpz, *temp_tmp;
     int *key_in, *key_out, *val_in, *val_out;
     int *g_str, *g_end;
-    int2* rows;                  // per-cell stencil rows (for_rows)
+    int4* rows;                  // per-cell stencil rows (for_rows)
     int *nbr, *ncnt;
     int *wall_idx, *buf_idx, *counters;   // per-step compacted wall / buffer slots
     SphRec<R> rec;
@@ -74,7 +74,7 @@ struct DemWork {
     R *magf;                     // |u_f - u_a| of the drag closure (VTK mag_uijf)
     int *key_in, *key_out, *val_in, *val_out;
     int *g_str, *g_end;
-    int2* rows;
+    int4* rows;
 };
 
 // device-side status words (checked by the host at sync points)

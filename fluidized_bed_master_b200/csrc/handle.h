@@ -26,7 +26,8 @@ struct SphdemHandle {
     double bbox[6] = {0, 0, 0, 0, 0, 0};
     int nijk[3] = {0, 0, 0};
     double dcell = 0.0;
-    void* eng = nullptr;     // sphdem::Engine<float|double>*
+    void* eng = nullptr;     // engine host state (EngineHost or WEngineHost, by kind)
+    int kind = 0;            // 0 ISPH-DEM step, 1 2-D WCSPH step
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int64_t> graph_launches;
     std::map<int, std::vector<int>> graph_kused;

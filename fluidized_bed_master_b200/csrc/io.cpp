@@ -65,6 +65,9 @@ void sphdem_io_params_default(SphdemParams* p) {
     p->mlp_updates = 4;
     p->mlp_seed = 0;
     p->mlp_lr = 3e-4;
+    p->art_visc_alpha = 0.1;
+    p->art_visc_beta = 0.02;
+    p->delta_sph = 0.1;
     p->precision = SPHDEM_PREC_FP32;
     p->dem_wall_mask = 7;
     p->kappa = 2.0;

@@ -57,8 +57,8 @@ __device__ __forceinline__ void kgc3(const R* __restrict__ Cm, int n, int i, int
 // inside a row.
 template <typename F>
 __device__ __forceinline__ void for_stencil_j(const DevParams& P, int ic, int jc, int kc,
-                                              const int2* __restrict__ rows, F f) {
-    for_rows(P, ic, jc, kc, rows, [&](int a, int b) {
+                                              const int4* __restrict__ rows, const Cull& C, F f) {
+    for_rows(P, ic, jc, kc, rows, C, [&](int a, int b) {
         for (int j = a; j < b; j++) f(j);
     });
 }
@@ -93,12 +93,12 @@ __device__ __forceinline__ void cell_bounds(const DevParams& P, int i, int n, co
 }
 
 // per-cell stencil row table (for_rows), one thread per cell
-__global__ void k_rows(DevParams P, const int* __restrict__ gs, const int* __restrict__ ge, int2* rows) {
+__global__ void k_rows(DevParams P, const int* __restrict__ gs, const int* __restrict__ ge, int4* rows) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int nc = P.NI * P.NJ * P.NK;
     if (c >= nc) return;
     int ic = c % P.NI, base = c - ic;
-    rows[c] = row_range(gs, ge, P.NI, base, ic);
+    rows[c] = row_bounds(gs, ge, P.NI, base, ic);
 }
 
 // reorder of every persistent SPH field, source of m/rho/pres/u/temp is
@@ -174,7 +174,7 @@ __global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst
 // candidate rows and their position-record loads coalesce.
 template <typename R>
 __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, SphRec<R> rec,
-                                                    const int2* __restrict__ rows,
+                                                    const int4* __restrict__ rows,
                                                     int* __restrict__ nbr, int* __restrict__ ncnt, DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.ns) return;
@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     int c = 0, cap = P.nb_cap, n = P.ns;
-    for_rows(P, ic, jc, kc, rows, [&](int a, int b) {
+    const Cull cu = make_cull(xi, yi, zi, Rr);
+    for_rows(P, ic, jc, kc, rows, cu, [&](int a, int b) {
         for (int j = a; j < b; j++) {
             PosRec<R> qj = ldr(rec.pos + j);
             Disp<R> d;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                               const int2* __restrict__ drows) {
+                                               const int4* __restrict__ drows) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -290,7 +291,8 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
     R por = 0, dfx = 0, dfy = 0, dfz = 0;
     if (P.nd > 0) {
         float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
-        for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
+        const Cull cu = make_cull(xi, yi, zi, Rr);
+        for_stencil_j(P, ic, jc, kc, drows, cu, [&](int j) {
             if (D.ptype[j] <= 1000) return;
             PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
             if (!g.in) return;
@@ -346,7 +348,7 @@ __global__ void k_gather_history(int n, const int* __restrict__ perm, const int*
 // One warp per DEM sphere; lanes stride over the candidate rows.
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<R> D,
-                                                  DemWork<R> DW, const int2* __restrict__ srows, const int2* __restrict__ drows) {
+                                                  DemWork<R> DW, const int4* __restrict__ srows, const int4* __restrict__ drows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -363,7 +365,8 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R f1 = 0, f3 = 0, por = 0;
-    for_rows_warp(P, ic, jc, kc, srows, sm, lane, [&](int j) {
+    const Cull cu = make_cull(xi, yi, zi, Rr);
+    for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
         PosRec<R> qj = ldr(rec.pos + j);
         int ptj = tag_ptype(qj.w);
         if (ptj != 1 && ptj != 3) return;
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
         if (ptj == 1) f1 += c;
         else f3 += c;
     });
-    for_rows_warp(P, ic, jc, kc, drows, sm, lane, [&](int j) {
+    for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, [&](int j) {
         if (D.ptype[j] <= 1000) return;
         PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
         if (!g.in) return;
@@ -514,7 +517,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D, DemWork<R> DW,
-                                                     const int2* __restrict__ drows,
+                                                     const int4* __restrict__ drows,
                                                      DevFlags* F) {
     // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
     // in visit order (for_rows_warp) and the pair terms are reduced with
@@ -562,7 +565,8 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     int new_t = -1, new_id = 0;
     double new_dx = 0, new_dy = 0, new_dz = 0;
     int t_visit = lane - 32;
-    for_rows_warp(P, ic, jc, kc, drows, sm, lane, [&](int j) {
+    const Cull cu = make_cull(xi, yi, zi, P.r_search * radi);
+    for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, [&](int j) {
         t_visit += 32;
         if (D.ptype[j] <= 1000) return;
         double xj = D.x[j], yj = D.y[j], zj = D.z[j], radj = D.rad[j];
@@ -742,7 +746,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int2* __restrict__ srows) {
+                                                      DemWork<R> DW, const int4* __restrict__ srows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -767,7 +771,8 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         R tx = 0, ty = 0, tz = 0, ufx = 0, ufy = 0, ufz = 0, uax = 0, uay = 0, uaz = 0, por = 0, ttf = 0, tta = 0;
         int has_f = 0, has_a = 0;
         R pgc = voli / (mi * ff + (R)1.0e-15);
-        for_rows_warp(P, ic, jc, kc, srows, sm, lane, [&](int j) {
+        const Cull cu = make_cull(xi, yi, zi, Rr);
+        for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
             PosRec<R> qj = ldr(rec.pos + j);
             int ptj = tag_ptype(qj.w);
             if (ptj > 1000) return;
@@ -899,7 +904,7 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int2* __restrict__ drows, int time_zero) {
+                                                      DemWork<R> DW, const int4* __restrict__ drows, int time_zero) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -920,7 +925,8 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
             int ic, jc, kc;
             cell_ijk(P, xi, yi, zi, ic, jc, kc);
             float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
-            for_stencil_j(P, ic, jc, kc, drows, [&](int j) {
+            const Cull cu = make_cull(xi, yi, zi, Rr);
+            for_stencil_j(P, ic, jc, kc, drows, cu, [&](int j) {
                 if (D.ptype[j] <= 1000) return;
                 PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 0.0, r2l, r2h);
                 if (!g.in) return;
@@ -973,7 +979,7 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, SphWork<R> W, R* pres,
-                                                 const int2* __restrict__ rows,
+                                                 const int4* __restrict__ rows,
                                                  int patch_up) {
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
@@ -992,7 +998,8 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R tp = 0, flt = 0, tt = 0, tr = 0;
-    for_rows_warp(P, ic, jc, kc, rows, sm, lane, [&](int j) {
+    const Cull cu = make_cull(xi, yi, zi, R2);
+    for_rows_warp(P, ic, jc, kc, rows, cu, sm, lane, [&](int j) {
         PosRec<R> qj = ldr(rec.pos + j);
         int ptj = tag_ptype(qj.w);
         if (ptj < 1 || ptj >= 1000) return;
@@ -1326,7 +1333,7 @@ __global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, 
 // is done in place.  One warp per buffer particle (W.buf_idx).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int2* __restrict__ rows) {
+__global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int4* __restrict__ rows) {
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -1345,7 +1352,8 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     cell_ijk(P, xi, yi, zg, ic, jc, kc);
     R hd = (R)P.h_over_dx;
     R trho = 0, tp = 0, tux = 0, tuy = 0, tuz = 0, tt = 0, flt = 0;
-    for_rows_warp(P, ic, jc, kc, rows, sm, lane, [&](int j) {
+    const Cull cu = make_cull(xi, yi, zg, Rr);
+    for_rows_warp(P, ic, jc, kc, rows, cu, sm, lane, [&](int j) {
         if (S.ptype[j] != 1 || S.btype[j] != 0) return;
         PairT<R> g = pair_test<R>(xi, yi, zg, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
         if (!g.in) return;
@@ -1461,8 +1469,8 @@ __global__ void k_tick(DevFlags* F) { F->step_count += 1; }
 // caller).  Grid-stride blocks; block maxima are combined with an integer
 // atomicMax on the bit patterns, which orders non-negative doubles.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256) k_stats(int n, const R* __restrict__ rho, const R* __restrict__ ux,
+template <typename R, typename RR = R>
+__global__ void __launch_bounds__(256) k_stats(int n, const RR* __restrict__ rho, const R* __restrict__ ux,
                                                const R* __restrict__ uy, const R* __restrict__ uz,
                                                const R* __restrict__ ft, const int* __restrict__ ptype,
                                                const int* __restrict__ itype, double* out, DevFlags* F) {
@@ -1470,7 +1478,8 @@ __global__ void __launch_bounds__(256) k_stats(int n, const R* __restrict__ rho,
     double a = 0, b = 0, c = 0;
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double u = sqrt((double)ux[i] * ux[i] + (double)uy[i] * uy[i] + (double)uz[i] * uz[i]);
+        double uzi = uz ? (double)uz[i] : 0.0;   // 2-D sets pass no uz
+        double u = sqrt((double)ux[i] * ux[i] + (double)uy[i] * uy[i] + uzi * uzi);
         if (!isfinite(u) || !isfinite((double)rho[i])) bad = 1;
         if (ptype[i] == 0 || itype[i] >= 2) continue;
         a = fmax(a, (double)rho[i]);

@@ -40,7 +40,8 @@ _fields += [("margin", C.c_double * 6)]
 _fields += [(n, C.c_double) for n in _F64_B]
 _fields += [("box_c", C.c_double * 3), ("box_L", C.c_double * 3), ("cone_c", C.c_double * 3)]
 _fields += [(n, C.c_double) for n in _F64_C]
-_fields += [("mlp_lr", C.c_double), ("reserved_d", C.c_double * 7)]
+_fields += [("mlp_lr", C.c_double), ("art_visc_alpha", C.c_double), ("art_visc_beta", C.c_double),
+            ("delta_sph", C.c_double), ("reserved_d", C.c_double * 4)]
 
 
 class SphdemParams(C.Structure):
@@ -74,6 +75,7 @@ class SphdemStats(C.Structure):
 
 # PPE modes and warm starts (SPHDEM_PPE_*, SPHDEM_WARM_*)
 PPE_REFERENCE, PPE_KRYLOV, PPE_PCG = 0, 1, 2
+WCSPH, ISPH = 0, 1
 WARM_PREVIOUS, WARM_MLP, WARM_EXTRAPOLATE = 0, 1, 2
 
 
@@ -83,7 +85,7 @@ F = dict(
     h=13, rad=14, ri=15, DEMpor=16, dDEMpor=17, flt_s=18, flt_sd=19, flt_sd2=20,
     ftotalx=21, ftotaly=22, ftotalz=23, fpx=24, fpy=25, fpz=26, pgfx=27, pgfy=28, pgfz=29,
     Fdx_df=30, Fdy_df=31, Fdz_df=32, torqx=33, torqy=34, torqz=35, rho_ref=36,
-    temp1=37, temp2=38, temp3=39, dtemp=40, Q_sd=41,
+    temp1=37, temp2=38, temp3=39, dtemp=40, Q_sd=41, ftotal=42, drho=43, grad_rhox=44, grad_rhoy=45,
     p_type=64, i_type=65, buffer_type=66, dem_idx=67, pid=68, cell=69,
 )
 INT_FIELDS = {"p_type", "i_type", "buffer_type", "dem_idx", "pid", "cell"}
@@ -128,6 +130,9 @@ def reference_params():
     p.mlp_train_steps = 500
     p.mlp_updates = 4
     p.mlp_lr = 3e-4
+    p.art_visc_alpha = 0.1
+    p.art_visc_beta = 0.02
+    p.delta_sph = 0.1
     p.dem_wall_mask = 7
     p.kappa = 2.0
     p.gamma = 1.0

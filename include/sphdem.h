@@ -176,7 +176,10 @@ typedef struct SphdemParams {
     double cone_c[3], cone_r1, cone_r2, cone_h; /* functions_DEM_BC.cuh:723-725,4237-4243 */
     double wall_rest_n, wall_rest_s, wall_mu_s, wall_mu_rs; /* functions_DEM_BC.cuh:1-5 */
     double mlp_lr;              /* WARM_MLP: Adam learning rate */
-    double reserved_d[7];
+    double art_visc_alpha;      /* WCSPH artificial viscosity alpha, Alpha 0.1 (Parameters.cuh:83) */
+    double art_visc_beta;       /* WCSPH artificial viscosity beta, Beta 0.02 (Parameters.cuh:84) */
+    double delta_sph;           /* WCSPH delta-SPH coefficient, delta 0.1 (Parameters.cuh:92) */
+    double reserved_d[4];
 } SphdemParams;
 
 /* Particle fields addressable through get/set.  Values cross the ABI as
@@ -197,6 +200,7 @@ typedef enum SphdemField {
     SPHDEM_F_TORQX, SPHDEM_F_TORQY, SPHDEM_F_TORQZ,
     SPHDEM_F_RHO_REF, SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3,
     SPHDEM_F_DTEMP, SPHDEM_F_Q_SD,
+    SPHDEM_F_FTOTAL, SPHDEM_F_DRHO, SPHDEM_F_GRAD_RHOX, SPHDEM_F_GRAD_RHOY,
     /* integer fields (int32 buffers) */
     SPHDEM_F_PTYPE = 64, SPHDEM_F_ITYPE, SPHDEM_F_BUFFER_TYPE,
     SPHDEM_F_DEM_IDX, SPHDEM_F_PID, SPHDEM_F_CELL

@@ -3,7 +3,8 @@
 // Compiles the reference (SOPHIA_gpu.cu and the headers it includes, read
 // unchanged from REF_DIR via -I) into a shared library and drives its own
 // step function SOPHIA_single_ISPH (ISPH_Calc_seperate.cuh:13-503) on a
-// GPU.  The set-up below repeats what ISPH() (ISPH.cuh:10-200) and
+// GPU, and the 2-D WCSPH kernels of SOPHIA_single (WCSPH_Calc.cuh:15-340)
+// in the Lagrangian order described at ref_load_wcsph.  The set-up below repeats what ISPH() (ISPH.cuh:10-200) and
 // ISPH_Calc() (ISPH_Calc_seperate.cuh:508-903) do for one GPU, without the
 // pthread fan-out and without the run-to-time_end loop, so that the state
 // can be read back after a chosen number of steps.  Used only to generate
@@ -49,14 +50,16 @@ using namespace refh;
         if ((call) != cudaSuccess) return -100;     \
     } while (0)
 
-extern "C" int ref_load(const char* workdir) {
+// want: Isph (SOPHIA_single_ISPH) or Wcsph (the 2-D SOPHIA_single below)
+static int load_impl(const char* workdir, int want) {
     if (chdir(workdir) != 0) return -1;
     memset(vii, 0, sizeof(int_t) * vii_size);
     memset(vif, 0, sizeof(Real) * vif_size);
     ngpu = 1;
     read_solv_input(vii, vif, "./input/solv.txt");
     read_table("./input/data.txt");
-    if (solver_type != Isph) return -2;
+    if (solver_type != want) return -2;
+    if (want == Wcsph && dim != 2) return -3;
     // ISPH.cuh:55-120
     num_part = gpu_count_particle_numbers2("./input/input.txt");
     HP1 = (part1*)malloc(num_part * sizeof(part1));
@@ -70,6 +73,10 @@ extern "C" int ref_load(const char* workdir) {
     memset(HP1_dem, 0, sizeof(part1) * num_part_dem);
     read_sph_dem(HP1, HP1_sph, HP1_dem);
     for (int k = 0; k < num_part_sph; k++) HP1_sph[k].concn = (Real)k;   // identity tag
+    if (want == Wcsph) {
+        if (num_part_dem != 0) return -4;
+        for (int k = 0; k < num_part; k++) HP1[k].concn = (Real)k;
+    }
     Real cell_reduction_factor = 1.1;
     search_incr_factor = 1.0;
     search_kappa = kappa;
@@ -149,6 +156,8 @@ extern "C" int ref_load(const char* workdir) {
     for (int k = 0; k < num_part2_sph; k++) DHP1_sph[0][k].i_type = 3;
     for (int k = 0; k < num_part2_dem; k++) DHP1_dem[0][k].i_type = 3;
     c_initial_inner_outer_particle_single(HP1, DHP1[0], 0);
+    if (want == Wcsph)   // Lagrangian: ALE flags 1 (KERNEL_set_alpha is not launched)
+        for (int k = 0; k < num_part2; k++) DHP1[0][k].elix = DHP1[0][k].eliy = DHP1[0][k].eliz = 1.0;
     c_initial_inner_outer_particle_single_sph(HP1_sph, DHP1_sph[0], 0);
     c_initial_inner_outer_particle_single_dem(HP1_dem, DHP1_dem[0], 0);
     HCK(cudaMemcpy(dP1, DHP1[0], num_part2 * sizeof(part1), cudaMemcpyHostToDevice));
@@ -163,12 +172,68 @@ extern "C" int ref_load(const char* workdir) {
     HCK(cudaMalloc(&st_all, sb_all ? sb_all : 16));
     HCK(cudaMalloc(&st_sph, sb_sph ? sb_sph : 16));
     HCK(cudaMalloc(&st_dem, sb_dem ? sb_dem : 16));
-    loaded = 1;
+    loaded = want == Wcsph ? 2 : 1;
+    return 0;
+}
+
+extern "C" int ref_load(const char* workdir) { return load_impl(workdir, Isph); }
+
+// 2-D WCSPH: SOPHIA_single (WCSPH_Calc.cuh:15-340) for a Lagrangian fluid.
+// The stock driver makes SPH Eulerian (KERNEL_set_alpha), sorts only at
+// count 0 and does not launch KERNEL_interaction2D (WCSPH_Calc.cuh:187), so
+// no particle moves.  This driver launches the same kernels in the same
+// order with ALE flags 1 (set at load), NNPS every step (the count == 0
+// branch) and KERNEL_interaction2D(1, ...) at the place of the disabled line.
+extern "C" int ref_load_wcsph(const char* workdir) { return load_impl(workdir, Wcsph); }
+
+static void wcsph2d_step() {
+    dim3 b, t;
+    t.x = 128;
+    int s = sizeof(int) * (t.x + 1);
+    b.x = (num_part2 - 1) / t.x + 1;
+    if (time_type == Pre_Cor) KERNEL_clc_predictor<<<b, t>>>(dt, time, dP1, dP2, dP3);
+    cudaMemset(g_str, cu_memset, sizeof(int_t) * num_cells);
+    KERNEL_index_particle_to_cell<<<b, t>>>(g_idx_in, p_idx_in, dP1);
+    cub::DeviceRadixSort::SortPairs(st_all, sb_all, g_idx_in, g_idx, p_idx_in, p_idx, num_part2);
+    KERNEL_reorder<<<b, t, s>>>(g_idx, p_idx, g_str, g_end, dP1, dP2, dSP1, dSP2);
+    cudaMemset(dP3, 0, sizeof(part3) * num_part2);
+    cudaMemcpy(dP1, dSP1, sizeof(part1) * num_part2, cudaMemcpyDeviceToDevice);
+    KERNEL_clc_mass_update<<<b, t>>>(g_str, g_end, dSP1, dSP2, count);
+    if ((kgc_solve > 0) || (delSPH_solve == Antuono)) gradient_correction(g_str, g_end, dSP1, dP3);
+    KERNEL_clc_prep2D_coupling<<<b, t>>>(g_str, g_end, dSP1, count);
+    KERNEL_clc_prep2D<<<b, t>>>(g_str, g_end, dSP1, dSP2, dP3, count);
+    if (rho_type == Mass_Sum) KERNEL_clc_mass_sum_norm2D<<<b, t>>>(g_str, g_end, dSP1, dSP2);
+    else KERNEL_clc_continuity_norm2D<<<b, t>>>(g_str, g_end, dSP1, dSP2, dP3);
+    KERNEL_EOS<<<b, t>>>(dSP1, dSP2);
+    KERNEL_interaction2D<<<b, t>>>(1, g_str, g_end, dSP1, dSP2, dP3);
+    KERNEL_time_update_single<<<b, t>>>(dt, dSP1, dP1, dSP2, dP2, dP3, time, count);
+    KERNEL_open_boundary_extrapolation3D_1<<<b, t>>>(time, g_str, g_end, dP1, dSP2, dP3, count, dt);
+    if (xsph_solve) KERNEL_xsph2D<<<b, t>>>(1, g_str, g_end, dt, time, dSP1, dP1, dSP2);
+}
+
+extern "C" int ref_run_wcsph(int nsteps) {
+    if (loaded != 2) return -1;
+    cudaDeviceSynchronize();
+    auto t0 = refh_now();
+    for (int k = 0; k < nsteps; k++) {
+        wcsph2d_step();
+        time += dt;
+        count++;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return -100;
+    auto t1 = refh_now();
+    last_ms = refh_ms(t0, t1);
+    if (cudaGetLastError() != cudaSuccess) return -101;
+    // state after the step: dev_P1 (part1), dev_SP2 (part2), dev_P3 (part3),
+    // read back through the SPH slots of ref_get
+    HCK(cudaMemcpy(fP1s, dP1, num_part2 * sizeof(part1), cudaMemcpyDeviceToHost));
+    HCK(cudaMemcpy(fP2s, dSP2, num_part2 * sizeof(part2), cudaMemcpyDeviceToHost));
+    HCK(cudaMemcpy(fP3s, dP3, num_part2 * sizeof(part3), cudaMemcpyDeviceToHost));
     return 0;
 }
 
 extern "C" int ref_run(int nsteps) {
-    if (!loaded) return -1;
+    if (loaded != 1) return -1;
     cudaDeviceSynchronize();
     auto t0 = refh_now();
     for (int k = 0; k < nsteps; k++) {
@@ -228,7 +293,8 @@ extern "C" int ref_get(int which, const char* name, double* out) {
     G1("ftotalx", P3[k].ftotalx) G1("ftotaly", P3[k].ftotaly) G1("ftotalz", P3[k].ftotalz)
     G1("fpx", P3[k].fpx) G1("fpy", P3[k].fpy) G1("fpz", P3[k].fpz)
     G1("torqx", P3[k].torqx) G1("torqy", P3[k].torqy) G1("torqz", P3[k].torqz)
-    G1("dtemp", P3[k].dtemp) G1("Q_sd", P1[k].Q_sd)
+    G1("dtemp", P3[k].dtemp) G1("Q_sd", P1[k].Q_sd) G1("drho", P3[k].drho) G1("ftotal", P3[k].ftotal)
+    G1("grad_rhox", P1[k].grad_rhox) G1("grad_rhoy", P1[k].grad_rhoy)
 #undef G1
     if (f.rfind("ct_idx", 0) == 0) {   // ct_idx<s>
         int s = atoi(f.c_str() + 6);

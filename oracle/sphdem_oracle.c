@@ -36,7 +36,7 @@
 #define OR_SFIELDS(X)                                                       \
     X(ftotalx) X(ftotaly) X(ftotalz) X(ftotal) X(fpx) X(fpy) X(fpz)         \
     X(torqx) X(torqy) X(torqz) X(dtemp) X(dtemp1) X(dtemp2) X(dtemp3)       \
-    X(drad)
+    X(drad) X(drho)
 #define OR_IFIELDS(X) X(p_type) X(i_type) X(buffer_type) X(dem_idx) X(pid)
 
 #define NSLOT 16
@@ -1744,6 +1744,326 @@ static void k_xsph(OracleState* S) {
 /* ---------------------------------------------------------------------- */
 /* one step: SOPHIA_single_ISPH (ISPH_Calc_seperate.cuh:13-503)            */
 /* ---------------------------------------------------------------------- */
+/* ---------------------------------------------------------------------- */
+/* 2-D WCSPH step (solver_type WCSPH, dim 2): SOPHIA_single               */
+/* (WCSPH_Calc.cuh:15-340) in its Lagrangian variant -- ALE flags 1, NNPS  */
+/* every step, KERNEL_interaction2D launched -- which the stock driver     */
+/* does not run (set_alpha makes SPH Eulerian, NNPS only at count 0,       */
+/* interaction2D commented out at WCSPH_Calc.cuh:187).  Viscosity is the   */
+/* one constant of viscosity() without property tables (mu_gas), DEM      */
+/* porosity is 1.  The 2-D loops are the 27-cell loop on a one-layer grid. */
+/* ---------------------------------------------------------------------- */
+/* KERNEL_clc_predictor: functions_TIME.cuh:77-228 */
+static void w_predictor(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    double tdt = P->dt;
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] == 3) continue;
+        int pt = o->p_type[i], bt = o->buffer_type[i];
+        double tx0 = o->x[i], ty0 = o->y[i], tux0 = o->ux[i], tuy0 = o->uy[i];
+        if (pt >= 0) {
+            o->x[i] = tx0 + tux0 * (tdt * 0.5) * (pt > 0) * 1.0;
+            o->y[i] = ty0 + tuy0 * (tdt * 0.5) * (pt > 0) * 1.0;
+            o->ux[i] = tux0 + o->ftotalx[i] * (bt == 0) * (tdt * 0.5);
+            o->uy[i] = tuy0 + o->ftotaly[i] * (bt == 0) * (tdt * 0.5);
+        }
+        o->x0[i] = tx0;
+        o->y0[i] = ty0;
+        o->ux0[i] = tux0;
+        o->uy0[i] = tuy0;
+        double trho = o->rho[i];
+        o->rho0[i] = trho;
+        if (P->rho_type == 1 && pt > 0) o->rho[i] = trho + o->drho[i] * (tdt * 0.5);
+    }
+}
+
+static inline void w_kgc_apply(const SphdemParams* P, const double* Cm, double* dx, double* dy) {
+    if (P->kgc_solve != 1) return;
+    double a = *dx, b = *dy;
+    *dx = Cm[0] * a + Cm[1] * b;
+    *dy = Cm[3] * a + Cm[4] * b;
+}
+
+/* KERNEL_clc_correction_KGC_2D: functions_PREP2.cuh:73-160 (Cm rows 0,1) */
+static void w_kgc2d(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] > 2 || o->p_type[i] > 1000) continue;
+        double h = o->h[i], tA = knl_tmpA(P->kernel_type, 2, h), R = P->kappa * h;
+        double xi = o->x[i], yi = o->y[i], zi = o->z[i];
+        int ic, jc, kc;
+        cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+        double txx = 0, txy = 0, tyy = 0;
+        FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+            if (o->p_type[j] > 1000) continue;
+            double xj = o->x[j], yj = o->y[j];
+            double td = dist3(xi, yi, zi, xj, yj, o->z[j]);
+            if (td > 0 && td < R) {
+                double dw = knl_dw(P->kernel_type, tA, h, td);
+                double mtd = o->m[j] * dw, rtd = 1.0 / (o->rho[j] * td), t;
+                t = -mtd * (xi - xj) * (xi - xj); t *= rtd; txx += t;
+                t = -mtd * (yi - yj) * (xi - xj); t *= rtd; txy += t;
+                t = -mtd * (yi - yj) * (yi - yj); t *= rtd; tyy += t;
+            }
+        }
+        double* Cm = o->Cm + (size_t)i * 9;
+        double det = txx * tyy - txy * txy;
+        if (fabs(det) > 1e-4) {
+            double r = 1.0 / det;
+            Cm[0] = tyy * r; Cm[1] = -txy * r; Cm[3] = -txy * r; Cm[4] = txx * r;
+        } else {
+            Cm[0] = 1; Cm[1] = 0; Cm[3] = 0; Cm[4] = 1;
+        }
+    }
+}
+
+/* KERNEL_clc_prep2D: functions_PREP2.cuh:1247-1420 (no SPS, no surface tension) */
+static void w_prep2d(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    int filt = (S->count % P->freq_filt) == 0, anto = P->delSPH_solve == 2;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] > 2 || o->p_type[i] > 1000) continue;
+        double h = o->h[i], tA = knl_tmpA(P->kernel_type, 2, h), R = P->kappa * h;
+        double xi = o->x[i], yi = o->y[i], zi = o->z[i], rhoi = o->rho[i], mi = o->m[i];
+        int ic, jc, kc;
+        cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+        double flt = 0, gx = 0, gy = 0;
+        FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+            if (o->p_type[j] > 1000) continue;
+            double xj = o->x[j], yj = o->y[j];
+            double td = dist3(xi, yi, zi, xj, yj, o->z[j]) + 1e-20;
+            if (td < R) {
+                double w = knl_w(P->kernel_type, tA, h, td), dw = knl_dw(P->kernel_type, tA, h, td);
+                double tx = dw * (xi - xj) / td, ty = dw * (yi - yj) / td;
+                double mj = o->m[j], rhoj = o->rho[j];
+                if (filt) flt += mj / rhoj * w;
+                if (anto) {
+                    w_kgc_apply(P, o->Cm + (size_t)i * 9, &tx, &ty);
+                    gx += -(rhoj - rhoi) * (mj / rhoj) * tx;
+                    gy += -(rhoj - rhoi) * (mj / rhoj) * ty;
+                }
+            }
+        }
+        o->rho_ref[i] = mi / ((h / 1.600) * (h / 1.600));
+        if (filt) o->flt_s[i] = flt;
+        if (anto) {
+            o->grad_rhox[i] = gx;
+            o->grad_rhoy[i] = gy;
+        }
+    }
+}
+
+/* KERNEL_clc_continuity_norm2D: functions_MASS.cuh:670-769 */
+static void w_continuity2d(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    int anto = P->delSPH_solve == 2;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] > 2 || o->p_type[i] > 1000) continue;
+        int pti = o->p_type[i];
+        double h = o->h[i], tA = knl_tmpA(P->kernel_type, 2, h), R = P->kappa * h;
+        double xi = o->x[i], yi = o->y[i], zi = o->z[i];
+        double uxi = o->ux[i] * (pti > 0), uyi = o->uy[i] * (pti > 0), rhoi = o->rho[i];
+        double gxi = o->grad_rhox[i], gyi = o->grad_rhoy[i];
+        int ic, jc, kc;
+        cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+        double tx = 0, ty = 0, tr = 0;
+        FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+            if (o->p_type[j] > 1000) continue;
+            double xj = o->x[j], yj = o->y[j];
+            double td = dist3(xi, yi, zi, xj, yj, o->z[j]) + 1e-20;
+            if (td < R) {
+                int ptj = o->p_type[j];
+                double dw = knl_dw(P->kernel_type, tA, h, td);
+                double mj = o->m[j], rhoj = o->rho[j];
+                double uxj = o->ux[j] * (ptj > 0), uyj = o->uy[j] * (ptj > 0);
+                double gx = dw * (xi - xj) / td, gy = dw * (yi - yj) / td;
+                if (P->kgc_solve > 0) w_kgc_apply(P, o->Cm + (size_t)i * 9, &gx, &gy);
+                double tm = mj * (rhoi / rhoj);
+                tx += (uxi - uxj) * tm * gx;
+                ty += (uyi - uyj) * tm * gy;
+                if (P->delSPH_solve > 0) {
+                    double phi = (gxi + o->grad_rhox[j]) * (xj - xi);
+                    phi += (gyi + o->grad_rhoy[j]) * (yj - yi);
+                    phi = (-0.5 * phi) * anto + (rhoj - rhoi);
+                    double t = -2 * (P->delta_sph * 1.0) * h * P->soundspeed * (mj / rhoj);
+                    t *= phi * dw / td;
+                    tr += t;
+                }
+            }
+        }
+        o->drho[i] = (tx + ty) * (rhoi / o->rho_ref[i]) + tr * (P->delSPH_solve > 0);
+    }
+}
+
+/* KERNEL_EOS: functions_PROP.cuh:7-28 */
+static void w_eos(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    double tB = P->soundspeed * P->soundspeed * (1.186) / P->gamma;
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] > 2 || o->p_type[i] > 1000 || o->buffer_type[i] != 0) continue;
+        double tP = pow(o->rho[i] / o->rho_ref[i], P->gamma);
+        o->pres[i] = tB * (tP - 1.0);
+    }
+}
+
+/* KERNEL_interaction2D: functions_INTERACTION.cuh:64-410 (i_type 1) */
+static void w_interaction2d(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+    for (int i = 0; i < o->n; i++) {
+        if (o->i_type[i] != 1 || o->p_type[i] > 1000) continue;
+        double h = o->h[i], tA = knl_tmpA(P->kernel_type, 2, h), R = P->kappa * h;
+        double xi = o->x[i], yi = o->y[i], zi = o->z[i];
+        double uxi = o->ux[i], uyi = o->uy[i], pi = o->pres[i], mi = o->m[i], rhoi = o->rho[i];
+        double pori = 1.0, vis = P->mu_gas;
+        int ic, jc, kc;
+        cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+        double tx = 0, ty = 0, pgx = 0, pgy = 0;
+        FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+            if (o->p_type[j] > 1000) continue;
+            double xj = o->x[j], yj = o->y[j];
+            double td = dist3(xi, yi, zi, xj, yj, o->z[j]) + 1e-20;
+            if (td < R) {
+                double dw = knl_dw(P->kernel_type, tA, h, td);
+                double gx = dw * (xi - xj) / td, gy = dw * (yi - yj) / td;
+                if (P->kgc_solve > 0) w_kgc_apply(P, o->Cm + (size_t)i * 9, &gx, &gy);
+                double uxj = o->ux[j], uyj = o->uy[j], mj = o->m[j], rhoj = o->rho[j], pj = o->pres[j];
+                double hj = o->h[j], porj = 1.0;
+                if (P->fp_solve) {
+                    double Cp = -mj * (pi + pj) / (pori * rhoi * porj * rhoj);
+                    double px = Cp * gx, py = Cp * gy;
+                    tx += px;
+                    ty += py;
+                    pgx += rhoi * pori * px;
+                    pgy += rhoi * pori * py;
+                }
+                if (P->fv_solve) {
+                    double Cv = (xi - xj) * gx + (yi - yj) * gy;
+                    Cv *= 4 * (mj / (rhoi * rhoj));
+                    Cv *= (vis * vis) / (vis + vis);
+                    Cv /= td;
+                    Cv /= td;
+                    tx += Cv * (uxi - uxj);
+                    ty += Cv * (uyi - uyj);
+                }
+                if (P->fva_solve) {
+                    double uij = (uxi - uxj) * (xi - xj) + (uyi - uyj) * (yi - yj);
+                    if (uij < 0) {
+                        double hij = (h + hj) * 0.5;
+                        double phi = hij * uij;
+                        phi /= (td * td + 0.01 * hij * hij);
+                        double Pij = mi * phi * (-P->art_visc_alpha * P->soundspeed + P->art_visc_beta * phi);
+                        Pij /= (rhoi + rhoj);
+                        Pij *= 0.5;
+                        tx += -Pij * gx;
+                        ty += -Pij * gy;
+                    }
+                }
+            }
+        }
+        if (P->fg_solve) ty += -P->g_sph;
+        o->ftotalx[i] = tx;
+        o->ftotaly[i] = ty;
+        o->ftotal[i] = sqrt(tx * tx + ty * ty);
+        o->pgf_x[i] = pgx;
+        o->pgf_y[i] = pgy;
+    }
+}
+
+/* KERNEL_time_update_single (functions_TIME.cuh:676-880) and KERNEL_xsph2D
+ * (functions_TIME.cuh:1520-1605): the corrector writes TP1 (new velocity,
+ * density; positions when XSPH is off), XSPH reads the corrected velocity
+ * and the predicted positions and density. */
+static void w_correct_xsph(OracleState* S) {
+    OSet* o = &S->s;
+    const SphdemParams* P = &S->p;
+    int n = o->n;
+    double tdt = P->dt;
+    double* xn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
+    double* yn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
+    double* rn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
+    double* un = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
+    double* vn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
+    for (int i = 0; i < n; i++) {
+        xn[i] = o->x[i];
+        yn[i] = o->y[i];
+        rn[i] = o->rho[i];
+        un[i] = o->ux[i];
+        vn[i] = o->uy[i];
+        if (o->i_type[i] == 3) continue;
+        int pt = o->p_type[i], bt = o->buffer_type[i];
+        double tux0 = o->ux0[i], tuy0 = o->uy0[i], ax = 0, ay = 0;
+        if (pt > 0) {
+            ax = o->ftotalx[i] * (bt == 0);
+            ay = o->ftotaly[i] * (bt == 0);
+        }
+        double uxc = tux0 + ax * tdt, uyc = tuy0 + ay * tdt;
+        if ((uxc * uxc + uyc * uyc) >= P->u_limit * P->u_limit) {
+            uxc = tux0;
+            uyc = tuy0;
+        }
+        if (!P->xsph_solve) {
+            xn[i] = o->x0[i] + uxc * tdt * (pt > 0) * 1.0;
+            yn[i] = o->y0[i] + uyc * tdt * (pt > 0) * 1.0;
+        }
+        un[i] = uxc;
+        vn[i] = uyc;
+        if (P->rho_type == 1 && pt > 0) rn[i] = o->rho0[i] + o->drho[i] * tdt;
+    }
+    if (P->xsph_solve) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(S->nthreads)
+        for (int i = 0; i < n; i++) {
+            if (o->i_type[i] != 1 || o->p_type[i] > 1000) continue;
+            int pt = o->p_type[i];
+            double h = o->h[i], tA = knl_tmpA(P->kernel_type, 2, h), R = P->kappa * h;
+            double xi = o->x[i], yi = o->y[i], zi = o->z[i], uxi = un[i], uyi = vn[i], flt = o->flt_s[i];
+            int ic, jc, kc;
+            cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
+            double tx = 0, ty = 0;
+            FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
+                if (o->p_type[j] > 1000) continue;
+                double xj = o->x[j], yj = o->y[j];
+                double td = dist3(xi, yi, zi, xj, yj, o->z[j]);
+                if (td < R) {
+                    double w = knl_w(P->kernel_type, tA, h, td);
+                    double mj = o->m[j], rhoj = o->rho[j];
+                    tx += P->c_xsph * mj / rhoj * (-uxi + un[j]) * w / flt;
+                    ty += P->c_xsph * mj / rhoj * (-uyi + vn[j]) * w / flt;
+                }
+            }
+            xn[i] = o->x0[i] + (uxi + tx) * tdt * (pt > 0);
+            yn[i] = o->y0[i] + (uyi + ty) * tdt * (pt > 0);
+        }
+    }
+    memcpy(o->x, xn, sizeof(double) * (size_t)n);
+    memcpy(o->y, yn, sizeof(double) * (size_t)n);
+    memcpy(o->rho, rn, sizeof(double) * (size_t)n);
+    memcpy(o->ux, un, sizeof(double) * (size_t)n);
+    memcpy(o->uy, vn, sizeof(double) * (size_t)n);
+    free(xn); free(yn); free(rn); free(un); free(vn);
+}
+
+static void oracle_wcsph2d_step(OracleState* S) {
+    w_predictor(S);
+    nnps(S, &S->s);   /* every step; P3 (forces, drho) zeroed after the predictor */
+    build_sph_list(S);
+    if (S->p.kgc_solve == 1 || S->p.delSPH_solve == 2) w_kgc2d(S);
+    w_prep2d(S);
+    w_continuity2d(S);
+    w_eos(S);
+    w_interaction2d(S);
+    w_correct_xsph(S);
+}
+
 static void oracle_one_step(OracleState* S) {
     const SphdemParams* P = &S->p;
     int sph_turn = (S->count % P->decouple_stride) == 0;
@@ -1826,6 +2146,8 @@ static double* dfield(OSet* o, int f) {
     case SPHDEM_F_TORQX: return o->torqx; case SPHDEM_F_TORQY: return o->torqy; case SPHDEM_F_TORQZ: return o->torqz;
     case SPHDEM_F_RHO_REF: return o->rho_ref; case SPHDEM_F_TEMP1: return o->temp1; case SPHDEM_F_TEMP2: return o->temp2;
     case SPHDEM_F_TEMP3: return o->temp3; case SPHDEM_F_DTEMP: return o->dtemp; case SPHDEM_F_Q_SD: return o->Q_sd;
+    case SPHDEM_F_FTOTAL: return o->ftotal; case SPHDEM_F_DRHO: return o->drho;
+    case SPHDEM_F_GRAD_RHOX: return o->grad_rhox; case SPHDEM_F_GRAD_RHOY: return o->grad_rhoy;
     default: return NULL;
     }
 }
@@ -1924,7 +2246,8 @@ int oracle_commit(OracleState* S) {
 int oracle_step(OracleState* s, int nsteps) {
     if (!s || !s->committed) return SPHDEM_E_ARG;
     for (int k = 0; k < nsteps; k++) {
-        oracle_one_step(s);
+        if (s->p.solver_type == SPHDEM_WCSPH) oracle_wcsph2d_step(s);
+        else oracle_one_step(s);
         s->time += s->p.dt; /* ISPH_Calc_seperate.cuh:924-925 */
         s->count++;
     }

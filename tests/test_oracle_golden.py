@@ -2,8 +2,8 @@
 
 tests/golden/*.npz were produced by tests/golden/make_golden.py: the
 unmodified reference kernels (oracle/_ref, compiled from the reference
-sources) advanced seeded spouted beds on a B200 and their state was read
-back.  Here the CPU oracle replays the same inputs and must agree:
+sources) advanced seeded spouted beds (ISPH-DEM) and 2-D dam breaks
+(WCSPH) on a B200 and their state was read back.  Here the CPU oracle replays the same inputs and must agree:
 integer fields exactly, contact-history partners exactly, real fields to
 rel. L2 <= 1e-9 (FP64 on both sides; only rounding, FMA contraction in
 the reference build and summation order differ).
@@ -30,7 +30,53 @@ def test_fixtures_present():
     assert GOLD, "tests/golden/*.npz missing: run tests/golden/make_golden.py on a GPU machine"
 
 
-@pytest.mark.parametrize("path", GOLD, ids=[p.split("/")[-1] for p in GOLD])
+REAL_W = ["x", "y", "ux", "uy", "m", "rho", "pres", "flt_s", "pgfx", "pgfy", "rho_ref", "ftotalx", "ftotaly",
+          "ftotal", "drho", "grad_rhox", "grad_rhoy"]
+
+
+def _meta(path):
+    return json.loads(np.load(path)["meta"].tobytes())
+
+
+ISPH_GOLD = [p for p in GOLD if _meta(p).get("solver", "isph") == "isph"]
+WCSPH_GOLD = [p for p in GOLD if _meta(p).get("solver") == "wcsph"]
+
+
+def test_wcsph_fixtures_present():
+    assert WCSPH_GOLD, "tests/golden/dam2d*.npz missing: run tests/golden/make_golden.py on a GPU machine"
+
+
+@pytest.mark.parametrize("path", WCSPH_GOLD, ids=[p.split("/")[-1] for p in WCSPH_GOLD])
+def test_oracle_matches_reference_wcsph2d(path):
+    """2-D WCSPH dam breaks: cell-sorted order and types exact, real fields
+    rel. L2 <= 1e-9 at every checkpoint (up to 1000 steps)."""
+    g, p, sph, dem = load_golden(path)
+    meta = json.loads(g["meta"].tobytes())
+    orc = Oracle(p, sph, dem, threads=4)
+    nijk, _, _ = orc.grid()
+    assert list(nijk) == list(g["nijk"]), "cell grid differs from the reference's NI, NJ, NK"
+    done = 0
+    bad = []
+    for cp in g["checkpoints"]:
+        orc.step(int(cp) - done)
+        done = int(cp)
+        pre = f"s{cp}_sph_"
+        ref_pid = g[pre + "pid"].astype(np.int64)
+        opid = orc.get(SPH, "pid")
+        assert np.array_equal(np.sort(ref_pid), np.arange(meta["ns"]))
+        assert np.array_equal(ref_pid, opid), f"cell-sorted order differs from the reference at step {cp}"
+        for f in ("p_type", "i_type", "buffer_type"):
+            assert np.array_equal(g[pre + f].astype(np.int64), orc.get(SPH, f)), f
+        for f in REAL_W:
+            e = rel_l2(orc.get(SPH, f), g[pre + f])
+            if not e <= TOL:
+                bad.append((int(cp), f, e))
+    moved = np.abs(by_id(ref_pid, g[f"s{done}_sph_y"]) - g["in_sph_y"]).max()
+    assert moved > 0, "nothing moved: the comparison would be vacuous"
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("path", ISPH_GOLD, ids=[p.split("/")[-1] for p in ISPH_GOLD])
 def test_oracle_matches_reference(path):
     g, p, sph, dem = load_golden(path)
     meta = json.loads(g["meta"].tobytes())

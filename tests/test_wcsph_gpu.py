@@ -1,0 +1,148 @@
+"""2-D WCSPH (solver_type WCSPH, dim 2) on the GPU through the C ABI.
+
+The dam break of the 2-D configuration (1.6 x 1.0 m tank, 0.4 x 0.8 m
+column, three wall layers, Wendland C2, Tait EOS) at dx = 5 mm
+(14,978 particles) and, for the reference fixtures, dx = 1 cm.
+
+Bar (written into each assert):
+* cell keys, sorted order and neighbour lists bit-exact with the oracle;
+* FP64 build vs the FP64 oracle: rel. L2 <= 1e-9 per field;
+* FP32 build vs the FP64 oracle: rel. L2 <= 1e-5 per state field after
+  100 steps (pressure, a difference of two nearly equal numbers in the
+  Tait EOS, against its own scale: max abs error <= 1e-5 of max |p|);
+* the engine against the reference's own run (tests/golden/dam2d*.npz)
+  to the same FP64 bar, up to 1000 steps.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from fluidized_bed_master_b200.beds import dam_break_2d
+from fluidized_bed_master_b200.params import SPH
+from oracle import Oracle
+from tests.helpers import by_id, golden_files, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["x", "y", "ux", "uy", "m", "rho", "pres", "flt_s", "pgfx", "pgfy", "rho_ref", "ftotalx", "ftotaly",
+          "ftotal", "drho", "grad_rhox", "grad_rhoy"]
+VARIANTS = {
+    "plain": dict(),
+    "kgc_antuono_xsph": dict(kgc_solve=1, delSPH_solve=2, xsph_solve=1, c_xsph=0.5),
+    "molteni_xsph": dict(delSPH_solve=1, xsph_solve=1, c_xsph=0.5),
+}
+
+
+def _engine(p, sph, prec):
+    from fluidized_bed_master_b200.engine import Engine
+
+    q = p.copy()
+    q.precision = prec
+    return Engine(q, sph, {})
+
+
+def _bed(variant, seed=41, dx=5.0e-3):
+    p, sph, _ = dam_break_2d(dx=dx, seed=seed)
+    for k, v in VARIANTS[variant].items():
+        setattr(p, k, v)
+    return p, sph
+
+
+def _compare(eng, orc, fields, tol):
+    ie, io = eng.get(SPH, "pid"), orc.get(SPH, "pid")
+    bad = []
+    for f in fields:
+        e = rel_l2(by_id(ie, eng.get(SPH, f)), by_id(io, orc.get(SPH, f)))
+        if not e <= tol:
+            bad.append((f, e))
+    return bad
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_wcsph_cells_sort_and_neighbor_lists_bit_exact(prec):
+    p, sph = _bed("kgc_antuono_xsph")
+    eng = _engine(p, sph, prec)
+    orc = Oracle(p, sph, {}, threads=8)
+    for _ in range(3):
+        eng.step(1)
+        orc.step(1)
+        assert np.array_equal(eng.get(SPH, "pid"), orc.get(SPH, "pid")), "sorted order differs"
+        assert np.array_equal(eng.get(SPH, "cell"), orc.get(SPH, "cell")), "cell keys differ"
+        ce, le = eng.neighbors()
+        co, lo = orc.neighbors()
+        assert np.array_equal(ce, co), "neighbour counts differ"
+        for i in range(eng.ns):
+            assert np.array_equal(le[i, : ce[i]], lo[i, : co[i]]), f"neighbour list of slot {i} differs"
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_wcsph_fp64_matches_oracle(variant):
+    """FP64 build vs oracle: rel. L2 <= 1e-9 per field after 1 and 20 steps."""
+    p, sph = _bed(variant)
+    eng = _engine(p, sph, 1)
+    orc = Oracle(p, sph, {}, threads=8)
+    bad = []
+    done = 0
+    for cp in (1, 20):
+        eng.step(cp - done)
+        orc.step(cp - done)
+        done = cp
+        bad += [(cp,) + b for b in _compare(eng, orc, FIELDS, 1e-9)]
+    st = eng.stats()
+    assert st["count"] == 20 and st["nan_flag"] == 0 and st["overflow_flags"] == 0
+    assert not bad, bad
+
+
+def test_wcsph_fp32_within_1e5_after_100_steps():
+    p, sph = _bed("plain", seed=42)
+    eng = _engine(p, sph, 0)
+    orc = Oracle(p, sph, {}, threads=8)
+    eng.step(100)
+    orc.step(100)
+    bad = _compare(eng, orc, ["x", "y", "ux", "uy", "rho", "flt_s"], 1e-5)
+    pe = by_id(eng.get(SPH, "pid"), eng.get(SPH, "pres"))
+    po = by_id(orc.get(SPH, "pid"), orc.get(SPH, "pres"))
+    assert np.max(np.abs(pe - po)) <= 1e-5 * np.max(np.abs(po)), np.max(np.abs(pe - po)) / np.max(np.abs(po))
+    assert not bad, bad
+
+
+def test_wcsph_runs_are_deterministic_and_stats():
+    """Two handles on the same input give bit-identical states (no atomics
+    in any sum); stats report the fluid's motion."""
+    p, sph = _bed("kgc_antuono_xsph", seed=43)
+    a = _engine(p, sph, 1)
+    b = _engine(p, sph, 1)
+    a.step(10)
+    b.step(5)
+    b.step(5)
+    for f in ("x", "y", "ux", "uy", "rho", "pres"):
+        assert np.array_equal(a.get(SPH, f), b.get(SPH, f)), f
+    st = a.stats()
+    uy = a.get(SPH, "uy")
+    assert st["count"] == 10 and abs(st["time"] - 10 * p.dt) < 1e-15
+    assert st["u_max_sph"] == pytest.approx(np.sqrt(a.get(SPH, "ux") ** 2 + uy ** 2).max(), rel=1e-12)
+    assert uy.min() < 0
+
+
+W_GOLD = [g for g in golden_files() if json.loads(np.load(g)["meta"].tobytes()).get("solver") == "wcsph"]
+
+
+@pytest.mark.parametrize("path", W_GOLD, ids=[g.split("/")[-1] for g in W_GOLD])
+def test_wcsph_engine_matches_reference_run(path):
+    g, p, sph, _ = load_golden(path)
+    q = p.copy()
+    eng = _engine(q, sph, 1)
+    done = 0
+    bad = []
+    for cp in g["checkpoints"]:
+        eng.step(int(cp) - done)
+        done = int(cp)
+        pre = f"s{cp}_sph_"
+        ref_pid = g[pre + "pid"].astype(np.int64)
+        assert np.array_equal(eng.get(SPH, "pid"), ref_pid), f"sorted order differs at step {cp}"
+        for f in FIELDS:
+            e = rel_l2(eng.get(SPH, f), g[pre + f])
+            if not e <= 1e-9:
+                bad.append((int(cp), f, e))
+    assert not bad, bad
