@@ -282,10 +282,9 @@ static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cud
     const int* nb = EH->E.sw.nbr;
     int n = P.ns;
     if (H->p.ppe_mode == SPHDEM_PPE_PCG) {
-        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.p, K.v, K.p, KP_PQ, nullptr, 0, 0);
-        k_cg_x<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.p, K.v, K.x, K.r, K.z, K.part, K.sc);
-        k_cg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.z, K.p, K.part, K.sc);
-        k_kry_check<<<1, KRY_T, 0, st>>>(K.part, K.sc, hnd, in_graph, 1);
+        // u in z, w in v, s in s
+        k_cg_upd<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.z, K.v, K.p, K.s, K.x, K.r, K.sc);
+        k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 0, hnd, in_graph);
     } else {
         k_bicg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.r, K.p, K.v, K.y, K.part, K.sc);
         k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.y, K.v, K.rh, KP_RHV, nullptr, 0, 0);
@@ -297,7 +296,8 @@ static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cud
 }
 
 // learned warm start, before the solve: statistics (training steps),
-// normalised features, and in use the network's initial iterate
+// normalised features, and in use the network's predicted change (its
+// direction in the projected initial iterate)
 template <typename R>
 static int mlp_before_solve(SphdemHandle* H, EngineHost<R>* EH, int phase) {
     KryWork<R>& K = EH->K;
@@ -311,18 +311,26 @@ static int mlp_before_solve(SphdemHandle* H, EngineHost<R>* EH, int phase) {
     if (phase == 2) {
         int r = mlp_forward(EH->net, K.feat, n, K.yp, st);
         if (r) return r;
-        // x0 = p_prev + sum_k c_k d_k, c from the minimal-residual fit
-        // (directions in p, s, t; their images under A in v, rh, z)
-        const int* nb = EH->E.sw.nbr;
-        k_blend_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, EH->E.S[1 - EH->E.cur_s].dpres, K.p, K.s, K.t);
-        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.pprev, K.y, K.pprev, KP_SS, nullptr, 0, 0);
-        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.p, K.v, K.p, KP_SS, nullptr, 0, 0);
-        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.s, K.rh, K.s, KP_SS, nullptr, 0, 0);
-        k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.t, K.z, K.t, KP_SS, nullptr, 0, 0);
-        k_blend_dots<<<KRY_G, KRY_T, 0, st>>>(n, K.b, K.y, K.v, K.rh, K.z, K.part);
-        k_blend_solve<<<1, KRY_T, 0, st>>>(K.part, K.sc);
-        k_blend_apply<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, K.p, K.s, K.t);
     }
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+// projected initial iterate (warm starts PROJECT and MLP): A p_prev, the
+// directions, their products and dots in one pass, the small solve, x0
+template <typename R>
+static int project_initial(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, int use_mlp, int cg) {
+    KryWork<R>& K = EH->K;
+    int n = EH->E.P.ns;
+    cudaStream_t st = H->stream;
+    k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, EH->E.sw.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
+    k_proj_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, S.pid, std::min(std::max(H->p.warm_hist, 0),
+                                                                          SPHDEM_WARM_HIST_MAX), use_mlp);
+    int fit = H->p.warm_fit | (cg ? 0 : SPHDEM_FIT_RESIDUAL);   // BiCGStab: the residual norm
+    int pb = std::min(KRY_G, std::max(1, (n + PROJ_T - 1) / PROJ_T));
+    k_proj_spmv<R><<<pb, PROJ_T, 0, st>>>(n, K, fit);
+    k_proj_solve<R><<<1, KRY_T, 0, st>>>(K, pb);
+    k_proj_apply<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, fit);
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -360,15 +368,22 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
         KTIME(KT_PPE_ASM);
         k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, H->p.warm_start == SPHDEM_WARM_EXTRAPOLATE);
     }
-    if (phase) {
+    if (phase || K.D) {
         KTIME(KT_PPE_WARM);
-        int r = mlp_before_solve<R>(H, EH, phase);
+        int r = phase ? mlp_before_solve<R>(H, EH, phase) : SPHDEM_OK;
+        if (!r && K.D) r = project_initial<R>(H, EH, S, phase == 2, cg);
         if (r) return r;
     }
     KTimer kt_solve(H, KT_PPE_SOLVE);
     k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
-    k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
-    k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);
+    if (cg) {
+        k_cg_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.z, K.p, K.s, K.sc, H->p.ppe_tol,
+                                           H->p.ppe_max_iter);
+        k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 1, 0, 0);
+    } else {
+        k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
+        k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);
+    }
     CK(cudaGetLastError());
     if (H->capturing) {
         cudaStreamCaptureStatus cs;
@@ -414,6 +429,7 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
         if (r) return r;
     }
     k_kry_final<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K);
+    if (K.hist) k_proj_ring<<<1, 1, 0, st>>>(K.hring);
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -754,17 +770,30 @@ static int commit_t(SphdemHandle* H) {
         if (!A.ok) return SPHDEM_E_NOMEM;
         if (p.ppe_mode != SPHDEM_PPE_REFERENCE) {
             KryWork<R>& K = EH->K;
-            K.a = A.get<R>((size_t)cap * ns);
+            K.e = A.get<typename KEnt<R>::T>((size_t)cap * ((ns + 31) / 32 * 32));
+            K.cap = cap;
+            K.ctr = A.get<unsigned>(1);
+            K.wm = A.get<double>(ns);
             K.kcnt = A.get<int>(ns);
             double** vecs[] = {&K.d, &K.b, &K.x, &K.r, &K.rh, &K.p, &K.v, &K.s, &K.t, &K.y, &K.z};
             for (double** v : vecs) *v = A.get<double>(ns);
             K.part = A.get<double>((size_t)KRY_NPART * KRY_G);
             K.sc = A.get<double>(KS_COUNT);
             if (!A.ok) return SPHDEM_E_NOMEM;
+            if (p.warm_start == SPHDEM_WARM_MLP || p.warm_start == SPHDEM_WARM_PROJECT) {
+                K.D = A.get<float>((size_t)ns * PROJ_MP);
+                K.hist = A.get<float>((size_t)SPHDEM_WARM_HIST_MAX * ns);
+                K.hist_n = ns;
+                K.hring = A.get<int>(2);
+                K.ppart = A.get<double>((size_t)PROJ_NV * KRY_G);
+                K.pc = A.get<double>(PROJ_MAX + 2);
+                if (!A.ok) return SPHDEM_E_NOMEM;
+            }
             if (p.warm_start == SPHDEM_WARM_MLP) {
                 K.fraw = A.get<float>((size_t)ns * MLP_FEAT);
                 K.feat = A.get<__nv_bfloat16>((size_t)ns * MLP_FEAT);
                 K.pprev = A.get<double>(ns);
+                K.x0 = A.get<double>(ns);
                 K.yp = A.get<float>(ns);
                 K.target = A.get<float>(ns);
                 K.weight = A.get<float>(ns);
@@ -941,6 +970,12 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
         out->ppe_rel_residual = sc[KS_RES];
         out->ppe_status = (int32_t)sc[KS_STATUS];
         out->ppe_initial_residual = sc[KS_RES0];
+        if (EH->K.pc) {
+            double pc[2];
+            CK(cudaMemcpy(pc, EH->K.pc + PROJ_MAX, sizeof(pc), cudaMemcpyDeviceToHost));
+            out->ppe_warm_dirs = (int32_t)pc[0];
+            out->ppe_warm_gain = pc[1];
+        }
     }
     if (EH->has_mlp) {
         float loss[2] = {0, 0};
@@ -1321,8 +1356,11 @@ static int check_supported(const SphdemParams* p) {
     if (p->ppe_mode != SPHDEM_PPE_REFERENCE && !(p->ppe_tol > 0)) return SPHDEM_E_ARG;
     // the reference sweep always starts from the previous pressure
     if (p->warm_start == SPHDEM_WARM_MLP && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
+    if (p->warm_start == SPHDEM_WARM_PROJECT && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
+    if (p->warm_hist < 0 || p->warm_hist > SPHDEM_WARM_HIST_MAX) return SPHDEM_E_ARG;
+    if (p->warm_fit & ~(SPHDEM_FIT_RESIDUAL | SPHDEM_FIT_AFFINE)) return SPHDEM_E_ARG;
     if (p->warm_start != SPHDEM_WARM_PREVIOUS && p->warm_start != SPHDEM_WARM_MLP &&
-        p->warm_start != SPHDEM_WARM_EXTRAPOLATE)
+        p->warm_start != SPHDEM_WARM_EXTRAPOLATE && p->warm_start != SPHDEM_WARM_PROJECT)
         return SPHDEM_E_ARG;
     if (p->warm_start == SPHDEM_WARM_EXTRAPOLATE && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
     if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
@@ -1365,6 +1403,12 @@ extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, S
         p.warm_start = ov->warm_start;
         p.ppe_tol = ov->ppe_tol;
         p.ppe_max_iter = ov->ppe_max_iter;
+        p.warm_hist = ov->warm_hist;
+        p.warm_fit = ov->warm_fit;
+        p.mlp_train_steps = ov->mlp_train_steps;
+        p.mlp_updates = ov->mlp_updates;
+        p.mlp_seed = ov->mlp_seed;
+        p.mlp_lr = ov->mlp_lr;
     }
     if ((r = sphdem_io_check_table((d + "/data.txt").c_str()))) return r;
     SphdemHandle tmp;
@@ -1748,6 +1792,13 @@ extern "C" int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const dou
     if (!h || !ids || !springs || !h->committed) return SPHDEM_E_ARG;
     return h->prec == SPHDEM_PREC_FP64 ? history_t<double>(h, (int32_t*)ids, (double*)springs, true)
                                        : history_t<float>(h, (int32_t*)ids, (double*)springs, true);
+}
+
+extern "C" int sphdem_set_graphs(SphdemHandle* h, int on) {
+    if (!h) return SPHDEM_E_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    h->use_graphs = on ? 1 : 0;
+    return SPHDEM_OK;
 }
 
 extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {

@@ -63,6 +63,7 @@ void sphdem_io_params_default(SphdemParams* p) {
     p->ppe_max_iter = 500;
     p->mlp_train_steps = 500;
     p->mlp_updates = 4;
+    p->warm_hist = 8;
     p->mlp_seed = 0;
     p->mlp_lr = 3e-4;
     p->art_visc_alpha = 0.1;

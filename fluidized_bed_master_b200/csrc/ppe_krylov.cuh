@@ -16,33 +16,81 @@
 // Solvers (Jacobi preconditioner M = diag(d)):
 //   KRYLOV: right-preconditioned BiCGStab (the operator is not symmetric
 //           once the gradient correction or unequal masses enter a_ij);
-//   PCG:    preconditioned conjugate gradients (symmetric operators).
+//   PCG:    preconditioned conjugate gradients in the Chronopoulos-Gear
+//           form, whose three dot products all follow the one
+//           matrix-vector product, so an iteration is two kernels: the
+//           vector update and the product with its dots.
+//           a_ij = m_j s_ij with s_ij symmetric (no gradient correction,
+//           one smoothing length), so A is not symmetric when the masses
+//           differ (they follow the porosity), but M A (M = diag(m)) is
+//           symmetric positive definite.  CG runs on M A p = M b with the
+//           preconditioner diag(M A) = M D, which is the same iteration on
+//           A with every inner product weighted by m_i.
 // Krylov vectors, dot products and norms are FP64; coefficients are R.
+// Coefficient storage: entry k of row i = {j, a_ij} (8 B in the FP32
+// build), solved neighbours only, in slices of 32 rows: the entries of
+// rows 32s..32s+31 are one contiguous block, entry k of the slice's rows
+// adjacent (kent_at), so a warp's load of entry k is one 256-B line pair
+// and a warp's whole row block one contiguous stream.
 // Dot products are reduced deterministically: every block writes a
-// partial sum, and the next kernel adds the partials in a fixed order.
+// partial sum; the kernel that needs the totals (or the last block of the
+// producing kernel) adds the partials in block order.
 // The iteration runs inside the step's CUDA graph as a conditional while
 // node; the last kernel of an iteration decides whether to continue.
 #pragma once
+#include "../../include/sphdem.h"
 #include "step_kernels.cuh"
 
 namespace sphdem {
 
-constexpr int KRY_G = 592;   // blocks of the vector kernels (4 per SM)
+constexpr int KRY_G = 1184;  // blocks of the vector kernels (8 per SM)
 constexpr int KRY_T = 256;
 constexpr int KRY_NPART = 10;
 
 // scalar slots
 enum {
     KS_RHO = 0, KS_RHO_NEW, KS_ALPHA, KS_OMEGA, KS_BNORM, KS_RES, KS_DONE, KS_ITER, KS_RZ, KS_RZ_NEW,
-    KS_TOL, KS_MAXIT, KS_STATUS, KS_RES0, KS_C0, KS_C1, KS_C2, KS_COUNT = 24
+    KS_TOL, KS_MAXIT, KS_STATUS, KS_RES0, KS_C0, KS_C1, KS_C2, KS_BETA, KS_COUNT = 24
 };
 // partial-sum slots
 enum { KP_RHR = 0, KP_RR, KP_RHV, KP_SS, KP_TS, KP_TT, KP_BB, KP_PQ };
 
+// one stored coefficient: {neighbour slot, a_ij}
+template <typename R>
+struct KEnt;
+template <>
+struct KEnt<float> {
+    using T = int2;
+    static __device__ __forceinline__ T make(int j, float a) { return make_int2(j, __float_as_int(a)); }
+    static __device__ __forceinline__ void get(const T& e, int& j, double& a) {
+        j = e.x;
+        a = (double)__int_as_float(e.y);
+    }
+};
+template <>
+struct KEnt<double> {
+    using T = int4;
+    static __device__ __forceinline__ T make(int j, double a) {
+        return make_int4(j, 0, __double2loint(a), __double2hiint(a));
+    }
+    static __device__ __forceinline__ void get(const T& e, int& j, double& a) {
+        j = e.x;
+        a = __hiloint2double(e.w, e.z);
+    }
+};
+
+// slot of entry k of row i (cap entries per row)
+__device__ __forceinline__ size_t kent_at(int i, int k, int cap) {
+    return ((size_t)(i >> 5) * cap + k) * 32 + (i & 31);
+}
+
 template <typename R>
 struct KryWork {
-    R* a;          // cap*ns coefficients a[k*n+i] of list entry k (0: not a solved neighbour)
-    int* kcnt;     // list entries a row uses (0 for rows that are not solved)
+    typename KEnt<R>::T* e;   // entries of the solved neighbours, slot kent_at(i, k, cap)
+    int cap;                  // entries per row
+    int* kcnt;     // 0 for rows that are not solved, else 1 + the row's entries
+    unsigned* ctr; // blocks finished in the current k_cg_spmv (the last one resets it)
+    double* wm;    // m_i of solved rows (0 elsewhere): the weight of the PCG inner products
     double *d, *b, *x, *r, *rh, *p, *v, *s, *t, *y, *z;
     double* part;  // KRY_NPART * KRY_G block partials
     double* sc;    // KS_COUNT scalars
@@ -50,9 +98,17 @@ struct KryWork {
     float* fraw;           // [n][16] raw features (0 on rows that are not solved)
     __nv_bfloat16* feat;   // [n][16] normalised features, the network's input
     double* pprev;         // previous pressure of every row
+    double* x0;            // the projected initial iterate of the solve (training target base)
     float *yp, *target, *weight;
     double* mpart;         // block partials of the feature statistics (33 per block)
     double* mstat;         // mean[16] | var[16] | pressure scale | rows | samples seen | Adam step
+    // projected warm start (nullptr when it is off)
+    float* D;              // [n][PROJ_MP] directions
+    float* hist;           // [SPHDEM_WARM_HIST_MAX][hist_n] solution changes by particle id
+    int hist_n;
+    int* hring;            // {next slot, changes stored}
+    double* ppart;         // PROJ_NV * KRY_G block partials
+    double* pc;            // PROJ_MAX coefficients, directions kept, c.h
 };
 
 // learned warm start statistics slots
@@ -108,6 +164,7 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
     V4<R> upi = rec.up[i];
     if (!kry_solve_row(P, it, pt, bt)) {
         K.kcnt[i] = 0;
+        K.wm[i] = 0.0;
         K.d[i] = 1.0;
         K.b[i] = 0.0;
         K.x[i] = 0.0;
@@ -136,6 +193,7 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
     int np = 0;
     const int* __restrict__ nb = W.nbr;
     int k = 0;
+    typename KEnt<R>::T* __restrict__ ent = K.e;
     nb_walk<2, NbQ44<R>>(
         cnt, nb, n, i,
         [&](int j) {
@@ -147,7 +205,6 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
         },
         [&](int j, const NbQ44<R>& t) {
             int tj = t.q.w;
-            R acoef = 0;
             if (!(tag_ptype(tj) >= 1000 || tag_itype(tj) == 4)) {
                 const V4<R>& fj = t.a;
                 const V4<R>& uj = t.b;
@@ -165,8 +222,12 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
                 R c = -(g.dx * gx + g.dy * gy + g.dz * gz) * rinv * rinv;
                 R a = mj * ((prhoi + porj * rhoj) * irj * irhoi) * c;
                 dsum += (double)a;
-                if (kry_solve_row(P, tag_itype(tj), tag_ptype(tj), tag_btype(tj))) acoef = a;
-                else bfix += (double)a * (double)uj.w;
+                if (kry_solve_row(P, tag_itype(tj), tag_ptype(tj), tag_btype(tj))) {
+                    ent[kent_at(i, k, K.cap)] = KEnt<R>::make(j, a);
+                    k++;
+                } else {
+                    bfix += (double)a * (double)uj.w;
+                }
                 double pj = (double)uj.w;
                 apsum += (double)a * pj;
                 pmean += pj;
@@ -174,13 +235,12 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
                 pmax = fmax(pmax, pj);
                 np++;
             }
-            K.a[(size_t)k * n + i] = acoef;
-            k++;
         });
     R bdiv = (R)P.rho_gas * (bx + by + bz) / (R)P.sdt;
     R bpor = (R)P.rho_gas * ((R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
     R bsrc = (R)P.rho_gas * (bx + by + bz + (R)2 * S.dDEMpor[i] - W.dDEMpor_prev[i]) / (R)P.sdt;
-    K.kcnt[i] = cnt;
+    K.kcnt[i] = k + 1;
+    K.wm[i] = (double)fi.x;
     K.d[i] = dsum;
     K.b[i] = (double)bsrc + bfix;
     K.x[i] = (double)upi.w + (extrapolate ? (double)S.dpres[i] : 0.0);
@@ -216,6 +276,44 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
     }
 }
 
+// y_i = d_i x_i - sum_k a_ik x_j(k) over the stored entries of row i, in
+// list order.  Software pipelined: the entries of the next group of eight
+// load while the current group's gathers are in flight.
+template <typename R>
+__device__ __forceinline__ double kry_row(const KryWork<R>& K, int n, int i, int cnt, const double* __restrict__ xin) {
+    using E = KEnt<R>;
+    using T = typename E::T;
+    const T* __restrict__ ent = K.e + kent_at(i, 0, K.cap);   // entry k at ent[32 k]
+    constexpr int B = 8;
+    T cur[B], nxt[B];
+#pragma unroll
+    for (int q = 0; q < B; q++)
+        if (q < cnt) cur[q] = __ldg(ent + (size_t)q * 32);
+    double acc = 0;
+    for (int k = 0; k < cnt; k += B) {
+#pragma unroll
+        for (int q = 0; q < B; q++)
+            if (k + B + q < cnt) nxt[q] = __ldg(ent + (size_t)(k + B + q) * 32);
+        double xv[B], av[B];
+#pragma unroll
+        for (int q = 0; q < B; q++) {
+            xv[q] = 0.0;
+            av[q] = 0.0;
+            if (k + q < cnt) {
+                int j;
+                E::get(cur[q], j, av[q]);
+                xv[q] = __ldg(xin + j);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < B; q++)
+            if (k + q < cnt) acc += av[q] * xv[q];
+#pragma unroll
+        for (int q = 0; q < B; q++) cur[q] = nxt[q];
+    }
+    return K.d[i] * xin[i] - acc;
+}
+
 // y = A x over the stored coefficients; optional fused dots
 // part[s0] += w0.y, part[s1] += w1.y (w1 == nullptr: y.y)
 template <typename R>
@@ -224,24 +322,12 @@ __global__ void __launch_bounds__(KRY_T) k_kry_spmv(int n, KryWork<R> K, const i
                                                     const double* __restrict__ w0, int s0, const double* w1, int s1,
                                                     int two) {
     __shared__ double sm[32];
+    (void)nb;
     if (K.sc[KS_DONE] != 0.0) return;
     double d0 = 0, d1 = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int cnt = K.kcnt[i];
-        double acc = 0;
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4) {
-            int j0 = __ldg(nb + (size_t)k * n + i), j1 = __ldg(nb + (size_t)(k + 1) * n + i);
-            int j2 = __ldg(nb + (size_t)(k + 2) * n + i), j3 = __ldg(nb + (size_t)(k + 3) * n + i);
-            R a0 = __ldg(K.a + (size_t)k * n + i), a1 = __ldg(K.a + (size_t)(k + 1) * n + i);
-            R a2 = __ldg(K.a + (size_t)(k + 2) * n + i), a3 = __ldg(K.a + (size_t)(k + 3) * n + i);
-            acc += (double)a0 * xin[j0];
-            acc += (double)a1 * xin[j1];
-            acc += (double)a2 * xin[j2];
-            acc += (double)a3 * xin[j3];
-        }
-        for (; k < cnt; k++) acc += (double)__ldg(K.a + (size_t)k * n + i) * xin[__ldg(nb + (size_t)k * n + i)];
-        double y = cnt ? K.d[i] * xin[i] - acc : 0.0;
+        double y = cnt ? kry_row<R>(K, n, i, cnt - 1, xin) : 0.0;
         yout[i] = y;
         d0 += w0[i] * y;
         if (two) d1 += (w1 ? w1[i] : y) * y;
@@ -367,45 +453,142 @@ __global__ void __launch_bounds__(KRY_T) k_bicg_x(int n, const double* __restric
     if (blockIdx.x == 0 && threadIdx.x == 0) sc[KS_OMEGA] = om;
 }
 
-// ---- PCG iteration --------------------------------------------------------
-// C2: alpha = rz/(p.q); x += alpha p; r -= alpha q; z = r/d; part: r.z, r.r
-__global__ void __launch_bounds__(KRY_T) k_cg_x(int n, const double* __restrict__ d, const double* __restrict__ p,
-                                                const double* __restrict__ q, double* x, double* r, double* z,
-                                                double* part, double* sc) {
-    __shared__ double sm[32];
-    if (sc[KS_DONE] != 0.0) return;
-    double pq = part_total(part, KP_PQ, sm);
-    if (!(pq != 0.0) || !isfinite(pq)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            sc[KS_DONE] = 1.0;
-            sc[KS_STATUS] = 2.0;
-        }
-        return;
+// ---- PCG iteration (Chronopoulos-Gear) ----------------------------------
+// With u = M^-1 r and w = A u, one iteration is
+//     p = u + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;
+//     u = M^-1 r;  w = A u;  gamma = r.u, delta = w.u, rho = r.r;
+//     beta' = gamma/gamma_old;  alpha' = gamma / (delta - beta' gamma/alpha)
+// (alpha = gamma/delta, beta = 0 at the start).  The iterates equal those
+// of the textbook recurrences in exact arithmetic.
+enum { KP_G = 0, KP_D = 1, KP_R = 2, KP_B = 3 };
+
+// r = b - y, u = r/d, p = s = 0; the tolerance and the iteration cap
+__global__ void __launch_bounds__(KRY_T) k_cg_init(int n, const double* __restrict__ d, const double* __restrict__ b,
+                                                   const double* __restrict__ y, double* r, double* u, double* p,
+                                                   double* s, double* sc, double tol, int maxit) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc[KS_TOL] = tol;
+        sc[KS_MAXIT] = (double)maxit;
     }
-    double alpha = sc[KS_RZ] / pq;
-    double a0 = 0, a1 = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        double ri = r[i] - alpha * q[i];
+        double ri = b[i] - y[i];
         r[i] = ri;
-        double zi = ri / d[i];
-        z[i] = zi;
-        a0 += ri * zi;
-        a1 += ri * ri;
+        u[i] = ri / d[i];
+        p[i] = 0.0;
+        s[i] = 0.0;
     }
-    part_store(part, KP_RHR, a0, sm);
-    part_store(part, KP_RR, a1, sm);
 }
 
-// C3: beta = rz'/rz; p = z + beta p
-__global__ void __launch_bounds__(KRY_T) k_cg_p(int n, const double* __restrict__ z, double* p, double* part,
-                                                double* sc) {
-    __shared__ double sm[32];
+// p = u + beta p; s = w + beta s; x += alpha p; r -= alpha s; u = r/d
+__global__ void __launch_bounds__(KRY_T) k_cg_upd(int n, const double* __restrict__ d, double* u,
+                                                  const double* __restrict__ w, double* p, double* s, double* x,
+                                                  double* r, const double* sc) {
     if (sc[KS_DONE] != 0.0) return;
-    double rz_new = part_total(part, KP_RHR, sm);
-    double beta = rz_new / sc[KS_RZ];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + beta * p[i];
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc[KS_RZ_NEW] = rz_new;
+    const double al = sc[KS_ALPHA], be = sc[KS_BETA];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double pi = u[i] + be * p[i];
+        double si = w[i] + be * s[i];
+        p[i] = pi;
+        s[i] = si;
+        x[i] += al * pi;
+        double ri = r[i] - al * si;
+        r[i] = ri;
+        u[i] = ri / d[i];
+    }
+}
+
+// w = A u with the partials of the m-weighted r.u and w.u, and of r.r
+// (and b.b on the first call);
+// the last block to finish adds the partials in block order and advances
+// the scalars: the residual, the stop decision (and the while node's
+// condition), alpha and beta of the next update
+template <typename R>
+__global__ void __launch_bounds__(KRY_T) k_cg_spmv(int n, KryWork<R> K, const double* __restrict__ u,
+                                                   double* __restrict__ w, const double* __restrict__ r,
+                                                   const double* __restrict__ b, int first,
+                                                   cudaGraphConditionalHandle h, int in_graph) {
+    __shared__ double sm[32];
+    __shared__ int last;
+    double* sc = K.sc;
+    if (sc[KS_DONE] != 0.0) {
+        if (in_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+        return;
+    }
+    double g = 0, dl = 0, rr = 0, bb = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int cnt = K.kcnt[i];
+        double ui = u[i];
+        double wi = cnt ? kry_row<R>(K, n, i, cnt - 1, u) : 0.0;
+        w[i] = wi;
+        double ri = r[i], mi = K.wm[i];
+        g += mi * ri * ui;
+        dl += mi * wi * ui;
+        rr += ri * ri;
+        if (first) bb += b[i] * b[i];
+    }
+    part_store(K.part, KP_G, g, sm);
+    part_store(K.part, KP_D, dl, sm);
+    part_store(K.part, KP_R, rr, sm);
+    if (first) part_store(K.part, KP_B, bb, sm);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(K.ctr, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // totals in block order (the partials bypass L1: other SMs wrote them)
+    double tot[4];
+    for (int q = 0; q < (first ? 4 : 3); q++) {
+        double v = 0;
+        for (int k = threadIdx.x; k < gridDim.x; k += blockDim.x) v += __ldcg(K.part + q * KRY_G + k);
+        tot[q] = block_sum(v, sm);
+    }
+    if (threadIdx.x != 0) return;
+    *K.ctr = 0u;
+    const double gam = tot[KP_G], del = tot[KP_D], rho = tot[KP_R];
+    bool done;
+    if (first) {
+        double bn = sqrt(tot[KP_B]);
+        sc[KS_BNORM] = bn;
+        sc[KS_ITER] = 0;
+        sc[KS_STATUS] = 0;
+        double res = bn > 0 ? sqrt(rho) / bn : 0.0;
+        sc[KS_RES] = res;
+        sc[KS_RES0] = res;
+        done = bn == 0.0 || res <= sc[KS_TOL] || sc[KS_MAXIT] <= 0;
+        if (!done && (!(del != 0.0) || !isfinite(del))) {
+            sc[KS_STATUS] = 2.0;
+            done = true;
+        }
+        if (!done) {
+            sc[KS_ALPHA] = gam / del;
+            sc[KS_BETA] = 0.0;
+            sc[KS_RZ] = gam;
+        }
+    } else {
+        double it = sc[KS_ITER] + 1.0;
+        sc[KS_ITER] = it;
+        double res = sqrt(rho) / sc[KS_BNORM];
+        sc[KS_RES] = res;
+        done = true;
+        if (!isfinite(res)) sc[KS_STATUS] = 2.0;
+        else if (res <= sc[KS_TOL]) {
+        } else if (it >= sc[KS_MAXIT]) sc[KS_STATUS] = 1.0;   // iteration cap
+        else {
+            double be = gam / sc[KS_RZ];
+            double den = del - be * gam / sc[KS_ALPHA];
+            if (!(den != 0.0) || !isfinite(den)) sc[KS_STATUS] = 2.0;
+            else {
+                sc[KS_BETA] = be;
+                sc[KS_ALPHA] = gam / den;
+                sc[KS_RZ] = gam;
+                done = false;
+            }
+        }
+    }
+    if (done) sc[KS_DONE] = 1.0;
+    if (in_graph) cudaGraphSetConditional(h, done ? 0u : 1u);
 }
 
 // last kernel of an iteration (one block): residual, iteration count, and
@@ -436,7 +619,7 @@ __global__ void __launch_bounds__(KRY_T) k_kry_check(double* part, double* sc, c
 
 // ---- learned warm start: statistics, normalisation, targets ---------------
 // Block partials over the solved rows (kcnt > 0): mode 0 sums the raw
-// features and their squares; mode 1 sums (x - p_prev)^2 of the solution.
+// features and their squares; mode 1 sums (x - x0)^2 of the solution.
 template <typename R>
 __global__ void __launch_bounds__(KRY_T) k_mlp_stats(int n, KryWork<R> K, int mode) {
     __shared__ double sm[32];
@@ -455,7 +638,7 @@ __global__ void __launch_bounds__(KRY_T) k_mlp_stats(int n, KryWork<R> K, int mo
                 acc[MLP_FEAT + q] += v * v;
             }
         } else {
-            double dp = K.x[i] - K.pprev[i];
+            double dp = K.x[i] - K.x0[i];
             acc[2 * MLP_FEAT + 1] += dp * dp;
         }
     }
@@ -518,109 +701,234 @@ __global__ void k_mlp_x0(int n, KryWork<R> K) {
     K.x[i] = K.pprev[i] + K.mstat[MS_PS] * (double)K.yp[i];
 }
 
-// training pairs: target = (x - p_prev) / scale, weight = 1 / rows on solved rows
+// training pairs: target = (x - x0) / scale, the part of the solution that
+// the projection without the network missed; weight = 1 / rows on solved rows
 template <typename R>
 __global__ void k_mlp_targets(int n, KryWork<R> K) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     bool on = K.kcnt[i] > 0;
     double rows = K.mstat[MS_ROWS];
-    K.target[i] = on ? (float)((K.x[i] - K.pprev[i]) / K.mstat[MS_PS]) : 0.f;
+    K.target[i] = on ? (float)((K.x[i] - K.x0[i]) / K.mstat[MS_PS]) : 0.f;
     K.weight[i] = (on && rows > 0) ? (float)(1.0 / rows) : 0.f;
 }
 
 __global__ void k_mlp_tick(double* mstat) { mstat[MS_T] += 1.0; }
 
-// ---- minimal-residual blend of the initial iterate ---------------------------
-// x0 = p_prev + sum_k c_k d_k with the directions d0 = the network's
-// predicted change (scale * y), d1 = the last pressure change, d2 = the
-// one-sweep increment; c minimises ||r0 - sum_k c_k A d_k|| with
-// r0 = b - A p_prev, so x0 is never worse (in residual) than p_prev.
-constexpr int BLEND_N = 3;
+// ---- projected initial iterate (warm starts PROJECT and MLP) ---------------
+// x0 = sum_q c_q d_q over the directions
+//     d0 = the previous pressure, d1 = D^-1 (b - A d0) (the one-sweep
+//     increment), d2 = the network's predicted change (MLP in use, else 0),
+//     d3.. = the last warm_hist solution changes, newest first,
+// with c from the Galerkin equations (D^T M A D) c = D^T M b (the optimal
+// combination in the norm of the symmetric operator M A, never worse than
+// d0 alone in that norm), or (warm_fit RESIDUAL) from the least-squares equations
+// (AD)^T (AD) c = (AD)^T b.  With warm_fit AFFINE, c0 = 1 and the other
+// directions are fitted to r0 = b - A d0.  Directions
+// are FP32 rows of PROJ_MP floats (one 48-B gather per list entry for all
+// of them); their products with A and the dots are FP64.  Directions that
+// are zero or dependent are dropped from the system.
+constexpr int PROJ_MAX = 3 + SPHDEM_WARM_HIST_MAX;   // 11
+constexpr int PROJ_MP = 12;                          // floats per direction row
+constexpr int PROJ_NG = PROJ_MAX * (PROJ_MAX + 1) / 2;
+constexpr int PROJ_NV = PROJ_NG + PROJ_MAX;          // upper triangle of G, then h
+
 template <typename R>
-__global__ void k_blend_dirs(int n, KryWork<R> K, const R* __restrict__ dpres, double* d0, double* d1, double* d2) {
+__global__ void k_proj_dirs(int n, KryWork<R> K, const int* __restrict__ pid, int nhist, int use_mlp) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     bool on = K.kcnt[i] > 0;
-    d0[i] = on ? K.mstat[MS_PS] * (double)K.yp[i] : 0.0;
-    d1[i] = on ? (double)dpres[i] : 0.0;
-    d2[i] = on ? (double)K.fraw[(size_t)i * MLP_FEAT + 2] : 0.0;
-}
-// r0 = b - A p_prev (A p_prev in y); block partials of (Ad_k, Ad_l), (Ad_k, r0)
-__global__ void __launch_bounds__(KRY_T) k_blend_dots(int n, const double* __restrict__ b, const double* __restrict__ y,
-                                                      const double* __restrict__ a0, const double* __restrict__ a1,
-                                                      const double* __restrict__ a2, double* part) {
-    __shared__ double sm[32];
-    double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double r0 = b[i] - y[i], u0 = a0[i], u1 = a1[i], u2 = a2[i];
-        g[0] += u0 * u0; g[1] += u0 * u1; g[2] += u0 * u2;
-        g[3] += u1 * u1; g[4] += u1 * u2; g[5] += u2 * u2;
-        g[6] += u0 * r0; g[7] += u1 * r0; g[8] += u2 * r0;
+    float d[PROJ_MP];
+#pragma unroll
+    for (int q = 0; q < PROJ_MP; q++) d[q] = 0.f;
+    if (on) {
+        d[0] = (float)K.x[i];
+        d[1] = (float)((K.b[i] - K.y[i]) / K.d[i]);
+        if (use_mlp) d[2] = (float)(K.mstat[MS_PS] * (double)K.yp[i]);
+        const int slot = K.hring[0], have = min(K.hring[1], nhist), p = pid[i];
+        for (int k = 0; k < have; k++) {
+            int s = (slot - 1 - k + SPHDEM_WARM_HIST_MAX) % SPHDEM_WARM_HIST_MAX;
+            d[3 + k] = K.hist[(size_t)s * K.hist_n + p];
+        }
     }
-    for (int q = 0; q < 9; q++) {
-        double t = block_sum(g[q], sm);
-        if (threadIdx.x == 0) part[q * KRY_G + blockIdx.x] = t;
-    }
+    float4* o = reinterpret_cast<float4*>(K.D + (size_t)i * PROJ_MP);
+#pragma unroll
+    for (int q = 0; q < PROJ_MP / 4; q++) o[q] = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
 }
-// one block: totals, then the 3x3 least-squares solve (Gaussian elimination
-// with a relative Tikhonov floor on the diagonal); c = 0 for a degenerate set
-__global__ void __launch_bounds__(KRY_T) k_blend_solve(const double* part, double* sc) {
-    __shared__ double sm[32];
-    __shared__ double g[9];
-    for (int q = 0; q < 9; q++) {
-        double t = part_total(part, q, sm);
-        if (threadIdx.x == 0) g[q] = t;
+
+// (A d_q)_i for every direction in one pass over the stored coefficients,
+// and the block partials of G (upper triangle) and h.  Each thread stages
+// its row's products in shared memory; then thread v < PROJ_NV forms value
+// v over the block's rows in row order: deterministic, no shuffles.
+constexpr int PROJ_T = 128;
+template <typename R>
+__global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int fit) {
+    using E = KEnt<R>;
+    const bool least_squares = fit & SPHDEM_FIT_RESIDUAL, affine = fit & SPHDEM_FIT_AFFINE;
+    __shared__ double su[PROJ_T][PROJ_MAX + 1];   // left factors (+ b or r0)
+    __shared__ double sa[PROJ_T][PROJ_MAX];       // A d_q
+    const float4* __restrict__ D4 = reinterpret_cast<const float4*>(K.D);
+    const typename E::T* __restrict__ ent = K.e;
+    double accv = 0.0;   // value threadIdx.x of this block
+    int vk = 0, vq = 0;  // (k, q) of an upper-triangle value
+    if (threadIdx.x < PROJ_NG) {
+        int v = threadIdx.x;
+        while (v >= PROJ_MAX - vk) { v -= PROJ_MAX - vk; vk++; }
+        vq = vk + v;
+    }
+    for (int i0 = blockIdx.x * PROJ_T; i0 < n; i0 += gridDim.x * PROJ_T) {
+        const int i = i0 + threadIdx.x;
+        double ad[PROJ_MAX], dv[PROJ_MAX], bi = 0;
+#pragma unroll
+        for (int q = 0; q < PROJ_MAX; q++) ad[q] = dv[q] = 0.0;
+        int cnt = i < n ? K.kcnt[i] : 0;
+        if (cnt) {
+            float4 a0 = D4[(size_t)i * 3], a1 = D4[(size_t)i * 3 + 1], a2 = D4[(size_t)i * 3 + 2];
+            float di[PROJ_MP] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+            const double dg = K.d[i];
+#pragma unroll
+            for (int q = 0; q < PROJ_MAX; q++) {
+                dv[q] = (double)di[q];
+                ad[q] = dg * dv[q];
+            }
+            for (int k = 0; k < cnt - 1; k++) {
+                int j;
+                double a;
+                E::get(__ldg(ent + kent_at(i, k, K.cap)), j, a);
+                float4 b0 = __ldg(D4 + (size_t)j * 3), b1 = __ldg(D4 + (size_t)j * 3 + 1), b2 = __ldg(D4 + (size_t)j * 3 + 2);
+                float dj[PROJ_MP] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+#pragma unroll
+                for (int q = 0; q < PROJ_MAX; q++) ad[q] -= a * (double)dj[q];
+            }
+            bi = affine ? K.b[i] - K.y[i] : K.b[i];   // y = A p_prev
+            if (affine) dv[0] = ad[0] = 0.0;          // p_prev is not fitted
+            // Galerkin: the m-weighted products (M A is the symmetric operator)
+            if (!least_squares) {
+                const double wgt = K.wm[i];
+#pragma unroll
+                for (int q = 0; q < PROJ_MAX; q++) dv[q] *= wgt;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PROJ_MAX; q++) {
+            su[threadIdx.x][q] = least_squares ? ad[q] : dv[q];
+            sa[threadIdx.x][q] = ad[q];
+        }
+        su[threadIdx.x][PROJ_MAX] = bi;
+        __syncthreads();
+        if (threadIdx.x < PROJ_NG) {
+            for (int r = 0; r < PROJ_T; r++) accv += su[r][vk] * sa[r][vq];
+        } else if (threadIdx.x < PROJ_NV) {
+            const int k = threadIdx.x - PROJ_NG;
+            for (int r = 0; r < PROJ_T; r++) accv += su[r][k] * su[r][PROJ_MAX];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < PROJ_NV) K.ppart[(size_t)threadIdx.x * KRY_G + blockIdx.x] = accv;
+}
+
+// one block: totals in block order (thread v adds value v), then the
+// reduced system of the kept directions (Gaussian elimination with partial
+// pivoting and a relative ridge of 1e-12 trace); c = e0 (the previous
+// pressure) if it fails
+template <typename R>
+__global__ void __launch_bounds__(KRY_T) k_proj_solve(KryWork<R> K, int nblk) {
+    __shared__ double tot[PROJ_NV];
+    if (threadIdx.x < PROJ_NV) {
+        const double* pv = K.ppart + (size_t)threadIdx.x * KRY_G;
+        double t = 0;
+        for (int k = 0; k < nblk; k++) t += pv[k];
+        tot[threadIdx.x] = t;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    double A[3][4] = {{g[0], g[1], g[2], g[6]}, {g[1], g[3], g[4], g[7]}, {g[2], g[4], g[5], g[8]}};
-    double tr = g[0] + g[3] + g[5];
-    double c[3] = {0, 0, 0};
-    if (tr > 0 && isfinite(tr)) {
-        for (int k = 0; k < 3; k++) A[k][k] += 1e-12 * tr;
-        bool ok = true;
-        for (int k = 0; k < 3 && ok; k++) {
-            int piv = k;
-            for (int r = k + 1; r < 3; r++)
-                if (fabs(A[r][k]) > fabs(A[piv][k])) piv = r;
-            if (!(fabs(A[piv][k]) > 0)) { ok = false; break; }
-            for (int q = 0; q < 4; q++) { double t = A[k][q]; A[k][q] = A[piv][q]; A[piv][q] = t; }
-            for (int r = k + 1; r < 3; r++) {
-                double f = A[r][k] / A[k][k];
-                for (int q = k; q < 4; q++) A[r][q] -= f * A[k][q];
-            }
-        }
-        if (ok) {
-            for (int k = 2; k >= 0; k--) {
-                double t = A[k][3];
-                for (int q = k + 1; q < 3; q++) t -= A[k][q] * c[q];
-                c[k] = t / A[k][k];
-            }
-            if (!(isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2]))) c[0] = c[1] = c[2] = 0;
+    double G[PROJ_MAX][PROJ_MAX], h[PROJ_MAX], c[PROJ_MAX];
+    int v = 0;
+    for (int k = 0; k < PROJ_MAX; k++)
+        for (int q = k; q < PROJ_MAX; q++, v++) G[k][q] = G[q][k] = tot[v];
+    double gmax = 0;
+    for (int k = 0; k < PROJ_MAX; k++) {
+        h[k] = tot[PROJ_NG + k];
+        c[k] = 0;
+        gmax = fmax(gmax, fabs(G[k][k]));
+    }
+    // kept directions: a diagonal above 1e-14 of the largest
+    int idx[PROJ_MAX], m = 0;
+    for (int k = 0; k < PROJ_MAX; k++)
+        if (G[k][k] > 1e-14 * gmax && isfinite(G[k][k])) idx[m++] = k;
+    double M[PROJ_MAX][PROJ_MAX + 1];
+    double tr = 0;
+    for (int a = 0; a < m; a++) tr += G[idx[a]][idx[a]];
+    for (int a = 0; a < m; a++) {
+        for (int b = 0; b < m; b++) M[a][b] = G[idx[a]][idx[b]];
+        M[a][a] += 1e-12 * tr;
+        M[a][m] = h[idx[a]];
+    }
+    bool ok = m > 0 && tr > 0 && isfinite(tr);
+    for (int k = 0; k < m && ok; k++) {
+        int piv = k;
+        for (int r = k + 1; r < m; r++)
+            if (fabs(M[r][k]) > fabs(M[piv][k])) piv = r;
+        if (!(fabs(M[piv][k]) > 0)) { ok = false; break; }
+        for (int q = 0; q <= m; q++) { double t = M[k][q]; M[k][q] = M[piv][q]; M[piv][q] = t; }
+        for (int r = k + 1; r < m; r++) {
+            double f = M[r][k] / M[k][k];
+            for (int q = k; q <= m; q++) M[r][q] -= f * M[k][q];
         }
     }
-    sc[KS_C0] = c[0];
-    sc[KS_C1] = c[1];
-    sc[KS_C2] = c[2];
-}
-template <typename R>
-__global__ void k_blend_apply(int n, KryWork<R> K, const double* __restrict__ d0, const double* __restrict__ d1,
-                              const double* __restrict__ d2) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || K.kcnt[i] == 0) return;
-    K.x[i] = K.pprev[i] + K.sc[KS_C0] * d0[i] + K.sc[KS_C1] * d1[i] + K.sc[KS_C2] * d2[i];
+    double x[PROJ_MAX];
+    if (ok) {
+        for (int k = m - 1; k >= 0; k--) {
+            double t = M[k][m];
+            for (int q = k + 1; q < m; q++) t -= M[k][q] * x[q];
+            x[k] = t / M[k][k];
+            ok = ok && isfinite(x[k]);
+        }
+    }
+    double gain = 0;
+    if (ok)
+        for (int a = 0; a < m; a++) {
+            c[idx[a]] = x[a];
+            gain += x[a] * h[idx[a]];
+        }
+    else c[0] = 1.0;   // (an affine fit keeps p_prev whatever c0 is)
+    for (int k = 0; k < PROJ_MAX; k++) K.pc[k] = c[k];
+    K.pc[PROJ_MAX] = ok ? m : 0;   // diagnostics: directions kept, c.h
+    K.pc[PROJ_MAX + 1] = gain;
 }
 
-// p_new = x on solved rows, the current pressure elsewhere
+// x0 = c0 p_prev (FP64) + sum_{q>0} c_q d_q   (c0 = 1 for an affine fit)
+template <typename R>
+__global__ void k_proj_apply(int n, KryWork<R> K, int fit) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || K.kcnt[i] == 0) return;
+    const float* d = K.D + (size_t)i * PROJ_MP;
+    double x = ((fit & SPHDEM_FIT_AFFINE) ? 1.0 : K.pc[0]) * K.x[i];
+#pragma unroll
+    for (int q = 1; q < PROJ_MAX; q++) x += K.pc[q] * (double)d[q];
+    K.x[i] = x;
+    if (K.x0) K.x0[i] = x;
+}
+
+// advance the ring of solution changes after k_kry_final wrote the newest
+__global__ void k_proj_ring(int* hring) {
+    hring[0] = (hring[0] + 1) % SPHDEM_WARM_HIST_MAX;
+    hring[1] = min(hring[1] + 1, SPHDEM_WARM_HIST_MAX);
+}
+
+// p_new = x on solved rows, the current pressure elsewhere; the change
+// also goes into the ring of solution changes (by particle id) when the
+// projected warm start keeps one
 template <typename R>
 __global__ void __launch_bounds__(128) k_kry_final(DevParams P, SphState<R> S, SphWork<R> W, KryWork<R> K) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.ns) return;
     bool solve = kry_solve_row(P, S.itype[i], S.ptype[i], S.btype[i]);
     R pold = W.rec.up[i].w;
+    double dp = solve ? K.x[i] - (double)pold : 0.0;
     W.p_new[i] = solve ? (R)K.x[i] : pold;
-    S.dpres[i] = solve ? (R)(K.x[i] - (double)pold) : (R)0;
+    S.dpres[i] = (R)dp;
+    if (K.hist) K.hist[(size_t)K.hring[0] * K.hist_n + S.pid[i]] = (float)dp;
 }
 
 }  // namespace sphdem

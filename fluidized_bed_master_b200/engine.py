@@ -48,6 +48,7 @@ def lib():
     L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
     L.sphdem_set_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
+    L.sphdem_set_graphs.argtypes = [vp, C.c_int]
     L.sphdem_collect_timing.argtypes = [vp]
     L.sphdem_get_timing.argtypes = [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_double), P(C.c_int64)]
     L.sphdem_input_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
@@ -223,6 +224,10 @@ class Engine:
 
     def set_timing(self, on):
         _chk(lib().sphdem_set_timing(self._h, int(bool(on))), "sphdem_set_timing")
+
+    def set_graphs(self, on):
+        """Step graphs on/off (off: kernel profilers see every launch)."""
+        _chk(lib().sphdem_set_graphs(self._h, int(bool(on))), "sphdem_set_graphs")
 
     def collect_timing(self):
         _chk(lib().sphdem_collect_timing(self._h), "sphdem_collect_timing")

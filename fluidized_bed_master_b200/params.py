@@ -17,7 +17,7 @@ _I32 = [
     "turbulence_model", "concn_solve", "min_iteration", "max_iteration",
     "penetration_solve", "switch_ptype", "noslip_bc", "decouple_stride",
     "ppe_mode", "warm_start", "ppe_max_iter", "precision", "dem_wall_mask",
-    "mlp_train_steps", "mlp_updates", "mlp_seed",
+    "mlp_train_steps", "mlp_updates", "mlp_seed", "warm_hist", "warm_fit",
 ]
 _F64_A = [
     "kappa", "p_ref", "gamma", "dt", "time", "time_end",
@@ -34,7 +34,7 @@ _F64_B = [
 _F64_C = ["cone_r1", "cone_r2", "cone_h", "wall_rest_n", "wall_rest_s", "wall_mu_s", "wall_mu_rs"]
 
 _fields = [(n, C.c_int32) for n in _I32]
-_fields += [("reserved_i", C.c_int32 * 3)]
+_fields += [("reserved_i", C.c_int32 * 1)]
 _fields += [(n, C.c_double) for n in _F64_A]
 _fields += [("margin", C.c_double * 6)]
 _fields += [(n, C.c_double) for n in _F64_B]
@@ -70,13 +70,16 @@ class SphdemStats(C.Structure):
         ("ppe_status", C.c_int32), ("mlp_phase", C.c_int32), ("mlp_loss", C.c_double),
         ("mlp_trained_steps", C.c_int32), ("reserved_stats", C.c_int32),
         ("ppe_initial_residual", C.c_double),
+        ("ppe_warm_gain", C.c_double), ("ppe_warm_dirs", C.c_int32), ("reserved_stats2", C.c_int32),
     ]
 
 
 # PPE modes and warm starts (SPHDEM_PPE_*, SPHDEM_WARM_*)
 PPE_REFERENCE, PPE_KRYLOV, PPE_PCG = 0, 1, 2
 WCSPH, ISPH = 0, 1
-WARM_PREVIOUS, WARM_MLP, WARM_EXTRAPOLATE = 0, 1, 2
+WARM_PREVIOUS, WARM_MLP, WARM_EXTRAPOLATE, WARM_PROJECT = 0, 1, 2, 3
+WARM_HIST_MAX = 8
+FIT_RESIDUAL, FIT_AFFINE = 1, 2
 
 
 # field ids (enum SphdemField)
@@ -128,6 +131,7 @@ def reference_params():
     p.decouple_stride = 1
     p.ppe_max_iter = 500
     p.mlp_train_steps = 500
+    p.warm_hist = 8
     p.mlp_updates = 4
     p.mlp_lr = 3e-4
     p.art_visc_alpha = 0.1

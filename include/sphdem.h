@@ -63,14 +63,31 @@ extern "C" {
 #define SPHDEM_PPE_KRYLOV    1
 #define SPHDEM_PPE_PCG       2
 
-/* Initial iterate of the KRYLOV/PCG modes: the previous pressure, or the
- * learned MLP (trained on the solver's own solutions during the first
- * mlp_train_steps steps, which start from the previous pressure; after
- * that the network predicts the pressure change and the solver still
- * converges to ppe_tol, so results do not depend on the prediction). */
+/* Initial iterate of the KRYLOV/PCG modes.
+ *   PREVIOUS:    the previous pressure.
+ *   EXTRAPOLATE: the previous pressure plus its last change.
+ *   PROJECT:     the best combination of the directions {previous
+ *                pressure, its one-sweep Jacobi increment, the last
+ *                warm_hist pressure changes}: A-norm optimal (Galerkin)
+ *                for PCG, minimal residual for KRYLOV.  Never worse than
+ *                PREVIOUS in that norm.
+ *   MLP:         PROJECT plus one more direction, the learned MLP's
+ *                prediction of what PROJECT misses (x - x0).  The network
+ *                trains on the solver's own solutions during the first
+ *                mlp_train_steps steps (which use PROJECT).
+ * The solver still converges to ppe_tol from any of them, so results do
+ * not depend on the initial iterate beyond that tolerance. */
 #define SPHDEM_WARM_PREVIOUS    0
 #define SPHDEM_WARM_MLP         1
-#define SPHDEM_WARM_EXTRAPOLATE 2   /* previous pressure + its last change */
+#define SPHDEM_WARM_EXTRAPOLATE 2
+#define SPHDEM_WARM_PROJECT     3
+#define SPHDEM_WARM_HIST_MAX    8   /* largest warm_hist */
+/* warm_fit: how the projected initial iterate weighs its directions.
+ * RESIDUAL: least squares on the residual (default: A-norm, Galerkin);
+ * AFFINE: the previous pressure keeps coefficient 1 and only the other
+ * directions are fitted (to r0 = b - A p_prev). */
+#define SPHDEM_FIT_RESIDUAL     1
+#define SPHDEM_FIT_AFFINE       2
 
 /* Precision of the non-position fields inside the engine. */
 #define SPHDEM_PREC_FP32 0
@@ -124,10 +141,12 @@ typedef struct SphdemParams {
     int32_t ppe_max_iter;       /* KRYLOV iteration cap                  */
     int32_t precision;          /* SPHDEM_PREC_* (engine extension)      */
     int32_t dem_wall_mask;      /* bit0 cylinder_z, bit1 box_z, bit2 truncated_cone_z */
-    int32_t mlp_train_steps;    /* WARM_MLP: steps that train the network (plain warm start) */
+    int32_t mlp_train_steps;    /* WARM_MLP: steps that train the network (projected warm start) */
     int32_t mlp_updates;        /* WARM_MLP: Adam steps per training step */
     int32_t mlp_seed;           /* WARM_MLP: initialisation seed */
-    int32_t reserved_i[3];
+    int32_t warm_hist;          /* WARM_PROJECT/MLP: previous pressure changes used (0..SPHDEM_WARM_HIST_MAX) */
+    int32_t warm_fit;           /* WARM_PROJECT/MLP: SPHDEM_FIT_* bits */
+    int32_t reserved_i[1];
 
     /* -- real switches: vif[] of function_init.cuh:59-100 -- */
     double kappa;               /* vif[0]  */
@@ -225,6 +244,11 @@ typedef struct SphdemStats {
     int32_t mlp_trained_steps;  /* training steps taken */
     int32_t reserved_stats;
     double  ppe_initial_residual;  /* ||b - A x0|| / ||b|| of the last solve's initial iterate */
+    double  ppe_warm_gain;      /* WARM_PROJECT/MLP: c.h of the last fit, the drop of the squared
+                                   error norm that the fit achieves (larger is better; comparable
+                                   between runs on the same state with the same warm_fit) */
+    int32_t ppe_warm_dirs;      /* directions the last fit kept */
+    int32_t reserved_stats2;
 } SphdemStats;
 
 typedef struct SphdemHandle SphdemHandle;
@@ -253,8 +277,8 @@ int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem,
 /* Read input_dir/solv.txt, input_dir/data.txt and input_dir/input.txt
  * (function_init.cuh:216-1182, ISPH.cuh:55-113) and create an engine.
  * ov may be NULL; when given, its non-switch engine extensions
- * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter) override the
- * defaults. */
+ * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit,
+ * mlp_train_steps, mlp_updates, mlp_seed, mlp_lr) override the defaults. */
 int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
                            SphdemHandle** out);
 
@@ -351,6 +375,12 @@ int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* spring
  * sphdem_get_timing reports (kernel k = 0..n-1, name, total ms, count). */
 int sphdem_set_timing(SphdemHandle* h, int on);
 int sphdem_collect_timing(SphdemHandle* h);
+
+/* Step graphs on (default) or off.  Off, every step launches its kernels
+ * one by one and the KRYLOV/PCG iterations are driven from the host (one
+ * status read per iteration): slower, but visible to kernel profilers,
+ * which cannot see inside graphs with conditional nodes. */
+int sphdem_set_graphs(SphdemHandle* h, int on);
 int sphdem_get_timing(SphdemHandle* h, int k, char* name, int name_cap,
                       double* total_ms, int64_t* launches);
 

@@ -299,6 +299,7 @@ static void permute_i(int* f, const int* perm, int n, int* tmp) {
     memcpy(f, tmp, sizeof(int) * (size_t)n);
 }
 static void permute_blk(double* f, const int* perm, int n, int w, double* tmp) {
+    if (n <= 0 || w <= 0) return;
     for (int i = 0; i < n; i++) memcpy(tmp + (size_t)i * w, f + (size_t)perm[i] * w, sizeof(double) * (size_t)w);
     memcpy(f, tmp, sizeof(double) * (size_t)n * w);
 }
@@ -1221,6 +1222,11 @@ static double ppe_dot(int n, const double* a, const double* b) {
     for (int i = 0; i < n; i++) s += a[i] * b[i];
     return s;
 }
+static double ppe_wdot(int n, const double* w, const double* a, const double* b) {
+    double s = 0;
+    for (int i = 0; i < n; i++) s += w[i] * a[i] * b[i];
+    return s;
+}
 
 static void ppe_krylov(OracleState* S, double tdt) {
     OSet* o = &S->s;
@@ -1309,24 +1315,43 @@ static void ppe_krylov(OracleState* S, double tdt) {
     int it = 0, status = 0;
     double tol = P->ppe_tol;
     if (cg) {
-        double rz = ppe_dot(n, r, z);
-        while (bn > 0 && res > tol && it < P->ppe_max_iter) {
-            ppe_matvec(&A, solved, pp, v, S->nthreads);
-            double pq = ppe_dot(n, pp, v);
-            if (!(pq != 0.0) || !isfinite(pq)) { status = 2; break; }
-            double alpha = rz / pq;
+        /* Chronopoulos-Gear PCG (the engine's form): u = M^-1 r, w = A u;
+         * p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s,
+         * u = M^-1 r, w = A u, gamma = r.u, delta = w.u,
+         * beta' = gamma/gamma_old, alpha' = gamma/(delta - beta' gamma/alpha) */
+        /* a_ij = m_j s_ij with s symmetric: CG on M A p = M b with the
+         * preconditioner M D, i.e. inner products weighted by m_i */
+        double* w = v;
+        double* u = z;
+        double* wm = t;
+        for (int i = 0; i < n; i++) ss[i] = 0.0, pp[i] = 0.0, wm[i] = solved[i] ? o->m[i] : 0.0;
+        ppe_matvec(&A, solved, u, w, S->nthreads);
+        double gam = ppe_wdot(n, wm, r, u), del = ppe_wdot(n, wm, w, u);
+        double alpha = 0, beta = 0;
+        if (bn > 0 && res > tol && it < P->ppe_max_iter) {
+            if (!(del != 0.0) || !isfinite(del)) status = 2;
+            else alpha = gam / del;
+        }
+        while (status == 0 && bn > 0 && res > tol && it < P->ppe_max_iter) {
             for (int i = 0; i < n; i++) {
+                pp[i] = u[i] + beta * pp[i];
+                ss[i] = w[i] + beta * ss[i];
                 x[i] += alpha * pp[i];
-                r[i] -= alpha * v[i];
-                z[i] = r[i] / (solved[i] ? A.d[i] : 1.0);
+                r[i] -= alpha * ss[i];
+                u[i] = r[i] / (solved[i] ? A.d[i] : 1.0);
             }
-            double rz_new = ppe_dot(n, r, z);
-            double beta = rz_new / rz;
-            for (int i = 0; i < n; i++) pp[i] = z[i] + beta * pp[i];
-            rz = rz_new;
+            ppe_matvec(&A, solved, u, w, S->nthreads);
+            double g1 = ppe_wdot(n, wm, r, u), d1 = ppe_wdot(n, wm, w, u);
             it++;
             res = sqrt(ppe_dot(n, r, r)) / bn;
             if (!isfinite(res)) { status = 2; break; }
+            if (res <= tol || it >= P->ppe_max_iter) break;
+            double be = g1 / gam;
+            double den = d1 - be * g1 / alpha;
+            if (!(den != 0.0) || !isfinite(den)) { status = 2; break; }
+            beta = be;
+            alpha = g1 / den;
+            gam = g1;
         }
     } else {
         double rho = 1, alpha = 1, om = 1;
@@ -1988,6 +2013,7 @@ static void w_correct_xsph(OracleState* S) {
     const SphdemParams* P = &S->p;
     int n = o->n;
     double tdt = P->dt;
+    if (n <= 0) return;
     double* xn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
     double* yn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));
     double* rn = (double*)malloc(sizeof(double) * (size_t)(n ? n : 1));

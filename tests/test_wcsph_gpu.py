@@ -125,6 +125,18 @@ def test_wcsph_runs_are_deterministic_and_stats():
     assert uy.min() < 0
 
 
+def test_wcsph_graphs_equal_eager():
+    """The captured step graph and eager launches give identical states."""
+    p, sph = _bed("kgc_antuono_xsph", seed=44)
+    a = _engine(p, sph, 1)
+    b = _engine(p, sph, 1)
+    b.set_graphs(False)
+    a.step(6)
+    b.step(6)
+    for f in ("x", "y", "ux", "uy", "rho", "pres", "flt_s"):
+        assert np.array_equal(a.get(SPH, f), b.get(SPH, f)), f
+
+
 W_GOLD = [g for g in golden_files() if json.loads(np.load(g)["meta"].tobytes()).get("solver") == "wcsph"]
 
 
