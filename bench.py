@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "ppe-profile"],
+                    help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
+                         "(its protocol is --steps 1000); ppe-profile: --steps steps of the bed with the "
+                         "projected-start PCG and step graphs off, so that a kernel profiler sees the PPE "
+                         "kernels (no timing)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -265,6 +270,200 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------------------
+# 2-D WCSPH dam break (--workload dam2d)
+# ---------------------------------------------------------------------------
+DAM_TEXT = ("2-D WCSPH dam break: 1.6x1.0 m tank, 0.4x0.8 m water column at dx=5 mm (12,800 fluid + 2,178 wall "
+            "particles, seeded jitter 0.01 dx), Wendland C2, h=1.3dx, Tait EOS gamma=7, c0=10 sqrt(2 g 0.8), "
+            "artificial viscosity alpha=0.02, gravity 9.81, dt=0.2 h/c0, predictor-corrector, continuity")
+W_STATE = ["x", "y", "ux", "uy", "rho", "pres", "flt_s", "ftotalx", "ftotaly", "drho"]
+
+
+def w_manifest_bytes(kernel, n, avg_nb, r):
+    """Bytes each 2-D WCSPH pass must move (own fields once, neighbour
+    fields once per particle, 4 B per list entry): positions x, y, h and
+    mass, density are FP64 (8 B), the other fields r bytes."""
+    L = 4 * avg_nb + 4
+    pos = 24
+    per = {
+        "w.list": n * (pos + 4 + L),
+        "w.prep": n * (pos + 16 + L + 8 + 3 * r),
+        "w.continuity": n * (pos + 4 + 16 + L + 8 + 5 * r),
+        "w.interaction": n * (pos + 16 + L + 3 * r + 5 * r),
+        "w.kgc": n * (pos + 16 + L + 4 * r),
+        "w.xsph": n * (pos + 16 + L + 3 * r + 16),
+        "w.predictor": n * (16 + 16 + 4 * r + 8 + 16 + 2 * r + 8),
+        "w.corrector": n * (16 + 16 + 4 * r + 24 + 2 * r),
+        "w.eos": n * (8 + 8 + r),
+        "w.finish": n * 48,
+    }
+    return per.get(kernel)
+
+
+def dam2d_cpu(seconds):
+    from fluidized_bed_master_b200.beds import dam_break_2d
+    from oracle import Oracle
+
+    p, sph, _ = dam_break_2d(seed=0)
+    threads = os.cpu_count() or 1
+    orc = Oracle(p, sph, {}, threads=threads)
+    orc.step(1)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        orc.step(10)
+        k += 10
+        if time.perf_counter() - t0 >= seconds or k >= 5000:
+            break
+    el = time.perf_counter() - t0
+    return orc.ns * k / el, threads, f"the whole dam break ({orc.ns} particles), {k} steps after 1 warm-up", el / k
+
+
+def run_ppe_profile(args):
+    """A few steps of the bench bed with the PCG PPE (projected start over 8
+    solution changes) and graphs off: the launch sequence a kernel profiler
+    can see (kernels inside conditional graph nodes are hidden from it)."""
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import PPE_PCG, WARM_PROJECT
+
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    p.precision = 0
+    p.ppe_mode = PPE_PCG
+    p.kgc_solve = 0
+    p.ppe_tol = 1e-6
+    p.ppe_max_iter = 2000
+    p.warm_start = WARM_PROJECT
+    p.warm_hist = 8
+    eng = Engine(p, sph, dem)
+    eng.set_graphs(False)
+    eng.step(args.steps)
+    s = eng.stats()
+    print(json.dumps({"workload": "ppe-profile", "steps": args.steps, "ppe_iters": s["ppe_iters"],
+                      "ppe_status": s["ppe_status"], "n_sph": eng.ns, "n_dem": eng.nd}), flush=True)
+    eng.close()
+
+
+def run_dam2d(args, world, rank, local, pg):
+    import torch
+
+    from fluidized_bed_master_b200.beds import dam_break_2d
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import SPH
+
+    metric = "2-D WCSPH particle-updates/s on 1 B200 (dam break)"
+    unit = "particle-updates/s"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        val, cores, sample, s_per_step = dam2d_cpu(max(5.0, args.cpu_seconds))
+        line = {"metric": metric, "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": s_per_step * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded dam break)", "config": {"workload": DAM_TEXT},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local)
+    p, sph, _ = dam_break_2d(seed=rank)
+    p.precision = 1 if args.precision == "fp64" else 0
+    eng = Engine(p, sph, {})
+    n = eng.ns
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    eng.set_timing(True)
+    eng.step(2)
+    eng.collect_timing()
+    counts, _ = eng.neighbors(cap=1)
+    avg_nb = float(counts.mean())
+    base = eng.timing()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
+    sampler = ClockSampler(int(vis) if vis.isdigit() else local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms, launches = 0.0, 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        eng.step(1)
+        launches += eng.launches()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        eng.collect_timing()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    t_max = reduce_over_ranks(pg, total_ms, "max", "cuda")
+    n_all = reduce_over_ranks(pg, n, "sum", "cuda")
+    value = n_all * args.steps / (t_max / 1e3)
+    tim = eng.timing()
+    per_kernel = {k: (v[0] - base.get(k, (0, 0))[0], v[1] - base.get(k, (0, 0))[1]) for k, v in tim.items()}
+    # dominant single kernel (the NNPS timer spans hash, CUB's sort, gather and rows)
+    single = {k: v for k, v in per_kernel.items() if k != "w.nnps"}
+    dom_name, (dom_ms, dom_n) = max(single.items(), key=lambda kv: kv[1][0])
+    r = 8 if args.precision == "fp64" else 4
+    bytes_dom = w_manifest_bytes(dom_name, n, avg_nb, r)
+    peak, peak_kind = load_peaks()
+    achieved = bytes_dom / (dom_ms / max(dom_n, 1) / 1e3) / 1e9 if (bytes_dom and dom_n) else None
+    traffic = profiled_traffic(dom_name) if args.precision == "fp32" else None
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "bytes_per_launch": bytes_dom, "launch_ms": dom_ms / max(dom_n, 1), "peak_source": peak_kind,
+                "share_of_step": dom_ms / max(sum(v[0] for v in per_kernel.values()), 1e-12)}
+    e2e = None
+    if not args.no_e2e:
+        def pinned(k, dt):
+            return torch.empty(k, dtype=dt, pin_memory=True).numpy()
+        hs = {f: pinned(n, torch.float64) for f in W_STATE}
+        for f in W_STATE:
+            hs[f][:] = eng.get(SPH, f)
+        hb = sum(a.nbytes for a in hs.values())
+        eng.set_timing(False)
+        ke = max(3, min(args.steps, 200))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            eng.set_fields(SPH, hs)
+            eng.step(1)
+            eng.get_fields(SPH, hs)
+        torch.cuda.synchronize()
+        te = reduce_over_ranks(pg, time.perf_counter() - t0, "max", "cuda")
+        e2e = {"value": n_all * ke / te, "unit": unit, "h2d_bytes_per_step": hb, "d2h_bytes_per_step": hb,
+               "ms_per_step": te / ke * 1e3,
+               "how": "per step: sphdem_set_fields of the WCSPH state (incl. the rates the predictor reads) from "
+                      "pinned host arrays, sphdem_step, sphdem_get_fields back"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample, _ = dam2d_cpu(min(args.cpu_seconds, 10.0))
+        cpu = {"value": v, "unit": unit, "cores": cores, "kind": "port", "sample": sample}
+    stats = eng.stats()
+    eng.close()
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if r == 4 else "f64", "data": "synthetic (seeded dam break)",
+        "config": {"workload": DAM_TEXT, "n": n, "l2": "256 MB buffer written before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "positions": "f64",
+                   "density_mass": "f64", "fields": "f32" if r == 4 else "f64"},
+        "avg_neighbours": avg_nb, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clocks,
+        "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "overflow_flags", "nan_flag")},
+        "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # engine arm
 # ---------------------------------------------------------------------------
 def run_engine(args, world, rank, local, pg):
@@ -475,7 +674,12 @@ def main():
     args = parse()
     world, rank, local, pg = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.workload == "dam2d":
+            run_dam2d(args, world, rank, local, pg)
+        elif args.workload == "ppe-profile":
+            if rank == 0:
+                run_ppe_profile(args)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_engine(args, world, rank, local, pg)

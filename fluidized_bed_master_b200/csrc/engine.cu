@@ -32,13 +32,18 @@ static const int TPB = 128;
 enum {
     KT_HASH_S, KT_SORT_S, KT_GATHER_S, KT_HASH_D, KT_SORT_D, KT_GATHER_D, KT_LIST, KT_PASSA, KT_DEMPREP, KT_PASSB,
     KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
-    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN, KT_COUNT
+    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN,
+    // 2-D WCSPH step
+    KT_W_PRED, KT_W_NNPS, KT_W_LIST, KT_W_KGC, KT_W_PREP, KT_W_CONT, KT_W_EOS, KT_W_INTER, KT_W_CORR, KT_W_XSPH,
+    KT_W_FINISH, KT_COUNT
 };
 static const char* KT_NAMES[KT_COUNT] = {
     "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
     "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem",
-    "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training"};
+    "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training",
+    "w.predictor", "w.nnps", "w.list", "w.kgc", "w.prep", "w.continuity", "w.eos", "w.interaction", "w.corrector",
+    "w.xsph", "w.finish"};
 
 // Event records inside a captured step graph must be external event
 // nodes (cudaEventRecordExternal); a plain record during capture only
@@ -1049,43 +1054,52 @@ static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst) {
 
 // one step of WCSPH_Calc.cuh:15-340 (Lagrangian variant)
 template <typename R>
-static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH) {
+static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
     const DevParams& P = EH->P;
     const WParams& Q = EH->Q;
     WWork<R>& W = EH->W;
     cudaStream_t st = H->stream;
     int n = P.ns, so = EH->cur, sn = 1 - EH->cur;
     int bs = nblocks(n, TPB);
-    k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W);
-    int r = w_nnps<R>(H, EH, so, sn);
-    if (r) return r;
+    { KTIME(KT_W_PRED); k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W); }
+    {
+        KTIME(KT_W_NNPS);
+        int r = w_nnps<R>(H, EH, so, sn);
+        if (r) return r;
+    }
     WState<R>& S = EH->S[sn];
-    k_w_list<R><<<bs, TPB, 0, st>>>(P, S, W.rows, W.nbr, W.ncnt, EH->flags);
+    { KTIME(KT_W_LIST); k_w_list<R><<<bs, TPB, 0, st>>>(P, S, W.rows, W.nbr, W.ncnt, EH->flags); }
     // gradient_correction() runs for kgc_solve > 0 or Antuono, but only the
     // KGC case fills Cm, and only KGC reads it (apply_gradient_correction_2D)
-    if (P.kgc == 1) k_w_kgc<R><<<bs, TPB, 0, st>>>(P, S, W);
-    k_w_prep<R><<<bs, TPB, 0, st>>>(P, Q, S, W, EH->flags);
-    k_w_continuity<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
-    k_w_eos<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
-    k_w_interaction<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
-    k_w_corrector<R><<<bs, TPB, 0, st>>>(P, Q, S, W);
-    if (P.xsph) k_w_xsph<R><<<bs, TPB, 0, st>>>(P, S, W);
-    k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W);
+    if (P.kgc == 1) { KTIME(KT_W_KGC); k_w_kgc<R><<<bs, TPB, 0, st>>>(P, S, W); }
+    { KTIME(KT_W_PREP); k_w_prep<R><<<bs, TPB, 0, st>>>(P, Q, S, W, EH->flags); }
+    { KTIME(KT_W_CONT); k_w_continuity<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
+    { KTIME(KT_W_EOS); k_w_eos<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
+    { KTIME(KT_W_INTER); k_w_interaction<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
+    { KTIME(KT_W_CORR); k_w_corrector<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
+    if (P.xsph) { KTIME(KT_W_XSPH); k_w_xsph<R><<<bs, TPB, 0, st>>>(P, S, W); }
+    { KTIME(KT_W_FINISH); k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W); }
     k_tick<<<1, 1, 0, st>>>(EH->flags);
     CK(cudaGetLastError());
+    // engine kernels of the step (CUB's sort passes not counted): predictor,
+    // hash, gather, rows, list, [kgc], prep, continuity, eos, interaction,
+    // corrector, [xsph], finish, tick
+    *nl += 12 + (P.kgc == 1) + (P.xsph != 0);
     return SPHDEM_OK;
 }
 
 template <typename R>
-static int w_run_step(SphdemHandle* H, WEngineHost<R>* EH) {
+static int w_run_step(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
     int key = (1 << 16) | EH->cur;
+    int64_t n = 0;
     if (H->use_graphs) {
         auto it = H->graphs.find(key);
         if (it == H->graphs.end()) {
             cudaGraph_t g;
+            if (H->timing) std::fill(H->ev_used.begin(), H->ev_used.end(), 0);
             CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
             H->capturing = true;
-            int r = w_enqueue<R>(H, EH);
+            int r = w_enqueue<R>(H, EH, &n);
             H->capturing = false;
             cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
             if (r) return r;
@@ -1094,13 +1108,18 @@ static int w_run_step(SphdemHandle* H, WEngineHost<R>* EH) {
             CK(cudaGraphInstantiate(&ge, g, 0));
             cudaGraphDestroy(g);
             H->graphs[key] = ge;
+            H->graph_launches[key] = n;
+            H->graph_kused[key] = H->ev_used;
             it = H->graphs.find(key);
         }
+        n = H->graph_launches[key];
+        if (H->timing) H->ev_used = H->graph_kused[key];
         CK(cudaGraphLaunch(it->second, H->stream));
     } else {
-        int r = w_enqueue<R>(H, EH);
+        int r = w_enqueue<R>(H, EH, &n);
         if (r) return r;
     }
+    *nl += n;
     EH->cur ^= 1;
     return SPHDEM_OK;
 }
@@ -1501,17 +1520,32 @@ static bool is_settable_state(int f) {
     return false;
 }
 
+// state of the 2-D WCSPH step that a caller may replace between steps: the
+// particle fields and the last step's rates, which the next predictor reads
+static bool is_settable_wcsph(int f) {
+    static const int allowed[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_UX, SPHDEM_F_UY, SPHDEM_F_M, SPHDEM_F_RHO,
+                                  SPHDEM_F_PRES, SPHDEM_F_TEMP, SPHDEM_F_FLT_S, SPHDEM_F_FTOTALX, SPHDEM_F_FTOTALY,
+                                  SPHDEM_F_DRHO};
+    for (int a : allowed)
+        if (a == f) return true;
+    return false;
+}
+
 template <typename R>
 static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, void* const* host, bool set) {
     int n = which ? H->nd : H->ns;
+    const bool w = H->kind == 1;
+    if (w && which != 0) return SPHDEM_E_ARG;
     XTab t;
     t.dbl = 0;
     for (int k = 0; k < nf; k++) {
         if (!host[k]) return SPHDEM_E_ARG;
-        if (set ? !is_settable_state(fields[k]) : !is_real_field(fields[k])) return SPHDEM_E_ARG;
+        bool ok = set ? (w ? is_settable_wcsph(fields[k]) : is_settable_state(fields[k])) : is_real_field(fields[k]);
+        if (!ok) return SPHDEM_E_ARG;
         const void* ptr;
         int kind;
-        if (field_ptr<R>(H, which, fields[k], &ptr, &kind) || kind == 2) return SPHDEM_E_ARG;
+        int e = w ? w_field_ptr<R>(H, fields[k], &ptr, &kind) : field_ptr<R>(H, which, fields[k], &ptr, &kind);
+        if (e || kind == 2) return SPHDEM_E_ARG;
         t.p[k] = (void*)ptr;
         if (kind == 0) t.dbl |= 1u << k;
     }
@@ -1538,7 +1572,6 @@ static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, voi
 
 extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
                                  const double* const* host_src) {
-    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !fields || !host_src || (which != 0 && which != 1) || nfields < 0 ||
         nfields > SPHDEM_BULK_MAX_FIELDS)
         return SPHDEM_E_ARG;
@@ -1549,7 +1582,6 @@ extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, co
 
 extern "C" int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
                                  double* const* host_dst) {
-    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !h->committed || !fields || !host_dst || (which != 0 && which != 1) || nfields < 0 ||
         nfields > SPHDEM_BULK_MAX_FIELDS)
         return SPHDEM_E_ARG;
@@ -1561,8 +1593,14 @@ extern "C" int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields, co
 extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const void* src, size_t bytes) {
     if (!h || !src || (which != 0 && which != 1)) return SPHDEM_E_ARG;
     if (h->committed) {
-        if (h->kind == 1) return SPHDEM_E_UNSUPPORTED;
         int n = which ? h->nd : h->ns;
+        if (h->kind == 1) {   // 2-D WCSPH: through the bulk path
+            if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
+            int32_t f = field;
+            const void* srcs[1] = {src};
+            return h->prec == SPHDEM_PREC_FP64 ? bulk_t<double>(h, which, 1, &f, (void* const*)srcs, true)
+                                               : bulk_t<float>(h, which, 1, &f, (void* const*)srcs, true);
+        }
         if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
         return h->prec == SPHDEM_PREC_FP64 ? set_state_t<double>(h, which, field, src, n)
                                            : set_state_t<float>(h, which, field, src, n);
@@ -1620,8 +1658,8 @@ extern "C" int sphdem_step(SphdemHandle* h, int32_t nsteps) {
     for (int k = 0; k < nsteps; k++) {
         int r;
         if (h->kind == 1)
-            r = h->prec == SPHDEM_PREC_FP64 ? w_run_step<double>(h, (WEngineHost<double>*)h->eng)
-                                            : w_run_step<float>(h, (WEngineHost<float>*)h->eng);
+            r = h->prec == SPHDEM_PREC_FP64 ? w_run_step<double>(h, (WEngineHost<double>*)h->eng, &nl)
+                                            : w_run_step<float>(h, (WEngineHost<float>*)h->eng, &nl);
         else
             r = h->prec == SPHDEM_PREC_FP64 ? run_step<double>(h, (EngineHost<double>*)h->eng, &nl)
                                             : run_step<float>(h, (EngineHost<float>*)h->eng, &nl);
@@ -1802,7 +1840,6 @@ extern "C" int sphdem_set_graphs(SphdemHandle* h, int on) {
 }
 
 extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
-    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h) return SPHDEM_E_ARG;
     if (h->ev_beg.empty()) {
         h->ev_beg.resize(KT_COUNT);

@@ -286,7 +286,9 @@ int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
  * memory.  Before sphdem_commit_particles: input order, any field.  After
  * it: the engine's current slot order (the order sphdem_get_field
  * returns), state fields only (positions, velocities, m, rho, pres, temp,
- * dDEMpor, flt_s, Fd*_df, Q_sd, temp1-3).  bytes = n * 8 (real fields) or
+ * dDEMpor, flt_s, Fd*_df, Q_sd, temp1-3; for a 2-D WCSPH handle x, y,
+ * ux, uy, m, rho, pres, temp, flt_s and the last step's ftotalx/y and
+ * drho, which its next predictor reads).  bytes = n * 8 (real fields) or
  * n * 4 (int). */
 int sphdem_set_field(SphdemHandle* h, int which, int field,
                      const void* host_src, size_t bytes);
