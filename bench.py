@@ -287,13 +287,12 @@ def w_manifest_bytes(kernel, n, avg_nb, r):
     per = {
         "w.list": n * (pos + 4 + L),
         "w.prep": n * (pos + 16 + L + 8 + 3 * r),
-        "w.continuity": n * (pos + 4 + 16 + L + 8 + 5 * r),
+        "w.continuity": n * (pos + 4 + 16 + L + 8 + 6 * r),   # with the EOS (pressure write)
         "w.interaction": n * (pos + 16 + L + 3 * r + 5 * r),
         "w.kgc": n * (pos + 16 + L + 4 * r),
         "w.xsph": n * (pos + 16 + L + 3 * r + 16),
         "w.predictor": n * (16 + 16 + 4 * r + 8 + 16 + 2 * r + 8),
         "w.corrector": n * (16 + 16 + 4 * r + 24 + 2 * r),
-        "w.eos": n * (8 + 8 + r),
         "w.finish": n * 48,
     }
     return per.get(kernel)
@@ -456,7 +455,7 @@ def run_dam2d(args, world, rank, local, pg):
                    "density_mass": "f64", "fields": "f32" if r == 4 else "f64"},
         "avg_neighbours": avg_nb, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks,
-        "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "overflow_flags", "nan_flag")},
+        "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "overflow_flags", "nan_flag", "w_lanes")},
         "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
     }
     if rank == 0:

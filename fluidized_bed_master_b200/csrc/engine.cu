@@ -34,7 +34,7 @@ enum {
     KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
     KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN,
     // 2-D WCSPH step
-    KT_W_PRED, KT_W_NNPS, KT_W_LIST, KT_W_KGC, KT_W_PREP, KT_W_CONT, KT_W_EOS, KT_W_INTER, KT_W_CORR, KT_W_XSPH,
+    KT_W_PRED, KT_W_NNPS, KT_W_LIST, KT_W_KGC, KT_W_PREP, KT_W_CONT, KT_W_INTER, KT_W_CORR, KT_W_XSPH,
     KT_W_FINISH, KT_COUNT
 };
 static const char* KT_NAMES[KT_COUNT] = {
@@ -42,7 +42,7 @@ static const char* KT_NAMES[KT_COUNT] = {
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
     "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem",
     "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training",
-    "w.predictor", "w.nnps", "w.list", "w.kgc", "w.prep", "w.continuity", "w.eos", "w.interaction", "w.corrector",
+    "w.predictor", "w.nnps", "w.list", "w.kgc", "w.prep", "w.continuity", "w.interaction", "w.corrector",
     "w.xsph", "w.finish"};
 
 // Event records inside a captured step graph must be external event
@@ -1020,8 +1020,21 @@ struct WEngineHost {
     void* sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
     int nb_cap = 0;
+    int lanes = 1;    // lanes per particle of the gathers (w_lanes, or the commit-time autotuner)
     Alloc A;
 };
+
+// launch KERN<R, L> with L lanes per particle (n L threads in blocks of TPB)
+#define W_LAUNCH(L, KERN, n, st, ...)                                                                      \
+    do {                                                                                                   \
+        switch (L) {                                                                                       \
+        case 1: KERN<R, 1><<<nblocks((n) * 1, TPB), TPB, 0, st>>>(__VA_ARGS__); break;                    \
+        case 2: KERN<R, 2><<<nblocks((n) * 2, TPB), TPB, 0, st>>>(__VA_ARGS__); break;                    \
+        case 4: KERN<R, 4><<<nblocks((n) * 4, TPB), TPB, 0, st>>>(__VA_ARGS__); break;                    \
+        case 8: KERN<R, 8><<<nblocks((n) * 8, TPB), TPB, 0, st>>>(__VA_ARGS__); break;                    \
+        default: KERN<R, 16><<<nblocks((n) * 16, TPB), TPB, 0, st>>>(__VA_ARGS__); break;                 \
+        }                                                                                                  \
+    } while (0)
 
 template <typename R>
 static void w_alloc_state(Alloc& A, WState<R>& S, int n) {
@@ -1033,15 +1046,16 @@ static void w_alloc_state(Alloc& A, WState<R>& S, int n) {
     S.ptype = A.get<int>(n); S.btype = A.get<int>(n); S.itype = A.get<int>(n); S.pid = A.get<int>(n);
 }
 
-// NNPS of the WCSPH state: S[src] -> S[dst] in cell order
+// NNPS of the WCSPH state: S[src] -> S[dst] in cell order (hashed: the
+// predictor already wrote the cell keys)
 template <typename R>
-static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst) {
+static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst, bool hashed = false) {
     const DevParams& P = EH->P;
     WWork<R>& W = EH->W;
     cudaStream_t st = H->stream;
     int n = P.ns;
     WState<R>& S = EH->S[src];
-    k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    if (!hashed) k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
     size_t bytes = EH->sort_tmp_bytes;
     CK(cub::DeviceRadixSort::SortPairs(EH->sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
                                        key_bits(P.num_cells), st));
@@ -1061,30 +1075,31 @@ static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
     cudaStream_t st = H->stream;
     int n = P.ns, so = EH->cur, sn = 1 - EH->cur;
     int bs = nblocks(n, TPB);
-    { KTIME(KT_W_PRED); k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W); }
+    { KTIME(KT_W_PRED); k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W, W.key_in, W.val_in); }
     {
         KTIME(KT_W_NNPS);
-        int r = w_nnps<R>(H, EH, so, sn);
+        int r = w_nnps<R>(H, EH, so, sn, true);
         if (r) return r;
     }
     WState<R>& S = EH->S[sn];
-    { KTIME(KT_W_LIST); k_w_list<R><<<bs, TPB, 0, st>>>(P, S, W.rows, W.nbr, W.ncnt, EH->flags); }
+    const int L = EH->lanes;
+    { KTIME(KT_W_LIST); W_LAUNCH(L, k_w_list, n, st, P, S, W.rows, W.nbr, W.ncnt, EH->flags); }
     // gradient_correction() runs for kgc_solve > 0 or Antuono, but only the
     // KGC case fills Cm, and only KGC reads it (apply_gradient_correction_2D)
-    if (P.kgc == 1) { KTIME(KT_W_KGC); k_w_kgc<R><<<bs, TPB, 0, st>>>(P, S, W); }
-    { KTIME(KT_W_PREP); k_w_prep<R><<<bs, TPB, 0, st>>>(P, Q, S, W, EH->flags); }
-    { KTIME(KT_W_CONT); k_w_continuity<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
-    { KTIME(KT_W_EOS); k_w_eos<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
-    { KTIME(KT_W_INTER); k_w_interaction<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
-    { KTIME(KT_W_CORR); k_w_corrector<R><<<bs, TPB, 0, st>>>(P, Q, S, W); }
-    if (P.xsph) { KTIME(KT_W_XSPH); k_w_xsph<R><<<bs, TPB, 0, st>>>(P, S, W); }
-    { KTIME(KT_W_FINISH); k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W); }
-    k_tick<<<1, 1, 0, st>>>(EH->flags);
+    if (P.kgc == 1) { KTIME(KT_W_KGC); W_LAUNCH(L, k_w_kgc, n, st, P, S, W); }
+    { KTIME(KT_W_PREP); W_LAUNCH(L, k_w_prep, n, st, P, Q, S, W, EH->flags); }
+    { KTIME(KT_W_CONT); W_LAUNCH(L, k_w_continuity, n, st, P, Q, S, W); }   // + EOS
+    { KTIME(KT_W_INTER); W_LAUNCH(L, k_w_interaction, n, st, P, Q, S, W); }
+    { KTIME(KT_W_CORR); k_w_corrector<R><<<bs, TPB, 0, st>>>(P, Q, S, W, EH->flags); }
+    if (P.xsph) {
+        { KTIME(KT_W_XSPH); W_LAUNCH(L, k_w_xsph, n, st, P, S, W); }
+        { KTIME(KT_W_FINISH); k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W); }
+    }
     CK(cudaGetLastError());
-    // engine kernels of the step (CUB's sort passes not counted): predictor,
-    // hash, gather, rows, list, [kgc], prep, continuity, eos, interaction,
-    // corrector, [xsph], finish, tick
-    *nl += 12 + (P.kgc == 1) + (P.xsph != 0);
+    // engine kernels of the step (CUB's sort passes not counted): predictor
+    // (+ cell keys), gather, rows, list, [kgc], prep, continuity (+ EOS),
+    // interaction, corrector (+ step counter), [xsph, finish]
+    *nl += 8 + (P.kgc == 1) + 2 * (P.xsph != 0);
     return SPHDEM_OK;
 }
 
@@ -1121,6 +1136,72 @@ static int w_run_step(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
     }
     *nl += n;
     EH->cur ^= 1;
+    return SPHDEM_OK;
+}
+
+// Lanes per particle of the gathers.  w_lanes > 0 fixes it; 0 times the
+// gather kernels (list, [kgc], prep, continuity, interaction, [xsph]) on the
+// committed, cell-sorted state for L = 1, 2, 4, 8, 16 and keeps the fastest
+// (the minimum of 3 repetitions after one warm-up launch each).  The work
+// arrays those kernels write are cleared afterwards, so the run starts from
+// the same state whatever L was chosen; L changes only the order of the
+// neighbour sums inside a particle, i.e. results at the rounding level.
+template <typename R>
+static int w_tune_lanes(SphdemHandle* H, WEngineHost<R>* EH) {
+    const DevParams& P = EH->P;
+    const WParams& Q = EH->Q;
+    WWork<R>& W = EH->W;
+    WState<R>& S = EH->S[1];   // the sorted copy that w_nnps left there
+    cudaStream_t st = H->stream;
+    const int n = P.ns;
+    int want = H->p.w_lanes;
+    if (want != 0) {
+        EH->lanes = want;
+        return SPHDEM_OK;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto pass = [&](int L) {
+        W_LAUNCH(L, k_w_list, n, st, P, S, W.rows, W.nbr, W.ncnt, EH->flags);
+        if (P.kgc == 1) W_LAUNCH(L, k_w_kgc, n, st, P, S, W);
+        W_LAUNCH(L, k_w_prep, n, st, P, Q, S, W, EH->flags);
+        W_LAUNCH(L, k_w_continuity, n, st, P, Q, S, W);
+        W_LAUNCH(L, k_w_interaction, n, st, P, Q, S, W);
+        if (P.xsph) W_LAUNCH(L, k_w_xsph, n, st, P, S, W);
+    };
+    float best = 1e30f;
+    int bestL = 1;
+    int rc = SPHDEM_OK;
+    for (int L : {1, 2, 4, 8, 16}) {
+        pass(L);
+        if (cudaEventRecord(e0, st) != cudaSuccess) { rc = SPHDEM_E_CUDA; break; }
+        for (int rep = 0; rep < 3; rep++) pass(L);
+        float ms = 0.f;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = SPHDEM_E_CUDA;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            bestL = L;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    EH->lanes = bestL;
+    // back to the state of a run that never tuned
+    const size_t rb = sizeof(R) * (size_t)n;
+    R* rz[] = {W.ftx, W.fty, W.ftot, W.drho, W.grx, W.gry, W.pgfx, W.pgfy};
+    for (R* a : rz) CK(cudaMemsetAsync(a, 0, rb, st));
+    CK(cudaMemsetAsync(W.Cm, 0, rb * 4, st));
+    CK(cudaMemsetAsync(W.rho_ref, 0, sizeof(double) * n, st));
+    CK(cudaMemsetAsync(W.xn, 0, sizeof(double) * n, st));
+    CK(cudaMemsetAsync(W.yn, 0, sizeof(double) * n, st));
+    CK(cudaMemsetAsync(W.ncnt, 0, sizeof(int) * n, st));
+    CK(cudaStreamSynchronize(st));
     return SPHDEM_OK;
 }
 
@@ -1227,7 +1308,7 @@ static int w_commit_t(SphdemHandle* H) {
     if (r) return SPHDEM_E_CUDA;
     // neighbour-list capacity from an exact count on the sorted input
     if ((r = w_nnps<R>(H, EH, 0, 1))) return r;
-    k_w_list<R><<<nblocks(ns, TPB), TPB, 0, st>>>(P, EH->S[1], W.rows, nullptr, W.ncnt, EH->flags);
+    k_w_list<R, 1><<<nblocks(ns, TPB), TPB, 0, st>>>(P, EH->S[1], W.rows, nullptr, W.ncnt, EH->flags);
     CK(cudaGetLastError());
     DevFlags f;
     CK(cudaMemcpyAsync(&f, EH->flags, sizeof(f), cudaMemcpyDeviceToHost, st));
@@ -1237,6 +1318,7 @@ static int w_commit_t(SphdemHandle* H) {
     EH->nb_cap = cap;
     W.nbr = A.get<int>((size_t)cap * ns);
     if (!A.ok) return SPHDEM_E_NOMEM;
+    if ((r = w_tune_lanes<R>(H, EH))) return r;
     DevFlags f0;
     std::memset(&f0, 0, sizeof(f0));
     f0.step_count = H->count;
@@ -1318,6 +1400,7 @@ static int w_stats_t(SphdemHandle* H, SphdemStats* out) {
     out->ppe_iters = 0;
     out->overflow_flags = f.overflow;
     out->nan_flag = f.nan;
+    out->w_lanes = EH->lanes;
     return SPHDEM_OK;
 }
 
@@ -1358,6 +1441,9 @@ static int check_supported(const SphdemParams* p) {
         if (p->ppe_mode != SPHDEM_PPE_REFERENCE || p->warm_start != SPHDEM_WARM_PREVIOUS) return SPHDEM_E_ARG;
         if (p->kernel_type < 0 || p->kernel_type > 5) return SPHDEM_E_ARG;
         if (!(p->dt > 0) || !(p->kappa > 0) || p->freq_filt <= 0 || !(p->gamma > 0)) return SPHDEM_E_ARG;
+        if (p->w_lanes != 0 && p->w_lanes != 1 && p->w_lanes != 2 && p->w_lanes != 4 && p->w_lanes != 8 &&
+            p->w_lanes != 16)
+            return SPHDEM_E_ARG;
         return SPHDEM_OK;
     }
     if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
@@ -1424,6 +1510,7 @@ extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, S
         p.ppe_max_iter = ov->ppe_max_iter;
         p.warm_hist = ov->warm_hist;
         p.warm_fit = ov->warm_fit;
+        p.w_lanes = ov->w_lanes;
         p.mlp_train_steps = ov->mlp_train_steps;
         p.mlp_updates = ov->mlp_updates;
         p.mlp_seed = ov->mlp_seed;

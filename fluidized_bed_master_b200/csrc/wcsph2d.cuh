@@ -2,18 +2,19 @@
 // dim 2): the reference's SOPHIA_single (WCSPH_Calc.cuh:15-340) for a
 // Lagrangian fluid, in its kernel order:
 //
-//   k_w_predictor   KERNEL_clc_predictor (functions_TIME.cuh:77-228)
-//   NNPS            hash / stable sort / gather every step
+//   k_w_predictor   KERNEL_clc_predictor (functions_TIME.cuh:77-228), with
+//                   the NNPS cell key of the predicted position
+//   NNPS            stable sort / gather every step
 //   k_w_list        neighbour list (kappa h_i, 9-cell stencil)
 //   k_w_kgc         KERNEL_clc_correction_KGC_2D (functions_PREP2.cuh:73-160)
 //   k_w_prep        KERNEL_clc_prep2D (functions_PREP2.cuh:1247-1420):
 //                   reference density, Shepard filter, density gradient
 //   k_w_continuity  KERNEL_clc_continuity_norm2D (functions_MASS.cuh:670-769)
-//   k_w_eos         KERNEL_EOS (functions_PROP.cuh:7-28)
+//                   and KERNEL_EOS (functions_PROP.cuh:7-28) in its epilogue
 //   k_w_interaction KERNEL_interaction2D (functions_INTERACTION.cuh:64-410)
 //   k_w_corrector   KERNEL_time_update_single (functions_TIME.cuh:676-880)
 //   k_w_xsph        KERNEL_xsph2D (functions_TIME.cuh:1520-1605)
-//   k_w_finish      corrected positions and density become the state
+//   k_w_finish      (XSPH on) corrected positions and density become the state
 //
 // The reference's stock 2-D driver cannot run a moving fluid: it sets the
 // ALE flags to Eulerian (KERNEL_set_alpha, functions_ALE.cuh:2-20), runs
@@ -74,18 +75,29 @@ __device__ __forceinline__ double w_dist(double xi, double yi, double xj, double
     return __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
 }
 
-// KERNEL_clc_predictor, Lagrangian (ALE flags 1), no MOVING particles
+// KERNEL_clc_predictor, Lagrangian (ALE flags 1), no MOVING particles,
+// fused with the NNPS cell key of the predicted position
+// (KERNEL_index_particle_to_cell, functions_NNPS.cuh:732-760): key[i],
+// val[i] = i, i_type 3 -> num_cells
 template <typename R>
-__global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
+__global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W, int* key, int* val) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ns || S.itype[i] == 3) return;
+    if (i >= P.ns) return;
+    val[i] = i;
+    if (S.itype[i] == 3) {
+        key[i] = P.num_cells;
+        return;
+    }
     int pt = S.ptype[i], bt = S.btype[i];
     double x0 = S.x[i], y0 = S.y[i];
     R ux0 = S.ux[i], uy0 = S.uy[i];
     double hdt = P.dt * 0.5;
+    double xp = x0, yp = y0;
     if (pt >= 0) {
-        S.x[i] = x0 + (double)ux0 * hdt * (double)(pt > 0);
-        S.y[i] = y0 + (double)uy0 * hdt * (double)(pt > 0);
+        xp = x0 + (double)ux0 * hdt * (double)(pt > 0);
+        yp = y0 + (double)uy0 * hdt * (double)(pt > 0);
+        S.x[i] = xp;
+        S.y[i] = yp;
         R b = (R)(bt == 0);
         S.ux[i] = ux0 + W.ftx[i] * b * (R)hdt;
         S.uy[i] = uy0 + W.fty[i] * b * (R)hdt;
@@ -97,32 +109,70 @@ __global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
     double rho = S.rho[i];
     S.rho0[i] = rho;
     if (Q.rho_cont && pt > 0) S.rho[i] = rho + (double)W.drho[i] * hdt;
+    int ic, jc, kc;
+    cell_ijk(P, xp, yp, S.z[i], ic, jc, kc);
+    key[i] = ic + P.NI * jc + P.NI * P.NJ * kc;
 }
 
+// ---- lanes per particle ------------------------------------------------
+// The gathers run L lanes per particle (L = 1, 2, 4, 8, 16; a group of L
+// consecutive threads of one warp).  Lane l takes list entries l, l+L, ...
+// and the group adds its partial sums with a fixed xor tree, so a given L
+// gives bit-identical results run to run.  The list build visits candidate
+// slots in ascending order L at a time and compacts the hits with a ballot
+// in that order, so the list is the same for every L.
+template <int L>
+struct Grp {
+    int i, lane;
+    unsigned mask;   // the group's lanes in the warp
+    int base;        // the group's first lane in the warp
+    __device__ __forceinline__ Grp() {
+        int t = blockIdx.x * blockDim.x + threadIdx.x;
+        i = t / L;
+        lane = threadIdx.x % L;
+        base = (threadIdx.x & 31) & ~(L - 1);
+        mask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << base;
+    }
+    template <typename T>
+    __device__ __forceinline__ T sum(T v) const {
+#pragma unroll
+        for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+};
+
 // neighbour list: sqrt(dx^2+dy^2) + 1e-20 < kappa h_i, FP64, exact
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_list(DevParams P, WState<R> S, const int4* __restrict__ rows, int* nbr,
                                                 int* ncnt, DevFlags* F) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ns) return;
+    const Grp<L> g;
+    const int i = g.i;
+    if (i >= P.ns) return;   // the whole group
     double xi = S.x[i], yi = S.y[i];
     double Rr = __dmul_rn(P.kappa, S.h[i]);
     int ic, jc, kc;
     cell_ijk(P, xi, yi, 0.0, ic, jc, kc);
     int c = 0, cap = P.nb_cap, n = P.ns;
     const Cull cu = make_cull(xi, yi, 0.0, Rr);
+    const unsigned low = (1u << g.lane) - 1u;
     for_rows(P, ic, jc, kc, rows, cu, [&](int a, int b) {
-        for (int j = a; j < b; j++) {
-            if (S.ptype[j] > 1000) continue;
-            if (__dadd_rn(w_dist(xi, yi, S.x[j], S.y[j]), 1e-20) < Rr) {
-                if (nbr && c < cap) nbr[(size_t)c * n + i] = j;
-                c++;
+        for (int j0 = a; j0 < b; j0 += L) {
+            const int j = j0 + g.lane;
+            bool hit = false;
+            if (j < b && S.ptype[j] <= 1000) hit = __dadd_rn(w_dist(xi, yi, S.x[j], S.y[j]), 1e-20) < Rr;
+            unsigned grp = (__ballot_sync(g.mask, hit) & g.mask) >> g.base;
+            if (hit) {
+                int pos = c + __popc(grp & low);
+                if (nbr && pos < cap) nbr[(size_t)pos * n + i] = j;
             }
+            c += __popc(grp);
         }
     });
-    ncnt[i] = c;
-    if (c > cap) atomicOr(&F->overflow, 1);
-    atomicMax(&F->max_ncnt, c);
+    if (g.lane == 0) {
+        ncnt[i] = c;
+        if (c > cap) atomicOr(&F->overflow, 1);
+        atomicMax(&F->max_ncnt, c);
+    }
 }
 
 template <typename R>
@@ -142,16 +192,16 @@ __device__ __forceinline__ void w_kgc(const R* __restrict__ Cm, int n, int i, R&
 }
 
 // KERNEL_clc_correction_KGC_2D
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_kgc(DevParams P, WState<R> S, WWork<R> W) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.ns;
+    const Grp<L> g;
+    const int i = g.i, n = P.ns;
     if (i >= n || S.itype[i] > 2 || S.ptype[i] > 1000) return;
     double xi = S.x[i], yi = S.y[i];
     R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, 2, th);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R txx = 0, txy = 0, tyy = 0;
-    for (int k = 0; k < cnt; k++) {
+    for (int k = g.lane; k < cnt; k += L) {
         int j = W.nbr[(size_t)k * n + i];
         R dx, dy, r;
         w_pair<R>(xi, yi, S.x[j], S.y[j], dx, dy, r);
@@ -162,6 +212,10 @@ __global__ void __launch_bounds__(128) k_w_kgc(DevParams P, WState<R> S, WWork<R
         t = -mtd * dy * dx; t *= rtd; txy += t;
         t = -mtd * dy * dy; t *= rtd; tyy += t;
     }
+    txx = g.sum(txx);
+    txy = g.sum(txy);
+    tyy = g.sum(tyy);
+    if (g.lane) return;
     R det = txx * tyy - txy * txy;
     R c00 = 1, c01 = 0, c10 = 0, c11 = 1;
     if (fabs(det) > (R)1e-4) {
@@ -179,11 +233,11 @@ __global__ void __launch_bounds__(128) k_w_kgc(DevParams P, WState<R> S, WWork<R
 
 // KERNEL_clc_prep2D: reference density, Shepard filter (every freq_filt
 // steps), density gradient for Antuono's delta-SPH (corrected when KGC)
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_prep(DevParams P, WParams Q, WState<R> S, WWork<R> W,
                                                 const DevFlags* F) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.ns;
+    const Grp<L> g;
+    const int i = g.i, n = P.ns;
     if (i >= n || S.itype[i] > 2 || S.ptype[i] > 1000) return;
     const int count = F->step_count;   // the host loop's count (vii[43])
     double xi = S.x[i], yi = S.y[i];
@@ -192,7 +246,7 @@ __global__ void __launch_bounds__(128) k_w_prep(DevParams P, WParams Q, WState<R
     const bool filt = (count % Q.freq_filt) == 0, anto = Q.delsph == 2, kgc = P.kgc == 1;
     int cnt = min(W.ncnt[i], P.nb_cap);
     R flt = 0, gx = 0, gy = 0;
-    for (int k = 0; k < cnt; k++) {
+    for (int k = g.lane; k < cnt; k += L) {
         int j = W.nbr[(size_t)k * n + i];
         R dx, dy, r;
         w_pair<R>(xi, yi, S.x[j], S.y[j], dx, dy, r);
@@ -208,6 +262,10 @@ __global__ void __launch_bounds__(128) k_w_prep(DevParams P, WParams Q, WState<R
             gy += -dr * (mj / rhoj) * ty;
         }
     }
+    flt = g.sum(flt);
+    gx = g.sum(gx);
+    gy = g.sum(gy);
+    if (g.lane) return;
     double v = S.h[i] / 1.6;
     W.rho_ref[i] = S.m[i] / (v * v);
     if (filt) S.flt_s[i] = flt;
@@ -218,10 +276,10 @@ __global__ void __launch_bounds__(128) k_w_prep(DevParams P, WParams Q, WState<R
 }
 
 // KERNEL_clc_continuity_norm2D
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_continuity(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.ns;
+    const Grp<L> g;
+    const int i = g.i, n = P.ns;
     if (i >= n || S.itype[i] > 2 || S.ptype[i] > 1000) return;
     int pti = S.ptype[i];
     double xi = S.x[i], yi = S.y[i];
@@ -233,7 +291,7 @@ __global__ void __launch_bounds__(128) k_w_continuity(DevParams P, WParams Q, WS
     const bool kgc = P.kgc == 1, anto = Q.delsph == 2;
     int cnt = min(W.ncnt[i], P.nb_cap);
     R tx = 0, ty = 0, tr = 0;
-    for (int k = 0; k < cnt; k++) {
+    for (int k = g.lane; k < cnt; k += L) {
         int j = W.nbr[(size_t)k * n + i];
         R dx, dy, r;
         w_pair<R>(xi, yi, S.x[j], S.y[j], dx, dy, r);
@@ -255,24 +313,26 @@ __global__ void __launch_bounds__(128) k_w_continuity(DevParams P, WParams Q, WS
             tr += t;
         }
     }
+    tx = g.sum(tx);
+    ty = g.sum(ty);
+    tr = g.sum(tr);
+    if (g.lane) return;
     W.drho[i] = (tx + ty) * (R)(rhoi_d / W.rho_ref[i]) + tr * (R)(Q.delsph > 0);
-}
-
-// KERNEL_EOS (Tait)
-template <typename R>
-__global__ void k_w_eos(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ns || S.itype[i] > 2 || S.ptype[i] > 1000 || S.btype[i] != 0) return;
-    double tP = pow(S.rho[i] / W.rho_ref[i], Q.gamma);
-    S.pres[i] = (R)(Q.eos_B * (tP - 1.0));
+    // KERNEL_EOS (functions_PROP.cuh:7-28), Tait, for the same rows with
+    // buffer_type 0: it reads only row i's density and reference density,
+    // and nothing in this pass reads a pressure
+    if (S.btype[i] == 0) {
+        double tP = pow(rhoi_d / W.rho_ref[i], Q.gamma);
+        S.pres[i] = (R)(Q.eos_B * (tP - 1.0));
+    }
 }
 
 // KERNEL_interaction2D (i_type 1): pressure, viscous and artificial-viscosity
 // forces and gravity along -y
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_interaction(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.ns;
+    const Grp<L> g;
+    const int i = g.i, n = P.ns;
     if (i >= n || S.itype[i] != 1 || S.ptype[i] > 1000) return;
     double xi = S.x[i], yi = S.y[i];
     R th = (R)S.h[i], tA = knl_tmpA<R>(P.kernel_type, 2, th);
@@ -282,7 +342,7 @@ __global__ void __launch_bounds__(128) k_w_interaction(DevParams P, WParams Q, W
     const bool kgc = P.kgc == 1;
     int cnt = min(W.ncnt[i], P.nb_cap);
     R tx = 0, ty = 0, pgx = 0, pgy = 0;
-    for (int k = 0; k < cnt; k++) {
+    for (int k = g.lane; k < cnt; k += L) {
         int j = W.nbr[(size_t)k * n + i];
         R dx, dy, r;
         w_pair<R>(xi, yi, S.x[j], S.y[j], dx, dy, r);
@@ -322,6 +382,11 @@ __global__ void __launch_bounds__(128) k_w_interaction(DevParams P, WParams Q, W
             }
         }
     }
+    tx = g.sum(tx);
+    ty = g.sum(ty);
+    pgx = g.sum(pgx);
+    pgy = g.sum(pgy);
+    if (g.lane) return;
     if (P.fg) ty += -(R)P.g_sph;
     W.ftx[i] = tx;
     W.fty[i] = ty;
@@ -330,14 +395,22 @@ __global__ void __launch_bounds__(128) k_w_interaction(DevParams P, WParams Q, W
     W.pgfy[i] = pgy;
 }
 
-// KERNEL_time_update_single (velocity, density; positions when XSPH is off)
+// KERNEL_time_update_single (velocity, density; positions when XSPH is off).
+// Without XSPH no later pass reads the predicted positions and density, so
+// the corrected ones go straight into the state; with XSPH they wait in
+// xn, yn, rhon for k_w_finish.  Thread 0 also advances the device step
+// counter (read by the next step's prep).
 template <typename R>
-__global__ void k_w_corrector(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
+__global__ void k_w_corrector(DevParams P, WParams Q, WState<R> S, WWork<R> W, DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) F->step_count += 1;
     if (i >= P.ns) return;
-    W.xn[i] = S.x[i];
-    W.yn[i] = S.y[i];
-    W.rhon[i] = S.rho[i];
+    const bool direct = !P.xsph;
+    if (!direct) {
+        W.xn[i] = S.x[i];
+        W.yn[i] = S.y[i];
+        W.rhon[i] = S.rho[i];
+    }
     if (S.itype[i] == 3) return;
     int pt = S.ptype[i], bt = S.btype[i];
     R ux0 = S.ux0[i], uy0 = S.uy0[i], ax = 0, ay = 0;
@@ -353,21 +426,25 @@ __global__ void k_w_corrector(DevParams P, WParams Q, WState<R> S, WWork<R> W) {
         uxc = ux0;
         uyc = uy0;
     }
-    if (!P.xsph) {
-        W.xn[i] = S.x0[i] + (double)uxc * P.dt * (double)(pt > 0);
-        W.yn[i] = S.y0[i] + (double)uyc * P.dt * (double)(pt > 0);
+    if (direct) {
+        S.x[i] = S.x0[i] + (double)uxc * P.dt * (double)(pt > 0);
+        S.y[i] = S.y0[i] + (double)uyc * P.dt * (double)(pt > 0);
     }
     S.ux[i] = uxc;
     S.uy[i] = uyc;
-    if (Q.rho_cont && pt > 0) W.rhon[i] = S.rho0[i] + (double)W.drho[i] * P.dt;
+    if (Q.rho_cont && pt > 0) {
+        double rn = S.rho0[i] + (double)W.drho[i] * P.dt;
+        if (direct) S.rho[i] = rn;
+        else W.rhon[i] = rn;
+    }
 }
 
 // KERNEL_xsph2D: positions from the corrected velocity plus the XSPH term
 // (neighbours' corrected velocity, predicted positions and density)
-template <typename R>
+template <typename R, int L>
 __global__ void __launch_bounds__(128) k_w_xsph(DevParams P, WState<R> S, WWork<R> W) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.ns;
+    const Grp<L> g;
+    const int i = g.i, n = P.ns;
     if (i >= n || S.itype[i] != 1 || S.ptype[i] > 1000) return;
     int pt = S.ptype[i];
     double xi = S.x[i], yi = S.y[i];
@@ -376,7 +453,7 @@ __global__ void __launch_bounds__(128) k_w_xsph(DevParams P, WState<R> S, WWork<
     R c = (R)P.c_xsph;
     int cnt = min(W.ncnt[i], P.nb_cap);
     R tx = 0, ty = 0;
-    for (int k = 0; k < cnt; k++) {
+    for (int k = g.lane; k < cnt; k += L) {
         int j = W.nbr[(size_t)k * n + i];
         R dx, dy, r;
         w_pair<R>(xi, yi, S.x[j], S.y[j], dx, dy, r);
@@ -385,6 +462,9 @@ __global__ void __launch_bounds__(128) k_w_xsph(DevParams P, WState<R> S, WWork<
         tx += c * mj / rhoj * (-uxi + S.ux[j]) * w / flt;
         ty += c * mj / rhoj * (-uyi + S.uy[j]) * w / flt;
     }
+    tx = g.sum(tx);
+    ty = g.sum(ty);
+    if (g.lane) return;
     W.xn[i] = S.x0[i] + ((double)uxi + (double)tx) * P.dt * (double)(pt > 0);
     W.yn[i] = S.y0[i] + ((double)uyi + (double)ty) * P.dt * (double)(pt > 0);
 }

@@ -17,7 +17,7 @@ _I32 = [
     "turbulence_model", "concn_solve", "min_iteration", "max_iteration",
     "penetration_solve", "switch_ptype", "noslip_bc", "decouple_stride",
     "ppe_mode", "warm_start", "ppe_max_iter", "precision", "dem_wall_mask",
-    "mlp_train_steps", "mlp_updates", "mlp_seed", "warm_hist", "warm_fit",
+    "mlp_train_steps", "mlp_updates", "mlp_seed", "warm_hist", "warm_fit", "w_lanes",
 ]
 _F64_A = [
     "kappa", "p_ref", "gamma", "dt", "time", "time_end",
@@ -34,7 +34,6 @@ _F64_B = [
 _F64_C = ["cone_r1", "cone_r2", "cone_h", "wall_rest_n", "wall_rest_s", "wall_mu_s", "wall_mu_rs"]
 
 _fields = [(n, C.c_int32) for n in _I32]
-_fields += [("reserved_i", C.c_int32 * 1)]
 _fields += [(n, C.c_double) for n in _F64_A]
 _fields += [("margin", C.c_double * 6)]
 _fields += [(n, C.c_double) for n in _F64_B]
@@ -70,7 +69,7 @@ class SphdemStats(C.Structure):
         ("ppe_status", C.c_int32), ("mlp_phase", C.c_int32), ("mlp_loss", C.c_double),
         ("mlp_trained_steps", C.c_int32), ("reserved_stats", C.c_int32),
         ("ppe_initial_residual", C.c_double),
-        ("ppe_warm_gain", C.c_double), ("ppe_warm_dirs", C.c_int32), ("reserved_stats2", C.c_int32),
+        ("ppe_warm_gain", C.c_double), ("ppe_warm_dirs", C.c_int32), ("w_lanes", C.c_int32),
     ]
 
 

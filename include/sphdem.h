@@ -146,7 +146,7 @@ typedef struct SphdemParams {
     int32_t mlp_seed;           /* WARM_MLP: initialisation seed */
     int32_t warm_hist;          /* WARM_PROJECT/MLP: previous pressure changes used (0..SPHDEM_WARM_HIST_MAX) */
     int32_t warm_fit;           /* WARM_PROJECT/MLP: SPHDEM_FIT_* bits */
-    int32_t reserved_i[1];
+    int32_t w_lanes;            /* 2-D WCSPH: lanes per particle of the gathers (1,2,4,8,16); 0 = timed at commit */
 
     /* -- real switches: vif[] of function_init.cuh:59-100 -- */
     double kappa;               /* vif[0]  */
@@ -248,7 +248,7 @@ typedef struct SphdemStats {
                                    error norm that the fit achieves (larger is better; comparable
                                    between runs on the same state with the same warm_fit) */
     int32_t ppe_warm_dirs;      /* directions the last fit kept */
-    int32_t reserved_stats2;
+    int32_t w_lanes;            /* 2-D WCSPH: lanes per particle in use (w_lanes or the commit-time choice) */
 } SphdemStats;
 
 typedef struct SphdemHandle SphdemHandle;
@@ -277,7 +277,7 @@ int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem,
 /* Read input_dir/solv.txt, input_dir/data.txt and input_dir/input.txt
  * (function_init.cuh:216-1182, ISPH.cuh:55-113) and create an engine.
  * ov may be NULL; when given, its non-switch engine extensions
- * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit,
+ * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit, w_lanes,
  * mlp_train_steps, mlp_updates, mlp_seed, mlp_lr) override the defaults. */
 int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
                            SphdemHandle** out);

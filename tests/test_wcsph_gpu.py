@@ -42,8 +42,9 @@ def _engine(p, sph, prec):
     return Engine(q, sph, {})
 
 
-def _bed(variant, seed=41, dx=5.0e-3):
+def _bed(variant, seed=41, dx=5.0e-3, lanes=0):
     p, sph, _ = dam_break_2d(dx=dx, seed=seed)
+    p.w_lanes = lanes
     for k, v in VARIANTS[variant].items():
         setattr(p, k, v)
     return p, sph
@@ -110,7 +111,7 @@ def test_wcsph_fp32_within_1e5_after_100_steps():
 def test_wcsph_runs_are_deterministic_and_stats():
     """Two handles on the same input give bit-identical states (no atomics
     in any sum); stats report the fluid's motion."""
-    p, sph = _bed("kgc_antuono_xsph", seed=43)
+    p, sph = _bed("kgc_antuono_xsph", seed=43, lanes=4)
     a = _engine(p, sph, 1)
     b = _engine(p, sph, 1)
     a.step(10)
@@ -127,7 +128,7 @@ def test_wcsph_runs_are_deterministic_and_stats():
 
 def test_wcsph_graphs_equal_eager():
     """The captured step graph and eager launches give identical states."""
-    p, sph = _bed("kgc_antuono_xsph", seed=44)
+    p, sph = _bed("kgc_antuono_xsph", seed=44, lanes=8)
     a = _engine(p, sph, 1)
     b = _engine(p, sph, 1)
     b.set_graphs(False)
@@ -141,7 +142,7 @@ def test_wcsph_bulk_state_roundtrip():
     """get_fields/set_fields of the whole WCSPH state (the e2e path) leave
     the run bit-identical."""
     fields = ["x", "y", "ux", "uy", "rho", "pres", "flt_s", "ftotalx", "ftotaly", "drho"]
-    p, sph = _bed("plain", seed=45)
+    p, sph = _bed("plain", seed=45, lanes=2)
     a = _engine(p, sph, 0)
     b = _engine(p, sph, 0)
     a.step(3)
@@ -155,6 +156,32 @@ def test_wcsph_bulk_state_roundtrip():
     b.step(2)
     for f in fields:
         assert np.array_equal(a.get(SPH, f), b.get(SPH, f)), f
+
+
+def test_wcsph_lanes_per_particle_agree():
+    """Every lane count gives the same cell order and neighbour lists, and
+    the same FP64 fields to rounding (rel. L2 <= 1e-12 after 10 steps): L
+    only changes the order of the sums inside a particle.  The commit-time
+    autotuner picks one of them and reports it."""
+    p, sph = _bed("kgc_antuono_xsph", seed=46)
+    ref = None
+    for lanes in (1, 2, 4, 8, 16):
+        q = p.copy()
+        q.w_lanes = lanes
+        e = _engine(q, sph, 1)
+        e.step(10)
+        assert e.stats()["w_lanes"] == lanes
+        c, lst = e.neighbors()
+        st = {f: e.get(SPH, f) for f in ("pid", "x", "y", "ux", "uy", "rho", "pres")}
+        if ref is None:
+            ref = (c, lst, st)
+            continue
+        assert np.array_equal(c, ref[0]) and np.array_equal(lst, ref[1]), lanes
+        assert np.array_equal(st["pid"], ref[2]["pid"]), lanes
+        for f in ("x", "y", "ux", "uy", "rho", "pres"):
+            assert rel_l2(st[f], ref[2][f]) <= 1e-12, (lanes, f)
+    auto = _engine(p, sph, 1)
+    assert auto.stats()["w_lanes"] in (1, 2, 4, 8, 16)
 
 
 W_GOLD = [g for g in golden_files() if json.loads(np.load(g)["meta"].tobytes()).get("solver") == "wcsph"]
