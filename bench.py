@@ -46,9 +46,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "ppe-profile"],
+    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "dam2d-batch", "ppe-profile"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
-                         "(its protocol is --steps 1000); ppe-profile: --steps steps of the bed with the "
+                         "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
+                         "against the same beds run one after another; ppe-profile: --steps steps of the bed with the "
                          "projected-start PCG and step graphs off, so that a kernel profiler sees the PPE "
                          "kernels (no timing)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
@@ -340,6 +341,143 @@ def run_ppe_profile(args):
     print(json.dumps({"workload": "ppe-profile", "steps": args.steps, "ppe_iters": s["ppe_iters"],
                       "ppe_status": s["ppe_status"], "n_sph": eng.ns, "n_dem": eng.nd}), flush=True)
     eng.close()
+
+
+def _timed_steps(eng, stream, flush, k):
+    """Device time (ms) of k steps, each timed with events on the engine's
+    stream after a 256 MB L2 flush."""
+    import torch
+
+    tot = 0.0
+    for _ in range(k):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        eng.step(1)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        tot += e0.elapsed_time(e1)
+    return tot
+
+
+def run_dam2d_batch(args, world, rank, local, pg):
+    """64 dam breaks of uneven size (fluid counts log-uniform in [2k, 50k],
+    seeded) in one handle, one step graph for all; against the same beds
+    stepped one after another, each in its own handle."""
+    import torch
+
+    from fluidized_bed_master_b200.beds import dam_break_batch
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import SPH
+
+    metric = "2-D WCSPH particle-updates/s on 1 B200 (64 uneven dam breaks in one handle)"
+    unit = "particle-updates/s"
+    text = ("64 independent 2-D WCSPH dam breaks in one handle (sphdem_create_batch), fluid counts log-uniform in "
+            "[2,000, 50,000] (seeded), columns twice as high as wide in tanks 4 columns wide, three wall layers, "
+            "dx=5 mm, shared parameters (sound speed and CFL dt of the tallest column)")
+    p, beds = dam_break_batch(seed=rank)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import Oracle
+        threads = os.cpu_count() or 1
+        sel = [b for b in beds if len(b["x"]) < 8000][:2]
+        t0, k, npart = time.perf_counter(), 0, sum(len(b["x"]) for b in sel)
+        orcs = [Oracle(p, b, {}, threads=threads) for b in sel]
+        while time.perf_counter() - t0 < max(5.0, args.cpu_seconds) and k < 2000:
+            for o in orcs:
+                o.step(5)
+            k += 5
+        el = time.perf_counter() - t0
+        val = npart * k / el
+        line = {"metric": metric, "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded dam breaks)",
+                "config": {"workload": text},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": f"2 of the beds ({npart} particles), {k} steps each"},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local)
+    q = p.copy()
+    q.precision = 1 if args.precision == "fp64" else 0
+    eng = Engine.batch(q, beds)
+    n = eng.ns
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
+    sampler = ClockSampler(int(vis) if vis.isdigit() else local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches = 0
+    t_batch = 0.0
+    for _ in range(args.steps):
+        t_batch += _timed_steps(eng, stream, flush, 1)
+        launches += eng.launches()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    t_max = reduce_over_ranks(pg, t_batch, "max", "cuda")
+    n_all = reduce_over_ranks(pg, n, "sum", "cuda")
+    value = n_all * args.steps / (t_max / 1e3)
+    lanes = eng.stats()["w_lanes"]
+    e2e = None
+    if not args.no_e2e:
+        def pinned(k, dt):
+            return torch.empty(k, dtype=dt, pin_memory=True).numpy()
+        hs = {f: pinned(n, torch.float64) for f in W_STATE}
+        for f in W_STATE:
+            hs[f][:] = eng.get(SPH, f)
+        hb = sum(a.nbytes for a in hs.values())
+        ke = max(3, min(args.steps, 50))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            eng.set_fields(SPH, hs)
+            eng.step(1)
+            eng.get_fields(SPH, hs)
+        torch.cuda.synchronize()
+        te = reduce_over_ranks(pg, time.perf_counter() - t0, "max", "cuda")
+        e2e = {"value": n_all * ke / te, "unit": unit, "h2d_bytes_per_step": hb, "d2h_bytes_per_step": hb,
+               "ms_per_step": te / ke * 1e3,
+               "how": "per step: sphdem_set_fields of all beds' state (x, y in each bed's own coordinates) from "
+                      "pinned host arrays, sphdem_step, sphdem_get_fields back"}
+    eng.close()
+    # the same beds one after another, each in its own handle (same lanes)
+    seq_ms, ks = 0.0, 10
+    if rank == 0:
+        q1 = q.copy()
+        q1.w_lanes = lanes
+        for bd in beds:
+            e = Engine(q1, bd, {})
+            st = torch.cuda.ExternalStream(e.stream_ptr())
+            e.step(3)
+            seq_ms += _timed_steps(e, st, flush, ks) / ks
+            e.close()
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if q.precision == 0 else "f64", "data": "synthetic (seeded dam breaks)",
+        "config": {"workload": text, "n": n, "beds": len(beds), "bed_sizes": [len(b["x"]) for b in beds],
+                   "l2": "256 MB buffer written before every timed step", "w_lanes": lanes,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "sequential": {"ms_per_step": seq_ms, "how": f"each bed alone in its own handle, {ks} timed steps each "
+                       "after 3 warm-up steps, per-step device times summed over the beds",
+                       "value": n * 1e3 / seq_ms if seq_ms else None, "unit": unit},
+        "batch_speedup_vs_sequential": (seq_ms / (t_max / args.steps)) if seq_ms else None,
+        "roofline": None, "cpu_baseline": None, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_dam2d(args, world, rank, local, pg):
@@ -675,6 +813,8 @@ def main():
     try:
         if args.workload == "dam2d":
             run_dam2d(args, world, rank, local, pg)
+        elif args.workload == "dam2d-batch":
+            run_dam2d_batch(args, world, rank, local, pg)
         elif args.workload == "ppe-profile":
             if rank == 0:
                 run_ppe_profile(args)

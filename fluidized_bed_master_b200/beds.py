@@ -363,3 +363,26 @@ def write_input_dir(path, p, sph, dem):
     write_input_txt(os.path.join(path, "input.txt"), sph, dem)
     with open(os.path.join(path, "data.txt"), "w") as fh:
         fh.write(DATA_TXT)
+
+
+def dam_break_batch(n_beds=64, n_min=2_000, n_max=50_000, seed=0, dx=5.0e-3, reference_compat=False):
+    """Uneven batch of 2-D dam breaks for sphdem_create_batch: bed b has a
+    water column of about N_b fluid particles (N_b drawn log-uniform in
+    [n_min, n_max], seeded), twice as high as wide, in a tank 4 columns wide
+    and 1.25 columns high, with three wall layers.  The beds share one
+    parameter set: the sound speed of the tallest column and its CFL time
+    step.  Returns (params, [sph dict per bed])."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=n_beds))
+    beds, params = [], None
+    hmax = 0.0
+    for b, nf in enumerate(counts):
+        w = max(4, int(round(np.sqrt(nf / 2.0)))) * dx
+        col = (w, 2.0 * w)
+        tank = (4.0 * w, 2.5 * w)
+        p, sph, _ = dam_break_2d(dx=dx, seed=seed * 1000 + b, tank=tank, column=col,
+                                 reference_compat=reference_compat)
+        beds.append(sph)
+        if col[1] > hmax:
+            hmax, params = col[1], p
+    return params, beds

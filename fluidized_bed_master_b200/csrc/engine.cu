@@ -1044,6 +1044,8 @@ static void w_alloc_state(Alloc& A, WState<R>& S, int n) {
     S.x0 = A.get<double>(n); S.y0 = A.get<double>(n); S.rho0 = A.get<double>(n);
     S.ux0 = A.get<R>(n); S.uy0 = A.get<R>(n);
     S.ptype = A.get<int>(n); S.btype = A.get<int>(n); S.itype = A.get<int>(n); S.pid = A.get<int>(n);
+    S.bed = nullptr;
+    S.boff = nullptr;
 }
 
 // NNPS of the WCSPH state: S[src] -> S[dst] in cell order (hashed: the
@@ -1055,7 +1057,7 @@ static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst, bool ha
     cudaStream_t st = H->stream;
     int n = P.ns;
     WState<R>& S = EH->S[src];
-    if (!hashed) k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+    if (!hashed) k_w_hash<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W.key_in, W.val_in);
     size_t bytes = EH->sort_tmp_bytes;
     CK(cub::DeviceRadixSort::SortPairs(EH->sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
                                        key_bits(P.num_cells), st));
@@ -1205,13 +1207,69 @@ static int w_tune_lanes(SphdemHandle* H, WEngineHost<R>* EH) {
     return SPHDEM_OK;
 }
 
+// Placement of a batch (sphdem_create_batch): bed b's cells are computed at
+// (x + ox_b, y + oy_b), which puts the beds side by side on shelves with a
+// gap of at least 8 cells (and 5 % of the bed) between beds, so that no
+// stencil of one bed reaches another; positions stay as given.
+static void place_batch(SphdemHandle* H, double dcell) {
+    const auto& X = H->stage_d[0][SPHDEM_F_X];
+    const auto& Y = H->stage_d[0][SPHDEM_F_Y];
+    int nb = (int)H->bed_start.size() - 1;
+    std::vector<double> x0(nb), x1(nb), y0(nb), y1(nb);
+    double area = 0, wmax = 0;
+    for (int b = 0; b < nb; b++) {
+        int a = H->bed_start[b], e = H->bed_start[b + 1];
+        x0[b] = x1[b] = X[a];
+        y0[b] = y1[b] = Y[a];
+        for (int k = a; k < e; k++) {
+            x0[b] = std::min(x0[b], X[k]); x1[b] = std::max(x1[b], X[k]);
+            y0[b] = std::min(y0[b], Y[k]); y1[b] = std::max(y1[b], Y[k]);
+        }
+        double g = std::max(8.0 * dcell, 0.05 * std::max(x1[b] - x0[b], y1[b] - y0[b]));
+        area += (x1[b] - x0[b] + g) * (y1[b] - y0[b] + g);
+        wmax = std::max(wmax, x1[b] - x0[b] + g);
+    }
+    double limit = std::max(wmax, std::sqrt(area));
+    double cx = 0, cy = 0, shelf = 0;
+    H->bed_off.assign(2 * nb, 0.0);
+    for (int b = 0; b < nb; b++) {
+        double g = std::max(8.0 * dcell, 0.05 * std::max(x1[b] - x0[b], y1[b] - y0[b]));
+        double w = x1[b] - x0[b] + g, h = y1[b] - y0[b] + g;
+        if (cx > 0 && cx + w > limit) {
+            cy += shelf;
+            cx = 0;
+            shelf = 0;
+        }
+        H->bed_off[2 * b] = cx - x0[b];
+        H->bed_off[2 * b + 1] = cy - y0[b];
+        cx += w;
+        shelf = std::max(shelf, h);
+    }
+}
+
 template <typename R>
 static int w_commit_t(SphdemHandle* H) {
     const SphdemParams& p = H->p;
     int ns = H->ns;
-    // bounding box and grid as the ISPH engine (function_init.cuh:913-950)
+    if (!H->bed_start.empty()) {
+        if (H->have_file_order) return SPHDEM_E_ARG;
+        auto& hv = H->stage_d[0][SPHDEM_F_H];
+        if ((int)hv.size() != ns || (int)H->stage_d[0][SPHDEM_F_X].size() != ns ||
+            (int)H->stage_d[0][SPHDEM_F_Y].size() != ns)
+            return SPHDEM_E_INPUT;
+        double hmax = 0;
+        for (double v : hv) hmax = std::max(hmax, v);
+        place_batch(H, 1.1 * p.kappa * hmax);
+    }
+    // bounding box and grid as the ISPH engine (function_init.cuh:913-950);
+    // a batch's box is that of the placed beds
     std::vector<double> fx = H->have_file_order ? H->file_x : H->stage_d[0][SPHDEM_F_X];
     std::vector<double> fy = H->have_file_order ? H->file_y : H->stage_d[0][SPHDEM_F_Y];
+    for (int b = 0; b + 1 < (int)H->bed_start.size(); b++)
+        for (int k = H->bed_start[b]; k < H->bed_start[b + 1]; k++) {
+            fx[k] += H->bed_off[2 * b];
+            fy[k] += H->bed_off[2 * b + 1];
+        }
     std::vector<double> fz = H->have_file_order ? H->file_z : H->stage_d[0][SPHDEM_F_Z];
     double h0 = H->have_file_order ? H->file_h0 : H->stage_d[0][SPHDEM_F_H][0];
     int n = (int)fx.size();
@@ -1251,6 +1309,19 @@ static int w_commit_t(SphdemHandle* H) {
     Alloc& A = EH->A;
     w_alloc_state<R>(A, EH->S[0], ns);
     w_alloc_state<R>(A, EH->S[1], ns);
+    if (!H->bed_start.empty()) {
+        int nb = (int)H->bed_start.size() - 1;
+        EH->S[0].bed = A.get<int>(ns);
+        EH->S[1].bed = A.get<int>(ns);
+        double2* boff = A.get<double2>(nb);
+        if (!A.ok) return SPHDEM_E_NOMEM;
+        CK(cudaMemcpy(boff, H->bed_off.data(), sizeof(double2) * nb, cudaMemcpyHostToDevice));
+        std::vector<int> bed(ns);
+        for (int b = 0; b < nb; b++)
+            for (int k = H->bed_start[b]; k < H->bed_start[b + 1]; k++) bed[k] = b;
+        CK(cudaMemcpy(EH->S[0].bed, bed.data(), sizeof(int) * ns, cudaMemcpyHostToDevice));
+        EH->S[0].boff = EH->S[1].boff = boff;
+    }
     WWork<R>& W = EH->W;
     W.ftx = A.get<R>(ns); W.fty = A.get<R>(ns); W.ftot = A.get<R>(ns); W.drho = A.get<R>(ns);
     W.rho_ref = A.get<double>(ns); W.grx = A.get<R>(ns); W.gry = A.get<R>(ns); W.pgfx = A.get<R>(ns);
@@ -1657,6 +1728,32 @@ static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, voi
     return SPHDEM_OK;
 }
 
+extern "C" int sphdem_create_batch(const SphdemParams* p, int32_t nbeds, const int32_t* n_per_bed,
+                                   SphdemHandle** out) {
+    if (!p || !out || !n_per_bed || nbeds <= 0) return SPHDEM_E_ARG;
+    *out = nullptr;
+    if (p->solver_type != SPHDEM_WCSPH || p->dim != 2) return SPHDEM_E_UNSUPPORTED;
+    std::vector<int> start(nbeds + 1, 0);
+    long long tot = 0;
+    for (int b = 0; b < nbeds; b++) {
+        if (n_per_bed[b] <= 0) return SPHDEM_E_ARG;
+        tot += n_per_bed[b];
+        if (tot > (1ll << 30)) return SPHDEM_E_NOMEM;
+        start[b + 1] = (int)tot;
+    }
+    int r = sphdem_create(p, (int32_t)tot, 0, out);
+    if (r) return r;
+    (*out)->bed_start = start;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_batch_offsets(SphdemHandle* h, double* offsets) {
+    if (!h || !offsets || h->bed_start.empty()) return SPHDEM_E_ARG;
+    if (!h->committed) return SPHDEM_E_ARG;
+    std::memcpy(offsets, h->bed_off.data(), sizeof(double) * h->bed_off.size());
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields, const int32_t* fields,
                                  const double* const* host_src) {
     if (!h || !h->committed || !fields || !host_src || (which != 0 && which != 1) || nfields < 0 ||
@@ -1684,9 +1781,8 @@ extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const voi
         if (h->kind == 1) {   // 2-D WCSPH: through the bulk path
             if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
             int32_t f = field;
-            const void* srcs[1] = {src};
-            return h->prec == SPHDEM_PREC_FP64 ? bulk_t<double>(h, which, 1, &f, (void* const*)srcs, true)
-                                               : bulk_t<float>(h, which, 1, &f, (void* const*)srcs, true);
+            const double* s = (const double*)src;
+            return sphdem_set_fields(h, which, 1, &f, &s);
         }
         if (!is_real_field(field) || bytes != sizeof(double) * (size_t)n) return SPHDEM_E_ARG;
         return h->prec == SPHDEM_PREC_FP64 ? set_state_t<double>(h, which, field, src, n)
@@ -1772,10 +1868,11 @@ extern "C" int sphdem_get_field(SphdemHandle* h, int which, int field, void* dst
     }
     size_t need = (is_int_field(field) ? sizeof(int) : sizeof(double)) * (size_t)n;
     if (bytes != need) return SPHDEM_E_ARG;
-    if (h->kind == 1)
-        return which ? SPHDEM_E_ARG
-                     : (h->prec == SPHDEM_PREC_FP64 ? w_get_field_t<double>(h, field, dst, n)
-                                                    : w_get_field_t<float>(h, field, dst, n));
+    if (h->kind == 1) {
+        if (which) return SPHDEM_E_ARG;
+        return h->prec == SPHDEM_PREC_FP64 ? w_get_field_t<double>(h, field, dst, n)
+                                           : w_get_field_t<float>(h, field, dst, n);
+    }
     return h->prec == SPHDEM_PREC_FP64 ? get_field_t<double>(h, which, field, dst, n)
                                        : get_field_t<float>(h, which, field, dst, n);
 }

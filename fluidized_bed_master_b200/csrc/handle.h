@@ -48,6 +48,11 @@ struct SphdemHandle {
     int ppe_iters = 0;
     double ppe_res = 0.0;
     double ppe_ms = 0.0;
+    // batch of independent 2-D beds in one handle (sphdem_create_batch):
+    // rows bed_start[b] .. bed_start[b+1]-1 of the input are bed b, placed
+    // at commit with its x, y shifted by bed_off[2b], bed_off[2b+1]
+    std::vector<int> bed_start;
+    std::vector<double> bed_off;
 };
 
 // io.cpp

@@ -50,7 +50,19 @@ struct WState {      // persistent, ping-pong, permuted by the cell gather
     double *x0, *y0, *rho0;      // predictor start positions and density (part2::x0, y0, rho0)
     R *ux0, *uy0;                // predictor start velocity
     int *ptype, *btype, *itype, *pid;
+    // batch of beds (sphdem_create_batch): the bed of each particle and the
+    // placement shift of every bed.  Cells are computed at x + shift, so the
+    // beds lie in separate cells of one grid; positions and every pair
+    // distance stay in the bed's own coordinates.  nullptr: one bed, no shift.
+    int* bed;
+    const double2* boff;
 };
+
+// shift of the cell computation of particle i (zero outside a batch)
+template <typename R>
+__device__ __forceinline__ double2 w_cell_off(const WState<R>& S, int i) {
+    return S.boff ? S.boff[S.bed[i]] : make_double2(0.0, 0.0);
+}
 
 template <typename R>
 struct WWork {
@@ -110,7 +122,8 @@ __global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W, i
     S.rho0[i] = rho;
     if (Q.rho_cont && pt > 0) S.rho[i] = rho + (double)W.drho[i] * hdt;
     int ic, jc, kc;
-    cell_ijk(P, xp, yp, S.z[i], ic, jc, kc);
+    const double2 o = w_cell_off(S, i);
+    cell_ijk(P, xp + o.x, yp + o.y, S.z[i], ic, jc, kc);
     key[i] = ic + P.NI * jc + P.NI * P.NJ * kc;
 }
 
@@ -151,9 +164,10 @@ __global__ void __launch_bounds__(128) k_w_list(DevParams P, WState<R> S, const 
     double xi = S.x[i], yi = S.y[i];
     double Rr = __dmul_rn(P.kappa, S.h[i]);
     int ic, jc, kc;
-    cell_ijk(P, xi, yi, 0.0, ic, jc, kc);
+    const double2 o = w_cell_off(S, i);
+    cell_ijk(P, xi + o.x, yi + o.y, 0.0, ic, jc, kc);
     int c = 0, cap = P.nb_cap, n = P.ns;
-    const Cull cu = make_cull(xi, yi, 0.0, Rr);
+    const Cull cu = make_cull(xi + o.x, yi + o.y, 0.0, Rr);
     const unsigned low = (1u << g.lane) - 1u;
     for_rows(P, ic, jc, kc, rows, cu, [&](int a, int b) {
         for (int j0 = a; j0 < b; j0 += L) {
@@ -498,6 +512,24 @@ __global__ void k_w_gather(DevParams P, WState<R> src, WState<R> dst, const int*
     dst.x0[i] = src.x0[p]; dst.y0[i] = src.y0[p];
     dst.ux0[i] = src.ux0[p]; dst.uy0[i] = src.uy0[p]; dst.rho0[i] = src.rho0[p];
     dst.ptype[i] = src.ptype[p]; dst.btype[i] = src.btype[p]; dst.itype[i] = src.itype[p]; dst.pid[i] = src.pid[p];
+    if (src.bed) dst.bed[i] = src.bed[p];
+}
+
+// cell key of the state as it stands (the first NNPS at commit; in a step
+// the predictor writes the keys): KERNEL_index_particle_to_cell
+template <typename R>
+__global__ void k_w_hash(DevParams P, WState<R> S, int* key, int* val) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.ns) return;
+    val[i] = i;
+    if (S.itype[i] == 3) {
+        key[i] = P.num_cells;
+        return;
+    }
+    int ic, jc, kc;
+    const double2 o = w_cell_off(S, i);
+    cell_ijk(P, S.x[i] + o.x, S.y[i] + o.y, S.z[i], ic, jc, kc);
+    key[i] = ic + P.NI * jc + P.NI * P.NJ * kc;
 }
 
 }  // namespace sphdem

@@ -38,6 +38,8 @@ def lib():
     L.sphdem_read_solv.argtypes = [C.c_char_p, P(SphdemParams)]
     L.sphdem_create.argtypes = [P(SphdemParams), C.c_int32, C.c_int32, P(vp)]
     L.sphdem_create_from_dir.argtypes = [C.c_char_p, P(SphdemParams), P(vp)]
+    L.sphdem_create_batch.argtypes = [P(SphdemParams), C.c_int32, P(C.c_int32), P(vp)]
+    L.sphdem_batch_offsets.argtypes = [vp, P(C.c_double)]
     L.sphdem_set_field.argtypes = [vp, C.c_int, C.c_int, vp, C.c_size_t]
     L.sphdem_commit_particles.argtypes = [vp]
     L.sphdem_step.argtypes = [vp, C.c_int32]
@@ -111,6 +113,39 @@ class Engine:
         except Exception:
             self.close()
             raise
+
+    @classmethod
+    def batch(cls, params, beds):
+        """Several independent 2-D WCSPH beds in one handle
+        (sphdem_create_batch): beds is a list of SPH dicts, each in its own
+        coordinates.  Rows are the beds concatenated in order; bed_of(pid)
+        maps a slot's input row back to its bed."""
+        self = cls.__new__(cls)
+        L = lib()
+        counts = [len(b["x"]) for b in beds]
+        arr = (C.c_int32 * len(counts))(*counts)
+        self._h = C.c_void_p()
+        _chk(L.sphdem_create_batch(C.byref(params), len(counts), arr, C.byref(self._h)), "sphdem_create_batch")
+        self.params = params.copy()
+        self.ns, self.nd = sum(counts), 0
+        self.bed_start = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        try:
+            for name in beds[0]:
+                self._set(SPH, name, np.concatenate([np.asarray(b[name]) for b in beds]))
+            _chk(L.sphdem_commit_particles(self._h), "sphdem_commit_particles")
+        except Exception:
+            self.close()
+            raise
+        return self
+
+    def bed_of(self, pid):
+        """Bed index of each input row (batch handles)."""
+        return np.searchsorted(self.bed_start, np.asarray(pid), side="right") - 1
+
+    def batch_offsets(self):
+        off = np.zeros(2 * (len(self.bed_start) - 1))
+        _chk(lib().sphdem_batch_offsets(self._h, off.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_batch_offsets")
+        return off.reshape(-1, 2)
 
     @classmethod
     def from_dir(cls, path, precision=0):

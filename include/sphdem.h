@@ -268,6 +268,23 @@ int sphdem_input_counts(const char* input_txt, int32_t* n_sph, int32_t* n_dem);
 int sphdem_input_column(const char* input_txt, int which, int field,
                         void* host_dst, size_t bytes);
 
+/* Batch of independent 2-D WCSPH beds in one handle (engine extension;
+ * the reference runs one bed per process and time loop, WCSPH_Calc.cuh:
+ * 767-1143).  Rows bed_start..bed_start+n_per_bed[b]-1 of the SPH input
+ * are bed b, beds in order; sphdem_set_field before commit takes the
+ * concatenated beds, each in its own coordinates, which the engine keeps.
+ * At commit each bed gets a placement shift for the cell computation only:
+ * shifted, the beds sit side by side on shelves of one cell grid with gaps
+ * wider than the search stencil, so no neighbour pair crosses beds, and
+ * every sphdem_step advances all beds in one graph launch.  SPHDEM_F_PID
+ * (the input row) tells the bed of a slot.  All beds share SphdemParams
+ * (dt, kernel, EOS, forces).  solver_type WCSPH, dim 2 only. */
+int sphdem_create_batch(const SphdemParams* p, int32_t nbeds, const int32_t* n_per_bed,
+                        SphdemHandle** out);
+/* The placement shift of every bed's cell computation after commit:
+ * offsets[2b], offsets[2b+1] (x, y) for bed b (2 nbeds doubles). */
+int sphdem_batch_offsets(SphdemHandle* h, double* offsets);
+
 /* Create an engine for n_sph SPH and n_dem DEM particles on the current
  * CUDA device.  Particle data is then uploaded with sphdem_set_field and
  * sphdem_commit_particles. */
