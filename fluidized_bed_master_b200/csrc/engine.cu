@@ -328,7 +328,6 @@ static int project_initial(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, i
     KryWork<R>& K = EH->K;
     int n = EH->E.P.ns;
     cudaStream_t st = H->stream;
-    k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, EH->E.sw.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
     k_proj_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, S.pid, std::min(std::max(H->p.warm_hist, 0),
                                                                           SPHDEM_WARM_HIST_MAX), use_mlp);
     int fit = H->p.warm_fit | (cg ? 0 : SPHDEM_FIT_RESIDUAL);   // BiCGStab: the residual norm
@@ -380,7 +379,8 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
         if (r) return r;
     }
     KTimer kt_solve(H, KT_PPE_SOLVE);
-    k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
+    // y = A x0 (the projection already formed it from its kept products)
+    if (!K.D) k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, W.nbr, K.x, K.y, K.x, KP_SS, nullptr, 0, 0);
     if (cg) {
         k_cg_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.z, K.p, K.s, K.sc, H->p.ppe_tol,
                                            H->p.ppe_max_iter);
@@ -792,6 +792,7 @@ static int commit_t(SphdemHandle* H) {
                 K.hring = A.get<int>(2);
                 K.ppart = A.get<double>((size_t)PROJ_NV * KRY_G);
                 K.pc = A.get<double>(PROJ_MAX + 2);
+                K.AD = A.get<double>((size_t)PROJ_MAX * ns);
                 if (!A.ok) return SPHDEM_E_NOMEM;
             }
             if (p.warm_start == SPHDEM_WARM_MLP) {

@@ -109,6 +109,7 @@ struct KryWork {
     int* hring;            // {next slot, changes stored}
     double* ppart;         // PROJ_NV * KRY_G block partials
     double* pc;            // PROJ_MAX coefficients, directions kept, c.h
+    double* AD;            // [PROJ_MAX][n] products A d_q of the last fit
 };
 
 // learned warm start statistics slots
@@ -718,18 +719,20 @@ __global__ void k_mlp_tick(double* mstat) { mstat[MS_T] += 1.0; }
 
 // ---- projected initial iterate (warm starts PROJECT and MLP) ---------------
 // x0 = sum_q c_q d_q over the directions
-//     d0 = the previous pressure, d1 = D^-1 (b - A d0) (the one-sweep
-//     increment), d2 = the network's predicted change (MLP in use, else 0),
-//     d3.. = the last warm_hist solution changes, newest first,
+//     d0 = the previous pressure (FP64), d1 = the network's predicted
+//     change (MLP in use, else 0), d2.. = the last warm_hist solution
+//     changes, newest first (FP32),
 // with c from the Galerkin equations (D^T M A D) c = D^T M b (the optimal
 // combination in the norm of the symmetric operator M A, never worse than
 // d0 alone in that norm), or (warm_fit RESIDUAL) from the least-squares equations
 // (AD)^T (AD) c = (AD)^T b.  With warm_fit AFFINE, c0 = 1 and the other
 // directions are fitted to r0 = b - A d0.  Directions
 // are FP32 rows of PROJ_MP floats (one 48-B gather per list entry for all
-// of them); their products with A and the dots are FP64.  Directions that
-// are zero or dependent are dropped from the system.
-constexpr int PROJ_MAX = 3 + SPHDEM_WARM_HIST_MAX;   // 11
+// of them) except d0, gathered as FP64; their products with A and the dots
+// are FP64.  The products are kept, so A x0 = sum_q c_q (A d_q) comes with
+// x0 and the solver needs no product of its own before its first step.
+// Directions that are zero or dependent are dropped from the system.
+constexpr int PROJ_MAX = 2 + SPHDEM_WARM_HIST_MAX;   // 10
 constexpr int PROJ_MP = 12;                          // floats per direction row
 constexpr int PROJ_NG = PROJ_MAX * (PROJ_MAX + 1) / 2;
 constexpr int PROJ_NV = PROJ_NG + PROJ_MAX;          // upper triangle of G, then h
@@ -743,13 +746,12 @@ __global__ void k_proj_dirs(int n, KryWork<R> K, const int* __restrict__ pid, in
 #pragma unroll
     for (int q = 0; q < PROJ_MP; q++) d[q] = 0.f;
     if (on) {
-        d[0] = (float)K.x[i];
-        d[1] = (float)((K.b[i] - K.y[i]) / K.d[i]);
-        if (use_mlp) d[2] = (float)(K.mstat[MS_PS] * (double)K.yp[i]);
+        // d[0] stays 0: the previous pressure enters the products as FP64
+        if (use_mlp) d[1] = (float)(K.mstat[MS_PS] * (double)K.yp[i]);
         const int slot = K.hring[0], have = min(K.hring[1], nhist), p = pid[i];
         for (int k = 0; k < have; k++) {
             int s = (slot - 1 - k + SPHDEM_WARM_HIST_MAX) % SPHDEM_WARM_HIST_MAX;
-            d[3 + k] = K.hist[(size_t)s * K.hist_n + p];
+            d[2 + k] = K.hist[(size_t)s * K.hist_n + p];
         }
     }
     float4* o = reinterpret_cast<float4*>(K.D + (size_t)i * PROJ_MP);
@@ -789,9 +791,10 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
             const double dg = K.d[i];
 #pragma unroll
             for (int q = 0; q < PROJ_MAX; q++) {
-                dv[q] = (double)di[q];
+                dv[q] = q == 0 ? K.x[i] : (double)di[q];
                 ad[q] = dg * dv[q];
             }
+            const double* __restrict__ xp = K.x;   // d0 = the previous pressure, FP64
             // entries in pairs: both entries' direction gathers are in
             // flight before their updates
             const typename E::T* __restrict__ er = ent + kent_at(i, 0, K.cap);
@@ -806,12 +809,15 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
                        p2 = __ldg(D4 + (size_t)j0 * 3 + 2);
                 float4 q0 = __ldg(D4 + (size_t)j1 * 3), q1 = __ldg(D4 + (size_t)j1 * 3 + 1),
                        q2 = __ldg(D4 + (size_t)j1 * 3 + 2);
+                const double x0j = __ldg(xp + j0), x1j = __ldg(xp + j1);
                 float d0[PROJ_MP] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w, p2.x, p2.y, p2.z, p2.w};
                 float d1[PROJ_MP] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+                ad[0] -= a0 * x0j;
 #pragma unroll
-                for (int q = 0; q < PROJ_MAX; q++) ad[q] -= a0 * (double)d0[q];
+                for (int q = 1; q < PROJ_MAX; q++) ad[q] -= a0 * (double)d0[q];
+                ad[0] -= a1 * x1j;
 #pragma unroll
-                for (int q = 0; q < PROJ_MAX; q++) ad[q] -= a1 * (double)d1[q];
+                for (int q = 1; q < PROJ_MAX; q++) ad[q] -= a1 * (double)d1[q];
             }
             for (; k < ne; k++) {
                 int j;
@@ -819,10 +825,18 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
                 E::get(__ldg(er + (size_t)k * 32), j, a);
                 float4 b0 = __ldg(D4 + (size_t)j * 3), b1 = __ldg(D4 + (size_t)j * 3 + 1), b2 = __ldg(D4 + (size_t)j * 3 + 2);
                 float dj[PROJ_MP] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+                ad[0] -= a * __ldg(xp + j);
 #pragma unroll
-                for (int q = 0; q < PROJ_MAX; q++) ad[q] -= a * (double)dj[q];
+                for (int q = 1; q < PROJ_MAX; q++) ad[q] -= a * (double)dj[q];
             }
-            bi = affine ? K.b[i] - K.y[i] : K.b[i];   // y = A p_prev
+        }
+        // the products, for A x0 in k_proj_apply (0 on rows that are not solved)
+        if (i < n) {
+#pragma unroll
+            for (int q = 0; q < PROJ_MAX; q++) K.AD[(size_t)q * n + i] = ad[q];
+        }
+        if (cnt) {
+            bi = affine ? K.b[i] - ad[0] : K.b[i];   // ad[0] = (A p_prev)_i
             if (affine) dv[0] = ad[0] = 0.0;          // p_prev is not fitted
             // Galerkin: the m-weighted products (M A is the symmetric operator)
             if (!least_squares) {
@@ -920,15 +934,25 @@ __global__ void __launch_bounds__(KRY_T) k_proj_solve(KryWork<R> K, int nblk) {
 }
 
 // x0 = c0 p_prev (FP64) + sum_{q>0} c_q d_q   (c0 = 1 for an affine fit)
+// and y = A x0 = c0 (A p_prev) + sum_{q>0} c_q (A d_q) from the kept products
 template <typename R>
 __global__ void k_proj_apply(int n, KryWork<R> K, int fit) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || K.kcnt[i] == 0) return;
+    if (i >= n) return;
+    if (K.kcnt[i] == 0) {
+        K.y[i] = 0.0;
+        return;
+    }
     const float* d = K.D + (size_t)i * PROJ_MP;
-    double x = ((fit & SPHDEM_FIT_AFFINE) ? 1.0 : K.pc[0]) * K.x[i];
+    const double c0 = (fit & SPHDEM_FIT_AFFINE) ? 1.0 : K.pc[0];
+    double x = c0 * K.x[i], y = c0 * K.AD[i];
 #pragma unroll
-    for (int q = 1; q < PROJ_MAX; q++) x += K.pc[q] * (double)d[q];
+    for (int q = 1; q < PROJ_MAX; q++) {
+        x += K.pc[q] * (double)d[q];
+        y += K.pc[q] * K.AD[(size_t)q * n + i];
+    }
     K.x[i] = x;
+    K.y[i] = y;
     if (K.x0) K.x0[i] = x;
 }
 

@@ -131,14 +131,14 @@ def test_warm_starts_converge_to_the_same_pressure(warm, fit):
     a = _engine(p, sph, dem, 0)
     b = _engine(q, sph, dem, 0)
     phases = set()
-    for _ in range(40):
+    for k in range(40):
         a.step(1)
         b.step(1)
         s = a.stats()
-        assert s["ppe_status"] == 0 and s["ppe_rel_residual"] <= 1e-6, s
+        assert s["ppe_status"] == 0 and s["ppe_rel_residual"] <= 1e-6, (k, s)
         phases.add(s["mlp_phase"])
-        if warm in (WARM_PROJECT, WARM_MLP):
-            assert s["ppe_warm_dirs"] >= 1
+        if warm in (WARM_PROJECT, WARM_MLP) and k >= 1:   # from the second step a solution change exists
+            assert s["ppe_warm_dirs"] >= 1, (k, s)
             if fit & FIT_AFFINE:   # an affine fit starts from p_prev plus a correction: never worse
                 assert s["ppe_warm_gain"] >= 0.0, s
     if warm == WARM_MLP:
