@@ -11,6 +11,7 @@
 #include <cstring>
 #include <set>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "handle.h"
@@ -462,7 +463,18 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
     if (ns > 0) {
-        { KTIME(KT_LIST); k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags); }
+        {
+            KTIME(KT_LIST);
+            if constexpr (std::is_same<R, float>::value) {
+                // one warp per cell; slots outside every cell (i_type 3) keep an empty list
+                CK(cudaMemsetAsync(W.ncnt, 0, sizeof(int) * ns, st));
+                int ncell = P.NI * P.NJ * P.NK;
+                k_build_list_tiled<<<(ncell + LT_WARPS - 1) / LT_WARPS, LT_WARPS * 32, 0, st>>>(
+                    P, S, W.rec, W.g_str, W.g_end, W.rows, W.nbr, W.ncnt, E.flags);
+            } else {
+                k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags);
+            }
+        }
         { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
         *nl += 2;
     }
