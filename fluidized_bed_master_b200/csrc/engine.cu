@@ -495,7 +495,11 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0); }
         if (flags & F_COUNT0) {
             KTIME(KT_NEUMANN0);
-            k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.rows, 1);
+            if constexpr (std::is_same<R, float>::value)
+                k_neumann_tiled<<<(P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st>>>(
+                    P, S, W, S.pres, W.g_str, W.g_end, W.rows, 1);
+            else
+                k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.rows, 1);
             *nl += 1;
         }
         {
@@ -503,7 +507,14 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W);
             else if ((r = enqueue_krylov<R>(H, EH, S, W))) return r;
         }
-        { KTIME(KT_NEUMANN); k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0); }
+        {
+            KTIME(KT_NEUMANN);
+            if constexpr (std::is_same<R, float>::value)
+                k_neumann_tiled<<<(P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st>>>(
+                    P, S, W, W.p_new, W.g_str, W.g_end, W.rows, 0);
+            else
+                k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0);
+        }
         { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
         *nl += 4;
     }

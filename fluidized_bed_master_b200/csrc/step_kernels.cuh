@@ -1199,6 +1199,182 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
     if (patch_up) *comp<R>(rec.up, i, 3) = pw;
 }
 
+// Cell-tiled Neumann pass (FP32 build): one warp per cell that holds wall
+// particles.  The fluid candidates of the cell's 9 stencil rows are staged
+// (compacted in order) in shared memory with the factors the sums need
+// ({x, y, z relative to a particle of the cell, slot} and {m/rho, p, T,
+// m/eps}); each lane -- one wall particle of the cell -- runs over them in
+// order with its own 2 kappa h radius, FP32 prefilter and the FP64
+// reference predicate inside the band.  Same sums as k_neumann in candidate
+// order per wall, so the FP32 results differ from it by rounding only.
+constexpr int NT_WARPS = 4, NT_CH = 128;
+__global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
+                                                                   float* pres, const int* __restrict__ gs,
+                                                                   const int* __restrict__ ge,
+                                                                   const int4* __restrict__ rows, int patch_up) {
+    __shared__ float4 sa[NT_WARPS][NT_CH + 32];
+    __shared__ float4 sb[NT_WARPS][NT_CH + 32];
+    __shared__ int srow[NT_WARPS][20];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * NT_WARPS + w;
+    if (c >= P.NI * P.NJ * P.NK) return;
+    const int a0 = __ldg(gs + c);
+    if (a0 < 0) return;
+    const int e0 = __ldg(ge + c);
+    const SphRec<float> rec = W.rec;
+    bool any_wall = false;
+    for (int i = a0 + lane; i < e0; i += 32) any_wall |= S.ptype[i] <= 0;
+    if (!__any_sync(0xffffffffu, any_wall)) return;
+    const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
+    int len = 0, lo = 0;
+    if (lane < 9) {
+        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
+        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
+            int4 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
+            lo = r.x;
+            len = max(r.w - r.x, 0);
+        }
+    }
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < 9) {
+        srow[w][lane + 1] = inc;
+        srow[w][10 + lane] = lo;
+    }
+    if (lane == 0) srow[w][0] = 0;
+    const int tot = __shfl_sync(0xffffffffu, inc, 8);
+    __syncwarp();
+    const int4 q0 = ldr(rec.pos + a0);
+    const bool o_oor = (q0.w & TAG_OOR) != 0;
+    const float sx = P.q_step[0], sy = P.q_step[1], sz = P.q_step[2];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int p0 = a0; p0 < e0; p0 += 32) {
+        const int i = p0 + lane;
+        const bool act = i < e0 && S.ptype[i] <= 0;
+        if (!__any_sync(0xffffffffu, act)) continue;
+        double xi = 0, yi = 0, zi = 0, R2 = 0;
+        float lo2 = 0, hi2 = 0, fx = 0, fy = 0, fz = 0;
+        Knl<float> K{};
+        bool slow = false;
+        if (act) {
+            xi = S.x[i];
+            yi = S.y[i];
+            zi = S.z[i];
+            const double hi = S.h[i];
+            const float th2 = 2.f * (float)hi;
+            K = knl_make<float>(P, (float)hi);
+            K.ih = rcp(th2);
+            K.th = th2;
+            R2 = 2.0 * (P.kappa * hi);
+            const double b = 4e-6 + P.q_abs / R2, r2 = R2 * R2;
+            lo2 = (float)(r2 * (1.0 - b));
+            hi2 = (float)(r2 * (1.0 + b));
+            const int4 qi = ldr(rec.pos + i);
+            slow = o_oor || (qi.w & TAG_OOR);
+            fx = (float)(qi.x - q0.x) * sx;
+            fy = (float)(qi.y - q0.y) * sy;
+            fz = (float)(qi.z - q0.z) * sz;
+        }
+        const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
+        float tp = 0.f, flt = 0.f, tt = 0.f, tr = 0.f;
+        int t = 0;   // next raw candidate
+        while (t < tot) {
+            // stage fluid candidates in order until the chunk is full
+            int ns = 0;
+            bool any_oor = false;
+            while (t < tot && ns <= NT_CH - 32) {
+                const int tl = t + lane;
+                bool keep = false;
+                int4 qj = make_int4(0, 0, 0, 0);
+                int j = 0;
+                if (tl < tot) {
+                    int r = 0;
+                    while (tl >= srow[w][r + 1]) r++;
+                    j = srow[w][10 + r] + (tl - srow[w][r]);
+                    qj = ldr(rec.pos + j);
+                    const int ptj = tag_ptype(qj.w);
+                    keep = ptj >= 1 && ptj < 1000;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = ns + __popc(m & lt);
+                    const bool oor = (qj.w & TAG_OOR) != 0;
+                    any_oor |= oor;
+                    const float4 fj = ldr(rec.f1 + j);
+                    const float mr = fj.x * rcp(fj.y);
+                    sa[w][pos] = make_float4((float)(qj.x - q0.x) * sx, (float)(qj.y - q0.y) * sy,
+                                             (float)(qj.z - q0.z) * sz, __int_as_float(j | (oor ? (int)0x80000000 : 0)));
+                    sb[w][pos] = make_float4(mr, pres[j], fj.z, fj.x * rcp(fj.w));
+                }
+                ns += __popc(m);
+                t += 32;
+            }
+            const bool slow_chunk = lanes_slow || __any_sync(0xffffffffu, any_oor);
+            __syncwarp();
+            if (act) {
+                for (int u = 0; u < ns; u++) {
+                    const float4 cj = sa[w][u];
+                    const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    bool in;
+                    if (!slow_chunk) {
+                        if (r2 > hi2) continue;
+                        in = r2 < lo2;
+                        if (!in) {
+                            const int j = __float_as_int(cj.w);
+                            in = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < R2;
+                        }
+                    } else {
+                        const int jb = __float_as_int(cj.w), j = jb & 0x7fffffff;
+                        if (!slow && jb >= 0) {
+                            if (r2 > hi2) continue;
+                            in = r2 < lo2 ||
+                                 __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < R2;
+                        } else {
+                            in = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < R2;
+                        }
+                    }
+                    if (!in) continue;
+                    float r, rinv;
+                    if (!slow_chunk || (!slow && __float_as_int(cj.w) >= 0)) {
+                        rdist(r2, r, rinv);
+                    } else {
+                        const int j = __float_as_int(cj.w) & 0x7fffffff;
+                        const float ex = (float)(xi - S.x[j]), ey = (float)(yi - S.y[j]), ez = (float)(zi - S.z[j]);
+                        rdist(ex * ex + ey * ey + ez * ez, r, rinv);
+                    }
+                    const float wk = kw(K, r);
+                    const float4 bj = sb[w][u];
+                    const float mr = bj.x * wk;
+                    tp += mr * bj.y;
+                    flt += mr;
+                    tt += mr * bj.z;
+                    tr += bj.w * wk;
+                }
+            }
+            __syncwarp();
+        }
+        if (!act) continue;
+        float pw, rw;
+        if (flt < 1e-6f) {
+            rw = W.rho_ref[i];
+            pw = 0.f;
+        } else {
+            pw = tp / flt;
+            S.temp[i] = tt / flt;
+            rw = rec.f1[i].w * tr / flt;
+        }
+        pres[i] = pw;
+        W.rho_new[i] = rw;
+        *comp<float>(rec.f1, i, 1) = rw;
+        if (patch_up) *comp<float>(rec.up, i, 3) = pw;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // KERNEL_PPE3D_sph + KERNEL_PPE3D_calc_sph (functions_PPE2.cuh:542-698,
 // 868-878): one Jacobi sweep; p_new = (b + sum A_ij p_j) / sum A_ij for
