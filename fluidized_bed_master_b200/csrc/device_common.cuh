@@ -21,6 +21,7 @@ struct DevParams {
     int kernel_type, dim, kgc, delsph, fp, fv, fva, fg, con, xsph, open_bc, rho_type;
     int NI, NJ, NK, num_cells;
     int ns, nd, nb_cap;
+    int nbd_cap;              // SPH -> DEM list entries per particle
     int nwall, nbuf;
     int filt_period;          // freq_filt * decouple_stride
     int wall_mask;

@@ -33,7 +33,7 @@ static const int TPB = 128;
 enum {
     KT_HASH_S, KT_SORT_S, KT_GATHER_S, KT_HASH_D, KT_SORT_D, KT_GATHER_D, KT_LIST, KT_PASSA, KT_DEMPREP, KT_PASSB,
     KT_DEMCONTACT, KT_DEMCOUPLING, KT_SPHCOUPLING, KT_NEUMANN0, KT_PPE, KT_NEUMANN, KT_PASSC, KT_DEMUPDATE,
-    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN,
+    KT_OPENBC, KT_XSPH, KT_ROWS_S, KT_ROWS_D, KT_PPE_ASM, KT_PPE_WARM, KT_PPE_SOLVE, KT_PPE_TRAIN, KT_DLIST,
     // 2-D WCSPH step
     KT_W_PRED, KT_W_NNPS, KT_W_LIST, KT_W_KGC, KT_W_PREP, KT_W_CONT, KT_W_INTER, KT_W_CORR, KT_W_XSPH,
     KT_W_FINISH, KT_COUNT
@@ -42,7 +42,7 @@ static const char* KT_NAMES[KT_COUNT] = {
     "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
     "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem",
-    "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training",
+    "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training", "build_dem_list",
     "w.predictor", "w.nnps", "w.list", "w.kgc", "w.prep", "w.continuity", "w.interaction", "w.corrector",
     "w.xsph", "w.finish"};
 
@@ -147,6 +147,8 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     W.g_str = A.get<int>(ncells + 1); W.g_end = A.get<int>(ncells + 1);
     W.rows = A.get<int4>(ncells);
     W.ncnt = A.get<int>(ns);
+    W.ncntd = A.get<int>(ns);
+    W.nbrd = nullptr;
     W.wall_idx = A.get<int>(ns); W.buf_idx = A.get<int>(ns); W.counters = A.get<int>(4);
     W.nbr = nullptr;
     W.rec.pos = A.get<PosRec<R>>(ns);
@@ -440,6 +442,17 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
     return SPHDEM_OK;
 }
 
+// SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
+template <typename R>
+void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<R>& D, cudaStream_t st) {
+    Engine<R>& E = EH->E;
+    const DevParams& P = E.P;
+    const int ncell = P.NI * P.NJ * P.NK;
+    k_build_dlist<<<(ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st>>>(
+        P, S.x, S.y, S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
+        P.nbd_cap, E.flags);
+}
+
 // ---------------------------------------------------------------------------
 // one step (SOPHIA_single_ISPH order).  flags: bit1 count==0, bit2 filter
 // step, bit3 time==0.
@@ -474,6 +487,11 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             } else {
                 k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags);
             }
+        }
+        if (nd > 0) {
+            KTIME(KT_DLIST);
+            launch_dlist<R>(EH, S, D, st);
+            *nl += 1;
         }
         { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
         *nl += 2;
@@ -796,6 +814,21 @@ static int commit_t(SphdemHandle* H) {
         EH->nb_cap = cap;
         W.nbr = A.get<int>((size_t)cap * ns);
         if (!A.ok) return SPHDEM_E_NOMEM;
+        // SPH -> DEM list capacity from an exact count on the sorted input; a
+        // particle above it later walks its stencil instead
+        P.nbd_cap = 0;
+        if (nd > 0) {
+            if ((r = nnps_dem<R>(H, EH, 0, 1, &nl))) return r;
+            CK(cudaMemsetAsync(W.ncntd, 0, sizeof(int) * ns, st));
+            launch_dlist<R>(EH, E.S[1], E.D[1], st);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(&f, E.flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            int capd = p.dem_list_cap > 0 ? p.dem_list_cap : std::max(8, ((int)(f.max_ncntd * 1.25) + 8 + 7) / 8 * 8);
+            P.nbd_cap = capd;
+            W.nbrd = A.get<int>((size_t)capd * ns);
+            if (!A.ok) return SPHDEM_E_NOMEM;
+        }
         if (p.ppe_mode != SPHDEM_PPE_REFERENCE) {
             KryWork<R>& K = EH->K;
             K.e = A.get<typename KEnt<R>::T>((size_t)cap * ((ns + 31) / 32 * 32));
@@ -1559,6 +1592,7 @@ static int check_supported(const SphdemParams* p) {
     if (p->warm_start == SPHDEM_WARM_PROJECT && p->ppe_mode == SPHDEM_PPE_REFERENCE) return SPHDEM_E_UNSUPPORTED;
     if (p->warm_hist < 0 || p->warm_hist > SPHDEM_WARM_HIST_MAX) return SPHDEM_E_ARG;
     if (p->warm_fit & ~(SPHDEM_FIT_RESIDUAL | SPHDEM_FIT_AFFINE)) return SPHDEM_E_ARG;
+    if (p->dem_list_cap < 0 || p->dem_list_cap > 4096) return SPHDEM_E_ARG;
     if (p->warm_start != SPHDEM_WARM_PREVIOUS && p->warm_start != SPHDEM_WARM_MLP &&
         p->warm_start != SPHDEM_WARM_EXTRAPOLATE && p->warm_start != SPHDEM_WARM_PROJECT)
         return SPHDEM_E_ARG;
@@ -1606,6 +1640,7 @@ extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, S
         p.warm_hist = ov->warm_hist;
         p.warm_fit = ov->warm_fit;
         p.w_lanes = ov->w_lanes;
+        p.dem_list_cap = ov->dem_list_cap;
         p.mlp_train_steps = ov->mlp_train_steps;
         p.mlp_updates = ov->mlp_updates;
         p.mlp_seed = ov->mlp_seed;

@@ -60,6 +60,7 @@ struct SphWork {
     int *g_str, *g_end;
     int4* rows;                  // per-cell stencil rows (for_rows)
     int *nbr, *ncnt;
+    int *nbrd, *ncntd;           // SPH -> DEM list (k_build_dlist): nbrd[k*n+i], exact count
     int *wall_idx, *buf_idx, *counters;   // per-step compacted wall / buffer slots
     SphRec<R> rec;
 };
@@ -83,6 +84,7 @@ struct DevFlags {
     int nan;
     int max_ncnt;
     int step_count; // the reference's count (vii[43]), advanced by k_tick at the end of a step
+    int max_ncntd;  // largest SPH -> DEM list count seen
 };
 
 template <typename R>

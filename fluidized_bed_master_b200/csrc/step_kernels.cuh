@@ -202,6 +202,41 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
     atomicMax(&F->max_ncnt, c);
 }
 
+// The 9 full stencil rows (z, y order) of cell (ic, jc, kc) for a whole
+// warp: s[0..9] the prefix of the row lengths, s[10..18] the first slot of
+// each row.  Returns the number of candidates; row_slot maps candidate t
+// (0 <= t < that number) to its slot, in the reference's visit order.
+__device__ __forceinline__ int stage_rows(const DevParams& P, int ic, int jc, int kc, const int4* __restrict__ rows,
+                                          int* s, int lane) {
+    int len = 0, lo = 0;
+    if (lane < 9) {
+        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
+        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
+            int4 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
+            lo = r.x;
+            len = max(r.w - r.x, 0);
+        }
+    }
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < 9) {
+        s[lane + 1] = inc;
+        s[10 + lane] = lo;
+    }
+    if (lane == 0) s[0] = 0;
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, inc, 8);
+}
+__device__ __forceinline__ int row_slot(const int* s, int t) {
+    int r = 0;
+    while (t >= s[r + 1]) r++;
+    return s[10 + r] + (t - s[r]);
+}
+
 // Cell-tiled list build (FP32 build).  One warp per cell: the particles of
 // a cell share one stencil, so the warp stages the candidates of the 9 rows
 // once, as FP32 coordinates relative to a particle of the cell, into shared
@@ -234,29 +269,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
     if (a0 < 0) return;
     const int e0 = __ldg(ge + c);
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
-    // the 9 full rows (z, y order) and their prefix
-    int len = 0, lo = 0;
-    if (lane < 9) {
-        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
-        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
-            int4 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
-            lo = r.x;
-            len = max(r.w - r.x, 0);
-        }
-    }
-    int inc = len;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += v;
-    }
-    if (lane < 9) {
-        srow[w][lane + 1] = inc;
-        srow[w][10 + lane] = lo;
-    }
-    if (lane == 0) srow[w][0] = 0;
-    const int tot = __shfl_sync(0xffffffffu, inc, 8);
-    __syncwarp();
+    const int tot = stage_rows(P, ic, jc, kc, rows, srow[w], lane);
     const int4 q0 = ldr(rec.pos + a0);   // origin of the relative coordinates
     const bool o_oor = (q0.w & TAG_OOR) != 0;
     const int n = P.ns, cap = P.nb_cap;
@@ -293,9 +306,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                 float4 v = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(0));
                 if (u < tn) {
                     const int t = t0 + u;
-                    int r = 0;
-                    while (t >= srow[w][r + 1]) r++;
-                    const int j = srow[w][10 + r] + (t - srow[w][r]);
+                    const int j = row_slot(srow[w], t);
                     const int4 qj = ldr(rec.pos + j);
                     const bool oor = (qj.w & TAG_OOR) != 0;
                     any_oor |= oor;
@@ -360,6 +371,131 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
             ncnt[i] = cnt;
             if (cnt > cap) atomicOr(&F->overflow, 1);
             atomicMax(&F->max_ncnt, cnt);
+        }
+    }
+}
+
+// SPH -> DEM candidate list.  The SPH kernels that sum over DEM spheres
+// (pass A's porosity, the reaction force of k_sph_coupling) visit the DEM
+// slots of the 27-cell stencil in the reference's order and keep those
+// with |x_i - x_j| < kappa h_i.  About one stencil candidate in ten is
+// inside, so this pass finds them once per step and the two kernels walk
+// the short list (same slots, same order) and repeat their own test on it.
+// The list holds every j with pair_dist < kappa h_i, the add = 0 form of
+// the predicate; the 1e-20 form of pass A keeps a subset of it.
+//
+// One warp per cell, as k_build_list_tiled: the cell's DEM candidates
+// (p_type > 1000) are staged compacted in shared memory as FP32 coordinates
+// relative to the cell's first SPH particle, and each lane -- one SPH
+// particle of the cell -- tests them in order.  A coordinate within
+// Lb = 4 cells of the origin is rounded by at most e = 2^-24 Lb, a
+// difference by 4 e, so r^2 moves by at most 2 sqrt(3) Rr (4 e) + 3 (4 e)^2
+// near the radius, plus a few FP32 roundings; the band below is wider and
+// pairs inside it take the FP64 predicate.  A particle or sphere farther
+// than Lb from the origin (one clamped into a boundary cell) always takes
+// the FP64 predicate.  ncntd holds the exact count; a particle with more
+// than cap hits keeps only its count, and the consumers walk its stencil
+// instead.
+constexpr int DL_WARPS = 4, DL_CH = 128;
+__global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, const double* __restrict__ sx,
+                                                                 const double* __restrict__ sy,
+                                                                 const double* __restrict__ sz,
+                                                                 const double* __restrict__ sh,
+                                                                 const int* __restrict__ gs, const int* __restrict__ ge,
+                                                                 const int4* __restrict__ drows,
+                                                                 const double* __restrict__ dx,
+                                                                 const double* __restrict__ dy,
+                                                                 const double* __restrict__ dz,
+                                                                 const int* __restrict__ dptype, int* __restrict__ nbrd,
+                                                                 int* __restrict__ ncntd, int cap, DevFlags* F) {
+    __shared__ float4 sc[DL_WARPS][DL_CH + 32];
+    __shared__ int srow[DL_WARPS][20];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * DL_WARPS + w;
+    if (c >= P.NI * P.NJ * P.NK) return;
+    const int a0 = __ldg(gs + c);
+    if (a0 < 0) return;
+    const int e0 = __ldg(ge + c);
+    const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
+    const int tot = stage_rows(P, ic, jc, kc, drows, srow[w], lane);
+    const int n = P.ns;
+    const double x0 = sx[a0], y0 = sy[a0], z0 = sz[a0];
+    const double Lb = 4.0 * fmax(fmax((P.xmax - P.xmin) / P.NI, (P.ymax - P.ymin) / P.NJ), (P.zmax - P.zmin) / P.NK);
+    const double e4 = 4.0 * 5.9604644775390625e-08 * Lb;   // 4 x 2^-24 x Lb
+    const unsigned lt = (1u << lane) - 1u;
+    for (int p0 = a0; p0 < e0; p0 += 32) {
+        const int i = p0 + lane;
+        const bool act = i < e0;
+        double xi = 0, yi = 0, zi = 0, Rr = 0;
+        float lo2 = 0, hi2 = 0, fx = 0, fy = 0, fz = 0;
+        bool slow = false;
+        if (act) {
+            xi = sx[i];
+            yi = sy[i];
+            zi = sz[i];
+            Rr = P.kappa * sh[i];
+            const double r2 = Rr * Rr, d = 3.5 * Rr * e4 + 3.0 * e4 * e4 + 2e-6 * r2;
+            lo2 = (float)(r2 - d);
+            hi2 = (float)(r2 + d);
+            const double ux = xi - x0, uy = yi - y0, uz = zi - z0;
+            slow = !(fabs(ux) <= Lb && fabs(uy) <= Lb && fabs(uz) <= Lb);
+            fx = (float)ux;
+            fy = (float)uy;
+            fz = (float)uz;
+        }
+        const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
+        int cnt = 0;
+        int* pw = nbrd ? nbrd + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
+        int t = 0;
+        while (t < tot) {
+            int ns = 0;
+            bool any_far = false;
+            while (t < tot && ns <= DL_CH - 32) {
+                const int tl = t + lane;
+                int j = 0;
+                bool keep = false;
+                if (tl < tot) {
+                    j = row_slot(srow[w], tl);
+                    keep = __ldg(dptype + j) > 1000;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const double ux = dx[j] - x0, uy = dy[j] - y0, uz = dz[j] - z0;
+                    const bool far = !(fabs(ux) <= Lb && fabs(uy) <= Lb && fabs(uz) <= Lb);
+                    any_far |= far;
+                    sc[w][ns + __popc(m & lt)] =
+                        make_float4((float)ux, (float)uy, (float)uz, __int_as_float(j | (far ? (int)0x80000000 : 0)));
+                }
+                ns += __popc(m);
+                t += 32;
+            }
+            const bool slow_chunk = lanes_slow || __any_sync(0xffffffffu, any_far);
+            __syncwarp();
+            if (act) {
+                for (int u = 0; u < ns; u++) {
+                    const float4 cj = sc[w][u];
+                    const int jb = __float_as_int(cj.w), j = jb & 0x7fffffff;
+                    bool hit;
+                    if (!slow_chunk || (!slow && jb >= 0)) {
+                        const float ex = fx - cj.x, ey = fy - cj.y, ez = fz - cj.z;
+                        const float r2 = ex * ex + ey * ey + ez * ez;
+                        if (r2 > hi2) continue;
+                        hit = r2 < lo2 || pair_dist(xi, yi, zi, dx[j], dy[j], dz[j]) < Rr;
+                    } else {
+                        hit = pair_dist(xi, yi, zi, dx[j], dy[j], dz[j]) < Rr;
+                    }
+                    if (hit) {
+                        if (pw && cnt < cap) *pw = j;
+                        pw += n;
+                        cnt++;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (act) {
+            ncntd[i] = cnt;
+            atomicMax(&F->max_ncntd, cnt);
         }
     }
 }
@@ -446,15 +582,13 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
 #pragma unroll
         for (int q = 0; q < 9; q++) W.Cm[(size_t)q * n + i] = C[q];
     }
-    // SPH-DEM porosity (DEM arrays are small and L2-resident: plain loads)
-    int ic, jc, kc;
-    cell_ijk(P, xi, yi, zi, ic, jc, kc);
+    // SPH-DEM porosity over the SPH -> DEM list (DEM arrays are small and
+    // L2-resident: plain loads)
     double Rr = P.kappa * hi;
     R por = 0, dfx = 0, dfy = 0, dfz = 0;
     if (P.nd > 0) {
         float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
-        const Cull cu = make_cull(xi, yi, zi, Rr);
-        for_stencil_j(P, ic, jc, kc, drows, cu, [&](int j) {
+        auto dem = [&](int j) {
             if (D.ptype[j] <= 1000) return;
             PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
             if (!g.in) return;
@@ -467,7 +601,15 @@ __global__ void __launch_bounds__(128) k_passA(DevParams P, SphState<R> S, SphWo
             dfx += dw * g.dx * ir * (R)D.ux[j] * v;
             dfy += dw * g.dy * ir * (R)D.uy[j] * v;
             dfz += dw * g.dz * ir * (R)D.uz[j] * v;
-        });
+        };
+        const int cd = W.ncntd[i];
+        if (cd <= P.nbd_cap) {
+            for (int k = 0; k < cd; k++) dem(W.nbrd[(size_t)k * n + i]);
+        } else {
+            int ic, jc, kc;
+            cell_ijk(P, xi, yi, zi, ic, jc, kc);
+            for_stencil_j(P, ic, jc, kc, drows, make_cull(xi, yi, zi, Rr), dem);
+        }
     }
     R isf = rcp(sflt + (R)1e-20);
     R pori = (R)1 - por * isf;
@@ -1084,11 +1226,8 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
         double Rr = P.kappa * hi;
         R tx = 0, ty = 0, tz = 0, tt = 0;
         if (P.nd > 0 && (pt == 1 || pt == 3)) {
-            int ic, jc, kc;
-            cell_ijk(P, xi, yi, zi, ic, jc, kc);
             float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
-            const Cull cu = make_cull(xi, yi, zi, Rr);
-            for_stencil_j(P, ic, jc, kc, drows, cu, [&](int j) {
+            auto dem = [&](int j) {
                 if (D.ptype[j] <= 1000) return;
                 PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 0.0, r2l, r2h);
                 if (!g.in) return;
@@ -1101,7 +1240,15 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
                 ty += -mr * D.Fdy_df[j] * c;
                 tz += -mr * D.Fdz_df[j] * c;
                 tt += -D.Q_sd[j] / (rhoi * cpi) * c;
-            });
+            };
+            const int cd = W.ncntd[i];
+            if (cd <= P.nbd_cap) {
+                for (int k = 0; k < cd; k++) dem(W.nbrd[(size_t)k * n + i]);
+            } else {
+                int ic, jc, kc;
+                cell_ijk(P, xi, yi, zi, ic, jc, kc);
+                for_stencil_j(P, ic, jc, kc, drows, make_cull(xi, yi, zi, Rr), dem);
+            }
         }
         ftx += tx;
         fty += ty;
@@ -1226,28 +1373,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, Sp
     for (int i = a0 + lane; i < e0; i += 32) any_wall |= S.ptype[i] <= 0;
     if (!__any_sync(0xffffffffu, any_wall)) return;
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
-    int len = 0, lo = 0;
-    if (lane < 9) {
-        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
-        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
-            int4 r = __ldg(rows + ic + P.NI * jy + P.NI * P.NJ * kz);
-            lo = r.x;
-            len = max(r.w - r.x, 0);
-        }
-    }
-    int inc = len;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += v;
-    }
-    if (lane < 9) {
-        srow[w][lane + 1] = inc;
-        srow[w][10 + lane] = lo;
-    }
-    if (lane == 0) srow[w][0] = 0;
-    const int tot = __shfl_sync(0xffffffffu, inc, 8);
-    __syncwarp();
+    const int tot = stage_rows(P, ic, jc, kc, rows, srow[w], lane);
     const int4 q0 = ldr(rec.pos + a0);
     const bool o_oor = (q0.w & TAG_OOR) != 0;
     const float sx = P.q_step[0], sy = P.q_step[1], sz = P.q_step[2];
@@ -1292,9 +1418,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, Sp
                 int4 qj = make_int4(0, 0, 0, 0);
                 int j = 0;
                 if (tl < tot) {
-                    int r = 0;
-                    while (tl >= srow[w][r + 1]) r++;
-                    j = srow[w][10 + r] + (tl - srow[w][r]);
+                    j = row_slot(srow[w], tl);
                     qj = ldr(rec.pos + j);
                     const int ptj = tag_ptype(qj.w);
                     keep = ptj >= 1 && ptj < 1000;

@@ -18,6 +18,7 @@ _I32 = [
     "penetration_solve", "switch_ptype", "noslip_bc", "decouple_stride",
     "ppe_mode", "warm_start", "ppe_max_iter", "precision", "dem_wall_mask",
     "mlp_train_steps", "mlp_updates", "mlp_seed", "warm_hist", "warm_fit", "w_lanes",
+    "dem_list_cap",
 ]
 _F64_A = [
     "kappa", "p_ref", "gamma", "dt", "time", "time_end",
@@ -57,6 +58,22 @@ class SphdemParams(C.Structure):
             v = getattr(self, name)
             out[name] = list(v) if hasattr(v, "__len__") else v
         return out
+
+    @classmethod
+    def from_dict(cls, d):
+        """Inverse of as_dict; fields missing from d stay zero."""
+        p = cls()
+        for name, typ in cls._fields_:
+            if name not in d:
+                continue
+            v = d[name]
+            if hasattr(v, "__len__"):
+                arr = getattr(p, name)
+                for k, x in enumerate(v):
+                    arr[k] = x
+            else:
+                setattr(p, name, v)
+        return p
 
 
 class SphdemStats(C.Structure):

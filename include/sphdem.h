@@ -147,6 +147,9 @@ typedef struct SphdemParams {
     int32_t warm_hist;          /* WARM_PROJECT/MLP: previous pressure changes used (0..SPHDEM_WARM_HIST_MAX) */
     int32_t warm_fit;           /* WARM_PROJECT/MLP: SPHDEM_FIT_* bits */
     int32_t w_lanes;            /* 2-D WCSPH: lanes per particle of the gathers (1,2,4,8,16); 0 = timed at commit */
+    int32_t dem_list_cap;       /* ISPH-DEM: SPH -> DEM list entries per particle; 0 = sized at commit from an
+                                   exact count.  A particle with more DEM neighbours walks its stencil instead
+                                   (same sums, same order). */
 
     /* -- real switches: vif[] of function_init.cuh:59-100 -- */
     double kappa;               /* vif[0]  */
@@ -294,7 +297,7 @@ int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem,
 /* Read input_dir/solv.txt, input_dir/data.txt and input_dir/input.txt
  * (function_init.cuh:216-1182, ISPH.cuh:55-113) and create an engine.
  * ov may be NULL; when given, its non-switch engine extensions
- * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit, w_lanes,
+ * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit, w_lanes, dem_list_cap,
  * mlp_train_steps, mlp_updates, mlp_seed, mlp_lr) override the defaults. */
 int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
                            SphdemHandle** out);

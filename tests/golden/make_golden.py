@@ -97,7 +97,8 @@ def w_worker(name, out):
     ns, nd = C.c_int(), C.c_int()
     nijk = (C.c_int * 3)()
     L.ref_counts(C.byref(ns), C.byref(nd), nijk)
-    blob = {"params": np.frombuffer(bytes(p), dtype=np.uint8), "nijk": np.array(list(nijk))}
+    blob = {"params_json": np.frombuffer(json.dumps(p.as_dict()).encode(), dtype=np.uint8),
+            "nijk": np.array(list(nijk))}
     for k, v in sph.items():
         blob["in_sph_" + k] = np.asarray(v)
     done = 0
@@ -136,7 +137,8 @@ def worker(name, out):
     ns, nd = C.c_int(), C.c_int()
     nijk = (C.c_int * 3)()
     L.ref_counts(C.byref(ns), C.byref(nd), nijk)
-    blob = {"params": np.frombuffer(bytes(p), dtype=np.uint8), "nijk": np.array(list(nijk))}
+    blob = {"params_json": np.frombuffer(json.dumps(p.as_dict()).encode(), dtype=np.uint8),
+            "nijk": np.array(list(nijk))}
     for k, v in sph.items():
         blob["in_sph_" + k] = np.asarray(v)
     for k, v in dem.items():

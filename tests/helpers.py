@@ -1,5 +1,6 @@
 """Comparison helpers shared by the parity tests."""
 import glob
+import json
 import os
 
 import numpy as np
@@ -33,7 +34,7 @@ def golden_files():
 
 def load_golden(path):
     g = np.load(path)
-    p = SphdemParams.from_buffer_copy(g["params"].tobytes())
+    p = SphdemParams.from_dict(json.loads(g["params_json"].tobytes().decode()))
     sph = {k[len("in_sph_"):]: g[k] for k in g.files if k.startswith("in_sph_")}
     dem = {k[len("in_dem_"):]: g[k] for k in g.files if k.startswith("in_dem_")}
     for d in (sph, dem):

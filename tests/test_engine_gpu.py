@@ -155,6 +155,26 @@ def test_fp32_vs_fp64_engine_builds(calm_bed):
     assert worst < 1e-3, sorted(report.items(), key=lambda kv: -kv[1])[:5]
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_dem_list_cap_walks_stencil_bit_identical(contact_bed, prec):
+    """The SPH kernels that sum over DEM spheres walk the per-step SPH -> DEM
+    list, or the 27-cell stencil for a particle with more DEM neighbours than
+    the list holds.  Both visit the same spheres in the same order, so a cap
+    of one entry (nearly every particle in the bed walks its stencil) gives
+    the same bits as the auto-sized list."""
+    p, sph, dem = contact_bed
+    a = _engine(p, sph, dem, prec)
+    q = p.copy()
+    q.dem_list_cap = 1
+    b = _engine(q, sph, dem, prec)
+    a.step(5)
+    b.step(5)
+    for which, fields in ((SPH, SPH_REAL), (DEM, DEM_REAL)):
+        assert np.array_equal(_ids(a, which), _ids(b, which))
+        for f in fields:
+            assert np.array_equal(a.get(which, f), b.get(which, f)), ("dem" if which else "sph", f)
+
+
 def test_stats_and_time(calm_bed):
     p, sph, dem = calm_bed
     eng = _engine(p, sph, dem, 0)
