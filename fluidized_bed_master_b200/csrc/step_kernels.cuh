@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                                                                       const int4* __restrict__ rows,
                                                                       int* __restrict__ nbr,
                                                                       int* __restrict__ ncnt, DevFlags* F) {
-    __shared__ float4 sc[LT_WARPS][LT_CH];
+    __shared__ float4 sc[LT_WARPS][LT_CH + 4];
     __shared__ int srow[LT_WARPS][20];   // prefix[10] | start[9]
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * LT_WARPS + w;
@@ -297,24 +297,57 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
         int cnt = 0;
         int* pw = nbr ? nbr + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
         const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
-        for (int t0 = 0; t0 < tot; t0 += LT_CH) {
-            const int tn = min(LT_CH, tot - t0);
-            const int tp = (tn + 3) & ~3;   // padded to whole groups of four
-            // stage candidates t0 .. t0+tn-1; the padding lies far outside every radius
+        // Candidates that no lane of this group can reach are not staged: the
+        // lanes' box [bl, bh] and their largest prefilter radius hb.  The box
+        // distance is formed like a lane's r^2 from differences that are no
+        // larger, and FP32 rounding is monotone, so a candidate with box
+        // distance^2 > hb (1 + 2^-20) has r^2 > hi2 for every lane.  Off while
+        // a lane takes the FP64 path; a candidate outside the fixed-point
+        // range is always staged.
+        float blx = act ? fx : 3e38f, bly = act ? fy : 3e38f, blz = act ? fz : 3e38f;
+        float bhx = act ? fx : -3e38f, bhy = act ? fy : -3e38f, bhz = act ? fz : -3e38f;
+        float hb = act ? hi2 : 0.f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            blx = fminf(blx, __shfl_xor_sync(0xffffffffu, blx, o));
+            bly = fminf(bly, __shfl_xor_sync(0xffffffffu, bly, o));
+            blz = fminf(blz, __shfl_xor_sync(0xffffffffu, blz, o));
+            bhx = fmaxf(bhx, __shfl_xor_sync(0xffffffffu, bhx, o));
+            bhy = fmaxf(bhy, __shfl_xor_sync(0xffffffffu, bhy, o));
+            bhz = fmaxf(bhz, __shfl_xor_sync(0xffffffffu, bhz, o));
+            hb = fmaxf(hb, __shfl_xor_sync(0xffffffffu, hb, o));
+        }
+        hb *= 1.f + 9.5367431640625e-07f;
+        const unsigned lt = (1u << lane) - 1u;
+        int t = 0;
+        while (t < tot) {
+            // stage the next candidates that pass the box test, in order
+            int tn = 0;
             bool any_oor = false;
-            for (int u = lane; u < tp; u += 32) {
-                float4 v = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(0));
-                if (u < tn) {
-                    const int t = t0 + u;
-                    const int j = row_slot(srow[w], t);
+            while (t < tot && tn <= LT_CH - 32) {
+                const int tl = t + lane;
+                bool keep = false;
+                float4 v;
+                if (tl < tot) {
+                    const int j = row_slot(srow[w], tl);
                     const int4 qj = ldr(rec.pos + j);
                     const bool oor = (qj.w & TAG_OOR) != 0;
-                    any_oor |= oor;
                     v = make_float4((float)(qj.x - q0.x) * sx, (float)(qj.y - q0.y) * sy, (float)(qj.z - q0.z) * sz,
                                     __int_as_float(j | (oor ? (int)0x80000000 : 0)));
+                    const float dx = fmaxf(fmaxf(blx - v.x, v.x - bhx), 0.f);
+                    const float dy = fmaxf(fmaxf(bly - v.y, v.y - bhy), 0.f);
+                    const float dz = fmaxf(fmaxf(blz - v.z, v.z - bhz), 0.f);
+                    keep = oor || lanes_slow || dx * dx + dy * dy + dz * dz <= hb;
+                    any_oor |= keep && oor;
                 }
-                sc[w][u] = v;
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) sc[w][tn + __popc(m & lt)] = v;
+                tn += __popc(m);
+                t += 32;
             }
+            // padded to whole groups of four; the padding lies far outside every radius
+            const int tp = (tn + 3) & ~3;
+            if (lane < tp - tn) sc[w][tn + lane] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(0));
             const bool slow_chunk = lanes_slow || __any_sync(0xffffffffu, any_oor);
             __syncwarp();
             if (act && !slow_chunk) {
