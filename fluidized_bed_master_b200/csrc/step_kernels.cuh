@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
 // rho_new so that no thread sees a half-updated neighbour.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128, 8) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
                                                const int4* __restrict__ drows) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
