@@ -237,6 +237,51 @@ __device__ __forceinline__ int row_slot(const int* s, int t) {
     return s[10 + r] + (t - s[r]);
 }
 
+// Relative FP32 coordinates of the cell-tiled passes.  A fixed-point
+// position q is staged as (q - q0) x step, q0 a particle of the cell.  A
+// position within Lk = 2 cell widths of q0 on every axis (all of a cell's
+// stencil, unless a particle outside the box was clamped into a boundary
+// cell) is 'near'; each staged coordinate then carries at most 2 x 2^-24 Lk
+// of rounding (int -> float and x step), a difference at most 6 x 2^-24 Lk,
+// and r^2 near Rr^2 moves by at most 2 sqrt(3) Rr (6 x 2^-24 L) + 3 FP32
+// roundings, L = max Lk.  rel_band returns b with |r^2 error| < b Rr^2:
+// 1.3e-6 L/Rr covers the rounding, q_abs/Rr the fixed-point quantisation
+// of both positions, 1e-6 the rest.  A pair with a position outside the
+// fixed-point range or not near takes the FP64 predicate.
+struct RelFrame {
+    int4 q0;
+    int lx, ly, lz;         // 2 cell widths in steps per axis
+    double L;               // max 2 cell widths (length)
+    float sx, sy, sz;
+    bool o_oor;             // q0 outside the fixed-point range: every pair exact
+};
+__device__ __forceinline__ RelFrame rel_frame(const DevParams& P, const int4& q0) {
+    RelFrame F;
+    F.q0 = q0;
+    const double wx = (P.xmax - P.xmin) / P.NI, wy = (P.ymax - P.ymin) / P.NJ, wz = (P.zmax - P.zmin) / P.NK;
+    F.lx = (int)fmin(2.0 * wx * P.q_inv[0] + 2.0, 2147483647.0);
+    F.ly = (int)fmin(2.0 * wy * P.q_inv[1] + 2.0, 2147483647.0);
+    F.lz = (int)fmin(2.0 * wz * P.q_inv[2] + 2.0, 2147483647.0);
+    F.L = 2.0 * fmax(fmax(wx, wy), wz);
+    F.sx = P.q_step[0];
+    F.sy = P.q_step[1];
+    F.sz = P.q_step[2];
+    F.o_oor = (q0.w & TAG_OOR) != 0;
+    return F;
+}
+// q outside the fixed-point range or not near q0.  In-range coordinates
+// are below 2^30 in magnitude (quantize), so the int differences are exact.
+__device__ __forceinline__ bool rel_slow(const RelFrame& F, const int4& q) {
+    return (q.w & TAG_OOR) || abs(q.x - F.q0.x) > F.lx || abs(q.y - F.q0.y) > F.ly || abs(q.z - F.q0.z) > F.lz;
+}
+__device__ __forceinline__ float4 rel_coord(const RelFrame& F, const int4& q, int tagw) {
+    return make_float4((float)(q.x - F.q0.x) * F.sx, (float)(q.y - F.q0.y) * F.sy, (float)(q.z - F.q0.z) * F.sz,
+                       __int_as_float(tagw));
+}
+__device__ __forceinline__ double rel_band(const DevParams& P, const RelFrame& F, double Rr) {
+    return 1e-6 + 1.3e-6 * F.L / Rr + P.q_abs / Rr;
+}
+
 // Cell-tiled list build (FP32 build).  One warp per cell: the particles of
 // a cell share one stencil, so the warp stages the candidates of the 9 rows
 // once, as FP32 coordinates relative to a particle of the cell, into shared
@@ -247,10 +292,9 @@ __device__ __forceinline__ int row_slot(const int* s, int t) {
 // conversion.  Each lane appends its hits in staged order, which is the
 // reference's z, y, x cell order with ascending slots, so the list equals
 // the one-particle-per-thread build.  Prefilter: r^2 against Rr^2 (1 -/+ b)
-// with b = 4e-6 + 8 steps/Rr; the staged coordinates are within 2 cells
-// (2.2 Rr) of the origin, so their FP32 rounding moves r^2 by at most
-// 1.3e-6 of Rr^2, inside b.  Pairs in the band, or with a particle outside
-// the fixed-point range, take the reference predicate in FP64.
+// with b from rel_band.  Pairs in the band, or with a position outside the
+// fixed-point range or not near the origin, take the reference predicate in
+// FP64.
 constexpr int LT_WARPS = 4, LT_CH = 256;
 __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P, SphState<float> S,
                                                                       SphRec<float> rec,
@@ -270,10 +314,8 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
     const int e0 = __ldg(ge + c);
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
     const int tot = stage_rows(P, ic, jc, kc, rows, srow[w], lane);
-    const int4 q0 = ldr(rec.pos + a0);   // origin of the relative coordinates
-    const bool o_oor = (q0.w & TAG_OOR) != 0;
+    const RelFrame Fr = rel_frame(P, ldr(rec.pos + a0));   // origin of the relative coordinates
     const int n = P.ns, cap = P.nb_cap;
-    const float sx = P.q_step[0], sy = P.q_step[1], sz = P.q_step[2];
     for (int p0 = a0; p0 < e0; p0 += 32) {
         const int i = p0 + lane;
         const bool act = i < e0;
@@ -285,14 +327,15 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
             yi = S.y[i];
             zi = S.z[i];
             Rr = __dmul_rn(P.kappa, S.h[i]);
-            const double b = 4e-6 + P.q_abs / Rr, r2 = Rr * Rr;
+            const double b = rel_band(P, Fr, Rr), r2 = Rr * Rr;
             lo2 = (float)(r2 * (1.0 - b));
             hi2 = (float)(r2 * (1.0 + b));
             const int4 qi = ldr(rec.pos + i);
-            slow = o_oor || (qi.w & TAG_OOR);
-            fx = (float)(qi.x - q0.x) * sx;
-            fy = (float)(qi.y - q0.y) * sy;
-            fz = (float)(qi.z - q0.z) * sz;
+            slow = Fr.o_oor || rel_slow(Fr, qi);
+            const float4 f = rel_coord(Fr, qi, 0);
+            fx = f.x;
+            fy = f.y;
+            fz = f.z;
         }
         int cnt = 0;
         int* pw = nbr ? nbr + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
@@ -331,9 +374,8 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                 if (tl < tot) {
                     const int j = row_slot(srow[w], tl);
                     const int4 qj = ldr(rec.pos + j);
-                    const bool oor = (qj.w & TAG_OOR) != 0;
-                    v = make_float4((float)(qj.x - q0.x) * sx, (float)(qj.y - q0.y) * sy, (float)(qj.z - q0.z) * sz,
-                                    __int_as_float(j | (oor ? (int)0x80000000 : 0)));
+                    const bool oor = rel_slow(Fr, qj);
+                    v = rel_coord(Fr, qj, j | (oor ? (int)0x80000000 : 0));
                     const float dx = fmaxf(fmaxf(blx - v.x, v.x - bhx), 0.f);
                     const float dy = fmaxf(fmaxf(bly - v.y, v.y - bhy), 0.f);
                     const float dz = fmaxf(fmaxf(blz - v.z, v.z - bhz), 0.f);
@@ -1077,79 +1119,73 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
 // ---------------------------------------------------------------------------
 // KERNEL_DEM_coupling3D_dem (functions_SPH_DEM_COUPLING2.cuh:627-1129) with
 // KERNEL_clc_projection_dem (functions_TIME_ISPH2.cuh:206-308) fused into its
-// epilogue (the predictor only needs this particle's force).  One warp per
-// DEM sphere; lanes stride over the SPH candidate rows and the partial
-// Shepard sums are reduced with shuffles.
+// epilogue (the predictor only needs this particle's force).  The pair sums
+// of one sphere over its SPH neighbours (dc_pair) are formed by a warp --
+// lanes over the candidates, partial sums reduced with shuffles -- and one
+// lane runs the drag closure and the predictor (dem_coupling_finish).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int4* __restrict__ srows) {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
-    int* sm = s_rows[threadIdx.x >> 5];
-    if (i >= P.nd) return;
-    int it = D.itype[i], pt = D.ptype[i];
-    if (it > 2) return;
+struct DcSums {
+    R tx, ty, tz, ufx, ufy, ufz, uax, uay, uaz, por, ttf, tta;
+    int has_f, has_a;
+};
+
+// one SPH neighbour j of sphere i at distance r (the pair already passed the
+// kappa h_i test): Shepard sums of fluid/air velocity, temperature and
+// porosity, and the pressure-gradient force
+template <typename R>
+__device__ __forceinline__ void dc_pair(const SphWork<R>& W, const Knl<R>& K, R ff, R fa, R pgc, int j, int ptj, R r,
+                                        DcSums<R>& a) {
+    const V4<R> fj = ldr(W.rec.f1 + j);
+    const R porj = fj.w;
+    if (!(porj < (R)1)) return;
+    R w = kw(K, r);
+    R mj = fj.x, rhoj = fj.y, c = mj * w * rcp(rhoj);
+    if ((ptj == 1 && ff > (R)0.000001) || (ptj == 3 && fa > (R)0.000001)) {
+        V4<R> uj = ldr(W.rec.up + j);
+        if (ptj == 1) {
+            a.has_f = 1;
+            a.ufx += uj.x * c; a.ufy += uj.y * c; a.ufz += uj.z * c;
+            a.ttf += fj.z * c;
+        } else {
+            a.has_a = 1;
+            a.uax += uj.x * c; a.uay += uj.y * c; a.uaz += uj.z * c;
+            a.tta += fj.z * c;
+        }
+        a.por += porj * c;
+    }
+    if (ptj != 0 && ptj != 9 && ptj != -3 && ptj != 3 && ff > (R)0.01) {
+        R q = c * pgc;
+        a.tx += W.pgfx[j] * q;
+        a.ty += W.pgfy[j] * q;
+        a.tz += W.pgfz[j] * q;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void dc_warp_sum(DcSums<R>& a) {
+    a.tx = warp_sum(a.tx); a.ty = warp_sum(a.ty); a.tz = warp_sum(a.tz);
+    a.ufx = warp_sum(a.ufx); a.ufy = warp_sum(a.ufy); a.ufz = warp_sum(a.ufz);
+    a.uax = warp_sum(a.uax); a.uay = warp_sum(a.uay); a.uaz = warp_sum(a.uaz);
+    a.por = warp_sum(a.por); a.ttf = warp_sum(a.ttf); a.tta = warp_sum(a.tta);
+    a.has_f = __any_sync(0xffffffffu, a.has_f);
+    a.has_a = __any_sync(0xffffffffu, a.has_a);
+}
+
+// drag closure on the reduced sums (when coupled) and the DEM predictor
+template <typename R>
+__device__ void dem_coupling_finish(const DevParams& P, DemState<R>& D, DemWork<R>& DW, int i, bool coupled,
+                                    const DcSums<R>& a) {
+    const int pt = D.ptype[i];
     R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i];
     R ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
-    if (it == 1 && pt > 1000) {
-        const SphRec<R> rec = W.rec;
-        double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
-        R radi = (R)D.rad[i], di = (R)2 * radi, voli = ((R)4 / (R)3) * (R)3.14159 * radi * radi * radi;
+    if (coupled) {
+        R radi = (R)D.rad[i], di = (R)2 * radi;
         R mi = D.m[i], rhoi = D.rho[i], tempi = D.temp[i];
         R fa = DW.flt_s[i], ff = DW.flt_sd[i];
-        R th = (R)hi;
-        Knl<R> K = knl_make<R>(P, th);
-        double Rr = P.kappa * hi;
-        Band bd = make_band(P, Rr);
-        PosRec<R> qp = make_pos<R>(P, xi, yi, zi, 0, 0, 0);
-        int ic, jc, kc;
-        cell_ijk(P, xi, yi, zi, ic, jc, kc);
-        R tx = 0, ty = 0, tz = 0, ufx = 0, ufy = 0, ufz = 0, uax = 0, uay = 0, uaz = 0, por = 0, ttf = 0, tta = 0;
-        int has_f = 0, has_a = 0;
-        R pgc = voli / (mi * ff + (R)1.0e-15);
-        const Cull cu = make_cull(xi, yi, zi, Rr);
-        for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
-            PosRec<R> qj = ldr(rec.pos + j);
-            int ptj = tag_ptype(qj.w);
-            if (ptj > 1000) return;
-            V4<R> fj = ldr(rec.f1 + j);
-            R porj = fj.w;
-            if (!(porj < (R)1)) return;
-            Disp<R> d;
-            R r2;
-            if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 0.0, bd, d, r2)) return;
-            R r, rinv;
-            rdist(r2, r, rinv);
-            R w = kw(K, r);
-            R mj = fj.x, rhoj = fj.y, c = mj * w * rcp(rhoj);
-            if ((ptj == 1 && ff > (R)0.000001) || (ptj == 3 && fa > (R)0.000001)) {
-                V4<R> uj = ldr(rec.up + j);
-                if (ptj == 1) {
-                    has_f = 1;
-                    ufx += uj.x * c; ufy += uj.y * c; ufz += uj.z * c;
-                    ttf += fj.z * c;
-                } else {
-                    has_a = 1;
-                    uax += uj.x * c; uay += uj.y * c; uaz += uj.z * c;
-                    tta += fj.z * c;
-                }
-                por += porj * c;
-            }
-            if (ptj != 0 && ptj != 9 && ptj != -3 && ptj != 3 && ff > (R)0.01) {
-                R q = c * pgc;
-                tx += W.pgfx[j] * q;
-                ty += W.pgfy[j] * q;
-                tz += W.pgfz[j] * q;
-            }
-        });
-        tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
-        ufx = warp_sum(ufx); ufy = warp_sum(ufy); ufz = warp_sum(ufz);
-        uax = warp_sum(uax); uay = warp_sum(uay); uaz = warp_sum(uaz);
-        por = warp_sum(por); ttf = warp_sum(ttf); tta = warp_sum(tta);
-        has_f = __any_sync(0xffffffffu, has_f);
-        has_a = __any_sync(0xffffffffu, has_a);
-        if (lane != 0) return;
+        const R tx = a.tx, ty = a.ty, tz = a.tz, ufx = a.ufx, ufy = a.ufy, ufz = a.ufz;
+        const R uax = a.uax, uay = a.uay, uaz = a.uaz, por = a.por, ttf = a.ttf, tta = a.tta;
+        const int has_f = a.has_f, has_a = a.has_a;
         R rho_f = has_f ? (R)P.rho_gas : (R)0, rho_a = has_a ? (R)P.rho_gas : (R)0;
         R ki = (radi < (R)0.0012) ? (R)55.0 : (R)0.84;
         R ali = (radi < (R)0.0012) ? (R)1.77e-5 : (R)2.5e-6;
@@ -1219,7 +1255,6 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         DW.Fdx_da[i] = dax; DW.Fdy_da[i] = day; DW.Fdz_da[i] = daz;
         DW.Fdx_b[i] = tx; DW.Fdy_b[i] = ty; DW.Fdz_b[i] = tz;
     }
-    if (lane != 0) return;
     // predictor (DEM): u* = u + f dt
     DW.ux0[i] = uxi; DW.uy0[i] = uyi; DW.uz0[i] = uzi;
     if (pt == 9) {
@@ -1233,6 +1268,49 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         D.uz[i] = uzi + ftz * b * dt;
     }
     if (P.con && pt > 0) DW.temp0[i] = D.temp[i];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+                                                      DemWork<R> DW, const int4* __restrict__ srows) {
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_rows[4][20];   // 128 threads = 4 warps
+    int* sm = s_rows[threadIdx.x >> 5];
+    if (i >= P.nd) return;
+    int it = D.itype[i], pt = D.ptype[i];
+    if (it > 2) return;
+    DcSums<R> a{};
+    const bool coupled = it == 1 && pt > 1000;
+    if (coupled) {
+        const SphRec<R> rec = W.rec;
+        double xi = D.x[i], yi = D.y[i], zi = D.z[i], hi = D.h[i];
+        R radi = (R)D.rad[i], voli = ((R)4 / (R)3) * (R)3.14159 * radi * radi * radi;
+        R mi = D.m[i];
+        R fa = DW.flt_s[i], ff = DW.flt_sd[i];
+        R th = (R)hi;
+        Knl<R> K = knl_make<R>(P, th);
+        double Rr = P.kappa * hi;
+        Band bd = make_band(P, Rr);
+        PosRec<R> qp = make_pos<R>(P, xi, yi, zi, 0, 0, 0);
+        int ic, jc, kc;
+        cell_ijk(P, xi, yi, zi, ic, jc, kc);
+        R pgc = voli / (mi * ff + (R)1.0e-15);
+        const Cull cu = make_cull(xi, yi, zi, Rr);
+        for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
+            PosRec<R> qj = ldr(rec.pos + j);
+            int ptj = tag_ptype(qj.w);
+            if (ptj > 1000) return;
+            Disp<R> d;
+            R r2;
+            if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 0.0, bd, d, r2)) return;
+            R r, rinv;
+            rdist(r2, r, rinv);
+            dc_pair(W, K, ff, fa, pgc, j, ptj, r, a);
+        });
+        dc_warp_sum(a);
+    }
+    if (lane != 0) return;
+    dem_coupling_finish(P, D, DW, i, coupled, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -1388,7 +1466,7 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
 // reference predicate inside the band.  Same sums as k_neumann in candidate
 // order per wall, so the FP32 results differ from it by rounding only.
 constexpr int NT_WARPS = 4, NT_CH = 128;
-__global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
+__global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
                                                                    float* pres, const int* __restrict__ gs,
                                                                    const int* __restrict__ ge,
                                                                    const int4* __restrict__ rows, int patch_up) {
@@ -1407,9 +1485,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, Sp
     if (!__any_sync(0xffffffffu, any_wall)) return;
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
     const int tot = stage_rows(P, ic, jc, kc, rows, srow[w], lane);
-    const int4 q0 = ldr(rec.pos + a0);
-    const bool o_oor = (q0.w & TAG_OOR) != 0;
-    const float sx = P.q_step[0], sy = P.q_step[1], sz = P.q_step[2];
+    const RelFrame Fr = rel_frame(P, ldr(rec.pos + a0));
     const unsigned lt = (1u << lane) - 1u;
     for (int p0 = a0; p0 < e0; p0 += 32) {
         const int i = p0 + lane;
@@ -1429,14 +1505,15 @@ __global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, Sp
             K.ih = rcp(th2);
             K.th = th2;
             R2 = 2.0 * (P.kappa * hi);
-            const double b = 4e-6 + P.q_abs / R2, r2 = R2 * R2;
+            const double b = rel_band(P, Fr, R2), r2 = R2 * R2;
             lo2 = (float)(r2 * (1.0 - b));
             hi2 = (float)(r2 * (1.0 + b));
             const int4 qi = ldr(rec.pos + i);
-            slow = o_oor || (qi.w & TAG_OOR);
-            fx = (float)(qi.x - q0.x) * sx;
-            fy = (float)(qi.y - q0.y) * sy;
-            fz = (float)(qi.z - q0.z) * sz;
+            slow = Fr.o_oor || rel_slow(Fr, qi);
+            const float4 f = rel_coord(Fr, qi, 0);
+            fx = f.x;
+            fy = f.y;
+            fz = f.z;
         }
         const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
         float tp = 0.f, flt = 0.f, tt = 0.f, tr = 0.f;
@@ -1459,12 +1536,11 @@ __global__ void __launch_bounds__(NT_WARPS * 32) k_neumann_tiled(DevParams P, Sp
                 const unsigned m = __ballot_sync(0xffffffffu, keep);
                 if (keep) {
                     const int pos = ns + __popc(m & lt);
-                    const bool oor = (qj.w & TAG_OOR) != 0;
+                    const bool oor = rel_slow(Fr, qj);
                     any_oor |= oor;
                     const float4 fj = ldr(rec.f1 + j);
                     const float mr = fj.x * rcp(fj.y);
-                    sa[w][pos] = make_float4((float)(qj.x - q0.x) * sx, (float)(qj.y - q0.y) * sy,
-                                             (float)(qj.z - q0.z) * sz, __int_as_float(j | (oor ? (int)0x80000000 : 0)));
+                    sa[w][pos] = rel_coord(Fr, qj, j | (oor ? (int)0x80000000 : 0));
                     sb[w][pos] = make_float4(mr, pres[j], fj.z, fj.x * rcp(fj.w));
                 }
                 ns += __popc(m);
