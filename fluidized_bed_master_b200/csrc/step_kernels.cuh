@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     int cnt = min(W.ncnt[i], P.nb_cap);
     R flt = 0, tx = 0, ty = 0, tz = 0, px = 0, py = 0, pz = 0, Rc = 0, ex = 0, ey = 0, ez = 0, et = 0;
     const int* __restrict__ nb = W.nbr;
-    nb_walk<2, NbQ44<R>>(
+    nb_walk<4, NbQ44<R>>(
         cnt, nb, n, i,
         [&](int j) {
             NbQ44<R> t;
