@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "dam2d-batch", "ppe-profile"],
+    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
                          "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
                          "against the same beds run one after another; ppe-profile: --steps steps of the bed with the "
@@ -361,6 +361,134 @@ def _timed_steps(eng, stream, flush, k):
         e1.synchronize()
         tot += e0.elapsed_time(e1)
     return tot
+
+
+COLUMN_TEXT = ("3-D ISPH column without DEM: 0.2x0.2x0.4 m water-like column at dx=4 mm (50x50x100 = 250,000 "
+               "fluid, seeded jitter +/-0.01 dx) in a closed box of three wall layers, Wendland C2, h=1.3dx, "
+               "hydrostatic pressure plus one sloshing roll (max 0.05 m/s), projection with the PPE solved by "
+               "Jacobi-PCG to relative residual 1e-6, dt=1e-4 s")
+COLUMN_CHECK_STEPS = 200
+
+
+def run_column(args, world, rank, local, pg):
+    """The 3-D ISPH column: particle-updates/s of the FP32 build, PCG
+    iterations per step, and every field of the FP32 build against the FP64
+    build of the same kernels after 200 steps."""
+    import torch
+
+    from fluidized_bed_master_b200.beds import isph_column
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import SPH
+
+    metric = "ISPH particle-updates/s on 1 B200 (3-D column, PPE by PCG to 1e-6)"
+    unit = "particle-updates/s"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import Oracle
+        threads = os.cpu_count() or 1
+        p, sph, _ = isph_column(dx=1.0e-2, seed=0)
+        o = Oracle(p, sph, {}, threads=threads)
+        o.step(1)
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < max(5.0, args.cpu_seconds) and k < 2000:
+            o.step(2)
+            k += 2
+        el = time.perf_counter() - t0
+        val = o.ns * k / el
+        line = {"metric": metric, "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded column)",
+                "config": {"workload": COLUMN_TEXT},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": f"the same column at dx=10 mm ({o.ns} particles), {k} steps"},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local)
+    p, sph, _ = isph_column(seed=rank)
+    q = p.copy()
+    q.precision = 1 if args.precision == "fp64" else 0
+    eng = Engine(q, sph, {})
+    n = eng.ns
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
+    sampler = ClockSampler(int(vis) if vis.isdigit() else local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    t_tot, launches, iters = 0.0, 0, []
+    for _ in range(args.steps):
+        t_tot += _timed_steps(eng, stream, flush, 1)
+        launches += eng.launches()
+        st = eng.stats()
+        iters.append(st["ppe_iters"])
+        if st["ppe_status"] != 0 or not st["ppe_rel_residual"] <= p.ppe_tol:
+            raise RuntimeError(f"PCG did not reach {p.ppe_tol}: {st}")
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    t_max = reduce_over_ranks(pg, t_tot, "max", "cuda")
+    n_all = reduce_over_ranks(pg, n, "sum", "cuda")
+    value = n_all * args.steps / (t_max / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        def pinned(k, dt):
+            return torch.empty(k, dtype=dt, pin_memory=True).numpy()
+        fields = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp"]
+        hs = {f: pinned(n, torch.float64) for f in fields}
+        for f in fields:
+            hs[f][:] = eng.get(SPH, f)
+        hb = sum(a.nbytes for a in hs.values())
+        ke = max(3, min(args.steps, 20))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            eng.set_fields(SPH, hs)
+            eng.step(1)
+            eng.get_fields(SPH, hs)
+        torch.cuda.synchronize()
+        te = reduce_over_ranks(pg, time.perf_counter() - t0, "max", "cuda")
+        e2e = {"value": n_all * ke / te, "unit": unit, "h2d_bytes_per_step": hb, "d2h_bytes_per_step": hb,
+               "ms_per_step": te / ke * 1e3,
+               "how": "per step: sphdem_set_fields of the particle state from pinned host arrays, sphdem_step, "
+                      "sphdem_get_fields back"}
+    eng.close()
+    check = None
+    if rank == 0 and not args.no_cpu:
+        # every field of the FP32 build against the FP64 build after 200 steps
+        runs = {}
+        for prec in (0, 1):
+            r = p.copy()
+            r.precision = prec
+            e = Engine(r, sph, {})
+            e.step(COLUMN_CHECK_STEPS)
+            ids = e.get(SPH, "pid")
+            runs[prec] = {f: np.empty(n) for f in ("x", "y", "z", "ux", "uy", "uz", "rho", "pres")}
+            for f in runs[prec]:
+                runs[prec][f][ids] = e.get(SPH, f)
+            e.close()
+        rel = {f: float(np.linalg.norm(runs[0][f] - runs[1][f]) / max(np.linalg.norm(runs[1][f]), 1e-300))
+               for f in runs[0]}
+        check = {"steps": COLUMN_CHECK_STEPS, "rel_l2": rel, "max": max(rel.values())}
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if q.precision == 0 else "f64", "data": "synthetic (seeded column)",
+        "config": {"workload": COLUMN_TEXT, "n": n, "n_fluid": int((sph["p_type"] == 1).sum()),
+                   "l2": "256 MB buffer written before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "ppe_iters_per_step": float(np.mean(iters)) if iters else None,
+        "fp32_vs_fp64": check, "roofline": None, "cpu_baseline": None, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_dam2d_batch(args, world, rank, local, pg):
@@ -815,6 +943,8 @@ def main():
             run_dam2d(args, world, rank, local, pg)
         elif args.workload == "dam2d-batch":
             run_dam2d_batch(args, world, rank, local, pg)
+        elif args.workload == "column":
+            run_column(args, world, rank, local, pg)
         elif args.workload == "ppe-profile":
             if rank == 0:
                 run_ppe_profile(args)

@@ -14,6 +14,8 @@ run uses one of these generators.  Two families:
   z-major order), Wendland C2 with h = 1.3 dx, DEM spheres of 2 mm +/-5 %
   at density 2500 on random FCC sites in the lower 0.1 m, inlet at the
   bottom, heat transfer on.
+* ``isph_column`` -- a 3-D water column with no DEM in a wall box: the
+  plain ISPH projection with the PPE solved to 1e-6.
 
 Lattice positions get seeded uniform jitter of +/-0.01 dx so that no pair
 sits exactly on a kernel-support boundary.
@@ -178,6 +180,67 @@ def box_bed(n_fluid=200_000, n_dem=20_000, dx=1.25e-3, seed=0, u_in=0.15, t_flui
     p.box_c[:] = [0.5 * lx, 0.5 * ly, 0.5 * lz]
     p.box_L[:] = [lx, ly, lz]
     return p, sph, dem
+
+
+def isph_column(dx=4.0e-3, lx=0.2, ly=0.2, hz=0.4, seed=0, u_slosh=0.05, g=9.81, dt=1.0e-4):
+    """3-D ISPH column without DEM: a 0.2 x 0.2 x 0.4 m water-like column on
+    a dx lattice (50 x 50 x 100 = 250,000 fluid at dx = 4 mm) in a closed
+    box of three wall layers, Wendland C2 with h = 1.3 dx.  The box is
+    closed because the reference's ISPH has no free-surface condition (its
+    p = 0 line for surface particles is commented out,
+    functions_PPE2.cuh:533-534), so a PPE solved to a tolerance has no
+    pressure datum at an open top.  Initial state: hydrostatic pressure
+    rho g (hz - z) and one sloshing roll in the x-z plane,
+    psi = A sin(pi x / lx) sin(pi z / hz), scaled so that the largest speed
+    is u_slosh; it is divergence-free with no normal velocity at any wall.
+    The PPE solves to a relative residual with the Jacobi-preconditioned CG
+    (ppe_mode PCG, 1e-6).  Returns (params, sph, dem) with an empty DEM
+    set."""
+    from .params import PPE_PCG
+
+    rng = np.random.default_rng(seed)
+    p = reference_params()
+    h = 1.3 * dx
+    p.kernel_type = 3
+    p.h_over_dx = 1.3
+    p.rho_gas = 1000.0           # the p_type 1 fluid: water-like
+    p.mu_gas = 1.0e-3
+    p.nu_gas = 1.0e-6
+    p.g_sph = g
+    p.con_solve = 0
+    p.open_boundary = 0
+    p.xsph_solve = 0
+    p.dt = dt
+    p.ppe_mode = PPE_PCG
+    p.kgc_solve = 0              # the CG needs the uncorrected (M-symmetric) operator
+    p.ppe_tol = 1.0e-6
+    p.ppe_max_iter = 2000
+    p.dem_wall_mask = 0
+    nx, ny, nz = int(round(lx / dx)), int(round(ly / dx)), int(round(hz / dx))
+    I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    fluid = np.stack([(I.T.ravel() + 0.5) * dx, (J.T.ravel() + 0.5) * dx, (K.T.ravel() + 0.5) * dx], 1)
+    wx, wy, wz = np.arange(-3, nx + 3), np.arange(-3, ny + 3), np.arange(-3, nz + 3)
+    WI, WJ, WK = np.meshgrid(wx, wy, wz, indexing="ij")
+    side = (WI < 0) | (WI >= nx) | (WJ < 0) | (WJ >= ny) | (WK < 0) | (WK >= nz)
+    walls = np.stack([(WI[side] + 0.5) * dx, (WJ[side] + 0.5) * dx, (WK[side] + 0.5) * dx], 1)
+    pos = np.concatenate([fluid, walls])
+    ptype = np.concatenate([np.ones(len(fluid), np.int32), np.zeros(len(walls), np.int32)])
+    n = len(pos)
+    pos = pos + rng.uniform(-0.01 * dx, 0.01 * dx, size=(n, 3))
+    kx, kz = np.pi / lx, np.pi / hz
+    x, z = pos[:, 0], pos[:, 2]
+    ux = kz * np.sin(kx * x) * np.cos(kz * z)
+    uz = -kx * np.cos(kx * x) * np.sin(kz * z)
+    fl = ptype == 1
+    scale = u_slosh / max(np.sqrt(ux[fl] ** 2 + uz[fl] ** 2).max(), 1e-30)
+    ux, uz = ux * scale * fl, uz * scale * fl
+    vol = (h / p.h_over_dx) ** 3
+    pres = p.rho_gas * g * np.clip(hz - pos[:, 2], 0.0, None)
+    sph = dict(x=pos[:, 0], y=pos[:, 1], z=pos[:, 2], ux=ux, uy=np.zeros(n), uz=uz,
+               m=np.full(n, p.rho_gas * vol), rho=np.full(n, p.rho_gas), pres=pres,
+               temp=np.full(n, 300.0), h=np.full(n, h), flt_s=np.ones(n), p_type=ptype,
+               rad=np.zeros(n), ri=np.zeros(n))
+    return p, sph, {}
 
 
 def scaled_box_bed(n_fluid=2_000_000, n_dem=200_000, seed=0):
