@@ -868,7 +868,8 @@ def run_engine(args, world, rank, local, pg):
 
 def ppe_comparison(args):
     """PPE ms/step and iterations at a relative residual of 1e-6 on the same
-    bed, for four initial iterates of the same Jacobi-PCG:
+    bed, for four initial iterates of the same Jacobi-PCG (and three of them
+    again with the two-level preconditioner, arms *_two_level):
       plain        the previous pressure;
       extrapolated the previous pressure plus its last change;
       projected    the Galerkin projection onto {previous pressure, its
@@ -887,7 +888,7 @@ def ppe_comparison(args):
     DEM) unless args.ppe_bed says "bench"."""
     from fluidized_bed_master_b200.beds import box_bed, scaled_box_bed
     from fluidized_bed_master_b200.engine import Engine
-    from fluidized_bed_master_b200.params import PPE_PCG, WARM_EXTRAPOLATE, WARM_MLP, WARM_PROJECT
+    from fluidized_bed_master_b200.params import PPE_PCG, PRECOND_TWO_LEVEL, WARM_EXTRAPOLATE, WARM_MLP, WARM_PROJECT
 
     if args.ppe_bed == "bench":
         p, sph, dem = box_bed(seed=0, **WORKLOAD)
@@ -899,8 +900,10 @@ def ppe_comparison(args):
     out = {"solver": "Jacobi-PCG, Chronopoulos-Gear form, mass-weighted inner products (FP64 vectors and dots, "
                      "FP32 operator)", "tol": 1e-6, "kgc": 0, "bed": bed, "n_sph": len(sph["x"]),
            "n_dem": len(dem["x"]), "steps_before": args.ppe_train, "measured_steps": meas, "warm_hist": 8}
-    for name, warm in (("plain", 0), ("extrapolated", WARM_EXTRAPOLATE), ("projected", WARM_PROJECT),
-                       ("learned", WARM_MLP)):
+    arms = (("plain", 0, 0), ("extrapolated", WARM_EXTRAPOLATE, 0), ("projected", WARM_PROJECT, 0),
+            ("learned", WARM_MLP, 0), ("plain_two_level", 0, PRECOND_TWO_LEVEL),
+            ("projected_two_level", WARM_PROJECT, PRECOND_TWO_LEVEL), ("learned_two_level", WARM_MLP, PRECOND_TWO_LEVEL))
+    for name, warm, precond in arms:
         q = p.copy()
         q.precision = 0
         q.ppe_mode = PPE_PCG
@@ -911,6 +914,7 @@ def ppe_comparison(args):
         q.warm_hist = 8
         q.warm_fit = 0
         q.mlp_train_steps = args.ppe_train
+        q.ppe_precond = precond
         eng = Engine(q, sph, dem)
         eng.step(args.ppe_train)
         eng.set_timing(True)
@@ -932,6 +936,10 @@ def ppe_comparison(args):
         eng.close()
     out["learned_speedup_vs_plain"] = out["plain"]["ppe_ms_per_step"] / out["learned"]["ppe_ms_per_step"]
     out["learned_speedup_vs_projected"] = out["projected"]["ppe_ms_per_step"] / out["learned"]["ppe_ms_per_step"]
+    # the same starts with the two-level preconditioner (ppe_precond TWO_LEVEL) against the Jacobi arms
+    out["two_level_speedup_plain"] = out["plain"]["ppe_ms_per_step"] / out["plain_two_level"]["ppe_ms_per_step"]
+    out["learned_two_level_speedup_vs_plain"] = (out["plain"]["ppe_ms_per_step"] /
+                                                 out["learned_two_level"]["ppe_ms_per_step"])
     return out
 
 

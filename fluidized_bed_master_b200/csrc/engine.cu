@@ -16,6 +16,7 @@
 
 #include "handle.h"
 #include "ppe_krylov.cuh"
+#include "ppe_mg.cuh"
 #include "mlp.h"
 #include "wcsph2d.cuh"
 
@@ -105,6 +106,8 @@ struct EngineHost {
     Alloc A;
     int nb_cap = 0;
     size_t list_elems = 0;
+    MgWork mg{};             // two-level PCG preconditioner (ppe_precond TWO_LEVEL)
+    bool has_mg = false;
 };
 
 template <typename R>
@@ -282,6 +285,34 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
 // while node of the step graph (captured on a side stream into the node's
 // body graph).  Without a graph the host drives the same body.
 // ---------------------------------------------------------------------------
+// two-level preconditioner: the cell operator and its coarse levels, once
+// per step after the coefficients are assembled
+template <typename R>
+static void mg_setup(EngineHost<R>* EH, cudaStream_t st) {
+    const MgWork& M = EH->mg;
+    k_mg_cellxyz<<<nblocks(EH->E.P.ns, 256), 256, 0, st>>>(EH->E.P.ns, M);
+    k_mg_assemble0<R><<<nblocks(M.L[0].n * 32, 128), 128, 0, st>>>(EH->K, M);
+    for (int l = 1; l < M.nlev; l++) k_mg_coarsen<<<nblocks(M.L[l].n, 128), 128, 0, st>>>(M.L[l - 1], M.L[l]);
+    k_mg_chol<<<1, 256, 0, st>>>(M.L[M.nlev - 1], M.chol);
+}
+
+// z += P0 V (P0^T M r): the coarse part of the preconditioner
+template <typename R>
+static void mg_apply(EngineHost<R>* EH, cudaStream_t st) {
+    const MgWork& M = EH->mg;
+    const KryWork<R>& K = EH->K;
+    const int n0 = M.L[0].n;
+    k_mg_restrict0<<<nblocks(n0 * 32, 128), 128, 0, st>>>(K.r, K.wm, M, K.sc);
+    k_mg_resid<<<nblocks(n0 * 32, 128), 128, 0, st>>>(M.L[0], K.sc);
+    const int nl = M.nlev;
+    for (int l = 1; l < nl - 1; l++)
+        k_mg_down<<<nblocks(M.L[l].n * 32, 128), 128, 0, st>>>(M.L[l - 1], M.L[l], K.sc);
+    k_mg_last<<<1, MG_CHOL_MAX, 0, st>>>(M.L[nl - 2], M.L[nl - 1], M.chol, K.sc);
+    for (int l = nl - 2; l >= 1; l--)
+        k_mg_post<<<nblocks(M.L[l].n * 32, 128), 128, 0, st>>>(M.L[l], M.L[l + 1], K.sc);
+    k_mg_post0<<<nblocks(n0 * 32, 128), 128, 0, st>>>(M, K.kcnt, K.z, K.sc);
+}
+
 template <typename R>
 static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cudaGraphConditionalHandle hnd,
                         int in_graph) {
@@ -292,6 +323,7 @@ static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cud
     if (H->p.ppe_mode == SPHDEM_PPE_PCG) {
         // u in z, w in v, s in s
         k_cg_upd<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.z, K.v, K.p, K.s, K.x, K.r, K.sc);
+        if (EH->has_mg) mg_apply<R>(EH, st);
         k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 0, hnd, in_graph);
     } else {
         k_bicg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.r, K.p, K.v, K.y, K.part, K.sc);
@@ -374,6 +406,7 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
     {
         KTIME(KT_PPE_ASM);
         k_kry_assemble<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W, K, H->p.warm_start == SPHDEM_WARM_EXTRAPOLATE);
+        if (EH->has_mg) mg_setup<R>(EH, st);
     }
     if (phase || K.D) {
         KTIME(KT_PPE_WARM);
@@ -387,6 +420,7 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
     if (cg) {
         k_cg_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.z, K.p, K.s, K.sc, H->p.ppe_tol,
                                            H->p.ppe_max_iter);
+        if (EH->has_mg) mg_apply<R>(EH, st);
         k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 1, 0, 0);
     } else {
         k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
@@ -841,6 +875,30 @@ static int commit_t(SphdemHandle* H) {
             K.part = A.get<double>((size_t)KRY_NPART * KRY_G);
             K.sc = A.get<double>(KS_COUNT);
             if (!A.ok) return SPHDEM_E_NOMEM;
+            if (p.ppe_precond == SPHDEM_PRECOND_TWO_LEVEL) {
+                // cell grid, then 2x2x2 aggregates down to at most MG_CHOL_MAX cells (two levels at least)
+                MgWork& M = EH->mg;
+                int nx = P.NI, ny = P.NJ, nz = P.NK, l = 0;
+                while (true) {
+                    MgLevel& L = M.L[l];
+                    L.nx = nx; L.ny = ny; L.nz = nz; L.n = nx * ny * nz;
+                    L.A = A.get<double>((size_t)32 * L.n);
+                    L.dinv = A.get<double>(L.n);
+                    L.b = A.get<double>(L.n); L.x = A.get<double>(L.n); L.t = A.get<double>(L.n);
+                    l++;
+                    if ((L.n <= MG_CHOL_MAX && l >= 2) || l == MG_MAXLEV) break;
+                    nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
+                }
+                if (M.L[l - 1].n > MG_CHOL_MAX) return SPHDEM_E_UNSUPPORTED;
+                M.nlev = l;
+                M.chol = A.get<double>((size_t)MG_CHOL_MAX * MG_CHOL_MAX);
+                M.key = W.key_out;
+                M.cxyz = A.get<long long>(ns);
+                M.gs = W.g_str;
+                M.ge = W.g_end;
+                if (!A.ok) return SPHDEM_E_NOMEM;
+                EH->has_mg = true;
+            }
             if (p.warm_start == SPHDEM_WARM_MLP || p.warm_start == SPHDEM_WARM_PROJECT) {
                 K.D = A.get<float>((size_t)ns * PROJ_MP);
                 K.hist = A.get<float>((size_t)SPHDEM_WARM_HIST_MAX * ns);
@@ -1593,6 +1651,8 @@ static int check_supported(const SphdemParams* p) {
     if (p->warm_hist < 0 || p->warm_hist > SPHDEM_WARM_HIST_MAX) return SPHDEM_E_ARG;
     if (p->warm_fit & ~(SPHDEM_FIT_RESIDUAL | SPHDEM_FIT_AFFINE)) return SPHDEM_E_ARG;
     if (p->dem_list_cap < 0 || p->dem_list_cap > 4096) return SPHDEM_E_ARG;
+    if (p->ppe_precond != SPHDEM_PRECOND_JACOBI && p->ppe_precond != SPHDEM_PRECOND_TWO_LEVEL) return SPHDEM_E_ARG;
+    if (p->ppe_precond == SPHDEM_PRECOND_TWO_LEVEL && p->ppe_mode != SPHDEM_PPE_PCG) return SPHDEM_E_UNSUPPORTED;
     if (p->warm_start != SPHDEM_WARM_PREVIOUS && p->warm_start != SPHDEM_WARM_MLP &&
         p->warm_start != SPHDEM_WARM_EXTRAPOLATE && p->warm_start != SPHDEM_WARM_PROJECT)
         return SPHDEM_E_ARG;
@@ -1641,6 +1701,7 @@ extern "C" int sphdem_create_from_dir(const char* dir, const SphdemParams* ov, S
         p.warm_fit = ov->warm_fit;
         p.w_lanes = ov->w_lanes;
         p.dem_list_cap = ov->dem_list_cap;
+        p.ppe_precond = ov->ppe_precond;
         p.mlp_train_steps = ov->mlp_train_steps;
         p.mlp_updates = ov->mlp_updates;
         p.mlp_seed = ov->mlp_seed;

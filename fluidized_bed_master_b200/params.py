@@ -18,7 +18,7 @@ _I32 = [
     "penetration_solve", "switch_ptype", "noslip_bc", "decouple_stride",
     "ppe_mode", "warm_start", "ppe_max_iter", "precision", "dem_wall_mask",
     "mlp_train_steps", "mlp_updates", "mlp_seed", "warm_hist", "warm_fit", "w_lanes",
-    "dem_list_cap",
+    "dem_list_cap", "ppe_precond",
 ]
 _F64_A = [
     "kappa", "p_ref", "gamma", "dt", "time", "time_end",
@@ -92,6 +92,7 @@ class SphdemStats(C.Structure):
 
 # PPE modes and warm starts (SPHDEM_PPE_*, SPHDEM_WARM_*)
 PPE_REFERENCE, PPE_KRYLOV, PPE_PCG = 0, 1, 2
+PRECOND_JACOBI, PRECOND_TWO_LEVEL = 0, 1
 WCSPH, ISPH = 0, 1
 WARM_PREVIOUS, WARM_MLP, WARM_EXTRAPOLATE, WARM_PROJECT = 0, 1, 2, 3
 WARM_HIST_MAX = 8

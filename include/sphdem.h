@@ -89,6 +89,14 @@ extern "C" {
 #define SPHDEM_FIT_RESIDUAL     1
 #define SPHDEM_FIT_AFFINE       2
 
+/* ppe_precond (PCG only): the diagonal of the operator, or the diagonal plus
+ * a coarse correction on the NNPS cells (cell aggregates of the solved
+ * particles, Galerkin 27-point operators on the cell grid and on 2x2x2
+ * aggregates of it, one damped-Jacobi V-cycle, the last level by Cholesky).
+ * An engine extension; the reference has no preconditioner. */
+#define SPHDEM_PRECOND_JACOBI 0
+#define SPHDEM_PRECOND_TWO_LEVEL 1
+
 /* Precision of the non-position fields inside the engine. */
 #define SPHDEM_PREC_FP32 0
 #define SPHDEM_PREC_FP64 1
@@ -150,6 +158,7 @@ typedef struct SphdemParams {
     int32_t dem_list_cap;       /* ISPH-DEM: SPH -> DEM list entries per particle; 0 = sized at commit from an
                                    exact count.  A particle with more DEM neighbours walks its stencil instead
                                    (same sums, same order). */
+    int32_t ppe_precond;        /* PCG: SPHDEM_PRECOND_JACOBI (0) or SPHDEM_PRECOND_TWO_LEVEL (1) */
 
     /* -- real switches: vif[] of function_init.cuh:59-100 -- */
     double kappa;               /* vif[0]  */
@@ -298,6 +307,7 @@ int sphdem_create(const SphdemParams* p, int32_t n_sph, int32_t n_dem,
  * (function_init.cuh:216-1182, ISPH.cuh:55-113) and create an engine.
  * ov may be NULL; when given, its non-switch engine extensions
  * (precision, ppe_mode, warm_start, ppe_tol, ppe_max_iter, warm_hist, warm_fit, w_lanes, dem_list_cap,
+ * ppe_precond,
  * mlp_train_steps, mlp_updates, mlp_seed, mlp_lr) override the defaults. */
 int sphdem_create_from_dir(const char* input_dir, const SphdemParams* ov,
                            SphdemHandle** out);
