@@ -449,3 +449,45 @@ def dam_break_batch(n_beds=64, n_min=2_000, n_max=50_000, seed=0, dx=5.0e-3, ref
         if col[1] > hmax:
             hmax, params = col[1], p
     return params, beds
+
+
+GENERATORS = {"spouted_bed": spouted_bed, "box_bed": box_bed, "scaled_box_bed": scaled_box_bed,
+              "isph_column": isph_column, "dam_break_2d": dam_break_2d}
+
+
+def _cli(argv=None):
+    """Write one seeded bed as a reference input directory:
+
+        python -m fluidized_bed_master_b200.beds box_bed --out input --seed 3 --set n_fluid=50000 dx=2e-3
+
+    input.txt, solv.txt and data.txt in the reference's formats, plus
+    params.json with every SphdemParams field (the engine extensions such as
+    ppe_mode are not solv.txt keys; pass them to sphdem_create_from_dir)."""
+    import argparse
+    import ast
+    import json
+
+    ap = argparse.ArgumentParser(prog="python -m fluidized_bed_master_b200.beds", description=_cli.__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("bed", choices=sorted(GENERATORS))
+    ap.add_argument("--out", required=True, help="input directory to write")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--set", nargs="*", default=[], metavar="KEY=VALUE",
+                    help="generator arguments, e.g. n_fluid=50000 dx=2e-3 (Python literals)")
+    a = ap.parse_args(argv)
+    kw = {"seed": a.seed}
+    for item in a.set:
+        k, _, v = item.partition("=")
+        if not k or not _:
+            ap.error(f"--set wants KEY=VALUE, got {item!r}")
+        kw[k] = ast.literal_eval(v)
+    p, sph, dem = GENERATORS[a.bed](**kw)
+    write_input_dir(a.out, p, sph, dem)
+    with open(os.path.join(a.out, "params.json"), "w") as fh:
+        json.dump(p.as_dict(), fh, indent=1)
+    print(f"{a.bed}: {len(sph['x'])} SPH + {len(dem['x']) if dem else 0} DEM -> {a.out}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_cli())
