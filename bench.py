@@ -459,6 +459,23 @@ def run_column(args, world, rank, local, pg):
                "how": "per step: sphdem_set_fields of the particle state from pinned host arrays, sphdem_step, "
                       "sphdem_get_fields back"}
     eng.close()
+    # the same steps with the two-level preconditioner (ppe_precond TWO_LEVEL)
+    two = None
+    if rank == 0:
+        from fluidized_bed_master_b200.params import PRECOND_TWO_LEVEL
+
+        q2 = q.copy()
+        q2.ppe_precond = PRECOND_TWO_LEVEL
+        e2 = Engine(q2, sph, {})
+        s2 = torch.cuda.ExternalStream(e2.stream_ptr())
+        e2.step(args.warmup)
+        it2, t2 = [], 0.0
+        for _ in range(args.steps):
+            t2 += _timed_steps(e2, s2, flush, 1)
+            it2.append(e2.stats()["ppe_iters"])
+        e2.close()
+        two = {"ms_per_step": t2 / args.steps, "value": n * args.steps / (t2 / 1e3), "unit": unit,
+               "ppe_iters_per_step": float(np.mean(it2))}
     check = None
     if rank == 0 and not args.no_cpu:
         # every field of the FP32 build against the FP64 build after 200 steps
@@ -484,6 +501,7 @@ def run_column(args, world, rank, local, pg):
                    "l2": "256 MB buffer written before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "ppe_iters_per_step": float(np.mean(iters)) if iters else None,
+        "two_level": two,
         "fp32_vs_fp64": check, "roofline": None, "cpu_baseline": None, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks,
     }
