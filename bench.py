@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--no-ppe", action="store_true", help="skip the PPE solver comparison")
     ap.add_argument("--ppe-train", type=int, default=80,
                     help="steps before the PPE measurement (the learned warm start trains there)")
+    ap.add_argument("--ppe-precond", default="jacobi", choices=["jacobi", "two-level"],
+                    help="--workload ppe-profile: the PCG preconditioner")
+    ap.add_argument("--profile-bed", default="bench", choices=["bench", "scaled"],
+                    help="--workload ppe-profile: the bench bed or the scaled bed")
     ap.add_argument("--ppe-bed", default="scaled", choices=["scaled", "bench"],
                     help="bed of the PPE comparison: the 2.2 M-particle scaled bed or the bench bed")
     return ap.parse_args()
@@ -319,14 +323,20 @@ def dam2d_cpu(seconds):
 
 
 def run_ppe_profile(args):
-    """A few steps of the bench bed with the PCG PPE (projected start over 8
-    solution changes) and graphs off: the launch sequence a kernel profiler
-    can see (kernels inside conditional graph nodes are hidden from it)."""
-    from fluidized_bed_master_b200.beds import box_bed
+    """A few steps of the bench bed (or, with --profile-bed scaled, the
+    scaled bed) with the PCG PPE (projected start over 8 solution changes;
+    --ppe-precond two-level for the two-level preconditioner) and graphs
+    off: the launch sequence a kernel profiler can see (kernels inside
+    conditional graph nodes are hidden from it)."""
+    from fluidized_bed_master_b200.beds import box_bed, scaled_box_bed
     from fluidized_bed_master_b200.engine import Engine
-    from fluidized_bed_master_b200.params import PPE_PCG, WARM_PROJECT
+    from fluidized_bed_master_b200.params import PPE_PCG, PRECOND_TWO_LEVEL, WARM_PROJECT
 
-    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    if args.profile_bed == "scaled":
+        p, sph, dem = scaled_box_bed(seed=0)
+    else:
+        p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    p.ppe_precond = PRECOND_TWO_LEVEL if args.ppe_precond == "two-level" else 0
     p.precision = 0
     p.ppe_mode = PPE_PCG
     p.kgc_solve = 0
