@@ -897,7 +897,8 @@ def run_engine(args, world, rank, local, pg):
 def ppe_comparison(args):
     """PPE ms/step and iterations at a relative residual of 1e-6 on the same
     bed, for four initial iterates of the same Jacobi-PCG (and three of them
-    again with the two-level preconditioner, arms *_two_level):
+    again with the two-level preconditioner, arms *_two_level; *_hist2 with
+    2 solution changes instead of 8):
       plain        the previous pressure;
       extrapolated the previous pressure plus its last change;
       projected    the Galerkin projection onto {previous pressure, its
@@ -928,10 +929,13 @@ def ppe_comparison(args):
     out = {"solver": "Jacobi-PCG, Chronopoulos-Gear form, mass-weighted inner products (FP64 vectors and dots, "
                      "FP32 operator)", "tol": 1e-6, "kgc": 0, "bed": bed, "n_sph": len(sph["x"]),
            "n_dem": len(dem["x"]), "steps_before": args.ppe_train, "measured_steps": meas, "warm_hist": 8}
-    arms = (("plain", 0, 0), ("extrapolated", WARM_EXTRAPOLATE, 0), ("projected", WARM_PROJECT, 0),
-            ("learned", WARM_MLP, 0), ("plain_two_level", 0, PRECOND_TWO_LEVEL),
-            ("projected_two_level", WARM_PROJECT, PRECOND_TWO_LEVEL), ("learned_two_level", WARM_MLP, PRECOND_TWO_LEVEL))
-    for name, warm, precond in arms:
+    arms = (("plain", 0, 0, 8), ("extrapolated", WARM_EXTRAPOLATE, 0, 8), ("projected", WARM_PROJECT, 0, 8),
+            ("learned", WARM_MLP, 0, 8), ("plain_two_level", 0, PRECOND_TWO_LEVEL, 8),
+            ("projected_two_level", WARM_PROJECT, PRECOND_TWO_LEVEL, 8),
+            ("learned_two_level", WARM_MLP, PRECOND_TWO_LEVEL, 8),
+            ("projected_two_level_hist2", WARM_PROJECT, PRECOND_TWO_LEVEL, 2),
+            ("learned_two_level_hist2", WARM_MLP, PRECOND_TWO_LEVEL, 2))
+    for name, warm, precond, hist in arms:
         q = p.copy()
         q.precision = 0
         q.ppe_mode = PPE_PCG
@@ -939,7 +943,7 @@ def ppe_comparison(args):
         q.ppe_tol = 1e-6
         q.ppe_max_iter = 2000
         q.warm_start = warm
-        q.warm_hist = 8
+        q.warm_hist = hist
         q.warm_fit = 0
         q.mlp_train_steps = args.ppe_train
         q.ppe_precond = precond
@@ -968,6 +972,8 @@ def ppe_comparison(args):
     out["two_level_speedup_plain"] = out["plain"]["ppe_ms_per_step"] / out["plain_two_level"]["ppe_ms_per_step"]
     out["learned_two_level_speedup_vs_plain"] = (out["plain"]["ppe_ms_per_step"] /
                                                  out["learned_two_level"]["ppe_ms_per_step"])
+    out["learned_two_level_hist2_speedup_vs_plain"] = (out["plain"]["ppe_ms_per_step"] /
+                                                       out["learned_two_level_hist2"]["ppe_ms_per_step"])
     return out
 
 

@@ -363,11 +363,15 @@ static int project_initial(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, i
     KryWork<R>& K = EH->K;
     int n = EH->E.P.ns;
     cudaStream_t st = H->stream;
-    k_proj_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, S.pid, std::min(std::max(H->p.warm_hist, 0),
-                                                                          SPHDEM_WARM_HIST_MAX), use_mlp);
+    const int nhist = std::min(std::max(H->p.warm_hist, 0), SPHDEM_WARM_HIST_MAX);
+    k_proj_dirs<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, S.pid, nhist, use_mlp);
     int fit = H->p.warm_fit | (cg ? 0 : SPHDEM_FIT_RESIDUAL);   // BiCGStab: the residual norm
     int pb = std::min(KRY_G, std::max(1, (n + PROJ_T - 1) / PROJ_T));
-    k_proj_spmv<R><<<pb, PROJ_T, 0, st>>>(n, K, fit);
+    switch (proj_groups(nhist)) {
+    case 1: k_proj_spmv<R, 1><<<pb, PROJ_T, 0, st>>>(n, K, fit); break;
+    case 2: k_proj_spmv<R, 2><<<pb, PROJ_T, 0, st>>>(n, K, fit); break;
+    default: k_proj_spmv<R, 3><<<pb, PROJ_T, 0, st>>>(n, K, fit); break;
+    }
     k_proj_solve<R><<<1, KRY_T, 0, st>>>(K, pb);
     k_proj_apply<R><<<nblocks(n, 256), 256, 0, st>>>(n, K, fit);
     CK(cudaGetLastError());

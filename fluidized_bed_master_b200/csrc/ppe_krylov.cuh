@@ -763,8 +763,12 @@ __global__ void k_proj_dirs(int n, KryWork<R> K, const int* __restrict__ pid, in
 // and the block partials of G (upper triangle) and h.  Each thread stages
 // its row's products in shared memory; then thread v < PROJ_NV forms value
 // v over the block's rows in row order: deterministic, no shuffles.
+// G = the float4 groups of D that can be non-zero (slots 0..4G-1): with
+// fewer history directions the pass gathers fewer direction bytes per
+// neighbour; the slots above are zero, so their products are zero anyway.
 constexpr int PROJ_T = 128;
-template <typename R>
+__host__ __device__ constexpr int proj_groups(int nhist) { return (1 + nhist) / 4 + 1 < 3 ? (1 + nhist) / 4 + 1 : 3; }
+template <typename R, int G = 3>
 __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int fit) {
     using E = KEnt<R>;
     const bool least_squares = fit & SPHDEM_FIT_RESIDUAL, affine = fit & SPHDEM_FIT_AFFINE;
@@ -786,7 +790,9 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
         for (int q = 0; q < PROJ_MAX; q++) ad[q] = dv[q] = 0.0;
         int cnt = i < n ? K.kcnt[i] : 0;
         if (cnt) {
-            float4 a0 = D4[(size_t)i * 3], a1 = D4[(size_t)i * 3 + 1], a2 = D4[(size_t)i * 3 + 2];
+            const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 a0 = D4[(size_t)i * 3], a1 = G > 1 ? D4[(size_t)i * 3 + 1] : z4,
+                   a2 = G > 2 ? D4[(size_t)i * 3 + 2] : z4;
             float di[PROJ_MP] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
             const double dg = K.d[i];
 #pragma unroll
@@ -805,10 +811,10 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
                 double a0, a1;
                 E::get(__ldg(er + (size_t)k * 32), j0, a0);
                 E::get(__ldg(er + (size_t)(k + 1) * 32), j1, a1);
-                float4 p0 = __ldg(D4 + (size_t)j0 * 3), p1 = __ldg(D4 + (size_t)j0 * 3 + 1),
-                       p2 = __ldg(D4 + (size_t)j0 * 3 + 2);
-                float4 q0 = __ldg(D4 + (size_t)j1 * 3), q1 = __ldg(D4 + (size_t)j1 * 3 + 1),
-                       q2 = __ldg(D4 + (size_t)j1 * 3 + 2);
+                float4 p0 = __ldg(D4 + (size_t)j0 * 3), p1 = G > 1 ? __ldg(D4 + (size_t)j0 * 3 + 1) : z4,
+                       p2 = G > 2 ? __ldg(D4 + (size_t)j0 * 3 + 2) : z4;
+                float4 q0 = __ldg(D4 + (size_t)j1 * 3), q1 = G > 1 ? __ldg(D4 + (size_t)j1 * 3 + 1) : z4,
+                       q2 = G > 2 ? __ldg(D4 + (size_t)j1 * 3 + 2) : z4;
                 const double x0j = __ldg(xp + j0), x1j = __ldg(xp + j1);
                 float d0[PROJ_MP] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w, p2.x, p2.y, p2.z, p2.w};
                 float d1[PROJ_MP] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
@@ -823,7 +829,8 @@ __global__ void __launch_bounds__(PROJ_T) k_proj_spmv(int n, KryWork<R> K, int f
                 int j;
                 double a;
                 E::get(__ldg(er + (size_t)k * 32), j, a);
-                float4 b0 = __ldg(D4 + (size_t)j * 3), b1 = __ldg(D4 + (size_t)j * 3 + 1), b2 = __ldg(D4 + (size_t)j * 3 + 2);
+                float4 b0 = __ldg(D4 + (size_t)j * 3), b1 = G > 1 ? __ldg(D4 + (size_t)j * 3 + 1) : z4,
+                       b2 = G > 2 ? __ldg(D4 + (size_t)j * 3 + 2) : z4;
                 float dj[PROJ_MP] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
                 ad[0] -= a * __ldg(xp + j);
 #pragma unroll
