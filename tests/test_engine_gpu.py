@@ -299,3 +299,51 @@ def test_history_roundtrip_keeps_the_run(contact_bed):
     b.step(3)
     for f in ("x", "uz", "wx"):
         assert np.array_equal(a.get(DEM, f), b.get(DEM, f)), f
+
+
+@pytest.mark.parametrize("case", ["column", "bed"])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_clamped_particle_takes_the_exact_path(case, prec):
+    """The last input row does not enter the bounding box (the reference's
+    box skips it), so a last row placed three cells beyond the box is
+    clamped into a boundary cell.  The cell-tiled scans (list build, wall
+    Neumann pass, SPH -> DEM list) stage coordinates relative to a particle
+    of the cell and use the FP32 prefilter only for positions within two
+    cell widths of it; this one must take the FP64 predicate.  Bar: sorted
+    order, cell keys and neighbour lists bit-exact against the oracle over
+    two steps; the FP64 build's SPH fields within rel. L2 1e-9 (a sphere
+    that far has no fluid around it, and the reference's drag closure
+    turns its own state non-finite, in the oracle and the engine alike)."""
+    from fluidized_bed_master_b200.beds import box_bed, isph_column
+
+    if case == "column":
+        # the last row is a wall particle of the closed box
+        p, sph, dem = isph_column(dx=1.0e-2, seed=9)
+        p.ppe_mode = 0
+        sph = {k: np.array(v, copy=True) for k, v in sph.items()}
+        dcell = 1.1 * p.kappa * sph["h"][0]
+        sph["x"][-1] = sph["x"][:-1].max() + 3.0 * dcell
+    else:
+        # spheres inside the fluid layer; the last row is a sphere
+        p, sph, dem = box_bed(n_fluid=8000, n_dem=300, dem_height=0.006, seed=9)
+        dem = {k: np.array(v, copy=True) for k, v in dem.items()}
+        dcell = 1.1 * p.kappa * sph["h"][0]
+        dem["x"][-1] = max(sph["x"].max(), dem["x"][:-1].max()) + 3.0 * dcell
+    eng = _engine(p, sph, dem, prec)
+    orc = Oracle(p, sph, dem, threads=8)
+    for _ in range(2):
+        eng.step(1)
+        orc.step(1)
+        for which in (SPH, DEM):
+            if (eng.nd if which == DEM else eng.ns) == 0:
+                continue
+            assert np.array_equal(_ids(eng, which), _ids(orc, which)), "sorted order differs"
+            assert np.array_equal(eng.get(which, "cell"), orc.get(which, "cell")), "cell keys differ"
+        ce, le = eng.neighbors()
+        co, lo = orc.neighbors()
+        assert np.array_equal(ce, co), "neighbour counts differ"
+        for i in range(eng.ns):
+            assert np.array_equal(le[i, : ce[i]], lo[i, : co[i]]), f"neighbour list of slot {i} differs"
+    if prec == 1:
+        bad = _compare(eng, orc, SPH_REAL, [], 1e-9, case)
+        assert not bad, bad
