@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(128) k_kry_assemble(DevParams P, SphState<R> S
     const int* __restrict__ nb = W.nbr;
     int k = 0;
     typename KEnt<R>::T* __restrict__ ent = K.e;
-    nb_walk<2, NbQ44<R>>(
+    nb_walk<4, NbQ44<R>>(
         cnt, nb, n, i,
         [&](int j) {
             NbQ44<R> t;
