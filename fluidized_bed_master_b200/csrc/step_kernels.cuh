@@ -285,7 +285,7 @@ __device__ __forceinline__ double rel_band(const DevParams& P, const RelFrame& F
 // Cell-tiled list build (FP32 build).  One warp per cell: the particles of
 // a cell share one stencil, so the warp stages the candidates of the 9 rows
 // once, as FP32 coordinates relative to a particle of the cell, into shared
-// memory (chunks of 256), and every lane -- one particle of the cell --
+// memory (chunks of 128), and every lane -- one particle of the cell --
 // tests them in the same order against its own radius.  All lanes read the
 // same staged candidate (a broadcast) and run in lockstep; a pair costs a
 // few FP32 operations instead of a global load and the fixed-point
@@ -295,7 +295,7 @@ __device__ __forceinline__ double rel_band(const DevParams& P, const RelFrame& F
 // with b from rel_band.  Pairs in the band, or with a position outside the
 // fixed-point range or not near the origin, take the reference predicate in
 // FP64.
-constexpr int LT_WARPS = 4, LT_CH = 256;
+constexpr int LT_WARPS = 4, LT_CH = 128;
 __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P, SphState<float> S,
                                                                       SphRec<float> rec,
                                                                       const int* __restrict__ gs,
