@@ -324,7 +324,7 @@ static void krylov_body(SphdemHandle* H, EngineHost<R>* EH, cudaStream_t st, cud
         // u in z, w in v, s in s
         k_cg_upd<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.z, K.v, K.p, K.s, K.x, K.r, K.sc);
         if (EH->has_mg) mg_apply<R>(EH, st);
-        k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 0, hnd, in_graph);
+        k_cg_spmv<R><<<KRY_GS, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 0, hnd, in_graph);
     } else {
         k_bicg_p<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.r, K.p, K.v, K.y, K.part, K.sc);
         k_kry_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, nb, K.y, K.v, K.rh, KP_RHV, nullptr, 0, 0);
@@ -425,7 +425,7 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
         k_cg_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.z, K.p, K.s, K.sc, H->p.ppe_tol,
                                            H->p.ppe_max_iter);
         if (EH->has_mg) mg_apply<R>(EH, st);
-        k_cg_spmv<R><<<KRY_G, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 1, 0, 0);
+        k_cg_spmv<R><<<KRY_GS, KRY_T, 0, st>>>(n, K, K.z, K.v, K.r, K.b, 1, 0, 0);
     } else {
         k_kry_init<<<KRY_G, KRY_T, 0, st>>>(n, K.d, K.b, K.y, K.r, K.rh, K.p, K.v, K.z, K.part, cg);
         k_kry_init_scalars<<<1, KRY_T, 0, st>>>(K.part, K.sc, H->p.ppe_tol, H->p.ppe_max_iter, cg);

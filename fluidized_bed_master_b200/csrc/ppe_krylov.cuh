@@ -44,6 +44,7 @@
 namespace sphdem {
 
 constexpr int KRY_G = 1184;  // blocks of the vector kernels (8 per SM)
+constexpr int KRY_GS = 444;  // blocks of the CG product: the 3 per SM its registers allow, one wave
 constexpr int KRY_T = 256;
 constexpr int KRY_NPART = 10;
 
