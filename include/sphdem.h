@@ -55,10 +55,13 @@ extern "C" {
 /* PPE solution method.  REFERENCE = one Jacobi sweep per step with the
  * previous pressure as iterate (functions_PPE2.cuh:542-698, 868-878).
  * KRYLOV = Jacobi-preconditioned BiCGStab on the same operator to a
- * relative residual ppe_tol; PCG = Jacobi-preconditioned conjugate
- * gradients (for symmetric operators: no gradient correction, equal
- * masses).  Neither has a reference counterpart; one Jacobi sweep of
- * either operator from the previous pressure is the reference update. */
+ * relative residual ppe_tol; PCG = conjugate gradients in the m-weighted
+ * inner product sum m_i x_i y_i, in which the operator is self-adjoint
+ * without gradient correction (set kgc_solve 0; unequal masses are fine),
+ * preconditioned by its diagonal or, with ppe_precond TWO_LEVEL, by the
+ * diagonal plus a cell-level coarse correction.  Neither has a reference
+ * counterpart; one Jacobi sweep of either operator from the previous
+ * pressure is the reference update. */
 #define SPHDEM_PPE_REFERENCE 0
 #define SPHDEM_PPE_KRYLOV    1
 #define SPHDEM_PPE_PCG       2
