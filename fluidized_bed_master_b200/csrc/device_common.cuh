@@ -359,6 +359,57 @@ __device__ __forceinline__ void for_rows_warp(const DevParams& P, int ic, int jc
     __syncwarp();
 }
 
+// for_rows_warp for a body that needs the whole warp every round (a
+// ballot): every lane calls f(j) once per round of 32 candidates, j = -1
+// where the lane has no candidate.  Lane l still visits candidates l,
+// l+32, ... in order.
+template <typename F>
+__device__ __forceinline__ void for_rows_warp_all(const DevParams& P, int ic, int jc, int kc,
+                                                  const int4* __restrict__ rows, const Cull& C, int* sm, int lane,
+                                                  F f) {
+    int len = 0, lo = 0;
+    if (lane < 9) {
+        int kz = kc + lane / 3 - 1, jy = jc + lane % 3 - 1;
+        if (kz >= 0 && kz <= P.NK - 1 && jy >= 0 && jy <= P.NJ - 1) {
+            double gxm2, gxp2;
+            x_gaps(P, ic, C, gxm2, gxp2);
+            int a, b;
+            if (row_range_cull(P, rows, ic, jy, kz, C, gxm2, gxp2, a, b)) {
+                lo = a;
+                len = b - a;
+            }
+        }
+    }
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane < 9) {
+        sm[lane + 1] = inc;
+        sm[10 + lane] = lo;
+    }
+    if (lane == 0) sm[0] = 0;
+    int tot = __shfl_sync(0xffffffffu, inc, 8);
+    __syncwarp();
+    int r = 0, nxt = sm[1], base = sm[10];
+    for (int t0 = 0; t0 < tot; t0 += 32) {
+        const int t = t0 + lane;
+        int j = -1;
+        if (t < tot) {
+            while (t >= nxt) {
+                r++;
+                nxt = sm[r + 1];
+                base = sm[10 + r] - sm[r];
+            }
+            j = base + t;
+        }
+        f(j);
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

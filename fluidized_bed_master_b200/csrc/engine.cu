@@ -170,6 +170,8 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = A.get<int>(nd); DW.val_out = A.get<int>(nd);
     DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
     DW.rows = A.get<int4>(ncells);
+    DW.nbs = A.get<int>((size_t)nd * DEM_SPH_CAP);
+    DW.ncs = A.get<int>(nd);
 }
 
 int key_bits(int num_cells) {

@@ -76,7 +76,9 @@ struct DemWork {
     int *key_in, *key_out, *val_in, *val_out;
     int *g_str, *g_end;
     int4* rows;
+    int *nbs, *ncs;              // SPH neighbours of each sphere (k_dem_prep): nbs[i*DEM_SPH_CAP+k], exact count
 };
+constexpr int DEM_SPH_CAP = 256;
 
 // device-side status words (checked by the host at sync points)
 struct DevFlags {

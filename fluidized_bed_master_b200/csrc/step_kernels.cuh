@@ -745,10 +745,32 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
     R f1 = 0, f3 = 0, por = 0;
     const Cull cu = make_cull(xi, yi, zi, Rr);
-    for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
-        PosRec<R> qj = ldr(rec.pos + j);
-        int ptj = tag_ptype(qj.w);
-        if (ptj != 1 && ptj != 3) return;
+    // the sphere's SPH neighbours (p_type <= 1000, |x_i - x_j| < kappa h_i,
+    // the add = 0 form that k_dem_coupling uses) into DW.nbs in visit order,
+    // ranked by a ballot per round; the filter sums take their own subset
+    // (p_type 1 or 3, the 1e-20 form)
+    const unsigned lt = (1u << lane) - 1u;
+    int cs = 0;
+    for_rows_warp_all(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
+        bool in = false;
+        int ptj = 0;
+        PosRec<R> qj;
+        if (j >= 0) {
+            qj = ldr(rec.pos + j);
+            ptj = tag_ptype(qj.w);
+            if (ptj <= 1000) {
+                Disp<R> d;
+                R r2;
+                in = test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 0.0, bd, d, r2);
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int pos = cs + __popc(m & lt);
+            if (pos < DEM_SPH_CAP) DW.nbs[(size_t)i * DEM_SPH_CAP + pos] = j;
+        }
+        cs += __popc(m);
+        if (!in || (ptj != 1 && ptj != 3)) return;
         Disp<R> d;
         R r2;
         if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) return;
@@ -759,6 +781,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
         if (ptj == 1) f1 += c;
         else f3 += c;
     });
+    if (lane == 0) DW.ncs[i] = cs;
     for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, [&](int j) {
         if (D.ptype[j] <= 1000) return;
         PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
@@ -1295,8 +1318,7 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         int ic, jc, kc;
         cell_ijk(P, xi, yi, zi, ic, jc, kc);
         R pgc = voli / (mi * ff + (R)1.0e-15);
-        const Cull cu = make_cull(xi, yi, zi, Rr);
-        for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
+        auto pair = [&](int j) {
             PosRec<R> qj = ldr(rec.pos + j);
             int ptj = tag_ptype(qj.w);
             if (ptj > 1000) return;
@@ -1306,7 +1328,17 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
             R r, rinv;
             rdist(r2, r, rinv);
             dc_pair(W, K, ff, fa, pgc, j, ptj, r, a);
-        });
+        };
+        // the neighbours k_dem_prep listed (same positions, same predicate);
+        // a sphere with more than the list holds walks its stencil
+        const int cs = DW.ncs[i];
+        if (cs <= DEM_SPH_CAP) {
+            const int* __restrict__ nbs = DW.nbs + (size_t)i * DEM_SPH_CAP;
+            for (int k = lane; k < cs; k += 32) pair(__ldg(nbs + k));
+        } else {
+            const Cull cu = make_cull(xi, yi, zi, Rr);
+            for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, pair);
+        }
         dc_warp_sum(a);
     }
     if (lane != 0) return;
