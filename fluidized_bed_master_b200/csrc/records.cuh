@@ -218,6 +218,39 @@ __device__ __forceinline__ bool test_pair(const DevParams& P, const int4& a, con
     }
     return __dadd_rn(pair_dist(ax, ay, az, X[j], Y[j], Z[j]), add) < Rr;
 }
+// test_pair for the two forms of the predicate at once: in0 with add = 0,
+// in20 with add = 1e-20 (in20 implies in0); one prefilter, one FP64 distance
+__device__ __forceinline__ void test_pair2(const DevParams& P, const int4& a, const int4& b, double ax, double ay,
+                                           double az, const double* X, const double* Y, const double* Z, int j,
+                                           double Rr, Band bd, Disp<float>& d, float& r2, bool& in0, bool& in20) {
+    if (((a.w | b.w) & TAG_OOR) == 0) {
+        d.dx = (float)(a.x - b.x) * P.q_step[0];
+        d.dy = (float)(a.y - b.y) * P.q_step[1];
+        d.dz = (float)(a.z - b.z) * P.q_step[2];
+        r2 = d.dx * d.dx + d.dy * d.dy + d.dz * d.dz;
+        if (r2 < bd.lo) { in0 = in20 = true; return; }
+        if (r2 > bd.hi) { in0 = in20 = false; return; }
+    } else {
+        d.dx = (float)(ax - X[j]);
+        d.dy = (float)(ay - Y[j]);
+        d.dz = (float)(az - Z[j]);
+        r2 = d.dx * d.dx + d.dy * d.dy + d.dz * d.dz;
+    }
+    const double r = pair_dist(ax, ay, az, X[j], Y[j], Z[j]);
+    in0 = __dadd_rn(r, 0.0) < Rr;
+    in20 = __dadd_rn(r, 1e-20) < Rr;
+}
+__device__ __forceinline__ void test_pair2(const DevParams&, const QPos64&, const QPos64& b, double ax, double ay,
+                                           double az, const double*, const double*, const double*, int, double Rr,
+                                           Band, Disp<double>& d, double& r2, bool& in0, bool& in20) {
+    d.dx = ax - b.x;
+    d.dy = ay - b.y;
+    d.dz = az - b.z;
+    const double r = pair_dist(ax, ay, az, b.x, b.y, b.z);
+    r2 = d.dx * d.dx + d.dy * d.dy + d.dz * d.dz;
+    in0 = __dadd_rn(r, 0.0) < Rr;
+    in20 = __dadd_rn(r, 1e-20) < Rr;
+}
 __device__ __forceinline__ bool test_pair(const DevParams&, const QPos64&, const QPos64& b, double ax, double ay,
                                           double az, const double*, const double*, const double*, int, double Rr,
                                           double add, Band, Disp<double>& d, double& r2) {

@@ -752,17 +752,14 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
     const unsigned lt = (1u << lane) - 1u;
     int cs = 0;
     for_rows_warp_all(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
-        bool in = false;
+        bool in = false, in20 = false;
         int ptj = 0;
-        PosRec<R> qj;
+        Disp<R> d;
+        R r2 = 0;
         if (j >= 0) {
-            qj = ldr(rec.pos + j);
+            const PosRec<R> qj = ldr(rec.pos + j);
             ptj = tag_ptype(qj.w);
-            if (ptj <= 1000) {
-                Disp<R> d;
-                R r2;
-                in = test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 0.0, bd, d, r2);
-            }
+            if (ptj <= 1000) test_pair2(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, bd, d, r2, in, in20);
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
         if (in) {
@@ -770,10 +767,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
             if (pos < DEM_SPH_CAP) DW.nbs[(size_t)i * DEM_SPH_CAP + pos] = j;
         }
         cs += __popc(m);
-        if (!in || (ptj != 1 && ptj != 3)) return;
-        Disp<R> d;
-        R r2;
-        if (!test_pair(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) return;
+        if (!in20 || (ptj != 1 && ptj != 3)) return;
         R r, rinv;
         rdist(r2, r, rinv);
         V2<R> mr = ldr(rec.mr0 + j);
