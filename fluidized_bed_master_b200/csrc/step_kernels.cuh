@@ -1944,17 +1944,24 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     R th = (R)hi;
     Knl<R> K = knl_make<R>(P, th);
     double Rr = P.kappa * hi;
-    float r2l = r2_lo(Rr), r2h = r2_hi(Rr);
+    const Band bd = make_band(P, Rr);
+    const PosRec<R> qp = make_pos<R>(P, xi, yi, zg, 0, 0, 0);   // the mirror point
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zg, ic, jc, kc);
     R hd = (R)P.h_over_dx;
     R trho = 0, tp = 0, tux = 0, tuy = 0, tuz = 0, tt = 0, flt = 0;
     const Cull cu = make_cull(xi, yi, zg, Rr);
+    // the candidate's type and the prefilter from its packed record (one
+    // load); the FP64 predicate only inside the band
     for_rows_warp(P, ic, jc, kc, rows, cu, sm, lane, [&](int j) {
-        if (S.ptype[j] != 1 || S.btype[j] != 0) return;
-        PairT<R> g = pair_test<R>(xi, yi, zg, S.x[j], S.y[j], S.z[j], Rr, 1e-20, r2l, r2h);
-        if (!g.in) return;
-        R wk = kw(K, g.r);
+        const PosRec<R> qj = ldr(W.rec.pos + j);
+        if (tag_ptype(qj.w) != 1 || tag_btype(qj.w) != 0) return;
+        Disp<R> d;
+        R r2;
+        if (!test_pair(P, qp, qj, xi, yi, zg, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) return;
+        R r, rinv;
+        rdist(r2, r, rinv);
+        R wk = kw(K, r);
         R hj = (R)S.h[j];
         R volj = (hj / hd) * (hj / hd) * (hj / hd);
         R vw = volj * wk;
