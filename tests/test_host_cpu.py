@@ -112,3 +112,21 @@ def test_failures_before_the_device():
     assert L.sphdem_get_stats(None, None) == -1
     for code in (0, -1, -2, -3, -4, -5, -6, -7, -8):
         assert L.sphdem_strerror(code)
+
+
+def test_params_dict_roundtrip():
+    """SphdemParams survive as_dict -> JSON -> from_dict (the golden fixtures
+    and the generator's params.json keep parameters by name)."""
+    import json
+
+    from fluidized_bed_master_b200.params import PRECOND_TWO_LEVEL, SphdemParams, reference_params
+
+    p = reference_params()
+    p.ppe_precond = PRECOND_TWO_LEVEL
+    p.dem_list_cap = 40
+    p.margin[3] = 0.125
+    q = SphdemParams.from_dict(json.loads(json.dumps(p.as_dict())))
+    assert bytes(q) == bytes(p)
+    # fields a dictionary does not name stay zero
+    r = SphdemParams.from_dict({"kappa": 2.0})
+    assert r.kappa == 2.0 and r.ppe_precond == 0 and r.dem_list_cap == 0
