@@ -81,3 +81,20 @@ def test_reference_arm_under_torchrun_world2():
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["parallelism"] == "replicas x2"
+
+
+@pytest.mark.timeout(600)
+def test_column_reference_arm():
+    """bench.py --workload column --impl reference: the CPU port on the 3-D
+    ISPH column (PCG to 1e-6) prints one JSON line of the same metric."""
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = "2"
+    cmd = [sys.executable, "bench.py", "--workload", "column", "--impl", "reference", "--steps", "1",
+           "--warmup", "0", "--cpu-seconds", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and "column" in d["metric"]
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
