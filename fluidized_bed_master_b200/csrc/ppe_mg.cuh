@@ -21,10 +21,12 @@
 // V-cycle smooths with one damped-Jacobi sweep before and after the coarse
 // correction (omega = MG_OMEGA), so it is a fixed symmetric operator.
 //
-// Per PCG iteration this adds a restriction over the particles, two passes
-// over the cells, one single-CTA kernel for the levels below the cells,
-// and the prolongation over the particles; per step, the assembly of the
-// cell operator from the stored coefficients and the Galerkin products.
+// Per PCG iteration this adds the m-weighted restriction over the
+// particles, the level-0 residual, one fused restriction-and-residual pass
+// per coarser level, the last level's product with its inverse, one
+// smoothing pass per level on the way up, the last of them fused with the
+// prolongation into z; per step, the assembly of the cell operator from
+// the stored coefficients, the Galerkin products and the inverse.
 // No atomics: every sum has one owner and a fixed order, so a solve is
 // bit-identical run to run.
 #pragma once
