@@ -1138,6 +1138,7 @@ struct WEngineHost {
     int cur = 0;
     WWork<R> W;
     DevFlags* flags = nullptr;
+    double* red_buf = nullptr;    // maxima of sphdem_get_stats (3 doubles)
     void* sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
     int nb_cap = 0;
@@ -1454,6 +1455,7 @@ static int w_commit_t(SphdemHandle* H) {
     W.ncnt = A.get<int>(ns);
     W.nbr = nullptr;
     EH->flags = A.get<DevFlags>(1);
+    EH->red_buf = A.get<double>(4);
     if (!A.ok) return SPHDEM_E_NOMEM;
     {
         size_t b = 0;
@@ -1573,8 +1575,7 @@ static int w_stats_t(SphdemHandle* H, SphdemStats* out) {
     std::memset(out, 0, sizeof(*out));
     cudaStream_t st = H->stream;
     WState<R>& S = EH->S[EH->cur];
-    double* buf = nullptr;
-    CK(cudaMalloc(&buf, sizeof(double) * 4));
+    double* buf = EH->red_buf;
     CK(cudaMemsetAsync(buf, 0, sizeof(double) * 3, st));
     k_stats<R, double><<<std::min(nblocks(EH->P.ns, 256), 592), 256, 0, st>>>(EH->P.ns, S.rho, S.ux, S.uy, nullptr, EH->W.ftot,
                                                                      S.ptype, S.itype, buf, EH->flags);
@@ -1583,7 +1584,6 @@ static int w_stats_t(SphdemHandle* H, SphdemStats* out) {
     DevFlags f;
     CK(cudaMemcpyAsync(&f, EH->flags, sizeof(f), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    cudaFree(buf);
     out->rho_max_sph = hb[0];
     out->u_max_sph = hb[1];
     out->ftotal_max_sph = hb[2];

@@ -5,10 +5,11 @@
 // but it never allocates device memory: its scratch (unsorted keys, slot
 // indices and the radix-sort workspace) lives in one file-scope
 // __device__ array of SPHDEM_STATIC_SCRATCH_BYTES.  It exists for callers
-// that must not allocate once their time loop runs -- a host code that
-// captures its time step into a CUDA graph (cudaMalloc is not allowed while
-// a stream is being captured), or a host application that hands all device
-// memory out of its own pool and forbids allocations after start-up.
+// that must not allocate once their time loop runs: a host application that
+// hands all device memory out of its own pool and forbids allocations after
+// start-up (its footprint is fixed when the run starts), or a coupled solver
+// whose other streams must not stall, since cudaMalloc and cudaFree may
+// synchronise the whole device.
 //
 // Every GPU that loads the library holds the array until the process exits.
 // All calls on a device share it, so calls that overlap on the GPU (two
@@ -26,6 +27,9 @@ namespace {
 
 constexpr size_t kScratchBytes = SPHDEM_STATIC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
+// the two key/slot arrays of the largest call must leave room for the sort's workspace
+static_assert(2 * (((size_t)SPHDEM_STATIC_MAX_PARTICLES * sizeof(int) + 255) & ~(size_t)255) < kScratchBytes,
+              "SPHDEM_STATIC_MAX_PARTICLES does not fit SPHDEM_STATIC_SCRATCH_BYTES");
 
 __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
@@ -93,6 +97,7 @@ extern "C" int sphdem_sort_cells_static(const double* x, const double* y, const 
     int* key_in = (int*)base;
     int* val_in = (int*)((char*)base + kbytes);
     void* tmp = (char*)base + 2 * kbytes;
+    if (2 * kbytes >= kScratchBytes) return SPHDEM_E_NOMEM;
     size_t tmp_cap = kScratchBytes - 2 * kbytes;
     int bits = 1;
     while ((1ll << bits) <= ncells) bits++;

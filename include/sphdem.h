@@ -445,16 +445,19 @@ int sphdem_params_size(void);
 
 /* Allocation-free cell sort.  No counterpart in the reference: an extra
  * entry point for callers that cannot allocate device memory once their
- * time loop runs (a host code capturing its step into a CUDA graph, where
- * cudaMalloc is not allowed during capture, or an application that hands
- * out all device memory from its own pool).  It does the engine's NNPS
+ * time loop runs (an application that hands out all device memory from its
+ * own pool and fixes its footprint at start-up, or a coupled solver whose
+ * other streams must not stall on the device-wide synchronisation that
+ * cudaMalloc/cudaFree may imply).  It does the engine's NNPS
  * step on caller-owned device arrays: cell key of every particle
  * (functions_NNPS.cuh:762-821), stable sort by cell, cell start/end
  * (functions_NNPS.cuh:670-730).  Inputs: x, y, z (n doubles, device), the
  * grid bbox[6] = xmin,xmax,ymin,ymax,zmin,zmax and nijk[3] = NI,NJ,NK on the
  * host.  Outputs (device, caller-allocated): perm[n] (input index of each
  * sorted slot), cell_key[n] (sorted cell keys), cell_start/cell_end
- * [NI*NJ*NK] (-1 start for an empty cell).  Work is enqueued on stream.
+ * [NI*NJ*NK] (-1 start for an empty cell; cell_end of an empty cell is
+ * not written and keeps what the caller's array held).  Work is enqueued
+ * on stream.
  * Its scratch is a file-scope __device__ array of
  * SPHDEM_STATIC_SCRATCH_BYTES that every GPU loading the library keeps
  * until exit; n above SPHDEM_STATIC_MAX_PARTICLES returns SPHDEM_E_NOMEM.

@@ -13,6 +13,10 @@ import numpy as np
 from fluidized_bed_master_b200.params import DEM, F, INT_FIELDS, SPH, SphdemParams
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference sources lie on a machine that has them (the fixture and
+# reference-build recipes read them there).  The one place this path is named
+# besides oracle/Makefile's default.
+REFERENCE_DIR = os.environ.get("SPHDEM_REFERENCE_DIR", "/root/reference")
 LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 

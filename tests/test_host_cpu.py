@@ -13,6 +13,7 @@ import pytest
 from fluidized_bed_master_b200 import beds
 from fluidized_bed_master_b200.engine import SphdemError, default_params, lib, read_input_txt, read_solv
 from fluidized_bed_master_b200.params import SphdemParams, reference_params
+from oracle import REFERENCE_DIR
 
 HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "sphdem.h")
 
@@ -61,9 +62,10 @@ def test_solv_roundtrip():
     assert q.margin[4] == 0.25
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/input/solv.txt"), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE_DIR, "input", "solv.txt")),
+                    reason="reference tree not present")
 def test_parses_reference_solv():
-    q = read_solv("/root/reference/input/solv.txt")
+    q = read_solv(os.path.join(REFERENCE_DIR, "input", "solv.txt"))
     assert q.solver_type == 1 and q.dim == 3 and q.kernel_type == 5 and q.kgc_solve == 1
     assert q.delSPH_solve == 2 and q.xsph_solve == 1 and q.open_boundary == 1 and q.con_solve == 0
     assert q.dt == 5.0e-7 and q.kappa == 2.0 and q.freq_filt == 40 and q.u_limit == 40.0 and q.c_xsph == 0.1

@@ -1,8 +1,10 @@
 """The allocation-free cell sort (sphdem_sort_cells_static).
 
-Some callers cannot allocate device memory inside their time loop -- a
-host code that captures its step into a CUDA graph, or one that owns all
-device memory through its own pool -- so the library offers one entry
+Some callers cannot allocate device memory inside their time loop -- an
+application that owns all device memory through its own pool and fixes its
+footprint at start-up, or a coupled solver whose other streams must not
+stall on the device-wide synchronisation that cudaMalloc/cudaFree may
+imply -- so the library offers one entry
 point whose scratch is a file-scope device array instead of cudaMalloc.
 This test calls it through the C ABI on device arrays the test owns and
 checks, on consecutive calls, that it returns the same sorted order and
