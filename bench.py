@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="reference arm: skip the reference CUDA build")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP64-build and FP32-vs-FP64 keys")
     ap.add_argument("--no-ppe", action="store_true", help="skip the PPE solver comparison")
     ap.add_argument("--ppe-train", type=int, default=80,
                     help="steps before the PPE measurement (the learned warm start trains there)")
@@ -228,7 +230,105 @@ def load_peaks():
 # ---------------------------------------------------------------------------
 # CPU reference (oracle port of the reference step)
 # ---------------------------------------------------------------------------
+class RefHarness:
+    """A build of oracle/ref_harness.cu (the reference's own sources): the
+    CUDA build (oracle/_ref/libsophia_ref.so) or the host build of the same
+    kernels, looped with OpenMP over the CPU cores (libsophia_ref_host.so).
+    It is loaded with one bed written in the reference's input formats and
+    stepped with SOPHIA_single_ISPH's launch sequence without the three
+    hard-wired DEM wall kernels (ref_run_without_dem_walls).  The bed runs
+    with its open boundary off: the reference hard-wires its inlet/outlet
+    slabs to its own spouted geometry.  The reference keeps its state in
+    globals, so a process loads one bed per build."""
+
+    def __init__(self, kind, p, sph, dem):
+        import ctypes as C
+        import tempfile
+
+        from fluidized_bed_master_b200.beds import write_input_dir
+
+        name = "libsophia_ref.so" if kind == "cuda" else "libsophia_ref_host.so"
+        path = os.path.join(ROOT, "oracle", "_ref", name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle/_ref/{name} was not built (needs the reference sources)")
+        q = p.copy()
+        q.open_boundary = 0
+        q.freq_output = 1 << 30
+        work = tempfile.mkdtemp(prefix="ref_")
+        write_input_dir(os.path.join(work, "input"), q, sph, dem)
+        os.makedirs(os.path.join(work, "plotdata"), exist_ok=True)
+        L = C.CDLL(path)
+        L.ref_load.argtypes = [C.c_char_p]
+        L.ref_run_without_dem_walls.argtypes = [C.c_int]
+        L.ref_last_ms.restype = C.c_double
+        L.ref_counts.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        cwd = os.getcwd()
+        try:
+            rc = L.ref_load(work.encode())
+        finally:
+            os.chdir(cwd)
+        if rc != 0:
+            raise RuntimeError(f"ref_load returned {rc}")
+        ns, nd = C.c_int(), C.c_int()
+        nijk = (C.c_int * 3)()
+        L.ref_counts(C.byref(ns), C.byref(nd), nijk)
+        self.L, self.work, self.ns, self.nd = L, work, ns.value, nd.value
+
+    def run(self, nsteps):
+        """nsteps steps; returns their wall-clock ms (device sync at both ends)."""
+        cwd = os.getcwd()
+        try:
+            os.chdir(self.work)
+            rc = self.L.ref_run_without_dem_walls(nsteps)
+        finally:
+            os.chdir(cwd)
+        if rc != 0:
+            raise RuntimeError(f"ref_run_without_dem_walls returned {rc}")
+        return self.L.ref_last_ms()
+
+
+def omp_threads():
+    """Threads an OpenMP CPU leg uses: OMP_NUM_THREADS when set, else every core."""
+    try:
+        return int(os.environ["OMP_NUM_THREADS"])
+    except (KeyError, ValueError):
+        return os.cpu_count() or 1
+
+
+HOST_REF_TEXT = ("the reference's own kernel bodies (its sources host-compiled with g++ -O2 -fopenmp, oracle/Makefile "
+                 "refhost), FP64 AoS, blocks spread over the OpenMP threads, SOPHIA_single_ISPH's launch sequence "
+                 "without the 3 hard-wired DEM wall kernels, open boundary off")
+
+
 def cpu_reference(seconds=None, warmup=1, steps=None):
+    """The CPU baseline on a bounded sample of the bench bed (a quarter-height
+    slice with the same lattice and sphere density): the host build of the
+    reference's kernels when it was built, else the oracle port."""
+    from fluidized_bed_master_b200.beds import box_bed
+
+    p, sph, dem = box_bed(**SAMPLE)
+    threads = omp_threads()
+    try:
+        ref = RefHarness("host", p, sph, dem)
+    except FileNotFoundError:
+        return cpu_port(seconds, warmup, steps)
+    n = ref.ns + ref.nd
+    ref.run(warmup)
+    ms, k = 0.0, 0
+    while True:
+        ms += ref.run(1)
+        k += 1
+        if steps is not None and k >= steps:
+            break
+        if steps is None and (ms / 1e3 >= seconds or k >= 200):
+            break
+    sample = (f"box bed slice: {ref.ns} SPH + {ref.nd} DEM (n_fluid=50000, n_dem=5000, same dx and sphere "
+              f"density), {k} steps after {warmup} warm-up; {HOST_REF_TEXT}")
+    return n * k / (ms / 1e3), threads, sample, ms / 1e3 / k, "reference"
+
+
+def cpu_port(seconds=None, warmup=1, steps=None):
+    """The oracle port of the reference step on the same slice (all host threads)."""
     from fluidized_bed_master_b200.beds import box_bed
     from oracle import Oracle
 
@@ -249,8 +349,65 @@ def cpu_reference(seconds=None, warmup=1, steps=None):
             break
     el = time.perf_counter() - t0
     sample = (f"box bed slice: {orc.ns} SPH + {orc.nd} DEM (n_fluid=50000, n_dem=5000, same dx and sphere "
-              f"density), {k} steps after {warmup} warm-up")
-    return n * k / el, threads, sample, el / k
+              f"density), {k} steps after {warmup} warm-up; the oracle's FP64 port of the reference step")
+    return n * k / el, threads, sample, el / k, "port"
+
+
+def cpu_reference_full(warmup, steps):
+    """The host build of the reference's kernels on the whole bench bed (all
+    host threads): particle-updates/s, threads, sample text, s/step, kind."""
+    from fluidized_bed_master_b200.beds import box_bed
+
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    threads = omp_threads()
+    ref = RefHarness("host", p, sph, dem)
+    n = ref.ns + ref.nd
+    ref.run(warmup)
+    ms = ref.run(steps)
+    sample = (f"the whole bench bed ({ref.ns} SPH + {ref.nd} DEM), {steps} steps after {warmup} warm-up, "
+              f"{threads} threads; {HOST_REF_TEXT}")
+    return n * steps / (ms / 1e3), threads, sample, ms / 1e3 / steps, "reference"
+
+
+def cpu_reference_full_port(warmup, steps):
+    """The oracle port on the whole bench bed (when the reference was not built)."""
+    from fluidized_bed_master_b200.beds import box_bed
+    from oracle import Oracle
+
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    threads = os.cpu_count() or 1
+    orc = Oracle(p, sph, dem, threads=threads)
+    n = orc.ns + orc.nd
+    orc.step(warmup)
+    t0 = time.perf_counter()
+    orc.step(steps)
+    el = time.perf_counter() - t0
+    sample = (f"the whole bench bed ({orc.ns} SPH + {orc.nd} DEM), {steps} steps after {warmup} warm-up, "
+              f"{threads} threads; the oracle's FP64 port of the reference step")
+    return n * steps / el, threads, sample, el / steps
+
+
+def reference_cuda(warmup, steps):
+    """The reference's own CUDA kernels (oracle/_ref/libsophia_ref.so, built
+    from the unmodified reference sources with its nvcc flags for sm_100a) on
+    this GPU, on the bench bed's particle set (RefHarness), with the
+    reference's hard-wired material constants.  Wall clock around the step
+    loop with a device sync at both ends, as the reference's time loop runs."""
+    from fluidized_bed_master_b200.beds import box_bed
+
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    try:
+        ref = RefHarness("cuda", p, sph, dem)
+        ref.run(warmup)
+        ms = ref.run(steps) / steps
+    except (FileNotFoundError, RuntimeError) as e:
+        return {"unavailable": str(e)}
+    n = ref.ns + ref.nd
+    return {"value": n / (ms / 1e3), "unit": "particle-updates/s", "ms_per_step": ms, "n_sph": ref.ns,
+            "n_dem": ref.nd, "steps": steps, "warmup": warmup, "dtype": "f64",
+            "how": "reference CUDA build (sm_100a, the reference's nvcc flags), SOPHIA_single_ISPH launch "
+                   "sequence without the 3 hard-wired DEM wall kernels, open boundary off, the reference's "
+                   "hard-wired materials; wall clock around the step loop, device sync at both ends"}
 
 
 def run_reference(args, world, rank):
@@ -260,17 +417,23 @@ def run_reference(args, world, rank):
 
     _, sph_full, dem_full = box_bed(seed=0, **WORKLOAD)
     config = bench_config(len(sph_full["x"]), len(dem_full["x"]), world, "f64")
-    val, cores, sample, s_per_step = cpu_reference(warmup=args.warmup, steps=args.steps)
+    try:
+        val, cores, sample, s_per_step, kind = cpu_reference_full(args.warmup, args.steps)
+    except FileNotFoundError:
+        val, cores, sample, s_per_step = cpu_reference_full_port(args.warmup, args.steps)
+        kind = "port"
     unit = "particle-updates/s"
     line = {
         "metric": "SPH-DEM particle-updates/s on 1 B200 (3-D fluidized bed, ISPH-DEM step)",
         "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded box bed; bounded slice per step)",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded box bed, the whole bed every step)",
         "config": config,
-        "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_cuda:
+        line["reference_cuda"] = reference_cuda(args.warmup, args.steps)
     print(json.dumps(line), flush=True)
 
 
@@ -865,11 +1028,14 @@ def run_engine(args, world, rank, local, pg):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, sample, _ = cpu_reference(seconds=args.cpu_seconds)
-        cpu = {"value": v, "unit": "particle-updates/s", "cores": cores, "kind": "port", "sample": sample}
+        v, cores, sample, _, kind = cpu_reference(seconds=args.cpu_seconds)
+        cpu = {"value": v, "unit": "particle-updates/s", "cores": cores, "kind": kind, "sample": sample}
 
     stats = eng.stats()
     eng.close()
+    fp64, fp32_vs_fp64 = None, None
+    if rank == 0 and world == 1 and not args.no_precision and r == 4:
+        fp64, fp32_vs_fp64 = precision_keys(args, rank)
     ppe = None
     if rank == 0 and world == 1 and not args.no_ppe:
         ppe = ppe_comparison(args)
@@ -888,10 +1054,81 @@ def run_engine(args, world, rank, local, pg):
         "clocks": clocks,
         "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "u_max_dem", "overflow_flags", "nan_flag")},
         "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
+        "fp64_build": fp64,
+        "fp32_vs_fp64": fp32_vs_fp64,
         "ppe": ppe,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+PREC_SPH = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor", "dDEMpor", "flt_s", "ftotalx",
+            "ftotaly", "ftotalz", "fpx", "fpy", "fpz", "pgfx", "pgfy", "pgfz", "rho_ref", "dtemp"]
+PREC_DEM = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "DEMpor", "flt_sd", "flt_sd2", "Fdx_df",
+            "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz", "dtemp", "Q_sd"]
+PREC_STEPS = 100
+
+
+def precision_keys(args, seed):
+    """The FP64 build of the same kernels on the bench bed: its throughput
+    (same protocol as the headline: warm-up, L2 flush and CUDA events per
+    step) and, after PREC_STEPS steps from the same input, every field of
+    the FP32 build against it (rel. L2 per field, matched by particle id)."""
+    import torch
+
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import DEM, SPH
+
+    p, sph, dem = box_bed(seed=seed, **WORKLOAD)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    q = p.copy()
+    q.precision = 1
+    e64 = Engine(q, sph, dem)
+    stream = torch.cuda.ExternalStream(e64.stream_ptr())
+    e64.step(args.warmup)
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        e64.step(1)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    n = e64.ns + e64.nd
+    fp64 = {"value": n * args.steps / (total / 1e3), "unit": "particle-updates/s", "ms_per_step": total / args.steps,
+            "dtype": "f64", "how": "FP64 build of the same kernels (positions and every field FP64), same bed, "
+                                   "warm-up, L2 flush and CUDA events as the headline"}
+    e64.close()
+    q32 = p.copy()
+    q32.precision = 0
+    e32 = Engine(q32, sph, dem)
+    e64 = Engine(q, sph, dem)
+    e32.step(PREC_STEPS)
+    e64.step(PREC_STEPS)
+
+    def rel(a, b):
+        den = np.linalg.norm(b)
+        return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+    err = {}
+    for which, fields, idn in ((SPH, PREC_SPH, "pid"), (DEM, PREC_DEM, "dem_idx")):
+        o32 = np.argsort(e32.get(which, idn))
+        o64 = np.argsort(e64.get(which, idn))
+        for f in fields:
+            err[("dem." if which else "sph.") + f] = rel(e32.get(which, f)[o32], e64.get(which, f)[o64])
+    e32.close()
+    e64.close()
+    worst = max(err, key=err.get)
+    cmp = {"steps": PREC_STEPS, "rel_l2": err, "worst_field": worst, "worst": err[worst],
+           "how": "FP32 build (FP32 fields, FP64 positions) vs the FP64 build of the same kernels, same input, "
+                  f"after {PREC_STEPS} steps, rel. L2 per field matched by particle id"}
+    return fp64, cmp
 
 
 def ppe_comparison(args):

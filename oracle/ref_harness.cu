@@ -262,6 +262,129 @@ extern "C" int ref_run(int nsteps) {
     return 0;
 }
 
+// SOPHIA_single_ISPH (ISPH_Calc_seperate.cuh:44-466) for decouple_stride 1,
+// launch for launch, without the three DEM wall kernels (KERNEL_treat_DEM_
+// {cylinder_z,box_z,truncated_cone_z}_dem), whose wall geometry the
+// reference hard-wires (functions_DEM_BC.cuh): beds of another shape (the
+// box bed) are timed with it.  The VTK output branch is left out as well
+// (freq_output is set beyond the run).  Each step ends with a device sync,
+// as the reference's does.
+static void isph_step_without_dem_walls() {
+    dim3 b, t;
+    t.x = 128;
+    int s = sizeof(int) * (t.x + 1);
+    const int bs = (num_part2_sph - 1) / t.x + 1, bd = (num_part2_dem - 1) / t.x + 1;
+    b.x = bs; KERNEL_set_alpha_sph<<<b, t>>>(dP1s);
+    b.x = bd; KERNEL_set_alpha_dem<<<b, t>>>(dP1d);
+    cudaDeviceSynchronize();
+    cudaMemset(g_str_sph, cu_memset, sizeof(int_t) * num_cells);
+    cudaMemset(g_str_dem, cu_memset, sizeof(int_t) * num_cells);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_index_particle_to_cell_sph<<<b, t>>>(g_idx_sph_in, p_idx_sph_in, dP1s);
+    b.x = bd; KERNEL_index_particle_to_cell_dem<<<b, t>>>(g_idx_dem_in, p_idx_dem_in, dP1d);
+    cudaDeviceSynchronize();
+    cub::DeviceRadixSort::SortPairs(st_sph, sb_sph, g_idx_sph_in, g_idx_sph, p_idx_sph_in, p_idx_sph, num_part2_sph);
+    cub::DeviceRadixSort::SortPairs(st_dem, sb_dem, g_idx_dem_in, g_idx_dem, p_idx_dem_in, p_idx_dem, num_part2_dem);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_reorder_sph<<<b, t, s>>>(g_idx_sph, p_idx_sph, g_str_sph, g_end_sph, dP1s, dP2s, dSP1s, dSP2s);
+    b.x = bd; KERNEL_reorder_dem<<<b, t, s>>>(g_idx_dem, p_idx_dem, g_str_dem, g_end_dem, dP1d, dP2d, dSP1d, dSP2d);
+    cudaDeviceSynchronize();
+    cudaMemset(dP3s, 0, sizeof(part3) * num_part2_sph);
+    cudaMemset(dP3d, 0, sizeof(part3) * num_part2_dem);
+    cudaMemcpy(dP1s, dSP1s, sizeof(part1) * num_part2_sph, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(dP1d, dSP1d, sizeof(part1) * num_part2_dem, cudaMemcpyDeviceToDevice);
+    b.x = bs; KERNEL_clc_mass_init_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, count);
+    cudaDeviceSynchronize();
+    if (kgc_solve > 0) gradient_correction_sph(g_str_sph, g_end_sph, dSP1s, dP3s);
+    b.x = bs;
+    KERNEL_clc_prep3D_coupling_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, g_str_dem, g_end_dem, dSP1d, dSP2d,
+                                             count, time);
+    b.x = bd;
+    KERNEL_clc_prep3D_coupling_dem<<<b, t>>>(g_str_dem, g_end_dem, dSP1d, dSP2d, g_str_sph, g_end_sph, dSP1s, dSP2s,
+                                             count, time);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_clc_prep3D_prep_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s, count);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_clc_prep3D_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s, count);
+    cudaDeviceSynchronize();
+    b.x = (num_part2 - 1) / t.x + 1;
+    if ((noslip_bc == 1) || (penetration_solve == 1)) {
+        KERNEL_boundary3D<<<b, t>>>(g_str, g_end, dSP1);
+        cudaDeviceSynchronize();
+    }
+    b.x = bs; KERNEL_advection_force3D_sph<<<b, t>>>(1, g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bd; KERNEL_DEM_interaction3D_dem<<<b, t>>>(1, g_str_dem, g_end_dem, dSP1d, dP1d, dP3d, time);
+    cudaDeviceSynchronize();
+    b.x = bs;   // the reference sizes this launch by the SPH count
+    KERNEL_DEM_coupling3D_dem<<<b, t>>>(1, g_str_dem, g_end_dem, dSP1d, dSP2d, dP3d, g_str_sph, g_end_sph, dSP1s,
+                                        dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bs;
+    KERNEL_SPH_coupling3D_sph<<<b, t>>>(1, g_str_sph, g_end_sph, dSP1s, dP3s, g_str_dem, g_end_dem, dSP1d, dP3d);
+    cudaDeviceSynchronize();
+    if (time_type == Pre_Cor) {
+        b.x = bs; KERNEL_clc_projection_sph<<<b, t>>>(count, dt, time, dSP1s, dSP2s, dP3s);
+        b.x = bd; KERNEL_clc_projection_dem<<<b, t>>>(count, dt, time, dSP1d, dSP2d, dP3d);
+        cudaDeviceSynchronize();
+    }
+    if (count == 0) {
+        b.x = bs; KERNEL_Neumann_boundary3D_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+        cudaDeviceSynchronize();
+    }
+    b.x = bs; KERNEL_PPE3D_sph<<<b, t>>>(dt, g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_PPE3D_calc_sph<<<b, t>>>(dt, g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_Neumann_boundary3D_sph<<<b, t>>>(g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_pressureforce3D_sph<<<b, t>>>(1, g_str_sph, g_end_sph, dSP1s, dSP2s, dP3s);
+    cudaDeviceSynchronize();
+    b.x = bs; KERNEL_time_update_projection_sph<<<b, t>>>(dt, dSP1s, dP1s, dSP2s, dP2s, dP3s);
+    b.x = bd; KERNEL_time_update_projection_dem<<<b, t>>>(dt, dSP1d, dP1d, dSP2d, dP2d, dP3d);
+    cudaDeviceSynchronize();
+    if (open_boundary > 0) {
+        b.x = bs;
+        KERNEL_open_boundary_extrapolation3D_1_sph<<<b, t>>>(time, g_str_sph, g_end_sph, dP1s, dSP2s, dP3s, count, dt);
+        cudaDeviceSynchronize();
+        KERNEL_open_boundary_extrapolation3D_1_calc_sph<<<b, t>>>(time, g_str_sph, g_end_sph, dP1s, dSP2s, dP3s, count,
+                                                                  dt);
+        cudaDeviceSynchronize();
+    }
+    if (xsph_solve) {
+        b.x = bs; KERNEL_xsph3D_sph<<<b, t>>>(1, g_str_sph, g_end_sph, dt, time, dP1s, dSP2s);
+        cudaDeviceSynchronize();
+        b.x = bs; KERNEL_xsph3D_calc_sph<<<b, t>>>(1, g_str_sph, g_end_sph, dt, time, dP1s, dSP2s);
+        cudaDeviceSynchronize();
+    }
+}
+
+// nsteps of isph_step_without_dem_walls (3-D ISPH-DEM input, decouple_stride 1)
+extern "C" int ref_run_without_dem_walls(int nsteps) {
+    if (loaded != 1) return -1;
+    if (decouple_stride != 1 || dim != 3) return -2;
+    cudaDeviceSynchronize();
+    auto t0 = refh_now();
+    for (int k = 0; k < nsteps; k++) {
+        isph_step_without_dem_walls();
+        time += dt;
+        count++;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return -100;
+    auto t1 = refh_now();
+    last_ms = refh_ms(t0, t1);
+    if (cudaGetLastError() != cudaSuccess) return -101;
+    HCK(cudaMemcpy(fP1s, dP1s, num_part2_sph * sizeof(part1), cudaMemcpyDeviceToHost));
+    HCK(cudaMemcpy(fP2s, dSP2s, num_part2_sph * sizeof(part2), cudaMemcpyDeviceToHost));
+    HCK(cudaMemcpy(fP3s, dP3s, num_part2_sph * sizeof(part3), cudaMemcpyDeviceToHost));
+    if (num_part2_dem) {
+        HCK(cudaMemcpy(fP1d, dP1d, num_part2_dem * sizeof(part1), cudaMemcpyDeviceToHost));
+        HCK(cudaMemcpy(fP2d, dSP2d, num_part2_dem * sizeof(part2), cudaMemcpyDeviceToHost));
+        HCK(cudaMemcpy(fP3d, dP3d, num_part2_dem * sizeof(part3), cudaMemcpyDeviceToHost));
+    }
+    return 0;
+}
+
 extern "C" double ref_last_ms(void) { return last_ms; }
 
 extern "C" int ref_counts(int* ns, int* nd, int* nijk) {

@@ -58,11 +58,11 @@ CASES = {
     # reference-compat bed, spheres starting in contact (Hertz-Mindlin,
     # tangential history insert/lookup/release), drag from moving spheres
     "contact": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=11, spacing=1.9, u_dem=0.05),
-                dict(), [1, 8]),
+                dict(), [1, 8, 100]),
     # same bed with heat transfer on (SPH conduction, DEM shells,
     # radiation, contact conduction, convective exchange)
     "heat": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=12, spacing=1.9, u_dem=0.05),
-             dict(con_solve=1), [1, 8]),
+             dict(con_solve=1), [1, 8, 100]),
 }
 
 

@@ -67,19 +67,24 @@ def test_reduce_without_process_group_is_identity():
 @pytest.mark.timeout(600)
 def test_reference_arm_under_torchrun_world2():
     """torchrun --nproc-per-node 2 bench.py --impl reference: rank 0 alone
-    times the CPU port and prints one JSON line; rank 1 exits 0."""
+    times the CPU baseline (the host build of the reference's kernels when it
+    was built, else the oracle port) and prints one JSON line; rank 1 exits 0."""
     env = dict(os.environ)
     env["OMP_NUM_THREADS"] = "2"
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0"]
+           "--gpus", "2", "--steps", "1", "--warmup", "0", "--no-ref-cuda"]
     r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1, r.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
-    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+    host_ref = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsophia_ref_host.so"))
+    assert d["cpu_baseline"]["kind"] == ("reference" if host_ref else "port")
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["n_sph"] == 301760 and d["config"]["n_dem"] == 20000
+    assert str(d["config"]["n_sph"]) in d["cpu_baseline"]["sample"], "the sample must be the whole bed"
     assert d["config"]["parallelism"] == "replicas x2"
 
 
