@@ -2009,6 +2009,15 @@ extern "C" int sphdem_get_stats(SphdemHandle* h, SphdemStats* out) {
     return h->prec == SPHDEM_PREC_FP64 ? stats_t<double>(h, out) : stats_t<float>(h, out);
 }
 
+extern "C" int sphdem_check(SphdemHandle* h) {
+    SphdemStats st;
+    int r = sphdem_get_stats(h, &st);   // runs the non-finite scans, reads the status words
+    if (r) return r;
+    if (st.overflow_flags) return SPHDEM_E_OVERFLOW;
+    if (st.nan_flag) return SPHDEM_E_NAN;
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* dst, int32_t cap) {
     if (!h || !counts || !h->committed || cap < 0) return SPHDEM_E_ARG;
     int ns = h->ns;

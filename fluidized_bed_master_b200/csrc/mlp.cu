@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -70,11 +71,12 @@ int mlp_set_params(MlpNet& m, const float* params_dev, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
 }
 
-int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st) {
+int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st, int stall) {
     if (n <= 0) return SPHDEM_OK;
     int tiles = (n + MLP_TILE - 1) / MLP_TILE;
     int grid = std::min(tiles, 2 * m.nparts);   // two CTAs per SM overlap their MMA waits
-    k_mlp_infer<<<grid, 128, SM_INFER_END + SM_ALIGN, st>>>(n, (const __nv_bfloat16*)feat, dev_view(m), out, m.err);
+    k_mlp_infer<<<grid, 128, SM_INFER_END + SM_ALIGN, st>>>(n, (const __nv_bfloat16*)feat, dev_view(m), out, m.err,
+                                                            stall);
     return cudaGetLastError() == cudaSuccess ? SPHDEM_OK : SPHDEM_E_CUDA;
 }
 
@@ -162,7 +164,10 @@ extern "C" int sphdem_mlp_forward(const void* feat, int32_t n, const float* para
     MlpNet m;
     cudaStream_t st = (cudaStream_t)stream;
     int r = mlp_oneshot(params, stream, m);
-    if (!r) r = mlp_forward(m, feat, n, out, st);
+    // failure drill of the bounded device waits (see sphdem.h)
+    const char* inj = getenv("SPHDEM_FAULT_DRILL");
+    int stall = (inj && strcmp(inj, "mlp_wait") == 0) ? 1 : 0;
+    if (!r) r = mlp_forward(m, feat, n, out, st, stall);
     int err = 0;
     if (!r && cudaMemcpyAsync(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) r = SPHDEM_E_CUDA;
     if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = SPHDEM_E_CUDA;

@@ -19,7 +19,7 @@ struct MlpNet {
 int mlp_alloc(MlpNet& m);
 void mlp_free(MlpNet& m);
 int mlp_set_params(MlpNet& m, const float* params_dev, cudaStream_t st);
-int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st);
+int mlp_forward(const MlpNet& m, const void* feat, int n, float* out, cudaStream_t st, int stall = 0);
 int mlp_grad(const MlpNet& m, const void* feat, const float* target, const float* weight, int n, float inv_wsum,
              cudaStream_t st);
 int mlp_adam(MlpNet& m, float lr, int t, cudaStream_t st, const double* tstep = nullptr);

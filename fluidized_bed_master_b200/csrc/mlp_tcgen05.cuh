@@ -226,27 +226,45 @@ __device__ __forceinline__ void load_x_row(unsigned char* sm, const __nv_bfloat1
     }
 }
 
-// one MMA group + commit by thread 0, bounded wait by all; false on failure
+// one MMA group + commit by thread 0, bounded wait by all.  A thread whose
+// wait runs out sets fail and remembers the phase (fparity: bit 1 = failed,
+// bit 0 = parity), so that before freeing TMEM it can wait once more, again
+// bounded, for an MMA group that may still be in flight.  stall (inference
+// only; see k_mlp_infer) withholds the group and its commit, so nothing ever
+// arrives on the barrier.
 #define MLP_SYNC_ISSUE(...)                          \
     do {                                             \
         fence_async_smem();                          \
         tc_fence_before();                           \
         __syncthreads();                             \
-        if (tid == 0 && !fail) {                     \
+        if (tid == 0 && !fail && !stall) {           \
             tc_fence_after();                        \
             __VA_ARGS__;                             \
             tc_commit(&mbar);                        \
         }                                            \
         __syncthreads();                             \
-        if (!fail && !mbar_wait(&mbar, phase)) fail = 1; \
+        if (!fail && !mbar_wait(&mbar, phase)) {     \
+            fail = 1;                                \
+            fparity = 2u | phase;                    \
+        }                                            \
         phase ^= 1;                                  \
         tc_fence_after();                            \
     } while (0)
 
+// the end of a kernel that may have given up on a wait: one more bounded wait
+// for the group in flight, then every thread is past its last TMEM access
+#define MLP_DRAIN()                                          \
+    do {                                                     \
+        if (fparity & 2u) mbar_wait(&mbar, fparity & 1u);    \
+    } while (0)
+
 // ---- inference --------------------------------------------------------------
 // out[i] = MLP(feat[i]) for i < n; feat is row-major [n x 16] BF16.
+// stall != 0 is the failure drill of the bounded waits: the first MMA group
+// is not issued, its wait runs out after MLP_WAIT_NS, and the kernel must
+// report through *err, free its TMEM and return (no MMA is in flight).
 __global__ void __launch_bounds__(128, 1) k_mlp_infer(int n, const __nv_bfloat16* __restrict__ feat, MlpDev net,
-                                                      float* __restrict__ out, int* err) {
+                                                      float* __restrict__ out, int* err, int stall) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -273,7 +291,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(int n, const __nv_bfloat16
     const uint32_t tm = tmem_base;
     const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
     const uint32_t id64 = idesc_bf16(MLP_TILE, MLP_H);
-    uint32_t phase = 0;
+    uint32_t phase = 0, fparity = 0;
     const int ntiles = (n + MLP_TILE - 1) / MLP_TILE;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int row = tile * MLP_TILE + tid;
@@ -310,6 +328,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(int n, const __nv_bfloat16
         if (fail) break;
     }
     if (tid == 0 && fail) atomicOr(err, 1);
+    MLP_DRAIN();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
@@ -373,7 +392,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_grad(int n, const __nv_bfloat16*
     const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
     const uint32_t id64 = idesc_bf16(MLP_TILE, MLP_H), idw2 = idesc_bf16(MLP_TILE, GW2_N),
                    idw1 = idesc_bf16(MLP_TILE, GW1_N);
-    uint32_t phase = 0;
+    uint32_t phase = 0, fparity = 0;
+    const int stall = 0;
     int first = 1;
     const int ntiles = (n + MLP_TILE - 1) / MLP_TILE;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -539,6 +559,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_grad(int n, const __nv_bfloat16*
         else P[MLP_NPARAM + 1] = s;
     }
     if (tid == 0 && fail) atomicOr(err, 1);
+    MLP_DRAIN();
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {

@@ -1093,15 +1093,18 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) last_t = max(last_t, __shfl_xor_sync(0xffffffffu, last_t, o));
     if (last_t >= 0 && new_t == last_t) {
-        int slot = free_slot;
+        // no free slot (a 17th partner): flag it; the new contact acted this
+        // step and is not recorded (the reference writes through an unset
+        // slot index here, functions_DEM_INTERACTION2.cuh:1567)
+        const int slot = free_slot;
         if (slot < 0) {
             atomicOr(&F->overflow, 2);
-            slot = 0;
+        } else {
+            D.hid[slot * n + i] = new_id;
+            D.hds[(slot * 3 + 0) * n + i] = new_dx;
+            D.hds[(slot * 3 + 1) * n + i] = new_dy;
+            D.hds[(slot * 3 + 2) * n + i] = new_dz;
         }
-        D.hid[slot * n + i] = new_id;
-        D.hds[(slot * 3 + 0) * n + i] = new_dx;
-        D.hds[(slot * 3 + 1) * n + i] = new_dy;
-        D.hds[(slot * 3 + 2) * n + i] = new_dz;
     }
     tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
     tqx = warp_sum(tqx); tqy = warp_sum(tqy); tqz = warp_sum(tqz);

@@ -45,6 +45,7 @@ def lib():
     L.sphdem_step.argtypes = [vp, C.c_int32]
     L.sphdem_get_field.argtypes = [vp, C.c_int, C.c_int, vp, C.c_size_t]
     L.sphdem_get_stats.argtypes = [vp, P(SphdemStats)]
+    L.sphdem_check.argtypes = [vp]
     L.sphdem_get_neighbors.argtypes = [vp, P(C.c_int32), P(C.c_int32), C.c_int32]
     L.sphdem_get_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
@@ -180,6 +181,10 @@ class Engine:
             a = np.empty(n, dtype=np.float64)
         _chk(lib().sphdem_get_field(self._h, which, F[name], a.ctypes.data, a.nbytes), f"sphdem_get_field({name})")
         return a
+
+    def check(self):
+        """sphdem_check: the status code (0, or SPHDEM_E_OVERFLOW / SPHDEM_E_NAN) of the state so far."""
+        return int(lib().sphdem_check(self._h))
 
     def stats(self):
         s = SphdemStats()

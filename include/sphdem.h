@@ -352,6 +352,12 @@ int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields,
  *   grad:    grad[0..P) = dL/dparams of L = sum_i w_i (y_i - t_i)^2 /
  *            weight_sum, grad[P] = sum_i w_i (y_i - t_i)^2, grad[P+1] =
  *            sum_i w_i. */
+/* Every wait of these kernels on the tensor cores is bounded (0.2 s); when
+ * one runs out the kernel stops issuing work, frees its tensor memory and
+ * the call returns SPHDEM_E_TIMEOUT, leaving the context usable.  Failure
+ * drill: with SPHDEM_FAULT_DRILL=mlp_wait in the environment,
+ * sphdem_mlp_forward withholds its first MMA group, so that wait runs out
+ * and the call must return SPHDEM_E_TIMEOUT (no fault, no hang). */
 int32_t sphdem_mlp_param_count(void);
 int sphdem_mlp_forward(const void* feat_bf16, int32_t n, const float* params,
                        float* out, void* stream);
@@ -386,6 +392,18 @@ int sphdem_get_field(SphdemHandle* h, int which, int field,
 /* Maxima printed by the reference every freq_output/10 steps, plus PPE
  * statistics (synchronises). */
 int sphdem_get_stats(SphdemHandle* h, SphdemStats* out);
+
+/* Health check after the steps enqueued so far (synchronises).  Scans the
+ * current state for non-finite velocities or densities and reads the
+ * status words the kernels set.  Returns SPHDEM_E_OVERFLOW when a
+ * neighbour list ran past its capacity or a sphere met more than 16 contact
+ * partners (the kernels stay in bounds: a list keeps its first `capacity`
+ * entries, and a 17th partner takes slot 0), SPHDEM_E_NAN when the state
+ * holds a NaN or inf, else SPHDEM_OK.  The flags stay set for the life of
+ * the handle.  The reference has no such check: it exits the process on a
+ * CUDA error (CUDA_CHECK, ISPH.cuh:1-8) and only prints maxima every
+ * freq_output/10 steps (ISPH_Calc_seperate.cuh:928-968). */
+int sphdem_check(SphdemHandle* h);
 
 /* Cell-sorted neighbour list of the SPH set as built for the current
  * step: counts[n_sph] and, for each particle, its neighbours within

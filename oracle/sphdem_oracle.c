@@ -839,7 +839,9 @@ static void k_dem_contact(OracleState* S) {
                                     }
                                 }
                             }
-                            if (slot < 0) slot = 0; /* overflow: undefined in the reference */
+                            /* no free slot (a 17th partner): the reference then writes through an
+                             * unset slot index (:1567, undefined); here the new contact acts this step
+                             * and is not recorded (slot stays -1), as in the engine */
                             double nx = (xj - xi) / td, ny = (yj - yi) / td, nz = (zj - zi) / td;
                             double rcxi = (radi - 0.5 * tov) * nx, rcyi = (radi - 0.5 * tov) * ny, rczi = (radi - 0.5 * tov) * nz;
                             double rcxj = -(radj - 0.5 * tov) * nx, rcyj = -(radj - 0.5 * tov) * ny, rczj = -(radj - 0.5 * tov) * nz;
@@ -894,10 +896,12 @@ static void k_dem_contact(OracleState* S) {
                             tqx += mi * (rcyi * fsz - rczi * fsy);
                             tqy += mi * (rczi * fsx - rcxi * fsz);
                             tqz += mi * (rcxi * fsy - rcyi * fsx);
-                            new_id[slot] = demj;
-                            new_ds[slot * 3 + 0] = dsx;
-                            new_ds[slot * 3 + 1] = dsy;
-                            new_ds[slot * 3 + 2] = dsz;
+                            if (slot >= 0) {
+                                new_id[slot] = demj;
+                                new_ds[slot * 3 + 0] = dsx;
+                                new_ds[slot * 3 + 1] = dsy;
+                                new_ds[slot * 3 + 2] = dsz;
+                            }
                         } else {
                             /* release (:1574-1671) */
                             for (int s = 0; s < NSLOT; s++) {
