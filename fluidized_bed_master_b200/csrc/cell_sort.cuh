@@ -1,0 +1,181 @@
+// cell_sort.cuh -- the NNPS sort by cell, written for this engine.
+//
+// Replaces cub::DeviceRadixSort::SortPairs of the reference's NNPS
+// (ISPH_Calc_seperate.cuh:83-85, WCSPH_Calc.cuh:36) and the cell start/end
+// search of KERNEL_reorder_* (functions_NNPS.cuh:670-730).  The values are
+// the slot indices 0..n-1 and CUB's radix sort is stable, so the reference's
+// permutation is: keys ascending, equal keys in ascending slot order.  A
+// counting sort gives exactly that with one pass over the keys per phase:
+//
+//   count   fused into the hash kernels (cell_count): cnt[key] += 1, one
+//           atomic per distinct key of a warp (__match_any_sync);
+//   scan    k_sort_tile_sums + k_sort_scan: exclusive prefix of cnt over the
+//           ncell + 1 buckets (the last bucket holds the i_type 3 slots that
+//           the reference keys num_cells) -> start[]; resets fill[];
+//   scatter k_sort_scatter: tmp[start[k] + fill[k]++] = slot, one atomic
+//           per distinct key of a warp; order inside a cell is arbitrary;
+//   settle  k_sort_settle, one warp per bucket: ranks the bucket's slots by
+//           value (unique, so ranks are a permutation), writes perm/key in
+//           ascending slot order, the cell's start (-1 when empty) and end,
+//           and zeroes cnt[] for the next step.
+//
+// Every bucket is owned by one warp in the settle pass and the ranks depend
+// only on the values, so the result is deterministic and bit-identical to
+// CUB's.  No memset runs per step: cnt is zeroed by the settle pass, fill by
+// the scan (both start at zero after allocation).
+#pragma once
+#include <climits>
+#include <cuda_runtime.h>
+
+namespace sphdem {
+
+constexpr int SORT_TILE = 4096;   // scan tile: 1024 threads x 4 buckets
+
+struct CellSort {
+    int* cnt;        // [nb] bucket counts (zero between steps)
+    int* fill;       // [nb] scatter cursors
+    int* start;      // [nb] exclusive prefix of cnt
+    int* tile_sum;   // [ntiles]
+    int* tmp;        // [n] slots grouped by bucket, unordered inside a bucket
+    int nb;          // buckets: num_cells + 1
+    int ntiles;
+};
+
+// count one key (called by every thread of a warp that hashes; inactive
+// threads pass key < 0)
+__device__ __forceinline__ void cell_count(int* cnt, int key) {
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, key);
+    const int lane = threadIdx.x & 31;
+    if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[key], __popc(peers));
+}
+
+__global__ void __launch_bounds__(1024) k_sort_tile_sums(const int* __restrict__ cnt, int nb, int* tile_sum) {
+    const int base = blockIdx.x * SORT_TILE + threadIdx.x * 4;
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) s += (base + q < nb) ? cnt[base + q] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ int ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int v = ws[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) tile_sum[blockIdx.x] = v;
+    }
+}
+
+// start[b] = sum of cnt[0..b); the tile's offset is the sum of the earlier
+// tiles' sums (in tile order); fill[] is reset for the scatter
+__global__ void __launch_bounds__(1024) k_sort_scan(const int* __restrict__ cnt, const int* __restrict__ tile_sum,
+                                                    int nb, int* start, int* fill) {
+    __shared__ int ws[32];
+    __shared__ int toff;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        int acc = 0;
+        for (int t0 = 0; t0 < (int)blockIdx.x; t0 += 32) {
+            int v = (t0 + lane < (int)blockIdx.x) ? tile_sum[t0 + lane] : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc += v;
+        }
+        if (lane == 0) toff = acc;
+    }
+    const int base = blockIdx.x * SORT_TILE + threadIdx.x * 4;
+    int c[4], s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        c[q] = (base + q < nb) ? cnt[base + q] : 0;
+        s += c[q];
+    }
+    // inclusive warp scan of the thread sums
+    int inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int v = ws[lane], w = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        ws[lane] = w - v;   // exclusive prefix of the warp totals
+    }
+    __syncthreads();
+    int run = toff + ws[warp] + inc - s;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (base + q < nb) {
+            start[base + q] = run;
+            fill[base + q] = 0;
+        }
+        run += c[q];
+    }
+}
+
+__global__ void k_sort_scatter(int n, const int* __restrict__ key, const int* __restrict__ start, int* fill,
+                               int* tmp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = i < n ? key[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (k >= 0 && lane == leader) base = atomicAdd(&fill[k], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (k >= 0) tmp[start[k] + base + __popc(peers & ((1u << lane) - 1u))] = i;
+}
+
+// one warp per bucket b < nb; cell b < nb - 1 gets gs (start or -1) and ge
+// (end, written only for a non-empty cell, as the reference's reorder does)
+__global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
+                                                     const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
+                                                     int* ge) {
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= nb) return;
+    const int m = cnt[b];
+    const int s = start[b];
+    __syncwarp();
+    if (lane == 0) {
+        cnt[b] = 0;
+        if (b < nb - 1) {
+            gs[b] = m ? s : -1;
+            if (m) ge[b] = s + m;
+        }
+    }
+    for (int a = 0; a < m; a += 32) {
+        const int v = (a + lane < m) ? tmp[s + a + lane] : INT_MAX;
+        int r = 0;
+        for (int a2 = 0; a2 < m; a2 += 32) {
+            const int w0 = (a2 + lane < m) ? tmp[s + a2 + lane] : INT_MAX;
+#pragma unroll
+            for (int j = 0; j < 32; j++) r += (__shfl_sync(0xffffffffu, w0, j) < v);
+        }
+        if (a + lane < m) {
+            perm[s + r] = v;
+            key_out[s + r] = b;
+        }
+    }
+}
+
+// scan + scatter + settle for n keys already counted into cs.cnt
+inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* perm, int* key_out, int* gs, int* ge,
+                             cudaStream_t st) {
+    k_sort_tile_sums<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.nb, cs.tile_sum);
+    k_sort_scan<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.tile_sum, cs.nb, cs.start, cs.fill);
+    if (n > 0) k_sort_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, key_in, cs.start, cs.fill, cs.tmp);
+    k_sort_settle<<<(cs.nb * 32 + 255) / 256, 256, 0, st>>>(cs.nb, cs.cnt, cs.start, cs.tmp, perm, key_out, gs, ge);
+    return cudaGetLastError();
+}
+
+}  // namespace sphdem

@@ -32,6 +32,12 @@ struct DevParams {
     double k_sph, cp_sph, k_dem, cp_dem;
     double G, nu_p, damp, fric, r_contact, r_search;
     double inlet_uz, inlet_temp, L2, L3, ball_vel;
+    // The SPH temperature is stored as T - t_ref (t_ref: the mean initial SPH
+    // temperature, an FP32 value): in the FP32 build a temperature near
+    // 300 K keeps increments of 1e-4 K per step only as an offset, and the
+    // pair sums read differences of neighbours' temperatures.  Kernels that
+    // need the absolute temperature add t_ref; the C ABI converts.
+    double t_ref;
     double cyl_cx, cyl_cy, cyl_r;
     double box_c[3], box_L[3];
     double cone_c[3], cone_r1, cone_r2, cone_h;

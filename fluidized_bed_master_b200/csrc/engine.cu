@@ -3,7 +3,6 @@
 // The time loop of the reference (ISPH_Calc_seperate.cuh:905-975) calls
 // SOPHIA_single_ISPH once per step; sphdem_step does the same work as one
 // CUDA graph per step (captured once per step variant and replayed).
-#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -40,7 +39,7 @@ enum {
     KT_W_FINISH, KT_COUNT
 };
 static const char* KT_NAMES[KT_COUNT] = {
-    "hash_sph", "sort_sph(cub)", "cells_gather_sph", "hash_dem", "sort_dem(cub)", "cells_gather_dem",
+    "hash_sph", "sort_sph", "cells_gather_sph", "hash_dem", "sort_dem", "cells_gather_dem",
     "build_list", "passA", "dem_prep", "passB", "dem_contact", "dem_coupling", "sph_coupling", "neumann0",
     "ppe", "neumann", "passC", "dem_update", "open_bc", "xsph", "rows_sph", "rows_dem",
     "ppe.assemble", "ppe.warm_start", "ppe.iterations", "ppe.training", "build_dem_list",
@@ -96,6 +95,19 @@ struct Alloc {
     }
 };
 
+// scratch of the NNPS cell sort (cell_sort.cuh) for n keys on num_cells cells
+CellSort alloc_cell_sort(Alloc& A, int num_cells, int n) {
+    CellSort c;
+    c.nb = num_cells + 1;
+    c.ntiles = (c.nb + SORT_TILE - 1) / SORT_TILE;
+    c.cnt = A.get<int>(c.nb);
+    c.fill = A.get<int>(c.nb);
+    c.start = A.get<int>(c.nb);
+    c.tile_sum = A.get<int>(c.ntiles);
+    c.tmp = A.get<int>(n);
+    return c;
+}
+
 template <typename R>
 struct EngineHost {
     Engine<R> E;
@@ -146,7 +158,7 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     W.ux0 = A.get<R>(ns); W.uy0 = A.get<R>(ns); W.uz0 = A.get<R>(ns);
     W.p_new = A.get<R>(ns);
     W.u_tmpx = A.get<R>(ns); W.u_tmpy = A.get<R>(ns); W.u_tmpz = A.get<R>(ns); W.temp_tmp = A.get<R>(ns);
-    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
+    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = nullptr; W.val_out = A.get<int>(ns);
     W.g_str = A.get<int>(ncells + 1); W.g_end = A.get<int>(ncells + 1);
     W.rows = A.get<int4>(ncells);
     W.ncnt = A.get<int>(ns);
@@ -167,37 +179,39 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     DW.Fdx_da = A.get<R>(nd); DW.Fdy_da = A.get<R>(nd); DW.Fdz_da = A.get<R>(nd);
     DW.ux0 = A.get<R>(nd); DW.uy0 = A.get<R>(nd); DW.uz0 = A.get<R>(nd); DW.temp0 = A.get<R>(nd);
     DW.magf = A.get<R>(nd);
-    DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = A.get<int>(nd); DW.val_out = A.get<int>(nd);
+    DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = nullptr; DW.val_out = A.get<int>(nd);
     DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
     DW.rows = A.get<int4>(ncells);
     DW.nbs = A.get<int>((size_t)nd * DEM_SPH_CAP);
     DW.ncs = A.get<int>(nd);
 }
 
-int key_bits(int num_cells) {
-    int b = 1;
-    while ((1ll << b) <= (long long)num_cells) b++;
-    return b;
-}
 
 // ---------------------------------------------------------------------------
 // host <-> device field transfer (conversion R <-> double on the host)
 // ---------------------------------------------------------------------------
+// (a field stored with an offset, see field_offset, holds value - off)
 template <typename R>
-int upload_real(R* dst, const double* src, int n, cudaStream_t s) {
+int upload_real(R* dst, const double* src, int n, cudaStream_t s, double off = 0.0) {
     std::vector<R> tmp(n);
-    for (int i = 0; i < n; i++) tmp[i] = (R)src[i];
+    for (int i = 0; i < n; i++) tmp[i] = (R)(src[i] - off);
     CK(cudaMemcpyAsync(dst, tmp.data(), sizeof(R) * n, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
     return SPHDEM_OK;
 }
 template <typename R>
-int download_real(double* dst, const R* src, int n, cudaStream_t s) {
+int download_real(double* dst, const R* src, int n, cudaStream_t s, double off = 0.0) {
     std::vector<R> tmp(n);
     CK(cudaMemcpyAsync(tmp.data(), src, sizeof(R) * n, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    for (int i = 0; i < n; i++) dst[i] = (double)tmp[i];
+    for (int i = 0; i < n; i++) dst[i] = (double)tmp[i] + off;
     return SPHDEM_OK;
+}
+
+// offset the ISPH-DEM engine stores a field with: the SPH temperature is
+// kept as T - t_ref (DevParams::t_ref)
+static double field_offset(const DevParams& P, int which, int field) {
+    return (which == 0 && field == SPHDEM_F_TEMP) ? P.t_ref : 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -214,15 +228,12 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     SphState<R>& S = E.S[src];
     {
         KTIME(KT_HASH_S);
-        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, W.val_in);
+        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, E.cs_s.cnt);
     }
-    size_t bytes = E.sort_tmp_bytes;
     {
         KTIME(KT_SORT_S);
-        CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
-                                           key_bits(P.num_cells), st));
+        CK(cell_sort(E.cs_s, n, W.key_in, W.val_out, W.key_out, W.g_str, W.g_end, st));
     }
-    CK(cudaMemsetAsync(W.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
     CK(cudaMemsetAsync(W.counters, 0, sizeof(int) * 4, st));
     SphGatherSrc<R> g;
     if (P.xsph) { g.ux = W.u_tmpx; g.uy = W.u_tmpy; g.uz = W.u_tmpz; g.temp = W.temp_tmp; }
@@ -230,14 +241,14 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     g.m = W.m_new; g.rho = W.rho_new; g.pres = W.p_new;
     {
         KTIME(KT_GATHER_S);
-        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.rec, W.key_out, W.val_out, W.g_str,
-                                                                W.g_end, W.wall_idx, W.buf_idx, W.counters);
+        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.rec, W.val_out, W.wall_idx,
+                                                                W.buf_idx, W.counters);
     }
     {
         KTIME(KT_ROWS_S);
         k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, W.g_str, W.g_end, W.rows);
     }
-    *nl += 4;
+    *nl += 7;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -249,26 +260,23 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     DemWork<R>& DW = E.dw;
     cudaStream_t st = H->stream;
     int n = P.nd;
-    CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
     if (n == 0) {
+        CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
         CK(cudaMemsetAsync(DW.rows, 0, sizeof(int4) * P.NI * P.NJ * P.NK, st));
         return SPHDEM_OK;
     }
     DemState<R>& D = E.D[src];
     {
         KTIME(KT_HASH_D);
-        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, DW.val_in);
+        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, E.cs_d.cnt);
     }
-    size_t bytes = E.sort_tmp_bytes;
     {
         KTIME(KT_SORT_D);
-        CK(cub::DeviceRadixSort::SortPairs(E.sort_tmp, bytes, DW.key_in, DW.key_out, DW.val_in, DW.val_out, n, 0,
-                                           key_bits(P.num_cells), st));
+        CK(cell_sort(E.cs_d, n, DW.key_in, DW.val_out, DW.key_out, DW.g_str, DW.g_end, st));
     }
     {
         KTIME(KT_GATHER_D);
-        k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.key_out, DW.val_out, DW.g_str,
-                                                                DW.g_end);
+        k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.val_out);
         k_gather_history<<<nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st>>>(n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
                                                                          E.D[dst].hds);
     }
@@ -276,7 +284,7 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
         KTIME(KT_ROWS_D);
         k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, DW.g_str, DW.g_end, DW.rows);
     }
-    *nl += 5;
+    *nl += 8;
     CK(cudaGetLastError());
     return SPHDEM_OK;
 }
@@ -709,6 +717,14 @@ static int commit_t(SphdemHandle* H) {
     P.r_contact = p.dem_contact_range; P.r_search = p.dem_search_range;
     P.inlet_uz = p.inlet_uz_mirror; P.inlet_temp = p.inlet_temp; P.L2 = p.obc_L2; P.L3 = p.obc_L3;
     P.ball_vel = p.ball_vel;
+    {
+        // offset of the stored SPH temperature (DevParams::t_ref), an FP32 value
+        auto& tv = H->stage_d[0][SPHDEM_F_TEMP];
+        double s = 0;
+        for (double v : tv) s += v;
+        P.t_ref = tv.empty() ? 0.0 : (double)(float)(s / (double)tv.size());
+        if (!std::isfinite(P.t_ref)) P.t_ref = 0.0;
+    }
     P.cyl_cx = p.cyl_cx; P.cyl_cy = p.cyl_cy; P.cyl_r = p.cyl_r;
     for (int k = 0; k < 3; k++) { P.box_c[k] = p.box_c[k]; P.box_L[k] = p.box_L[k]; P.cone_c[k] = p.cone_c[k]; }
     P.cone_r1 = p.cone_r1; P.cone_r2 = p.cone_r2; P.cone_h = p.cone_h;
@@ -738,17 +754,10 @@ static int commit_t(SphdemHandle* H) {
     E.red_buf = A.get<double>(8);
     if (!A.ok) return SPHDEM_E_NOMEM;
     E.cur_s = 0; E.cur_d = 0;
-    // CUB temporary storage, sized for the larger set
-    {
-        size_t b1 = 0, b2 = 0;
-        int nmax = std::max(ns, nd);
-        cub::DeviceRadixSort::SortPairs(nullptr, b1, E.sw.key_in, E.sw.key_out, E.sw.val_in, E.sw.val_out,
-                                        std::max(nmax, 1), 0, key_bits(num_cells), H->stream);
-        (void)b2;
-        E.sort_tmp_bytes = b1;
-        E.sort_tmp = A.get<char>(b1);
-        if (!A.ok) return SPHDEM_E_NOMEM;
-    }
+    // cell sort scratch of both sets (zeroed by the allocator, as cell_sort expects)
+    E.cs_s = alloc_cell_sort(A, num_cells, ns);
+    E.cs_d = alloc_cell_sort(A, num_cells, nd);
+    if (!A.ok) return SPHDEM_E_NOMEM;
     // buffer tags (c_initial_inner_outer_particle_single_{sph,dem}, functions_NNPS.cuh:60-200)
     for (int q = 0; q < 2; q++) {
         int nq = q ? nd : ns;
@@ -800,7 +809,7 @@ static int commit_t(SphdemHandle* H) {
     auto up_r = [&](R* dst, int q, int f, int nq) -> int {
         auto& v = H->stage_d[q][f];
         if ((int)v.size() != nq) v.assign(nq, 0.0);
-        return nq ? upload_real<R>(dst, v.data(), nq, st) : SPHDEM_OK;
+        return nq ? upload_real<R>(dst, v.data(), nq, st, field_offset(P, q, f)) : SPHDEM_OK;
     };
     auto up_i = [&](int* dst, int q, int f, int nq) -> int {
         auto& v = H->stage_i[q][f];
@@ -1047,7 +1056,8 @@ static int get_field_t(SphdemHandle* H, int which, int field, void* dst, int n) 
     if (kind == 0) {
         CK(cudaMemcpy(dst, ptr, sizeof(double) * n, cudaMemcpyDeviceToHost));
     } else if (kind == 1) {
-        return download_real<R>((double*)dst, (const R*)ptr, n, H->stream);
+        const DevParams& P = ((EngineHost<R>*)H->eng)->E.P;
+        return download_real<R>((double*)dst, (const R*)ptr, n, H->stream, field_offset(P, which, field));
     } else {
         CK(cudaMemcpy(dst, ptr, sizeof(int) * n, cudaMemcpyDeviceToHost));
     }
@@ -1139,8 +1149,7 @@ struct WEngineHost {
     WWork<R> W;
     DevFlags* flags = nullptr;
     double* red_buf = nullptr;    // maxima of sphdem_get_stats (3 doubles)
-    void* sort_tmp = nullptr;
-    size_t sort_tmp_bytes = 0;
+    CellSort cs;      // NNPS sort by cell
     int nb_cap = 0;
     int lanes = 1;    // lanes per particle of the gathers (w_lanes, or the commit-time autotuner)
     Alloc A;
@@ -1179,12 +1188,9 @@ static int w_nnps(SphdemHandle* H, WEngineHost<R>* EH, int src, int dst, bool ha
     cudaStream_t st = H->stream;
     int n = P.ns;
     WState<R>& S = EH->S[src];
-    if (!hashed) k_w_hash<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W.key_in, W.val_in);
-    size_t bytes = EH->sort_tmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(EH->sort_tmp, bytes, W.key_in, W.key_out, W.val_in, W.val_out, n, 0,
-                                       key_bits(P.num_cells), st));
-    CK(cudaMemsetAsync(W.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
-    k_w_gather<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, EH->S[dst], W.key_out, W.val_out, W.g_str, W.g_end);
+    if (!hashed) k_w_hash<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, W.key_in, EH->cs.cnt);
+    CK(cell_sort(EH->cs, n, W.key_in, W.val_out, W.key_out, W.g_str, W.g_end, st));
+    k_w_gather<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, EH->S[dst], W.val_out);
     k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, W.g_str, W.g_end, W.rows);
     CK(cudaGetLastError());
     return SPHDEM_OK;
@@ -1199,7 +1205,7 @@ static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
     cudaStream_t st = H->stream;
     int n = P.ns, so = EH->cur, sn = 1 - EH->cur;
     int bs = nblocks(n, TPB);
-    { KTIME(KT_W_PRED); k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W, W.key_in, W.val_in); }
+    { KTIME(KT_W_PRED); k_w_predictor<R><<<bs, TPB, 0, st>>>(P, Q, EH->S[so], W, W.key_in, EH->cs.cnt); }
     {
         KTIME(KT_W_NNPS);
         int r = w_nnps<R>(H, EH, so, sn, true);
@@ -1220,10 +1226,10 @@ static int w_enqueue(SphdemHandle* H, WEngineHost<R>* EH, int64_t* nl) {
         { KTIME(KT_W_FINISH); k_w_finish<R><<<bs, TPB, 0, st>>>(P, S, W); }
     }
     CK(cudaGetLastError());
-    // engine kernels of the step (CUB's sort passes not counted): predictor
-    // (+ cell keys), gather, rows, list, [kgc], prep, continuity (+ EOS),
-    // interaction, corrector (+ step counter), [xsph, finish]
-    *nl += 8 + (P.kgc == 1) + 2 * (P.xsph != 0);
+    // engine kernels of the step: predictor (+ cell keys and counts), the
+    // four cell-sort passes, gather, rows, list, [kgc], prep, continuity
+    // (+ EOS), interaction, corrector (+ step counter), [xsph, finish]
+    *nl += 12 + (P.kgc == 1) + 2 * (P.xsph != 0);
     return SPHDEM_OK;
 }
 
@@ -1449,7 +1455,7 @@ static int w_commit_t(SphdemHandle* H) {
     W.rho_ref = A.get<double>(ns); W.grx = A.get<R>(ns); W.gry = A.get<R>(ns); W.pgfx = A.get<R>(ns);
     W.pgfy = A.get<R>(ns); W.Cm = A.get<R>((size_t)ns * 4);
     W.xn = A.get<double>(ns); W.yn = A.get<double>(ns); W.rhon = A.get<double>(ns);
-    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = A.get<int>(ns); W.val_out = A.get<int>(ns);
+    W.key_in = A.get<int>(ns); W.key_out = A.get<int>(ns); W.val_in = nullptr; W.val_out = A.get<int>(ns);
     W.g_str = A.get<int>(P.num_cells + 1); W.g_end = A.get<int>(P.num_cells + 1);
     W.rows = A.get<int4>(NI * NJ * NK);
     W.ncnt = A.get<int>(ns);
@@ -1457,14 +1463,8 @@ static int w_commit_t(SphdemHandle* H) {
     EH->flags = A.get<DevFlags>(1);
     EH->red_buf = A.get<double>(4);
     if (!A.ok) return SPHDEM_E_NOMEM;
-    {
-        size_t b = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, b, W.key_in, W.key_out, W.val_in, W.val_out, std::max(ns, 1), 0,
-                                        key_bits(P.num_cells), H->stream);
-        EH->sort_tmp_bytes = b;
-        EH->sort_tmp = A.get<char>(b);
-        if (!A.ok) return SPHDEM_E_NOMEM;
-    }
+    EH->cs = alloc_cell_sort(A, P.num_cells, ns);
+    if (!A.ok) return SPHDEM_E_NOMEM;
     cudaStream_t st = H->stream;
     auto& pt = H->stage_i[0][SPHDEM_F_PTYPE];
     for (int v : pt)
@@ -1749,7 +1749,8 @@ static int set_state_t(SphdemHandle* H, int which, int field, const void* src, i
         CK(cudaMemcpy((void*)ptr, src, sizeof(double) * n, cudaMemcpyHostToDevice));
         return SPHDEM_OK;
     }
-    return upload_real<R>((R*)ptr, (const double*)src, n, H->stream);
+    const DevParams& P = ((EngineHost<R>*)H->eng)->E.P;
+    return upload_real<R>((R*)ptr, (const double*)src, n, H->stream, field_offset(P, which, field));
 }
 
 // ---------------------------------------------------------------------------
@@ -1760,6 +1761,7 @@ static int set_state_t(SphdemHandle* H, int which, int field, const void* src, i
 namespace {
 struct XTab {
     void* p[SPHDEM_BULK_MAX_FIELDS];
+    double off[SPHDEM_BULK_MAX_FIELDS];   // stored value = value - off (field_offset)
     unsigned dbl;   // bit f set: field f is stored as double
 };
 
@@ -1770,7 +1772,7 @@ __global__ void k_unstage(int n, int nf, const double* __restrict__ st, XTab t) 
         int f = (int)(q / n), i = (int)(q - (long long)f * n);
         double v = st[q];
         if ((t.dbl >> f) & 1u) ((double*)t.p[f])[i] = v;
-        else ((R*)t.p[f])[i] = (R)v;
+        else ((R*)t.p[f])[i] = (R)(v - t.off[f]);
     }
 }
 
@@ -1779,7 +1781,7 @@ __global__ void k_stage(int n, int nf, double* __restrict__ st, XTab t) {
     long long tot = (long long)n * nf;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
         int f = (int)(q / n), i = (int)(q - (long long)f * n);
-        st[q] = ((t.dbl >> f) & 1u) ? ((const double*)t.p[f])[i] : (double)((const R*)t.p[f])[i];
+        st[q] = ((t.dbl >> f) & 1u) ? ((const double*)t.p[f])[i] : (double)((const R*)t.p[f])[i] + t.off[f];
     }
 }
 }  // namespace
@@ -1831,6 +1833,7 @@ static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, voi
         int e = w ? w_field_ptr<R>(H, fields[k], &ptr, &kind) : field_ptr<R>(H, which, fields[k], &ptr, &kind);
         if (e || kind == 2) return SPHDEM_E_ARG;
         t.p[k] = (void*)ptr;
+        t.off[k] = w ? 0.0 : field_offset(((EngineHost<R>*)H->eng)->E.P, which, fields[k]);
         if (kind == 0) t.dbl |= 1u << k;
     }
     if (n == 0 || nf == 0) return SPHDEM_OK;

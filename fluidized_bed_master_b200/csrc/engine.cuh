@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "cell_sort.cuh"
 #include "device_common.cuh"
 #include "records.cuh"
 
@@ -98,8 +99,7 @@ struct Engine {
     SphWork<R> sw;
     DemWork<R> dw;
     DevFlags* flags;
-    void* sort_tmp;
-    size_t sort_tmp_bytes;
+    CellSort cs_s, cs_d; // NNPS sort by cell of the SPH and DEM sets
     double* red_buf;     // reductions for stats
 };
 

@@ -38,6 +38,7 @@
 // The iteration runs inside the step's CUDA graph as a conditional while
 // node; the last kernel of an iteration decides whether to continue.
 #pragma once
+#include <cuda_bf16.h>
 #include "../../include/sphdem.h"
 #include "step_kernels.cuh"
 

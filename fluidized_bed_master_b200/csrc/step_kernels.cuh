@@ -67,29 +67,21 @@ __device__ __forceinline__ void for_stencil_j(const DevParams& P, int ic, int jc
 // NNPS
 // ---------------------------------------------------------------------------
 // KERNEL_index_particle_to_cell_{sph,dem}: functions_NNPS.cuh:762-821
+// The cell-sort count (cell_count, cell_sort.cuh) is fused in.
 __global__ void k_hash(DevParams P, int n, const double* __restrict__ x, const double* __restrict__ y,
-                       const double* __restrict__ z, const int* __restrict__ itype, int* key, int* val) {
+                       const double* __restrict__ z, const int* __restrict__ itype, int* key, int* cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int k;
-    if (itype[i] == 3) k = P.num_cells;
-    else {
-        int ic, jc, kc;
-        cell_ijk(P, x[i], y[i], z[i], ic, jc, kc);
-        k = ic + P.NI * jc + P.NI * P.NJ * kc;
+    int k = -1;
+    if (i < n) {
+        if (itype[i] == 3) k = P.num_cells;
+        else {
+            int ic, jc, kc;
+            cell_ijk(P, x[i], y[i], z[i], ic, jc, kc);
+            k = ic + P.NI * jc + P.NI * P.NJ * kc;
+        }
+        key[i] = k;
     }
-    key[i] = k;
-    val[i] = i;
-}
-
-// cell start/end of KERNEL_reorder_{sph,dem} (functions_NNPS.cuh:670-730)
-__device__ __forceinline__ void cell_bounds(const DevParams& P, int i, int n, const int* __restrict__ key, int* gs, int* ge) {
-    int k = key[i];
-    if (i == 0 || k != key[i - 1]) {
-        if (k < P.num_cells) gs[k] = i;
-        if (i > 0 && key[i - 1] < P.num_cells) ge[key[i - 1]] = i;
-    }
-    if (i == n - 1 && k < P.num_cells) ge[k] = n;
+    cell_count(cnt, k);
 }
 
 // per-cell stencil row table (for_rows), one thread per cell
@@ -110,12 +102,11 @@ struct SphGatherSrc {
 
 template <typename R>
 __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R> gsrc, SphState<R> dst,
-                                   SphRec<R> rec, const int* __restrict__ key, const int* __restrict__ perm, int* gs,
-                                   int* ge, int* wall_idx, int* buf_idx, int* counters) {
+                                   SphRec<R> rec, const int* __restrict__ perm, int* wall_idx, int* buf_idx,
+                                   int* counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
-    cell_bounds(P, i, n, key, gs, ge);
     int p = perm[i];
     double x = src.x[p], y = src.y[p], z = src.z[p];
     dst.x[i] = x;
@@ -146,12 +137,10 @@ __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R>
 }
 
 template <typename R>
-__global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst, const int* __restrict__ key,
-                                   const int* __restrict__ perm, int* gs, int* ge) {
+__global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst, const int* __restrict__ perm) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.nd;
     if (i >= n) return;
-    cell_bounds(P, i, n, key, gs, ge);
     int p = perm[i];
     dst.x[i] = src.x[p]; dst.y[i] = src.y[p]; dst.z[i] = src.z[p];
     dst.h[i] = src.h[p]; dst.rad[i] = src.rad[p];
@@ -932,20 +921,23 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
         DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
     }
     if (D.itype[i] != 1 || D.ptype[i] <= 1000) return;
+    // the pair terms and their sums run in FP64 in both builds: the tangential
+    // relative velocity and the torques are small differences of the state
+    using Q = double;
     double xi = D.x[i], yi = D.y[i], zi = D.z[i], radi = D.rad[i];
-    R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
-    R mi = D.m[i], rii = D.ri[i], rhoi = D.rho[i], tempi = D.temp[i];
-    R pri = (R)P.nu_p, Gi = (R)P.G, ymi = Gi * ((R)2 * ((R)1 + pri));
-    R ymij = (R)1 / ((((R)1 - pri * pri) / ymi) + (((R)1 - pri * pri) / ymi));
-    R Gij = (R)1 / ((((R)2 - pri) / Gi) + (((R)2 - pri) / Gi));
-    R cdamp = sqrt((R)3.333333333) * (R)P.damp;
-    R kci = (R)P.k_dem, cpi = (R)P.cp_dem;
-    R emi = (tempi >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tempi - (R)5.228643e-7 * tempi * tempi +
-                                 (R)1.10479e-10 * tempi * tempi * tempi)
-                              : (R)0.842337;
-    R radiR = (R)radi;
-    R dr2 = ((R)1 / (R)6) * radiR;
-    R volm = ((R)4 / (R)3) * (R)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
+    Q uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
+    Q mi = D.m[i], rii = D.ri[i], rhoi = D.rho[i], tempi = D.temp[i];
+    Q pri = (Q)P.nu_p, Gi = (Q)P.G, ymi = Gi * ((Q)2 * ((Q)1 + pri));
+    Q ymij = (Q)1 / ((((Q)1 - pri * pri) / ymi) + (((Q)1 - pri * pri) / ymi));
+    Q Gij = (Q)1 / ((((Q)2 - pri) / Gi) + (((Q)2 - pri) / Gi));
+    Q cdamp = sqrt((Q)3.333333333) * (Q)P.damp;
+    Q kci = (Q)P.k_dem, cpi = (Q)P.cp_dem;
+    Q emi = (tempi >= (Q)700) ? ((Q)0.505586 + (Q)7.92943e-4 * tempi - (Q)5.228643e-7 * tempi * tempi +
+                                 (Q)1.10479e-10 * tempi * tempi * tempi)
+                              : (Q)0.842337;
+    Q radiR = (Q)radi;
+    Q dr2 = ((Q)1 / (Q)6) * radiR;
+    Q volm = ((Q)4 / (Q)3) * (Q)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
     int oid[SPHDEM_NSLOT];
     int free_slot = -1;
 #pragma unroll
@@ -955,7 +947,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     }
     int ic, jc, kc;
     cell_ijk(P, xi, yi, zi, ic, jc, kc);
-    R tx = 0, ty = 0, tz = 0, tqx = 0, tqy = 0, tqz = 0, dtr = 0, dtc = 0;
+    Q tx = 0, ty = 0, tz = 0, tqx = 0, tqy = 0, tqz = 0, dtr = 0, dtc = 0;
     const double kdt = P.dt;
     // this lane's last new contact (visit order t) and its spring
     int new_t = -1, new_id = 0;
@@ -970,32 +962,32 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
         if (!(td < P.r_search * radi && td > 0.0)) return;
         double ovlp = radi + radj - td;
         int demj = D.dem_idx[j];
-        R radjR = (R)radj;
-        R radij = (R)1 / ((R)1 / radiR + (R)1 / radjR);
-        R tdR = (R)td;
+        Q radjR = (Q)radj;
+        Q radij = (Q)1 / ((Q)1 / radiR + (Q)1 / radjR);
+        Q tdR = (Q)td;
         if (P.con) {
-            R tempj = D.temp[j];
-            R emj = (tempj >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tempj - (R)5.228643e-7 * tempj * tempj +
-                                         (R)1.10479e-10 * tempj * tempj * tempj)
-                                      : (R)0.842337;
-            R ai = radiR / tdR, aj = radjR / tdR, dij = aj - ai;
-            R dc_r = (R)0.56 * ((R)2 * radij);
-            R dc_ar = (R)3.14159 * dc_r * dc_r;
-            R dmax = (R)0.5 * (sqrt((R)1 + (R)4 * dc_ar / ((R)3.14159 * tdR * tdR * ((R)1 - dij * dij))) - dij);
-            R ci = ((R)1 - dij * dij) / ((R)2 * dmax) - dij;
-            R cj = ((R)1 - dij * dij) / ((R)2 * (dmax + dij)) + dij;
-            R si = sqrt((R)1 - ci * ci), sj = sqrt((R)1 - cj * cj);
-            R ri_cr = radiR * si, rj_cr = radjR * sj;
-            R td_cr = tdR - radiR * ci - radjR * cj;
-            R z_cr = (R)1 + ((R)4 * rj_cr * rj_cr + td_cr * td_cr) / (ri_cr * ri_cr);
-            R F_cr = (R)0.5 * (z_cr - sqrt(z_cr * z_cr - (R)4 * rj_cr * rj_cr / (ri_cr * ri_cr)));
-            R F_ij = ((R)1 + ci) * F_cr * (R)0.5;
-            R ar_i = (R)2 * (R)3.14159 * radiR * radiR * ((R)1 - ci);
-            R ar_j = (R)2 * (R)3.14159 * radjR * radjR * ((R)1 - cj);
-            R arr = ar_j / ar_i;
-            R Y = F_ij + ((R)1 - F_ij) * (arr / ((R)1 + arr));
-            R einv = ((R)1 - emi) / (emi * ar_i) + ((R)1 - emj) / (emj * ar_j) + (R)1 / (Y * ar_i);
-            dtr += -(R)5.6704e-8 * (tempi * tempi * tempi * tempi - tempj * tempj * tempj * tempj) /
+            Q tempj = D.temp[j];
+            Q emj = (tempj >= (Q)700) ? ((Q)0.505586 + (Q)7.92943e-4 * tempj - (Q)5.228643e-7 * tempj * tempj +
+                                         (Q)1.10479e-10 * tempj * tempj * tempj)
+                                      : (Q)0.842337;
+            Q ai = radiR / tdR, aj = radjR / tdR, dij = aj - ai;
+            Q dc_r = (Q)0.56 * ((Q)2 * radij);
+            Q dc_ar = (Q)3.14159 * dc_r * dc_r;
+            Q dmax = (Q)0.5 * (sqrt((Q)1 + (Q)4 * dc_ar / ((Q)3.14159 * tdR * tdR * ((Q)1 - dij * dij))) - dij);
+            Q ci = ((Q)1 - dij * dij) / ((Q)2 * dmax) - dij;
+            Q cj = ((Q)1 - dij * dij) / ((Q)2 * (dmax + dij)) + dij;
+            Q si = sqrt((Q)1 - ci * ci), sj = sqrt((Q)1 - cj * cj);
+            Q ri_cr = radiR * si, rj_cr = radjR * sj;
+            Q td_cr = tdR - radiR * ci - radjR * cj;
+            Q z_cr = (Q)1 + ((Q)4 * rj_cr * rj_cr + td_cr * td_cr) / (ri_cr * ri_cr);
+            Q F_cr = (Q)0.5 * (z_cr - sqrt(z_cr * z_cr - (Q)4 * rj_cr * rj_cr / (ri_cr * ri_cr)));
+            Q F_ij = ((Q)1 + ci) * F_cr * (Q)0.5;
+            Q ar_i = (Q)2 * (Q)3.14159 * radiR * radiR * ((Q)1 - ci);
+            Q ar_j = (Q)2 * (Q)3.14159 * radjR * radjR * ((Q)1 - cj);
+            Q arr = ar_j / ar_i;
+            Q Y = F_ij + ((Q)1 - F_ij) * (arr / ((Q)1 + arr));
+            Q einv = ((Q)1 - emi) / (emi * ar_i) + ((Q)1 - emj) / (emj * ar_j) + (Q)1 / (Y * ar_i);
+            dtr += -(Q)5.6704e-8 * (tempi * tempi * tempi * tempi - tempj * tempj * tempj * tempj) /
                    (einv * (rhoi * volm) * cpi);
         }
         if (!(td < P.r_contact * radi)) return;
@@ -1004,10 +996,10 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
         for (int s = 0; s < SPHDEM_NSLOT; s++)
             if (slot < 0 && oid[s] == demj) slot = s;
         if (td > 0 && ovlp > 0) {
-            R tov = (R)ovlp;
+            Q tov = (Q)ovlp;
             if (P.con) {
-                R kij = (R)1 / ((R)1 / kci + (R)1 / kci);
-                dtc += -(R)4 * kij * sqrt(((R)2 * tov) * (radij - (R)0.5 * tov)) * (tempi - D.temp[j]) /
+                Q kij = (Q)1 / ((Q)1 / kci + (Q)1 / kci);
+                dtc += -(Q)4 * kij * sqrt(((Q)2 * tov) * (radij - (Q)0.5 * tov)) * (tempi - D.temp[j]) /
                        ((rhoi * volm) * cpi);
             }
             double dsx = 0, dsy = 0, dsz = 0;
@@ -1016,52 +1008,52 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
                 dsy = D.hds[(slot * 3 + 1) * n + i];
                 dsz = D.hds[(slot * 3 + 2) * n + i];
             }
-            R mj = D.m[j];
-            R nx = (R)((xj - xi) / td), ny = (R)((yj - yi) / td), nz = (R)((zj - zi) / td);
-            R li = radiR - (R)0.5 * tov, lj = radjR - (R)0.5 * tov;
-            R rcxi = li * nx, rcyi = li * ny, rczi = li * nz;
-            R rcxj = -lj * nx, rcyj = -lj * ny, rczj = -lj * nz;
-            R wxj = D.wx[j], wyj = D.wy[j], wzj = D.wz[j];
-            R urxi = wyi * rczi - wzi * rcyi, uryi = wzi * rcxi - wxi * rczi, urzi = wxi * rcyi - wyi * rcxi;
-            R urxj = wyj * rczj - wzj * rcyj, uryj = wzj * rcxj - wxj * rczj, urzj = wxj * rcyj - wyj * rcxj;
-            R urx = (D.ux[j] + urxj) - (uxi + urxi);
-            R ury = (D.uy[j] + uryj) - (uyi + uryi);
-            R urz = (D.uz[j] + urzj) - (uzi + urzi);
-            R unm = nx * urx + ny * ury + nz * urz;
-            R unx = unm * nx, uny = unm * ny, unz = unm * nz;
-            R usx = urx - unx, usy = ury - uny, usz = urz - unz;
+            Q mj = D.m[j];
+            Q nx = (Q)((xj - xi) / td), ny = (Q)((yj - yi) / td), nz = (Q)((zj - zi) / td);
+            Q li = radiR - (Q)0.5 * tov, lj = radjR - (Q)0.5 * tov;
+            Q rcxi = li * nx, rcyi = li * ny, rczi = li * nz;
+            Q rcxj = -lj * nx, rcyj = -lj * ny, rczj = -lj * nz;
+            Q wxj = D.wx[j], wyj = D.wy[j], wzj = D.wz[j];
+            Q urxi = wyi * rczi - wzi * rcyi, uryi = wzi * rcxi - wxi * rczi, urzi = wxi * rcyi - wyi * rcxi;
+            Q urxj = wyj * rczj - wzj * rcyj, uryj = wzj * rcxj - wxj * rczj, urzj = wxj * rcyj - wyj * rcxj;
+            Q urx = (D.ux[j] + urxj) - (uxi + urxi);
+            Q ury = (D.uy[j] + uryj) - (uyi + uryi);
+            Q urz = (D.uz[j] + urzj) - (uzi + urzi);
+            Q unm = nx * urx + ny * ury + nz * urz;
+            Q unx = unm * nx, uny = unm * ny, unz = unm * nz;
+            Q usx = urx - unx, usy = ury - uny, usz = urz - unz;
             dsx += (double)usx * kdt;
             dsy += (double)usy * kdt;
             dsz += (double)usz * kdt;
-            R usm = sqrt(usx * usx + usy * usy + usz * usz) + (R)1e-20;
-            R sx = usx / usm, sy = usy / usm, sz = usz / usm;
-            R mij = (R)1 / ((R)1 / mi + (R)1 / mj);
-            R sq = sqrt(radij * tov);
-            R Cspr = (R)1.33333 * ymij * sqrt(radij) * sqrt(tov) * tov / mi;
-            R Cspr_s = (R)8 * Gij * sq / mi;
-            R Kn = (R)2 * ymij * sq;
-            R Cd = cdamp * sqrt(mij * Kn) / mi;
-            R Cds = cdamp * sqrt(mij * Cspr_s * mi) / mi;
-            tx += Cspr * (R)((xi - xj) / td);
-            ty += Cspr * (R)((yi - yj) / td);
-            tz += Cspr * (R)((zi - zj) / td);
+            Q usm = sqrt(usx * usx + usy * usy + usz * usz) + (Q)1e-20;
+            Q sx = usx / usm, sy = usy / usm, sz = usz / usm;
+            Q mij = (Q)1 / ((Q)1 / mi + (Q)1 / mj);
+            Q sq = sqrt(radij * tov);
+            Q Cspr = (Q)1.33333 * ymij * sqrt(radij) * sqrt(tov) * tov / mi;
+            Q Cspr_s = (Q)8 * Gij * sq / mi;
+            Q Kn = (Q)2 * ymij * sq;
+            Q Cd = cdamp * sqrt(mij * Kn) / mi;
+            Q Cds = cdamp * sqrt(mij * Cspr_s * mi) / mi;
+            tx += Cspr * (Q)((xi - xj) / td);
+            ty += Cspr * (Q)((yi - yj) / td);
+            tz += Cspr * (Q)((zi - zj) / td);
             tx += Cd * unx;
             ty += Cd * uny;
             tz += Cd * unz;
-            R fssx = Cspr_s * (R)dsx + Cds * usx;
-            R fssy = Cspr_s * (R)dsy + Cds * usy;
-            R fssz = Cspr_s * (R)dsz + Cds * usz;
-            R sgx = (fssx >= (R)0) ? (R)1 : (R)-1;
-            R sgy = (fssy >= (R)0) ? (R)1 : (R)-1;
-            R sgz = (fssz >= (R)0) ? (R)1 : (R)-1;
-            R mfss = sqrt(fssx * fssx + fssy * fssy + fssz * fssz);
-            R fr = (R)P.fric * Cspr;
-            R ffx = fr * sx, ffy = fr * sy, ffz = fr * sz;
-            R mfsf = sqrt(ffx * ffx + ffy * ffy + ffz * ffz);
+            Q fssx = Cspr_s * (Q)dsx + Cds * usx;
+            Q fssy = Cspr_s * (Q)dsy + Cds * usy;
+            Q fssz = Cspr_s * (Q)dsz + Cds * usz;
+            Q sgx = (fssx >= (Q)0) ? (Q)1 : (Q)-1;
+            Q sgy = (fssy >= (Q)0) ? (Q)1 : (Q)-1;
+            Q sgz = (fssz >= (Q)0) ? (Q)1 : (Q)-1;
+            Q mfss = sqrt(fssx * fssx + fssy * fssy + fssz * fssz);
+            Q fr = (Q)P.fric * Cspr;
+            Q ffx = fr * sx, ffy = fr * sy, ffz = fr * sz;
+            Q mfsf = sqrt(ffx * ffx + ffy * ffy + ffz * ffz);
             bool stick = mfss < mfsf;
-            R fsx = stick ? fssx : sgx * fabs(ffx);
-            R fsy = stick ? fssy : sgy * fabs(ffy);
-            R fsz = stick ? fssz : sgz * fabs(ffz);
+            Q fsx = stick ? fssx : sgx * fabs(ffx);
+            Q fsy = stick ? fssy : sgy * fabs(ffy);
+            Q fsz = stick ? fssz : sgz * fabs(ffz);
             tx += fsx;
             ty += fsy;
             tz += fsz;
@@ -1110,19 +1102,19 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     tqx = warp_sum(tqx); tqy = warp_sum(tqy); tqz = warp_sum(tqz);
     dtr = warp_sum(dtr); dtc = warp_sum(dtc);
     if (lane != 0) return;
-    if (P.fg) tz += -(R)P.g_dem;
+    if (P.fg) tz += -(Q)P.g_dem;
     if (P.con) {
-        R temp1i = D.temp1[i], temp2i = D.temp2[i], temp3i = D.temp3[i];
-        R a0 = kci / (rhoi * cpi);
-        R dr1 = ((R)5 / (R)6) * radiR / (R)3;
-        R A = ((R)2 * kci / dr1) / ((R)2 * kci / dr1 + kci / dr2), B = (R)1 - A;
-        R ts = A * temp1i + B * tempi;
-        R d0 = (R)2 * (a0 / radiR) * (tempi - ts) / ((R)2 * dr2) + a0 * (tempi - (R)2 * tempi + ts) / (dr2 * dr2);
-        R d1 = ((R)2 * a0 / ((R)2.5 * dr1)) * ((R)2 * ts - temp1i - temp2i) / ((R)2 * dr1) +
-               a0 * ((R)2 * ts - (R)3 * temp1i + temp2i) / (dr1 * dr1);
-        R d2 = (R)2 * (a0 / ((R)1.5 * dr1)) * (temp1i - temp3i) / ((R)2 * dr1) +
-               a0 * (temp1i - (R)2 * temp2i + temp3i) / (dr1 * dr1);
-        R d3 = (R)2 * (a0 / ((R)0.5 * dr1)) * ((temp2i - temp3i) / ((R)2 * dr1)) + a0 * (temp2i - temp3i) / (dr1 * dr1);
+        Q temp1i = D.temp1[i], temp2i = D.temp2[i], temp3i = D.temp3[i];
+        Q a0 = kci / (rhoi * cpi);
+        Q dr1 = ((Q)5 / (Q)6) * radiR / (Q)3;
+        Q A = ((Q)2 * kci / dr1) / ((Q)2 * kci / dr1 + kci / dr2), B = (Q)1 - A;
+        Q ts = A * temp1i + B * tempi;
+        Q d0 = (Q)2 * (a0 / radiR) * (tempi - ts) / ((Q)2 * dr2) + a0 * (tempi - (Q)2 * tempi + ts) / (dr2 * dr2);
+        Q d1 = ((Q)2 * a0 / ((Q)2.5 * dr1)) * ((Q)2 * ts - temp1i - temp2i) / ((Q)2 * dr1) +
+               a0 * ((Q)2 * ts - (Q)3 * temp1i + temp2i) / (dr1 * dr1);
+        Q d2 = (Q)2 * (a0 / ((Q)1.5 * dr1)) * (temp1i - temp3i) / ((Q)2 * dr1) +
+               a0 * (temp1i - (Q)2 * temp2i + temp3i) / (dr1 * dr1);
+        Q d3 = (Q)2 * (a0 / ((Q)0.5 * dr1)) * ((temp2i - temp3i) / ((Q)2 * dr1)) + a0 * (temp2i - temp3i) / (dr1 * dr1);
         DW.dtemp[i] = d0 + dtr + dtc;
         DW.dtemp1[i] = d1;
         DW.dtemp2[i] = d2;
@@ -1147,6 +1139,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
 template <typename R>
 struct DcSums {
     R tx, ty, tz, ufx, ufy, ufz, uax, uay, uaz, por, ttf, tta;
+    R wtf, wta;   // the weights of ttf/tta: their SPH temperatures are stored as T - t_ref
     int has_f, has_a;
 };
 
@@ -1167,10 +1160,12 @@ __device__ __forceinline__ void dc_pair(const SphWork<R>& W, const Knl<R>& K, R 
             a.has_f = 1;
             a.ufx += uj.x * c; a.ufy += uj.y * c; a.ufz += uj.z * c;
             a.ttf += fj.z * c;
+            a.wtf += c;
         } else {
             a.has_a = 1;
             a.uax += uj.x * c; a.uay += uj.y * c; a.uaz += uj.z * c;
             a.tta += fj.z * c;
+            a.wta += c;
         }
         a.por += porj * c;
     }
@@ -1188,6 +1183,7 @@ __device__ __forceinline__ void dc_warp_sum(DcSums<R>& a) {
     a.ufx = warp_sum(a.ufx); a.ufy = warp_sum(a.ufy); a.ufz = warp_sum(a.ufz);
     a.uax = warp_sum(a.uax); a.uay = warp_sum(a.uay); a.uaz = warp_sum(a.uaz);
     a.por = warp_sum(a.por); a.ttf = warp_sum(a.ttf); a.tta = warp_sum(a.tta);
+    a.wtf = warp_sum(a.wtf); a.wta = warp_sum(a.wta);
     a.has_f = __any_sync(0xffffffffu, a.has_f);
     a.has_a = __any_sync(0xffffffffu, a.has_a);
 }
@@ -1213,12 +1209,15 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<R>& D, DemWork<
         R eps = (R)1.0e-15;
         R pori = por / (ff + eps);
         R ux_f = ufx / (ff + eps) - uxi, uy_f = ufy / (ff + eps) - uyi, uz_f = ufz / (ff + eps) - uzi;
-        R tf = ttf / (ff + eps) - tempi;
+        // the SPH temperatures in ttf/tta are stored as T - t_ref: absolute sums
+        const R tr = (R)P.t_ref;
+        const R ttfa = ttf + tr * a.wtf, ttaa = tta + tr * a.wta;
+        R tf = ttfa / (ff + eps) - tempi;
         R ux_a = uax / (fa + eps) - uxi, uy_a = uay / (fa + eps) - uyi, uz_a = uaz / (fa + eps) - uzi;
-        R ta = tta / (fa + eps) - tempi;
+        R ta = ttaa / (fa + eps) - tempi;
         R ux_fa = (ufx + uax) / (ff + fa + eps) - uxi, uy_fa = (ufy + uay) / (ff + fa + eps) - uyi,
           uz_fa = (ufz + uaz) / (ff + fa + eps) - uzi;
-        R tfa = (ttf + tta) / (ff + fa + eps) - tempi;
+        R tfa = (ttfa + ttaa) / (ff + fa + eps) - tempi;
         R f_fluid = ff / (ff + fa + eps), f_air = fa / (ff + fa + eps);
         R mf = sqrt(ux_f * ux_f + uy_f * uy_f + uz_f * uz_f);
         DW.magf[i] = mf;
@@ -1360,7 +1359,7 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
         R rhoi = W.rho_new[i], tempi = S.temp[i];
         // heat_capacity(ptypei, tempi): the reference passes the arguments
         // swapped (functions_SPH_DEM_COUPLING2.cuh:1860)
-        R cpi = (abs((int)tempi) > 1000) ? (R)P.cp_dem : (R)P.cp_sph;
+        R cpi = (abs((int)(tempi + (R)P.t_ref)) > 1000) ? (R)P.cp_dem : (R)P.cp_sph;   // stored T - t_ref
         R th = (R)hi;
         Knl<R> K = knl_make<R>(P, th);
         double Rr = P.kappa * hi;
@@ -1989,7 +1988,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
         uz = (R)P.inlet_uz * (R)2 - tuz / flt;
         ux = (R)0 - tux / flt;
         uy = (R)0 - tuy / flt;
-        tn = (R)P.inlet_temp;
+        tn = (R)(P.inlet_temp - P.t_ref);   // stored T - t_ref
     } else {
         pn = (R)0;
         rn = pori * (trho / flt);

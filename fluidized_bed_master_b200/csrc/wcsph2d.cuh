@@ -90,16 +90,24 @@ __device__ __forceinline__ double w_dist(double xi, double yi, double xj, double
 // KERNEL_clc_predictor, Lagrangian (ALE flags 1), no MOVING particles,
 // fused with the NNPS cell key of the predicted position
 // (KERNEL_index_particle_to_cell, functions_NNPS.cuh:732-760): key[i],
-// val[i] = i, i_type 3 -> num_cells
+// i_type 3 -> num_cells; the cell-sort count (cell_count) is fused in
 template <typename R>
-__global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W, int* key, int* val) {
+__device__ __forceinline__ int w_predict(const DevParams& P, const WParams& Q, WState<R>& S, WWork<R>& W, int i);
+
+template <typename R>
+__global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W, int* key, int* cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ns) return;
-    val[i] = i;
-    if (S.itype[i] == 3) {
-        key[i] = P.num_cells;
-        return;
+    int k = -1;
+    if (i < P.ns) {
+        k = (S.itype[i] == 3) ? P.num_cells : w_predict<R>(P, Q, S, W, i);
+        key[i] = k;
     }
+    cell_count(cnt, k);
+}
+
+// predictor of slot i (i_type != 3); returns the cell key of the predicted position
+template <typename R>
+__device__ __forceinline__ int w_predict(const DevParams& P, const WParams& Q, WState<R>& S, WWork<R>& W, int i) {
     int pt = S.ptype[i], bt = S.btype[i];
     double x0 = S.x[i], y0 = S.y[i];
     R ux0 = S.ux[i], uy0 = S.uy[i];
@@ -124,7 +132,7 @@ __global__ void k_w_predictor(DevParams P, WParams Q, WState<R> S, WWork<R> W, i
     int ic, jc, kc;
     const double2 o = w_cell_off(S, i);
     cell_ijk(P, xp + o.x, yp + o.y, S.z[i], ic, jc, kc);
-    key[i] = ic + P.NI * jc + P.NI * P.NJ * kc;
+    return ic + P.NI * jc + P.NI * P.NJ * kc;
 }
 
 // ---- lanes per particle ------------------------------------------------
@@ -494,17 +502,10 @@ __global__ void k_w_finish(DevParams P, WState<R> S, WWork<R> W) {
 
 // cell gather of the WCSPH state
 template <typename R>
-__global__ void k_w_gather(DevParams P, WState<R> src, WState<R> dst, const int* __restrict__ key,
-                           const int* __restrict__ perm, int* gs, int* ge) {
+__global__ void k_w_gather(DevParams P, WState<R> src, WState<R> dst, const int* __restrict__ perm) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
-    int k = key[i];
-    if (i == 0 || k != key[i - 1]) {
-        if (k < P.num_cells) gs[k] = i;
-        if (i > 0 && key[i - 1] < P.num_cells) ge[key[i - 1]] = i;
-    }
-    if (i == n - 1 && k < P.num_cells) ge[k] = n;
     int p = perm[i];
     dst.x[i] = src.x[p]; dst.y[i] = src.y[p]; dst.z[i] = src.z[p]; dst.h[i] = src.h[p];
     dst.ux[i] = src.ux[p]; dst.uy[i] = src.uy[p]; dst.m[i] = src.m[p]; dst.rho[i] = src.rho[p];
@@ -518,18 +519,21 @@ __global__ void k_w_gather(DevParams P, WState<R> src, WState<R> dst, const int*
 // cell key of the state as it stands (the first NNPS at commit; in a step
 // the predictor writes the keys): KERNEL_index_particle_to_cell
 template <typename R>
-__global__ void k_w_hash(DevParams P, WState<R> S, int* key, int* val) {
+__global__ void k_w_hash(DevParams P, WState<R> S, int* key, int* cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ns) return;
-    val[i] = i;
-    if (S.itype[i] == 3) {
-        key[i] = P.num_cells;
-        return;
+    int k = -1;
+    if (i < P.ns) {
+        if (S.itype[i] == 3) {
+            k = P.num_cells;
+        } else {
+            int ic, jc, kc;
+            const double2 o = w_cell_off(S, i);
+            cell_ijk(P, S.x[i] + o.x, S.y[i] + o.y, S.z[i], ic, jc, kc);
+            k = ic + P.NI * jc + P.NI * P.NJ * kc;
+        }
+        key[i] = k;
     }
-    int ic, jc, kc;
-    const double2 o = w_cell_off(S, i);
-    cell_ijk(P, S.x[i] + o.x, S.y[i] + o.y, S.z[i], ic, jc, kc);
-    key[i] = ic + P.NI * jc + P.NI * P.NJ * kc;
+    cell_count(cnt, k);
 }
 
 }  // namespace sphdem
