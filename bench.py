@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="bed", choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column"],
+    ap.add_argument("--workload", default="bed",
+                    choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column", "mlp"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
                          "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
                          "against the same beds run one after another; ppe-profile: --steps steps of the bed with the "
@@ -1131,6 +1132,68 @@ def precision_keys(args, seed):
     return fp64, cmp
 
 
+MLP_FWD_FLOP = 2 * (16 * 64 + 64 * 64 + 64)            # per row: 16->64->64->1
+MLP_GRAD_FLOP = MLP_FWD_FLOP + 2 * (64 * 64 + 64 * 64 + 16 * 64 + 64)   # + dH1, dW2, dW1, output layer
+
+
+def run_mlp(args):
+    """--workload mlp: the learned warm start's tcgen05 kernels on the scaled
+    bed's row count (2,827,520 rows of 16 BF16 features), through the C ABI
+    (sphdem_mlp_forward / sphdem_mlp_grad on device arrays); each call's
+    kernel time comes from CUDA events around its launch (sphdem_mlp_last_ms).
+    Dense BF16 tensor-core work: 10,368 FLOP per row forward, 29,120 per row
+    for the gradient pass, against the measured cuBLAS BF16 peak."""
+    import ctypes as C
+
+    import torch
+
+    from fluidized_bed_master_b200.engine import lib
+
+    L = lib()
+    L.sphdem_mlp_param_count.restype = C.c_int32
+    L.sphdem_mlp_forward.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sphdem_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_double,
+                                  C.c_void_p, C.c_void_p]
+    L.sphdem_mlp_last_ms.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    n = 2_827_520
+    g = torch.Generator(device="cpu").manual_seed(3)
+    feat = torch.randn(n, 16, generator=g).to(torch.bfloat16).cuda()
+    npar = L.sphdem_mlp_param_count()
+    params = (0.2 * torch.randn(npar, generator=g)).float().cuda()
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    target = torch.randn(n, generator=g).float().cuda()
+    weight = torch.ones(n, dtype=torch.float32, device="cuda")
+    grad = torch.empty(npar + 2, dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    fwd, grd = C.c_double(), C.c_double()
+    tf, tg = [], []
+    for k in range(args.warmup + args.steps):
+        r = L.sphdem_mlp_forward(feat.data_ptr(), n, params.data_ptr(), out.data_ptr(), st)
+        r |= L.sphdem_mlp_grad(feat.data_ptr(), target.data_ptr(), weight.data_ptr(), n, params.data_ptr(),
+                               float(n), grad.data_ptr(), st)
+        if r:
+            raise RuntimeError(f"mlp entry returned {r}")
+        L.sphdem_mlp_last_ms(C.byref(fwd), C.byref(grd))
+        if k >= args.warmup:
+            tf.append(fwd.value)
+            tg.append(grd.value)
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops") if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
+    mf, mg = float(np.median(tf)), float(np.median(tg))
+    tff = MLP_FWD_FLOP * n / (mf / 1e3) / 1e12
+    tfg = MLP_GRAD_FLOP * n / (mg / 1e3) / 1e12
+    line = {"metric": "learned warm start network: rows/s through the tcgen05 kernels", "value": n / (mf / 1e3),
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded normal features)",
+            "config": {"workload": "MLP 16->64->64->1 on 2,827,520 rows (the scaled bed's SPH count)"},
+            "forward": {"ms": mf, "tflops": tff, "frac_of_bf16_peak": tff / peak},
+            "grad": {"ms": mg, "tflops": tfg, "frac_of_bf16_peak": tfg / peak},
+            "roofline": {"bound": "tensor", "achieved": tff, "peak": peak, "unit": "TFLOP/s", "frac": tff / peak,
+                         "traffic": None, "kernel": "k_mlp_infer"},
+            "how": "median over the timed calls of the CUDA-event time around each kernel launch"}
+    print(json.dumps(line), flush=True)
+
+
 def ppe_comparison(args):
     """PPE ms/step and iterations at a relative residual of 1e-6 on the same
     bed, for four initial iterates of the same Jacobi-PCG (and three of them
@@ -1224,6 +1287,9 @@ def main():
             run_dam2d_batch(args, world, rank, local, pg)
         elif args.workload == "column":
             run_column(args, world, rank, local, pg)
+        elif args.workload == "mlp":
+            if rank == 0:
+                run_mlp(args)
         elif args.workload == "ppe-profile":
             if rank == 0:
                 run_ppe_profile(args)

@@ -132,7 +132,7 @@ void alloc_sph_state(Alloc& A, SphState<R>& S, int n) {
 }
 
 template <typename R>
-void alloc_dem_state(Alloc& A, DemState<R>& D, int n) {
+void alloc_dem_state(Alloc& A, DemState<double>& D, int n) {
     D.x = A.get<double>(n); D.y = A.get<double>(n); D.z = A.get<double>(n); D.h = A.get<double>(n);
     D.rad = A.get<double>(n);
     D.ux = A.get<R>(n); D.uy = A.get<R>(n); D.uz = A.get<R>(n);
@@ -147,7 +147,7 @@ void alloc_dem_state(Alloc& A, DemState<R>& D, int n) {
 }
 
 template <typename R>
-void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int ncells) {
+void alloc_work(Alloc& A, SphWork<R>& W, DemWork<double>& DW, int ns, int nd, int ncells) {
     W.m_new = A.get<R>(ns); W.rho_new = A.get<R>(ns); W.rho_ref = A.get<R>(ns); W.DEMpor = A.get<R>(ns);
     W.dDEMpor_prev = A.get<R>(ns);
     W.Cm = A.get<R>((size_t)ns * 9);
@@ -171,14 +171,14 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<R>& DW, int ns, int nd, int nce
     W.rec.f1 = A.get<V4<R>>(ns);
     W.rec.up = A.get<V4<R>>(ns);
     W.rec.ut = A.get<V4<R>>(ns);
-    DW.flt_s = A.get<R>(nd); DW.flt_sd = A.get<R>(nd); DW.flt_sd2 = A.get<R>(nd); DW.DEMpor = A.get<R>(nd);
-    DW.ftx = A.get<R>(nd); DW.fty = A.get<R>(nd); DW.ftz = A.get<R>(nd);
-    DW.tqx = A.get<R>(nd); DW.tqy = A.get<R>(nd); DW.tqz = A.get<R>(nd);
-    DW.dtemp = A.get<R>(nd); DW.dtemp1 = A.get<R>(nd); DW.dtemp2 = A.get<R>(nd); DW.dtemp3 = A.get<R>(nd);
-    DW.Fdx_b = A.get<R>(nd); DW.Fdy_b = A.get<R>(nd); DW.Fdz_b = A.get<R>(nd);
-    DW.Fdx_da = A.get<R>(nd); DW.Fdy_da = A.get<R>(nd); DW.Fdz_da = A.get<R>(nd);
-    DW.ux0 = A.get<R>(nd); DW.uy0 = A.get<R>(nd); DW.uz0 = A.get<R>(nd); DW.temp0 = A.get<R>(nd);
-    DW.magf = A.get<R>(nd);
+    DW.flt_s = A.get<double>(nd); DW.flt_sd = A.get<double>(nd); DW.flt_sd2 = A.get<double>(nd); DW.DEMpor = A.get<double>(nd);
+    DW.ftx = A.get<double>(nd); DW.fty = A.get<double>(nd); DW.ftz = A.get<double>(nd);
+    DW.tqx = A.get<double>(nd); DW.tqy = A.get<double>(nd); DW.tqz = A.get<double>(nd);
+    DW.dtemp = A.get<double>(nd); DW.dtemp1 = A.get<double>(nd); DW.dtemp2 = A.get<double>(nd); DW.dtemp3 = A.get<double>(nd);
+    DW.Fdx_b = A.get<double>(nd); DW.Fdy_b = A.get<double>(nd); DW.Fdz_b = A.get<double>(nd);
+    DW.Fdx_da = A.get<double>(nd); DW.Fdy_da = A.get<double>(nd); DW.Fdz_da = A.get<double>(nd);
+    DW.ux0 = A.get<double>(nd); DW.uy0 = A.get<double>(nd); DW.uz0 = A.get<double>(nd); DW.temp0 = A.get<double>(nd);
+    DW.magf = A.get<double>(nd);
     DW.key_in = A.get<int>(nd); DW.key_out = A.get<int>(nd); DW.val_in = nullptr; DW.val_out = A.get<int>(nd);
     DW.g_str = A.get<int>(ncells + 1); DW.g_end = A.get<int>(ncells + 1);
     DW.rows = A.get<int4>(ncells);
@@ -257,7 +257,7 @@ template <typename R>
 int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) {
     Engine<R>& E = EH->E;
     DevParams& P = E.P;
-    DemWork<R>& DW = E.dw;
+    DemWork<double>& DW = E.dw;
     cudaStream_t st = H->stream;
     int n = P.nd;
     if (n == 0) {
@@ -265,7 +265,7 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
         CK(cudaMemsetAsync(DW.rows, 0, sizeof(int4) * P.NI * P.NJ * P.NK, st));
         return SPHDEM_OK;
     }
-    DemState<R>& D = E.D[src];
+    DemState<double>& D = E.D[src];
     {
         KTIME(KT_HASH_D);
         k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, E.cs_d.cnt);
@@ -276,7 +276,7 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     }
     {
         KTIME(KT_GATHER_D);
-        k_cells_gather_dem<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.val_out);
+        k_cells_gather_dem<double><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.val_out);
         k_gather_history<<<nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st>>>(n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
                                                                          E.D[dst].hds);
     }
@@ -492,7 +492,7 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
 
 // SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
 template <typename R>
-void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<R>& D, cudaStream_t st) {
+void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double>& D, cudaStream_t st) {
     Engine<R>& E = EH->E;
     const DevParams& P = E.P;
     const int ncell = P.NI * P.NJ * P.NK;
@@ -512,7 +512,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     Engine<R>& E = EH->E;
     DevParams& P = E.P;
     SphWork<R>& W = E.sw;
-    DemWork<R>& DW = E.dw;
+    DemWork<double>& DW = E.dw;
     cudaStream_t st = H->stream;
     int ns = P.ns, nd = P.nd;
     int so = E.cur_s, sn = 1 - E.cur_s, dox = E.cur_d, dn = 1 - E.cur_d;
@@ -520,7 +520,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if ((r = nnps_sph<R>(H, EH, so, sn, nl))) return r;
     if ((r = nnps_dem<R>(H, EH, dox, dn, nl))) return r;
     SphState<R>& S = E.S[sn];
-    DemState<R>& D = E.D[dn];
+    DemState<double>& D = E.D[dn];
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
     if (ns > 0) {
@@ -553,7 +553,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 1;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
+        { KTIME(KT_DEMCONTACT); k_dem_contact<double><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
         { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows); }
         *nl += 2;
     }
@@ -585,7 +585,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 4;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMUPDATE); k_dem_update<R><<<bd, TPB, 0, st>>>(P, D, DW); }
+        { KTIME(KT_DEMUPDATE); k_dem_update<double><<<bd, TPB, 0, st>>>(P, D, DW); }
         *nl += 1;
     }
     if (ns > 0) {
@@ -748,7 +748,7 @@ static int commit_t(SphdemHandle* H) {
 
     Alloc& A = EH->A;
     alloc_sph_state<R>(A, E.S[0], ns); alloc_sph_state<R>(A, E.S[1], ns);
-    alloc_dem_state<R>(A, E.D[0], nd); alloc_dem_state<R>(A, E.D[1], nd);
+    alloc_dem_state<double>(A, E.D[0], nd); alloc_dem_state<double>(A, E.D[1], nd);
     alloc_work<R>(A, E.sw, E.dw, ns, nd, num_cells);
     E.flags = A.get<DevFlags>(1);
     E.red_buf = A.get<double>(8);
@@ -834,16 +834,16 @@ static int commit_t(SphdemHandle* H) {
     r |= up_r(W.p_new, 0, SPHDEM_F_PRES, ns);
     r |= up_r(W.u_tmpx, 0, SPHDEM_F_UX, ns); r |= up_r(W.u_tmpy, 0, SPHDEM_F_UY, ns);
     r |= up_r(W.u_tmpz, 0, SPHDEM_F_UZ, ns); r |= up_r(W.temp_tmp, 0, SPHDEM_F_TEMP, ns);
-    DemState<R>& D = E.D[0];
+    DemState<double>& D = E.D[0];
     r |= up_d(D.x, 1, SPHDEM_F_X, nd); r |= up_d(D.y, 1, SPHDEM_F_Y, nd); r |= up_d(D.z, 1, SPHDEM_F_Z, nd);
     r |= up_d(D.h, 1, SPHDEM_F_H, nd); r |= up_d(D.rad, 1, SPHDEM_F_RAD, nd);
-    r |= up_r(D.ux, 1, SPHDEM_F_UX, nd); r |= up_r(D.uy, 1, SPHDEM_F_UY, nd); r |= up_r(D.uz, 1, SPHDEM_F_UZ, nd);
-    r |= up_r(D.wx, 1, SPHDEM_F_WX, nd); r |= up_r(D.wy, 1, SPHDEM_F_WY, nd); r |= up_r(D.wz, 1, SPHDEM_F_WZ, nd);
-    r |= up_r(D.m, 1, SPHDEM_F_M, nd); r |= up_r(D.rho, 1, SPHDEM_F_RHO, nd); r |= up_r(D.ri, 1, SPHDEM_F_RI, nd);
-    r |= up_r(D.temp, 1, SPHDEM_F_TEMP, nd); r |= up_r(D.temp1, 1, SPHDEM_F_TEMP1, nd);
-    r |= up_r(D.temp2, 1, SPHDEM_F_TEMP2, nd); r |= up_r(D.temp3, 1, SPHDEM_F_TEMP3, nd);
-    r |= up_r(D.Fdx_df, 1, SPHDEM_F_FDX_DF, nd); r |= up_r(D.Fdy_df, 1, SPHDEM_F_FDY_DF, nd);
-    r |= up_r(D.Fdz_df, 1, SPHDEM_F_FDZ_DF, nd); r |= up_r(D.Q_sd, 1, SPHDEM_F_Q_SD, nd);
+    r |= up_d(D.ux, 1, SPHDEM_F_UX, nd); r |= up_d(D.uy, 1, SPHDEM_F_UY, nd); r |= up_d(D.uz, 1, SPHDEM_F_UZ, nd);
+    r |= up_d(D.wx, 1, SPHDEM_F_WX, nd); r |= up_d(D.wy, 1, SPHDEM_F_WY, nd); r |= up_d(D.wz, 1, SPHDEM_F_WZ, nd);
+    r |= up_d(D.m, 1, SPHDEM_F_M, nd); r |= up_d(D.rho, 1, SPHDEM_F_RHO, nd); r |= up_d(D.ri, 1, SPHDEM_F_RI, nd);
+    r |= up_d(D.temp, 1, SPHDEM_F_TEMP, nd); r |= up_d(D.temp1, 1, SPHDEM_F_TEMP1, nd);
+    r |= up_d(D.temp2, 1, SPHDEM_F_TEMP2, nd); r |= up_d(D.temp3, 1, SPHDEM_F_TEMP3, nd);
+    r |= up_d(D.Fdx_df, 1, SPHDEM_F_FDX_DF, nd); r |= up_d(D.Fdy_df, 1, SPHDEM_F_FDY_DF, nd);
+    r |= up_d(D.Fdz_df, 1, SPHDEM_F_FDZ_DF, nd); r |= up_d(D.Q_sd, 1, SPHDEM_F_Q_SD, nd);
     r |= up_i(D.ptype, 1, SPHDEM_F_PTYPE, nd); r |= up_i(D.btype, 1, SPHDEM_F_BUFFER_TYPE, nd);
     r |= up_i(D.itype, 1, SPHDEM_F_ITYPE, nd); r |= up_i(D.pid, 1, SPHDEM_F_PID, nd);
     r |= up_i(D.dem_idx, 1, SPHDEM_F_DEM_IDX, nd);
@@ -999,42 +999,42 @@ static int field_ptr(SphdemHandle* H, int which, int field, const void** ptr, in
         case SPHDEM_F_CELL: *ptr = W.key_out; *kind = 2; return 0;
         }
     } else {
-        DemState<R>& D = E.D[E.cur_d];
-        DemWork<R>& DW = E.dw;
+        DemState<double>& D = E.D[E.cur_d];
+        DemWork<double>& DW = E.dw;
         switch (field) {
         case SPHDEM_F_X: *ptr = D.x; *kind = 0; return 0;
         case SPHDEM_F_Y: *ptr = D.y; *kind = 0; return 0;
         case SPHDEM_F_Z: *ptr = D.z; *kind = 0; return 0;
         case SPHDEM_F_H: *ptr = D.h; *kind = 0; return 0;
         case SPHDEM_F_RAD: *ptr = D.rad; *kind = 0; return 0;
-        case SPHDEM_F_UX: *ptr = D.ux; *kind = 1; return 0;
-        case SPHDEM_F_UY: *ptr = D.uy; *kind = 1; return 0;
-        case SPHDEM_F_UZ: *ptr = D.uz; *kind = 1; return 0;
-        case SPHDEM_F_WX: *ptr = D.wx; *kind = 1; return 0;
-        case SPHDEM_F_WY: *ptr = D.wy; *kind = 1; return 0;
-        case SPHDEM_F_WZ: *ptr = D.wz; *kind = 1; return 0;
-        case SPHDEM_F_M: *ptr = D.m; *kind = 1; return 0;
-        case SPHDEM_F_RHO: *ptr = D.rho; *kind = 1; return 0;
-        case SPHDEM_F_RI: *ptr = D.ri; *kind = 1; return 0;
-        case SPHDEM_F_TEMP: *ptr = D.temp; *kind = 1; return 0;
-        case SPHDEM_F_TEMP1: *ptr = D.temp1; *kind = 1; return 0;
-        case SPHDEM_F_TEMP2: *ptr = D.temp2; *kind = 1; return 0;
-        case SPHDEM_F_TEMP3: *ptr = D.temp3; *kind = 1; return 0;
-        case SPHDEM_F_FDX_DF: *ptr = D.Fdx_df; *kind = 1; return 0;
-        case SPHDEM_F_FDY_DF: *ptr = D.Fdy_df; *kind = 1; return 0;
-        case SPHDEM_F_FDZ_DF: *ptr = D.Fdz_df; *kind = 1; return 0;
-        case SPHDEM_F_Q_SD: *ptr = D.Q_sd; *kind = 1; return 0;
-        case SPHDEM_F_DEMPOR: *ptr = DW.DEMpor; *kind = 1; return 0;
-        case SPHDEM_F_FLT_S: *ptr = DW.flt_s; *kind = 1; return 0;
-        case SPHDEM_F_FLT_SD: *ptr = DW.flt_sd; *kind = 1; return 0;
-        case SPHDEM_F_FLT_SD2: *ptr = DW.flt_sd2; *kind = 1; return 0;
-        case SPHDEM_F_FTOTALX: *ptr = DW.ftx; *kind = 1; return 0;
-        case SPHDEM_F_FTOTALY: *ptr = DW.fty; *kind = 1; return 0;
-        case SPHDEM_F_FTOTALZ: *ptr = DW.ftz; *kind = 1; return 0;
-        case SPHDEM_F_TORQX: *ptr = DW.tqx; *kind = 1; return 0;
-        case SPHDEM_F_TORQY: *ptr = DW.tqy; *kind = 1; return 0;
-        case SPHDEM_F_TORQZ: *ptr = DW.tqz; *kind = 1; return 0;
-        case SPHDEM_F_DTEMP: *ptr = DW.dtemp; *kind = 1; return 0;
+        case SPHDEM_F_UX: *ptr = D.ux; *kind = 0; return 0;
+        case SPHDEM_F_UY: *ptr = D.uy; *kind = 0; return 0;
+        case SPHDEM_F_UZ: *ptr = D.uz; *kind = 0; return 0;
+        case SPHDEM_F_WX: *ptr = D.wx; *kind = 0; return 0;
+        case SPHDEM_F_WY: *ptr = D.wy; *kind = 0; return 0;
+        case SPHDEM_F_WZ: *ptr = D.wz; *kind = 0; return 0;
+        case SPHDEM_F_M: *ptr = D.m; *kind = 0; return 0;
+        case SPHDEM_F_RHO: *ptr = D.rho; *kind = 0; return 0;
+        case SPHDEM_F_RI: *ptr = D.ri; *kind = 0; return 0;
+        case SPHDEM_F_TEMP: *ptr = D.temp; *kind = 0; return 0;
+        case SPHDEM_F_TEMP1: *ptr = D.temp1; *kind = 0; return 0;
+        case SPHDEM_F_TEMP2: *ptr = D.temp2; *kind = 0; return 0;
+        case SPHDEM_F_TEMP3: *ptr = D.temp3; *kind = 0; return 0;
+        case SPHDEM_F_FDX_DF: *ptr = D.Fdx_df; *kind = 0; return 0;
+        case SPHDEM_F_FDY_DF: *ptr = D.Fdy_df; *kind = 0; return 0;
+        case SPHDEM_F_FDZ_DF: *ptr = D.Fdz_df; *kind = 0; return 0;
+        case SPHDEM_F_Q_SD: *ptr = D.Q_sd; *kind = 0; return 0;
+        case SPHDEM_F_DEMPOR: *ptr = DW.DEMpor; *kind = 0; return 0;
+        case SPHDEM_F_FLT_S: *ptr = DW.flt_s; *kind = 0; return 0;
+        case SPHDEM_F_FLT_SD: *ptr = DW.flt_sd; *kind = 0; return 0;
+        case SPHDEM_F_FLT_SD2: *ptr = DW.flt_sd2; *kind = 0; return 0;
+        case SPHDEM_F_FTOTALX: *ptr = DW.ftx; *kind = 0; return 0;
+        case SPHDEM_F_FTOTALY: *ptr = DW.fty; *kind = 0; return 0;
+        case SPHDEM_F_FTOTALZ: *ptr = DW.ftz; *kind = 0; return 0;
+        case SPHDEM_F_TORQX: *ptr = DW.tqx; *kind = 0; return 0;
+        case SPHDEM_F_TORQY: *ptr = DW.tqy; *kind = 0; return 0;
+        case SPHDEM_F_TORQZ: *ptr = DW.tqz; *kind = 0; return 0;
+        case SPHDEM_F_DTEMP: *ptr = DW.dtemp; *kind = 0; return 0;
         case SPHDEM_F_PTYPE: *ptr = D.ptype; *kind = 2; return 0;
         case SPHDEM_F_ITYPE: *ptr = D.itype; *kind = 2; return 0;
         case SPHDEM_F_BUFFER_TYPE: *ptr = D.btype; *kind = 2; return 0;
@@ -1073,7 +1073,7 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
     cudaStream_t st = H->stream;
     SphState<R>& S = E.S[E.cur_s];
     SphWork<R>& W = E.sw;
-    DemState<R>& D = E.D[E.cur_d];
+    DemState<double>& D = E.D[E.cur_d];
     double hb[8] = {0};
     if (P.ns > 0) {
         CK(cudaMemsetAsync(E.red_buf, 0, sizeof(double) * 3, st));
@@ -1085,7 +1085,7 @@ static int stats_t(SphdemHandle* H, SphdemStats* out) {
     }
     if (P.nd > 0) {
         CK(cudaMemsetAsync(E.red_buf, 0, sizeof(double) * 3, st));
-        k_stats<R><<<std::min(nblocks(P.nd, 256), 592), 256, 0, st>>>(P.nd, D.rho, D.ux, D.uy, D.uz, (const R*)nullptr, D.ptype, D.itype, E.red_buf,
+        k_stats<double><<<std::min(nblocks(P.nd, 256), 592), 256, 0, st>>>(P.nd, D.rho, D.ux, D.uy, D.uz, (const double*)nullptr, D.ptype, D.itype, E.red_buf,
                                       E.flags);
         CK(cudaMemcpyAsync(hb, E.red_buf, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -2077,7 +2077,7 @@ __global__ void k_hist_in(int n, const int* __restrict__ ids, const double* __re
 template <typename R>
 static int history_t(SphdemHandle* H, int32_t* ids, double* sp, bool set) {
     EngineHost<R>* EH = (EngineHost<R>*)H->eng;
-    DemState<R>& D = EH->E.D[EH->E.cur_d];
+    DemState<double>& D = EH->E.D[EH->E.cur_d];
     int n = H->nd;
     if (n == 0) return SPHDEM_OK;
     size_t m = (size_t)n * SPHDEM_NSLOT;
@@ -2241,12 +2241,36 @@ extern "C" int sphdem_write_vtk_dem(SphdemHandle* h, const char* path) {
             if (download_real<double>(magf.data(), EH->E.dw.magf, n, h->stream)) return SPHDEM_E_CUDA;
         } else {
             auto* EH = (EngineHost<float>*)h->eng;
-            if (download_real<float>(magf.data(), EH->E.dw.magf, n, h->stream)) return SPHDEM_E_CUDA;
+            if (download_real<double>(magf.data(), EH->E.dw.magf, n, h->stream)) return SPHDEM_E_CUDA;
         }
     }
     return sphdem_io_write_vtk_dem(path, n, x.data(), y.data(), z.data(), itype.data(), ptype.data(), idx.data(),
                                    magf.data(), eliz.data(), por.data(), uz.data(), qsd.data(), ftz.data(),
                                    temp.data(), rad.data(), dtemp.data());
+}
+
+extern "C" int sphdem_write_vtk_fluid(SphdemHandle* h, const char* path) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
+    if (!h || !path || !h->committed) return SPHDEM_E_ARG;
+    int n = h->ns;
+    std::vector<double> x(n), y(n), z(n), por(n), pres(n), dtemp(n), rho(n), temp(n), uz(n);
+    std::vector<int> ptype(n), btype(n);
+    size_t bd = sizeof(double) * n, bi = sizeof(int) * n;
+    int r = 0;
+    r |= sphdem_get_field(h, 0, SPHDEM_F_X, x.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_Y, y.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_Z, z.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_DEMPOR, por.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_PRES, pres.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_DTEMP, dtemp.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_RHO, rho.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_TEMP, temp.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_UZ, uz.data(), bd);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_PTYPE, ptype.data(), bi);
+    r |= sphdem_get_field(h, 0, SPHDEM_F_BUFFER_TYPE, btype.data(), bi);
+    if (r) return SPHDEM_E_CUDA;
+    return sphdem_io_write_vtk_fluid(path, n, ptype.data(), x.data(), y.data(), z.data(), por.data(), pres.data(),
+                                     dtemp.data(), btype.data(), rho.data(), temp.data(), uz.data());
 }
 
 extern "C" int sphdem_write_restart(SphdemHandle* h, const char* path) {

@@ -2,7 +2,11 @@
 //
 // Layout in HBM (structure of arrays, one array per field, cell-sorted):
 //   positions, smoothing length and DEM radius: double
-//   every other field: R (float in the FP32 build, double in the FP64 one)
+//   the DEM set (state and work arrays): double in both builds -- it is
+//     small (spheres are ~6 % of the particles), and its stiff contacts
+//     amplify rounding in the tangential and angular terms
+//   every other field: R (float in the FP32 build, double in the FP64 one);
+//     the SPH temperature is stored as T - DevParams::t_ref
 //   DEM contact history: SPHDEM_NSLOT slot-major planes, partner id int32
 //     and tangential spring double[3]  (slot s of particle i at s*n+i)
 //   packed records of what the neighbour passes read of a neighbour
@@ -94,10 +98,10 @@ template <typename R>
 struct Engine {
     DevParams P;
     SphState<R> S[2];    // ping-pong; cur = S[cur_s]
-    DemState<R> D[2];
+    DemState<double> D[2];   // the DEM set is FP64 in both builds (see DevParams)
     int cur_s, cur_d;
     SphWork<R> sw;
-    DemWork<R> dw;
+    DemWork<double> dw;
     DevFlags* flags;
     CellSort cs_s, cs_d; // NNPS sort by cell of the SPH and DEM sets
     double* red_buf;     // reductions for stats

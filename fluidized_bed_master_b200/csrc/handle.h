@@ -63,3 +63,8 @@ int sphdem_io_write_vtk_dem(const char* path, int n, const double* x, const doub
                             const int* itype, const int* ptype, const int* dem_idx, const double* magf,
                             const double* eliz, const double* por, const double* uz, const double* qsd,
                             const double* ftz, const double* temp, const double* rad, const double* dtemp);
+// fluid particles (p_type 1) of the SPH set in the layout of
+// save_plot_fluid_vtk_bin_fluid_sph (functions_OUTPUT.cuh:445-651)
+int sphdem_io_write_vtk_fluid(const char* path, int n, const int* ptype, const double* x, const double* y,
+                              const double* z, const double* por, const double* pres, const double* dtemp,
+                              const int* btype, const double* rho, const double* temp, const double* uz);

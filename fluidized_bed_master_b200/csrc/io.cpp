@@ -505,6 +505,65 @@ int sphdem_io_write_vtk_dem(const char* path, int n, const double* x, const doub
     return SPHDEM_OK;
 }
 
+static int be_int(int v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u = (u >> 24) | ((u >> 8) & 0xff00u) | ((u << 8) & 0xff0000u) | (u << 24);
+    std::memcpy(&v, &u, 4);
+    return v;
+}
+
+// The reference's fluid writer (functions_OUTPUT.cuh:445-651): fluid
+// particles only (p_type 1), big-endian float positions, then nine point
+// arrays.  Its conv_rate and cond_rate arrays print part1::Q_sdf and
+// part1::Q_f, which no kernel of the compiled tree assigns, so they are
+// zero there and zero here.
+int sphdem_io_write_vtk_fluid(const char* path, int n, const int* ptype, const double* x, const double* y,
+                              const double* z, const double* por, const double* pres, const double* dtemp,
+                              const int* btype, const double* rho, const double* temp, const double* uz) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return SPHDEM_E_INPUT;
+    int np = 0;
+    for (int i = 0; i < n; i++)
+        if (ptype[i] == 1) np++;
+    std::fprintf(f, "# vtk DataFile Version 3.0\n");
+    std::fprintf(f, "Print out results in vtk format\n");
+    std::fprintf(f, "BINARY\n");
+    std::fprintf(f, "DATASET POLYDATA\n");
+    std::fprintf(f, "POINTS\t%d\tfloat\n", np);
+    for (int i = 0; i < n; i++) {
+        if (ptype[i] != 1) continue;
+        float v[3] = {be_float(x[i]), be_float(y[i]), be_float(z[i])};
+        std::fwrite(v, sizeof(float), 3, f);
+    }
+    std::fprintf(f, "POINT_DATA\t%d\n", np);
+    std::fprintf(f, "FIELD FieldData\t9\n");
+    auto arr = [&](const char* name, const double* a) {
+        std::fprintf(f, "%s\t1\t%d\tfloat\n", name, np);
+        for (int i = 0; i < n; i++) {
+            if (ptype[i] != 1) continue;
+            float v = be_float(a ? a[i] : 0.0);
+            std::fwrite(&v, sizeof(float), 1, f);
+        }
+    };
+    arr("porosity", por);
+    arr("conv_rate", nullptr);
+    arr("pressure", pres);
+    arr("cond_rate", nullptr);
+    arr("dtemp", dtemp);
+    std::fprintf(f, "buffer_type\t1\t%d\tint\n", np);
+    for (int i = 0; i < n; i++) {
+        if (ptype[i] != 1) continue;
+        int v = be_int(btype[i]);
+        std::fwrite(&v, sizeof(int), 1, f);
+    }
+    arr("density", rho);
+    arr("temperature", temp);
+    arr("uz", uz);
+    std::fclose(f);
+    return SPHDEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // host-only input.txt access
 // ---------------------------------------------------------------------------

@@ -153,6 +153,29 @@ __global__ void k_mlp_sum(int nparts, const float* __restrict__ part, float* out
 
 using namespace sphdem;
 
+// device time of the last forward / gradient kernel of this host thread
+static thread_local double g_last_fwd_ms = 0.0, g_last_grad_ms = 0.0;
+
+// CUDA events around one launch on stream st (elapsed read after the caller's sync)
+struct LaunchTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool ok = false;
+    void start(cudaStream_t st) {
+        ok = cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess &&
+             cudaEventRecord(a, st) == cudaSuccess;
+    }
+    void stop(cudaStream_t st) { ok = ok && cudaEventRecord(b, st) == cudaSuccess; }
+    double ms() {
+        float t = 0.f;
+        if (ok && cudaEventElapsedTime(&t, a, b) != cudaSuccess) t = 0.f;
+        return (double)t;
+    }
+    ~LaunchTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
 static int mlp_oneshot(const float* params, void* stream, MlpNet& m) {
     int r = mlp_alloc(m);
     if (r) return r;
@@ -167,11 +190,15 @@ extern "C" int sphdem_mlp_forward(const void* feat, int32_t n, const float* para
     // failure drill of the bounded device waits (see sphdem.h)
     const char* inj = getenv("SPHDEM_FAULT_DRILL");
     int stall = (inj && strcmp(inj, "mlp_wait") == 0) ? 1 : 0;
+    LaunchTimer tm;
+    tm.start(st);
     if (!r) r = mlp_forward(m, feat, n, out, st, stall);
+    tm.stop(st);
     int err = 0;
     if (!r && cudaMemcpyAsync(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) r = SPHDEM_E_CUDA;
     if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = SPHDEM_E_CUDA;
     if (!r && err) r = SPHDEM_E_TIMEOUT;
+    g_last_fwd_ms = r ? 0.0 : tm.ms();
     mlp_free(m);
     return r;
 }
@@ -182,7 +209,10 @@ extern "C" int sphdem_mlp_grad(const void* feat, const float* target, const floa
     MlpNet m;
     cudaStream_t st = (cudaStream_t)stream;
     int r = mlp_oneshot(params, stream, m);
+    LaunchTimer tm;
+    tm.start(st);
     if (!r) r = mlp_grad(m, feat, target, weight, n, (float)(1.0 / weight_sum), st);
+    tm.stop(st);
     if (!r) {
         k_mlp_sum<<<(MLP_NPARAM + 2 + 255) / 256, 256, 0, st>>>(m.nparts, m.part, grad);
         if (cudaGetLastError() != cudaSuccess) r = SPHDEM_E_CUDA;
@@ -191,8 +221,15 @@ extern "C" int sphdem_mlp_grad(const void* feat, const float* target, const floa
     if (!r && cudaMemcpyAsync(&err, m.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) r = SPHDEM_E_CUDA;
     if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = SPHDEM_E_CUDA;
     if (!r && err) r = SPHDEM_E_TIMEOUT;
+    g_last_grad_ms = r ? 0.0 : tm.ms();
     mlp_free(m);
     return r;
+}
+
+extern "C" int sphdem_mlp_last_ms(double* forward_ms, double* grad_ms) {
+    if (forward_ms) *forward_ms = g_last_fwd_ms;
+    if (grad_ms) *grad_ms = g_last_grad_ms;
+    return SPHDEM_OK;
 }
 
 extern "C" int32_t sphdem_mlp_param_count(void) { return MLP_NPARAM; }

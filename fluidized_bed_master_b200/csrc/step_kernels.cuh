@@ -188,7 +188,10 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
     });
     ncnt[i] = c;
     if (c > cap) atomicOr(&F->overflow, 1);
-    atomicMax(&F->max_ncnt, c);
+    // one atomic per converged group of threads for the largest count
+    const unsigned am = __activemask();
+    const int wmax = __reduce_max_sync(am, c);
+    if ((threadIdx.x & 31) == __ffs(am) - 1) atomicMax(&F->max_ncnt, wmax);
 }
 
 // The 9 full stencil rows (z, y order) of cell (ic, jc, kc) for a whole
@@ -434,8 +437,10 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
         if (act) {
             ncnt[i] = cnt;
             if (cnt > cap) atomicOr(&F->overflow, 1);
-            atomicMax(&F->max_ncnt, cnt);
         }
+        // one atomic per warp for the largest count
+        const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
+        if (lane == 0 && wmax > 0) atomicMax(&F->max_ncnt, wmax);
     }
 }
 
@@ -557,10 +562,9 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
             }
             __syncwarp();
         }
-        if (act) {
-            ncntd[i] = cnt;
-            atomicMax(&F->max_ncntd, cnt);
-        }
+        if (act) ncntd[i] = cnt;
+        const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
+        if (lane == 0 && wmax > 0) atomicMax(&F->max_ncntd, wmax);
     }
 }
 
@@ -573,7 +577,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
 // rho_new so that no thread sees a half-updated neighbour.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                const int4* __restrict__ drows) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
@@ -715,8 +719,8 @@ __global__ void k_gather_history(int n, const int* __restrict__ perm, const int*
 // KERNEL_clc_prep3D_coupling_dem: functions_PREP2.cuh:3367-3523.
 // One warp per DEM sphere; lanes stride over the candidate rows.
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<R> D,
-                                                  DemWork<R> DW, const int4* __restrict__ srows, const int4* __restrict__ drows) {
+__global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<double> D,
+                                                  DemWork<double> DW, const int4* __restrict__ srows, const int4* __restrict__ drows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -1190,76 +1194,77 @@ __device__ __forceinline__ void dc_warp_sum(DcSums<R>& a) {
 
 // drag closure on the reduced sums (when coupled) and the DEM predictor
 template <typename R>
-__device__ void dem_coupling_finish(const DevParams& P, DemState<R>& D, DemWork<R>& DW, int i, bool coupled,
+__device__ void dem_coupling_finish(const DevParams& P, DemState<double>& D, DemWork<double>& DW, int i, bool coupled,
                                     const DcSums<R>& a) {
+    using Q = double;   // the DEM set is FP64: the closure and the predictor run in FP64
     const int pt = D.ptype[i];
-    R uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i];
-    R ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
+    Q uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i];
+    Q ftx = DW.ftx[i], fty = DW.fty[i], ftz = DW.ftz[i];
     if (coupled) {
-        R radi = (R)D.rad[i], di = (R)2 * radi;
-        R mi = D.m[i], rhoi = D.rho[i], tempi = D.temp[i];
-        R fa = DW.flt_s[i], ff = DW.flt_sd[i];
-        const R tx = a.tx, ty = a.ty, tz = a.tz, ufx = a.ufx, ufy = a.ufy, ufz = a.ufz;
-        const R uax = a.uax, uay = a.uay, uaz = a.uaz, por = a.por, ttf = a.ttf, tta = a.tta;
+        Q radi = (Q)D.rad[i], di = (Q)2 * radi;
+        Q mi = D.m[i], rhoi = D.rho[i], tempi = D.temp[i];
+        Q fa = DW.flt_s[i], ff = DW.flt_sd[i];
+        const Q tx = a.tx, ty = a.ty, tz = a.tz, ufx = a.ufx, ufy = a.ufy, ufz = a.ufz;
+        const Q uax = a.uax, uay = a.uay, uaz = a.uaz, por = a.por, ttf = a.ttf, tta = a.tta;
         const int has_f = a.has_f, has_a = a.has_a;
-        R rho_f = has_f ? (R)P.rho_gas : (R)0, rho_a = has_a ? (R)P.rho_gas : (R)0;
-        R ki = (radi < (R)0.0012) ? (R)55.0 : (R)0.84;
-        R ali = (radi < (R)0.0012) ? (R)1.77e-5 : (R)2.5e-6;
-        R cpi = ki / (ali * rhoi);
-        R eps = (R)1.0e-15;
-        R pori = por / (ff + eps);
-        R ux_f = ufx / (ff + eps) - uxi, uy_f = ufy / (ff + eps) - uyi, uz_f = ufz / (ff + eps) - uzi;
+        Q rho_f = has_f ? (Q)P.rho_gas : (Q)0, rho_a = has_a ? (Q)P.rho_gas : (Q)0;
+        Q ki = (radi < (Q)0.0012) ? (Q)55.0 : (Q)0.84;
+        Q ali = (radi < (Q)0.0012) ? (Q)1.77e-5 : (Q)2.5e-6;
+        Q cpi = ki / (ali * rhoi);
+        Q eps = (Q)1.0e-15;
+        Q pori = por / (ff + eps);
+        Q ux_f = ufx / (ff + eps) - uxi, uy_f = ufy / (ff + eps) - uyi, uz_f = ufz / (ff + eps) - uzi;
         // the SPH temperatures in ttf/tta are stored as T - t_ref: absolute sums
-        const R tr = (R)P.t_ref;
-        const R ttfa = ttf + tr * a.wtf, ttaa = tta + tr * a.wta;
-        R tf = ttfa / (ff + eps) - tempi;
-        R ux_a = uax / (fa + eps) - uxi, uy_a = uay / (fa + eps) - uyi, uz_a = uaz / (fa + eps) - uzi;
-        R ta = ttaa / (fa + eps) - tempi;
-        R ux_fa = (ufx + uax) / (ff + fa + eps) - uxi, uy_fa = (ufy + uay) / (ff + fa + eps) - uyi,
+        const Q tr = (Q)P.t_ref;
+        const Q ttfa = ttf + tr * (Q)a.wtf, ttaa = tta + tr * (Q)a.wta;
+        Q tf = ttfa / (ff + eps) - tempi;
+        Q ux_a = uax / (fa + eps) - uxi, uy_a = uay / (fa + eps) - uyi, uz_a = uaz / (fa + eps) - uzi;
+        Q ta = ttaa / (fa + eps) - tempi;
+        Q ux_fa = (ufx + uax) / (ff + fa + eps) - uxi, uy_fa = (ufy + uay) / (ff + fa + eps) - uyi,
           uz_fa = (ufz + uaz) / (ff + fa + eps) - uzi;
-        R tfa = (ttfa + ttaa) / (ff + fa + eps) - tempi;
-        R f_fluid = ff / (ff + fa + eps), f_air = fa / (ff + fa + eps);
-        R mf = sqrt(ux_f * ux_f + uy_f * uy_f + uz_f * uz_f);
+        Q tfa = (ttfa + ttaa) / (ff + fa + eps) - tempi;
+        Q f_fluid = ff / (ff + fa + eps), f_air = fa / (ff + fa + eps);
+        Q mf = sqrt(ux_f * ux_f + uy_f * uy_f + uz_f * uz_f);
         DW.magf[i] = mf;
-        R ma = sqrt(ux_a * ux_a + uy_a * uy_a + uz_a * uz_a);
-        R mfa = sqrt(ux_fa * ux_fa + uy_fa * uy_fa + uz_fa * uz_fa);
-        R dfx = 0, dfy = 0, dfz = 0, dax = 0, day = 0, daz = 0, dq = 0;
-        R a_ht = (R)6 / di;
-        R nu = (R)P.nu_gas;
+        Q ma = sqrt(ux_a * ux_a + uy_a * uy_a + uz_a * uz_a);
+        Q mfa = sqrt(ux_fa * ux_fa + uy_fa * uy_fa + uz_fa * uz_fa);
+        Q dfx = 0, dfy = 0, dfz = 0, dax = 0, day = 0, daz = 0, dq = 0;
+        Q a_ht = (Q)6 / di;
+        Q nu = (Q)P.nu_gas;
         DW.DEMpor[i] = pori;
-        if (mf > (R)1.0e-8 && (ff + fa) > (R)0.00001 && f_fluid > (R)0.65) {
-            R Re = di * mf * pori / (nu + eps);
-            R q = (R)0.63 + (R)4.8 / sqrt(Re);
-            R Cdf = q * q;
-            R lr = (R)1.5 - log10(Re);
-            R bf = (R)3.7 - (R)0.65 * exp(-lr * lr / (R)2);
-            R c = ((R)1 / (R)8) * Cdf * rho_f * (R)3.14159 * di * di * mf * pow(pori, (R)2 - bf) / mi;
+        if (mf > (Q)1.0e-8 && (ff + fa) > (Q)0.00001 && f_fluid > (Q)0.65) {
+            Q Re = di * mf * pori / (nu + eps);
+            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
+            Q Cdf = q * q;
+            Q lr = (Q)1.5 - log10(Re);
+            Q bf = (Q)3.7 - (Q)0.65 * exp(-lr * lr / (Q)2);
+            Q c = ((Q)1 / (Q)8) * Cdf * rho_f * (Q)3.14159 * di * di * mf * pow(pori, (Q)2 - bf) / mi;
             dfx = c * ux_f; dfy = c * uy_f; dfz = c * uz_f;
-            dq = ((R)2 + (R)0.6 * sqrt(Re)) * (R)0.0518 / di * a_ht * tf;
+            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * (Q)0.0518 / di * a_ht * tf;
             D.Fdx_df[i] = dfx;
             D.Fdy_df[i] = dfy;
             D.Fdz_df[i] = dfz;
         }
-        if (ma > (R)1.0e-8 && (ff + fa) > (R)0.00001 && f_air > (R)0.65) {
-            R Re = di * pori * ma / (nu + eps);
-            R q = (R)0.63 + (R)4.8 / sqrt(Re);
-            R lr = (R)1.5 - log10(Re);
-            R b = (R)2.65 * ((R)1 + pori) - ((R)5.3 - (R)3.5 * pori) * pori * pori * exp(-lr * lr / (R)2);
-            R c = ((R)1 / (R)8) * q * q * rho_a * (R)3.14159 * di * di * ma * pow(pori, (R)-1 - b) / mi;
+        if (ma > (Q)1.0e-8 && (ff + fa) > (Q)0.00001 && f_air > (Q)0.65) {
+            Q Re = di * pori * ma / (nu + eps);
+            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
+            Q lr = (Q)1.5 - log10(Re);
+            Q b = (Q)2.65 * ((Q)1 + pori) - ((Q)5.3 - (Q)3.5 * pori) * pori * pori * exp(-lr * lr / (Q)2);
+            Q c = ((Q)1 / (Q)8) * q * q * rho_a * (Q)3.14159 * di * di * ma * pow(pori, (Q)-1 - b) / mi;
             dax = c * ux_a; day = c * uy_a; daz = c * uz_a;
-            dq = ((R)2 + (R)0.6 * sqrt(Re)) * ki / di * a_ht * ta;
+            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * ki / di * a_ht * ta;
         }
-        if ((ma > (R)1.0e-8 || mf > (R)1.0e-8) && (ff + fa) > (R)0.00001 && f_air <= (R)0.65 && f_fluid <= (R)0.65) {
-            R rfa = (R)P.rho_gas * f_air + (R)P.rho_liquid * f_fluid;
-            R vfa = (R)P.mu_gas * f_air + (R)P.mu_liquid * f_fluid;
-            R vk = vfa / (rfa + eps);
-            R Re = di * pori * mfa / (vk + eps);
-            R q = (R)0.63 + (R)4.8 / sqrt(Re);
-            R lr = (R)1.5 - log10(Re);
-            R b = (R)2.65 * ((R)1 + pori) - ((R)5.3 - (R)3.5 * pori) * pori * pori * exp(-lr * lr / (R)2);
-            R c = ((R)1 / (R)8) * q * q * rfa * (R)3.14159 * di * di * mfa * pow(pori, (R)-1 - b) / mi;
+        if ((ma > (Q)1.0e-8 || mf > (Q)1.0e-8) && (ff + fa) > (Q)0.00001 && f_air <= (Q)0.65 && f_fluid <= (Q)0.65) {
+            Q rfa = (Q)P.rho_gas * f_air + (Q)P.rho_liquid * f_fluid;
+            Q vfa = (Q)P.mu_gas * f_air + (Q)P.mu_liquid * f_fluid;
+            Q vk = vfa / (rfa + eps);
+            Q Re = di * pori * mfa / (vk + eps);
+            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
+            Q lr = (Q)1.5 - log10(Re);
+            Q b = (Q)2.65 * ((Q)1 + pori) - ((Q)5.3 - (Q)3.5 * pori) * pori * pori * exp(-lr * lr / (Q)2);
+            Q c = ((Q)1 / (Q)8) * q * q * rfa * (Q)3.14159 * di * di * mfa * pow(pori, (Q)-1 - b) / mi;
             dax = c * ux_fa; day = c * uy_fa; daz = c * uz_fa;
-            dq = ((R)2 + (R)0.6 * sqrt(Re)) * ki / di * a_ht * tfa;
+            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * ki / di * a_ht * tfa;
         }
         ftx = ftx + dfx / pori + tx;
         fty = fty + dfy / pori + ty;
@@ -1277,11 +1282,11 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<R>& D, DemWork<
     // predictor (DEM): u* = u + f dt
     DW.ux0[i] = uxi; DW.uy0[i] = uyi; DW.uz0[i] = uzi;
     if (pt == 9) {
-        D.ux[i] = (R)P.ball_vel; D.uy[i] = (R)0; D.uz[i] = (R)0;
-        DW.ux0[i] = (R)P.ball_vel; DW.uy0[i] = (R)0; DW.uz0[i] = (R)0;
+        D.ux[i] = (Q)P.ball_vel; D.uy[i] = (Q)0; D.uz[i] = (Q)0;
+        DW.ux0[i] = (Q)P.ball_vel; DW.uy0[i] = (Q)0; DW.uz0[i] = (Q)0;
     } else if (pt >= 0) {
-        R b = (R)(D.btype[i] == 0);
-        R dt = (R)P.dt;
+        Q b = (Q)(D.btype[i] == 0);
+        Q dt = (Q)P.dt;
         D.ux[i] = uxi + ftx * b * dt;
         D.uy[i] = uyi + fty * b * dt;
         D.uz[i] = uzi + ftz * b * dt;
@@ -1290,8 +1295,8 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<R>& D, DemWork<
 }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int4* __restrict__ srows) {
+__global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
+                                                      DemWork<double> DW, const int4* __restrict__ srows) {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -1346,8 +1351,8 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
 // KERNEL_clc_projection_sph (functions_TIME_ISPH2.cuh:104-204).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<R> D,
-                                                      DemWork<R> DW, const int4* __restrict__ drows, int time_zero) {
+__global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
+                                                      DemWork<double> DW, const int4* __restrict__ drows, int time_zero) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -1370,15 +1375,15 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
                 if (D.ptype[j] <= 1000) return;
                 PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 0.0, r2l, r2h);
                 if (!g.in) return;
-                R ffj = DW.flt_sd2[j] + DW.flt_s[j];
+                R ffj = (R)DW.flt_sd2[j] + (R)DW.flt_s[j];
                 if (!(ffj > (R)0)) return;
                 R w = kw(K, g.r);
                 R c = w / (ffj + (R)1.0e-20);
-                R mr = D.m[j] / rhoi;
-                tx += -mr * D.Fdx_df[j] * c;
-                ty += -mr * D.Fdy_df[j] * c;
-                tz += -mr * D.Fdz_df[j] * c;
-                tt += -D.Q_sd[j] / (rhoi * cpi) * c;
+                R mr = (R)D.m[j] / rhoi;
+                tx += -mr * (R)D.Fdx_df[j] * c;
+                ty += -mr * (R)D.Fdy_df[j] * c;
+                tz += -mr * (R)D.Fdz_df[j] * c;
+                tt += -(R)D.Q_sd[j] / (rhoi * cpi) * c;
             };
             const int cd = W.ncntd[i];
             if (cd <= P.nbd_cap) {

@@ -49,6 +49,7 @@ def lib():
     L.sphdem_get_neighbors.argtypes = [vp, P(C.c_int32), P(C.c_int32), C.c_int32]
     L.sphdem_get_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
+    L.sphdem_write_vtk_fluid.argtypes = [vp, C.c_char_p]
     L.sphdem_set_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
     L.sphdem_set_graphs.argtypes = [vp, C.c_int]
@@ -302,6 +303,9 @@ class Engine:
 
     def write_vtk_dem(self, path):
         _chk(lib().sphdem_write_vtk_dem(self._h, os.fsencode(path)), "sphdem_write_vtk_dem")
+
+    def write_vtk_fluid(self, path):
+        _chk(lib().sphdem_write_vtk_fluid(self._h, os.fsencode(path)), "sphdem_write_vtk_fluid")
 
     def write_restart(self, path):
         _chk(lib().sphdem_write_restart(self._h, os.fsencode(path)), "sphdem_write_restart")

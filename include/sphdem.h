@@ -365,6 +365,12 @@ int sphdem_mlp_grad(const void* feat_bf16, const float* target,
                     const float* weight, int32_t n, const float* params,
                     double weight_sum, float* grad, void* stream);
 
+/* Device time (CUDA events on the call's stream) of the network kernel of
+ * the last successful sphdem_mlp_forward / sphdem_mlp_grad call of this
+ * host thread (the gradient kernel only, without its reduction), in ms;
+ * either pointer may be NULL. */
+int sphdem_mlp_last_ms(double* forward_ms, double* grad_ms);
+
 /* State of the learned warm start of a handle (warm_start = WARM_MLP):
  * the flattened FP32 parameters (sphdem_mlp_param_count() values), the
  * feature statistics (SPHDEM_MLP_STATS doubles: feature means[16] and
@@ -440,6 +446,14 @@ int sphdem_get_timing(SphdemHandle* h, int k, char* name, int name_cap,
 /* Binary legacy-VTK POLYDATA of the DEM set, the format of
  * save_plot_fluid_vtk_bin_solid_dem (functions_OUTPUT.cuh:1135-1446). */
 int sphdem_write_vtk_dem(SphdemHandle* h, const char* path);
+
+/* Binary legacy-VTK POLYDATA of the fluid particles (p_type 1) of the SPH
+ * set, the format of save_plot_fluid_vtk_bin_fluid_sph
+ * (functions_OUTPUT.cuh:445-651): positions, porosity, conv_rate,
+ * pressure, cond_rate, dtemp, buffer_type, density, temperature, uz.  The
+ * reference's conv_rate/cond_rate print fields no compiled kernel sets
+ * (zero), and are zero here. */
+int sphdem_write_vtk_fluid(SphdemHandle* h, const char* path);
 
 /* Restart file in input.txt format: tab-separated column labels then one
  * row per particle with all columns (fixes save_restart,

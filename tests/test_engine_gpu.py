@@ -273,8 +273,16 @@ def test_bulk_field_transfer(calm_bed, prec):
         rng = np.random.default_rng(5)
         new = {f: bulk[f] * (1.0 + 1e-3 * rng.standard_normal(n)) for f in settable}
         e.set_fields(which, new)
+        # the DEM set and positions are FP64 in both builds; SPH fields are
+        # FP32 in the FP32 build, and the SPH temperature is stored as
+        # T - t_ref with t_ref the FP32-rounded mean input temperature
+        t_ref = float(np.float32(np.mean(sph["temp"])))
         for f in settable:
-            ref = new[f].astype(np.float32).astype(np.float64) if (prec == 0 and f != "x") else new[f]
+            ref = new[f]
+            if prec == 0 and which == SPH and f == "temp":
+                ref = (new[f] - t_ref).astype(np.float32).astype(np.float64) + t_ref
+            elif prec == 0 and which == SPH and f != "x":
+                ref = new[f].astype(np.float32).astype(np.float64)
             assert np.array_equal(e.get(which, f), ref), f
     with pytest.raises(Exception):
         e.set_fields(SPH, {"ftotalx": np.zeros(e.ns)})
