@@ -553,7 +553,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 1;
     }
     if (nd > 0) {
-        { KTIME(KT_DEMCONTACT); k_dem_contact<double><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
+        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
         { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows); }
         *nl += 2;
     }

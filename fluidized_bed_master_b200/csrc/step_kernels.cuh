@@ -905,7 +905,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // the reference).  Spring increments and overlap are FP64.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D, DemWork<R> DW,
+__global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
                                                      const int4* __restrict__ drows,
                                                      DevFlags* F) {
     // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
@@ -936,9 +936,10 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
     Q Gij = (Q)1 / ((((Q)2 - pri) / Gi) + (((Q)2 - pri) / Gi));
     Q cdamp = sqrt((Q)3.333333333) * (Q)P.damp;
     Q kci = (Q)P.k_dem, cpi = (Q)P.cp_dem;
-    Q emi = (tempi >= (Q)700) ? ((Q)0.505586 + (Q)7.92943e-4 * tempi - (Q)5.228643e-7 * tempi * tempi +
-                                 (Q)1.10479e-10 * tempi * tempi * tempi)
-                              : (Q)0.842337;
+    const R tiR = (R)tempi;
+    const R emiR = (tiR >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tiR - (R)5.228643e-7 * tiR * tiR +
+                                      (R)1.10479e-10 * tiR * tiR * tiR)
+                                   : (R)0.842337;
     Q radiR = (Q)radi;
     Q dr2 = ((Q)1 / (Q)6) * radiR;
     Q volm = ((Q)4 / (Q)3) * (Q)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
@@ -970,29 +971,36 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<R> D,
         Q radij = (Q)1 / ((Q)1 / radiR + (Q)1 / radjR);
         Q tdR = (Q)td;
         if (P.con) {
-            Q tempj = D.temp[j];
-            Q emj = (tempj >= (Q)700) ? ((Q)0.505586 + (Q)7.92943e-4 * tempj - (Q)5.228643e-7 * tempj * tempj +
-                                         (Q)1.10479e-10 * tempj * tempj * tempj)
-                                      : (Q)0.842337;
-            Q ai = radiR / tdR, aj = radjR / tdR, dij = aj - ai;
-            Q dc_r = (Q)0.56 * ((Q)2 * radij);
-            Q dc_ar = (Q)3.14159 * dc_r * dc_r;
-            Q dmax = (Q)0.5 * (sqrt((Q)1 + (Q)4 * dc_ar / ((Q)3.14159 * tdR * tdR * ((Q)1 - dij * dij))) - dij);
-            Q ci = ((Q)1 - dij * dij) / ((Q)2 * dmax) - dij;
-            Q cj = ((Q)1 - dij * dij) / ((Q)2 * (dmax + dij)) + dij;
-            Q si = sqrt((Q)1 - ci * ci), sj = sqrt((Q)1 - cj * cj);
-            Q ri_cr = radiR * si, rj_cr = radjR * sj;
-            Q td_cr = tdR - radiR * ci - radjR * cj;
-            Q z_cr = (Q)1 + ((Q)4 * rj_cr * rj_cr + td_cr * td_cr) / (ri_cr * ri_cr);
-            Q F_cr = (Q)0.5 * (z_cr - sqrt(z_cr * z_cr - (Q)4 * rj_cr * rj_cr / (ri_cr * ri_cr)));
-            Q F_ij = ((Q)1 + ci) * F_cr * (Q)0.5;
-            Q ar_i = (Q)2 * (Q)3.14159 * radiR * radiR * ((Q)1 - ci);
-            Q ar_j = (Q)2 * (Q)3.14159 * radjR * radjR * ((Q)1 - cj);
-            Q arr = ar_j / ar_i;
-            Q Y = F_ij + ((Q)1 - F_ij) * (arr / ((Q)1 + arr));
-            Q einv = ((Q)1 - emi) / (emi * ar_i) + ((Q)1 - emj) / (emj * ar_j) + (Q)1 / (Y * ar_i);
-            dtr += -(Q)5.6704e-8 * (tempi * tempi * tempi * tempi - tempj * tempj * tempj * tempj) /
-                   (einv * (rhoi * volm) * cpi);
+            // radiation between spheres within the search range (functions_DEM_INTERACTION2.cuh:
+            // 1080-1194): a heat rate, formed in the field precision R
+            const R ti = (R)tempi, tj = (R)D.temp[j];
+            const R riR = (R)radiR, rjR = (R)radjR, rijR = (R)radij, tdF = (R)tdR;
+            R emj = (tj >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tj - (R)5.228643e-7 * tj * tj +
+                                      (R)1.10479e-10 * tj * tj * tj)
+                                   : (R)0.842337;
+            R ai = riR / tdF, aj = rjR / tdF, dij = aj - ai;
+            R dc_r = (R)0.56 * ((R)2 * rijR);
+            R dc_ar = (R)3.14159 * dc_r * dc_r;
+            R dmax = (R)0.5 * (sqrt((R)1 + (R)4 * dc_ar / ((R)3.14159 * tdF * tdF * ((R)1 - dij * dij))) - dij);
+            R ci = ((R)1 - dij * dij) / ((R)2 * dmax) - dij;
+            R cj = ((R)1 - dij * dij) / ((R)2 * (dmax + dij)) + dij;
+            R si = sqrt((R)1 - ci * ci), sj = sqrt((R)1 - cj * cj);
+            R ri_cr = riR * si, rj_cr = rjR * sj;
+            R td_cr = tdF - riR * ci - rjR * cj;
+            R z_cr = (R)1 + ((R)4 * rj_cr * rj_cr + td_cr * td_cr) / (ri_cr * ri_cr);
+            R F_cr = (R)0.5 * (z_cr - sqrt(z_cr * z_cr - (R)4 * rj_cr * rj_cr / (ri_cr * ri_cr)));
+            R F_ij = ((R)1 + ci) * F_cr * (R)0.5;
+            R ar_i = (R)2 * (R)3.14159 * riR * riR * ((R)1 - ci);
+            R ar_j = (R)2 * (R)3.14159 * rjR * rjR * ((R)1 - cj);
+            R arr = ar_j / ar_i;
+            R Y = F_ij + ((R)1 - F_ij) * (arr / ((R)1 + arr));
+            R einv = ((R)1 - emiR) / (emiR * ar_i) + ((R)1 - emj) / (emj * ar_j) + (R)1 / (Y * ar_i);
+            // Ti^4 - Tj^4; in FP32 as (Ti - Tj)(Ti + Tj)(Ti^2 + Tj^2), which keeps the
+            // relative precision of a difference of nearly equal temperatures
+            R d4;
+            if constexpr (sizeof(R) == 4) d4 = (ti - tj) * (ti + tj) * (ti * ti + tj * tj);
+            else d4 = ti * ti * ti * ti - tj * tj * tj * tj;
+            dtr += (Q)(-(R)5.6704e-8 * d4 / (einv * ((R)rhoi * (R)volm) * (R)cpi));
         }
         if (!(td < P.r_contact * radi)) return;
         int slot = -1;
@@ -1232,39 +1240,43 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<double>& D, Dem
         Q a_ht = (Q)6 / di;
         Q nu = (Q)P.nu_gas;
         DW.DEMpor[i] = pori;
+        // the Di Felice closure (functions_SPH_DEM_COUPLING2.cuh:979-1009) in the
+        // field precision R: an empirical coefficient, applied to the FP64 slip
+        const R diR = (R)di, poriR = (R)pori, miR = (R)mi, nuR = (R)nu, epsR = (R)1.0e-15;
+        const R mfR = (R)mf, maR = (R)ma, mfaR = (R)mfa, kiR = (R)ki, ahtR = (R)a_ht;
         if (mf > (Q)1.0e-8 && (ff + fa) > (Q)0.00001 && f_fluid > (Q)0.65) {
-            Q Re = di * mf * pori / (nu + eps);
-            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
-            Q Cdf = q * q;
-            Q lr = (Q)1.5 - log10(Re);
-            Q bf = (Q)3.7 - (Q)0.65 * exp(-lr * lr / (Q)2);
-            Q c = ((Q)1 / (Q)8) * Cdf * rho_f * (Q)3.14159 * di * di * mf * pow(pori, (Q)2 - bf) / mi;
+            R Re = diR * mfR * poriR / (nuR + epsR);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R Cdf = q * q;
+            R lr = (R)1.5 - log10(Re);
+            R bf = (R)3.7 - (R)0.65 * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * Cdf * (R)rho_f * (R)3.14159 * diR * diR * mfR * pow(poriR, (R)2 - bf) / miR;
             dfx = c * ux_f; dfy = c * uy_f; dfz = c * uz_f;
-            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * (Q)0.0518 / di * a_ht * tf;
+            dq = (Q)(((R)2 + (R)0.6 * sqrt(Re)) * (R)0.0518 / diR * ahtR) * tf;
             D.Fdx_df[i] = dfx;
             D.Fdy_df[i] = dfy;
             D.Fdz_df[i] = dfz;
         }
         if (ma > (Q)1.0e-8 && (ff + fa) > (Q)0.00001 && f_air > (Q)0.65) {
-            Q Re = di * pori * ma / (nu + eps);
-            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
-            Q lr = (Q)1.5 - log10(Re);
-            Q b = (Q)2.65 * ((Q)1 + pori) - ((Q)5.3 - (Q)3.5 * pori) * pori * pori * exp(-lr * lr / (Q)2);
-            Q c = ((Q)1 / (Q)8) * q * q * rho_a * (Q)3.14159 * di * di * ma * pow(pori, (Q)-1 - b) / mi;
+            R Re = diR * poriR * maR / (nuR + epsR);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R lr = (R)1.5 - log10(Re);
+            R b = (R)2.65 * ((R)1 + poriR) - ((R)5.3 - (R)3.5 * poriR) * poriR * poriR * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * q * q * (R)rho_a * (R)3.14159 * diR * diR * maR * pow(poriR, (R)-1 - b) / miR;
             dax = c * ux_a; day = c * uy_a; daz = c * uz_a;
-            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * ki / di * a_ht * ta;
+            dq = (Q)(((R)2 + (R)0.6 * sqrt(Re)) * kiR / diR * ahtR) * ta;
         }
         if ((ma > (Q)1.0e-8 || mf > (Q)1.0e-8) && (ff + fa) > (Q)0.00001 && f_air <= (Q)0.65 && f_fluid <= (Q)0.65) {
-            Q rfa = (Q)P.rho_gas * f_air + (Q)P.rho_liquid * f_fluid;
-            Q vfa = (Q)P.mu_gas * f_air + (Q)P.mu_liquid * f_fluid;
-            Q vk = vfa / (rfa + eps);
-            Q Re = di * pori * mfa / (vk + eps);
-            Q q = (Q)0.63 + (Q)4.8 / sqrt(Re);
-            Q lr = (Q)1.5 - log10(Re);
-            Q b = (Q)2.65 * ((Q)1 + pori) - ((Q)5.3 - (Q)3.5 * pori) * pori * pori * exp(-lr * lr / (Q)2);
-            Q c = ((Q)1 / (Q)8) * q * q * rfa * (Q)3.14159 * di * di * mfa * pow(pori, (Q)-1 - b) / mi;
+            R rfa = (R)P.rho_gas * (R)f_air + (R)P.rho_liquid * (R)f_fluid;
+            R vfa = (R)P.mu_gas * (R)f_air + (R)P.mu_liquid * (R)f_fluid;
+            R vk = vfa / (rfa + epsR);
+            R Re = diR * poriR * mfaR / (vk + epsR);
+            R q = (R)0.63 + (R)4.8 / sqrt(Re);
+            R lr = (R)1.5 - log10(Re);
+            R b = (R)2.65 * ((R)1 + poriR) - ((R)5.3 - (R)3.5 * poriR) * poriR * poriR * exp(-lr * lr / (R)2);
+            R c = ((R)1 / (R)8) * q * q * rfa * (R)3.14159 * diR * diR * mfaR * pow(poriR, (R)-1 - b) / miR;
             dax = c * ux_fa; day = c * uy_fa; daz = c * uz_fa;
-            dq = ((Q)2 + (Q)0.6 * sqrt(Re)) * ki / di * a_ht * tfa;
+            dq = (Q)(((R)2 + (R)0.6 * sqrt(Re)) * kiR / diR * ahtR) * tfa;
         }
         ftx = ftx + dfx / pori + tx;
         fty = fty + dfy / pori + ty;

@@ -139,20 +139,26 @@ def test_fp32_within_1e5_after_100_steps(calm_bed):
     assert not bad, bad
 
 
+RATE_FIELDS = {"dDEMpor", "ftotalx", "ftotaly", "ftotalz", "fpx", "fpy", "fpz", "pgfx", "pgfy", "pgfz", "Fdx_df",
+               "Fdy_df", "Fdz_df", "torqx", "torqy", "torqz", "dtemp"}
+
+
 def test_fp32_vs_fp64_engine_builds(calm_bed):
-    """Every field of the FP32 build against the FP64 build of the same kernels."""
+    """Every field of the FP32 build against the FP64 build of the same
+    kernels after 100 steps: state fields within rel. L2 1e-5, rate fields
+    (forces, gradients, torques, heat rates) within 1e-4."""
     p, sph, dem = calm_bed
     e32 = _engine(p, sph, dem, 0)
     e64 = _engine(p, sph, dem, 1)
-    e32.step(10)
-    e64.step(10)
-    report = {}
+    e32.step(100)
+    e64.step(100)
+    bad = {}
     for which, fields in ((SPH, SPH_REAL), (DEM, DEM_REAL)):
         for f in fields:
-            report[("dem" if which else "sph", f)] = rel_l2(by_id(_ids(e32, which), e32.get(which, f)),
-                                                           by_id(_ids(e64, which), e64.get(which, f)))
-    worst = max(report.values())
-    assert worst < 1e-3, sorted(report.items(), key=lambda kv: -kv[1])[:5]
+            e = rel_l2(by_id(_ids(e32, which), e32.get(which, f)), by_id(_ids(e64, which), e64.get(which, f)))
+            if not e <= (1e-4 if f in RATE_FIELDS else 1e-5):
+                bad[("dem" if which else "sph", f)] = e
+    assert not bad, sorted(bad.items(), key=lambda kv: -kv[1])
 
 
 @pytest.mark.parametrize("prec", [0, 1])
