@@ -242,7 +242,7 @@ class RefHarness:
     slabs to its own spouted geometry.  The reference keeps its state in
     globals, so a process loads one bed per build."""
 
-    def __init__(self, kind, p, sph, dem):
+    def __init__(self, kind, p, sph, dem, solver="isph"):
         import ctypes as C
         import tempfile
 
@@ -260,16 +260,19 @@ class RefHarness:
         os.makedirs(os.path.join(work, "plotdata"), exist_ok=True)
         L = C.CDLL(path)
         L.ref_load.argtypes = [C.c_char_p]
+        L.ref_load_wcsph.argtypes = [C.c_char_p]
         L.ref_run_without_dem_walls.argtypes = [C.c_int]
+        L.ref_run_wcsph.argtypes = [C.c_int]
         L.ref_last_ms.restype = C.c_double
         L.ref_counts.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         cwd = os.getcwd()
         try:
-            rc = L.ref_load(work.encode())
+            rc = (L.ref_load_wcsph if solver == "wcsph" else L.ref_load)(work.encode())
         finally:
             os.chdir(cwd)
         if rc != 0:
             raise RuntimeError(f"ref_load returned {rc}")
+        self.run_fn = L.ref_run_wcsph if solver == "wcsph" else L.ref_run_without_dem_walls
         ns, nd = C.c_int(), C.c_int()
         nijk = (C.c_int * 3)()
         L.ref_counts(C.byref(ns), C.byref(nd), nijk)
@@ -280,11 +283,11 @@ class RefHarness:
         cwd = os.getcwd()
         try:
             os.chdir(self.work)
-            rc = self.L.ref_run_without_dem_walls(nsteps)
+            rc = self.run_fn(nsteps)
         finally:
             os.chdir(cwd)
         if rc != 0:
-            raise RuntimeError(f"ref_run_without_dem_walls returned {rc}")
+            raise RuntimeError(f"reference step returned {rc}")
         return self.L.ref_last_ms()
 
 
@@ -812,13 +815,37 @@ def run_dam2d(args, world, rank, local, pg):
     if args.impl == "reference":
         if rank != 0:
             return
-        val, cores, sample, s_per_step = dam2d_cpu(max(5.0, args.cpu_seconds))
+        p0, sph0, _ = dam_break_2d(seed=0)
+        kind = "reference"
+        try:
+            ref = RefHarness("host", p0, sph0, {}, solver="wcsph")
+            ref.run(args.warmup)
+            ms = ref.run(args.steps) / args.steps
+            val, cores, s_per_step = ref.ns / (ms / 1e3), omp_threads(), ms / 1e3
+            sample = (f"the whole dam break ({ref.ns} particles), {args.steps} steps after {args.warmup} warm-up; "
+                      "the reference's own 2-D WCSPH kernel bodies host-compiled (oracle/Makefile refhost), FP64, "
+                      "in the Lagrangian order of oracle/ref_harness.cu")
+        except FileNotFoundError:
+            val, cores, sample, s_per_step = dam2d_cpu(max(5.0, args.cpu_seconds))
+            kind = "port"
         line = {"metric": metric, "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": s_per_step * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded dam break)", "config": {"workload": DAM_TEXT},
-                "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
                 "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not args.no_ref_cuda:
+            try:
+                rc_ = RefHarness("cuda", p0, sph0, {}, solver="wcsph")
+                rc_.run(args.warmup)
+                ms = rc_.run(args.steps) / args.steps
+                line["reference_cuda"] = {
+                    "value": rc_.ns / (ms / 1e3), "unit": unit, "ms_per_step": ms, "n": rc_.ns, "steps": args.steps,
+                    "warmup": args.warmup, "dtype": "f64",
+                    "how": "reference CUDA build (sm_100a), its 2-D WCSPH kernels in the Lagrangian order of "
+                           "oracle/ref_harness.cu (ref_run_wcsph); wall clock around the step loop"}
+            except (FileNotFoundError, RuntimeError) as e:
+                line["reference_cuda"] = {"unavailable": str(e)}
         print(json.dumps(line), flush=True)
         return
     torch.cuda.set_device(local)

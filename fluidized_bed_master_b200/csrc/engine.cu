@@ -184,6 +184,8 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<double>& DW, int ns, int nd, in
     DW.rows = A.get<int4>(ncells);
     DW.nbs = A.get<int>((size_t)nd * DEM_SPH_CAP);
     DW.ncs = A.get<int>(nd);
+    DW.dcs = A.get<double>((size_t)nd * 14);
+    DW.dcf = A.get<int>(nd);
 }
 
 
@@ -554,8 +556,12 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     }
     if (nd > 0) {
         { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
-        { KTIME(KT_DEMCOUPLING); k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows); }
-        *nl += 2;
+        {
+            KTIME(KT_DEMCOUPLING);
+            k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows);
+            k_dem_finish<R><<<bd, TPB, 0, st>>>(P, D, DW);
+        }
+        *nl += 3;
     }
     if (ns > 0) {
         { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0); }

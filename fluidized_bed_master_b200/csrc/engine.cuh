@@ -82,6 +82,8 @@ struct DemWork {
     int *g_str, *g_end;
     int4* rows;
     int *nbs, *ncs;              // SPH neighbours of each sphere (k_dem_prep): nbs[i*DEM_SPH_CAP+k], exact count
+    R* dcs;                      // 14*n pair sums of k_dem_coupling for k_dem_finish (DcSums, plane-major)
+    int* dcf;                    // n: bit0 coupled, bit1 fluid seen, bit2 air seen; -1 not reached
 };
 constexpr int DEM_SPH_CAP = 256;
 

@@ -925,9 +925,10 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
         DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
     }
     if (D.itype[i] != 1 || D.ptype[i] <= 1000) return;
-    // the pair terms and their sums run in FP64 in both builds: the tangential
-    // relative velocity and the torques are small differences of the state
-    using Q = double;
+    // the contact mechanics in the field precision R over the FP64 state;
+    // overlap and tangential spring in FP64 (functions_DEM_INTERACTION2.cuh
+    // keeps them in Real)
+    using Q = R;
     double xi = D.x[i], yi = D.y[i], zi = D.z[i], radi = D.rad[i];
     Q uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
     Q mi = D.m[i], rii = D.ri[i], rhoi = D.rho[i], tempi = D.temp[i];
@@ -1314,7 +1315,10 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
     int* sm = s_rows[threadIdx.x >> 5];
     if (i >= P.nd) return;
     int it = D.itype[i], pt = D.ptype[i];
-    if (it > 2) return;
+    if (it > 2) {
+        if (lane == 0) DW.dcf[i] = -1;   // k_dem_finish skips it
+        return;
+    }
     DcSums<R> a{};
     const bool coupled = it == 1 && pt > 1000;
     if (coupled) {
@@ -1355,7 +1359,37 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         dc_warp_sum(a);
     }
     if (lane != 0) return;
-    dem_coupling_finish(P, D, DW, i, coupled, a);
+    // the closure and the predictor run in k_dem_finish (thread per sphere),
+    // so this pair pass keeps the registers of the FP32 sums only
+    const int nd = P.nd;
+    double* o = DW.dcs;
+    o[0 * nd + i] = a.tx; o[1 * nd + i] = a.ty; o[2 * nd + i] = a.tz;
+    o[3 * nd + i] = a.ufx; o[4 * nd + i] = a.ufy; o[5 * nd + i] = a.ufz;
+    o[6 * nd + i] = a.uax; o[7 * nd + i] = a.uay; o[8 * nd + i] = a.uaz;
+    o[9 * nd + i] = a.por; o[10 * nd + i] = a.ttf; o[11 * nd + i] = a.tta;
+    o[12 * nd + i] = a.wtf; o[13 * nd + i] = a.wta;
+    DW.dcf[i] = (coupled ? 1 : 0) | (a.has_f ? 2 : 0) | (a.has_a ? 4 : 0);
+}
+
+// the drag closure and the DEM predictor of every sphere the pair pass
+// reached (dcf >= 0), on the sums it left in DW.dcs
+template <typename R>
+__global__ void __launch_bounds__(128) k_dem_finish(DevParams P, DemState<double> D, DemWork<double> DW) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nd = P.nd;
+    if (i >= nd) return;
+    const int f = DW.dcf[i];
+    if (f < 0) return;
+    const double* o = DW.dcs;
+    DcSums<R> a;
+    a.tx = (R)o[0 * nd + i]; a.ty = (R)o[1 * nd + i]; a.tz = (R)o[2 * nd + i];
+    a.ufx = (R)o[3 * nd + i]; a.ufy = (R)o[4 * nd + i]; a.ufz = (R)o[5 * nd + i];
+    a.uax = (R)o[6 * nd + i]; a.uay = (R)o[7 * nd + i]; a.uaz = (R)o[8 * nd + i];
+    a.por = (R)o[9 * nd + i]; a.ttf = (R)o[10 * nd + i]; a.tta = (R)o[11 * nd + i];
+    a.wtf = (R)o[12 * nd + i]; a.wta = (R)o[13 * nd + i];
+    a.has_f = (f >> 1) & 1;
+    a.has_a = (f >> 2) & 1;
+    dem_coupling_finish(P, D, DW, i, (f & 1) != 0, a);
 }
 
 // ---------------------------------------------------------------------------
