@@ -925,10 +925,10 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
         DW.dtemp[i] = 0; DW.dtemp1[i] = 0; DW.dtemp2[i] = 0; DW.dtemp3[i] = 0;
     }
     if (D.itype[i] != 1 || D.ptype[i] <= 1000) return;
-    // the contact mechanics in the field precision R over the FP64 state;
-    // overlap and tangential spring in FP64 (functions_DEM_INTERACTION2.cuh
-    // keeps them in Real)
-    using Q = R;
+    // the contact mechanics run in FP64 in both builds (the state is FP64 and
+    // stiff colliding contacts amplify rounding; 0.01 ms per step against R);
+    // the radiation heat rate below is formed in R
+    using Q = double;
     double xi = D.x[i], yi = D.y[i], zi = D.z[i], radi = D.rad[i];
     Q uxi = D.ux[i], uyi = D.uy[i], uzi = D.uz[i], wxi = D.wx[i], wyi = D.wy[i], wzi = D.wz[i];
     Q mi = D.m[i], rii = D.ri[i], rhoi = D.rho[i], tempi = D.temp[i];
