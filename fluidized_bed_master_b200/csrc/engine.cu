@@ -2279,6 +2279,136 @@ extern "C" int sphdem_write_vtk_fluid(SphdemHandle* h, const char* path) {
                                      dtemp.data(), btype.data(), rho.data(), temp.data(), uz.data());
 }
 
+// ---------------------------------------------------------------------------
+// asynchronous output: sphdem_snapshot / sphdem_write_snapshot
+// ---------------------------------------------------------------------------
+static const int SNAP_DEM[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_DEMPOR, SPHDEM_F_UZ, SPHDEM_F_Q_SD,
+                               SPHDEM_F_FTOTALZ, SPHDEM_F_TEMP, SPHDEM_F_RAD, SPHDEM_F_DTEMP, SPHDEM_F_ITYPE,
+                               SPHDEM_F_PTYPE, SPHDEM_F_DEM_IDX};
+static const int SNAP_SPH[] = {SPHDEM_F_X, SPHDEM_F_Y, SPHDEM_F_Z, SPHDEM_F_DEMPOR, SPHDEM_F_PRES, SPHDEM_F_DTEMP,
+                               SPHDEM_F_RHO, SPHDEM_F_TEMP, SPHDEM_F_UZ, SPHDEM_F_PTYPE, SPHDEM_F_BUFFER_TYPE};
+static const int SNAP_MAGF = -1;   // the DEM drag slip magnitude (no ABI field), packed after the fields
+
+template <typename R>
+static int snapshot_t(SphdemHandle* H) {
+    auto* EH = (EngineHost<R>*)H->eng;
+    cudaStream_t st = H->stream;
+    if (!H->snap_stream) {
+        CK(cudaStreamCreateWithFlags(&H->snap_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&H->snap_packed, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&H->snap_done, cudaEventDisableTiming));
+    }
+    // the previous snapshot's copy must be out of the buffers first
+    if (H->snap_pending) CK(cudaEventSynchronize(H->snap_done));
+    std::vector<SphdemHandle::SnapField> fl;
+    std::vector<const void*> src;
+    size_t off = 0;
+    auto add = [&](int which, int field, const void* ptr, int kind, int n) {
+        size_t es = kind == 0 ? sizeof(double) : kind == 1 ? sizeof(R) : sizeof(int);
+        size_t b = es * (size_t)n;
+        fl.push_back({which, field, kind, off, b});
+        src.push_back(ptr);
+        off += (b + 255) & ~(size_t)255;
+    };
+    for (int w = 0; w < 2; w++) {
+        const int* list = w ? SNAP_DEM : SNAP_SPH;
+        int cnt = w ? (int)(sizeof(SNAP_DEM) / sizeof(int)) : (int)(sizeof(SNAP_SPH) / sizeof(int));
+        int n = w ? H->nd : H->ns;
+        for (int k = 0; k < cnt; k++) {
+            const void* ptr;
+            int kind;
+            if (field_ptr<R>(H, w, list[k], &ptr, &kind)) return SPHDEM_E_ARG;
+            add(w, list[k], ptr, kind, n);
+        }
+    }
+    add(1, SNAP_MAGF, EH->E.dw.magf, 0, H->nd);
+    if (off > H->snap_bytes) {
+        if (H->snap_dev) CK(cudaFree(H->snap_dev));
+        if (H->snap_host) CK(cudaFreeHost(H->snap_host));
+        H->snap_dev = nullptr;
+        H->snap_host = nullptr;
+        H->snap_bytes = 0;
+        if (cudaMalloc(&H->snap_dev, off) != cudaSuccess) return SPHDEM_E_NOMEM;
+        if (cudaMallocHost(&H->snap_host, off) != cudaSuccess) return SPHDEM_E_NOMEM;
+        H->snap_bytes = off;
+    }
+    // pack on the step stream: ordered after the steps so far, before the next
+    for (size_t k = 0; k < fl.size(); k++)
+        if (fl[k].bytes)
+            CK(cudaMemcpyAsync(H->snap_dev + fl[k].off, src[k], fl[k].bytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaEventRecord(H->snap_packed, st));
+    // copy out on the output stream while the next steps run
+    CK(cudaStreamWaitEvent(H->snap_stream, H->snap_packed, 0));
+    CK(cudaMemcpyAsync(H->snap_host, H->snap_dev, off, cudaMemcpyDeviceToHost, H->snap_stream));
+    CK(cudaEventRecord(H->snap_done, H->snap_stream));
+    H->snap_fields = fl;
+    H->snap_pending = true;
+    H->snap_t_ref = EH->E.P.t_ref;
+    H->snap_count = H->count;
+    H->snap_time = H->time;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_snapshot(SphdemHandle* h) {
+    if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
+    if (!h || !h->committed) return SPHDEM_E_ARG;
+    return h->prec == SPHDEM_PREC_FP64 ? snapshot_t<double>(h) : snapshot_t<float>(h);
+}
+
+extern "C" int sphdem_write_snapshot(SphdemHandle* h, const char* dem_vtk_path, const char* fluid_vtk_path) {
+    if (!h || !h->snap_pending) return SPHDEM_E_ARG;
+    CK(cudaEventSynchronize(h->snap_done));
+    const bool f32 = h->prec != SPHDEM_PREC_FP64;
+    auto real = [&](int which, int field, double off) {
+        std::vector<double> v;
+        for (auto& f : h->snap_fields) {
+            if (f.which != which || f.field != field) continue;
+            const unsigned char* p = h->snap_host + f.off;
+            size_t es = f.kind == 0 ? 8 : (f.kind == 1 ? (f32 ? 4 : 8) : 4);
+            size_t n = f.bytes / es;
+            v.resize(n);
+            for (size_t i = 0; i < n; i++) {
+                if (f.kind == 0 || (f.kind == 1 && !f32)) v[i] = ((const double*)p)[i] + off;
+                else v[i] = (double)((const float*)p)[i] + off;
+            }
+        }
+        return v;
+    };
+    auto ints = [&](int which, int field) {
+        std::vector<int> v;
+        for (auto& f : h->snap_fields)
+            if (f.which == which && f.field == field) {
+                v.resize(f.bytes / 4);
+                std::memcpy(v.data(), h->snap_host + f.off, f.bytes);
+            }
+        return v;
+    };
+    int r = SPHDEM_OK;
+    if (dem_vtk_path) {
+        int n = h->nd;
+        auto x = real(1, SPHDEM_F_X, 0), y = real(1, SPHDEM_F_Y, 0), z = real(1, SPHDEM_F_Z, 0);
+        auto por = real(1, SPHDEM_F_DEMPOR, 0), uz = real(1, SPHDEM_F_UZ, 0), qsd = real(1, SPHDEM_F_Q_SD, 0);
+        auto ftz = real(1, SPHDEM_F_FTOTALZ, 0), temp = real(1, SPHDEM_F_TEMP, 0), rad = real(1, SPHDEM_F_RAD, 0);
+        auto dtemp = real(1, SPHDEM_F_DTEMP, 0), magf = real(1, SNAP_MAGF, 0);
+        auto it = ints(1, SPHDEM_F_ITYPE), pt = ints(1, SPHDEM_F_PTYPE), idx = ints(1, SPHDEM_F_DEM_IDX);
+        std::vector<double> eliz(n, 1.0);
+        r = sphdem_io_write_vtk_dem(dem_vtk_path, n, x.data(), y.data(), z.data(), it.data(), pt.data(), idx.data(),
+                                    magf.data(), eliz.data(), por.data(), uz.data(), qsd.data(), ftz.data(),
+                                    temp.data(), rad.data(), dtemp.data());
+        if (r) return r;
+    }
+    if (fluid_vtk_path) {
+        int n = h->ns;
+        auto x = real(0, SPHDEM_F_X, 0), y = real(0, SPHDEM_F_Y, 0), z = real(0, SPHDEM_F_Z, 0);
+        auto por = real(0, SPHDEM_F_DEMPOR, 0), pres = real(0, SPHDEM_F_PRES, 0), dtemp = real(0, SPHDEM_F_DTEMP, 0);
+        auto rho = real(0, SPHDEM_F_RHO, 0), temp = real(0, SPHDEM_F_TEMP, h->snap_t_ref), uz = real(0, SPHDEM_F_UZ, 0);
+        auto pt = ints(0, SPHDEM_F_PTYPE), bt = ints(0, SPHDEM_F_BUFFER_TYPE);
+        r = sphdem_io_write_vtk_fluid(fluid_vtk_path, n, pt.data(), x.data(), y.data(), z.data(), por.data(),
+                                      pres.data(), dtemp.data(), bt.data(), rho.data(), temp.data(), uz.data());
+    }
+    return r;
+}
+
 extern "C" int sphdem_write_restart(SphdemHandle* h, const char* path) {
     if (h && h->kind == 1) return SPHDEM_E_UNSUPPORTED;   // ISPH-DEM engine only
     if (!h || !path || !h->committed) return SPHDEM_E_ARG;
@@ -2357,6 +2487,12 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     for (cudaEvent_t e : h->ev_end) cudaEventDestroy(e);
     if (h->eng) engine_destroy(h);
     if (h->xfer) cudaFree(h->xfer);
+    if (h->snap_stream) cudaStreamSynchronize(h->snap_stream);
+    if (h->snap_dev) cudaFree(h->snap_dev);
+    if (h->snap_host) cudaFreeHost(h->snap_host);
+    if (h->snap_packed) cudaEventDestroy(h->snap_packed);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
+    if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -53,6 +53,23 @@ struct SphdemHandle {
     // at commit with its x, y shifted by bed_off[2b], bed_off[2b+1]
     std::vector<int> bed_start;
     std::vector<double> bed_off;
+    // asynchronous output (sphdem_snapshot): the VTK fields packed into a
+    // device buffer on the step stream, copied to pinned host memory on a
+    // second stream; one entry per packed field
+    struct SnapField {
+        int which, field, kind;   // kind: 0 double, 1 R, 2 int32
+        size_t off, bytes;
+    };
+    std::vector<SnapField> snap_fields;
+    unsigned char* snap_dev = nullptr;
+    unsigned char* snap_host = nullptr;
+    size_t snap_bytes = 0;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_packed = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
+    double snap_t_ref = 0.0;      // offset of the SPH temperature at the snapshot
+    int snap_count = 0;
+    double snap_time = 0.0;
 };
 
 // io.cpp

@@ -50,6 +50,8 @@ def lib():
     L.sphdem_get_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_write_vtk_dem.argtypes = [vp, C.c_char_p]
     L.sphdem_write_vtk_fluid.argtypes = [vp, C.c_char_p]
+    L.sphdem_snapshot.argtypes = [vp]
+    L.sphdem_write_snapshot.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.sphdem_set_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
     L.sphdem_set_graphs.argtypes = [vp, C.c_int]
@@ -306,6 +308,15 @@ class Engine:
 
     def write_vtk_fluid(self, path):
         _chk(lib().sphdem_write_vtk_fluid(self._h, os.fsencode(path)), "sphdem_write_vtk_fluid")
+
+    def snapshot(self):
+        """sphdem_snapshot: start copying the output fields of this step to the host."""
+        _chk(lib().sphdem_snapshot(self._h), "sphdem_snapshot")
+
+    def write_snapshot(self, dem_vtk=None, fluid_vtk=None):
+        """sphdem_write_snapshot: wait for the last snapshot and write its VTK files."""
+        _chk(lib().sphdem_write_snapshot(self._h, os.fsencode(dem_vtk) if dem_vtk else None,
+                                         os.fsencode(fluid_vtk) if fluid_vtk else None), "sphdem_write_snapshot")
 
     def write_restart(self, path):
         _chk(lib().sphdem_write_restart(self._h, os.fsencode(path)), "sphdem_write_restart")

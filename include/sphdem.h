@@ -455,6 +455,20 @@ int sphdem_write_vtk_dem(SphdemHandle* h, const char* path);
  * (zero), and are zero here. */
 int sphdem_write_vtk_fluid(SphdemHandle* h, const char* path);
 
+/* Output off the critical path.  sphdem_snapshot enqueues, on the handle's
+ * stream after the steps enqueued so far, copies of the fields of the DEM
+ * and fluid VTK files into a device buffer, and their copy into pinned host
+ * memory on a second stream; it returns without waiting, and the next
+ * sphdem_step calls run on the GPU while that copy is in flight (the
+ * reference copies P1/P2/P3 to the host synchronously inside its step,
+ * ISPH_Calc_seperate.cuh:468-490).  sphdem_write_snapshot waits for the copy
+ * and writes the files of the snapshot's step (either path may be NULL);
+ * they are byte-identical to sphdem_write_vtk_dem / sphdem_write_vtk_fluid
+ * at that step.  A new snapshot first waits for the previous copy and
+ * replaces it. */
+int sphdem_snapshot(SphdemHandle* h);
+int sphdem_write_snapshot(SphdemHandle* h, const char* dem_vtk_path, const char* fluid_vtk_path);
+
 /* Restart file in input.txt format: tab-separated column labels then one
  * row per particle with all columns (fixes save_restart,
  * functions_OUTPUT.cuh:1926-1955). */

@@ -104,3 +104,30 @@ def test_fluid_vtk_layout():
     assert not v["conv_rate"].any() and not v["cond_rate"].any()
     assert list(v)[1:] == ["porosity", "conv_rate", "pressure", "cond_rate", "dtemp", "buffer_type", "density",
                            "temperature", "uz"]
+
+
+def test_snapshot_files_equal_sync_writers():
+    """sphdem_snapshot copies the output fields while the next steps run;
+    sphdem_write_snapshot then writes the files of the snapshot's step,
+    byte-identical to the synchronous writers at that step, and the run
+    itself is unchanged by the snapshot."""
+    g, p, sph, dem = load_golden(ISPH_GOLD[0])
+    q = p.copy()
+    q.con_solve = 1
+    a = _engine(q, sph, dem, 0)
+    b = _engine(q, sph, dem, 0)
+    a.step(3)
+    a.snapshot()
+    a.step(2)                      # runs while the snapshot is copied out
+    b.step(3)
+    with tempfile.TemporaryDirectory() as d:
+        ad, af = os.path.join(d, "a_dem.vtk"), os.path.join(d, "a_fluid.vtk")
+        bd, bf = os.path.join(d, "b_dem.vtk"), os.path.join(d, "b_fluid.vtk")
+        a.write_snapshot(ad, af)
+        b.write_vtk_dem(bd)
+        b.write_vtk_fluid(bf)
+        for x, y in ((ad, bd), (af, bf)):
+            assert open(x, "rb").read() == open(y, "rb").read(), os.path.basename(x)
+    b.step(2)
+    for f in ("x", "uz", "pres", "temp"):
+        assert np.array_equal(a.get(SPH, f), b.get(SPH, f)), f
