@@ -19,6 +19,8 @@ namespace sphdem {
 // the grid computed at commit time.
 struct DevParams {
     int kernel_type, dim, kgc, delsph, fp, fv, fva, fg, con, xsph, open_bc, rho_type;
+    int iface, fb;            // interface sharpness force, repulsive boundary force (pass B)
+    double c_repulsive;       // vif[14], strength of the repulsive boundary force
     int NI, NJ, NK, num_cells;
     int ns, nd, nb_cap;
     int nbd_cap;              // SPH -> DEM list entries per particle

@@ -707,6 +707,7 @@ static int commit_t(SphdemHandle* H) {
     std::memset(&P, 0, sizeof(P));
     P.kernel_type = p.kernel_type; P.dim = p.dim; P.kgc = p.kgc_solve; P.delsph = p.delSPH_solve;
     P.fp = p.fp_solve; P.fv = p.fv_solve; P.fva = p.fva_solve; P.fg = p.fg_solve; P.con = p.con_solve;
+    P.iface = p.interface_solve; P.fb = p.fb_solve; P.c_repulsive = p.c_repulsive;
     P.xsph = p.xsph_solve; P.open_bc = p.open_boundary; P.rho_type = p.rho_type;
     P.NI = NI; P.NJ = NJ; P.NK = NK; P.num_cells = num_cells;
     P.ns = ns; P.nd = nd;
@@ -1646,8 +1647,8 @@ static int check_supported(const SphdemParams* p) {
     }
     if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
     if (p->dim != 3) return SPHDEM_E_UNSUPPORTED;
-    if (p->prop_table || p->fs_solve || p->fb_solve || p->interface_solve || p->boussinesq_solve ||
-        p->concn_solve || p->pst_solve || p->turbulence_model != 0 || p->penetration_solve || p->noslip_bc)
+    if (p->prop_table || p->fs_solve || p->boussinesq_solve || p->concn_solve || p->pst_solve ||
+        p->turbulence_model != 0 || p->penetration_solve || p->noslip_bc)
         return SPHDEM_E_UNSUPPORTED;
     if (p->kgc_solve != 0 && p->kgc_solve != 1) return SPHDEM_E_UNSUPPORTED;
     if (p->time_type != 1) return SPHDEM_E_UNSUPPORTED;

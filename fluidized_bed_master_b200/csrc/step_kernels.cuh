@@ -874,6 +874,29 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                     tz += -Pij * gz;
                 }
             }
+            if (P.iface | P.fb) {
+                const int ptj = tag_ptype(t.q.w);
+                if (P.iface) {
+                    // interface sharpness force (functions_PPE2.cuh:1450-1464): raw
+                    // kernel slope; the neighbour's pressure only across a fluid-fluid
+                    // interface (wall 0 and moving 9 excluded)
+                    const bool flag = (pt != 0) && (pt != 9) && (ptj != 0) && (ptj != 9) && (pt != ptj);
+                    const R mri = mi * irhoi, mrj = mj * irj;
+                    R Ci = fabs(pi) * mri * mri + fabs(uj.w) * mrj * mrj * (R)flag;
+                    Ci *= ((R)0.08 / mi) * dw * rinv;
+                    tx += Ci * -g.dx;
+                    ty += Ci * -g.dy;
+                    tz += Ci * -g.dz;
+                }
+                if (P.fb && pt == 1 && ptj != 1) {
+                    // repulsive force of non-fluid neighbours (functions_PPE2.cuh:1465-1472)
+                    const R rr = r + (R)1e-10;
+                    const R fb = (R)P.c_repulsive / rr / rr * kw(K, r) * ((R)2 * mj / (mi + mj));
+                    tx += fb * g.dx;
+                    ty += fb * g.dy;
+                    tz += fb * g.dz;
+                }
+            }
             if (eli < (R)1) {
                 R mr = mj * irj * ((R)1 - eli);
                 R ug = uxi * gx + uyi * gy + uzi * gz;

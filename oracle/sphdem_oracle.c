@@ -622,9 +622,9 @@ static void k_prep3d_sph(OracleState* S) {
 
 /* KERNEL_advection_force3D_sph: functions_PPE2.cuh:1251-1607 (pressure-
  * gradient force density, viscous Laplacian, artificial viscosity,
- * gravity, Eulerian convection, conduction).  Surface tension,
- * interface, boundary-force, concentration and Boussinesq branches are
- * rejected by the switch check. */
+ * interface sharpness force, repulsive boundary force, gravity, Eulerian
+ * convection, conduction).  Surface tension, concentration and Boussinesq
+ * branches are rejected by the switch check. */
 static void k_advection(OracleState* S) {
     OSet* o = &S->s;
     const SphdemParams* P = &S->p;
@@ -693,6 +693,28 @@ static void k_advection(OracleState* S) {
                             tx += -(Pij) * tdwx;
                             ty += -(Pij) * tdwy;
                             tz += -(Pij) * tdwz;
+                        }
+                    }
+                    if (P->interface_solve) {
+                        /* interface sharpness force (functions_PPE2.cuh:1450-1464): the raw
+                         * kernel slope, the neighbour's pressure only across a fluid-fluid
+                         * interface (BOUNDARY 0, MOVING 9) */
+                        int flag = (pti != 0) && (pti != 9) && (ptj != 0) && (ptj != 9) && (pti != ptj);
+                        double mri = mi / rhoi, mrj = mj / rhoj;
+                        double Ci = fabs(pi) * mri * mri + fabs(pj) * mrj * mrj * (flag);
+                        Ci *= (0.08 / mi) * dw / td;
+                        tx += Ci * (xj - xi);
+                        ty += Ci * (yj - yi);
+                        tz += Ci * (zj - zi);
+                    }
+                    if (P->fb_solve) {
+                        /* repulsive force of non-fluid neighbours on a fluid particle
+                         * (functions_PPE2.cuh:1465-1472), with the kernel value */
+                        if ((pti == 1) & (ptj != 1)) {
+                            double fb = P->c_repulsive / (td + 1e-10) / (td + 1e-10) * w * (2 * mj / (mi + mj));
+                            tx += fb * (xi - xj);
+                            ty += fb * (yi - yj);
+                            tz += fb * (zi - zj);
                         }
                     }
                     if (elix < 1.0 || eliy < 1.0) {

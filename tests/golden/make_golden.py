@@ -63,6 +63,10 @@ CASES = {
     # radiation, contact conduction, convective exchange)
     "heat": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=12, spacing=1.9, u_dem=0.05),
              dict(con_solve=1), [1, 8, 100]),
+    # the interface-sharpness and repulsive boundary forces of the advection
+    # pass switched on (functions_PPE2.cuh:1450-1472)
+    "forces": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=13, spacing=1.9, u_dem=0.05),
+               dict(interface_solve=1, fb_solve=1), [1, 8, 100]),
 }
 
 
