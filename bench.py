@@ -188,12 +188,13 @@ def manifest_bytes(kernel, ns, nd, nwall, nbuf, avg_nb, r):
         "neumann": nwall * (pos + 4 * r),
         "open_bc": nbuf * (pos + 8 * r),
         "sph_coupling": ns * (pos + 12 * r),
-        "dem_contact": nd * (5 * 8 + 12 * r + 16 * 28),
-        "dem_coupling": nd * (5 * 8 + 20 * r),
-        "dem_prep": nd * (5 * 8 + 6 * r),
-        "dem_update": nd * (3 * 8 + 20 * r),
+        # the DEM set is FP64 in both builds
+        "dem_contact": nd * (5 * 8 + 12 * 8 + 16 * 28),
+        "dem_coupling": nd * (5 * 8 + 20 * 8),
+        "dem_prep": nd * (5 * 8 + 6 * 8),
+        "dem_update": nd * (3 * 8 + 20 * 8),
         "cells_gather_sph": ns * 2 * (pos + 9 * r + 16) + ns * 8,
-        "cells_gather_dem": nd * 2 * (5 * 8 + 17 * r + 20 + 16 * 28) + nd * 8,
+        "cells_gather_dem": nd * 2 * (5 * 8 + 17 * 8 + 20 + 16 * 28) + nd * 8,
         "hash_sph": ns * (24 + 4 + 8),
         "hash_dem": nd * (24 + 4 + 8),
     }

@@ -551,7 +551,11 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         *nl += 1;
     }
     if (ns > 0) {
-        { KTIME(KT_PASSB); k_passB<R><<<bs, TPB, 0, st>>>(P, S, W, E.flags); }
+        {
+            KTIME(KT_PASSB);
+            if (P.iface | P.fb) k_passB<R, true><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
+            else k_passB<R, false><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
+        }
         *nl += 1;
     }
     if (nd > 0) {

@@ -794,8 +794,20 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
 // The delta-SPH density gradient of prep3D is not formed: no kernel of the
 // ISPH step reads it.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
+// FORCES: the interface-sharpness / repulsive boundary force switches are on
+// (a separate instantiation, so that the default pass keeps its registers)
+#ifdef SPHDEM_PASSB_MINB
+#define SPHDEM_PASSB_BOUNDS __launch_bounds__(128, SPHDEM_PASSB_MINB)
+#else
+#define SPHDEM_PASSB_BOUNDS __launch_bounds__(128)
+#endif
+#ifdef SPHDEM_CONTACT_MINB
+#define SPHDEM_CONTACT_BOUNDS __launch_bounds__(128, SPHDEM_CONTACT_MINB)
+#else
+#define SPHDEM_CONTACT_BOUNDS __launch_bounds__(128)
+#endif
+template <typename R, bool FORCES>
+__global__ void SPHDEM_PASSB_BOUNDS k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -874,7 +886,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                     tz += -Pij * gz;
                 }
             }
-            if (P.iface | P.fb) {
+            if (FORCES) {
                 const int ptj = tag_ptype(t.q.w);
                 if (P.iface) {
                     // interface sharpness force (functions_PPE2.cuh:1450-1464): raw
@@ -928,7 +940,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // the reference).  Spring increments and overlap are FP64.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
+__global__ void SPHDEM_CONTACT_BOUNDS k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
                                                      const int4* __restrict__ drows,
                                                      DevFlags* F) {
     // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
@@ -965,6 +977,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
                                       (R)1.10479e-10 * tiR * tiR * tiR)
                                    : (R)0.842337;
     Q radiR = (Q)radi;
+    const Q imi = (Q)1 / mi, iradi = (Q)1 / radiR;   // hoisted reciprocals of the sphere's own terms
     Q dr2 = ((Q)1 / (Q)6) * radiR;
     Q volm = ((Q)4 / (Q)3) * (Q)3.141592 * (radiR * radiR * radiR - (radiR - dr2) * (radiR - dr2) * (radiR - dr2));
     int oid[SPHDEM_NSLOT];
@@ -992,7 +1005,7 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
         double ovlp = radi + radj - td;
         int demj = D.dem_idx[j];
         Q radjR = (Q)radj;
-        Q radij = (Q)1 / ((Q)1 / radiR + (Q)1 / radjR);
+        Q radij = (Q)1 / (iradi + (Q)1 / radjR);
         Q tdR = (Q)td;
         if (P.con) {
             // radiation between spheres within the search range (functions_DEM_INTERACTION2.cuh:
@@ -1002,7 +1015,8 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
             R emj = (tj >= (R)700) ? ((R)0.505586 + (R)7.92943e-4 * tj - (R)5.228643e-7 * tj * tj +
                                       (R)1.10479e-10 * tj * tj * tj)
                                    : (R)0.842337;
-            R ai = riR / tdF, aj = rjR / tdF, dij = aj - ai;
+            const R itdF = rcp(tdF);
+            R ai = riR * itdF, aj = rjR * itdF, dij = aj - ai;
             R dc_r = (R)0.56 * ((R)2 * rijR);
             R dc_ar = (R)3.14159 * dc_r * dc_r;
             R dmax = (R)0.5 * (sqrt((R)1 + (R)4 * dc_ar / ((R)3.14159 * tdF * tdF * ((R)1 - dij * dij))) - dij);
@@ -1045,7 +1059,8 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
                 dsz = D.hds[(slot * 3 + 2) * n + i];
             }
             Q mj = D.m[j];
-            Q nx = (Q)((xj - xi) / td), ny = (Q)((yj - yi) / td), nz = (Q)((zj - zi) / td);
+            const Q itd = (Q)1 / (Q)td;
+            Q nx = (Q)(xj - xi) * itd, ny = (Q)(yj - yi) * itd, nz = (Q)(zj - zi) * itd;
             Q li = radiR - (Q)0.5 * tov, lj = radjR - (Q)0.5 * tov;
             Q rcxi = li * nx, rcyi = li * ny, rczi = li * nz;
             Q rcxj = -lj * nx, rcyj = -lj * ny, rczj = -lj * nz;
@@ -1061,18 +1076,18 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
             dsx += (double)usx * kdt;
             dsy += (double)usy * kdt;
             dsz += (double)usz * kdt;
-            Q usm = sqrt(usx * usx + usy * usy + usz * usz) + (Q)1e-20;
-            Q sx = usx / usm, sy = usy / usm, sz = usz / usm;
-            Q mij = (Q)1 / ((Q)1 / mi + (Q)1 / mj);
-            Q sq = sqrt(radij * tov);
-            Q Cspr = (Q)1.33333 * ymij * sqrt(radij) * sqrt(tov) * tov / mi;
-            Q Cspr_s = (Q)8 * Gij * sq / mi;
+            const Q iusm = (Q)1 / (sqrt(usx * usx + usy * usy + usz * usz) + (Q)1e-20);
+            Q sx = usx * iusm, sy = usy * iusm, sz = usz * iusm;
+            Q mij = (Q)1 / (imi + (Q)1 / mj);
+            Q sq = sqrt(radij * tov);   // sqrt(R* delta): also stands for sqrt(R*) sqrt(delta)
+            Q Cspr = (Q)1.33333 * ymij * sq * tov * imi;
+            Q Cspr_s = (Q)8 * Gij * sq * imi;
             Q Kn = (Q)2 * ymij * sq;
-            Q Cd = cdamp * sqrt(mij * Kn) / mi;
-            Q Cds = cdamp * sqrt(mij * Cspr_s * mi) / mi;
-            tx += Cspr * (Q)((xi - xj) / td);
-            ty += Cspr * (Q)((yi - yj) / td);
-            tz += Cspr * (Q)((zi - zj) / td);
+            Q Cd = cdamp * sqrt(mij * Kn) * imi;
+            Q Cds = cdamp * sqrt(mij * Cspr_s * mi) * imi;
+            tx += Cspr * -nx;
+            ty += Cspr * -ny;
+            tz += Cspr * -nz;
             tx += Cd * unx;
             ty += Cd * uny;
             tz += Cd * unz;
@@ -1082,11 +1097,12 @@ __global__ void __launch_bounds__(128) k_dem_contact(DevParams P, DemState<doubl
             Q sgx = (fssx >= (Q)0) ? (Q)1 : (Q)-1;
             Q sgy = (fssy >= (Q)0) ? (Q)1 : (Q)-1;
             Q sgz = (fssz >= (Q)0) ? (Q)1 : (Q)-1;
-            Q mfss = sqrt(fssx * fssx + fssy * fssy + fssz * fssz);
+            // stick while |f_spring| < |f_friction| (the squares compare the same way)
+            Q mfss2 = fssx * fssx + fssy * fssy + fssz * fssz;
             Q fr = (Q)P.fric * Cspr;
             Q ffx = fr * sx, ffy = fr * sy, ffz = fr * sz;
-            Q mfsf = sqrt(ffx * ffx + ffy * ffy + ffz * ffz);
-            bool stick = mfss < mfsf;
+            Q mfsf2 = ffx * ffx + ffy * ffy + ffz * ffz;
+            bool stick = mfss2 < mfsf2;
             Q fsx = stick ? fssx : sgx * fabs(ffx);
             Q fsy = stick ? fssy : sgy * fabs(ffy);
             Q fsz = stick ? fssz : sgz * fabs(ffz);
