@@ -796,18 +796,8 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
 // ---------------------------------------------------------------------------
 // FORCES: the interface-sharpness / repulsive boundary force switches are on
 // (a separate instantiation, so that the default pass keeps its registers)
-#ifdef SPHDEM_PASSB_MINB
-#define SPHDEM_PASSB_BOUNDS __launch_bounds__(128, SPHDEM_PASSB_MINB)
-#else
-#define SPHDEM_PASSB_BOUNDS __launch_bounds__(128)
-#endif
-#ifdef SPHDEM_CONTACT_MINB
-#define SPHDEM_CONTACT_BOUNDS __launch_bounds__(128, SPHDEM_CONTACT_MINB)
-#else
-#define SPHDEM_CONTACT_BOUNDS __launch_bounds__(128)
-#endif
 template <typename R, bool FORCES>
-__global__ void SPHDEM_PASSB_BOUNDS k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
+__global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -940,7 +930,9 @@ __global__ void SPHDEM_PASSB_BOUNDS k_passB(DevParams P, SphState<R> S, SphWork<
 // the reference).  Spring increments and overlap are FP64.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void SPHDEM_CONTACT_BOUNDS k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
+// 4 blocks of 128 per SM (128 registers, a few spilled): 0.145 -> 0.124 ms on
+// the bench bed against the unbounded 162-register build
+__global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
                                                      const int4* __restrict__ drows,
                                                      DevFlags* F) {
     // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
