@@ -352,20 +352,20 @@ def write_solv_txt(path, p):
         "simulation type (Single_Phase/Two_Phase):\tSingle_Phase",
         "pressure-force solve(YES/NO): \t" + yn(p.fp_solve),
         "viscous-force solve(YES/NO): \t" + yn(p.fv_solve),
-        "turbulence-model (Laminar/k-lm/k-e/SPS/HB): Laminar",
+        "turbulence-model (Laminar/k-lm/k-e/SPS/HB): " + ("Laminar", "k-lm", "k-e", "SPS", "HB")[p.turbulence_model],
         "artificial-viscous-force solve(YES/NO): \t" + yn(p.fva_solve),
         "gravitational-force solve(YES/NO): \t" + yn(p.fg_solve),
         "surface-tension-force solve(YES/NO): \t" + yn(p.fs_solve),
-        "surface-tension-model (Potential/Curvature)\tPotential",
+        "surface-tension-model (Potential/Curvature)\t" + ("Curvature" if p.surf_model == 2 else "Potential"),
         "interface-sharpness-force solve(YES/NO):\t" + yn(p.interface_solve),
         "boundary-force solve(YES/NO):\t" + yn(p.fb_solve),
         "Conduction(YES/NO):\t" + yn(p.con_solve),
-        "Boussinesq-natural-convection solve(YES/NO):\tNO",
-        "Concentration-diffusion(YES/NO):\tNO",
+        "Boussinesq-natural-convection solve(YES/NO):\t" + yn(p.boussinesq_solve),
+        "Concentration-diffusion(YES/NO):\t" + yn(p.concn_solve),
         "XSPH solve(YES/NO): \t" + yn(p.xsph_solve),
         "kernel-gradient-correction solve(NO/KGC/FPM/DFPM/KGF):\t" + ("KGC" if p.kgc_solve == 1 else "NO"),
         "delta-SPH solve(NO/Molteni/Antuono):\t" + {0: "NO", 1: "Molteni", 2: "Antuono"}[p.delSPH_solve],
-        "particle-shifting solve(YES/NO):\tNO",
+        "particle-shifting solve(YES/NO):\t" + yn(p.pst_solve),
         "penetration_box solve(YES/NO):           NO",
         "noslip_boundary (YES/NO):                NO",
         "open boundary (OPEN/PERIODIC/NO):\t" + {0: "NO", 1: "OPEN", 2: "PERIODIC"}[p.open_boundary],

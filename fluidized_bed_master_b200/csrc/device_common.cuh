@@ -20,6 +20,8 @@ namespace sphdem {
 struct DevParams {
     int kernel_type, dim, kgc, delsph, fp, fv, fva, fg, con, xsph, open_bc, rho_type;
     int iface, fb;            // interface sharpness force, repulsive boundary force (pass B)
+    int sps;                  // fv_solve with the SPS turbulence model: eddy viscosity (k_sps)
+    int ipf;                  // surface tension, inter-particle force model (fs_solve, surf_model 1)
     double c_repulsive;       // vif[14], strength of the repulsive boundary force
     int NI, NJ, NK, num_cells;
     int ns, nd, nb_cap;

@@ -56,23 +56,26 @@ static void record_event(cudaEvent_t e, cudaStream_t s) {
     else cudaEventRecord(e, s);
 }
 
+// events around a kernel (group) on the stream it is launched on
 struct KTimer {
     SphdemHandle* H;
     int k;
-    KTimer(SphdemHandle* h, int kk) : H(h), k(kk) {
+    cudaStream_t s;
+    KTimer(SphdemHandle* h, int kk, cudaStream_t st = nullptr) : H(h), k(kk), s(st ? st : h->stream) {
         if (H->timing) {
-            record_event(H->ev_beg[k], H->stream);
+            record_event(H->ev_beg[k], s);
             H->ev_used[k] = 1;
         }
     }
     void stop() {
-        if (H->timing && !stopped) record_event(H->ev_end[k], H->stream);
+        if (H->timing && !stopped) record_event(H->ev_end[k], s);
         stopped = true;
     }
     ~KTimer() { stop(); }
     bool stopped = false;
 };
 #define KTIME(k) KTimer kt_##__LINE__(H, k)
+#define KTIME_ON(k, st) KTimer kt_##__LINE__(H, k, st)
 
 // ---------------------------------------------------------------------------
 // allocation
@@ -154,7 +157,7 @@ void alloc_work(Alloc& A, SphWork<R>& W, DemWork<double>& DW, int ns, int nd, in
     W.ftx = A.get<R>(ns); W.fty = A.get<R>(ns); W.ftz = A.get<R>(ns); W.ftot = A.get<R>(ns);
     W.fpx = A.get<R>(ns); W.fpy = A.get<R>(ns); W.fpz = A.get<R>(ns);
     W.pgfx = A.get<R>(ns); W.pgfy = A.get<R>(ns); W.pgfz = A.get<R>(ns);
-    W.dtemp = A.get<R>(ns); W.temp0 = A.get<R>(ns);
+    W.dtemp = A.get<R>(ns); W.temp0 = A.get<R>(ns); W.vist = A.get<R>(ns);
     W.ux0 = A.get<R>(ns); W.uy0 = A.get<R>(ns); W.uz0 = A.get<R>(ns);
     W.p_new = A.get<R>(ns);
     W.u_tmpx = A.get<R>(ns); W.u_tmpy = A.get<R>(ns); W.u_tmpz = A.get<R>(ns); W.temp_tmp = A.get<R>(ns);
@@ -256,11 +259,10 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
 }
 
 template <typename R>
-int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) {
+int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl, cudaStream_t st) {
     Engine<R>& E = EH->E;
     DevParams& P = E.P;
     DemWork<double>& DW = E.dw;
-    cudaStream_t st = H->stream;
     int n = P.nd;
     if (n == 0) {
         CK(cudaMemsetAsync(DW.g_str, 0xff, sizeof(int) * (P.num_cells + 1), st));
@@ -269,21 +271,21 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     }
     DemState<double>& D = E.D[src];
     {
-        KTIME(KT_HASH_D);
+        KTIME_ON(KT_HASH_D, st);
         k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, E.cs_d.cnt);
     }
     {
-        KTIME(KT_SORT_D);
+        KTIME_ON(KT_SORT_D, st);
         CK(cell_sort(E.cs_d, n, DW.key_in, DW.val_out, DW.key_out, DW.g_str, DW.g_end, st));
     }
     {
-        KTIME(KT_GATHER_D);
+        KTIME_ON(KT_GATHER_D, st);
         k_cells_gather_dem<double><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.val_out);
         k_gather_history<<<nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st>>>(n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
                                                                          E.D[dst].hds);
     }
     {
-        KTIME(KT_ROWS_D);
+        KTIME_ON(KT_ROWS_D, st);
         k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, DW.g_str, DW.g_end, DW.rows);
     }
     *nl += 8;
@@ -506,6 +508,20 @@ void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double
 // ---------------------------------------------------------------------------
 // one step (SOPHIA_single_ISPH order).  flags: bit1 count==0, bit2 filter
 // step, bit3 time==0.
+//
+// The DEM kernels that read no SPH pass run on a second stream, forked from
+// and joined to the step stream by events (in the step graph: parallel
+// branches):
+//   step stream: SPH NNPS -> list -> [DEM sorted] dlist -> pass A -> pass B
+//                -> [DEM prep done] DEM coupling -> SPH coupling -> walls, PPE,
+//                pass C, open boundary, XSPH -> [DEM update done] tick
+//   DEM stream:  DEM NNPS -> contact -> [SPH gathered] DEM prep
+//                ... [SPH coupling done] DEM corrector + walls
+// The DEM contact reads only the DEM set; the DEM prep reads the gathered
+// SPH records and the DEM set; the DEM corrector writes the DEM set after
+// the SPH coupling has read it, and no later SPH kernel reads it.  Without
+// both sets everything runs on the step stream in the same order.  The
+// per-kernel timing events of a DEM kernel are recorded on its own stream.
 // ---------------------------------------------------------------------------
 enum { F_COUNT0 = 2, F_FILT = 4, F_TIME0 = 8 };
 
@@ -519,12 +535,30 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int ns = P.ns, nd = P.nd;
     int so = E.cur_s, sn = 1 - E.cur_s, dox = E.cur_d, dn = 1 - E.cur_d;
     int r;
-    if ((r = nnps_sph<R>(H, EH, so, sn, nl))) return r;
-    if ((r = nnps_dem<R>(H, EH, dox, dn, nl))) return r;
+    const bool fork = ns > 0 && nd > 0 && H->dem_stream;
+    cudaStream_t sd = fork ? H->dem_stream : st;
+    // event k recorded on stream a / waited for on stream b (fork only)
+    auto rec = [&](int k, cudaStream_t a) { return fork ? cudaEventRecord(H->fork_ev[k], a) : cudaSuccess; };
+    auto wait = [&](int k, cudaStream_t b) { return fork ? cudaStreamWaitEvent(b, H->fork_ev[k], 0) : cudaSuccess; };
+    CK(rec(0, st));
+    CK(wait(0, sd));
+    if ((r = nnps_dem<R>(H, EH, dox, dn, nl, sd))) return r;
+    CK(rec(1, sd));   // DEM set sorted
     SphState<R>& S = E.S[sn];
     DemState<double>& D = E.D[dn];
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
+    if (nd > 0) {
+        { KTIME_ON(KT_DEMCONTACT, sd); k_dem_contact<R><<<bdw, TPB, 0, sd>>>(P, D, DW, DW.rows, E.flags); }
+        *nl += 1;
+    }
+    if ((r = nnps_sph<R>(H, EH, so, sn, nl))) return r;
+    CK(rec(2, st));   // SPH set gathered
+    CK(wait(2, sd));
+    if (nd > 0) {
+        { KTIME_ON(KT_DEMPREP, sd); k_dem_prep<R><<<bdw, TPB, 0, sd>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
+        *nl += 1;
+    }
     if (ns > 0) {
         {
             KTIME(KT_LIST);
@@ -538,6 +572,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
                 k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags);
             }
         }
+        CK(wait(1, st));
         if (nd > 0) {
             KTIME(KT_DLIST);
             launch_dlist<R>(EH, S, D, st);
@@ -545,30 +580,40 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         }
         { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
         *nl += 2;
-    }
-    if (nd > 0) {
-        { KTIME(KT_DEMPREP); k_dem_prep<R><<<bdw, TPB, 0, st>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
-        *nl += 1;
-    }
-    if (ns > 0) {
         {
             KTIME(KT_PASSB);
-            if (P.iface | P.fb) k_passB<R, true><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
+            if (P.sps) {
+                k_sps<R><<<bs, TPB, 0, st>>>(P, S, W);
+                *nl += 1;
+            }
+            if (P.iface | P.fb | P.sps | P.ipf) k_passB<R, true><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
             else k_passB<R, false><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
         }
         *nl += 1;
     }
+    CK(rec(3, sd));   // DEM contact and prep done
+    CK(wait(1, st));  // (without SPH particles the list wait above was skipped)
+    CK(wait(3, st));
     if (nd > 0) {
-        { KTIME(KT_DEMCONTACT); k_dem_contact<R><<<bdw, TPB, 0, st>>>(P, D, DW, DW.rows, E.flags); }
         {
             KTIME(KT_DEMCOUPLING);
             k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows);
             k_dem_finish<R><<<bd, TPB, 0, st>>>(P, D, DW);
         }
-        *nl += 3;
+        *nl += 2;
     }
     if (ns > 0) {
-        { KTIME(KT_SPHCOUPLING); k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0); }
+        KTIME(KT_SPHCOUPLING);
+        k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0);
+        *nl += 1;
+    }
+    CK(rec(4, st));   // the SPH coupling has read the DEM set
+    CK(wait(4, sd));
+    if (nd > 0) {
+        { KTIME_ON(KT_DEMUPDATE, sd); k_dem_update<double><<<bd, TPB, 0, sd>>>(P, D, DW); }
+        *nl += 1;
+    }
+    if (ns > 0) {
         if (flags & F_COUNT0) {
             KTIME(KT_NEUMANN0);
             if constexpr (std::is_same<R, float>::value)
@@ -592,13 +637,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
                 k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0);
         }
         { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
-        *nl += 4;
-    }
-    if (nd > 0) {
-        { KTIME(KT_DEMUPDATE); k_dem_update<double><<<bd, TPB, 0, st>>>(P, D, DW); }
-        *nl += 1;
-    }
-    if (ns > 0) {
+        *nl += 3;
         if (P.open_bc > 0) {
             KTIME(KT_OPENBC);
             k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.rows);
@@ -610,6 +649,8 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             *nl += 1;
         }
     }
+    CK(rec(5, sd));   // join
+    CK(wait(5, st));
     k_tick<<<1, 1, 0, st>>>(E.flags);
     *nl += 1;
     CK(cudaGetLastError());
@@ -712,6 +753,8 @@ static int commit_t(SphdemHandle* H) {
     P.kernel_type = p.kernel_type; P.dim = p.dim; P.kgc = p.kgc_solve; P.delsph = p.delSPH_solve;
     P.fp = p.fp_solve; P.fv = p.fv_solve; P.fva = p.fva_solve; P.fg = p.fg_solve; P.con = p.con_solve;
     P.iface = p.interface_solve; P.fb = p.fb_solve; P.c_repulsive = p.c_repulsive;
+    P.sps = p.fv_solve == 1 && p.turbulence_model == 3;   // SPS (Parameters.cuh:111)
+    P.ipf = p.fs_solve != 0 && p.surf_model == 1;         // Potential (inter-particle force)
     P.xsph = p.xsph_solve; P.open_bc = p.open_boundary; P.rho_type = p.rho_type;
     P.NI = NI; P.NJ = NJ; P.NK = NK; P.num_cells = num_cells;
     P.ns = ns; P.nd = nd;
@@ -878,7 +921,7 @@ static int commit_t(SphdemHandle* H) {
         // particle above it later walks its stencil instead
         P.nbd_cap = 0;
         if (nd > 0) {
-            if ((r = nnps_dem<R>(H, EH, 0, 1, &nl))) return r;
+            if ((r = nnps_dem<R>(H, EH, 0, 1, &nl, st))) return r;
             CK(cudaMemsetAsync(W.ncntd, 0, sizeof(int) * ns, st));
             launch_dlist<R>(EH, E.S[1], E.D[1], st);
             CK(cudaGetLastError());
@@ -960,6 +1003,10 @@ static int commit_t(SphdemHandle* H) {
         f0.step_count = H->count;
         CK(cudaMemcpy(E.flags, &f0, sizeof(f0), cudaMemcpyHostToDevice));
     }
+    if (ns > 0 && nd > 0 && !H->dem_stream) {
+        CK(cudaStreamCreateWithFlags(&H->dem_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : H->fork_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     H->committed = true;
     return SPHDEM_OK;
 }
@@ -1003,6 +1050,7 @@ static int field_ptr(SphdemHandle* H, int which, int field, const void** ptr, in
         case SPHDEM_F_PGFZ: *ptr = W.pgfz; *kind = 1; return 0;
         case SPHDEM_F_RHO_REF: *ptr = W.rho_ref; *kind = 1; return 0;
         case SPHDEM_F_DTEMP: *ptr = W.dtemp; *kind = 1; return 0;
+        case SPHDEM_F_VIS_T: *ptr = W.vist; *kind = 1; return 0;
         case SPHDEM_F_PTYPE: *ptr = S.ptype; *kind = 2; return 0;
         case SPHDEM_F_ITYPE: *ptr = S.itype; *kind = 2; return 0;
         case SPHDEM_F_BUFFER_TYPE: *ptr = S.btype; *kind = 2; return 0;
@@ -1627,7 +1675,7 @@ static void engine_destroy(SphdemHandle* h) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-static bool is_real_field(int f) { return f >= SPHDEM_F_X && f <= SPHDEM_F_GRAD_RHOY; }
+static bool is_real_field(int f) { return f >= SPHDEM_F_X && f <= SPHDEM_F_VIS_T; }
 static bool is_int_field(int f) { return f >= SPHDEM_F_PTYPE && f <= SPHDEM_F_CELL; }
 
 static int check_supported(const SphdemParams* p) {
@@ -1651,9 +1699,20 @@ static int check_supported(const SphdemParams* p) {
     }
     if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
     if (p->dim != 3) return SPHDEM_E_UNSUPPORTED;
-    if (p->prop_table || p->fs_solve || p->boussinesq_solve || p->concn_solve || p->pst_solve ||
-        p->turbulence_model != 0 || p->penetration_solve || p->noslip_bc)
+    // Switches of the ISPH step that are not built: property tables, the
+    // Boussinesq term (functions_PPE2.cuh:1575 reads temp0, a local that is
+    // never assigned), and the wall velocity condition of noslip_bc /
+    // penetration_solve (ISPH_Calc_seperate.cuh:189-193 runs it on the
+    // combined-mode arrays dev_SP1 / g_str, which this step never fills).
+    // Accepted with their reference effect: the SPS eddy viscosity and the
+    // inter-particle surface tension (pass B); other turbulence models (no
+    // eddy viscosity), the curvature surface tension (its colour function is
+    // never formed, so the force is zero), concentration diffusion (zero
+    // diffusion coefficient, functions_PROP.cuh:460-466, and no update of
+    // concn) and particle shifting (no kernel of this step reads it).
+    if (p->prop_table || p->boussinesq_solve || p->penetration_solve || p->noslip_bc)
         return SPHDEM_E_UNSUPPORTED;
+    if (p->turbulence_model < 0 || p->turbulence_model > 4) return SPHDEM_E_ARG;
     if (p->kgc_solve != 0 && p->kgc_solve != 1) return SPHDEM_E_UNSUPPORTED;
     if (p->time_type != 1) return SPHDEM_E_UNSUPPORTED;
     if (p->decouple_stride != 1) return SPHDEM_E_UNSUPPORTED;
@@ -2499,6 +2558,9 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     if (h->snap_done) cudaEventDestroy(h->snap_done);
     if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
     if (h->side) cudaStreamDestroy(h->side);
+    if (h->dem_stream) cudaStreamDestroy(h->dem_stream);
+    for (cudaEvent_t e : h->fork_ev)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

@@ -58,6 +58,7 @@ struct SphWork {
     R *fpx, *fpy, *fpz;
     R *pgfx, *pgfy, *pgfz;
     R *dtemp, *temp0;
+    R* vist;                     // SPS eddy viscosity (k_sps), read by pass B
     R *ux0, *uy0, *uz0;
     R *p_new;
     R *u_tmpx, *u_tmpy, *u_tmpz, *temp_tmp;

@@ -35,6 +35,11 @@ struct SphdemHandle {
     bool capturing = false;              // inside the capture of a step graph
     int mlp_phase = 0;                   // learned warm start of the step being built: 0 off, 1 train, 2 use
     cudaStream_t side = nullptr;         // captures the body of the PPE while node
+    // DEM branch of the ISPH-DEM step: the DEM kernels that depend on no SPH
+    // pass run on their own stream, forked from and joined to the step
+    // stream by events (captured into the step graph as parallel branches)
+    cudaStream_t dem_stream = nullptr;
+    cudaEvent_t fork_ev[6] = {};
     int64_t last_launches = 0;
     // per-kernel timing (events recorded inside the step graph)
     int timing = 0;

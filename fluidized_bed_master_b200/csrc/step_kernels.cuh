@@ -789,12 +789,65 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
 }
 
 // ---------------------------------------------------------------------------
+// Sub-particle-scale eddy viscosity, the strain-rate branch of
+// KERNEL_clc_prep3D_sph (functions_PREP2.cuh:2113-2118, 2166-2171), run
+// with fv_solve and the SPS turbulence model only:
+//   S_i = sum_j -m_j (rho_i + rho_j) |u_i - u_j|^2 / (2 rho_i rho_j r^2) (x_ij . grad W_ij)
+// with the uncorrected kernel slope, and vis_t_i = (C_s L h_i)^2 max(S_i, 1e-20) rho_i
+// (C_s = 0.12, L = 0.01, Parameters.cuh:102-104).  Pass B's viscous term
+// reads vis_t of both particles of a pair, so this runs as its own pass
+// just before it.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork<R> W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = P.ns;
+    if (i >= n) return;
+    if (S.itype[i] > 2 || S.ptype[i] > 1000) {
+        W.vist[i] = 0;
+        return;
+    }
+    const SphRec<R> rec = W.rec;
+    R th = (R)S.h[i];
+    Knl<R> K = knl_make<R>(P, th);
+    PosRec<R> qi = ldr(rec.pos + i);
+    V4<R> upi = rec.up[i];
+    V4<R> fi = rec.f1[i];
+    R uxi = upi.x, uyi = upi.y, uzi = upi.z, rhoi = fi.y;
+    R irhoi = rcp(rhoi);
+    int cnt = min(W.ncnt[i], P.nb_cap);
+    R sr = 0;
+    nb_walk<4, NbQ44<R>>(
+        cnt, W.nbr, n, i,
+        [&](int j) {
+            NbQ44<R> t;
+            t.q = ldr(rec.pos + j);
+            t.a = ldr(rec.f1 + j);
+            t.b = ldr(rec.up + j);
+            return t;
+        },
+        [&](int j, const NbQ44<R>& t) {
+            Disp<R> g = disp(P, qi, t.q, S.x, S.y, S.z, i, j);
+            R r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz, r, rinv;
+            rdist(r2, r, rinv);
+            R dw = kdw(K, r) * rinv;
+            R ux = uxi - t.b.x, uy = uyi - t.b.y, uz = uzi - t.b.z;
+            R v = (R)-0.5 * t.a.x * (rhoi + t.a.y) * (ux * ux + uy * uy + uz * uz) * irhoi * rcp(t.a.y) * rinv * rinv;
+            sr += v * r2 * dw;   // v (x_ij . x_ij) W'/r
+        });
+    sr = sr > (R)1e-20 ? sr : (R)1e-20;
+    R cl = (R)0.12 * (th * (R)0.01);
+    W.vist[i] = cl * cl * sr * rhoi;
+}
+
+// ---------------------------------------------------------------------------
 // pass B: KERNEL_clc_prep3D_sph (functions_PREP2.cuh:1985-2227, Shepard
 // filter) + KERNEL_advection_force3D_sph (functions_PPE2.cuh:1251-1607).
 // The delta-SPH density gradient of prep3D is not formed: no kernel of the
 // ISPH step reads it.
 // ---------------------------------------------------------------------------
-// FORCES: the interface-sharpness / repulsive boundary force switches are on
+// FORCES: one of the interface-sharpness force, the repulsive boundary
+// force, the SPS eddy viscosity or the inter-particle surface tension is on
 // (a separate instantiation, so that the default pass keeps its registers)
 template <typename R, bool FORCES>
 __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
@@ -827,6 +880,8 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     // per-particle factors of the pair terms
     R cp_i = -pori * irhoi * (rhoi / pori);      // rho_i/eps_i * (-eps_i / rho_i)
     R cv_i = vis_h * (R)4 * pori * irhoi;
+    R visi = vis;
+    if (FORCES && P.sps) visi += W.vist[i];   // viscosity + P3.vis_t (functions_PPE2.cuh:1323)
     R ch_i = (R)4 * pori * kc * kc * irhoi / (kc + kc);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R flt = 0, tx = 0, ty = 0, tz = 0, px = 0, py = 0, pz = 0, Rc = 0, ex = 0, ey = 0, ez = 0, et = 0;
@@ -860,7 +915,13 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                 pz += s * gz;
             }
             if (P.fv) {
-                R Cv = (g.dx * gx + g.dy * gy + g.dz * gz) * cv_i * mj * irj * rinv * rinv;
+                R cv = cv_i;
+                if (FORCES && P.sps) {
+                    // harmonic mean of the two particles' viscosity + vis_t
+                    const R visj = vis + W.vist[j];
+                    cv = visi * visj / (visi + visj) * (R)4 * pori * irhoi;
+                }
+                R Cv = (g.dx * gx + g.dy * gy + g.dz * gz) * cv * mj * irj * rinv * rinv;
                 tx += Cv * (uxi - uj.x);
                 ty += Cv * (uyi - uj.y);
                 tz += Cv * (uzi - uj.z);
@@ -897,6 +958,19 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                     tx += fb * g.dx;
                     ty += fb * g.dy;
                     tz += fb * g.dz;
+                }
+                if (P.ipf && pt == 1 && ptj == 1) {
+                    // inter-particle surface tension (functions_PPE2.cuh:1490-1542): of the
+                    // pair strengths of Parameters.cuh:134-148 only fluid-fluid (s_ff1 =
+                    // 1.1e-6) is non-zero and every A is zero, so
+                    // Cs = -s_ff1 w_ipf / (m_i (r + 1e-10)) with the cosine kernel
+                    // w_ipf = -cos(3 pi / 4 r / h) for r < 2h (functions_INTERACTION.cuh:1-33)
+                    const R tR = r * rcp(th);
+                    const R wipf = tR < (R)2 ? -cos((R)(3.0 * 3.141592653 / 4.0) * tR) : (R)0;
+                    const R Cs = -((R)1.1e-6 * (wipf / (mi * (r + (R)1e-10))));
+                    tx += Cs * g.dx;
+                    ty += Cs * g.dy;
+                    tz += Cs * g.dz;
                 }
             }
             if (eli < (R)1) {

@@ -106,6 +106,7 @@ F = dict(
     ftotalx=21, ftotaly=22, ftotalz=23, fpx=24, fpy=25, fpz=26, pgfx=27, pgfy=28, pgfz=29,
     Fdx_df=30, Fdy_df=31, Fdz_df=32, torqx=33, torqy=34, torqz=35, rho_ref=36,
     temp1=37, temp2=38, temp3=39, dtemp=40, Q_sd=41, ftotal=42, drho=43, grad_rhox=44, grad_rhoy=45,
+    vis_t=46,
     p_type=64, i_type=65, buffer_type=66, dem_idx=67, pid=68, cell=69,
 )
 INT_FIELDS = {"p_type", "i_type", "buffer_type", "dem_idx", "pid", "cell"}

@@ -235,6 +235,7 @@ typedef enum SphdemField {
     SPHDEM_F_RHO_REF, SPHDEM_F_TEMP1, SPHDEM_F_TEMP2, SPHDEM_F_TEMP3,
     SPHDEM_F_DTEMP, SPHDEM_F_Q_SD,
     SPHDEM_F_FTOTAL, SPHDEM_F_DRHO, SPHDEM_F_GRAD_RHOX, SPHDEM_F_GRAD_RHOY,
+    SPHDEM_F_VIS_T,             /* SPS eddy viscosity of the step (P3.vis_t; 0 unless fv_solve with SPS) */
     /* integer fields (int32 buffers) */
     SPHDEM_F_PTYPE = 64, SPHDEM_F_ITYPE, SPHDEM_F_BUFFER_TYPE,
     SPHDEM_F_DEM_IDX, SPHDEM_F_PID, SPHDEM_F_CELL

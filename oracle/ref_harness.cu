@@ -417,7 +417,7 @@ extern "C" int ref_get(int which, const char* name, double* out) {
     G1("fpx", P3[k].fpx) G1("fpy", P3[k].fpy) G1("fpz", P3[k].fpz)
     G1("torqx", P3[k].torqx) G1("torqy", P3[k].torqy) G1("torqz", P3[k].torqz)
     G1("dtemp", P3[k].dtemp) G1("Q_sd", P1[k].Q_sd) G1("drho", P3[k].drho) G1("ftotal", P3[k].ftotal)
-    G1("grad_rhox", P1[k].grad_rhox) G1("grad_rhoy", P1[k].grad_rhoy)
+    G1("grad_rhox", P1[k].grad_rhox) G1("grad_rhoy", P1[k].grad_rhoy) G1("vis_t", P3[k].vis_t)
 #undef G1
     if (f.rfind("ct_idx", 0) == 0) {   // ct_idx<s>
         int s = atoi(f.c_str() + 6);

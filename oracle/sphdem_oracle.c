@@ -36,7 +36,7 @@
 #define OR_SFIELDS(X)                                                       \
     X(ftotalx) X(ftotaly) X(ftotalz) X(ftotal) X(fpx) X(fpy) X(fpz)         \
     X(torqx) X(torqy) X(torqz) X(dtemp) X(dtemp1) X(dtemp2) X(dtemp3)       \
-    X(drad) X(drho)
+    X(drad) X(drho) X(vis_t)
 #define OR_IFIELDS(X) X(p_type) X(i_type) X(buffer_type) X(dem_idx) X(pid)
 
 #define NSLOT 16
@@ -574,9 +574,11 @@ static void k_prep_sph(OracleState* S) {
     }
 }
 
-/* KERNEL_clc_prep3D_sph: functions_PREP2.cuh:1985-2227 (filter, delta-SPH
- * density gradient; the strain-rate and surface-tension branches are off
- * for every supported switch set). */
+/* KERNEL_clc_prep3D_sph: functions_PREP2.cuh:1985-2227 (filter, strain
+ * rate and SPS eddy viscosity, delta-SPH density gradient).  The surface
+ * normals of its fs_solve branch are not formed: the colour function they
+ * differentiate is never computed in this step, and the only reader, the
+ * curvature model of the advection pass, then adds no force. */
 static void k_prep3d_sph(OracleState* S) {
     OSet* o = &S->s;
     const SphdemParams* P = &S->p;
@@ -590,7 +592,9 @@ static void k_prep3d_sph(OracleState* S) {
         const double* Cm = o->Cm + (size_t)i * 9;
         int ic, jc, kc;
         cell_ijk(S, xi, yi, zi, &ic, &jc, &kc);
-        double flt = 0, gx = 0, gy = 0, gz = 0;
+        double flt = 0, gx = 0, gy = 0, gz = 0, sr = 0;
+        double uxi = o->ux[i], uyi = o->uy[i], uzi = o->uz[i];
+        int turb = P->fv_solve == 1 && P->turbulence_model != 0;
         FOR_NEIGHBOR_CELLS(S, o, ic, jc, kc, j) {
             if (o->p_type[j] <= 1000) {
                 double xj = o->x[j], yj = o->y[j], zj = o->z[j];
@@ -601,6 +605,13 @@ static void k_prep3d_sph(OracleState* S) {
                     double dw = knl_dw(P->kernel_type, tA, th, td);
                     double tdwx = dw * (xi - xj) / td, tdwy = dw * (yi - yj) / td, tdwz = dw * (zi - zj) / td;
                     if (filt) flt += mj / rhoj * w;
+                    if (turb) {   /* strain rate, functions_PREP2.cuh:2113-2118 */
+                        double ux = uxi - o->ux[j], uy = uyi - o->uy[j], uz = uzi - o->uz[j];
+                        double uij2 = ux * ux + uy * uy + uz * uz;
+                        double v = -0.5 * mj * (rhoi + rhoj) * uij2;
+                        v /= (rhoi * rhoj * td * td);
+                        sr += v * (xi - xj) * tdwx + v * (yi - yj) * tdwy + v * (zi - zj) * tdwz;
+                    }
                     if (P->delSPH_solve == 2) {
                         kgc_apply(P, Cm, &tdwx, &tdwy, &tdwz);
                         double rj = o->rho_ref[j];
@@ -610,6 +621,12 @@ static void k_prep3d_sph(OracleState* S) {
                     }
                 }
             }
+        }
+        if (turb) {   /* functions_PREP2.cuh:2166-2171: Cs_SPS 0.12, L_SPS 0.01 (Parameters.cuh:102-104) */
+            double tv = 0.0, tl = th * 0.01;
+            sr = sr > 1e-20 ? sr : 1e-20;
+            if (P->turbulence_model == 3) tv = (0.12 * tl) * (0.12 * tl) * sr;
+            o->vis_t[i] = tv * rhoi;
         }
         if (filt) o->flt_s[i] = flt;
         if (P->delSPH_solve == 2) {
@@ -621,10 +638,14 @@ static void k_prep3d_sph(OracleState* S) {
 }
 
 /* KERNEL_advection_force3D_sph: functions_PPE2.cuh:1251-1607 (pressure-
- * gradient force density, viscous Laplacian, artificial viscosity,
- * interface sharpness force, repulsive boundary force, gravity, Eulerian
- * convection, conduction).  Surface tension, concentration and Boussinesq
- * branches are rejected by the switch check. */
+ * gradient force density, viscous Laplacian with the eddy viscosity,
+ * artificial viscosity, interface sharpness force, repulsive boundary
+ * force, inter-particle surface tension, gravity, Eulerian convection,
+ * conduction).  The curvature surface tension adds no force (its normals
+ * are zero, see k_prep3d_sph) and the concentration rate is zero (zero
+ * diffusion coefficient, functions_PROP.cuh:460-466); the Boussinesq term
+ * reads an unassigned local in the reference and is rejected by the
+ * engine's switch check. */
 static void k_advection(OracleState* S) {
     OSet* o = &S->s;
     const SphdemParams* P = &S->p;
@@ -644,7 +665,7 @@ static void k_advection(OracleState* S) {
             kci = prop_conductivity(P, pti);
             cpi = prop_heat_capacity(P, pti);
         }
-        double visi = prop_viscosity(P) + 0.0; /* + P3.vis_t (0, laminar) */
+        double visi = prop_viscosity(P) + o->vis_t[i];
         const double* Cm = o->Cm + (size_t)i * 9;
         double elix = o->elix[i], eliy = o->eliy[i], eliz = o->eliz[i];
         int ic, jc, kc;
@@ -671,7 +692,7 @@ static void k_advection(OracleState* S) {
                         pz += rhoi / pori * Cp * tdwz;
                     }
                     if (P->fv_solve) {
-                        double visj = prop_viscosity(P) + 0.0, Cv;
+                        double visj = prop_viscosity(P) + o->vis_t[j], Cv;
                         Cv = (xi - xj) * tdwx + (yi - yj) * tdwy + (zi - zj) * tdwz;
                         Cv *= (visi * visj) / (visi + visj);
                         Cv *= 4 * pori * (mj / (rhoi * rhoj));
@@ -716,6 +737,22 @@ static void k_advection(OracleState* S) {
                             ty += fb * (yi - yj);
                             tz += fb * (zi - zj);
                         }
+                    }
+                    if (P->fs_solve && P->surf_model == 1) {
+                        /* inter-particle force (functions_PPE2.cuh:1490-1542) with the
+                         * cosine kernel of functions_INTERACTION.cuh:1-33 and the half-
+                         * distance kernel 0; of the pair strengths of Parameters.cuh:
+                         * 134-148 only s_ff1 = 1.1e-6 (fluid-fluid) is non-zero, every
+                         * A is 0, and the other pairs add 0 */
+                        double tR = td / hi, wipf = -(tR < 2) * 1.0 * cos(3 * 3.141592653 / 4 * tR), whalf = 0.0;
+                        double Cs = 0.0;
+                        if ((pti == 1) & (ptj == 1)) {
+                            Cs = 1.1e-6 * (0.0 * whalf / (mi * (td + 1.0e-10)));
+                            Cs -= 1.1e-6 * (wipf / (mi * (td + 1.0e-10)));
+                        }
+                        tx += Cs * (xi - xj);
+                        ty += Cs * (yi - yj);
+                        tz += Cs * (zi - zj);
                     }
                     if (elix < 1.0 || eliy < 1.0) {
                         ex += (uxi * (uxj - uxi) * tdwx + uyi * (uxj - uxi) * tdwy + uzi * (uxj - uxi) * tdwz) * mj / rhoj * (1 - elix);
@@ -2200,6 +2237,7 @@ static double* dfield(OSet* o, int f) {
     case SPHDEM_F_TEMP3: return o->temp3; case SPHDEM_F_DTEMP: return o->dtemp; case SPHDEM_F_Q_SD: return o->Q_sd;
     case SPHDEM_F_FTOTAL: return o->ftotal; case SPHDEM_F_DRHO: return o->drho;
     case SPHDEM_F_GRAD_RHOX: return o->grad_rhox; case SPHDEM_F_GRAD_RHOY: return o->grad_rhoy;
+    case SPHDEM_F_VIS_T: return o->vis_t;
     default: return NULL;
     }
 }

@@ -32,7 +32,7 @@ from fluidized_bed_master_b200.beds import dam_break_2d, spouted_bed, write_inpu
 
 SPH_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor", "dDEMpor", "flt_s",
               "pgfx", "pgfy", "pgfz", "rho_ref", "ftotalx", "ftotaly", "ftotalz", "fpx", "fpy", "fpz",
-              "p_type", "i_type", "buffer_type", "pid"]
+              "p_type", "i_type", "buffer_type", "pid", "vis_t"]
 DEM_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "DEMpor", "flt_s", "flt_sd", "flt_sd2",
               "Fdx_df", "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz", "dtemp",
               "dem_idx"]
@@ -67,6 +67,17 @@ CASES = {
     # pass switched on (functions_PPE2.cuh:1450-1472)
     "forces": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=13, spacing=1.9, u_dem=0.05),
                dict(interface_solve=1, fb_solve=1), [1, 8, 100]),
+    # the SPS eddy viscosity (functions_PREP2.cuh:2113-2171) and the
+    # inter-particle surface tension (functions_PPE2.cuh:1490-1542), with the
+    # concentration and particle-shifting switches on as well (no effect in
+    # this step)
+    "sps_ipf": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=14, spacing=1.9, u_dem=0.05),
+                dict(fv_solve=1, turbulence_model=3, fs_solve=1, surf_model=1, concn_solve=1, pst_solve=1),
+                [1, 8, 100]),
+    # the curvature surface tension and the k-lm model: no force, no eddy
+    # viscosity in this step
+    "curvature": (dict(dx=2.0e-3, n_dem=100000, r_dem=1.0e-3, seed=15, spacing=1.9, u_dem=0.05),
+                  dict(fv_solve=1, turbulence_model=1, fs_solve=1, surf_model=2), [1, 8, 100]),
 }
 
 

@@ -67,7 +67,7 @@ def _run_against_fixture(path, prec, tol, last_only):
             assert set(v) == set(heng[k]), f"contact partners of sphere {k} differ at step {cp}"
         if last_only and cp != cps[-1]:
             continue
-        for f in REAL_SPH:
+        for f in REAL_SPH + (["vis_t"] if pre + "sph_vis_t" in g.files else []):
             e = rel_l2(by_id(epid, eng.get(SPH, f)), by_id(ref_pid, g[pre + "sph_" + f]))
             if not e <= tol:
                 bad.append((cp, "sph", f, e))

@@ -107,9 +107,15 @@ def test_failures_before_the_device():
     q = p.copy()
     q.solver_type = 2          # DFSPH: commented out in the reference driver (SOPHIA_gpu.cu:160-162)
     assert L.sphdem_create(C.byref(q), 10, 0, C.byref(h)) == -7
+    # switches of the ISPH step that are not built: property tables, the
+    # Boussinesq term and the wall velocity condition
+    for k in ("prop_table", "boussinesq_solve", "noslip_bc", "penetration_solve"):
+        q = p.copy()
+        setattr(q, k, 1)
+        assert L.sphdem_create(C.byref(q), 10, 0, C.byref(h)) == -7, k
     q = p.copy()
-    q.fs_solve = 1
-    assert L.sphdem_create(C.byref(q), 10, 0, C.byref(h)) == -7
+    q.turbulence_model = 5
+    assert L.sphdem_create(C.byref(q), 10, 0, C.byref(h)) == -1
     assert L.sphdem_step(None, 1) == -1
     assert L.sphdem_get_stats(None, None) == -1
     for code in (0, -1, -2, -3, -4, -5, -6, -7, -8):

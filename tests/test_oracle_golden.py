@@ -96,7 +96,7 @@ def test_oracle_matches_reference(path):
         assert np.array_equal(ref_pid, opid), "cell-sorted order differs from the reference"
         for f in ("p_type", "i_type", "buffer_type"):
             assert np.array_equal(g[pre + "sph_" + f].astype(np.int64), orc.get(SPH, f)), f
-        for f in REAL_SPH:
+        for f in REAL_SPH + (["vis_t"] if pre + "sph_vis_t" in g.files else []):
             e = rel_l2(by_id(opid, orc.get(SPH, f)), by_id(ref_pid, g[pre + "sph_" + f]))
             if not e <= TOL:
                 bad.append((int(cp), "sph", f, e))
@@ -116,6 +116,9 @@ def test_oracle_matches_reference(path):
         for k in href:
             assert set(href[k]) == set(hor[k]), f"partners of sphere {k} at step {cp}"
             for j in href[k]:
-                assert np.allclose(hor[k][j], href[k][j], rtol=1e-8, atol=1e-20)
+                # each spring vector to 1e-8 of its own magnitude (a component
+                # near zero carries the vector's rounding, not its own)
+                a, b = np.asarray(hor[k][j]), np.asarray(href[k][j])
+                assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max() + 1e-20, (cp, k, j, a, b)
         assert sum(len(v) for v in href.values()) > 0
     assert not bad, bad

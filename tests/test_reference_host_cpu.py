@@ -66,7 +66,7 @@ for cp in [int(c) for c in g["checkpoints"]]:
     pid = get(0, "pid", ns.value)
     did = get(1, "dem_idx", nd.value)
     out["order"] &= bool(np.array_equal(pid, g[pre + "sph_pid"]) and np.array_equal(did, g[pre + "dem_dem_idx"]))
-    for f in SPH:
+    for f in SPH + (["vis_t"] if pre + "sph_vis_t" in g.files else []):
         out["err"][f"{cp}.sph.{f}"] = rel_l2(get(0, f, ns.value), g[pre + "sph_" + f])
     for f in DEM:
         out["err"][f"{cp}.dem.{f}"] = rel_l2(get(1, f, nd.value), g[pre + "dem_" + f])
