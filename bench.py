@@ -1006,19 +1006,50 @@ def run_engine(args, world, rank, local, pg):
     # dominant kernel and its roofline
     tim = eng.timing()
     per_kernel = {k: (v[0] - base.get(k, (0, 0))[0], v[1] - base.get(k, (0, 0))[1]) for k, v in tim.items()}
-    dom = max(per_kernel.items(), key=lambda kv: kv[1][0])
-    dom_name, (dom_ms, dom_n) = dom[0], dom[1]
     r = 8 if args.precision == "fp64" else 4
     nwall = int((sph["p_type"] <= 0).sum())
     nbuf = int(((sph["p_type"] == 1) & ((sph["z"] < p.obc_L2 - 1e-6) | (sph["z"] >= p.obc_L3 - 1e-6))).sum())
-    bytes_dom = manifest_bytes(dom_name, eng.ns, eng.nd, nwall, nbuf, avg_nb, r)
     peak, peak_kind = load_peaks()
-    achieved = bytes_dom / (dom_ms / max(dom_n, 1) / 1e3) / 1e9 if (bytes_dom and dom_n) else None
-    traffic = profiled_traffic(dom_name) if args.precision == "fp32" else None
-    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+
+    def roofline_of(per):
+        dom_name, (dom_ms, dom_n) = max(per.items(), key=lambda kv: kv[1][0])
+        bytes_dom = manifest_bytes(dom_name, eng.ns, eng.nd, nwall, nbuf, avg_nb, r)
+        achieved = bytes_dom / (dom_ms / max(dom_n, 1) / 1e3) / 1e9 if (bytes_dom and dom_n) else None
+        traffic = profiled_traffic(dom_name) if args.precision == "fp32" else None
+        return {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "bytes_per_launch": bytes_dom, "launch_ms": dom_ms / max(dom_n, 1), "peak_source": peak_kind,
-                "share_of_step": dom_ms / max(sum(v[0] for v in per_kernel.values()), 1e-12)}
+                "share_of_step": dom_ms / max(sum(v[0] for v in per.values()), 1e-12)}
+
+    roofline = roofline_of(per_kernel)
+    # The DEM branch runs concurrently with the SPH passes, so the event
+    # times above include the SMs each kernel shares with the other branch.
+    # The same steps with the branch serialised on the step stream give
+    # each kernel's own duration (not timed as the headline).
+    serial = None
+    if eng.ns and eng.nd:
+        eng.set_concurrency(False)
+        eng.step(2)
+        eng.collect_timing()
+        b2 = eng.timing()
+        ks = max(3, min(args.steps, 10))
+        t_ser = 0.0
+        for _ in range(ks):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            eng.step(1)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            eng.collect_timing()
+            t_ser += e0.elapsed_time(e1)
+        t2 = eng.timing()
+        per_ser = {k: (v[0] - b2.get(k, (0, 0))[0], v[1] - b2.get(k, (0, 0))[1]) for k, v in t2.items()}
+        serial = {"ms_per_step": t_ser / ks, "steps": ks, "roofline": roofline_of(per_ser),
+                  "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_ser.items() if v[1]}}
+        eng.set_concurrency(True)
 
     # end to end through the C ABI with host buffers: each step uploads the
     # mutable particle state from pinned host arrays, steps, reads it back
@@ -1083,6 +1114,7 @@ def run_engine(args, world, rank, local, pg):
         "clocks": clocks,
         "stats": {k: stats[k] for k in ("rho_max_sph", "u_max_sph", "u_max_dem", "overflow_flags", "nan_flag")},
         "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in per_kernel.items() if v[1]},
+        "dem_branch_serialised": serial,
         "fp64_build": fp64,
         "fp32_vs_fp64": fp32_vs_fp64,
         "ppe": ppe,

@@ -512,16 +512,18 @@ void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double
 // The DEM kernels that read no SPH pass run on a second stream, forked from
 // and joined to the step stream by events (in the step graph: parallel
 // branches):
-//   step stream: SPH NNPS -> list -> [DEM sorted] dlist -> pass A -> pass B
+//   step stream: SPH NNPS -> list -> [SPH->DEM list built] pass A -> pass B
 //                -> [DEM prep done] DEM coupling -> SPH coupling -> walls, PPE,
 //                pass C, open boundary, XSPH -> [DEM update done] tick
-//   DEM stream:  DEM NNPS -> contact -> [SPH gathered] DEM prep
+//   DEM stream:  DEM NNPS -> [SPH gathered] SPH->DEM list -> contact -> DEM prep
 //                ... [SPH coupling done] DEM corrector + walls
-// The DEM contact reads only the DEM set; the DEM prep reads the gathered
-// SPH records and the DEM set; the DEM corrector writes the DEM set after
-// the SPH coupling has read it, and no later SPH kernel reads it.  Without
-// both sets everything runs on the step stream in the same order.  The
-// per-kernel timing events of a DEM kernel are recorded on its own stream.
+// The SPH -> DEM list reads both sorted sets; the DEM contact reads only
+// the DEM set; the DEM prep reads the gathered SPH records and the DEM set;
+// the DEM corrector writes the DEM set after the SPH coupling has read it,
+// and no later SPH kernel reads it.  Without
+// both sets, or with sphdem_set_concurrency(h, 0), everything runs on the
+// step stream in the same order.  The per-kernel timing events of a DEM
+// kernel are recorded on its own stream.
 // ---------------------------------------------------------------------------
 enum { F_COUNT0 = 2, F_FILT = 4, F_TIME0 = 8 };
 
@@ -535,7 +537,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int ns = P.ns, nd = P.nd;
     int so = E.cur_s, sn = 1 - E.cur_s, dox = E.cur_d, dn = 1 - E.cur_d;
     int r;
-    const bool fork = ns > 0 && nd > 0 && H->dem_stream;
+    const bool fork = H->concurrent && ns > 0 && nd > 0 && H->dem_stream;
     cudaStream_t sd = fork ? H->dem_stream : st;
     // event k recorded on stream a / waited for on stream b (fork only)
     auto rec = [&](int k, cudaStream_t a) { return fork ? cudaEventRecord(H->fork_ev[k], a) : cudaSuccess; };
@@ -543,21 +545,23 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     CK(rec(0, st));
     CK(wait(0, sd));
     if ((r = nnps_dem<R>(H, EH, dox, dn, nl, sd))) return r;
-    CK(rec(1, sd));   // DEM set sorted
     SphState<R>& S = E.S[sn];
     DemState<double>& D = E.D[dn];
     int bs = nblocks(ns, TPB), bd = nblocks(nd, TPB);
     int bdw = nblocks(nd * 32, TPB), bww = nblocks(P.nwall * 32, TPB), bbw = nblocks(P.nbuf * 32, TPB);
-    if (nd > 0) {
-        { KTIME_ON(KT_DEMCONTACT, sd); k_dem_contact<R><<<bdw, TPB, 0, sd>>>(P, D, DW, DW.rows, E.flags); }
-        *nl += 1;
-    }
     if ((r = nnps_sph<R>(H, EH, so, sn, nl))) return r;
     CK(rec(2, st));   // SPH set gathered
     CK(wait(2, sd));
-    if (nd > 0) {
-        { KTIME_ON(KT_DEMPREP, sd); k_dem_prep<R><<<bdw, TPB, 0, sd>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
+    if (ns > 0 && nd > 0) {
+        KTIME_ON(KT_DLIST, sd);
+        launch_dlist<R>(EH, S, D, sd);
         *nl += 1;
+    }
+    CK(rec(1, sd));   // SPH -> DEM list built
+    if (nd > 0) {
+        { KTIME_ON(KT_DEMCONTACT, sd); k_dem_contact<R><<<bdw, TPB, 0, sd>>>(P, D, DW, DW.rows, E.flags); }
+        { KTIME_ON(KT_DEMPREP, sd); k_dem_prep<R><<<bdw, TPB, 0, sd>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
+        *nl += 2;
     }
     if (ns > 0) {
         {
@@ -573,11 +577,6 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             }
         }
         CK(wait(1, st));
-        if (nd > 0) {
-            KTIME(KT_DLIST);
-            launch_dlist<R>(EH, S, D, st);
-            *nl += 1;
-        }
         { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
         *nl += 2;
         {
@@ -2253,6 +2252,20 @@ extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
         h->graph_kused.clear();
     }
     h->timing = on ? 1 : 0;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_set_concurrency(SphdemHandle* h, int on) {
+    if (!h) return SPHDEM_E_ARG;
+    if ((on != 0) != (h->concurrent != 0)) {
+        // the step graphs embed the fork (or not): recapture
+        CK(cudaStreamSynchronize(h->stream));
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+        h->graphs.clear();
+        h->graph_launches.clear();
+        h->graph_kused.clear();
+    }
+    h->concurrent = on ? 1 : 0;
     return SPHDEM_OK;
 }
 

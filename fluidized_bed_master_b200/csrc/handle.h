@@ -40,6 +40,7 @@ struct SphdemHandle {
     // stream by events (captured into the step graph as parallel branches)
     cudaStream_t dem_stream = nullptr;
     cudaEvent_t fork_ev[6] = {};
+    int concurrent = 1;                  // sphdem_set_concurrency
     int64_t last_launches = 0;
     // per-kernel timing (events recorded inside the step graph)
     int timing = 0;

@@ -55,6 +55,7 @@ def lib():
     L.sphdem_set_history.argtypes = [vp, P(C.c_int32), P(C.c_double)]
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
     L.sphdem_set_graphs.argtypes = [vp, C.c_int]
+    L.sphdem_set_concurrency.argtypes = [vp, C.c_int]
     L.sphdem_collect_timing.argtypes = [vp]
     L.sphdem_get_timing.argtypes = [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_double), P(C.c_int64)]
     L.sphdem_input_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
@@ -271,6 +272,10 @@ class Engine:
     def set_graphs(self, on):
         """Step graphs on/off (off: kernel profilers see every launch)."""
         _chk(lib().sphdem_set_graphs(self._h, int(bool(on))), "sphdem_set_graphs")
+
+    def set_concurrency(self, on):
+        """DEM branch of the step on its own stream (default) or on the step stream."""
+        _chk(lib().sphdem_set_concurrency(self._h, int(bool(on))), "sphdem_set_concurrency")
 
     def collect_timing(self):
         _chk(lib().sphdem_collect_timing(self._h), "sphdem_collect_timing")

@@ -429,12 +429,21 @@ int sphdem_get_history(SphdemHandle* h, int32_t* ids, double* springs);
 int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* springs);
 
 /* Per-kernel device timing.  While enabled, every step records a CUDA
- * event pair around each engine kernel on the handle's stream (inside the
+ * event pair around each engine kernel on the stream it runs on (inside the
  * captured step graph); sphdem_collect_timing synchronises and adds the
  * elapsed times of the last step to per-kernel totals, which
- * sphdem_get_timing reports (kernel k = 0..n-1, name, total ms, count). */
+ * sphdem_get_timing reports (kernel k = 0..n-1, name, total ms, count).
+ * With the DEM branch concurrent, a kernel's time includes the SMs it
+ * shares with the other branch. */
 int sphdem_set_timing(SphdemHandle* h, int on);
 int sphdem_collect_timing(SphdemHandle* h);
+
+/* The ISPH-DEM step runs the DEM kernels that read no SPH pass (DEM NNPS,
+ * contact, filters, corrector) on a second stream, forked from and joined
+ * to the handle's stream inside the step (on by default).  Off, every
+ * kernel runs on the handle's stream, one after another, in the same
+ * order; results are identical either way. */
+int sphdem_set_concurrency(SphdemHandle* h, int on);
 
 /* Step graphs on (default) or off.  Off, every step launches its kernels
  * one by one and the KRYLOV/PCG iterations are driven from the host (one

@@ -181,6 +181,37 @@ def test_dem_list_cap_walks_stencil_bit_identical(contact_bed, prec):
             assert np.array_equal(a.get(which, f), b.get(which, f)), ("dem" if which else "sph", f)
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_dem_branch_concurrency_bit_identical(contact_bed, prec):
+    """The DEM kernels that read no SPH pass run on a second stream forked
+    from the step stream; run serialised on the step stream
+    (sphdem_set_concurrency(h, 0)), the same step gives the same bits, with
+    graphs and without, and switching back and forth mid-run changes
+    nothing."""
+    p, sph, dem = contact_bed
+    a = _engine(p, sph, dem, prec)
+    b = _engine(p, sph, dem, prec)
+    b.set_concurrency(False)
+    c = _engine(p, sph, dem, prec)
+    c.set_graphs(False)
+    a.step(4)
+    b.step(4)
+    c.step(2)
+    c.set_concurrency(False)
+    c.step(1)
+    c.set_concurrency(True)
+    c.step(1)
+    for which, fields in ((SPH, SPH_REAL), (DEM, DEM_REAL)):
+        for e in (b, c):
+            assert np.array_equal(_ids(a, which), _ids(e, which))
+            for f in fields:
+                assert np.array_equal(a.get(which, f), e.get(which, f)), ("dem" if which else "sph", f)
+    ia, sa = a.history()
+    for e in (b, c):
+        ie, se = e.history()
+        assert np.array_equal(ia, ie) and np.array_equal(sa, se)
+
+
 def test_stats_and_time(calm_bed):
     p, sph, dem = calm_bed
     eng = _engine(p, sph, dem, 0)
