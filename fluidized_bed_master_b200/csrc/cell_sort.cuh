@@ -23,6 +23,12 @@
 // only on the values, so the result is deterministic and bit-identical to
 // CUB's.  No memset runs per step: cnt is zeroed by the settle pass, fill by
 // the scan (both start at zero after allocation).
+//
+// The warp's ranking costs m^2/32 for a bucket of m slots: fine for cells
+// (tens of particles), not for a last bucket holding the many parked spare
+// slots of a slab of a sharded bed.  With `big_last` set, that bucket is
+// written instead by a stable compaction of the slots keyed num_cells
+// (block counts, one-block scan, ordered writes): the same ascending order.
 #pragma once
 #include <climits>
 #include <cuda_runtime.h>
@@ -39,6 +45,8 @@ struct CellSort {
     int* tmp;        // [n] slots grouped by bucket, unordered inside a bucket
     int nb;          // buckets: num_cells + 1
     int ntiles;
+    int big_last;    // the last bucket by compaction (blk: per-block counts)
+    int* blk;
 };
 
 // count one key (called by every thread of a warp that hashes; inactive
@@ -139,7 +147,7 @@ __global__ void k_sort_scatter(int n, const int* __restrict__ key, const int* __
 // (end, written only for a non-empty cell, as the reference's reorder does)
 __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
                                                      const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
-                                                     int* ge) {
+                                                     int* ge, int skip_last) {
     const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (b >= nb) return;
@@ -153,6 +161,7 @@ __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int
             if (m) ge[b] = s + m;
         }
     }
+    if (skip_last && b == nb - 1) return;
     for (int a = 0; a < m; a += 32) {
         const int v = (a + lane < m) ? tmp[s + a + lane] : INT_MAX;
         int r = 0;
@@ -168,13 +177,70 @@ __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int
     }
 }
 
+// the last bucket (key last) by stable compaction: per-block counts ...
+__global__ void __launch_bounds__(256) k_sort_last_count(int n, const int* __restrict__ key, int last, int* blk) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = __syncthreads_count(i < n && key[i] == last);
+    if (threadIdx.x == 0) blk[blockIdx.x] = c;
+}
+
+// ... their exclusive prefix (one block of 1024 threads) ...
+__global__ void __launch_bounds__(1024) k_sort_last_scan(int nblk, int* blk) {
+    __shared__ int part[1024];
+    const int per = (nblk + 1023) / 1024, b0 = threadIdx.x * per, b1 = min(nblk, b0 + per);
+    int s = 0;
+    for (int b = b0; b < b1; b++) s += blk[b];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int acc = part[threadIdx.x] - s;
+    for (int b = b0; b < b1; b++) {
+        const int v = blk[b];
+        blk[b] = acc;
+        acc += v;
+    }
+}
+
+// ... and the slots in ascending order from the bucket's start
+__global__ void __launch_bounds__(256) k_sort_last_write(int n, const int* __restrict__ key, int last,
+                                                         const int* __restrict__ blk, const int* __restrict__ start,
+                                                         int* perm, int* key_out) {
+    __shared__ int wsum[8];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool f = i < n && key[i] == last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wsum[w] = __popc(m);
+    __syncthreads();
+    int pos = start[last] + blk[blockIdx.x];
+    for (int k = 0; k < w; k++) pos += wsum[k];
+    if (f) {
+        pos += __popc(m & ((1u << lane) - 1u));
+        perm[pos] = i;
+        key_out[pos] = last;
+    }
+}
+
 // scan + scatter + settle for n keys already counted into cs.cnt
 inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* perm, int* key_out, int* gs, int* ge,
                              cudaStream_t st) {
     k_sort_tile_sums<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.nb, cs.tile_sum);
     k_sort_scan<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.tile_sum, cs.nb, cs.start, cs.fill);
     if (n > 0) k_sort_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, key_in, cs.start, cs.fill, cs.tmp);
-    k_sort_settle<<<(cs.nb * 32 + 255) / 256, 256, 0, st>>>(cs.nb, cs.cnt, cs.start, cs.tmp, perm, key_out, gs, ge);
+    const int big = cs.big_last && n > 0;
+    k_sort_settle<<<(cs.nb * 32 + 255) / 256, 256, 0, st>>>(cs.nb, cs.cnt, cs.start, cs.tmp, perm, key_out, gs, ge,
+                                                            big);
+    if (big) {
+        const int nblk = (n + 255) / 256;
+        k_sort_last_count<<<nblk, 256, 0, st>>>(n, key_in, cs.nb - 1, cs.blk);
+        k_sort_last_scan<<<1, 1024, 0, st>>>(nblk, cs.blk);
+        k_sort_last_write<<<nblk, 256, 0, st>>>(n, key_in, cs.nb - 1, cs.blk, cs.start, perm, key_out);
+    }
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@
 #include "ppe_mg.cuh"
 #include "mlp.h"
 #include "wcsph2d.cuh"
+#include "slab.cuh"
 
 using namespace sphdem;
 
@@ -108,6 +109,8 @@ CellSort alloc_cell_sort(Alloc& A, int num_cells, int n) {
     c.start = A.get<int>(c.nb);
     c.tile_sum = A.get<int>(c.ntiles);
     c.tmp = A.get<int>(n);
+    c.big_last = 0;
+    c.blk = A.get<int>((n + 255) / 256 + 1);
     return c;
 }
 
@@ -247,7 +250,7 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     {
         KTIME(KT_GATHER_S);
         k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.rec, W.val_out, W.wall_idx,
-                                                                W.buf_idx, W.counters);
+                                                                W.buf_idx, W.counters, E.flags);
     }
     {
         KTIME(KT_ROWS_S);
@@ -704,6 +707,21 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
 // ---------------------------------------------------------------------------
 // commit: domain, grid, buffer tags, upload, list capacity
 // ---------------------------------------------------------------------------
+// bounding box: find_minmax (function_init.cuh:913-950) over the rows in
+// file order, stopping one row short (the reference loop bound), then the
+// margins; out = xmin, xmax, ymin, ymax, zmin, zmax
+static void bed_box(const SphdemParams& p, const double* fx, const double* fy, const double* fz, int n, double* out) {
+    double mnx = fx[0], mxx = fx[0], mny = fy[0], mxy = fy[0], mnz = fz[0], mxz = fz[0];
+    for (int k = 0; k < n - 1; k++) {
+        mnx = std::min(mnx, fx[k]); mxx = std::max(mxx, fx[k]);
+        mny = std::min(mny, fy[k]); mxy = std::max(mxy, fy[k]);
+        mnz = std::min(mnz, fz[k]); mxz = std::max(mxz, fz[k]);
+    }
+    mnx -= (mxx - mnx) * p.margin[0]; mxx += (mxx - mnx) * p.margin[1];
+    mny -= (mxy - mny) * p.margin[2]; mxy += (mxy - mny) * p.margin[3];
+    mnz -= (mxz - mnz) * p.margin[4]; mxz += (mxz - mnz) * p.margin[5];
+    out[0] = mnx; out[1] = mxx; out[2] = mny; out[3] = mxy; out[4] = mnz; out[5] = mxz;
+}
 template <typename R>
 static int commit_t(SphdemHandle* H) {
     const SphdemParams& p = H->p;
@@ -726,16 +744,16 @@ static int commit_t(SphdemHandle* H) {
         fz = sz; fz.insert(fz.end(), dz.begin(), dz.end());
         h0 = ns > 0 ? H->stage_d[0][SPHDEM_F_H][0] : H->stage_d[1][SPHDEM_F_H][0];
     }
-    int n = (int)fx.size();
-    double mnx = fx[0], mxx = fx[0], mny = fy[0], mxy = fy[0], mnz = fz[0], mxz = fz[0];
-    for (int k = 0; k < n - 1; k++) {
-        mnx = std::min(mnx, fx[k]); mxx = std::max(mxx, fx[k]);
-        mny = std::min(mny, fy[k]); mxy = std::max(mxy, fy[k]);
-        mnz = std::min(mnz, fz[k]); mxz = std::max(mxz, fz[k]);
+    double bb[6];
+    bed_box(p, fx.data(), fy.data(), fz.data(), (int)fx.size(), bb);
+    double mnx = bb[0], mxx = bb[1], mny = bb[2], mxy = bb[3], mnz = bb[4], mxz = bb[5];
+    if (H->dom_set) {
+        // a slab of a larger bed: the whole bed's box and h0, so that every
+        // slab has the same cell grid
+        mnx = H->dom_bbox[0]; mxx = H->dom_bbox[1]; mny = H->dom_bbox[2];
+        mxy = H->dom_bbox[3]; mnz = H->dom_bbox[4]; mxz = H->dom_bbox[5];
+        h0 = H->dom_h0;
     }
-    mnx -= (mxx - mnx) * p.margin[0]; mxx += (mxx - mnx) * p.margin[1];
-    mny -= (mxy - mny) * p.margin[2]; mxy += (mxy - mny) * p.margin[3];
-    mnz -= (mxz - mnz) * p.margin[4]; mxz += (mxz - mnz) * p.margin[5];
     double dcell = 1.1 * p.kappa * h0;
     int NI = (int)((mxx - mnx) / dcell) + 1, NJ = (int)((mxy - mny) / dcell) + 1, NK = (int)((mxz - mnz) / dcell) + 1;
     if (!(dcell > 0) || NI <= 0 || NJ <= 0 || NK <= 0 || (double)NI * NJ * NK > 2.0e9) return SPHDEM_E_INPUT;
@@ -777,6 +795,7 @@ static int commit_t(SphdemHandle* H) {
         for (double v : tv) s += v;
         P.t_ref = tv.empty() ? 0.0 : (double)(float)(s / (double)tv.size());
         if (!std::isfinite(P.t_ref)) P.t_ref = 0.0;
+        if (H->dom_set) P.t_ref = H->dom_tref;
     }
     P.cyl_cx = p.cyl_cx; P.cyl_cy = p.cyl_cy; P.cyl_r = p.cyl_r;
     for (int k = 0; k < 3; k++) { P.box_c[k] = p.box_c[k]; P.box_L[k] = p.box_L[k]; P.cone_c[k] = p.cone_c[k]; }
@@ -810,15 +829,27 @@ static int commit_t(SphdemHandle* H) {
     // cell sort scratch of both sets (zeroed by the allocator, as cell_sort expects)
     E.cs_s = alloc_cell_sort(A, num_cells, ns);
     E.cs_d = alloc_cell_sort(A, num_cells, nd);
+    // a slab's parked spare slots all sort into the last bucket
+    E.cs_s.big_last = E.cs_d.big_last = H->dom_set ? 1 : 0;
     if (!A.ok) return SPHDEM_E_NOMEM;
     // buffer tags (c_initial_inner_outer_particle_single_{sph,dem}, functions_NNPS.cuh:60-200)
+    // A slab of a larger bed (sphdem_set_domain) may pass i_type 3 for its
+    // parked spare slots and its own ids (the rows' ids in the whole bed).
     for (int q = 0; q < 2; q++) {
         int nq = q ? nd : ns;
         std::vector<int> itype(nq, 1), btype(nq, 0), pid(nq);
         auto& pt = H->stage_i[q][SPHDEM_F_PTYPE];
         auto& zz = H->stage_d[q][SPHDEM_F_Z];
+        const auto it_in = H->stage_i[q].find(SPHDEM_F_ITYPE);
+        const auto pid_in = H->stage_i[q].find(SPHDEM_F_PID);
+        const bool keep_it = H->dom_set && it_in != H->stage_i[q].end() && (int)it_in->second.size() == nq;
+        const bool keep_pid = H->dom_set && pid_in != H->stage_i[q].end() && (int)pid_in->second.size() == nq;
         for (int i = 0; i < nq; i++) {
-            pid[i] = i;
+            pid[i] = keep_pid ? pid_in->second[i] : i;
+            if (keep_it && it_in->second[i] == 3) {
+                itype[i] = 3;
+                continue;
+            }
             if (p.open_boundary > 0 && pt[i] < 1000 && pt[i] >= 1) {
                 if (zz[i] >= (p.obc_L1 - 1e-6) && (zz[i] < p.obc_L2 - 1e-6)) { btype[i] = 1; itype[i] = 2; }
                 if (zz[i] >= (p.obc_L3 - 1e-6) && (zz[i] < p.obc_L4 - 1e-6)) { btype[i] = 2; itype[i] = 2; }
@@ -831,13 +862,22 @@ static int commit_t(SphdemHandle* H) {
     {
         auto& pt = H->stage_i[0][SPHDEM_F_PTYPE];
         auto& bt = H->stage_i[0][SPHDEM_F_BUFFER_TYPE];
+        auto& itv = H->stage_i[0][SPHDEM_F_ITYPE];
         int nw = 0, nb = 0;
         // the position records carry p_type in 16 bits
         for (int i = 0; i < ns; i++)
             if (pt[i] < -32768 || pt[i] > 32767) return SPHDEM_E_UNSUPPORTED;
         for (int i = 0; i < ns; i++) {
+            if (itv[i] == 3) continue;
             if (pt[i] <= 0) nw++;
             if (bt[i] > 0 && pt[i] < 1000) nb++;
+        }
+        // launch bounds of the per-wall and per-buffer passes; the passes stop
+        // at the step's own count.  A slab's membership changes every step:
+        // headroom, and an overflow flag beyond it.
+        if (H->dom_set) {
+            nw = std::min(ns, nw + std::max(nw, 1024));
+            nb = std::min(ns, nb + std::max(nb, 1024));
         }
         P.nwall = nw;
         P.nbuf = nb;
@@ -1993,8 +2033,11 @@ extern "C" int sphdem_set_field(SphdemHandle* h, int which, int field, const voi
         h->stage_d[which][field].assign(s, s + n);
         return SPHDEM_OK;
     }
-    if (is_int_field(field) && field != SPHDEM_F_CELL && field != SPHDEM_F_PID && field != SPHDEM_F_ITYPE &&
-        field != SPHDEM_F_BUFFER_TYPE) {
+    // i_type, buffer type and id are derived at commit; a slab of a larger
+    // bed (sphdem_set_domain) passes its ids and parked slots (i_type 3)
+    const bool slab_field = h->dom_set && (field == SPHDEM_F_PID || field == SPHDEM_F_ITYPE);
+    if (is_int_field(field) && field != SPHDEM_F_CELL &&
+        (slab_field || (field != SPHDEM_F_PID && field != SPHDEM_F_ITYPE && field != SPHDEM_F_BUFFER_TYPE))) {
         if (bytes != sizeof(int) * (size_t)n) return SPHDEM_E_ARG;
         const int* s = (const int*)src;
         h->stage_i[which][field].assign(s, s + n);
@@ -2537,6 +2580,197 @@ extern "C" int sphdem_get_time(SphdemHandle* h, double* time, int32_t* count) {
     return SPHDEM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// slab exchange of a spatially sharded bed (slab.cuh)
+// ---------------------------------------------------------------------------
+extern "C" int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_ref) {
+    if (!h || !bbox6 || h->committed || h->kind != 0) return SPHDEM_E_ARG;
+    if (!(h0 > 0) || !std::isfinite(t_ref)) return SPHDEM_E_ARG;
+    for (int k = 0; k < 3; k++)
+        if (!(bbox6[2 * k + 1] >= bbox6[2 * k])) return SPHDEM_E_ARG;
+    for (int k = 0; k < 6; k++) h->dom_bbox[k] = bbox6[k];
+    h->dom_h0 = h0;
+    h->dom_tref = (double)(float)t_ref;
+    h->dom_set = true;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_bed_domain(const SphdemParams* p, const double* sx, const double* sy, const double* sz,
+                                  const double* sh, const double* stemp, int32_t ns, const double* dx,
+                                  const double* dy, const double* dz, const double* dh, int32_t nd, double* bbox6,
+                                  double* h0, double* t_ref) {
+    if (!p || !bbox6 || !h0 || !t_ref || ns < 0 || nd < 0 || ns + nd == 0) return SPHDEM_E_ARG;
+    if ((ns > 0 && (!sx || !sy || !sz || !sh || !stemp)) || (nd > 0 && (!dx || !dy || !dz || !dh))) return SPHDEM_E_ARG;
+    std::vector<double> fx(sx, sx + ns), fy(sy, sy + ns), fz(sz, sz + ns);
+    fx.insert(fx.end(), dx, dx + nd);
+    fy.insert(fy.end(), dy, dy + nd);
+    fz.insert(fz.end(), dz, dz + nd);
+    bed_box(*p, fx.data(), fy.data(), fz.data(), ns + nd, bbox6);
+    *h0 = ns > 0 ? sh[0] : dh[0];
+    double s = 0;
+    for (int i = 0; i < ns; i++) s += stemp[i];
+    *t_ref = ns > 0 ? (double)(float)(s / (double)ns) : 0.0;
+    if (!std::isfinite(*t_ref)) *t_ref = 0.0;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_slab_record_bytes(int which) {
+    return which == SPHDEM_SPH ? SLAB_SPH_BYTES : (which == SPHDEM_DEM ? SLAB_DEM_BYTES : SPHDEM_E_ARG);
+}
+
+namespace {
+
+template <typename R>
+SphCur<R> sph_cur(SphdemHandle* H) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    Engine<R>& E = EH->E;
+    SphState<R>& S = E.S[E.cur_s];
+    SphWork<R>& W = E.sw;
+    const bool xs = E.P.xsph;
+    SphCur<R> C;
+    C.x = S.x; C.y = S.y; C.z = S.z; C.h = S.h;
+    C.ux = xs ? W.u_tmpx : S.ux; C.uy = xs ? W.u_tmpy : S.uy; C.uz = xs ? W.u_tmpz : S.uz;
+    C.temp = xs ? W.temp_tmp : S.temp;
+    C.m = W.m_new; C.rho = W.rho_new; C.pres = W.p_new;
+    C.dDEMpor = S.dDEMpor; C.flt_s = S.flt_s;
+    C.ptype = S.ptype; C.btype = S.btype; C.itype = S.itype; C.pid = S.pid;
+    C.t_ref = E.P.t_ref;
+    return C;
+}
+
+// positions and i_type of the current state of one set
+template <typename R>
+void set_xyzi(SphdemHandle* H, int which, const double** x, const double** y, const double** z, int** it, int* n) {
+    EngineHost<R>* EH = (EngineHost<R>*)H->eng;
+    Engine<R>& E = EH->E;
+    if (which == SPHDEM_SPH) {
+        SphState<R>& S = E.S[E.cur_s];
+        *x = S.x; *y = S.y; *z = S.z; *it = S.itype; *n = E.P.ns;
+    } else {
+        DemState<double>& D = E.D[E.cur_d];
+        *x = D.x; *y = D.y; *z = D.z; *it = D.itype; *n = E.P.nd;
+    }
+}
+
+const DevParams& dev_params(SphdemHandle* H) {
+    return H->prec == SPHDEM_PREC_FP64 ? ((EngineHost<double>*)H->eng)->E.P : ((EngineHost<float>*)H->eng)->E.P;
+}
+
+// slots of one set selected by mode (0: active with layer in [lo, hi); 1:
+// parked), ascending, into slots[0, cap); the count to *count (host)
+int slab_select(SphdemHandle* H, int which, int axis, int lo, int hi, int mode, int* slots, int cap, int* count) {
+    const double *x, *y, *z;
+    int* it;
+    int n;
+    if (H->prec == SPHDEM_PREC_FP64) set_xyzi<double>(H, which, &x, &y, &z, &it, &n);
+    else set_xyzi<float>(H, which, &x, &y, &z, &it, &n);
+    const DevParams& P = dev_params(H);
+    cudaStream_t st = H->stream;
+    int nb = std::max(1, nblocks(n, TPB));
+    if (nb > H->slab_blk_n) {
+        if (H->slab_blk) CK(cudaFree(H->slab_blk));
+        CK(cudaMalloc(&H->slab_blk, sizeof(int) * nb));
+        H->slab_blk_n = nb;
+    }
+    if (!H->slab_tot) CK(cudaMalloc(&H->slab_tot, sizeof(int)));
+    k_slab_flag<<<nb, TPB, 0, st>>>(P, n, x, y, z, it, axis, lo, hi, mode, H->slab_blk);
+    k_slab_scan<<<1, 1024, 0, st>>>(nb, H->slab_blk, H->slab_tot);
+    k_slab_compact<<<nb, TPB, 0, st>>>(P, n, x, y, z, it, axis, lo, hi, mode, H->slab_blk, slots, cap);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(count, H->slab_tot, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPHDEM_OK;
+}
+
+}  // namespace
+
+extern "C" int sphdem_slab_select(SphdemHandle* h, int which, int axis, int32_t lo, int32_t hi, int32_t* d_slots,
+                                  int32_t cap, int32_t* count) {
+    if (!h || !h->committed || h->kind != 0 || !count || axis < 0 || axis > 2) return SPHDEM_E_ARG;
+    if (which != SPHDEM_SPH && which != SPHDEM_DEM) return SPHDEM_E_ARG;
+    if (cap > 0 && !d_slots) return SPHDEM_E_ARG;
+    return slab_select(h, which, axis, lo, hi, 0, d_slots, cap, count);
+}
+
+extern "C" int sphdem_slab_export(SphdemHandle* h, int which, const int32_t* d_slots, int32_t n, void* d_buf) {
+    if (!h || !h->committed || h->kind != 0 || n < 0 || (n > 0 && (!d_slots || !d_buf))) return SPHDEM_E_ARG;
+    if (n == 0) return SPHDEM_OK;
+    cudaStream_t st = h->stream;
+    unsigned char* buf = (unsigned char*)d_buf;
+    if (which == SPHDEM_SPH) {
+        if (h->prec == SPHDEM_PREC_FP64) k_slab_export_sph<double><<<nblocks(n, TPB), TPB, 0, st>>>(sph_cur<double>(h), d_slots, n, buf);
+        else k_slab_export_sph<float><<<nblocks(n, TPB), TPB, 0, st>>>(sph_cur<float>(h), d_slots, n, buf);
+    } else if (which == SPHDEM_DEM) {
+        if (h->prec == SPHDEM_PREC_FP64) {
+            Engine<double>& E = ((EngineHost<double>*)h->eng)->E;
+            k_slab_export_dem<<<nblocks(n, TPB), TPB, 0, st>>>(E.D[E.cur_d], E.P.nd, d_slots, n, buf);
+        } else {
+            Engine<float>& E = ((EngineHost<float>*)h->eng)->E;
+            k_slab_export_dem<<<nblocks(n, TPB), TPB, 0, st>>>(E.D[E.cur_d], E.P.nd, d_slots, n, buf);
+        }
+    } else {
+        return SPHDEM_E_ARG;
+    }
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_slab_keep(SphdemHandle* h, int which, int axis, int32_t lo, int32_t hi) {
+    if (!h || !h->committed || h->kind != 0 || axis < 0 || axis > 2) return SPHDEM_E_ARG;
+    if (which != SPHDEM_SPH && which != SPHDEM_DEM) return SPHDEM_E_ARG;
+    const double *x, *y, *z;
+    int* it;
+    int n;
+    if (h->prec == SPHDEM_PREC_FP64) set_xyzi<double>(h, which, &x, &y, &z, &it, &n);
+    else set_xyzi<float>(h, which, &x, &y, &z, &it, &n);
+    if (n == 0) return SPHDEM_OK;
+    k_slab_keep<<<nblocks(n, TPB), TPB, 0, h->stream>>>(dev_params(h), n, x, y, z, it, axis, lo, hi);
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_slab_import(SphdemHandle* h, int which, const void* d_buf, int32_t n) {
+    if (!h || !h->committed || h->kind != 0 || n < 0 || (n > 0 && !d_buf)) return SPHDEM_E_ARG;
+    if (which != SPHDEM_SPH && which != SPHDEM_DEM) return SPHDEM_E_ARG;
+    if (n == 0) return SPHDEM_OK;
+    if (n > h->slab_free_n) {
+        if (h->slab_free) CK(cudaFree(h->slab_free));
+        CK(cudaMalloc(&h->slab_free, sizeof(int) * n));
+        h->slab_free_n = n;
+    }
+    // the first n parked slots, ascending
+    int parked = 0;
+    int r = slab_select(h, which, 0, 0, 0, 1, h->slab_free, n, &parked);
+    if (r) return r;
+    if (parked < n) return SPHDEM_E_NOMEM;
+    cudaStream_t st = h->stream;
+    const unsigned char* buf = (const unsigned char*)d_buf;
+    if (which == SPHDEM_SPH) {
+        if (h->prec == SPHDEM_PREC_FP64) k_slab_import_sph<double><<<nblocks(n, TPB), TPB, 0, st>>>(sph_cur<double>(h), h->slab_free, n, buf);
+        else k_slab_import_sph<float><<<nblocks(n, TPB), TPB, 0, st>>>(sph_cur<float>(h), h->slab_free, n, buf);
+    } else {
+        if (h->prec == SPHDEM_PREC_FP64) {
+            Engine<double>& E = ((EngineHost<double>*)h->eng)->E;
+            k_slab_import_dem<<<nblocks(n, TPB), TPB, 0, st>>>(E.D[E.cur_d], E.P.nd, h->slab_free, n, buf);
+        } else {
+            Engine<float>& E = ((EngineHost<float>*)h->eng)->E;
+            k_slab_import_dem<<<nblocks(n, TPB), TPB, 0, st>>>(E.D[E.cur_d], E.P.nd, h->slab_free, n, buf);
+        }
+    }
+    CK(cudaGetLastError());
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_slab_active(SphdemHandle* h, int which, int32_t* n_active) {
+    if (!h || !h->committed || h->kind != 0 || !n_active) return SPHDEM_E_ARG;
+    if (which != SPHDEM_SPH && which != SPHDEM_DEM) return SPHDEM_E_ARG;
+    int parked = 0;
+    int r = slab_select(h, which, 0, 0, 0, 1, nullptr, 0, &parked);
+    if (r) return r;
+    *n_active = (which == SPHDEM_SPH ? h->ns : h->nd) - parked;
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_get_counts(SphdemHandle* h, int32_t* ns, int32_t* nd) {
     if (!h || !ns || !nd) return SPHDEM_E_ARG;
     *ns = h->ns;
@@ -2571,6 +2805,9 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     if (h->snap_done) cudaEventDestroy(h->snap_done);
     if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
     if (h->side) cudaStreamDestroy(h->side);
+    if (h->slab_blk) cudaFree(h->slab_blk);
+    if (h->slab_tot) cudaFree(h->slab_tot);
+    if (h->slab_free) cudaFree(h->slab_free);
     if (h->dem_stream) cudaStreamDestroy(h->dem_stream);
     for (cudaEvent_t e : h->fork_ev)
         if (e) cudaEventDestroy(e);

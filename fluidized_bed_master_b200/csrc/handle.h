@@ -41,6 +41,16 @@ struct SphdemHandle {
     cudaStream_t dem_stream = nullptr;
     cudaEvent_t fork_ev[6] = {};
     int concurrent = 1;                  // sphdem_set_concurrency
+    // the whole bed's domain for a slab of it (sphdem_set_domain, before commit)
+    bool dom_set = false;
+    double dom_bbox[6] = {};
+    double dom_h0 = 0, dom_tref = 0;
+    // device scratch of the slab calls
+    int* slab_blk = nullptr;             // per-block counts, then offsets
+    int slab_blk_n = 0;
+    int* slab_tot = nullptr;
+    int* slab_free = nullptr;            // parked slots found by sphdem_slab_import
+    int slab_free_n = 0;
     int64_t last_launches = 0;
     // per-kernel timing (events recorded inside the step graph)
     int timing = 0;

@@ -103,7 +103,7 @@ struct SphGatherSrc {
 template <typename R>
 __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R> gsrc, SphState<R> dst,
                                    SphRec<R> rec, const int* __restrict__ perm, int* wall_idx, int* buf_idx,
-                                   int* counters) {
+                                   int* counters, DevFlags* F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -132,8 +132,18 @@ __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R>
     store_pos(rec.pos, i, make_pos<R>(P, x, y, z, pt, bt, it));
     rec.mr0[i] = mk2<R>(m, rho);
     rec.up[i] = mk4<R>(ux, uy, uz, pr);
-    if (pt <= 0) wall_idx[atomicAdd(&counters[0], 1)] = i;
-    if (bt > 0 && pt < 1000) buf_idx[atomicAdd(&counters[1], 1)] = i;
+    // walls and buffer particles of the step (parked slots excluded), up to
+    // the launch bounds of their passes
+    if (it != 3 && pt <= 0) {
+        int k = atomicAdd(&counters[0], 1);
+        if (k < P.nwall) wall_idx[k] = i;
+        else atomicOr(&F->overflow, 4);
+    }
+    if (it != 3 && bt > 0 && pt < 1000) {
+        int k = atomicAdd(&counters[1], 1);
+        if (k < P.nbuf) buf_idx[k] = i;
+        else atomicOr(&F->overflow, 4);
+    }
 }
 
 template <typename R>
@@ -1588,7 +1598,7 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
-    if (w >= P.nwall) return;
+    if (w >= P.nwall || w >= W.counters[0]) return;
     const SphRec<R> rec = W.rec;
     int i = W.wall_idx[w];
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
@@ -2092,7 +2102,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
-    if (w >= P.nbuf) return;
+    if (w >= P.nbuf || w >= W.counters[1]) return;
     int i = W.buf_idx[w];
     int bt = S.btype[i];
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];

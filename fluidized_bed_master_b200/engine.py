@@ -56,6 +56,15 @@ def lib():
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
     L.sphdem_set_graphs.argtypes = [vp, C.c_int]
     L.sphdem_set_concurrency.argtypes = [vp, C.c_int]
+    L.sphdem_set_domain.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double]
+    L.sphdem_slab_record_bytes.argtypes = [C.c_int]
+    dp = C.POINTER(C.c_double)
+    L.sphdem_bed_domain.argtypes = [vp, dp, dp, dp, dp, dp, C.c_int32, dp, dp, dp, dp, C.c_int32, dp, dp, dp]
+    L.sphdem_slab_select.argtypes = [vp, C.c_int, C.c_int, C.c_int32, C.c_int32, vp, C.c_int32, C.POINTER(C.c_int32)]
+    L.sphdem_slab_export.argtypes = [vp, C.c_int, vp, C.c_int32, vp]
+    L.sphdem_slab_keep.argtypes = [vp, C.c_int, C.c_int, C.c_int32, C.c_int32]
+    L.sphdem_slab_import.argtypes = [vp, C.c_int, vp, C.c_int32]
+    L.sphdem_slab_active.argtypes = [vp, C.c_int, C.POINTER(C.c_int32)]
     L.sphdem_collect_timing.argtypes = [vp]
     L.sphdem_get_timing.argtypes = [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_double), P(C.c_int64)]
     L.sphdem_input_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
@@ -86,6 +95,42 @@ def _chk(status, what):
         raise SphdemError(status, what)
 
 
+def torch_sync():
+    """Finish the work torch queued on the current device (before a handle's
+    own stream reads a tensor torch wrote)."""
+    import torch
+
+    torch.cuda.current_stream().synchronize()
+
+
+def bed_domain(params, sph, dem):
+    """(bbox6, h0, t_ref) that a handle of the whole bed would compute at
+    commit (sphdem_bed_domain): the grid every slab of it must share."""
+    L = lib()
+    dp = C.POINTER(C.c_double)
+
+    def arr(d, k):
+        if not d or k not in d:
+            return None, None
+        a = np.ascontiguousarray(d[k], dtype=np.float64)
+        return a, a.ctypes.data_as(dp)
+
+    keep = []
+    ptrs = []
+    for d, keys in ((sph, ("x", "y", "z", "h", "temp")), (dem, ("x", "y", "z", "h"))):
+        for k in keys:
+            a, p = arr(d, k)
+            keep.append(a)
+            ptrs.append(p)
+    ns = len(sph["x"]) if sph else 0
+    nd = len(dem["x"]) if dem else 0
+    bb = (C.c_double * 6)()
+    h0, tr = C.c_double(), C.c_double()
+    _chk(L.sphdem_bed_domain(C.byref(params), *ptrs[:5], ns, *ptrs[5:], nd, bb, C.byref(h0), C.byref(tr)),
+         "sphdem_bed_domain")
+    return list(bb), h0.value, tr.value
+
+
 def default_params():
     p = SphdemParams()
     _chk(lib().sphdem_params_default(C.byref(p)), "sphdem_params_default")
@@ -101,8 +146,10 @@ def read_solv(path, params=None):
 class Engine:
     """One engine handle on the current CUDA device."""
 
-    def __init__(self, params, sph, dem):
-        """params: SphdemParams; sph/dem: dict field-name -> array in input order."""
+    def __init__(self, params, sph, dem, domain=None):
+        """params: SphdemParams; sph/dem: dict field-name -> array in input
+        order.  domain: (bbox6, h0, t_ref) of a larger bed this one is a slab
+        of (sphdem_set_domain; see bed_domain)."""
         L = lib()
         ns = len(sph["x"]) if sph else 0
         nd = len(dem["x"]) if dem else 0
@@ -110,7 +157,11 @@ class Engine:
         _chk(L.sphdem_create(C.byref(params), ns, nd, C.byref(self._h)), "sphdem_create")
         self.params = params.copy()
         self.ns, self.nd = ns, nd
+        self._slot_buf = {}
         try:
+            if domain is not None:
+                bb = (C.c_double * 6)(*[float(v) for v in domain[0]])
+                _chk(L.sphdem_set_domain(self._h, bb, float(domain[1]), float(domain[2])), "sphdem_set_domain")
             for which, d in ((SPH, sph), (DEM, dem)):
                 for name, arr in (d or {}).items():
                     self._set(which, name, arr)
@@ -292,6 +343,54 @@ class Engine:
             out[name.value.decode()] = (ms.value, n.value)
             k += 1
         return out
+
+    # -- slab exchange (sphdem_slab_*): device tensors on the engine's device --
+    def _slots(self, which):
+        import torch
+
+        n = self.ns if which == SPH else self.nd
+        t = self._slot_buf.get(which)
+        if t is None:
+            t = self._slot_buf[which] = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        return t
+
+    def slab_select(self, which, axis, lo, hi):
+        """Active slots whose cell layer along axis is in [lo, hi), ascending
+        (an int32 CUDA tensor)."""
+        buf = self._slots(which)
+        cnt = C.c_int32()
+        _chk(lib().sphdem_slab_select(self._h, which, axis, int(lo), int(hi), C.c_void_p(buf.data_ptr()),
+                                      buf.numel(), C.byref(cnt)), "sphdem_slab_select")
+        return buf[:cnt.value]
+
+    def slab_export(self, which, slots):
+        """Records of the given slots (a uint8 CUDA tensor), written on the
+        engine's stream; the call returns after the copy has finished."""
+        import torch
+
+        rb = lib().sphdem_slab_record_bytes(which)
+        out = torch.empty(max(slots.numel(), 1) * rb, dtype=torch.uint8, device="cuda")
+        _chk(lib().sphdem_slab_export(self._h, which, C.c_void_p(slots.data_ptr()), slots.numel(),
+                                      C.c_void_p(out.data_ptr())), "sphdem_slab_export")
+        torch.cuda.ExternalStream(self.stream_ptr()).synchronize()
+        return out[:slots.numel() * rb]
+
+    def slab_keep(self, which, axis, lo, hi):
+        _chk(lib().sphdem_slab_keep(self._h, which, axis, int(lo), int(hi)), "sphdem_slab_keep")
+
+    def slab_import(self, which, records):
+        """Unpack records (a uint8 CUDA tensor) into parked slots."""
+        rb = lib().sphdem_slab_record_bytes(which)
+        n = records.numel() // rb
+        if n:
+            records = records.contiguous()
+            torch_sync()
+            _chk(lib().sphdem_slab_import(self._h, which, C.c_void_p(records.data_ptr()), n), "sphdem_slab_import")
+
+    def slab_active(self, which):
+        n = C.c_int32()
+        _chk(lib().sphdem_slab_active(self._h, which, C.byref(n)), "sphdem_slab_active")
+        return n.value
 
     def time(self):
         t, c = C.c_double(), C.c_int32()

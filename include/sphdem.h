@@ -479,6 +479,63 @@ int sphdem_write_vtk_fluid(SphdemHandle* h, const char* path);
 int sphdem_snapshot(SphdemHandle* h);
 int sphdem_write_snapshot(SphdemHandle* h, const char* dem_vtk_path, const char* fluid_vtk_path);
 
+/* ---------------------------------------------------------------------
+ * Spatially sharded beds (one handle per slab of cell layers along one
+ * axis, one GPU each).  The reference shards only its WCSPH step, in x
+ * slabs with a halo copied between GPUs every step (SOPHIA_multi,
+ * WCSPH_Calc.cuh:368-738, functions_NNPS.cuh:202-303); these calls carry
+ * the same idea to the ISPH-DEM step.  A slab handle holds its own cell
+ * layers plus a ghost band of G layers on each side and spare slots parked
+ * with i_type 3 (outside every cell: skipped by every kernel, sorted behind
+ * all cells).  Between steps, each slab sends the particles of its own
+ * layers that lie in a neighbour's ghost band, parks everything outside its
+ * own layers, and imports what its neighbours sent.  With G at least the
+ * number of dependent neighbour passes of one step plus one, the particles
+ * of a slab's own layers step exactly as in the unsharded bed (up to the
+ * summation order inside a cell).  fluidized_bed_master_b200/slabs.py
+ * drives this over torch.distributed (NCCL between GPUs).
+ * All device pointers below are on the handle's device; the calls enqueue
+ * on the handle's stream after the steps so far.
+ * --------------------------------------------------------------------- */
+
+/* The domain a handle of the whole bed (SPH and DEM arrays in input order)
+ * would compute at commit: box with margins, h0, temperature offset. */
+int sphdem_bed_domain(const SphdemParams* p, const double* sx, const double* sy, const double* sz,
+                      const double* sh, const double* stemp, int32_t ns, const double* dx, const double* dy,
+                      const double* dz, const double* dh, int32_t nd, double* bbox6, double* h0,
+                      double* t_ref);
+
+/* Before commit: the whole bed's bounding box (xmin, xmax, ymin, ymax, zmin,
+ * zmax, margins applied), its h0 (cell edge 1.1 kappa h0) and the SPH
+ * temperature offset (rounded to FP32), so that every slab has the same
+ * cell grid and stores temperatures alike.  The per-wall and per-buffer
+ * passes of a slab get headroom for particles that enter its layers. */
+int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_ref);
+
+/* Bytes of one particle record of sphdem_slab_export/import (which: SPH or
+ * DEM); every real value as a double, the DEM record with its contact
+ * history. */
+int sphdem_slab_record_bytes(int which);
+
+/* The active (not parked) slots whose cell layer along axis (0 x, 1 y, 2 z)
+ * is in [lo, hi), ascending, into d_slots[0, cap); synchronises and returns
+ * their number in *count (which may exceed cap). */
+int sphdem_slab_select(SphdemHandle* h, int which, int axis, int32_t lo, int32_t hi, int32_t* d_slots,
+                       int32_t cap, int32_t* count);
+
+/* Pack the current state of n slots into n records at d_buf. */
+int sphdem_slab_export(SphdemHandle* h, int which, const int32_t* d_slots, int32_t n, void* d_buf);
+
+/* Park the active particles whose layer along axis is outside [lo, hi). */
+int sphdem_slab_keep(SphdemHandle* h, int which, int axis, int32_t lo, int32_t hi);
+
+/* Unpack n records into the first n parked slots (SPHDEM_E_NOMEM when
+ * fewer are parked); synchronises. */
+int sphdem_slab_import(SphdemHandle* h, int which, const void* d_buf, int32_t n);
+
+/* Number of active (not parked) particles of one set; synchronises. */
+int sphdem_slab_active(SphdemHandle* h, int which, int32_t* n_active);
+
 /* Restart file in input.txt format: tab-separated column labels then one
  * row per particle with all columns (fixes save_restart,
  * functions_OUTPUT.cuh:1926-1955). */

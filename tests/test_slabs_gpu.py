@@ -1,0 +1,138 @@
+"""A bed cut into slabs (fluidized_bed_master_b200/slabs.py) against the
+same bed in one handle.
+
+Two z slabs of the bench bed (301,760 SPH + 20,000 DEM, 56 cell layers)
+run as two handles on one GPU; between steps they exchange ghost bands and the
+particles that crossed the slab boundary through the engine's slab calls
+(LocalExchange: the records handed over on the device; nothing waits on
+anything inside a kernel).  The particles of each slab's own layers must
+step as in the whole bed: every particle owned by exactly one slab, every
+field within rel. L2 1e-9 (FP64) after 20 steps, contact partners
+identical; the FP32 build within the FP32 bars of the bench configuration
+(state 1e-5, rates 1e-4).  Only the order of the sums inside a cell
+differs (imported particles take the parked slots).
+"""
+import numpy as np
+import pytest
+
+from fluidized_bed_master_b200.beds import box_bed
+from fluidized_bed_master_b200.params import DEM, SPH
+from tests.helpers import by_id, history_map, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SPH_STATE = ["x", "y", "z", "ux", "uy", "uz", "m", "rho", "pres", "temp", "DEMpor", "flt_s", "rho_ref"]
+SPH_RATE = ["dDEMpor", "ftotalx", "ftotaly", "ftotalz", "fpx", "fpy", "fpz", "pgfx", "pgfy", "pgfz", "dtemp"]
+DEM_STATE = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "temp1", "temp2", "temp3", "flt_s",
+             "flt_sd", "flt_sd2"]
+DEM_RATE = ["Fdx_df", "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz", "dtemp"]
+STEPS = 20
+
+
+@pytest.fixture(scope="module")
+def bed():
+    return box_bed(seed=41)
+
+
+def _whole(p, sph, dem, prec):
+    from fluidized_bed_master_b200.engine import Engine
+
+    q = p.copy()
+    q.precision = prec
+    return Engine(q, sph, dem)
+
+
+def _slabs(p, sph, dem, prec, world=2):
+    from fluidized_bed_master_b200.slabs import LocalExchange, SlabBed
+
+    q = p.copy()
+    q.precision = prec
+    beds = [SlabBed(q, sph, dem, r, world, axis=2) for r in range(world)]
+    return beds, LocalExchange(world)
+
+
+def _owned(beds, which, fields):
+    parts = [b.owned(which, fields) for b in beds]
+    return {k: np.concatenate([pt[k] for pt in parts]) for k in parts[0]}
+
+
+def _partners_of(eng, mask=None):
+    ids, springs = eng.history()
+    m = history_map(np.asarray(ids, dtype=float), springs)
+    dem_ids = eng.get(DEM, "dem_idx")
+    it = eng.get(DEM, "i_type")
+    return {int(dem_ids[i]): m[i] for i in range(len(dem_ids)) if it[i] != 3 and (mask is None or mask[i])}
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_two_slabs_step_as_the_whole_bed(bed, prec):
+    from fluidized_bed_master_b200.slabs import cell_layer, step_local
+
+    p, sph, dem = bed
+    whole = _whole(p, sph, dem, prec)
+    beds, tr = _slabs(p, sph, dem, prec)
+    assert beds[0].hi == beds[1].lo and beds[0].lo == 0 and beds[1].hi == beds[1].n_layers
+    whole.step(STEPS)
+    step_local(beds, tr, STEPS)
+    bad = {}
+    for which, state, rate, idk in ((SPH, SPH_STATE, SPH_RATE, "pid"), (DEM, DEM_STATE, DEM_RATE, "pid")):
+        o = _owned(beds, which, state + rate)
+        n = whole.ns if which == SPH else whole.nd
+        assert np.array_equal(np.sort(o[idk]), np.arange(n)), "every particle owned by exactly one slab"
+        wid = whole.get(which, idk)
+        for f in state + rate:
+            e = rel_l2(by_id(o[idk], o[f]), by_id(wid, whole.get(which, f)))
+            tol = 1e-9 if prec == 1 else (1e-5 if f in state else 1e-4)
+            if not e <= tol:
+                bad[("sph" if which == SPH else "dem", f)] = e
+    assert not bad, sorted(bad.items(), key=lambda kv: -kv[1])
+    # contact partners of the owned spheres
+    pw = _partners_of(whole)
+    for b in beds:
+        bbox = b.domain[0]
+        lay = cell_layer(b.eng.get(DEM, "z"), bbox[4], bbox[5], b.n_layers)
+        mine = (lay >= b.lo) & (lay < b.hi)
+        for k, v in _partners_of(b.eng, mine).items():
+            assert set(v) == set(pw[k]), f"contact partners of sphere {k} differ"
+
+
+def test_slab_records_round_trip(bed):
+    """Export then import restores a particle's state exactly, and an import
+    beyond the parked slots is refused (SPHDEM_E_NOMEM, nothing written)."""
+    import torch
+
+    from fluidized_bed_master_b200.engine import SphdemError
+    from fluidized_bed_master_b200.slabs import SlabBed
+
+    p, sph, dem = bed
+    b = SlabBed(p, sph, dem, 0, 1, axis=2)
+    e = b.eng
+    e.step(2)
+    for which, fields in ((SPH, ["x", "z", "ux", "uz", "m", "rho", "pres", "temp", "flt_s", "dDEMpor"]),
+                          (DEM, ["x", "z", "ux", "wz", "temp", "temp2", "Fdz_df", "Q_sd"])):
+        idk = "pid"
+        before = {f: e.get(which, f) for f in fields + [idk, "i_type"]}
+        if which == DEM:
+            hid0, hds0 = e.history()
+        slots = e.slab_select(which, 2, 0, b.n_layers)
+        n_act = e.slab_active(which)
+        assert slots.numel() == n_act
+        rec = e.slab_export(which, slots[:100])
+        e.slab_keep(which, 2, 10 ** 9, 10 ** 9 + 1)          # park everything
+        assert e.slab_active(which) == 0
+        e.slab_import(which, rec)
+        assert e.slab_active(which) == 100
+        after = {f: e.get(which, f) for f in fields + [idk, "i_type"]}
+        got = {int(k): i for i, k in enumerate(after[idk]) if after["i_type"][i] != 3}
+        if which == DEM:
+            hid1, hds1 = e.history()
+        for i in slots[:100].cpu().numpy():
+            j = got[int(before[idk][i])]
+            for f in fields:
+                assert after[f][j] == before[f][i], (which, f)
+            if which == DEM:   # the contact history travels with its sphere
+                assert np.array_equal(hid1[j], hid0[i]) and np.array_equal(hds1[j], hds0[i])
+        rb = rec.numel() // 100
+        too_many = torch.zeros(rb * ((e.ns if which == SPH else e.nd) + 1), dtype=torch.uint8, device="cuda")
+        with pytest.raises(SphdemError):
+            e.slab_import(which, too_many)
