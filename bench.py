@@ -47,12 +47,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="bed",
-                    choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column", "mlp"],
+                    choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column", "mlp", "slabs"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
                          "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
                          "against the same beds run one after another; ppe-profile: --steps steps of the bed with the "
                          "projected-start PCG and step graphs off, so that a kernel profiler sees the PPE "
-                         "kernels (no timing)")
+                         "kernels (no timing); slabs: the bench bed cut into z slabs, one per rank (on one "
+                         "GPU: --slabs slabs in one process), exchanging ghost bands every step")
+    ap.add_argument("--slabs", type=int, default=2, help="slabs on one GPU for --workload slabs")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -1337,6 +1339,64 @@ def ppe_comparison(args):
     return out
 
 
+def run_slabs(args, world, rank, local, pg):
+    """The bench bed cut into z slabs (fluidized_bed_master_b200/slabs.py):
+    one slab per rank with the ghost bands exchanged over NCCL every step, or
+    with one rank --slabs slabs stepped one after another on one GPU.  Each
+    timed step is every slab's step plus the exchange; the time is taken by
+    the host clock between device synchronisations (the exchange synchronises
+    with the host), max over ranks.  value = particles of the whole bed x
+    steps / time: the same work at every N, so "scaling" is strong."""
+    import torch
+
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.params import DEM, SPH
+    from fluidized_bed_master_b200.slabs import DistExchange, LocalExchange, SlabBed, step_dist, step_local
+
+    torch.cuda.set_device(local)
+    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    p.precision = 1 if args.precision == "fp64" else 0
+    n_whole = len(sph["x"]) + len(dem["x"])
+    if world > 1:
+        beds = [SlabBed(p, sph, dem, rank, world, axis=2)]
+        tr = DistExchange()
+        run = lambda n: step_dist(beds[0], tr, n)
+    else:
+        beds = [SlabBed(p, sph, dem, r, args.slabs, axis=2) for r in range(args.slabs)]
+        tr = LocalExchange(args.slabs)
+        run = lambda n: step_local(beds, tr, n)
+    run(args.warmup)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    run(args.steps)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    if pg:
+        pg.barrier()
+    t_max = reduce_over_ranks(pg, t, "max", "cuda")
+    act = sum(b.eng.slab_active(SPH) + b.eng.slab_active(DEM) for b in beds)
+    act_all = reduce_over_ranks(pg, act, "sum", "cuda")
+    slabs = [(b.lo, b.hi) for b in beds] if world == 1 else None
+    line = {
+        "metric": "SPH-DEM particle-updates/s (3-D fluidized bed, ISPH-DEM step, z slabs)",
+        "value": n_whole * args.steps / t_max, "unit": "particle-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if p.precision == 1 else "f32", "data": "synthetic (seeded box bed)",
+        "config": {"workload": WORKLOAD_TEXT, "n_sph": len(sph["x"]), "n_dem": len(dem["x"]),
+                   "slabs": world if world > 1 else args.slabs, "ghost_layers": beds[0].ghost,
+                   "layers": beds[0].n_layers, "slab_layers": slabs,
+                   "parallelism": f"z slabs x{world}" if world > 1 else f"{args.slabs} z slabs on 1 GPU"},
+        "active_over_whole": act_all / n_whole,
+        "how": "each step: every slab steps, then sends its particles in the neighbours' ghost bands, parks what "
+               "left its layers and imports what its neighbours sent (host clock between device syncs)",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup()
@@ -1353,6 +1413,8 @@ def main():
         elif args.workload == "ppe-profile":
             if rank == 0:
                 run_ppe_profile(args)
+        elif args.workload == "slabs":
+            run_slabs(args, world, rank, local, pg)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

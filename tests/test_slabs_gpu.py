@@ -1,8 +1,10 @@
 """A bed cut into slabs (fluidized_bed_master_b200/slabs.py) against the
 same bed in one handle.
 
-Two z slabs of the bench bed (301,760 SPH + 20,000 DEM, 56 cell layers)
-run as two handles on one GPU; between steps they exchange ghost bands and the
+Two z slabs of the bench bed (301,760 SPH + 20,000 DEM, 56 cell layers;
+fluid velocities perturbed by U(-0.05, 0.05) m/s so that every neighbour
+pass carries information across the slab boundary) run as two handles on
+one GPU; between steps they exchange ghost bands and the
 particles that crossed the slab boundary through the engine's slab calls
 (LocalExchange: the records handed over on the device; nothing waits on
 anything inside a kernel).  The particles of each slab's own layers must
@@ -31,7 +33,11 @@ STEPS = 20
 
 @pytest.fixture(scope="module")
 def bed():
-    return box_bed(seed=41)
+    p, sph, dem = box_bed(seed=41)
+    rng = np.random.default_rng(7)
+    for k in ("ux", "uy", "uz"):
+        sph[k] = sph[k] + rng.uniform(-0.05, 0.05, len(sph["x"]))
+    return p, sph, dem
 
 
 def _whole(p, sph, dem, prec):
@@ -94,6 +100,27 @@ def test_two_slabs_step_as_the_whole_bed(bed, prec):
         mine = (lay >= b.lo) & (lay < b.hi)
         for k, v in _partners_of(b.eng, mine).items():
             assert set(v) == set(pw[k]), f"contact partners of sphere {k} differ"
+
+
+def test_thin_ghost_band_is_not_enough(bed):
+    """With 2 ghost layers instead of 12 the truncated neighbourhoods at the
+    outer edge of a ghost band reach a slab's own layers within a step, and
+    the FP64 comparison above sees it: the test is not vacuous.  (Measured on
+    this bed after 10 steps: 2 layers 1e-6, 3 layers 1e-12, 4 layers 1e-16,
+    5 and more bit-identical to the whole bed; 12 is the bound from the
+    passes of a step.)"""
+    from fluidized_bed_master_b200.slabs import LocalExchange, SlabBed, step_local
+
+    p, sph, dem = bed
+    q = p.copy()
+    q.precision = 1
+    whole = _whole(p, sph, dem, 1)
+    beds = [SlabBed(q, sph, dem, r, 2, axis=2, ghost=2) for r in range(2)]
+    whole.step(STEPS)
+    step_local(beds, LocalExchange(2), STEPS)
+    o = _owned(beds, SPH, ["pres", "ux"])
+    errs = [rel_l2(by_id(o["pid"], o[f]), by_id(whole.get(SPH, "pid"), whole.get(SPH, f))) for f in ("pres", "ux")]
+    assert max(errs) > 1e-8, errs
 
 
 def test_slab_records_round_trip(bed):
