@@ -62,17 +62,19 @@ struct KTimer {
     SphdemHandle* H;
     int k;
     cudaStream_t s;
-    KTimer(SphdemHandle* h, int kk, cudaStream_t st = nullptr) : H(h), k(kk), s(st ? st : h->stream) {
-        if (H->timing) {
+    KTimer(SphdemHandle* h, int kk, cudaStream_t st = nullptr)
+        : H(h), k(kk), s(st ? st : h->stream), on(h->timing && (h->time_only < 0 || h->time_only == kk)) {
+        if (on) {
             record_event(H->ev_beg[k], s);
             H->ev_used[k] = 1;
         }
     }
     void stop() {
-        if (H->timing && !stopped) record_event(H->ev_end[k], s);
+        if (on && !stopped) record_event(H->ev_end[k], s);
         stopped = true;
     }
     ~KTimer() { stop(); }
+    bool on;
     bool stopped = false;
 };
 #define KTIME(k) KTimer kt_##__LINE__(H, k)
@@ -2295,6 +2297,19 @@ extern "C" int sphdem_set_timing(SphdemHandle* h, int on) {
         h->graph_kused.clear();
     }
     h->timing = on ? 1 : 0;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_set_timing_only(SphdemHandle* h, int k) {
+    if (!h || k < -1 || k >= KT_COUNT) return SPHDEM_E_ARG;
+    if (k != h->time_only) {
+        CK(cudaStreamSynchronize(h->stream));
+        for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+        h->graphs.clear();
+        h->graph_launches.clear();
+        h->graph_kused.clear();
+    }
+    h->time_only = k;
     return SPHDEM_OK;
 }
 

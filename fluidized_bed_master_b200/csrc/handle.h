@@ -41,6 +41,7 @@ struct SphdemHandle {
     cudaStream_t dem_stream = nullptr;
     cudaEvent_t fork_ev[6] = {};
     int concurrent = 1;                  // sphdem_set_concurrency
+    int time_only = -1;                  // sphdem_set_timing_only: the one kernel timed (-1 all)
     // the whole bed's domain for a slab of it (sphdem_set_domain, before commit)
     bool dom_set = false;
     double dom_bbox[6] = {};

@@ -56,6 +56,7 @@ def lib():
     L.sphdem_set_timing.argtypes = [vp, C.c_int]
     L.sphdem_set_graphs.argtypes = [vp, C.c_int]
     L.sphdem_set_concurrency.argtypes = [vp, C.c_int]
+    L.sphdem_set_timing_only.argtypes = [vp, C.c_int]
     L.sphdem_set_domain.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double]
     L.sphdem_slab_record_bytes.argtypes = [C.c_int]
     dp = C.POINTER(C.c_double)
@@ -323,6 +324,22 @@ class Engine:
     def set_graphs(self, on):
         """Step graphs on/off (off: kernel profilers see every launch)."""
         _chk(lib().sphdem_set_graphs(self._h, int(bool(on))), "sphdem_set_graphs")
+
+    def set_timing_only(self, name=None):
+        """Time only the named kernel (a key of timing()), or every kernel."""
+        k = -1
+        if name is not None:
+            names = list(self.timing_names())
+            k = names.index(name)
+        _chk(lib().sphdem_set_timing_only(self._h, k), "sphdem_set_timing_only")
+
+    def timing_names(self):
+        out = []
+        name = C.create_string_buffer(64)
+        ms, n = C.c_double(), C.c_int64()
+        while lib().sphdem_get_timing(self._h, len(out), name, 64, C.byref(ms), C.byref(n)) == 0:
+            out.append(name.value.decode())
+        return out
 
     def set_concurrency(self, on):
         """DEM branch of the step on its own stream (default) or on the step stream."""

@@ -438,6 +438,12 @@ int sphdem_set_history(SphdemHandle* h, const int32_t* ids, const double* spring
 int sphdem_set_timing(SphdemHandle* h, int on);
 int sphdem_collect_timing(SphdemHandle* h);
 
+/* Restrict the per-kernel timing to kernel k (the index of
+ * sphdem_get_timing), or -1 for every kernel (the default).  Each timed
+ * kernel adds two event records to the step graph; timing one kernel keeps
+ * the step's own time within a few microseconds of the untimed step. */
+int sphdem_set_timing_only(SphdemHandle* h, int k);
+
 /* The ISPH-DEM step runs the DEM kernels that read no SPH pass (DEM NNPS,
  * contact, filters, corrector) on a second stream, forked from and joined
  * to the handle's stream inside the step (on by default).  Off, every
