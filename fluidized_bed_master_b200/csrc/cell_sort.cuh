@@ -35,6 +35,32 @@
 
 namespace sphdem {
 
+// Programmatic dependent launch (launch_pdl in engine.cu): a kernel launched
+// with programmatic stream serialization may be scheduled while the previous
+// kernel of its stream drains, and waits here, before touching memory, until
+// that kernel has completed and its writes are visible (a no-op for a plain
+// launch).  Every thread waits before any early return, so a kernel never
+// completes before its predecessor: the chain stays transitive.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// launch with programmatic stream serialization: the kernel may be
+// scheduled while its stream's previous kernel drains (it must begin with
+// grid_dep_wait).  Inside a captured graph this becomes a programmatic edge.
+template <typename... KP, typename... A>
+inline cudaError_t launch_pdl(void (*k)(KP...), dim3 g, dim3 b, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 constexpr int SORT_TILE = 4096;   // scan tile: 1024 threads x 4 buckets
 
 struct CellSort {
@@ -59,6 +85,7 @@ __device__ __forceinline__ void cell_count(int* cnt, int key) {
 }
 
 __global__ void __launch_bounds__(1024) k_sort_tile_sums(const int* __restrict__ cnt, int nb, int* tile_sum) {
+    grid_dep_wait();
     const int base = blockIdx.x * SORT_TILE + threadIdx.x * 4;
     int s = 0;
 #pragma unroll
@@ -80,6 +107,7 @@ __global__ void __launch_bounds__(1024) k_sort_tile_sums(const int* __restrict__
 // tiles' sums (in tile order); fill[] is reset for the scatter
 __global__ void __launch_bounds__(1024) k_sort_scan(const int* __restrict__ cnt, const int* __restrict__ tile_sum,
                                                     int nb, int* start, int* fill) {
+    grid_dep_wait();
     __shared__ int ws[32];
     __shared__ int toff;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -132,6 +160,7 @@ __global__ void __launch_bounds__(1024) k_sort_scan(const int* __restrict__ cnt,
 
 __global__ void k_sort_scatter(int n, const int* __restrict__ key, const int* __restrict__ start, int* fill,
                                int* tmp) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = i < n ? key[i] : -1;
     const unsigned peers = __match_any_sync(0xffffffffu, k);
@@ -148,6 +177,7 @@ __global__ void k_sort_scatter(int n, const int* __restrict__ key, const int* __
 __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
                                                      const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
                                                      int* ge, int skip_last) {
+    grid_dep_wait();
     const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (b >= nb) return;
@@ -229,12 +259,18 @@ __global__ void __launch_bounds__(256) k_sort_last_write(int n, const int* __res
 // scan + scatter + settle for n keys already counted into cs.cnt
 inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* perm, int* key_out, int* gs, int* ge,
                              cudaStream_t st) {
-    k_sort_tile_sums<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.nb, cs.tile_sum);
-    k_sort_scan<<<cs.ntiles, 1024, 0, st>>>(cs.cnt, cs.tile_sum, cs.nb, cs.start, cs.fill);
-    if (n > 0) k_sort_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, key_in, cs.start, cs.fill, cs.tmp);
+    cudaError_t e;
+    if ((e = launch_pdl(k_sort_tile_sums, cs.ntiles, 1024, 0, st, (const int*)cs.cnt, cs.nb, cs.tile_sum))) return e;
+    if ((e = launch_pdl(k_sort_scan, cs.ntiles, 1024, 0, st, (const int*)cs.cnt, (const int*)cs.tile_sum, cs.nb,
+                        cs.start, cs.fill)))
+        return e;
+    if (n > 0 && (e = launch_pdl(k_sort_scatter, (n + 255) / 256, 256, 0, st, n, key_in, (const int*)cs.start,
+                                 cs.fill, cs.tmp)))
+        return e;
     const int big = cs.big_last && n > 0;
-    k_sort_settle<<<(cs.nb * 32 + 255) / 256, 256, 0, st>>>(cs.nb, cs.cnt, cs.start, cs.tmp, perm, key_out, gs, ge,
-                                                            big);
+    if ((e = launch_pdl(k_sort_settle, (cs.nb * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt, (const int*)cs.start,
+                        (const int*)cs.tmp, perm, key_out, gs, ge, big)))
+        return e;
     if (big) {
         const int nblk = (n + 255) / 256;
         k_sort_last_count<<<nblk, 256, 0, st>>>(n, key_in, cs.nb - 1, cs.blk);

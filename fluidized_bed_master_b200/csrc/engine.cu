@@ -238,7 +238,7 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     SphState<R>& S = E.S[src];
     {
         KTIME(KT_HASH_S);
-        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, S.x, S.y, S.z, S.itype, W.key_in, E.cs_s.cnt);
+        CK((launch_pdl(k_hash, nblocks(n, TPB), TPB, 0, st, P, n, S.x, S.y, S.z, S.itype, W.key_in, E.cs_s.cnt)));
     }
     {
         KTIME(KT_SORT_S);
@@ -251,12 +251,12 @@ int nnps_sph(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl) 
     g.m = W.m_new; g.rho = W.rho_new; g.pres = W.p_new;
     {
         KTIME(KT_GATHER_S);
-        k_cells_gather_sph<R><<<nblocks(n, TPB), TPB, 0, st>>>(P, S, g, E.S[dst], W.rec, W.val_out, W.wall_idx,
-                                                                W.buf_idx, W.counters, E.flags);
+        CK((launch_pdl(k_cells_gather_sph<R>, nblocks(n, TPB), TPB, 0, st, P, S, g, E.S[dst], W.rec, W.val_out, W.wall_idx,
+                                                                W.buf_idx, W.counters, E.flags)));
     }
     {
         KTIME(KT_ROWS_S);
-        k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, W.g_str, W.g_end, W.rows);
+        CK((launch_pdl(k_rows, nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st, P, W.g_str, W.g_end, W.rows)));
     }
     *nl += 7;
     CK(cudaGetLastError());
@@ -277,7 +277,7 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl, 
     DemState<double>& D = E.D[src];
     {
         KTIME_ON(KT_HASH_D, st);
-        k_hash<<<nblocks(n, TPB), TPB, 0, st>>>(P, n, D.x, D.y, D.z, D.itype, DW.key_in, E.cs_d.cnt);
+        CK((launch_pdl(k_hash, nblocks(n, TPB), TPB, 0, st, P, n, D.x, D.y, D.z, D.itype, DW.key_in, E.cs_d.cnt)));
     }
     {
         KTIME_ON(KT_SORT_D, st);
@@ -285,13 +285,13 @@ int nnps_dem(SphdemHandle* H, EngineHost<R>* EH, int src, int dst, int64_t* nl, 
     }
     {
         KTIME_ON(KT_GATHER_D, st);
-        k_cells_gather_dem<double><<<nblocks(n, TPB), TPB, 0, st>>>(P, D, E.D[dst], DW.val_out);
-        k_gather_history<<<nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st>>>(n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
-                                                                         E.D[dst].hds);
+        CK((launch_pdl(k_cells_gather_dem<double>, nblocks(n, TPB), TPB, 0, st, P, D, E.D[dst], DW.val_out)));
+        CK((launch_pdl(k_gather_history, nblocks(n * SPHDEM_NSLOT, TPB), TPB, 0, st, n, DW.val_out, D.hid, D.hds, E.D[dst].hid,
+                                                                         E.D[dst].hds)));
     }
     {
         KTIME_ON(KT_ROWS_D, st);
-        k_rows<<<nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st>>>(P, DW.g_str, DW.g_end, DW.rows);
+        CK((launch_pdl(k_rows, nblocks(P.NI * P.NJ * P.NK, TPB), TPB, 0, st, P, DW.g_str, DW.g_end, DW.rows)));
     }
     *nl += 8;
     CK(cudaGetLastError());
@@ -501,13 +501,13 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
 
 // SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
 template <typename R>
-void launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double>& D, cudaStream_t st) {
+cudaError_t launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double>& D, cudaStream_t st) {
     Engine<R>& E = EH->E;
     const DevParams& P = E.P;
     const int ncell = P.NI * P.NJ * P.NK;
-    k_build_dlist<<<(ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st>>>(
-        P, S.x, S.y, S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
-        P.nbd_cap, E.flags);
+    return launch_pdl(k_build_dlist, (ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P, S.x, S.y, S.z,
+                      S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
+                      P.nbd_cap, E.flags);
 }
 
 // ---------------------------------------------------------------------------
@@ -559,13 +559,13 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     CK(wait(2, sd));
     if (ns > 0 && nd > 0) {
         KTIME_ON(KT_DLIST, sd);
-        launch_dlist<R>(EH, S, D, sd);
+        CK(launch_dlist<R>(EH, S, D, sd));
         *nl += 1;
     }
     CK(rec(1, sd));   // SPH -> DEM list built
     if (nd > 0) {
-        { KTIME_ON(KT_DEMCONTACT, sd); k_dem_contact<R><<<bdw, TPB, 0, sd>>>(P, D, DW, DW.rows, E.flags); }
-        { KTIME_ON(KT_DEMPREP, sd); k_dem_prep<R><<<bdw, TPB, 0, sd>>>(P, S, W.rec, D, DW, W.rows, DW.rows); }
+        { KTIME_ON(KT_DEMCONTACT, sd); CK((launch_pdl(k_dem_contact<R>, bdw, TPB, 0, sd, P, D, DW, DW.rows, E.flags))); }
+        { KTIME_ON(KT_DEMPREP, sd); CK((launch_pdl(k_dem_prep<R>, bdw, TPB, 0, sd, P, S, W.rec, D, DW, W.rows, DW.rows))); }
         *nl += 2;
     }
     if (ns > 0) {
@@ -575,23 +575,23 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
                 // one warp per cell; slots outside every cell (i_type 3) keep an empty list
                 CK(cudaMemsetAsync(W.ncnt, 0, sizeof(int) * ns, st));
                 int ncell = P.NI * P.NJ * P.NK;
-                k_build_list_tiled<<<(ncell + LT_WARPS - 1) / LT_WARPS, LT_WARPS * 32, 0, st>>>(
-                    P, S, W.rec, W.g_str, W.g_end, W.rows, W.nbr, W.ncnt, E.flags);
+                CK((launch_pdl(k_build_list_tiled, (ncell + LT_WARPS - 1) / LT_WARPS, LT_WARPS * 32, 0, st, 
+                    P, S, W.rec, W.g_str, W.g_end, W.rows, W.nbr, W.ncnt, E.flags)));
             } else {
-                k_build_list<R><<<bs, TPB, 0, st>>>(P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags);
+                CK((launch_pdl(k_build_list<R>, bs, TPB, 0, st, P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags)));
             }
         }
         CK(wait(1, st));
-        { KTIME(KT_PASSA); k_passA<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW.rows); }
+        { KTIME(KT_PASSA); CK((launch_pdl(k_passA<R>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
         *nl += 2;
         {
             KTIME(KT_PASSB);
             if (P.sps) {
-                k_sps<R><<<bs, TPB, 0, st>>>(P, S, W);
+                CK((launch_pdl(k_sps<R>, bs, TPB, 0, st, P, S, W)));
                 *nl += 1;
             }
-            if (P.iface | P.fb | P.sps | P.ipf) k_passB<R, true><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
-            else k_passB<R, false><<<bs, TPB, 0, st>>>(P, S, W, E.flags);
+            if (P.iface | P.fb | P.sps | P.ipf) CK((launch_pdl(k_passB<R, true>, bs, TPB, 0, st, P, S, W, E.flags)));
+            else CK((launch_pdl(k_passB<R, false>, bs, TPB, 0, st, P, S, W, E.flags)));
         }
         *nl += 1;
     }
@@ -601,61 +601,61 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if (nd > 0) {
         {
             KTIME(KT_DEMCOUPLING);
-            k_dem_coupling<R><<<bdw, TPB, 0, st>>>(P, S, W, D, DW, W.rows);
-            k_dem_finish<R><<<bd, TPB, 0, st>>>(P, D, DW);
+            CK((launch_pdl(k_dem_coupling<R>, bdw, TPB, 0, st, P, S, W, D, DW, W.rows)));
+            CK((launch_pdl(k_dem_finish<R>, bd, TPB, 0, st, P, D, DW)));
         }
         *nl += 2;
     }
     if (ns > 0) {
         KTIME(KT_SPHCOUPLING);
-        k_sph_coupling<R><<<bs, TPB, 0, st>>>(P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0);
+        CK((launch_pdl(k_sph_coupling<R>, bs, TPB, 0, st, P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0)));
         *nl += 1;
     }
     CK(rec(4, st));   // the SPH coupling has read the DEM set
     CK(wait(4, sd));
     if (nd > 0) {
-        { KTIME_ON(KT_DEMUPDATE, sd); k_dem_update<double><<<bd, TPB, 0, sd>>>(P, D, DW); }
+        { KTIME_ON(KT_DEMUPDATE, sd); CK((launch_pdl(k_dem_update<double>, bd, TPB, 0, sd, P, D, DW))); }
         *nl += 1;
     }
     if (ns > 0) {
         if (flags & F_COUNT0) {
             KTIME(KT_NEUMANN0);
             if constexpr (std::is_same<R, float>::value)
-                k_neumann_tiled<<<(P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st>>>(
-                    P, S, W, S.pres, W.g_str, W.g_end, W.rows, 1);
+                CK((launch_pdl(k_neumann_tiled, (P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st, 
+                    P, S, W, S.pres, W.g_str, W.g_end, W.rows, 1)));
             else
-                k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, S.pres, W.rows, 1);
+                CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, S.pres, W.rows, 1)));
             *nl += 1;
         }
         {
             KTIME(KT_PPE);
-            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) k_ppe<R><<<bs, TPB, 0, st>>>(P, S, W);
+            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) CK((launch_pdl(k_ppe<R>, bs, TPB, 0, st, P, S, W)));
             else if ((r = enqueue_krylov<R>(H, EH, S, W))) return r;
         }
         {
             KTIME(KT_NEUMANN);
             if constexpr (std::is_same<R, float>::value)
-                k_neumann_tiled<<<(P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st>>>(
-                    P, S, W, W.p_new, W.g_str, W.g_end, W.rows, 0);
+                CK((launch_pdl(k_neumann_tiled, (P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st, 
+                    P, S, W, W.p_new, W.g_str, W.g_end, W.rows, 0)));
             else
-                k_neumann<R><<<bww, TPB, 0, st>>>(P, S, W, W.p_new, W.rows, 0);
+                CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, W.p_new, W.rows, 0)));
         }
-        { KTIME(KT_PASSC); k_passC<R><<<bs, TPB, 0, st>>>(P, S, W); }
+        { KTIME(KT_PASSC); CK((launch_pdl(k_passC<R>, bs, TPB, 0, st, P, S, W))); }
         *nl += 3;
         if (P.open_bc > 0) {
             KTIME(KT_OPENBC);
-            k_open_bc<R><<<bbw, TPB, 0, st>>>(P, S, W, W.rows);
+            CK((launch_pdl(k_open_bc<R>, bbw, TPB, 0, st, P, S, W, W.rows)));
             *nl += 1;
         }
         if (P.xsph) {
             KTIME(KT_XSPH);
-            k_xsph<R><<<bs, TPB, 0, st>>>(P, S, W);
+            CK((launch_pdl(k_xsph<R>, bs, TPB, 0, st, P, S, W)));
             *nl += 1;
         }
     }
     CK(rec(5, sd));   // join
     CK(wait(5, st));
-    k_tick<<<1, 1, 0, st>>>(E.flags);
+    CK((launch_pdl(k_tick, 1, 1, 0, st, E.flags)));
     *nl += 1;
     CK(cudaGetLastError());
     return SPHDEM_OK;
@@ -964,7 +964,7 @@ static int commit_t(SphdemHandle* H) {
         if (nd > 0) {
             if ((r = nnps_dem<R>(H, EH, 0, 1, &nl, st))) return r;
             CK(cudaMemsetAsync(W.ncntd, 0, sizeof(int) * ns, st));
-            launch_dlist<R>(EH, E.S[1], E.D[1], st);
+            CK(launch_dlist<R>(EH, E.S[1], E.D[1], st));
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(&f, E.flags, sizeof(f), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));

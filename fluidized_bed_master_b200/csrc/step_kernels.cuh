@@ -70,6 +70,7 @@ __device__ __forceinline__ void for_stencil_j(const DevParams& P, int ic, int jc
 // The cell-sort count (cell_count, cell_sort.cuh) is fused in.
 __global__ void k_hash(DevParams P, int n, const double* __restrict__ x, const double* __restrict__ y,
                        const double* __restrict__ z, const int* __restrict__ itype, int* key, int* cnt) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int k = -1;
     if (i < n) {
@@ -86,6 +87,7 @@ __global__ void k_hash(DevParams P, int n, const double* __restrict__ x, const d
 
 // per-cell stencil row table (for_rows), one thread per cell
 __global__ void k_rows(DevParams P, const int* __restrict__ gs, const int* __restrict__ ge, int4* rows) {
+    grid_dep_wait();
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int nc = P.NI * P.NJ * P.NK;
     if (c >= nc) return;
@@ -104,6 +106,7 @@ template <typename R>
 __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R> gsrc, SphState<R> dst,
                                    SphRec<R> rec, const int* __restrict__ perm, int* wall_idx, int* buf_idx,
                                    int* counters, DevFlags* F) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -148,6 +151,7 @@ __global__ void k_cells_gather_sph(DevParams P, SphState<R> src, SphGatherSrc<R>
 
 template <typename R>
 __global__ void k_cells_gather_dem(DevParams P, DemState<R> src, DemState<R> dst, const int* __restrict__ perm) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.nd;
     if (i >= n) return;
@@ -175,6 +179,7 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, SphRec<R> rec,
                                                     const int4* __restrict__ rows,
                                                     int* __restrict__ nbr, int* __restrict__ ncnt, DevFlags* F) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.ns) return;
     double xi = S.x[i], yi = S.y[i], zi = S.z[i];
@@ -305,6 +310,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                                                                       const int4* __restrict__ rows,
                                                                       int* __restrict__ nbr,
                                                                       int* __restrict__ ncnt, DevFlags* F) {
+    grid_dep_wait();
     __shared__ float4 sc[LT_WARPS][LT_CH + 4];
     __shared__ int srow[LT_WARPS][20];   // prefix[10] | start[9]
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -487,6 +493,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
                                                                  const double* __restrict__ dz,
                                                                  const int* __restrict__ dptype, int* __restrict__ nbrd,
                                                                  int* __restrict__ ncntd, int cap, DevFlags* F) {
+    grid_dep_wait();
     __shared__ float4 sc[DL_WARPS][DL_CH + 32];
     __shared__ int srow[DL_WARPS][20];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -589,6 +596,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
 template <typename R>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                const int4* __restrict__ drows) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -717,6 +725,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
 // a slot plane are coalesced
 __global__ void k_gather_history(int n, const int* __restrict__ perm, const int* __restrict__ hid_src,
                                  const double* __restrict__ hds_src, int* hid_dst, double* hds_dst) {
+    grid_dep_wait();
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n * SPHDEM_NSLOT) return;
     int s = q / n, i = q - s * n;
@@ -731,6 +740,7 @@ __global__ void k_gather_history(int n, const int* __restrict__ perm, const int*
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<double> D,
                                                   DemWork<double> DW, const int4* __restrict__ srows, const int4* __restrict__ drows) {
+    grid_dep_wait();
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -810,6 +820,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork<R> W) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -861,6 +872,7 @@ __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork
 // (a separate instantiation, so that the default pass keeps its registers)
 template <typename R, bool FORCES>
 __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -1019,6 +1031,7 @@ template <typename R>
 __global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
                                                      const int4* __restrict__ drows,
                                                      DevFlags* F) {
+    grid_dep_wait();
     // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
     // in visit order (for_rows_warp) and the pair terms are reduced with
     // shuffles.  History writes keep the sequential semantics: lookups use
@@ -1425,6 +1438,7 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<double>& D, Dem
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                       DemWork<double> DW, const int4* __restrict__ srows) {
+    grid_dep_wait();
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -1490,6 +1504,7 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
 // reached (dcf >= 0), on the sums it left in DW.dcs
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_finish(DevParams P, DemState<double> D, DemWork<double> DW) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int nd = P.nd;
     if (i >= nd) return;
@@ -1514,6 +1529,7 @@ __global__ void __launch_bounds__(128) k_dem_finish(DevParams P, DemState<double
 template <typename R>
 __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                       DemWork<double> DW, const int4* __restrict__ drows, int time_zero) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -1595,6 +1611,7 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, SphWork<R> W, R* pres,
                                                  const int4* __restrict__ rows,
                                                  int patch_up) {
+    grid_dep_wait();
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -1664,6 +1681,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P,
                                                                    float* pres, const int* __restrict__ gs,
                                                                    const int* __restrict__ ge,
                                                                    const int4* __restrict__ rows, int patch_up) {
+    grid_dep_wait();
     __shared__ float4 sa[NT_WARPS][NT_CH + 32];
     __shared__ float4 sb[NT_WARPS][NT_CH + 32];
     __shared__ int srow[NT_WARPS][20];
@@ -1809,6 +1827,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P,
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork<R> W) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -1872,6 +1891,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWork<R> W) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -2015,6 +2035,7 @@ __device__ void dem_wall_response(const DevParams& P, DemState<R>& D, DemWork<R>
 
 template <typename R>
 __global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, DemWork<R> DW) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.nd) return;
     int it = D.itype[i], pt = D.ptype[i];
@@ -2099,6 +2120,7 @@ __global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, 
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int4* __restrict__ rows) {
+    grid_dep_wait();
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
@@ -2182,6 +2204,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWork<R> W) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
     if (i >= n) return;
@@ -2233,7 +2256,8 @@ __global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWor
 }
 
 // end of a step: the host loop's count++ (ISPH_Calc_seperate.cuh:925)
-__global__ void k_tick(DevFlags* F) { F->step_count += 1; }
+__global__ void k_tick(DevFlags* F) {
+    grid_dep_wait(); F->step_count += 1; }
 
 // ---------------------------------------------------------------------------
 // printed maxima (kernel_copy_max_*, functions_OUTPUT.cuh:19-65 + cub max)
