@@ -1895,7 +1895,50 @@ __global__ void k_stage(int n, int nf, double* __restrict__ st, XTab t) {
         st[q] = ((t.dbl >> f) & 1u) ? ((const double*)t.p[f])[i] : (double)((const R*)t.p[f])[i] + t.off[f];
     }
 }
+
+// The same conversions reading / writing the caller's page-locked host
+// arrays directly (mapped, through their device addresses): one kernel per
+// transfer instead of a copy per field, at the link's bandwidth.
+struct HTab {
+    double* h[SPHDEM_BULK_MAX_FIELDS];
+};
+
+template <typename R>
+__global__ void k_unstage_mapped(int n, int nf, HTab src, XTab t) {
+    long long tot = (long long)n * nf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int f = (int)(q / n), i = (int)(q - (long long)f * n);
+        double v = src.h[f][i];
+        if ((t.dbl >> f) & 1u) ((double*)t.p[f])[i] = v;
+        else ((R*)t.p[f])[i] = (R)(v - t.off[f]);
+    }
+}
+
+template <typename R>
+__global__ void k_stage_mapped(int n, int nf, HTab dst, XTab t) {
+    long long tot = (long long)n * nf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int f = (int)(q / n), i = (int)(q - (long long)f * n);
+        dst.h[f][i] = ((t.dbl >> f) & 1u) ? ((const double*)t.p[f])[i] : (double)((const R*)t.p[f])[i] + t.off[f];
+    }
+}
 }  // namespace
+
+// device address of a page-locked, mapped host range (nullptr for pageable
+// memory, which then goes through cudaMemcpyAsync)
+static void* mapped_host(const void* p, size_t bytes) {
+    if (!p || bytes == 0) return nullptr;
+    cudaPointerAttributes a, b;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&b, (const char*)p + bytes - 1) !=
+                                                              cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+        return nullptr;
+    if ((const char*)b.devicePointer - (const char*)a.devicePointer != (ptrdiff_t)(bytes - 1)) return nullptr;
+    return a.devicePointer;
+}
 
 static int ensure_xfer(SphdemHandle* H, size_t elems) {
     if (elems <= H->xfer_elems) return SPHDEM_OK;
@@ -1949,10 +1992,23 @@ static int bulk_t(SphdemHandle* H, int which, int nf, const int32_t* fields, voi
     }
     if (n == 0 || nf == 0) return SPHDEM_OK;
     size_t need = (size_t)n * nf;
-    int r = ensure_xfer(H, need);
-    if (r) return r;
     cudaStream_t st = H->stream;
     int blocks = (int)std::min<long long>(((long long)need + 255) / 256, 148 * 8);
+    HTab hm;
+    bool mapped = true;
+    for (int k = 0; k < nf && mapped; k++) {
+        hm.h[k] = (double*)mapped_host(host[k], sizeof(double) * (size_t)n);
+        mapped = hm.h[k] != nullptr;
+    }
+    if (mapped) {
+        if (set) k_unstage_mapped<R><<<blocks, 256, 0, st>>>(n, nf, hm, t);
+        else k_stage_mapped<R><<<blocks, 256, 0, st>>>(n, nf, hm, t);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        return SPHDEM_OK;
+    }
+    int r = ensure_xfer(H, need);
+    if (r) return r;
     if (set) {
         for (int k = 0; k < nf; k++)
             CK(cudaMemcpyAsync(H->xfer + (size_t)k * n, host[k], sizeof(double) * n, cudaMemcpyHostToDevice, st));
@@ -2195,12 +2251,24 @@ static int history_t(SphdemHandle* H, int32_t* ids, double* sp, bool set) {
     int n = H->nd;
     if (n == 0) return SPHDEM_OK;
     size_t m = (size_t)n * SPHDEM_NSLOT;
+    cudaStream_t st = H->stream;
+    int blocks = (int)((m + 255) / 256);
+    // page-locked host arrays are read in place on the way in; on the way
+    // out the slot-major planes are gathered on the device first (the
+    // interleaved writes of a gather straight into host memory cross the
+    // link at a fraction of its bandwidth: 1.2 ms against 0.2 ms here)
+    int* mid = set ? (int*)mapped_host(ids, sizeof(int) * m) : nullptr;
+    double* msp = set ? (double*)mapped_host(sp, sizeof(double) * m * 3) : nullptr;
+    if (mid && msp) {
+        k_hist_in<<<blocks, 256, 0, st>>>(n, mid, msp, D.hid, D.hds);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        return SPHDEM_OK;
+    }
     int r = ensure_xfer(H, m * 3 + (m + 1) / 2);
     if (r) return r;
     double* dsp = H->xfer;
     int* dids = (int*)(H->xfer + m * 3);
-    cudaStream_t st = H->stream;
-    int blocks = (int)((m + 255) / 256);
     if (set) {
         CK(cudaMemcpyAsync(dids, ids, sizeof(int) * m, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(dsp, sp, sizeof(double) * m * 3, cudaMemcpyHostToDevice, st));

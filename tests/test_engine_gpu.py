@@ -325,6 +325,48 @@ def test_bulk_field_transfer(calm_bed, prec):
         e.set_fields(SPH, {"ftotalx": np.zeros(e.ns)})
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_bulk_transfer_pinned_equals_pageable(contact_bed, prec):
+    """Page-locked host arrays are read and written in place by the transfer
+    kernels (mapped memory); pageable arrays go through copies.  Both give
+    the same bits, for fields and for the contact history."""
+    import torch
+
+    p, sph, dem = contact_bed
+    e = _engine(p, sph, dem, prec)
+    e.step(3)
+
+    def pinned(shape, dt):
+        return torch.empty(int(np.prod(shape)), dtype=dt, pin_memory=True).numpy().reshape(shape)
+
+    for which, names in ((SPH, ["x", "uz", "m", "rho", "pres", "temp", "flt_s", "dDEMpor"]),
+                         (DEM, ["x", "uy", "wz", "temp", "Fdz_df", "Q_sd", "ftotalz"])):
+        n = e.nd if which == DEM else e.ns
+        a = {f: np.empty(n) for f in names}
+        b = {f: pinned((n,), torch.float64) for f in names}
+        e.get_fields(which, a)
+        e.get_fields(which, b)
+        for f in names:
+            assert np.array_equal(a[f], b[f]), f
+        settable = [f for f in names if f != "ftotalz"]
+        rng = np.random.default_rng(9)
+        for f in settable:
+            b[f][:] = b[f] * (1.0 + 1e-3 * rng.standard_normal(n))
+        e.set_fields(which, {f: b[f] for f in settable})
+        after_pinned = {f: e.get(which, f) for f in settable}
+        e.set_fields(which, {f: np.array(b[f]) for f in settable})
+        for f in settable:
+            assert np.array_equal(e.get(which, f), after_pinned[f]), f
+    ids, sp = e.history()
+    pid, psp = pinned((e.nd, 16), torch.int32), pinned((e.nd, 16, 3), torch.float64)
+    e.history(out=(pid, psp))
+    assert np.array_equal(ids, pid) and np.array_equal(sp, psp)
+    psp[:] = psp * 0.5
+    e.set_history(pid, psp)
+    got_ids, got_sp = e.history()
+    assert np.array_equal(got_ids, ids) and np.array_equal(got_sp, sp * 0.5)
+
+
 def test_history_roundtrip_keeps_the_run(contact_bed):
     """get_history -> set_history is the identity, and a run continued after
     a round trip of the whole state equals the uninterrupted run."""
