@@ -337,6 +337,11 @@ int sphdem_set_field(SphdemHandle* h, int which, int field,
  * host that owns the particle state (the copies SOPHIA_gpu makes around
  * its output, ISPH_Calc_seperate.cuh:928-968, for every field). */
 #define SPHDEM_BULK_MAX_FIELDS 32
+/* (sphdem_set_fields / sphdem_get_fields: page-locked host arrays, such as
+ * those of cudaHostAlloc, are read or written in place by the conversion
+ * kernel through their mapped device addresses; pageable arrays go through
+ * a device staging buffer.  Either way the call returns when the transfer
+ * is complete.) */
 int sphdem_set_fields(SphdemHandle* h, int which, int32_t nfields,
                       const int32_t* fields, const double* const* host_src);
 int sphdem_get_fields(SphdemHandle* h, int which, int32_t nfields,
