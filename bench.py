@@ -55,6 +55,8 @@ def parse():
                          "kernels (no timing); slabs: the bench bed cut into z slabs, one per rank (on one "
                          "GPU: --slabs slabs in one process), exchanging ghost bands every step")
     ap.add_argument("--slabs", type=int, default=2, help="slabs on one GPU for --workload slabs")
+    ap.add_argument("--slab-bed", default="bench", choices=["bench", "scaled"],
+                    help="--workload slabs: the bench bed cut along z, or the 10x wider scaled bed cut along x")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -1378,16 +1380,23 @@ def run_slabs(args, world, rank, local, pg):
     from fluidized_bed_master_b200.params import DEM, SPH
     from fluidized_bed_master_b200.slabs import DistExchange, LocalExchange, SlabBed, step_dist, step_local
 
+    from fluidized_bed_master_b200.beds import scaled_box_bed
+
     torch.cuda.set_device(local)
-    p, sph, dem = box_bed(seed=0, **WORKLOAD)
+    if args.slab_bed == "scaled":
+        p, sph, dem = scaled_box_bed(seed=0)
+        axis, text = 0, "scaled box bed 1.0x0.02x0.4 m: 2,000,000 fluid SPH + 200,000 DEM, cut along x"
+    else:
+        p, sph, dem = box_bed(seed=0, **WORKLOAD)
+        axis, text = 2, WORKLOAD_TEXT
     p.precision = 1 if args.precision == "fp64" else 0
     n_whole = len(sph["x"]) + len(dem["x"])
     if world > 1:
-        beds = [SlabBed(p, sph, dem, rank, world, axis=2)]
+        beds = [SlabBed(p, sph, dem, rank, world, axis=axis)]
         tr = DistExchange()
         run = lambda n: step_dist(beds[0], tr, n)
     else:
-        beds = [SlabBed(p, sph, dem, r, args.slabs, axis=2) for r in range(args.slabs)]
+        beds = [SlabBed(p, sph, dem, r, args.slabs, axis=axis) for r in range(args.slabs)]
         tr = LocalExchange(args.slabs)
         run = lambda n: step_local(beds, tr, n)
     run(args.warmup)
@@ -1405,15 +1414,15 @@ def run_slabs(args, world, rank, local, pg):
     act_all = reduce_over_ranks(pg, act, "sum", "cuda")
     slabs = [(b.lo, b.hi) for b in beds] if world == 1 else None
     line = {
-        "metric": "SPH-DEM particle-updates/s (3-D fluidized bed, ISPH-DEM step, z slabs)",
+        "metric": "SPH-DEM particle-updates/s (3-D fluidized bed, ISPH-DEM step, slabs)",
         "value": n_whole * args.steps / t_max, "unit": "particle-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64" if p.precision == 1 else "f32", "data": "synthetic (seeded box bed)",
-        "config": {"workload": WORKLOAD_TEXT, "n_sph": len(sph["x"]), "n_dem": len(dem["x"]),
+        "config": {"workload": text, "axis": "xyz"[axis], "n_sph": len(sph["x"]), "n_dem": len(dem["x"]),
                    "slabs": world if world > 1 else args.slabs, "ghost_layers": beds[0].ghost,
                    "layers": beds[0].n_layers, "slab_layers": slabs,
-                   "parallelism": f"z slabs x{world}" if world > 1 else f"{args.slabs} z slabs on 1 GPU"},
+                   "parallelism": f"slabs x{world}" if world > 1 else f"{args.slabs} slabs on 1 GPU"},
         "active_over_whole": act_all / n_whole,
         "how": "each step: every slab steps, then sends its particles in the neighbours' ghost bands, parks what "
                "left its layers and imports what its neighbours sent (host clock between device syncs)",
