@@ -302,7 +302,21 @@ __device__ __forceinline__ double rel_band(const DevParams& P, const RelFrame& F
 // with b from rel_band.  Pairs in the band, or with a position outside the
 // fixed-point range or not near the origin, take the reference predicate in
 // FP64.
+//
+// The fast path forms r^2 as |c|^2 - 2 p.c + |p|^2: a candidate is staged
+// with |c|^2, a lane holds -2p and compares |c|^2 - 2 p.c (three FMAs)
+// against its threshold minus |p|^2.  Against the difference form this adds
+// rounding of the magnitudes: |c|^2 (3 roundings), the three FMAs and |p|^2
+// (3 more) and the threshold's subtraction, in all at most
+// 6u (|c| + |p|)^2 + u hi^2 with u = 2^-24; both positions are near the
+// origin (|c|, |p| <= sqrt(3) L), so dot_band widens the band by
+// 80u (L / Rr)^2 + 2u of Rr^2.  Within the wider band the FP64 predicate
+// decides, so the lists are unchanged.
 constexpr int LT_WARPS = 4, LT_CH = 128;
+__device__ __forceinline__ double dot_band(const RelFrame& F, double Rr) {
+    const double u = 5.9604644775390625e-08, q = F.L / Rr;
+    return 80.0 * u * q * q + 2.0 * u;
+}
 __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P, SphState<float> S,
                                                                       SphRec<float> rec,
                                                                       const int* __restrict__ gs,
@@ -311,7 +325,8 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                                                                       int* __restrict__ nbr,
                                                                       int* __restrict__ ncnt, DevFlags* F) {
     grid_dep_wait();
-    __shared__ float4 sc[LT_WARPS][LT_CH + 4];
+    __shared__ float4 sc[LT_WARPS][LT_CH + 4];   // relative x, y, z and |c|^2
+    __shared__ int sj[LT_WARPS][LT_CH + 4];      // slot, bit 31: not near the origin
     __shared__ int srow[LT_WARPS][20];   // prefix[10] | start[9]
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * LT_WARPS + w;
@@ -329,13 +344,14 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
         const bool act = i < e0;
         double xi = 0, yi = 0, zi = 0, Rr = 0;
         float lo2 = 0, hi2 = 0, fx = 0, fy = 0, fz = 0;
+        float ax = 0, ay = 0, az = 0, tlo = 0, thi = 0;   // -2p and the thresholds of the fast path
         bool slow = true;
         if (act) {
             xi = S.x[i];
             yi = S.y[i];
             zi = S.z[i];
             Rr = __dmul_rn(P.kappa, S.h[i]);
-            const double b = rel_band(P, Fr, Rr), r2 = Rr * Rr;
+            const double b = rel_band(P, Fr, Rr), r2 = Rr * Rr, bd = b + dot_band(Fr, Rr);
             lo2 = (float)(r2 * (1.0 - b));
             hi2 = (float)(r2 * (1.0 + b));
             const int4 qi = ldr(rec.pos + i);
@@ -344,6 +360,12 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
             fx = f.x;
             fy = f.y;
             fz = f.z;
+            ax = -2.f * fx;
+            ay = -2.f * fy;
+            az = -2.f * fz;
+            const float pp = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
+            tlo = (float)(r2 * (1.0 - bd)) - pp;
+            thi = (float)(r2 * (1.0 + bd)) - pp;
         }
         int cnt = 0;
         int* pw = nbr ? nbr + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
@@ -379,11 +401,14 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                 const int tl = t + lane;
                 bool keep = false;
                 float4 v;
+                int jt = 0;
                 if (tl < tot) {
                     const int j = row_slot(srow[w], tl);
                     const int4 qj = ldr(rec.pos + j);
                     const bool oor = rel_slow(Fr, qj);
-                    v = rel_coord(Fr, qj, j | (oor ? (int)0x80000000 : 0));
+                    v = rel_coord(Fr, qj, 0);
+                    v.w = fmaf(v.z, v.z, fmaf(v.y, v.y, v.x * v.x));
+                    jt = j | (oor ? (int)0x80000000 : 0);
                     const float dx = fmaxf(fmaxf(blx - v.x, v.x - bhx), 0.f);
                     const float dy = fmaxf(fmaxf(bly - v.y, v.y - bhy), 0.f);
                     const float dz = fmaxf(fmaxf(blz - v.z, v.z - bhz), 0.f);
@@ -391,31 +416,36 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                     any_oor |= keep && oor;
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (keep) sc[w][tn + __popc(m & lt)] = v;
+                if (keep) {
+                    const int pos = tn + __popc(m & lt);
+                    sc[w][pos] = v;
+                    sj[w][pos] = jt;
+                }
                 tn += __popc(m);
                 t += 32;
             }
-            // padded to whole groups of four; the padding lies far outside every radius
+            // padded to whole groups of four; the padding (|c|^2 = inf) fails every test
             const int tp = (tn + 3) & ~3;
-            if (lane < tp - tn) sc[w][tn + lane] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(0));
+            if (lane < tp - tn) {
+                sc[w][tn + lane] = make_float4(0.f, 0.f, 0.f, __int_as_float(0x7f800000));
+                sj[w][tn + lane] = 0;
+            }
             const bool slow_chunk = lanes_slow || __any_sync(0xffffffffu, any_oor);
             __syncwarp();
             if (act && !slow_chunk) {
                 // fast path: FP32 prefilter, FP64 only inside the band
                 for (int u = 0; u < tp; u += 4) {
-                    float r2v[4];
-                    float4 cv[4];
+                    float tv[4];
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        cv[k] = sc[w][u + k];
-                        const float dx = fx - cv[k].x, dy = fy - cv[k].y, dz = fz - cv[k].z;
-                        r2v[k] = dx * dx + dy * dy + dz * dz;
+                        const float4 cv = sc[w][u + k];
+                        tv[k] = fmaf(az, cv.z, fmaf(ay, cv.y, fmaf(ax, cv.x, cv.w)));
                     }
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        if (r2v[k] <= hi2) {
-                            const int j = __float_as_int(cv[k].w);
-                            bool hit = r2v[k] < lo2;
+                        if (tv[k] <= thi) {
+                            const int j = sj[w][u + k];
+                            bool hit = tv[k] < tlo;
                             if (!hit) hit = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < Rr;
                             if (hit) {
                                 if (pw && cnt < cap) *pw = j;
@@ -431,7 +461,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                     const float4 cj = sc[w][u];
                     const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
                     const float r2 = dx * dx + dy * dy + dz * dz;
-                    const int jb = __float_as_int(cj.w);
+                    const int jb = sj[w][u];
                     const int j = jb & 0x7fffffff;
                     bool hit;
                     if (!slow && jb >= 0) {
