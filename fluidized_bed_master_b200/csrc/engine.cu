@@ -2216,11 +2216,14 @@ extern "C" int sphdem_get_neighbors(SphdemHandle* h, int32_t* counts, int32_t* d
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaMemcpy(counts, ncnt, sizeof(int) * ns, cudaMemcpyDeviceToHost));
     if (!dst || cap == 0) return SPHDEM_OK;
-    std::vector<int> colmajor((size_t)ncap * ns);
-    CK(cudaMemcpy(colmajor.data(), nbr, sizeof(int) * colmajor.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> dev((size_t)ncap * ns);
+    CK(cudaMemcpy(dev.data(), nbr, sizeof(int) * dev.size(), cudaMemcpyDeviceToHost));
+    // the 2-D WCSPH list is column-major, the ISPH-DEM list in blocks of 8
+    // entries per particle (nb_at)
     for (int i = 0; i < ns; i++) {
         int c = std::min(std::min(counts[i], cap), ncap);
-        for (int k = 0; k < c; k++) dst[(size_t)i * cap + k] = colmajor[(size_t)k * ns + i];
+        for (int k = 0; k < c; k++)
+            dst[(size_t)i * cap + k] = h->kind == 1 ? dev[(size_t)k * ns + i] : dev[nb_at(k, ns, i)];
     }
     return SPHDEM_OK;
 }

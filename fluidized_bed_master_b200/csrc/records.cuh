@@ -379,26 +379,43 @@ struct NbQ24 {
     V4<R> b;
 };
 
+// ---- the SPH neighbour list ---------------------------------------------
+// Blocks of 8 entries per particle: entry k of particle i at
+// ((k / 8) n + i) 8 + k % 8.  A particle's 8 consecutive entries fill one
+// 32-byte sector: the list build's stores of one particle land in the same
+// sector (written back whole from L2) and a walk loads B entries in one
+// vector load, while the particles of a warp (consecutive i) still read
+// consecutive sectors.
+__host__ __device__ __forceinline__ size_t nb_at(int k, int n, int i) {
+    return ((size_t)(k >> 3) * n + i) * 8 + (k & 7);
+}
+
 // ---- batched neighbour-list walk -------------------------------------------
 // The list passes are bound by the latency of the dependent loads (list
 // entry -> neighbour records).  Loading the records of B neighbours before
 // any of their arithmetic keeps B independent load chains in flight; the
-// sums still run in list order.
+// sums still run in list order.  B = 2 or 4 entries come in one vector load.
 template <int B, typename T, typename L, typename C>
 __device__ __forceinline__ void nb_walk(int cnt, const int* __restrict__ nb, int n, int i, L load, C comp) {
+    static_assert(B == 2 || B == 4, "list walks load 2 or 4 entries at a time");
     int k = 0;
     for (; k + B <= cnt; k += B) {
         int j[B];
         T r[B];
-#pragma unroll
-        for (int u = 0; u < B; u++) j[u] = __ldg(nb + (size_t)(k + u) * n + i);
+        if constexpr (B == 4) {
+            const int4 v = __ldg(reinterpret_cast<const int4*>(nb + nb_at(k, n, i)));
+            j[0] = v.x; j[1] = v.y; j[2] = v.z; j[3] = v.w;
+        } else {
+            const int2 v = __ldg(reinterpret_cast<const int2*>(nb + nb_at(k, n, i)));
+            j[0] = v.x; j[1] = v.y;
+        }
 #pragma unroll
         for (int u = 0; u < B; u++) r[u] = load(j[u]);
 #pragma unroll
         for (int u = 0; u < B; u++) comp(j[u], r[u]);
     }
     for (; k < cnt; k++) {
-        int j = __ldg(nb + (size_t)k * n + i);
+        int j = __ldg(nb + nb_at(k, n, i));
         T r = load(j);
         comp(j, r);
     }

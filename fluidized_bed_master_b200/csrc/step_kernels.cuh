@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(128) k_build_list(DevParams P, SphState<R> S, 
             Disp<R> d;
             R r2;
             if (test_pair(P, qi, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, 1e-20, bd, d, r2)) {
-                if (nbr && c < cap) nbr[(size_t)c * n + i] = j;
+                if (nbr && c < cap) nbr[nb_at(c, n, i)] = j;
                 c++;
             }
         }
@@ -368,7 +368,15 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
             thi = (float)(r2 * (1.0 + bd)) - pp;
         }
         int cnt = 0;
-        int* pw = nbr ? nbr + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
+        // entry cnt of particle i at pw: +1 inside a block of 8 entries, to
+        // the particle's next block (8n further) after the eighth
+        int* pw = nbr ? nbr + nb_at(0, n, i) : nullptr;
+        const ptrdiff_t next_block = 8 * (ptrdiff_t)n - 7;
+        auto push = [&](int j) {
+            if (pw && cnt < cap) *pw = j;
+            pw += ((cnt & 7) == 7) ? next_block : 1;
+            cnt++;
+        };
         const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
         // Candidates that no lane of this group can reach are not staged: the
         // lanes' box [bl, bh] and their largest prefilter radius hb.  The box
@@ -447,11 +455,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                             const int j = sj[w][u + k];
                             bool hit = tv[k] < tlo;
                             if (!hit) hit = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < Rr;
-                            if (hit) {
-                                if (pw && cnt < cap) *pw = j;
-                                pw += n;
-                                cnt++;
-                            }
+                            if (hit) push(j);
                         }
                     }
                 }
@@ -471,11 +475,7 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                     } else {
                         hit = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < Rr;
                     }
-                    if (hit) {
-                        if (pw && cnt < cap) *pw = j;
-                        pw += n;
-                        cnt++;
-                    }
+                    if (hit) push(j);
                 }
             }
             __syncwarp();
