@@ -301,6 +301,18 @@ __device__ __forceinline__ Knl<R> knl_make(const DevParams& P, R th) {
     k.th = th;
     return k;
 }
+// The other kernel types (Gaussian, cubic/quintic splines, Wendland C4) are
+// called out of line: inlined into every neighbour loop, their exp/pow
+// code held registers and kept the loops from being scheduled well even
+// when the Wendland branches run.
+template <typename R>
+__device__ __noinline__ R knl_w_call(int kt, R tA, R tH, R rr) {
+    return knl_w<R>(kt, tA, tH, rr);
+}
+template <typename R>
+__device__ __noinline__ R knl_dw_call(int kt, R tA, R tH, R rr) {
+    return knl_dw<R>(kt, tA, tH, rr);
+}
 template <typename R>
 __device__ __forceinline__ R kw(const Knl<R>& k, R rr) {
     if (k.kt == 3) {
@@ -315,7 +327,7 @@ __device__ __forceinline__ R kw(const Knl<R>& k, R rr) {
         R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
         return k.tA * a4 * a4 * ((R)1 + (R)8 * q + (R)25 * q * q + (R)32 * q * q * q);
     }
-    return knl_w<R>(k.kt, k.tA, k.th, rr);
+    return knl_w_call<R>(k.kt, k.tA, k.th, rr);
 }
 template <typename R>
 __device__ __forceinline__ R kdw(const Knl<R>& k, R rr) {
@@ -331,7 +343,7 @@ __device__ __forceinline__ R kdw(const Knl<R>& k, R rr) {
         R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
         return ((R)0.5 * k.ih) * k.tA * ((R)-22 * q * a4 * a2 * a * ((R)16 * q * q + (R)7 * q + (R)1));
     }
-    return knl_dw<R>(k.kt, k.tA, k.th, rr);
+    return knl_dw_call<R>(k.kt, k.tA, k.th, rr);
 }
 
 // ---- gradient correction with the matrix held in registers --------------

@@ -1707,7 +1707,7 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
 // reference predicate inside the band.  Same sums as k_neumann in candidate
 // order per wall, so the FP32 results differ from it by rounding only.
 constexpr int NT_WARPS = 4, NT_CH = 128;
-__global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
+__global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
                                                                    float* pres, const int* __restrict__ gs,
                                                                    const int* __restrict__ ge,
                                                                    const int4* __restrict__ rows, int patch_up) {
@@ -1759,6 +1759,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P,
         }
         const bool lanes_slow = __any_sync(0xffffffffu, act && slow);
         float tp = 0.f, flt = 0.f, tt = 0.f, tr = 0.f;
+        float scale = 1.f;   // the sums times scale are the normalised sums
         int t = 0;   // next raw candidate
         while (t < tot) {
             // stage fluid candidates in order until the chunk is full
@@ -1790,7 +1791,62 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P,
             }
             const bool slow_chunk = lanes_slow || __any_sync(0xffffffffu, any_oor);
             __syncwarp();
-            if (act) {
+            if (act && !slow_chunk && K.kt == 3) {
+                // every candidate on the FP32 frame: the kernel is evaluated
+                // for all of them and the pairs outside the radius add
+                // nothing, so the lanes do not diverge (only a pair in the
+                // rounding band takes the FP64 predicate).  Wendland C2 in
+                // line without its normalisation tA, which cancels in the
+                // ratios below (only the empty-support test scales by it).
+                const float hq = 0.5f * K.ih;
+#pragma unroll 4
+                for (int u = 0; u < ns; u++) {
+                    const float4 cj = sa[w][u];
+                    const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    bool in = r2 < lo2;
+                    if (!in && r2 <= hi2) {
+                        const int j = __float_as_int(cj.w);
+                        in = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < R2;
+                    }
+                    const float q = r2 * rsqrtf(fmaxf(r2, 1e-30f)) * hq;
+                    const float a = 1.f - q, a2 = a * a;
+                    const float wk = a2 * a2 * (1.f + 4.f * q);
+                    const float4 bj = sb[w][u];
+                    if (in && q < 1.f) {
+                        const float mr = bj.x * wk;
+                        tp += mr * bj.y;
+                        flt += mr;
+                        tt += mr * bj.z;
+                        tr += bj.w * wk;
+                    }
+                }
+                scale = K.tA;
+            } else if (act && !slow_chunk) {
+                // as above, any kernel
+#pragma unroll 2
+                for (int u = 0; u < ns; u++) {
+                    const float4 cj = sa[w][u];
+                    const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    bool in = r2 < lo2;
+                    if (!in && r2 <= hi2) {
+                        const int j = __float_as_int(cj.w);
+                        in = __dadd_rn(pair_dist(xi, yi, zi, S.x[j], S.y[j], S.z[j]), 1e-20) < R2;
+                    }
+                    float r, rinv;
+                    rdist(r2, r, rinv);
+                    const float wk = kw(K, r);
+                    const float4 bj = sb[w][u];
+                    if (in) {
+                        const float mr = bj.x * wk;
+                        tp += mr * bj.y;
+                        flt += mr;
+                        tt += mr * bj.z;
+                        tr += bj.w * wk;
+                    }
+                }
+            } else if (act) {
                 for (int u = 0; u < ns; u++) {
                     const float4 cj = sa[w][u];
                     const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
@@ -1835,7 +1891,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 9) k_neumann_tiled(DevParams P,
         }
         if (!act) continue;
         float pw, rw;
-        if (flt < 1e-6f) {
+        if (flt * scale < 1e-6f) {
             rw = W.rho_ref[i];
             pw = 0.f;
         } else {
@@ -2233,7 +2289,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
 // into u_tmp/temp_tmp; the next reorder reads them.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_xsph(DevParams P, SphState<R> S, SphWork<R> W) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 1) k_xsph(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = P.ns;
