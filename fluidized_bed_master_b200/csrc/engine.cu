@@ -542,6 +542,9 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     int ns = P.ns, nd = P.nd;
     int so = E.cur_s, sn = 1 - E.cur_s, dox = E.cur_d, dn = 1 - E.cur_d;
     int r;
+    // Wendland C2 (the default): the neighbour passes are instantiated with
+    // the kernel type fixed
+    const bool kt3 = P.kernel_type == 3;
     const bool fork = H->concurrent && ns > 0 && nd > 0 && H->dem_stream;
     cudaStream_t sd = fork ? H->dem_stream : st;
     // event k recorded on stream a / waited for on stream b (fork only)
@@ -582,16 +585,16 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             }
         }
         CK(wait(1, st));
-        { KTIME(KT_PASSA); CK((launch_pdl(k_passA<R>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
+        { KTIME(KT_PASSA); CK((launch_pdl(kt3 ? k_passA<R, 3> : k_passA<R, -1>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
         *nl += 2;
         {
             KTIME(KT_PASSB);
             if (P.sps) {
-                CK((launch_pdl(k_sps<R>, bs, TPB, 0, st, P, S, W)));
+                CK((launch_pdl(kt3 ? k_sps<R, 3> : k_sps<R, -1>, bs, TPB, 0, st, P, S, W)));
                 *nl += 1;
             }
-            if (P.iface | P.fb | P.sps | P.ipf) CK((launch_pdl(k_passB<R, true>, bs, TPB, 0, st, P, S, W, E.flags)));
-            else CK((launch_pdl(k_passB<R, false>, bs, TPB, 0, st, P, S, W, E.flags)));
+            if (P.iface | P.fb | P.sps | P.ipf) CK((launch_pdl(kt3 ? k_passB<R, true, 3> : k_passB<R, true, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
+            else CK((launch_pdl(kt3 ? k_passB<R, false, 3> : k_passB<R, false, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
         }
         *nl += 1;
     }
@@ -601,14 +604,14 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if (nd > 0) {
         {
             KTIME(KT_DEMCOUPLING);
-            CK((launch_pdl(k_dem_coupling<R>, bdw, TPB, 0, st, P, S, W, D, DW, W.rows)));
+            CK((launch_pdl(kt3 ? k_dem_coupling<R, 3> : k_dem_coupling<R, -1>, bdw, TPB, 0, st, P, S, W, D, DW, W.rows)));
             CK((launch_pdl(k_dem_finish<R>, bd, TPB, 0, st, P, D, DW)));
         }
         *nl += 2;
     }
     if (ns > 0) {
         KTIME(KT_SPHCOUPLING);
-        CK((launch_pdl(k_sph_coupling<R>, bs, TPB, 0, st, P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0)));
+        CK((launch_pdl(kt3 ? k_sph_coupling<R, 3> : k_sph_coupling<R, -1>, bs, TPB, 0, st, P, S, W, D, DW, DW.rows, (flags & F_TIME0) ? 1 : 0)));
         *nl += 1;
     }
     CK(rec(4, st));   // the SPH coupling has read the DEM set
@@ -640,16 +643,16 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             else
                 CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, W.p_new, W.rows, 0)));
         }
-        { KTIME(KT_PASSC); CK((launch_pdl(k_passC<R>, bs, TPB, 0, st, P, S, W))); }
+        { KTIME(KT_PASSC); CK((launch_pdl(kt3 ? k_passC<R, 3> : k_passC<R, -1>, bs, TPB, 0, st, P, S, W))); }
         *nl += 3;
         if (P.open_bc > 0) {
             KTIME(KT_OPENBC);
-            CK((launch_pdl(k_open_bc<R>, bbw, TPB, 0, st, P, S, W, W.rows)));
+            CK((launch_pdl(kt3 ? k_open_bc<R, 3> : k_open_bc<R, -1>, bbw, TPB, 0, st, P, S, W, W.rows)));
             *nl += 1;
         }
         if (P.xsph) {
             KTIME(KT_XSPH);
-            CK((launch_pdl(k_xsph<R>, bs, TPB, 0, st, P, S, W)));
+            CK((launch_pdl(kt3 ? k_xsph<R, 3> : k_xsph<R, -1>, bs, TPB, 0, st, P, S, W)));
             *nl += 1;
         }
     }

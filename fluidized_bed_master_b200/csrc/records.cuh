@@ -287,14 +287,17 @@ __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 
 // ---- smoothing kernel with per-particle constants -----------------------
 // W and dW/dr of functions_KNL.cuh:2-144 with 1/h precomputed.
-template <typename R>
+// KT is the kernel type when the kernel instantiation fixes it (3: Wendland
+// C2, the loops then carry no type test), -1 when it is read from kt.
+template <typename R, int KT = -1>
 struct Knl {
+    static_assert(KT == -1 || KT == 3, "kernel types fixed at compile time: Wendland C2");
     int kt;
     R tA, ih, th;   // normalisation, 1/h, h
 };
-template <typename R>
-__device__ __forceinline__ Knl<R> knl_make(const DevParams& P, R th) {
-    Knl<R> k;
+template <typename R, int KT = -1>
+__device__ __forceinline__ Knl<R, KT> knl_make(const DevParams& P, R th) {
+    Knl<R, KT> k;
     k.kt = P.kernel_type;
     k.tA = knl_tmpA<R>(P.kernel_type, P.dim, th);
     k.ih = rcp(th);
@@ -313,37 +316,43 @@ template <typename R>
 __device__ __noinline__ R knl_dw_call(int kt, R tA, R tH, R rr) {
     return knl_dw<R>(kt, tA, tH, rr);
 }
-template <typename R>
-__device__ __forceinline__ R kw(const Knl<R>& k, R rr) {
-    if (k.kt == 3) {
+template <typename R, int KT>
+__device__ __forceinline__ R kw(const Knl<R, KT>& k, R rr) {
+    if (KT == 3 || k.kt == 3) {
         R q = rr * k.ih * (R)0.5;
         if (!(q < (R)1)) return (R)0;
         R a = (R)1 - q, a2 = a * a;
         return k.tA * a2 * a2 * ((R)1 + (R)4 * q);
     }
-    if (k.kt == 5) {
-        R q = rr * k.ih * (R)0.5;
-        if (!(q < (R)1)) return (R)0;
-        R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
-        return k.tA * a4 * a4 * ((R)1 + (R)8 * q + (R)25 * q * q + (R)32 * q * q * q);
+    if constexpr (KT == -1) {
+        if (k.kt == 5) {
+            R q = rr * k.ih * (R)0.5;
+            if (!(q < (R)1)) return (R)0;
+            R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
+            return k.tA * a4 * a4 * ((R)1 + (R)8 * q + (R)25 * q * q + (R)32 * q * q * q);
+        }
+        return knl_w_call<R>(k.kt, k.tA, k.th, rr);
     }
-    return knl_w_call<R>(k.kt, k.tA, k.th, rr);
+    return (R)0;
 }
-template <typename R>
-__device__ __forceinline__ R kdw(const Knl<R>& k, R rr) {
-    if (k.kt == 3) {
+template <typename R, int KT>
+__device__ __forceinline__ R kdw(const Knl<R, KT>& k, R rr) {
+    if (KT == 3 || k.kt == 3) {
         R q = rr * k.ih * (R)0.5;
         if (!(q < (R)1)) return (R)0;
         R a = (R)1 - q;
         return ((R)0.5 * k.ih) * k.tA * ((R)-20 * q * a * a * a);
     }
-    if (k.kt == 5) {
-        R q = rr * k.ih * (R)0.5;
-        if (!(q < (R)1)) return (R)0;
-        R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
-        return ((R)0.5 * k.ih) * k.tA * ((R)-22 * q * a4 * a2 * a * ((R)16 * q * q + (R)7 * q + (R)1));
+    if constexpr (KT == -1) {
+        if (k.kt == 5) {
+            R q = rr * k.ih * (R)0.5;
+            if (!(q < (R)1)) return (R)0;
+            R a = (R)1 - q, a2 = a * a, a4 = a2 * a2;
+            return ((R)0.5 * k.ih) * k.tA * ((R)-22 * q * a4 * a2 * a * ((R)16 * q * q + (R)7 * q + (R)1));
+        }
+        return knl_dw_call<R>(k.kt, k.tA, k.th, rr);
     }
-    return knl_dw_call<R>(k.kt, k.tA, k.th, rr);
+    return (R)0;
 }
 
 // ---- gradient correction with the matrix held in registers --------------

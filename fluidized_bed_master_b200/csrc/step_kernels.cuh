@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
 // Neighbours read the start-of-step m, rho; the new m, rho go to m_new,
 // rho_new so that no thread sees a half-updated neighbour.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                const int4* __restrict__ drows) {
     grid_dep_wait();
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
     W.dDEMpor_prev[i] = dprev;
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
     R th = (R)hi;
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     PosRec<R> qi = ldr(rec.pos + i);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R txx = 0, tyy = 0, tzz = 0, txy = 0, tyz = 0, tzx = 0, sflt = 0;
@@ -848,7 +848,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
 // reads vis_t of both particles of a pair, so this runs as its own pass
 // just before it.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -860,7 +860,7 @@ __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork
     }
     const SphRec<R> rec = W.rec;
     R th = (R)S.h[i];
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     PosRec<R> qi = ldr(rec.pos + i);
     V4<R> upi = rec.up[i];
     V4<R> fi = rec.f1[i];
@@ -900,7 +900,7 @@ __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork
 // FORCES: one of the interface-sharpness force, the repulsive boundary
 // force, the SPS eddy viscosity or the inter-particle surface tension is on
 // (a separate instantiation, so that the default pass keeps its registers)
-template <typename R, bool FORCES>
+template <typename R, bool FORCES, int KT>
 __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -917,7 +917,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     bool adv = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
     if (!filt && !adv) return;
     R th = (R)S.h[i];
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     PosRec<R> qi = ldr(rec.pos + i);
     V4<R> upi = rec.up[i];
     V4<R> fi = rec.f1[i];
@@ -1317,8 +1317,8 @@ struct DcSums {
 // one SPH neighbour j of sphere i at distance r (the pair already passed the
 // kappa h_i test): Shepard sums of fluid/air velocity, temperature and
 // porosity, and the pressure-gradient force
-template <typename R>
-__device__ __forceinline__ void dc_pair(const SphWork<R>& W, const Knl<R>& K, R ff, R fa, R pgc, int j, int ptj, R r,
+template <typename R, int KT>
+__device__ __forceinline__ void dc_pair(const SphWork<R>& W, const Knl<R, KT>& K, R ff, R fa, R pgc, int j, int ptj, R r,
                                         DcSums<R>& a) {
     const V4<R> fj = ldr(W.rec.f1 + j);
     const R porj = fj.w;
@@ -1465,7 +1465,7 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<double>& D, Dem
     if (P.con && pt > 0) DW.temp0[i] = D.temp[i];
 }
 
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                       DemWork<double> DW, const int4* __restrict__ srows) {
     grid_dep_wait();
@@ -1487,7 +1487,7 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         R mi = D.m[i];
         R fa = DW.flt_s[i], ff = DW.flt_sd[i];
         R th = (R)hi;
-        Knl<R> K = knl_make<R>(P, th);
+        Knl<R, KT> K = knl_make<R, KT>(P, th);
         double Rr = P.kappa * hi;
         Band bd = make_band(P, Rr);
         PosRec<R> qp = make_pos<R>(P, xi, yi, zi, 0, 0, 0);
@@ -1556,7 +1556,7 @@ __global__ void __launch_bounds__(128) k_dem_finish(DevParams P, DemState<double
 // KERNEL_SPH_coupling3D_sph (functions_SPH_DEM_COUPLING2.cuh:1815-2019) +
 // KERNEL_clc_projection_sph (functions_TIME_ISPH2.cuh:104-204).
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                       DemWork<double> DW, const int4* __restrict__ drows, int time_zero) {
     grid_dep_wait();
@@ -1573,7 +1573,7 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
         // swapped (functions_SPH_DEM_COUPLING2.cuh:1860)
         R cpi = (abs((int)(tempi + (R)P.t_ref)) > 1000) ? (R)P.cp_dem : (R)P.cp_sph;   // stored T - t_ref
         R th = (R)hi;
-        Knl<R> K = knl_make<R>(P, th);
+        Knl<R, KT> K = knl_make<R, KT>(P, th);
         double Rr = P.kappa * hi;
         R tx = 0, ty = 0, tz = 0, tt = 0;
         if (P.nd > 0 && (pt == 1 || pt == 3)) {
@@ -1975,7 +1975,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
 // pass C: KERNEL_pressureforce3D_sph (functions_PPE2.cuh:2154-2335) and
 // KERNEL_time_update_projection_sph (functions_TIME_ISPH2.cuh:467-620).
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1992,7 +1992,7 @@ __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWo
     bool pf = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
     if (pf && P.fp) {
         R th = (R)S.h[i];
-        Knl<R> K = knl_make<R>(P, th);
+        Knl<R, KT> K = knl_make<R, KT>(P, th);
         PosRec<R> qi = ldr(rec.pos + i);
         R pi = W.p_new[i], rhoi = W.rho_new[i], pori = rec.f1[i].w;
         R cpi = -pori * rcp(rhoi);
@@ -2204,7 +2204,7 @@ __global__ void __launch_bounds__(128) k_dem_update(DevParams P, DemState<R> D, 
 // around their mirror point.  Only non-buffer fluid is read, so the update
 // is done in place.  One warp per buffer particle (W.buf_idx).
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, SphWork<R> W, const int4* __restrict__ rows) {
     grid_dep_wait();
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -2218,7 +2218,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     if (bt == 1) zg = 2 * P.L2 - zi;
     else if (bt == 2) zg = 2 * P.L3 - zi;
     R th = (R)hi;
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     double Rr = P.kappa * hi;
     const Band bd = make_band(P, Rr);
     const PosRec<R> qp = make_pos<R>(P, xi, yi, zg, 0, 0, 0);   // the mirror point
@@ -2288,7 +2288,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
 // Writes the smoothed velocity/temperature of every particle (or a copy)
 // into u_tmp/temp_tmp; the next reorder reads them.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 1) k_xsph(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2303,7 +2303,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 1) k_xsph(DevParams 
         return;
     }
     R th = (R)S.h[i];
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     PosRec<R> qi = ldr(rec.pos + i);
     R c = (R)P.c_xsph;
     int cnt = min(W.ncnt[i], P.nb_cap);
