@@ -47,10 +47,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="bed",
-                    choices=["bed", "dam2d", "dam2d-batch", "ppe-profile", "column", "mlp", "slabs"],
+                    choices=["bed", "dam2d", "dam2d-batch", "bed2d-batch", "ppe-profile", "column", "mlp", "slabs"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
                          "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
-                         "against the same beds run one after another; ppe-profile: --steps steps of the bed with the "
+                         "against the same beds run one after another; bed2d-batch: 64 uneven 2-D ISPH-DEM beds "
+                         "(per-bed inlet velocities) in one handle, against the same beds one after another; "
+                         "ppe-profile: --steps steps of the bed with the "
                          "projected-start PCG and step graphs off, so that a kernel profiler sees the PPE "
                          "kernels (no timing); slabs: the bench bed cut into z slabs, one per rank (on one "
                          "GPU: --slabs slabs in one process), exchanging ghost bands every step")
@@ -808,6 +810,134 @@ def run_dam2d_batch(args, world, rank, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def run_bed2d_batch(args, world, rank, local, pg):
+    """64 two-dimensional ISPH-DEM beds of uneven size (fluid counts
+    log-uniform in [2k, 50k], seeded; spheres 10 %; inlet velocities
+    U(0.1, 0.3)) in one handle, each in its own plane with its own
+    open-boundary row, one step graph for all; against the same beds
+    stepped one after another, each in its own handle."""
+    import torch
+
+    from fluidized_bed_master_b200.beds import bed2d_batch
+    from fluidized_bed_master_b200.engine import Engine
+    from fluidized_bed_master_b200.params import DEM, SPH
+
+    metric = "2-D ISPH-DEM particle-updates/s on 1 B200 (64 uneven beds in one handle)"
+    unit = "particle-updates/s"
+    text = ("64 independent 2-D ISPH-DEM beds (box_bed_2d: 0.1 m wide, dx=1.25 mm, Wendland C2, h=1.3 dx, "
+            "water-like fluid, spheres d=2 mm +-5 % at 2500 kg/m3, Hertz-Mindlin E=1e7, heat transfer, XSPH, "
+            "inlet/outlet slabs) in one handle, fluid counts log-uniform in [2,000, 50,000] (seeded), spheres "
+            "10 % of the fluid count, inlet velocity U(0.1, 0.3) m/s per bed (sphdem_set_beds)")
+    p, sph, dem, rows, parts = bed2d_batch(seed=rank)
+    n_sph, n_dem = len(sph["x"]), len(dem["x"])
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import Oracle
+        threads = os.cpu_count() or 1
+        sel = sorted(parts, key=lambda pt: len(pt[0]["x"]))[:2]
+        npart = sum(len(s["x"]) + len(d["x"]) for s, d, _ in sel)
+        orcs = [Oracle(p, s, d, threads=threads, beds=r) for s, d, r in sel]
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < max(5.0, args.cpu_seconds) and k < 2000:
+            for o in orcs:
+                o.step(2)
+            k += 2
+        el = time.perf_counter() - t0
+        val = npart * k / el
+        line = {"metric": metric, "impl": "reference", "value": val, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 2-D beds)",
+                "config": {"workload": text},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": f"the 2 smallest beds ({npart} particles), {k} steps each"},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local)
+    q = p.copy()
+    q.precision = 1 if args.precision == "fp64" else 0
+    eng = Engine(q, sph, dem, beds=rows)
+    n = eng.ns + eng.nd
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
+    sampler = ClockSampler(int(vis) if vis.isdigit() else local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches = 0
+    t_batch = 0.0
+    for _ in range(args.steps):
+        t_batch += _timed_steps(eng, stream, flush, 1)
+        launches += eng.launches()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    t_max = reduce_over_ranks(pg, t_batch, "max", "cuda")
+    n_all = reduce_over_ranks(pg, n, "sum", "cuda")
+    value = n_all * args.steps / (t_max / 1e3)
+    finite = bool(np.all(np.isfinite(eng.get(SPH, "pres"))) and np.all(np.isfinite(eng.get(DEM, "uz"))))
+    e2e = None
+    if not args.no_e2e:
+        def pinned(k, dt):
+            return torch.empty(k, dtype=dt, pin_memory=True).numpy()
+        hs = {f: pinned(eng.ns, torch.float64) for f in ["x", "y", "z"] + SPH_STATE}
+        hd = {f: pinned(eng.nd, torch.float64) for f in DEM_STATE}
+        for f in hs:
+            hs[f][:] = eng.get(SPH, f)
+        for f in hd:
+            hd[f][:] = eng.get(DEM, f)
+        hb = sum(a.nbytes for a in hs.values()) + sum(a.nbytes for a in hd.values())
+        ke = max(3, min(args.steps, 30))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            eng.set_fields(SPH, hs)
+            eng.set_fields(DEM, hd)
+            eng.step(1)
+            eng.get_fields(SPH, hs)
+            eng.get_fields(DEM, hd)
+        torch.cuda.synchronize()
+        te = reduce_over_ranks(pg, time.perf_counter() - t0, "max", "cuda")
+        e2e = {"value": n_all * ke / te, "unit": unit, "h2d_bytes_per_step": hb, "d2h_bytes_per_step": hb,
+               "ms_per_step": te / ke * 1e3,
+               "how": "per step: sphdem_set_fields of every bed's SPH and DEM state from pinned host arrays, "
+                      "sphdem_step, sphdem_get_fields back"}
+    eng.close()
+    # the same beds one after another, each in its own handle
+    seq_ms, ks = 0.0, 5
+    if rank == 0:
+        for sb, db, rb in parts:
+            e = Engine(q, sb, db, beds=rb)
+            st = torch.cuda.ExternalStream(e.stream_ptr())
+            e.step(3)
+            seq_ms += _timed_steps(e, st, flush, ks) / ks
+            e.close()
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if q.precision == 0 else "f64", "data": "synthetic (seeded 2-D beds)",
+        "config": {"workload": text, "n_sph": n_sph, "n_dem": n_dem, "beds": len(parts),
+                   "fluid_counts": [int(np.sum((s["p_type"] == 1) & (s["z"] >= 0))) for s, _, _ in parts],
+                   "inlet_uz": [round(r["inlet_uz"], 4) for r in rows],
+                   "l2": "256 MB buffer written before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "state_finite": finite,
+        "sequential": {"ms_per_step": seq_ms, "how": f"each bed alone in its own handle, {ks} timed steps each "
+                       "after 3 warm-up steps, per-step device times summed over the beds",
+                       "value": n * 1e3 / seq_ms if seq_ms else None, "unit": unit},
+        "batch_speedup_vs_sequential": (seq_ms / (t_max / args.steps)) if seq_ms else None,
+        "roofline": None, "cpu_baseline": None, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_dam2d(args, world, rank, local, pg):
     import torch
 
@@ -1439,6 +1569,8 @@ def main():
             run_dam2d(args, world, rank, local, pg)
         elif args.workload == "dam2d-batch":
             run_dam2d_batch(args, world, rank, local, pg)
+        elif args.workload == "bed2d-batch":
+            run_bed2d_batch(args, world, rank, local, pg)
         elif args.workload == "column":
             run_column(args, world, rank, local, pg)
         elif args.workload == "mlp":

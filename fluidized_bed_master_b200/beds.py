@@ -16,6 +16,9 @@ run uses one of these generators.  Two families:
   bottom, heat transfer on.
 * ``isph_column`` -- a 3-D water column with no DEM in a wall box: the
   plain ISPH projection with the PPE solved to 1e-6.
+* ``box_bed_2d`` / ``bed2d_batch`` -- the box bed in two dimensions (a bed
+  in a plane y = const), and many such beds of uneven size, each in its own
+  plane with its own inlet velocity, for one handle.
 
 Lattice positions get seeded uniform jitter of +/-0.01 dx so that no pair
 sits exactly on a kernel-support boundary.
@@ -179,6 +182,75 @@ def box_bed(n_fluid=200_000, n_dem=20_000, dx=1.25e-3, seed=0, u_in=0.15, t_flui
     dem = _dem_arrays(dpos, rad, 2500.0, h, t_dem)
     p.box_c[:] = [0.5 * lx, 0.5 * ly, 0.5 * lz]
     p.box_L[:] = [lx, ly, lz]
+    return p, sph, dem
+
+
+def box_bed_2d(n_fluid=25_600, n_dem=None, dx=1.25e-3, seed=0, u_in=0.15, t_fluid=300.0, t_dem=350.0,
+               lx=0.1, d_dem=2.0e-3, y0=0.0):
+    """The benchmark bed in two dimensions: a bed of width lx in the x-z
+    plane y = y0 (the engine's dim-2 ISPH-DEM model), with the materials,
+    kernel, inlet and walls of box_bed.  n_fluid particles fill rows of
+    lx / dx columns from z = 0 up (the height follows from the count);
+    three inlet rows below z = 0 enter at u_in; three wall columns on each
+    side reach from the inlet bottom to the fluid top; the outlet slab is
+    the top three fluid rows.  n_dem spheres (default 10 % of n_fluid),
+    diameter d_dem +- 5 %, density 2500, centres on randomly chosen sites of
+    a hexagonal lattice of spacing 2.1 mm that covers the bed below the
+    outlet slab, so no two overlap.  At 10 % of the fluid count the discs
+    cover about a fifth of the bed's area (the 3-D bed's spheres about 40 %
+    of its lower volume): in two dimensions a sphere of d = 2 mm holds about
+    two thirds of a kernel's area at h = 1.625 mm, and a denser packing
+    drives the porosity-rate source of the pressure equation past what the
+    reference's one-sweep pressure step holds.  Returns (params, sph, dem)."""
+    rng = np.random.default_rng(seed)
+    p, _, _ = box_bed(n_fluid=1000, n_dem=1, dx=dx, seed=seed, u_in=u_in, t_fluid=t_fluid, t_dem=t_dem)
+    p.dim = 2
+    h = 1.3 * dx
+    nx = int(round(lx / dx))
+    nz = n_fluid // nx + (1 if n_fluid % nx else 0)
+    I, K = np.meshgrid(np.arange(nx), np.arange(-3, nz), indexing="xy")
+    I, K = I.ravel(), K.ravel()                  # x fastest, then z
+    lat = np.stack([(I + 0.5) * dx, (K + 0.5) * dx], 1)
+    inlet = lat[: 3 * nx]
+    fluid = lat[3 * nx: 3 * nx + n_fluid]
+    ztop = fluid[:, 1].max() + 0.5 * dx
+    WI, WK = np.meshgrid(np.r_[np.arange(-3, 0), np.arange(nx, nx + 3)], np.arange(-3, int(np.ceil(ztop / dx))),
+                         indexing="xy")
+    walls = np.stack([(WI.ravel() + 0.5) * dx, (WK.ravel() + 0.5) * dx], 1)
+    pos = np.concatenate([fluid, inlet, walls])
+    ptype = np.concatenate([np.ones(len(fluid) + len(inlet), np.int32), np.zeros(len(walls), np.int32)])
+    n = len(pos)
+    pos = pos + rng.uniform(-0.01 * dx, 0.01 * dx, size=(n, 2))
+    vol = (h / p.h_over_dx) ** 2
+    uz = np.where(pos[:, 1] < 0, u_in, 0.0) * (ptype == 1)
+    sph = dict(x=pos[:, 0], y=np.full(n, float(y0)), z=pos[:, 1], ux=np.zeros(n), uy=np.zeros(n), uz=uz,
+               m=np.full(n, p.rho_gas * vol), rho=np.full(n, p.rho_gas), pres=np.zeros(n),
+               temp=np.full(n, t_fluid), h=np.full(n, h), flt_s=np.ones(n), p_type=ptype,
+               rad=np.zeros(n), ri=np.zeros(n))
+    p.obc_L1 = -1.0
+    p.obc_L2 = 0.0
+    p.obc_L3 = ztop - 3 * dx
+    p.obc_L4 = ztop + 1.0
+    if n_dem is None:
+        n_dem = n_fluid // 10
+    rmax = 0.5 * d_dem * 1.05
+    s = 2.1e-3 * max(1.0, d_dem / 2.0e-3)
+    x0, x1 = rmax * 1.2, lx - rmax * 1.2
+    per_row = int(np.floor((x1 - x0) / s)) + 1
+    rows = int(np.floor((ztop - 4 * dx - rmax - rmax * 1.2) / (s * np.sqrt(3.0) / 2.0))) + 1
+    RI, RK = np.meshgrid(np.arange(per_row), np.arange(max(rows, 0)), indexing="xy")
+    sx = x0 + RI.ravel() * s + 0.5 * s * (RK.ravel() % 2)
+    sz = rmax * 1.2 + RK.ravel() * s * np.sqrt(3.0) / 2.0
+    keep = (sx <= x1) & (sz <= ztop - 4 * dx - rmax)
+    sites = np.stack([sx[keep], sz[keep]], 1)
+    n_dem = min(n_dem, len(sites))
+    pick = np.sort(rng.choice(len(sites), size=n_dem, replace=False))
+    dpos = np.stack([sites[pick, 0], np.full(n_dem, float(y0)), sites[pick, 1]], 1)
+    rad = 0.5 * d_dem * rng.uniform(0.95, 1.05, size=n_dem)
+    dem = _dem_arrays(dpos, rad, 2500.0, h, t_dem)
+    # DEM box walls in x and z only: the y extent never binds
+    p.box_c[:] = [0.5 * lx, float(y0), 0.5 * (ztop + 1.0)]
+    p.box_L[:] = [lx, 1.0, ztop + 1.0]
     return p, sph, dem
 
 
@@ -451,8 +523,48 @@ def dam_break_batch(n_beds=64, n_min=2_000, n_max=50_000, seed=0, dx=5.0e-3, ref
     return params, beds
 
 
+def bed2d_batch(n_beds=64, n_min=2_000, n_max=50_000, seed=0, u_range=(0.1, 0.3), dx=1.25e-3, plane_cells=2.05):
+    """Uneven batch of 2-D ISPH-DEM beds (box_bed_2d) for one handle: bed b
+    has N_b fluid particles (drawn log-uniform in [n_min, n_max], seeded),
+    N_b / 10 spheres, an inlet velocity drawn uniformly from u_range, and
+    lies in the plane y = b * plane_cells * 1.1 kappa h, so that no
+    neighbour pair crosses two beds (sphdem_set_beds wants the planes more
+    than two cells apart).  The beds share the bed width, kernel, materials
+    and DEM walls; their heights, outlet slabs and inlet velocities differ.
+
+    Returns (params, sph, dem, rows, parts): sph and dem concatenate the
+    beds in order (sphere ids renumbered to stay unique), rows are the
+    per-bed rows for Engine(beds=rows), parts[b] = (sph_b, dem_b, rows_b) is
+    bed b alone, in its own plane, for the same run in a handle of its own."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=n_beds)).astype(int)
+    u_in = rng.uniform(u_range[0], u_range[1], size=n_beds)
+    params, parts, rows = None, [], []
+    id0 = 0
+    for b in range(n_beds):
+        p, sph, dem = box_bed_2d(n_fluid=int(counts[b]), dx=dx, seed=seed * 1000 + b, u_in=float(u_in[b]))
+        gap = plane_cells * 1.1 * p.kappa * float(sph["h"][0])
+        y0 = b * gap
+        sph["y"] = np.full(len(sph["x"]), y0)
+        dem["y"] = np.full(len(dem["x"]), y0)
+        dem["dem_idx"] = dem["dem_idx"] + id0
+        id0 += len(dem["x"])
+        row = dict(y=y0, inlet_uz=float(u_in[b]), inlet_temp=p.inlet_temp, obc_L1=p.obc_L1, obc_L2=p.obc_L2,
+                   obc_L3=p.obc_L3, obc_L4=p.obc_L4)
+        rows.append(row)
+        parts.append((sph, dem, [row]))
+        if params is None or p.box_L[2] > params.box_L[2]:
+            params = p
+    params = params.copy()
+    params.box_c[1] = 0.5 * rows[-1]["y"]
+    params.box_L[1] = rows[-1]["y"] + 1.0      # the DEM walls' y extent never binds
+    sph = {k: np.concatenate([pt[0][k] for pt in parts]) for k in parts[0][0]}
+    dem = {k: np.concatenate([pt[1][k] for pt in parts]) for k in parts[0][1]}
+    return params, sph, dem, rows, parts
+
+
 GENERATORS = {"spouted_bed": spouted_bed, "box_bed": box_bed, "scaled_box_bed": scaled_box_bed,
-              "isph_column": isph_column, "dam_break_2d": dam_break_2d}
+              "isph_column": isph_column, "dam_break_2d": dam_break_2d, "box_bed_2d": box_bed_2d}
 
 
 def _cli(argv=None):

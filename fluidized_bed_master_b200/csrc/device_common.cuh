@@ -36,6 +36,10 @@ struct DevParams {
     double k_sph, cp_sph, k_dem, cp_dem;
     double G, nu_p, damp, fric, r_contact, r_search;
     double inlet_uz, inlet_temp, L2, L3, ball_vel;
+    // 2-D beds in planes y = const (sphdem_set_beds): nbeds rows of
+    // {y, inlet_uz, inlet_temp, L2, L3}, sorted by y; 0 = the values above
+    int nbeds;
+    const double* beds;
     // The SPH temperature is stored as T - t_ref (t_ref: the mean initial SPH
     // temperature, an FP32 value): in the FP32 build a temperature near
     // 300 K keeps increments of 1e-4 K per step only as an offset, and the
@@ -52,6 +56,24 @@ struct DevParams {
     double q_org[3], q_inv[3], q_abs;
     float q_step[3];
 };
+
+// The open-boundary parameters of the bed whose plane is nearest y.
+constexpr int BED_COLS = 5;
+struct BedObc {
+    double inlet_uz, inlet_temp, L2, L3;
+};
+__device__ __forceinline__ BedObc bed_obc(const DevParams& P, double y) {
+    if (P.nbeds <= 0) return BedObc{P.inlet_uz, P.inlet_temp, P.L2, P.L3};
+    int lo = 0, hi = P.nbeds - 1;   // the last row with plane <= y, or row 0
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.beds[mid * BED_COLS] <= y) lo = mid;
+        else hi = mid - 1;
+    }
+    if (lo + 1 < P.nbeds && fabs(P.beds[(lo + 1) * BED_COLS] - y) < fabs(P.beds[lo * BED_COLS] - y)) lo++;
+    const double* r = P.beds + lo * BED_COLS;
+    return BedObc{r[1], r[2], r[3], r[4]};
+}
 
 // ---- cell index ---------------------------------------------------------
 __device__ __forceinline__ int cell_coord(double v, double vmin, double vmax, int N) {

@@ -632,7 +632,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         }
         {
             KTIME(KT_PPE);
-            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) CK((launch_pdl(k_ppe<R>, bs, TPB, 0, st, P, S, W)));
+            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) CK((launch_pdl(kt3 ? k_ppe<R, 3> : k_ppe<R, -1>, bs, TPB, 0, st, P, S, W)));
             else if ((r = enqueue_krylov<R>(H, EH, S, W))) return r;
         }
         {
@@ -715,6 +715,15 @@ int run_step(SphdemHandle* H, EngineHost<R>* EH, int64_t* nl) {
 // bounding box: find_minmax (function_init.cuh:913-950) over the rows in
 // file order, stopping one row short (the reference loop bound), then the
 // margins; out = xmin, xmax, ymin, ymax, zmin, zmax
+// the row of sphdem_set_beds (sorted by plane) whose plane is nearest y
+static const SphdemBedRow& bed_row(const std::vector<SphdemBedRow>& rows, double y) {
+    size_t k = std::upper_bound(rows.begin(), rows.end(), y,
+                                [](double v, const SphdemBedRow& r) { return v < r.y; }) - rows.begin();
+    if (k == 0) return rows[0];
+    if (k == rows.size()) return rows[k - 1];
+    return (std::fabs(rows[k].y - y) < std::fabs(rows[k - 1].y - y)) ? rows[k] : rows[k - 1];
+}
+
 static void bed_box(const SphdemParams& p, const double* fx, const double* fy, const double* fz, int n, double* out) {
     double mnx = fx[0], mxx = fx[0], mny = fy[0], mxy = fy[0], mnz = fz[0], mxz = fz[0];
     for (int k = 0; k < n - 1; k++) {
@@ -766,6 +775,9 @@ static int commit_t(SphdemHandle* H) {
     H->nijk[0] = NI; H->nijk[1] = NJ; H->nijk[2] = NK;
     H->dcell = dcell;
     int num_cells = NI * NJ * NK + 1;
+    // beds in planes y = const: no neighbour pair may cross two planes
+    for (size_t b = 1; b < H->beds.size(); b++)
+        if (!(H->beds[b].y - H->beds[b - 1].y > 2.0 * dcell)) return SPHDEM_E_INPUT;
 
     EngineHost<R>* EH = new EngineHost<R>();
     H->eng = EH;
@@ -793,6 +805,17 @@ static int commit_t(SphdemHandle* H) {
     P.r_contact = p.dem_contact_range; P.r_search = p.dem_search_range;
     P.inlet_uz = p.inlet_uz_mirror; P.inlet_temp = p.inlet_temp; P.L2 = p.obc_L2; P.L3 = p.obc_L3;
     P.ball_vel = p.ball_vel;
+    if (!H->beds.empty()) {
+        std::vector<double> rows;
+        for (const SphdemBedRow& b : H->beds) {
+            const double r[BED_COLS] = {b.y, b.inlet_uz, b.inlet_temp, b.obc_L2, b.obc_L3};
+            rows.insert(rows.end(), r, r + BED_COLS);
+        }
+        CK(cudaMalloc(&H->d_beds, sizeof(double) * rows.size()));
+        CK(cudaMemcpy(H->d_beds, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice));
+        P.nbeds = (int)H->beds.size();
+        P.beds = H->d_beds;
+    }
     {
         // offset of the stored SPH temperature (DevParams::t_ref), an FP32 value
         auto& tv = H->stage_d[0][SPHDEM_F_TEMP];
@@ -856,8 +879,13 @@ static int commit_t(SphdemHandle* H) {
                 continue;
             }
             if (p.open_boundary > 0 && pt[i] < 1000 && pt[i] >= 1) {
-                if (zz[i] >= (p.obc_L1 - 1e-6) && (zz[i] < p.obc_L2 - 1e-6)) { btype[i] = 1; itype[i] = 2; }
-                if (zz[i] >= (p.obc_L3 - 1e-6) && (zz[i] < p.obc_L4 - 1e-6)) { btype[i] = 2; itype[i] = 2; }
+                double L1 = p.obc_L1, L2 = p.obc_L2, L3 = p.obc_L3, L4 = p.obc_L4;
+                if (!H->beds.empty()) {
+                    const SphdemBedRow& b = bed_row(H->beds, H->stage_d[q][SPHDEM_F_Y][i]);
+                    L1 = b.obc_L1; L2 = b.obc_L2; L3 = b.obc_L3; L4 = b.obc_L4;
+                }
+                if (zz[i] >= (L1 - 1e-6) && (zz[i] < L2 - 1e-6)) { btype[i] = 1; itype[i] = 2; }
+                if (zz[i] >= (L3 - 1e-6) && (zz[i] < L4 - 1e-6)) { btype[i] = 2; itype[i] = 2; }
             }
         }
         H->stage_i[q][SPHDEM_F_ITYPE] = itype;
@@ -1742,7 +1770,8 @@ static int check_supported(const SphdemParams* p) {
         return SPHDEM_OK;
     }
     if (p->solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
-    if (p->dim != 3) return SPHDEM_E_UNSUPPORTED;
+    // dim 2: a bed in a plane y = const (the step's 2-D model, step_kernels.cuh)
+    if (p->dim != 3 && p->dim != 2) return SPHDEM_E_UNSUPPORTED;
     // Switches of the ISPH step that are not built: property tables, the
     // Boussinesq term (functions_PPE2.cuh:1575 reads temp0, a local that is
     // never assigned), and the wall velocity condition of noslip_bc /
@@ -2672,6 +2701,21 @@ extern "C" int sphdem_get_time(SphdemHandle* h, double* time, int32_t* count) {
 // ---------------------------------------------------------------------------
 // slab exchange of a spatially sharded bed (slab.cuh)
 // ---------------------------------------------------------------------------
+extern "C" int sphdem_set_beds(SphdemHandle* h, int32_t nbeds, const SphdemBedRow* rows) {
+    if (!h || !rows || h->committed || h->kind != 0) return SPHDEM_E_ARG;
+    if (h->p.dim != 2 || h->p.solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;
+    if (nbeds < 1 || nbeds > SPHDEM_MAX_BEDS) return SPHDEM_E_ARG;
+    std::vector<SphdemBedRow> b(rows, rows + nbeds);
+    for (const SphdemBedRow& r : b) {
+        const double v[7] = {r.y, r.inlet_uz, r.inlet_temp, r.obc_L1, r.obc_L2, r.obc_L3, r.obc_L4};
+        for (double x : v)
+            if (!std::isfinite(x)) return SPHDEM_E_ARG;
+    }
+    std::stable_sort(b.begin(), b.end(), [](const SphdemBedRow& a, const SphdemBedRow& c) { return a.y < c.y; });
+    h->beds = b;
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_ref) {
     if (!h || !bbox6 || h->committed || h->kind != 0) return SPHDEM_E_ARG;
     if (!(h0 > 0) || !std::isfinite(t_ref)) return SPHDEM_E_ARG;
@@ -2897,6 +2941,7 @@ extern "C" void sphdem_destroy(SphdemHandle* h) {
     if (h->slab_blk) cudaFree(h->slab_blk);
     if (h->slab_tot) cudaFree(h->slab_tot);
     if (h->slab_free) cudaFree(h->slab_free);
+    if (h->d_beds) cudaFree(h->d_beds);
     if (h->dem_stream) cudaStreamDestroy(h->dem_stream);
     for (cudaEvent_t e : h->fork_ev)
         if (e) cudaEventDestroy(e);

@@ -43,6 +43,10 @@ struct SphdemHandle {
     int concurrent = 1;                  // sphdem_set_concurrency
     int time_only = -1;                  // sphdem_set_timing_only: the one kernel timed (-1 all)
     // the whole bed's domain for a slab of it (sphdem_set_domain, before commit)
+    // per-bed open-boundary rows of a handle of 2-D beds (sphdem_set_beds),
+    // sorted by plane; on the device as BED_COLS doubles per row
+    std::vector<SphdemBedRow> beds;
+    double* d_beds = nullptr;
     bool dom_set = false;
     double dom_bbox[6] = {};
     double dom_h0 = 0, dom_tref = 0;

@@ -52,6 +52,23 @@ __device__ __forceinline__ void kgc3(const R* __restrict__ Cm, int n, int i, int
     az = Cm[6 * n + i] * a + Cm[7 * n + i] * b + Cm[8 * n + i] * c;
 }
 
+// Two-dimensional beds (dim 2) lie in a plane y = const and run this step
+// with: the 2-D kernel normalisation; SPH particle volume (h / h_over_dx)^2;
+// the gradient correction on the x-z block; a DEM sphere (centre in the
+// plane; contact, drag and heat as for a sphere) in the porosity with its
+// equatorial disc 3.14159 r^2, as the reference's 2-D coupling prep
+// (KERNEL_clc_prep2D_coupling, functions_PREP2.cuh:2944-3033) -- the
+// sphere's volume over a depth 4 r / 3 -- and its drag and heat acting on
+// the fluid per unit depth (divided by that depth).
+template <typename R>
+__device__ __forceinline__ R dem_measure(const DevParams& P, R r) {
+    return P.dim == 2 ? (R)3.14159 * r * r : (R)4.18879 * r * r * r;
+}
+template <typename R>
+__device__ __forceinline__ R sph_volume(const DevParams& P, R th, R hd) {
+    return P.dim == 2 ? (th / hd) * (th / hd) : (th / hd) * (th / hd) * (th / hd);
+}
+
 // 27-cell stencil in the reference order (z,y,x), calling f(j) for every
 // slot j of every non-empty cell: the 9 rows in order, ascending slots
 // inside a row.
@@ -676,7 +693,20 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
                 tzz += c * g.dz * g.dz;
             }
         });
-    if (kgc) {
+    if (kgc && P.dim == 2) {
+        // a bed in a plane y = const: the x-z block of the moment matrix
+        const R det = txx * tzz - tzx * tzx;
+        R C[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        if (fabs(det) > (R)1e-4) {
+            const R rr = (R)1 / det;
+            C[0] = tzz * rr;
+            C[2] = -tzx * rr;
+            C[6] = -tzx * rr;
+            C[8] = txx * rr;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) W.Cm[(size_t)q * n + i] = C[q];
+    } else if (kgc) {
         R det = txx * (tyy * tzz - tyz * tyz);
         det -= txy * (txy * tzz - tyz * tzx);
         det += tzx * (txy * tyz - tyy * tzx);
@@ -712,7 +742,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
             R w = kw(K, r);
             R dw = kdw(K, r);
             R rj = (R)D.rad[j];
-            R v = (R)4.18879 * rj * rj * rj;
+            R v = dem_measure(P, rj);
             por += w * v;
             dfx += dw * g.dx * ir * (R)D.ux[j] * v;
             dfy += dw * g.dy * ir * (R)D.uy[j] * v;
@@ -733,7 +763,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
     S.dDEMpor[i] = (dfx + dfy + dfz) * isf;
     // prep_sph
     R hd = (R)P.h_over_dx;
-    R v = (th / hd) * (th / hd) * (th / hd);
+    R v = sph_volume(P, th, hd);
     R mref;
     if (pt == 9) mref = (R)P.rho_liquid * v * pori;
     else if (pt == -3 || pt == 0 || pt == 3 || pt == 1) mref = (R)P.rho_gas * v * pori;
@@ -825,7 +855,7 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
         if (!g.in) return;
         R w = kw(K, g.r);
         R rj = (R)D.rad[j];
-        por += w * (R)4.18879 * rj * rj * rj;
+        por += w * dem_measure(P, rj);
     });
     f1 = warp_sum(f1);
     f3 = warp_sum(f3);
@@ -1585,6 +1615,7 @@ __global__ void __launch_bounds__(128) k_sph_coupling(DevParams P, SphState<R> S
                 R ffj = (R)DW.flt_sd2[j] + (R)DW.flt_s[j];
                 if (!(ffj > (R)0)) return;
                 R w = kw(K, g.r);
+                if (P.dim == 2) w *= (R)0.75 / (R)D.rad[j];   // per unit depth (depth 4 r / 3)
                 R c = w / (ffj + (R)1.0e-20);
                 R mr = (R)D.m[j] / rhoi;
                 tx += -mr * (R)D.Fdx_df[j] * c;
@@ -1911,7 +1942,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
 // 868-878): one Jacobi sweep; p_new = (b + sum A_ij p_j) / sum A_ij for
 // fluid, every other particle keeps its pressure.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KT>
 __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1926,7 +1957,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
         return;
     }
     R th = (R)S.h[i];
-    Knl<R> K = knl_make<R>(P, th);
+    Knl<R, KT> K = knl_make<R, KT>(P, th);
     PosRec<R> qi = ldr(rec.pos + i);
     V4<R> fi = rec.f1[i];
     R uxi = upi.x, uyi = upi.y, uzi = upi.z, rhoi = fi.y, pori = fi.w;
@@ -1937,7 +1968,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
     int cnt = min(W.ncnt[i], P.nb_cap);
     R bx = 0, by = 0, bz = 0, A = 0, AP = 0;
     const int* __restrict__ nb = W.nbr;
-    nb_walk<2, NbQ44<R>>(
+    nb_walk<4, NbQ44<R>>(
         cnt, nb, n, i,
         [&](int j) {
             NbQ44<R> t;
@@ -2214,9 +2245,10 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     int i = W.buf_idx[w];
     int bt = S.btype[i];
     double xi = S.x[i], yi = S.y[i], zi = S.z[i], hi = S.h[i];
+    const BedObc ob = bed_obc(P, yi);
     double zg = zi;
-    if (bt == 1) zg = 2 * P.L2 - zi;
-    else if (bt == 2) zg = 2 * P.L3 - zi;
+    if (bt == 1) zg = 2 * ob.L2 - zi;
+    else if (bt == 2) zg = 2 * ob.L3 - zi;
     R th = (R)hi;
     Knl<R, KT> K = knl_make<R, KT>(P, th);
     double Rr = P.kappa * hi;
@@ -2239,7 +2271,7 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
         rdist(r2, r, rinv);
         R wk = kw(K, r);
         R hj = (R)S.h[j];
-        R volj = (hj / hd) * (hj / hd) * (hj / hd);
+        R volj = sph_volume(P, hj, hd);
         R vw = volj * wk;
         trho += W.rho_new[j] / W.DEMpor[j] * wk * volj;
         tp += vw * W.p_new[j];
@@ -2253,16 +2285,16 @@ __global__ void __launch_bounds__(128) k_open_bc(DevParams P, SphState<R> S, Sph
     tuz = warp_sum(tuz); tt = warp_sum(tt); flt = warp_sum(flt);
     if (lane != 0 || P.open_bc != 1) return;
     R pori = W.DEMpor[i];
-    R vol0 = (th / hd) * (th / hd) * (th / hd);
+    R vol0 = sph_volume(P, th, hd);
     R rho_old = W.rho_new[i];
     R pn, rn, ux, uy, uz, tn;
     if (bt == 1) {
         pn = tp / flt;
         rn = pori * (R)P.rho_gas;
-        uz = (R)P.inlet_uz * (R)2 - tuz / flt;
+        uz = (R)ob.inlet_uz * (R)2 - tuz / flt;
         ux = (R)0 - tux / flt;
         uy = (R)0 - tuy / flt;
-        tn = (R)(P.inlet_temp - P.t_ref);   // stored T - t_ref
+        tn = (R)(ob.inlet_temp - P.t_ref);   // stored T - t_ref
     } else {
         pn = (R)0;
         rn = pori * (trho / flt);

@@ -58,6 +58,7 @@ def lib():
     L.sphdem_set_concurrency.argtypes = [vp, C.c_int]
     L.sphdem_set_timing_only.argtypes = [vp, C.c_int]
     L.sphdem_set_domain.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double]
+    L.sphdem_set_beds.argtypes = [vp, C.c_int32, C.POINTER(BedRow)]
     L.sphdem_slab_record_bytes.argtypes = [C.c_int]
     dp = C.POINTER(C.c_double)
     L.sphdem_bed_domain.argtypes = [vp, dp, dp, dp, dp, dp, C.c_int32, dp, dp, dp, dp, C.c_int32, dp, dp, dp]
@@ -144,13 +145,21 @@ def read_solv(path, params=None):
     return p
 
 
+class BedRow(C.Structure):
+    """SphdemBedRow: a 2-D bed's plane and open-boundary parameters."""
+    _fields_ = [("y", C.c_double), ("inlet_uz", C.c_double), ("inlet_temp", C.c_double),
+                ("obc_L1", C.c_double), ("obc_L2", C.c_double), ("obc_L3", C.c_double), ("obc_L4", C.c_double)]
+
+
 class Engine:
     """One engine handle on the current CUDA device."""
 
-    def __init__(self, params, sph, dem, domain=None):
+    def __init__(self, params, sph, dem, domain=None, beds=None):
         """params: SphdemParams; sph/dem: dict field-name -> array in input
         order.  domain: (bbox6, h0, t_ref) of a larger bed this one is a slab
-        of (sphdem_set_domain; see bed_domain)."""
+        of (sphdem_set_domain; see bed_domain).  beds: rows (dicts with the
+        BedRow fields) of several 2-D beds in their own planes y = const
+        (sphdem_set_beds; see beds.bed2d_batch)."""
         L = lib()
         ns = len(sph["x"]) if sph else 0
         nd = len(dem["x"]) if dem else 0
@@ -163,6 +172,9 @@ class Engine:
             if domain is not None:
                 bb = (C.c_double * 6)(*[float(v) for v in domain[0]])
                 _chk(L.sphdem_set_domain(self._h, bb, float(domain[1]), float(domain[2])), "sphdem_set_domain")
+            if beds is not None:
+                rows = (BedRow * len(beds))(*[BedRow(**{k: float(r[k]) for k, _ in BedRow._fields_}) for r in beds])
+                _chk(L.sphdem_set_beds(self._h, len(beds), rows), "sphdem_set_beds")
             for which, d in ((SPH, sph), (DEM, dem)):
                 for name, arr in (d or {}).items():
                     self._set(which, name, arr)

@@ -523,6 +523,27 @@ int sphdem_bed_domain(const SphdemParams* p, const double* sx, const double* sy,
  * passes of a slab get headroom for particles that enter its layers. */
 int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_ref);
 
+/* Several two-dimensional ISPH-DEM beds in one handle (dim 2): each bed lies
+ * in its own plane y = const, and planes more than two cells
+ * (2 x 1.1 kappa h) apart share no neighbour pair, so the one handle steps
+ * all beds in every launch of its step graph.  A row gives a bed's plane
+ * and the open-boundary parameters that differ from bed to bed (they take
+ * the place of SphdemParams' inlet_uz_mirror, inlet_temp and obc_L1..L4 for
+ * the particles of that bed, the particles in the row's plane: the row
+ * with the nearest y).  Replaces what KERNEL_open_boundary_extrapolation3D
+ * (functions_BC.cuh:787-984) reads from k_vif and the slab tags of
+ * c_initial_inner_outer_particle_single (functions_NNPS.cuh:60-200). */
+#define SPHDEM_MAX_BEDS 4096
+typedef struct {
+    double y;                                 /* the bed's plane */
+    double inlet_uz, inlet_temp;              /* inlet velocity and temperature */
+    double obc_L1, obc_L2, obc_L3, obc_L4;    /* inlet slab [L1, L2), outlet slab [L3, L4) */
+} SphdemBedRow;
+/* Before sphdem_commit_particles, dim-2 ISPH handles only; nbeds in
+ * [1, SPHDEM_MAX_BEDS], planes more than two cells apart (checked at
+ * commit: SPHDEM_E_INPUT). */
+int sphdem_set_beds(SphdemHandle* h, int32_t nbeds, const SphdemBedRow* rows);
+
 /* Bytes of one particle record of sphdem_slab_export/import (which: SPH or
  * DEM); every real value as a double, the DEM record with its contact
  * history. */

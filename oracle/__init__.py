@@ -42,6 +42,7 @@ def lib():
     L.oracle_get_field.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int]
     L.oracle_commit.argtypes = [vp]
     L.oracle_set_domain.argtypes = [vp, P(C.c_double), P(C.c_double), C.c_double]
+    L.oracle_set_beds.argtypes = [vp, C.c_int, P(C.c_double)]
     L.oracle_step.argtypes = [vp, C.c_int]
     L.oracle_get_neighbors.argtypes = [vp, P(C.c_int), P(C.c_int), C.c_int]
     L.oracle_get_grid.argtypes = [vp, P(C.c_int), P(C.c_double), P(C.c_double)]
@@ -54,8 +55,14 @@ def lib():
     return L
 
 
+_BED_KEYS = ("y", "inlet_uz", "inlet_temp", "obc_L1", "obc_L2", "obc_L3", "obc_L4")
+
+
 class Oracle:
-    def __init__(self, params, sph, dem, threads=1):
+    def __init__(self, params, sph, dem, threads=1, beds=None, domain=None):
+        """beds: per-bed rows of 2-D beds in planes y = const (dicts with
+        the keys of the engine's BedRow), as Engine(beds=...).  domain:
+        (bbox6, h0, ...) fixing the cell grid, as Engine(domain=...)."""
         L = lib()
         self.ns = len(sph["x"]) if sph else 0
         self.nd = len(dem["x"]) if dem else 0
@@ -64,6 +71,15 @@ class Oracle:
         if not self._h:
             raise MemoryError("oracle_create failed")
         L.oracle_set_threads(self._h, int(threads))
+        if domain is not None:
+            bb = [float(v) for v in domain[0]]
+            mins = (C.c_double * 3)(bb[0], bb[2], bb[4])
+            maxs = (C.c_double * 3)(bb[1], bb[3], bb[5])
+            L.oracle_set_domain(self._h, mins, maxs, float(domain[1]))
+        if beds is not None:
+            rows = np.ascontiguousarray([[float(r[k]) for k in _BED_KEYS] for r in beds], dtype=np.float64)
+            if L.oracle_set_beds(self._h, len(beds), rows.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+                raise ValueError("oracle_set_beds")
         for which, d in ((SPH, sph), (DEM, dem)):
             for name, arr in (d or {}).items():
                 self._set(which, name, arr)

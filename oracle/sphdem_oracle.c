@@ -76,7 +76,18 @@ struct OracleState {
     int ppe_iters;         /* last PPE solve (Krylov modes) */
     double ppe_res;
     int ppe_status;
+    int nbeds;             /* 2-D beds in planes y = const: rows of */
+    double* beds;          /* {y, inlet_uz, inlet_temp, L1, L2, L3, L4} */
 };
+
+/* The row of the bed whose plane is nearest y (NULL: the global values). */
+static const double* bed_row(const OracleState* S, double y) {
+    if (S->nbeds <= 0) return NULL;
+    int best = 0;
+    for (int b = 1; b < S->nbeds; b++)
+        if (fabs(S->beds[7 * b] - y) < fabs(S->beds[7 * best] - y)) best = b;
+    return S->beds + 7 * best;
+}
 
 static void* xcalloc(size_t n, size_t sz) {
     void* p = calloc(n ? n : 1, sz);
@@ -393,6 +404,22 @@ static void k_set_alpha(OSet* o) {
     }
 }
 
+/* Two-dimensional ISPH-DEM beds (dim 2) lie in a plane y = const and use
+ * the three-dimensional step with these changes (the reference's ISPH step
+ * is three-dimensional only; its one two-dimensional coupling kernel,
+ * KERNEL_clc_prep2D_coupling, functions_PREP2.cuh:2944-3033, gives the
+ * porosity form):
+ *  - kernel normalisation and SPH particle volume (h / h_over_dx)^2;
+ *  - the gradient correction inverts the x-z block of the moment matrix;
+ *  - a DEM sphere (centre in the plane; contact, drag and heat as for a
+ *    sphere) enters the porosity with its equatorial disc, 3.14159 r^2, as
+ *    the reference's 2-D coupling prep does: its volume spread over a depth
+ *    4 r / 3, and its drag and heat act on the fluid per unit depth, i.e.
+ *    divided by that depth. */
+static double sph_volume(int dim, double th, double hd) {
+    return dim == 2 ? (th / hd) * (th / hd) : (th / hd) * (th / hd) * (th / hd);
+}
+
 /* KERNEL_clc_mass_init_sph: functions_MASS.cuh:24-43 */
 static void k_mass_init(OracleState* S) {
     OSet* o = &S->s;
@@ -434,10 +461,22 @@ static void k_kgc(OracleState* S) {
                 }
             }
         }
+        double* C = o->Cm + (size_t)i * 9;
+        if (P->dim == 2) {   /* the x-z block */
+            double det2 = txx * tzz - tzx * tzx;
+            for (int q = 0; q < 9; q++) C[q] = 0;
+            C[4] = 1;
+            if (fabs(det2) > 1e-4) {
+                double r = 1.0 / det2;
+                C[0] = tzz * r; C[2] = -tzx * r; C[6] = -tzx * r; C[8] = txx * r;
+            } else {
+                C[0] = 1; C[8] = 1;
+            }
+            continue;
+        }
         double det = txx * (tyy * tzz - tyz * tyz);
         det -= txy * (txy * tzz - tyz * tzx);
         det += tzx * (txy * tyz - tyy * tzx);
-        double* C = o->Cm + (size_t)i * 9;
         if (fabs(det) > 1e-4) { /* Min_det, Parameters.cuh:122 */
             double r = 1.0 / det;
             C[0] = (tyy * tzz - tyz * tyz) * r;
@@ -487,7 +526,12 @@ static void k_coupling_prep_sph(OracleState* S) {
                 double tdwx = dw * (xi - xj) / td, tdwy = dw * (yi - yj) / td, tdwz = dw * (zi - zj) / td;
                 double rj = d->rad[j];
                 int ptj = d->p_type[j];
-                if (pti <= 1000 && ptj > 1000) {
+                if (pti <= 1000 && ptj > 1000 && P->dim == 2) {
+                    por += w * 3.14159 * rj * rj;
+                    dfx += tdwx * d->ux[j] * 3.14159 * rj * rj;
+                    dfy += tdwy * d->uy[j] * 3.14159 * rj * rj;
+                    dfz += tdwz * d->uz[j] * 3.14159 * rj * rj;
+                } else if (pti <= 1000 && ptj > 1000) {
                     por += w * 4.18879 * rj * rj * rj;
                     dfx += tdwx * d->ux[j] * 4.18879 * rj * rj * rj;
                     dfy += tdwy * d->uy[j] * 4.18879 * rj * rj * rj;
@@ -535,7 +579,8 @@ static void k_coupling_prep_dem(OracleState* S) {
             if (td < R) {
                 double w = knl_w(P->kernel_type, tA, 1.0 * th, td);
                 double rj = d->rad[j];
-                if (pti > 1000 && d->p_type[j] > 1000) por += w * 4.18879 * rj * rj * rj;
+                if (pti > 1000 && d->p_type[j] > 1000)
+                    por += P->dim == 2 ? w * 3.14159 * rj * rj : w * 4.18879 * rj * rj * rj;
             }
         }
         if (pti > 1000) {
@@ -556,7 +601,7 @@ static void k_prep_sph(OracleState* S) {
         if (o->i_type[i] > 2 || o->p_type[i] > 1000) continue;
         int pt = o->p_type[i];
         double th = o->h[i], pori = o->DEMpor[i], zi = o->z[i], mref;
-        double v = (th / hd) * (th / hd) * (th / hd);
+        double v = sph_volume(P->dim, th, hd);
         if (pt == -3) mref = P->rho_gas * v * pori;
         else if (pt == 9) mref = P->rho_liquid * v * pori;
         else if (pt == 0) mref = P->rho_gas * v * pori;
@@ -567,8 +612,8 @@ static void k_prep_sph(OracleState* S) {
         if (P->dim == 2) o->rho_ref[i] = mref / ((th / hd) * (th / hd));
         if (P->dim == 3) o->rho_ref[i] = mref / ((th / hd) * (th / hd) * (th / hd));
         if (P->rho_type == 1) {
-            o->rho0[i] = mref / ((th / hd) * (th / hd) * (th / hd));
-            o->rho[i] = mref / ((th / hd) * (th / hd) * (th / hd));
+            o->rho0[i] = mref / sph_volume(P->dim, th, hd);
+            o->rho[i] = mref / sph_volume(P->dim, th, hd);
             o->m[i] = mref;
         }
     }
@@ -1151,6 +1196,7 @@ static void k_sph_coupling(OracleState* S) {
                 if (td < R) {
                     if (pti != 9 && pti != -3 && pti != 0) {
                         double w = knl_w(P->kernel_type, tA, 1.0 * hi, td);
+                        if (P->dim == 2) w *= 0.75 / d->rad[j];   /* per unit depth, depth 4 r / 3 */
                         double mj = d->m[j];
                         double ffj = d->flt_sd_2[j] + d->flt_s[j];
                         if (pti == 1 || pti == 3) {
@@ -1599,8 +1645,11 @@ static void k_open_boundary(OracleState* S) {
         double th = o->h[i], tA = knl_tmpA(P->kernel_type, P->dim, th), R = P->kappa * th;
         double pori = o->DEMpor[i], xi = o->x[i], yi = o->y[i], zi = o->z[i];
         double xg = xi, yg = yi, zg = zi;
-        if (o->buffer_type[i] == 1) zg = 2 * P->obc_L2 - zi;
-        else if (o->buffer_type[i] == 2) zg = 2 * P->obc_L3 - zi;
+        const double* br = bed_row(S, yi);
+        const double L2 = br ? br[4] : P->obc_L2, L3 = br ? br[5] : P->obc_L3;
+        const double u_in = br ? br[1] : P->inlet_uz_mirror, t_in = br ? br[2] : P->inlet_temp;
+        if (o->buffer_type[i] == 1) zg = 2 * L2 - zi;
+        else if (o->buffer_type[i] == 2) zg = 2 * L3 - zi;
         int ic, jc, kc;
         cell_ijk(S, xg, yg, zg, &ic, &jc, &kc);
         double trho = 0, tp = 0, tux = 0, tuy = 0, tuz = 0, tt = 0, flt = 0;
@@ -1623,22 +1672,22 @@ static void k_open_boundary(OracleState* S) {
         double* v = nv + (size_t)i * 7; /* pres rho m uz ux uy temp */
         if (P->open_boundary == 1) {
             if (o->buffer_type[i] == 1) {
-                v[0] = tp / flt + 0 * (2 * (zi - P->obc_L2)) * 0.0;
+                v[0] = tp / flt + 0 * (2 * (zi - L2)) * 0.0;
                 v[1] = pori * P->rho_gas;
                 v[2] = o->rho[i] * o->vol0[i];
-                v[3] = P->inlet_uz_mirror * 2 - tuz / flt;
+                v[3] = u_in * 2 - tuz / flt;
                 v[4] = 0 - tux / flt;
                 v[5] = 0 - tuy / flt;
-                v[6] = P->inlet_temp;
+                v[6] = t_in;
                 if (o->elix[i] < 0.9999 && o->p_type[i] > 0) v[2] = o->rho[i] * o->vol[i];
             } else {
                 v[0] = 0.0;
-                v[1] = pori * (trho / flt + 0 * (2 * (zi - P->obc_L3)) * 0.0);
+                v[1] = pori * (trho / flt + 0 * (2 * (zi - L3)) * 0.0);
                 v[2] = o->rho[i] * o->vol0[i];
-                v[3] = tuz / flt + 0 * (2 * (zi - P->obc_L3)) * 0.0;
+                v[3] = tuz / flt + 0 * (2 * (zi - L3)) * 0.0;
                 v[4] = tux / flt;
                 v[5] = tuy / flt;
-                v[6] = tt / flt + 0 * (2 * (zi - P->obc_L3)) * 0.0;
+                v[6] = tt / flt + 0 * (2 * (zi - L3)) * 0.0;
                 if (o->elix[i] < 0.9999 && o->p_type[i] > 0) v[2] = o->rho[i] * o->vol[i];
             }
         }
@@ -2162,7 +2211,7 @@ static void oracle_one_step(OracleState* S) {
     if (sph_turn) nnps(S, &S->s);
     nnps(S, &S->d);
     if (sph_turn) build_sph_list(S);
-    if (sph_turn && P->dim == 3) k_mass_init(S);
+    if (sph_turn) k_mass_init(S);   /* dim 3 in the reference; the 2-D model runs it too */
     if (sph_turn && P->kgc_solve > 0) k_kgc(S);
     if (sph_turn) k_coupling_prep_sph(S);
     k_coupling_prep_dem(S);
@@ -2216,6 +2265,7 @@ void oracle_destroy(OracleState* s) {
     oset_free(&s->d);
     free(s->nb_cnt);
     free(s->nb_list);
+    free(s->beds);
     free(s);
 }
 
@@ -2272,6 +2322,16 @@ int oracle_get_field(OracleState* s, int which, int field, void* dst, int n) {
     return SPHDEM_E_ARG;
 }
 
+int oracle_set_beds(OracleState* s, int nbeds, const double* rows7) {
+    if (!s || nbeds < 1 || !rows7) return SPHDEM_E_ARG;
+    free(s->beds);
+    s->beds = (double*)malloc(sizeof(double) * 7 * (size_t)nbeds);
+    if (!s->beds) return SPHDEM_E_NOMEM;
+    memcpy(s->beds, rows7, sizeof(double) * 7 * (size_t)nbeds);
+    s->nbeds = nbeds;
+    return 0;
+}
+
 int oracle_set_domain(OracleState* s, const double* mins, const double* maxs, double h0) {
     s->xmin = mins[0]; s->ymin = mins[1]; s->zmin = mins[2];
     s->xmax = maxs[0]; s->ymax = maxs[1]; s->zmax = maxs[2];
@@ -2321,8 +2381,11 @@ int oracle_commit(OracleState* S) {
             o->i_type[i] = 1;
             o->buffer_type[i] = 0;
             if (P->open_boundary > 0 && o->p_type[i] < 1000 && o->p_type[i] >= 1) {
-                if (o->z[i] >= (P->obc_L1 - 1e-6) && (o->z[i] < P->obc_L2 - 1e-6)) { o->buffer_type[i] = 1; o->i_type[i] = 2; }
-                if (o->z[i] >= (P->obc_L3 - 1e-6) && (o->z[i] < P->obc_L4 - 1e-6)) { o->buffer_type[i] = 2; o->i_type[i] = 2; }
+                const double* br = bed_row(S, o->y[i]);
+                double L1 = br ? br[3] : P->obc_L1, L2 = br ? br[4] : P->obc_L2;
+                double L3 = br ? br[5] : P->obc_L3, L4 = br ? br[6] : P->obc_L4;
+                if (o->z[i] >= (L1 - 1e-6) && (o->z[i] < L2 - 1e-6)) { o->buffer_type[i] = 1; o->i_type[i] = 2; }
+                if (o->z[i] >= (L3 - 1e-6) && (o->z[i] < L4 - 1e-6)) { o->buffer_type[i] = 2; o->i_type[i] = 2; }
             }
         }
     }

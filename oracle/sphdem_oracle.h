@@ -35,6 +35,10 @@ int oracle_get_field(OracleState* s, int which, int field, void* dst, int n);
  * bbox_* are computed over the concatenation SPH-then-DEM of the input
  * rows unless the caller fixes them first with oracle_set_domain. */
 int oracle_commit(OracleState* s);
+/* Per-bed open-boundary rows {y, inlet_uz, inlet_temp, L1, L2, L3, L4} of
+ * 2-D beds in planes y = const (the engine's sphdem_set_beds), before
+ * commit: a particle takes the row of the nearest plane. */
+int oracle_set_beds(OracleState* s, int nbeds, const double* rows7);
 int oracle_set_domain(OracleState* s, const double* mins, const double* maxs,
                       double h0);
 
