@@ -858,10 +858,27 @@ def run_bed2d_batch(args, world, rank, local, pg):
     q = p.copy()
     q.precision = 1 if args.precision == "fp64" else 0
     eng = Engine(q, sph, dem, beds=rows)
+    list_mode = eng.list_build()
     n = eng.ns + eng.nd
     stream = torch.cuda.ExternalStream(eng.stream_ptr())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     eng.step(args.warmup)
+    torch.cuda.synchronize()
+    # per-kernel breakdown (in-graph events, every kernel) before the timed
+    # region, which runs without events
+    eng.set_timing(True)
+    eng.step(2)
+    eng.collect_timing()
+    b0 = eng.timing()
+    for _ in range(PROFILE_STEPS // 2):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        eng.step(1)
+        eng.collect_timing()
+    kms = {k: (v[0] - b0.get(k, (0, 0))[0]) / (PROFILE_STEPS // 2) for k, v in eng.timing().items()}
+    kms = {k: round(v, 4) for k, v in sorted(kms.items(), key=lambda kv: -kv[1]) if v > 0}
+    eng.set_timing(False)
+    eng.step(2)
     torch.cuda.synchronize()
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0]
     sampler = ClockSampler(int(vis) if vis.isdigit() else local)
@@ -925,9 +942,12 @@ def run_bed2d_batch(args, world, rank, local, pg):
         "config": {"workload": text, "n_sph": n_sph, "n_dem": n_dem, "beds": len(parts),
                    "fluid_counts": [int(np.sum((s["p_type"] == 1) & (s["z"] >= 0))) for s, _, _ in parts],
                    "inlet_uz": [round(r["inlet_uz"], 4) for r in rows],
+                   "list_build": list_mode, "list_build_how": LIST_BUILD_HOW,
                    "l2": "256 MB buffer written before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "state_finite": finite,
+        "kernels_ms_per_step": kms,
+        "kernels_ms_per_step_from": f"{PROFILE_STEPS // 2} steps with every kernel timed, before the timed region",
         "sequential": {"ms_per_step": seq_ms, "how": f"each bed alone in its own handle, {ks} timed steps each "
                        "after 3 warm-up steps, per-step device times summed over the beds",
                        "value": n * 1e3 / seq_ms if seq_ms else None, "unit": unit},
@@ -1096,6 +1116,7 @@ def run_engine(args, world, rank, local, pg):
     p, sph, dem = box_bed(seed=rank, **WORKLOAD)
     p.precision = 1 if args.precision == "fp64" else 0
     eng = Engine(p, sph, dem)
+    list_mode = eng.list_build()
     n_part = eng.ns + eng.nd
     stream = torch.cuda.ExternalStream(eng.stream_ptr())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -1262,7 +1283,8 @@ def run_engine(args, world, rank, local, pg):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if r == 4 else "f64",
         "data": "synthetic (seeded box bed; reference input.txt not shipped)",
-        "config": bench_config(eng.ns, eng.nd, world, "f32" if r == 4 else "f64"),
+        "config": dict(bench_config(eng.ns, eng.nd, world, "f32" if r == 4 else "f64"),
+                       list_build=list_mode, list_build_how=LIST_BUILD_HOW),
         "avg_neighbours": avg_nb,
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -1287,6 +1309,8 @@ PREC_DEM = ["x", "y", "z", "ux", "uy", "uz", "wx", "wy", "wz", "temp", "DEMpor",
             "Fdy_df", "Fdz_df", "ftotalx", "ftotaly", "ftotalz", "torqx", "torqy", "torqz", "dtemp", "Q_sd"]
 PREC_STEPS = 100
 PROFILE_STEPS = 10
+LIST_BUILD_HOW = ("SPH list build picked at commit by timing (sphdem_get_list_build): 1 = a thread per particle, "
+                  "2/4/8 = a warp per cell with that many cells per block")
 
 
 def precision_keys(args, seed):

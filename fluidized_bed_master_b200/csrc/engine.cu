@@ -125,6 +125,9 @@ struct EngineHost {
     int mlp_trained = 0;     // training steps taken
     Alloc A;
     int nb_cap = 0;
+    // SPH list build: 1 = one thread per particle (k_build_list); 2, 4, 8 =
+    // one warp per cell, that many cells per block (k_build_list_tiled, FP32)
+    int list_mode = 1;
     size_t list_elems = 0;
     MgWork mg{};             // two-level PCG preconditioner (ppe_precond TWO_LEVEL)
     bool has_mg = false;
@@ -501,6 +504,75 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
 
 // SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
 template <typename R>
+cudaError_t launch_list(EngineHost<R>* EH, const SphState<R>& S, int mode, cudaStream_t st) {
+    Engine<R>& E = EH->E;
+    const DevParams& P = E.P;
+    SphWork<R>& W = E.sw;
+    if constexpr (std::is_same<R, float>::value) {
+        if (mode == 2 || mode == 4 || mode == 8) {
+            // slots outside every cell (i_type 3) keep an empty list
+            cudaError_t e = cudaMemsetAsync(W.ncnt, 0, sizeof(int) * P.ns, st);
+            if (e != cudaSuccess) return e;
+            const int ncell = P.NI * P.NJ * P.NK;
+            if (mode == 2)
+                return launch_pdl(k_build_list_tiled<2>, (ncell + 1) / 2, 64, 0, st, P, S, W.rec, W.g_str, W.g_end,
+                                  W.rows, W.nbr, W.ncnt, E.flags);
+            if (mode == 4)
+                return launch_pdl(k_build_list_tiled<4>, (ncell + 3) / 4, 128, 0, st, P, S, W.rec, W.g_str, W.g_end,
+                                  W.rows, W.nbr, W.ncnt, E.flags);
+            return launch_pdl(k_build_list_tiled<8>, (ncell + 7) / 8, 256, 0, st, P, S, W.rec, W.g_str, W.g_end,
+                              W.rows, W.nbr, W.ncnt, E.flags);
+        }
+    }
+    return launch_pdl(k_build_list<R>, nblocks(P.ns, TPB), TPB, 0, st, P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags);
+}
+
+// The list build of the step, picked per handle at commit (list_build 0):
+// each candidate (one thread per particle; one warp per cell with 2, 4 or 8
+// cells per block) builds the commit's list once untimed and three times
+// timed, and the fastest is kept.  The candidates write the same lists, so
+// the pick changes the speed only.  In two dimensions a cell holds a few
+// particles and most lanes of a warp per cell idle; in the 3-D bed a cell
+// holds ~23 and the warp shares the staged candidates.
+template <typename R>
+int tune_list_build(SphdemHandle* H, EngineHost<R>* EH, const SphState<R>& S) {
+    if (!std::is_same<R, float>::value) {
+        EH->list_mode = 1;
+        return SPHDEM_OK;
+    }
+    if (H->list_build_req != 0) {
+        EH->list_mode = H->list_build_req;
+        return SPHDEM_OK;
+    }
+    cudaStream_t st = H->stream;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    const int cand[4] = {1, 2, 4, 8};
+    float best = 0;
+    int pick = 4;
+    cudaError_t e = cudaSuccess;
+    for (int c : cand) {
+        if ((e = launch_list<R>(EH, S, c, st)) != cudaSuccess) break;
+        if ((e = cudaEventRecord(a, st)) != cudaSuccess) break;
+        for (int k = 0; k < 3 && e == cudaSuccess; k++) e = launch_list<R>(EH, S, c, st);
+        if (e != cudaSuccess || (e = cudaEventRecord(b, st)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(b)) != cudaSuccess) break;
+        float ms = 0;
+        if ((e = cudaEventElapsedTime(&ms, a, b)) != cudaSuccess) break;
+        if (c == cand[0] || ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return SPHDEM_E_CUDA;
+    EH->list_mode = pick;
+    return SPHDEM_OK;
+}
+
+template <typename R>
 cudaError_t launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState<double>& D, cudaStream_t st) {
     Engine<R>& E = EH->E;
     const DevParams& P = E.P;
@@ -574,15 +646,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if (ns > 0) {
         {
             KTIME(KT_LIST);
-            if constexpr (std::is_same<R, float>::value) {
-                // one warp per cell; slots outside every cell (i_type 3) keep an empty list
-                CK(cudaMemsetAsync(W.ncnt, 0, sizeof(int) * ns, st));
-                int ncell = P.NI * P.NJ * P.NK;
-                CK((launch_pdl(k_build_list_tiled, (ncell + LT_WARPS - 1) / LT_WARPS, LT_WARPS * 32, 0, st, 
-                    P, S, W.rec, W.g_str, W.g_end, W.rows, W.nbr, W.ncnt, E.flags)));
-            } else {
-                CK((launch_pdl(k_build_list<R>, bs, TPB, 0, st, P, S, W.rec, W.rows, W.nbr, W.ncnt, E.flags)));
-            }
+            CK(launch_list<R>(EH, S, EH->list_mode, st));
         }
         CK(wait(1, st));
         { KTIME(KT_PASSA); CK((launch_pdl(kt3 ? k_passA<R, 3> : k_passA<R, -1>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
@@ -989,6 +1053,7 @@ static int commit_t(SphdemHandle* H) {
         EH->nb_cap = cap;
         W.nbr = A.get<int>((size_t)cap * ns);
         if (!A.ok) return SPHDEM_E_NOMEM;
+        if ((r = tune_list_build<R>(H, EH, E.S[1]))) return r;
         // SPH -> DEM list capacity from an exact count on the sorted input; a
         // particle above it later walks its stencil instead
         P.nbd_cap = 0;
@@ -2701,6 +2766,20 @@ extern "C" int sphdem_get_time(SphdemHandle* h, double* time, int32_t* count) {
 // ---------------------------------------------------------------------------
 // slab exchange of a spatially sharded bed (slab.cuh)
 // ---------------------------------------------------------------------------
+extern "C" int sphdem_set_list_build(SphdemHandle* h, int32_t mode) {
+    if (!h || h->committed || h->kind != 0) return SPHDEM_E_ARG;
+    if (mode != 0 && mode != 1 && mode != 2 && mode != 4 && mode != 8) return SPHDEM_E_ARG;
+    h->list_build_req = mode;
+    return SPHDEM_OK;
+}
+
+extern "C" int sphdem_get_list_build(SphdemHandle* h, int32_t* mode) {
+    if (!h || !mode || !h->committed || h->kind != 0) return SPHDEM_E_ARG;
+    *mode = h->prec == SPHDEM_PREC_FP64 ? ((EngineHost<double>*)h->eng)->list_mode
+                                        : ((EngineHost<float>*)h->eng)->list_mode;
+    return SPHDEM_OK;
+}
+
 extern "C" int sphdem_set_beds(SphdemHandle* h, int32_t nbeds, const SphdemBedRow* rows) {
     if (!h || !rows || h->committed || h->kind != 0) return SPHDEM_E_ARG;
     if (h->p.dim != 2 || h->p.solver_type != SPHDEM_ISPH) return SPHDEM_E_UNSUPPORTED;

@@ -46,6 +46,7 @@ struct SphdemHandle {
     // per-bed open-boundary rows of a handle of 2-D beds (sphdem_set_beds),
     // sorted by plane; on the device as BED_COLS doubles per row
     std::vector<SphdemBedRow> beds;
+    int list_build_req = 0;   // sphdem_set_list_build: 0 = tuned at commit
     double* d_beds = nullptr;
     bool dom_set = false;
     double dom_bbox[6] = {};

@@ -329,12 +329,16 @@ __device__ __forceinline__ double rel_band(const DevParams& P, const RelFrame& F
 // origin (|c|, |p| <= sqrt(3) L), so dot_band widens the band by
 // 80u (L / Rr)^2 + 2u of Rr^2.  Within the wider band the FP64 predicate
 // decides, so the lists are unchanged.
-constexpr int LT_WARPS = 4, LT_CH = 128;
+// LW cells (warps) per block: 2, 4 or 8, picked per handle at commit with
+// the one-thread-per-particle build (k_build_list) as the fourth candidate
+// (list_build_mode, engine.cu); all four write the same lists.
+constexpr int LT_CH = 128;
 __device__ __forceinline__ double dot_band(const RelFrame& F, double Rr) {
     const double u = 5.9604644775390625e-08, q = F.L / Rr;
     return 80.0 * u * q * q + 2.0 * u;
 }
-__global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P, SphState<float> S,
+template <int LW>
+__global__ void __launch_bounds__(LW * 32) k_build_list_tiled(DevParams P, SphState<float> S,
                                                                       SphRec<float> rec,
                                                                       const int* __restrict__ gs,
                                                                       const int* __restrict__ ge,
@@ -342,11 +346,11 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_build_list_tiled(DevParams P,
                                                                       int* __restrict__ nbr,
                                                                       int* __restrict__ ncnt, DevFlags* F) {
     grid_dep_wait();
-    __shared__ float4 sc[LT_WARPS][LT_CH + 4];   // relative x, y, z and |c|^2
-    __shared__ int sj[LT_WARPS][LT_CH + 4];      // slot, bit 31: not near the origin
-    __shared__ int srow[LT_WARPS][20];   // prefix[10] | start[9]
+    __shared__ float4 sc[LW][LT_CH + 4];   // relative x, y, z and |c|^2
+    __shared__ int sj[LW][LT_CH + 4];      // slot, bit 31: not near the origin
+    __shared__ int srow[LW][20];   // prefix[10] | start[9]
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * LT_WARPS + w;
+    const int c = blockIdx.x * LW + w;
     const int ncell = P.NI * P.NJ * P.NK;
     if (c >= ncell) return;
     const int a0 = __ldg(gs + c);

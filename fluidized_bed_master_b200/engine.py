@@ -59,6 +59,8 @@ def lib():
     L.sphdem_set_timing_only.argtypes = [vp, C.c_int]
     L.sphdem_set_domain.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double]
     L.sphdem_set_beds.argtypes = [vp, C.c_int32, C.POINTER(BedRow)]
+    L.sphdem_set_list_build.argtypes = [vp, C.c_int32]
+    L.sphdem_get_list_build.argtypes = [vp, C.POINTER(C.c_int32)]
     L.sphdem_slab_record_bytes.argtypes = [C.c_int]
     dp = C.POINTER(C.c_double)
     L.sphdem_bed_domain.argtypes = [vp, dp, dp, dp, dp, dp, C.c_int32, dp, dp, dp, dp, C.c_int32, dp, dp, dp]
@@ -154,12 +156,14 @@ class BedRow(C.Structure):
 class Engine:
     """One engine handle on the current CUDA device."""
 
-    def __init__(self, params, sph, dem, domain=None, beds=None):
+    def __init__(self, params, sph, dem, domain=None, beds=None, list_build=None):
         """params: SphdemParams; sph/dem: dict field-name -> array in input
         order.  domain: (bbox6, h0, t_ref) of a larger bed this one is a slab
         of (sphdem_set_domain; see bed_domain).  beds: rows (dicts with the
         BedRow fields) of several 2-D beds in their own planes y = const
-        (sphdem_set_beds; see beds.bed2d_batch)."""
+        (sphdem_set_beds; see beds.bed2d_batch).  list_build: the SPH
+        list build (sphdem_set_list_build: 1 per particle, 2/4/8 cells per
+        block with a warp per cell, None/0 timed at commit)."""
         L = lib()
         ns = len(sph["x"]) if sph else 0
         nd = len(dem["x"]) if dem else 0
@@ -172,6 +176,8 @@ class Engine:
             if domain is not None:
                 bb = (C.c_double * 6)(*[float(v) for v in domain[0]])
                 _chk(L.sphdem_set_domain(self._h, bb, float(domain[1]), float(domain[2])), "sphdem_set_domain")
+            if list_build is not None:
+                _chk(L.sphdem_set_list_build(self._h, int(list_build)), "sphdem_set_list_build")
             if beds is not None:
                 rows = (BedRow * len(beds))(*[BedRow(**{k: float(r[k]) for k, _ in BedRow._fields_}) for r in beds])
                 _chk(L.sphdem_set_beds(self._h, len(beds), rows), "sphdem_set_beds")
@@ -329,6 +335,12 @@ class Engine:
         sp = np.ascontiguousarray(springs, dtype=np.float64)
         _chk(lib().sphdem_set_history(self._h, ids.ctypes.data_as(C.POINTER(C.c_int32)),
                                       sp.ctypes.data_as(C.POINTER(C.c_double))), "sphdem_set_history")
+
+    def list_build(self):
+        """The SPH list build the handle runs (sphdem_get_list_build)."""
+        m = C.c_int32()
+        _chk(lib().sphdem_get_list_build(self._h, C.byref(m)), "sphdem_get_list_build")
+        return m.value
 
     def set_timing(self, on):
         _chk(lib().sphdem_set_timing(self._h, int(bool(on))), "sphdem_set_timing")

@@ -533,6 +533,16 @@ int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_
  * with the nearest y).  Replaces what KERNEL_open_boundary_extrapolation3D
  * (functions_BC.cuh:787-984) reads from k_vif and the slab tags of
  * c_initial_inner_outer_particle_single (functions_NNPS.cuh:60-200). */
+/* The SPH neighbour-list build of the step (KERNEL_index_particle_to_cell
+ * + the list walk of every gather pass, functions_NNPS.cuh): 1 = one thread
+ * per particle; 2, 4, 8 = one warp per cell, that many cells per block (FP32
+ * build); 0 (the default) = timed at commit on the committed state, the
+ * fastest kept.  Every mode writes the same lists in the same order, so the
+ * choice changes only the speed.  FP64 handles build one thread per
+ * particle.  Set before sphdem_commit_particles; read after it. */
+int sphdem_set_list_build(SphdemHandle* h, int32_t mode);
+int sphdem_get_list_build(SphdemHandle* h, int32_t* mode);
+
 #define SPHDEM_MAX_BEDS 4096
 typedef struct {
     double y;                                 /* the bed's plane */
