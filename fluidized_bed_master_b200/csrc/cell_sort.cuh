@@ -14,7 +14,8 @@
 //           the reference keys num_cells) -> start[]; resets fill[];
 //   scatter k_sort_scatter: tmp[start[k] + fill[k]++] = slot, one atomic
 //           per distinct key of a warp; order inside a cell is arbitrary;
-//   settle  k_sort_settle, one warp per bucket: ranks the bucket's slots by
+//   settle  k_sort_settle, one warp per bucket (per 32 buckets when the grid
+//           has more than twice as many cells as keys): ranks the bucket's slots by
 //           value (unique, so ranks are a permutation), writes perm/key in
 //           ascending slot order, the cell's start (-1 when empty) and end,
 //           and zeroes cnt[] for the next step.
@@ -172,26 +173,9 @@ __global__ void k_sort_scatter(int n, const int* __restrict__ key, const int* __
     if (k >= 0) tmp[start[k] + base + __popc(peers & ((1u << lane) - 1u))] = i;
 }
 
-// one warp per bucket b < nb; cell b < nb - 1 gets gs (start or -1) and ge
-// (end, written only for a non-empty cell, as the reference's reorder does)
-__global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
-                                                     const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
-                                                     int* ge, int skip_last) {
-    grid_dep_wait();
-    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (b >= nb) return;
-    const int m = cnt[b];
-    const int s = start[b];
-    __syncwarp();
-    if (lane == 0) {
-        cnt[b] = 0;
-        if (b < nb - 1) {
-            gs[b] = m ? s : -1;
-            if (m) ge[b] = s + m;
-        }
-    }
-    if (skip_last && b == nb - 1) return;
+// the ranking of one bucket of m >= 2 slots from s by a warp
+__device__ __forceinline__ void settle_bucket(int b, int m, int s, const int* __restrict__ tmp, int* perm,
+                                              int* key_out, int lane) {
     for (int a = 0; a < m; a += 32) {
         const int v = (a + lane < m) ? tmp[s + a + lane] : INT_MAX;
         int r = 0;
@@ -204,6 +188,44 @@ __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int
             perm[s + r] = v;
             key_out[s + r] = b;
         }
+    }
+}
+
+// G buckets per warp (G = 1, or 32 for a grid of mostly empty cells): lane
+// l < G owns bucket b = warp * G + l; cell b < nb - 1 gets gs (start or -1)
+// and ge (end, written only for a non-empty cell, as the reference's reorder
+// does).  A bucket of one slot is settled by its lane; the warp ranks the
+// buckets of two or more slots one after another.
+template <int G>
+__global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
+                                                     const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
+                                                     int* ge, int skip_last) {
+    grid_dep_wait();
+    const int b0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G;
+    const int lane = threadIdx.x & 31;
+    if (b0 >= nb) return;
+    const int bl = b0 + lane;
+    const bool own = lane < G && bl < nb;
+    const int ml = own ? cnt[bl] : 0;
+    const int sl = own ? start[bl] : 0;
+    __syncwarp();
+    if (own) {
+        if (ml) cnt[bl] = 0;
+        if (bl < nb - 1) {
+            gs[bl] = ml ? sl : -1;
+            if (ml) ge[bl] = sl + ml;
+        }
+        if (ml == 1 && !(skip_last && bl == nb - 1)) {
+            perm[sl] = tmp[sl];
+            key_out[sl] = bl;
+        }
+    }
+    unsigned multi = __ballot_sync(0xffffffffu, own && ml >= 2 && !(skip_last && bl == nb - 1));
+    while (multi) {
+        const int k = __ffs(multi) - 1;
+        multi &= multi - 1;
+        const int b = b0 + k, m = __shfl_sync(0xffffffffu, ml, k), s = __shfl_sync(0xffffffffu, sl, k);
+        settle_bucket(b, m, s, tmp, perm, key_out, lane);
     }
 }
 
@@ -268,9 +290,16 @@ inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* 
                                  cs.fill, cs.tmp)))
         return e;
     const int big = cs.big_last && n > 0;
-    if ((e = launch_pdl(k_sort_settle, (cs.nb * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt, (const int*)cs.start,
-                        (const int*)cs.tmp, perm, key_out, gs, ge, big)))
+    // a grid of mostly empty cells (e.g. 2-D beds in planes): 32 buckets per warp
+    if (cs.nb > 2 * n) {
+        const int nw = (cs.nb + 31) / 32;
+        if ((e = launch_pdl(k_sort_settle<32>, (nw * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt,
+                            (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big)))
+            return e;
+    } else if ((e = launch_pdl(k_sort_settle<1>, (cs.nb * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt,
+                               (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big))) {
         return e;
+    }
     if (big) {
         const int nblk = (n + 255) / 256;
         k_sort_last_count<<<nblk, 256, 0, st>>>(n, key_in, cs.nb - 1, cs.blk);
