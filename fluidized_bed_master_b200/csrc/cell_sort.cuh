@@ -14,8 +14,8 @@
 //           the reference keys num_cells) -> start[]; resets fill[];
 //   scatter k_sort_scatter: tmp[start[k] + fill[k]++] = slot, one atomic
 //           per distinct key of a warp; order inside a cell is arbitrary;
-//   settle  k_sort_settle, one warp per bucket (per 32 buckets when the grid
-//           has more than twice as many cells as keys): ranks the bucket's slots by
+//   settle  k_sort_settle, one warp per bucket (per 32 buckets on a sparse
+//           grid, cell_sort_sparse): ranks the bucket's slots by
 //           value (unique, so ranks are a permutation), writes perm/key in
 //           ascending slot order, the cell's start (-1 when empty) and end,
 //           and zeroes cnt[] for the next step.
@@ -74,7 +74,19 @@ struct CellSort {
     int ntiles;
     int big_last;    // the last bucket by compaction (blk: per-block counts)
     int* blk;
+    // On a sparse grid (cell_sort_sparse), the occupied cells (< nb - 1) in
+    // no particular order and their count, for the passes that take a warp
+    // per cell; null when not kept.
+    int* occ = nullptr;
+    int* occ_n = nullptr;
 };
+
+// A sparse grid (e.g. 2-D beds in planes): the settle pass takes 32 buckets
+// per warp and, where the sort keeps the list, lists the occupied cells.
+// Sparse means more cells than keys / 4 for a sort that lists its occupied
+// cells (the SPH set, whose warp-per-cell passes then skip the empty
+// cells), else more than twice as many cells as keys.
+inline bool cell_sort_sparse(const CellSort& cs, int n) { return cs.occ ? 4ll * cs.nb > n : cs.nb > 2ll * n; }
 
 // count one key (called by every thread of a warp that hashes; inactive
 // threads pass key < 0)
@@ -85,8 +97,10 @@ __device__ __forceinline__ void cell_count(int* cnt, int key) {
     if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[key], __popc(peers));
 }
 
-__global__ void __launch_bounds__(1024) k_sort_tile_sums(const int* __restrict__ cnt, int nb, int* tile_sum) {
+__global__ void __launch_bounds__(1024) k_sort_tile_sums(const int* __restrict__ cnt, int nb, int* tile_sum,
+                                                         int* occ_n) {
     grid_dep_wait();
+    if (occ_n && blockIdx.x == 0 && threadIdx.x == 0) *occ_n = 0;   // refilled by the settle pass
     const int base = blockIdx.x * SORT_TILE + threadIdx.x * 4;
     int s = 0;
 #pragma unroll
@@ -199,7 +213,7 @@ __device__ __forceinline__ void settle_bucket(int b, int m, int s, const int* __
 template <int G>
 __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int* __restrict__ start,
                                                      const int* __restrict__ tmp, int* perm, int* key_out, int* gs,
-                                                     int* ge, int skip_last) {
+                                                     int* ge, int skip_last, int* occ, int* occ_n) {
     grid_dep_wait();
     const int b0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G;
     const int lane = threadIdx.x & 31;
@@ -219,6 +233,14 @@ __global__ void __launch_bounds__(256) k_sort_settle(int nb, int* cnt, const int
             perm[sl] = tmp[sl];
             key_out[sl] = bl;
         }
+    }
+    if (occ) {   // append the warp's occupied cells
+        const bool oc = own && ml > 0 && bl < nb - 1;
+        const unsigned om = __ballot_sync(0xffffffffu, oc);
+        int base = 0;
+        if (om && lane == 0) base = atomicAdd(occ_n, __popc(om));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (oc) occ[base + __popc(om & ((1u << lane) - 1u))] = bl;
     }
     unsigned multi = __ballot_sync(0xffffffffu, own && ml >= 2 && !(skip_last && bl == nb - 1));
     while (multi) {
@@ -282,7 +304,10 @@ __global__ void __launch_bounds__(256) k_sort_last_write(int n, const int* __res
 inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* perm, int* key_out, int* gs, int* ge,
                              cudaStream_t st) {
     cudaError_t e;
-    if ((e = launch_pdl(k_sort_tile_sums, cs.ntiles, 1024, 0, st, (const int*)cs.cnt, cs.nb, cs.tile_sum))) return e;
+    const bool sparse = cell_sort_sparse(cs, n);
+    int* occ_n = sparse ? cs.occ_n : nullptr;
+    if ((e = launch_pdl(k_sort_tile_sums, cs.ntiles, 1024, 0, st, (const int*)cs.cnt, cs.nb, cs.tile_sum, occ_n)))
+        return e;
     if ((e = launch_pdl(k_sort_scan, cs.ntiles, 1024, 0, st, (const int*)cs.cnt, (const int*)cs.tile_sum, cs.nb,
                         cs.start, cs.fill)))
         return e;
@@ -291,13 +316,15 @@ inline cudaError_t cell_sort(const CellSort& cs, int n, const int* key_in, int* 
         return e;
     const int big = cs.big_last && n > 0;
     // a grid of mostly empty cells (e.g. 2-D beds in planes): 32 buckets per warp
-    if (cs.nb > 2 * n) {
+    if (sparse) {
         const int nw = (cs.nb + 31) / 32;
         if ((e = launch_pdl(k_sort_settle<32>, (nw * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt,
-                            (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big)))
+                            (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big,
+                            occ_n ? cs.occ : (int*)nullptr, occ_n)))
             return e;
     } else if ((e = launch_pdl(k_sort_settle<1>, (cs.nb * 32 + 255) / 256, 256, 0, st, cs.nb, cs.cnt,
-                               (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big))) {
+                               (const int*)cs.start, (const int*)cs.tmp, perm, key_out, gs, ge, big,
+                               (int*)nullptr, (int*)nullptr))) {
         return e;
     }
     if (big) {

@@ -503,6 +503,24 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
 }
 
 // SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
+// warps of a grid-stride pass over the occupied cells of a sparse grid: at
+// most one per SPH particle, at most 128 per SM
+inline int occ_warps(const DevParams& P) { return std::max(1, std::min(P.ns, 148 * 128)); }
+
+// the tiled wall pass (FP32): a warp per cell, or per occupied cell on a sparse grid
+inline cudaError_t launch_neumann_tiled(Engine<float>& E, const SphState<float>& S, float* pres, int patch_up,
+                                        cudaStream_t st) {
+    const DevParams& P = E.P;
+    SphWork<float>& W = E.sw;
+    if (cell_sort_sparse(E.cs_s, P.ns))
+        return launch_pdl(k_neumann_tiled<true>, (occ_warps(P) + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st, P,
+                          S, W, pres, (const int*)W.g_str, (const int*)W.g_end, (const int4*)W.rows, patch_up,
+                          (const int*)E.cs_s.occ, (const int*)E.cs_s.occ_n);
+    return launch_pdl(k_neumann_tiled<false>, (P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st,
+                      P, S, W, pres, (const int*)W.g_str, (const int*)W.g_end, (const int4*)W.rows, patch_up,
+                      (const int*)nullptr, (const int*)nullptr);
+}
+
 template <typename R>
 cudaError_t launch_list(EngineHost<R>* EH, const SphState<R>& S, int mode, cudaStream_t st) {
     Engine<R>& E = EH->E;
@@ -577,9 +595,13 @@ cudaError_t launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState
     Engine<R>& E = EH->E;
     const DevParams& P = E.P;
     const int ncell = P.NI * P.NJ * P.NK;
-    return launch_pdl(k_build_dlist, (ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P, S.x, S.y, S.z,
-                      S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
-                      P.nbd_cap, E.flags);
+    if (cell_sort_sparse(E.cs_s, P.ns))   // the occupied cells, a warp each, grid-stride
+        return launch_pdl(k_build_dlist<true>, (occ_warps(P) + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P,
+                          S.x, S.y, S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd,
+                          E.sw.ncntd, P.nbd_cap, E.flags, (const int*)E.cs_s.occ, (const int*)E.cs_s.occ_n);
+    return launch_pdl(k_build_dlist<false>, (ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P, S.x, S.y,
+                      S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
+                      P.nbd_cap, E.flags, (const int*)nullptr, (const int*)nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -688,8 +710,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         if (flags & F_COUNT0) {
             KTIME(KT_NEUMANN0);
             if constexpr (std::is_same<R, float>::value)
-                CK((launch_pdl(k_neumann_tiled, (P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st, 
-                    P, S, W, S.pres, W.g_str, W.g_end, W.rows, 1)));
+                CK(launch_neumann_tiled(E, S, S.pres, 1, st));
             else
                 CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, S.pres, W.rows, 1)));
             *nl += 1;
@@ -702,8 +723,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         {
             KTIME(KT_NEUMANN);
             if constexpr (std::is_same<R, float>::value)
-                CK((launch_pdl(k_neumann_tiled, (P.NI * P.NJ * P.NK + NT_WARPS - 1) / NT_WARPS, NT_WARPS * 32, 0, st, 
-                    P, S, W, W.p_new, W.g_str, W.g_end, W.rows, 0)));
+                CK(launch_neumann_tiled(E, S, W.p_new, 0, st));
             else
                 CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, W.p_new, W.rows, 0)));
         }
@@ -920,6 +940,9 @@ static int commit_t(SphdemHandle* H) {
     E.cur_s = 0; E.cur_d = 0;
     // cell sort scratch of both sets (zeroed by the allocator, as cell_sort expects)
     E.cs_s = alloc_cell_sort(A, num_cells, ns);
+    // the occupied SPH cells, for the warp-per-cell passes on a sparse grid
+    E.cs_s.occ = A.get<int>((size_t)ns + 1);
+    E.cs_s.occ_n = A.get<int>(1);
     E.cs_d = alloc_cell_sort(A, num_cells, nd);
     // a slab's parked spare slots all sort into the last bucket
     E.cs_s.big_last = E.cs_d.big_last = H->dom_set ? 1 : 0;

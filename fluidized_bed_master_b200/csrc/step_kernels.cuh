@@ -533,7 +533,8 @@ __global__ void __launch_bounds__(LW * 32) k_build_list_tiled(DevParams P, SphSt
 // than cap hits keeps only its count, and the consumers walk its stencil
 // instead.
 constexpr int DL_WARPS = 4, DL_CH = 128;
-__global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, const double* __restrict__ sx,
+// one cell of k_build_dlist (scw, srw: the warp's shared staging)
+__device__ __forceinline__ void dlist_cell(int c, DevParams P, const double* __restrict__ sx,
                                                                  const double* __restrict__ sy,
                                                                  const double* __restrict__ sz,
                                                                  const double* __restrict__ sh,
@@ -543,18 +544,11 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
                                                                  const double* __restrict__ dy,
                                                                  const double* __restrict__ dz,
                                                                  const int* __restrict__ dptype, int* __restrict__ nbrd,
-                                                                 int* __restrict__ ncntd, int cap, DevFlags* F) {
-    grid_dep_wait();
-    __shared__ float4 sc[DL_WARPS][DL_CH + 32];
-    __shared__ int srow[DL_WARPS][20];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * DL_WARPS + w;
-    if (c >= P.NI * P.NJ * P.NK) return;
-    const int a0 = __ldg(gs + c);
+                                                                 int* __restrict__ ncntd, int cap, DevFlags* F, float4* scw, int* srw, int lane) {    const int a0 = __ldg(gs + c);
     if (a0 < 0) return;
     const int e0 = __ldg(ge + c);
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
-    const int tot = stage_rows(P, ic, jc, kc, drows, srow[w], lane);
+    const int tot = stage_rows(P, ic, jc, kc, drows, srw, lane);
     const int n = P.ns;
     const double x0 = sx[a0], y0 = sy[a0], z0 = sz[a0];
     const double Lb = 4.0 * fmax(fmax((P.xmax - P.xmin) / P.NI, (P.ymax - P.ymin) / P.NJ), (P.zmax - P.zmin) / P.NK);
@@ -592,7 +586,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
                 int j = 0;
                 bool keep = false;
                 if (tl < tot) {
-                    j = row_slot(srow[w], tl);
+                    j = row_slot(srw, tl);
                     keep = __ldg(dptype + j) > 1000;
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -600,7 +594,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
                     const double ux = dx[j] - x0, uy = dy[j] - y0, uz = dz[j] - z0;
                     const bool far = !(fabs(ux) <= Lb && fabs(uy) <= Lb && fabs(uz) <= Lb);
                     any_far |= far;
-                    sc[w][ns + __popc(m & lt)] =
+                    scw[ns + __popc(m & lt)] =
                         make_float4((float)ux, (float)uy, (float)uz, __int_as_float(j | (far ? (int)0x80000000 : 0)));
                 }
                 ns += __popc(m);
@@ -610,7 +604,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
             __syncwarp();
             if (act) {
                 for (int u = 0; u < ns; u++) {
-                    const float4 cj = sc[w][u];
+                    const float4 cj = scw[u];
                     const int jb = __float_as_int(cj.w), j = jb & 0x7fffffff;
                     bool hit;
                     if (!slow_chunk || (!slow && jb >= 0)) {
@@ -633,6 +627,36 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
         if (act) ncntd[i] = cnt;
         const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
         if (lane == 0 && wmax > 0) atomicMax(&F->max_ncntd, wmax);
+    }
+}
+
+template <bool OCC>
+__global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, const double* __restrict__ sx,
+                                                                 const double* __restrict__ sy,
+                                                                 const double* __restrict__ sz,
+                                                                 const double* __restrict__ sh,
+                                                                 const int* __restrict__ gs, const int* __restrict__ ge,
+                                                                 const int4* __restrict__ drows,
+                                                                 const double* __restrict__ dx,
+                                                                 const double* __restrict__ dy,
+                                                                 const double* __restrict__ dz,
+                                                                 const int* __restrict__ dptype, int* __restrict__ nbrd,
+                                                                 int* __restrict__ ncntd, int cap, DevFlags* F,
+                                                                 const int* __restrict__ occ, const int* __restrict__ occ_n) {
+    grid_dep_wait();
+    __shared__ float4 sc[DL_WARPS][DL_CH + 32];
+    __shared__ int srow[DL_WARPS][20];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if constexpr (OCC) {   // a sparse grid: the occupied cells, grid-stride
+        const int no = *occ_n;
+        for (int q = blockIdx.x * DL_WARPS + w; q < no; q += gridDim.x * DL_WARPS) {
+            dlist_cell(occ[q], P, sx, sy, sz, sh, gs, ge, drows, dx, dy, dz, dptype, nbrd, ncntd, cap, F, sc[w], srow[w], lane);
+            __syncwarp();
+        }
+    } else {
+        const int c = blockIdx.x * DL_WARPS + w;
+        if (c < P.NI * P.NJ * P.NK)
+            dlist_cell(c, P, sx, sy, sz, sh, gs, ge, drows, dx, dy, dz, dptype, nbrd, ncntd, cap, F, sc[w], srow[w], lane);
     }
 }
 
@@ -1742,18 +1766,11 @@ __global__ void __launch_bounds__(128) k_neumann(DevParams P, SphState<R> S, Sph
 // reference predicate inside the band.  Same sums as k_neumann in candidate
 // order per wall, so the FP32 results differ from it by rounding only.
 constexpr int NT_WARPS = 4, NT_CH = 128;
-__global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
+// one cell of k_neumann_tiled (saw, sbw, srw: the warp's shared staging)
+__device__ __forceinline__ void neumann_cell(int c, DevParams P, SphState<float> S, SphWork<float> W,
                                                                    float* pres, const int* __restrict__ gs,
                                                                    const int* __restrict__ ge,
-                                                                   const int4* __restrict__ rows, int patch_up) {
-    grid_dep_wait();
-    __shared__ float4 sa[NT_WARPS][NT_CH + 32];
-    __shared__ float4 sb[NT_WARPS][NT_CH + 32];
-    __shared__ int srow[NT_WARPS][20];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * NT_WARPS + w;
-    if (c >= P.NI * P.NJ * P.NK) return;
-    const int a0 = __ldg(gs + c);
+                                                                   const int4* __restrict__ rows, int patch_up, float4* saw, float4* sbw, int* srw, int lane) {    const int a0 = __ldg(gs + c);
     if (a0 < 0) return;
     const int e0 = __ldg(ge + c);
     const SphRec<float> rec = W.rec;
@@ -1761,7 +1778,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
     for (int i = a0 + lane; i < e0; i += 32) any_wall |= S.ptype[i] <= 0;
     if (!__any_sync(0xffffffffu, any_wall)) return;
     const int ic = c % P.NI, jc = (c / P.NI) % P.NJ, kc = c / (P.NI * P.NJ);
-    const int tot = stage_rows(P, ic, jc, kc, rows, srow[w], lane);
+    const int tot = stage_rows(P, ic, jc, kc, rows, srw, lane);
     const RelFrame Fr = rel_frame(P, ldr(rec.pos + a0));
     const unsigned lt = (1u << lane) - 1u;
     for (int p0 = a0; p0 < e0; p0 += 32) {
@@ -1806,7 +1823,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                 int4 qj = make_int4(0, 0, 0, 0);
                 int j = 0;
                 if (tl < tot) {
-                    j = row_slot(srow[w], tl);
+                    j = row_slot(srw, tl);
                     qj = ldr(rec.pos + j);
                     const int ptj = tag_ptype(qj.w);
                     keep = ptj >= 1 && ptj < 1000;
@@ -1818,8 +1835,8 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                     any_oor |= oor;
                     const float4 fj = ldr(rec.f1 + j);
                     const float mr = fj.x * rcp(fj.y);
-                    sa[w][pos] = rel_coord(Fr, qj, j | (oor ? (int)0x80000000 : 0));
-                    sb[w][pos] = make_float4(mr, pres[j], fj.z, fj.x * rcp(fj.w));
+                    saw[pos] = rel_coord(Fr, qj, j | (oor ? (int)0x80000000 : 0));
+                    sbw[pos] = make_float4(mr, pres[j], fj.z, fj.x * rcp(fj.w));
                 }
                 ns += __popc(m);
                 t += 32;
@@ -1836,7 +1853,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                 const float hq = 0.5f * K.ih;
 #pragma unroll 4
                 for (int u = 0; u < ns; u++) {
-                    const float4 cj = sa[w][u];
+                    const float4 cj = saw[u];
                     const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
                     const float r2 = dx * dx + dy * dy + dz * dz;
                     bool in = r2 < lo2;
@@ -1847,7 +1864,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                     const float q = r2 * rsqrtf(fmaxf(r2, 1e-30f)) * hq;
                     const float a = 1.f - q, a2 = a * a;
                     const float wk = a2 * a2 * (1.f + 4.f * q);
-                    const float4 bj = sb[w][u];
+                    const float4 bj = sbw[u];
                     if (in && q < 1.f) {
                         const float mr = bj.x * wk;
                         tp += mr * bj.y;
@@ -1861,7 +1878,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                 // as above, any kernel
 #pragma unroll 2
                 for (int u = 0; u < ns; u++) {
-                    const float4 cj = sa[w][u];
+                    const float4 cj = saw[u];
                     const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
                     const float r2 = dx * dx + dy * dy + dz * dz;
                     bool in = r2 < lo2;
@@ -1872,7 +1889,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                     float r, rinv;
                     rdist(r2, r, rinv);
                     const float wk = kw(K, r);
-                    const float4 bj = sb[w][u];
+                    const float4 bj = sbw[u];
                     if (in) {
                         const float mr = bj.x * wk;
                         tp += mr * bj.y;
@@ -1883,7 +1900,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                 }
             } else if (act) {
                 for (int u = 0; u < ns; u++) {
-                    const float4 cj = sa[w][u];
+                    const float4 cj = saw[u];
                     const float dx = fx - cj.x, dy = fy - cj.y, dz = fz - cj.z;
                     const float r2 = dx * dx + dy * dy + dz * dz;
                     bool in;
@@ -1914,7 +1931,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
                         rdist(ex * ex + ey * ey + ez * ez, r, rinv);
                     }
                     const float wk = kw(K, r);
-                    const float4 bj = sb[w][u];
+                    const float4 bj = sbw[u];
                     const float mr = bj.x * wk;
                     tp += mr * bj.y;
                     flt += mr;
@@ -1938,6 +1955,29 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
         W.rho_new[i] = rw;
         *comp<float>(rec.f1, i, 1) = rw;
         if (patch_up) *comp<float>(rec.up, i, 3) = pw;
+    }
+}
+
+template <bool OCC>
+__global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P, SphState<float> S, SphWork<float> W,
+                                                                   float* pres, const int* __restrict__ gs,
+                                                                   const int* __restrict__ ge,
+                                                                   const int4* __restrict__ rows, int patch_up,
+                                                                   const int* __restrict__ occ, const int* __restrict__ occ_n) {
+    grid_dep_wait();
+    __shared__ float4 sa[NT_WARPS][NT_CH + 32];
+    __shared__ float4 sb[NT_WARPS][NT_CH + 32];
+    __shared__ int srow[NT_WARPS][20];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if constexpr (OCC) {   // a sparse grid: the occupied cells, grid-stride
+        const int no = *occ_n;
+        for (int q = blockIdx.x * NT_WARPS + w; q < no; q += gridDim.x * NT_WARPS) {
+            neumann_cell(occ[q], P, S, W, pres, gs, ge, rows, patch_up, sa[w], sb[w], srow[w], lane);
+            __syncwarp();
+        }
+    } else {
+        const int c = blockIdx.x * NT_WARPS + w;
+        if (c < P.NI * P.NJ * P.NK) neumann_cell(c, P, S, W, pres, gs, ge, rows, patch_up, sa[w], sb[w], srow[w], lane);
     }
 }
 
