@@ -639,6 +639,8 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     // Wendland C2 (the default): the neighbour passes are instantiated with
     // the kernel type fixed
     const bool kt3 = P.kernel_type == 3;
+    // ... and, for the common switch set, with the switches fixed too
+    const bool swc = kt3 && switch_set(P) == SW_COMMON;
     const bool fork = H->concurrent && ns > 0 && nd > 0 && H->dem_stream;
     cudaStream_t sd = fork ? H->dem_stream : st;
     // event k recorded on stream a / waited for on stream b (fork only)
@@ -671,7 +673,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             CK(launch_list<R>(EH, S, EH->list_mode, st));
         }
         CK(wait(1, st));
-        { KTIME(KT_PASSA); CK((launch_pdl(kt3 ? k_passA<R, 3> : k_passA<R, -1>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
+        { KTIME(KT_PASSA); CK((launch_pdl(swc ? k_passA<R, 3, SW_COMMON> : kt3 ? k_passA<R, 3, -1> : k_passA<R, -1, -1>, bs, TPB, 0, st, P, S, W, D, DW.rows))); }
         *nl += 2;
         {
             KTIME(KT_PASSB);
@@ -679,8 +681,8 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
                 CK((launch_pdl(kt3 ? k_sps<R, 3> : k_sps<R, -1>, bs, TPB, 0, st, P, S, W)));
                 *nl += 1;
             }
-            if (P.iface | P.fb | P.sps | P.ipf) CK((launch_pdl(kt3 ? k_passB<R, true, 3> : k_passB<R, true, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
-            else CK((launch_pdl(kt3 ? k_passB<R, false, 3> : k_passB<R, false, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
+            if (P.iface | P.fb | P.sps | P.ipf) CK((launch_pdl(kt3 ? k_passB<R, true, 3, -1> : k_passB<R, true, -1, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
+            else CK((launch_pdl(swc ? k_passB<R, false, 3, SW_COMMON> : kt3 ? k_passB<R, false, 3, -1> : k_passB<R, false, -1, -1>, bs, TPB, 0, st, P, S, W, E.flags)));
         }
         *nl += 1;
     }
@@ -717,7 +719,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
         }
         {
             KTIME(KT_PPE);
-            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) CK((launch_pdl(kt3 ? k_ppe<R, 3> : k_ppe<R, -1>, bs, TPB, 0, st, P, S, W)));
+            if (H->p.ppe_mode == SPHDEM_PPE_REFERENCE) CK((launch_pdl(swc ? k_ppe<R, 3, SW_COMMON> : kt3 ? k_ppe<R, 3, -1> : k_ppe<R, -1, -1>, bs, TPB, 0, st, P, S, W)));
             else if ((r = enqueue_krylov<R>(H, EH, S, W))) return r;
         }
         {
@@ -727,7 +729,7 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
             else
                 CK((launch_pdl(k_neumann<R>, bww, TPB, 0, st, P, S, W, W.p_new, W.rows, 0)));
         }
-        { KTIME(KT_PASSC); CK((launch_pdl(kt3 ? k_passC<R, 3> : k_passC<R, -1>, bs, TPB, 0, st, P, S, W))); }
+        { KTIME(KT_PASSC); CK((launch_pdl(swc ? k_passC<R, 3, SW_COMMON> : kt3 ? k_passC<R, 3, -1> : k_passC<R, -1, -1>, bs, TPB, 0, st, P, S, W))); }
         *nl += 3;
         if (P.open_bc > 0) {
             KTIME(KT_OPENBC);

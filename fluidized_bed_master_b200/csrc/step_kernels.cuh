@@ -69,6 +69,23 @@ __device__ __forceinline__ R sph_volume(const DevParams& P, R th, R hd) {
     return P.dim == 2 ? (th / hd) * (th / hd) : (th / hd) * (th / hd) * (th / hd);
 }
 
+// The solver switches the neighbour loops test per pair (gradient
+// correction, pressure, viscous and artificial-viscosity forces, heat,
+// Lagrangian SPH), fixed at compile time for the common set (SW_COMMON:
+// KGC, pressure and viscous forces and heat on, Eulerian) so those loops
+// carry no switch tests; SW = -1 reads them from DevParams.
+constexpr int SW_KGC = 1, SW_FP = 2, SW_FV = 4, SW_FVA = 8, SW_CON = 16, SW_LAGR = 32;
+constexpr int SW_COMMON = SW_KGC | SW_FP | SW_FV | SW_CON;
+template <int SW>
+__device__ __forceinline__ bool sw_on(int bit, bool runtime) {
+    if constexpr (SW < 0) return runtime;
+    else return (SW & bit) != 0;
+}
+inline int switch_set(const DevParams& P) {
+    return (P.kgc == 1 ? SW_KGC : 0) | (P.fp ? SW_FP : 0) | (P.fv ? SW_FV : 0) | (P.fva ? SW_FVA : 0) |
+           (P.con ? SW_CON : 0) | (P.sph_lagrangian ? SW_LAGR : 0);
+}
+
 // 27-cell stencil in the reference order (z,y,x), calling f(j) for every
 // slot j of every non-empty cell: the 9 rows in order, ascending slots
 // inside a row.
@@ -668,7 +685,7 @@ __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, cons
 // Neighbours read the start-of-step m, rho; the new m, rho go to m_new,
 // rho_new so that no thread sees a half-updated neighbour.
 // ---------------------------------------------------------------------------
-template <typename R, int KT>
+template <typename R, int KT, int SW>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                const int4* __restrict__ drows) {
     grid_dep_wait();
@@ -693,7 +710,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_passA(DevParams
     int cnt = min(W.ncnt[i], P.nb_cap);
     R txx = 0, tyy = 0, tzz = 0, txy = 0, tyz = 0, tzx = 0, sflt = 0;
     const int* __restrict__ nb = W.nbr;
-    const bool kgc = P.kgc == 1;
+    const bool kgc = sw_on<SW>(SW_KGC, P.kgc == 1);
     nb_walk<4, NbQ2<R>>(
         cnt, nb, n, i,
         [&](int j) {
@@ -958,7 +975,7 @@ __global__ void __launch_bounds__(128) k_sps(DevParams P, SphState<R> S, SphWork
 // FORCES: one of the interface-sharpness force, the repulsive boundary
 // force, the SPS eddy viscosity or the inter-particle surface tension is on
 // (a separate instantiation, so that the default pass keeps its registers)
-template <typename R, bool FORCES, int KT>
+template <typename R, bool FORCES, int KT, int SW>
 __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWork<R> W, const DevFlags* F) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -982,11 +999,11 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     R uxi = upi.x, uyi = upi.y, uzi = upi.z, pi = upi.w;
     R rhoi = fi.y, tempi = fi.z, pori = fi.w, mi = fi.x;
     R irhoi = rcp(rhoi);
-    const bool kgc = P.kgc == 1;
+    const bool kgc = sw_on<SW>(SW_KGC, P.kgc == 1);
     Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
     R vis = (R)P.mu_gas, vis_h = (vis * vis) / (vis + vis);
     R kc = (R)P.k_sph;
-    R eli = P.sph_lagrangian ? (R)1 : (R)0;
+    R eli = sw_on<SW>(SW_LAGR, P.sph_lagrangian != 0) ? (R)1 : (R)0;
     // per-particle factors of the pair terms
     R cp_i = -pori * irhoi * (rhoi / pori);      // rho_i/eps_i * (-eps_i / rho_i)
     R cv_i = vis_h * (R)4 * pori * irhoi;
@@ -1018,13 +1035,13 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
             R gx = dw * g.dx * rinv, gy = dw * g.dy * rinv, gz = dw * g.dz * rinv;
             cm_apply(Cm, kgc, gx, gy, gz);
             R tj = fj.z;
-            if (P.fp) {
+            if (sw_on<SW>(SW_FP, P.fp != 0)) {
                 R s = cp_i * mj * (pi + uj.w) * irj;
                 px += s * gx;
                 py += s * gy;
                 pz += s * gz;
             }
-            if (P.fv) {
+            if (sw_on<SW>(SW_FV, P.fv != 0)) {
                 R cv = cv_i;
                 if (FORCES && P.sps) {
                     // harmonic mean of the two particles' viscosity + vis_t
@@ -1036,7 +1053,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                 ty += Cv * (uyi - uj.y);
                 tz += Cv * (uzi - uj.z);
             }
-            if (P.fva) {
+            if (sw_on<SW>(SW_FVA, P.fva != 0)) {
                 R uij = (uxi - uj.x) * g.dx + (uyi - uj.y) * g.dy + (uzi - uj.z) * g.dz;
                 if (uij < (R)0) {
                     R hij = (th + th) * (R)0.5;
@@ -1089,9 +1106,9 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
                 ex += (uj.x - uxi) * ug * mr;
                 ey += (uj.y - uyi) * ug * mr;
                 ez += (uj.z - uzi) * ug * mr;
-                if (P.con) et += (tj - tempi) * ug * mr;
+                if (sw_on<SW>(SW_CON, P.con != 0)) et += (tj - tempi) * ug * mr;
             }
-            if (P.con) Rc += ch_i * mj * (tempi - tj) * dw * irj * rcp(r + (R)1e-10);
+            if (sw_on<SW>(SW_CON, P.con != 0)) Rc += ch_i * mj * (tempi - tj) * dw * irj * rcp(r + (R)1e-10);
         });
     if (filt) S.flt_s[i] = flt;
     if (!adv) return;
@@ -1103,7 +1120,7 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
     W.pgfx[i] = px;
     W.pgfy[i] = py;
     W.pgfz[i] = pz;
-    if (P.con) W.dtemp[i] = Rc / (R)P.cp_sph * (R)(pt != -1) - et;
+    if (sw_on<SW>(SW_CON, P.con != 0)) W.dtemp[i] = Rc / (R)P.cp_sph * (R)(pt != -1) - et;
 }
 
 // ---------------------------------------------------------------------------
@@ -1986,7 +2003,7 @@ __global__ void __launch_bounds__(NT_WARPS * 32, 8) k_neumann_tiled(DevParams P,
 // 868-878): one Jacobi sweep; p_new = (b + sum A_ij p_j) / sum A_ij for
 // fluid, every other particle keeps its pressure.
 // ---------------------------------------------------------------------------
-template <typename R, int KT>
+template <typename R, int KT, int SW>
 __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2007,7 +2024,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
     R uxi = upi.x, uyi = upi.y, uzi = upi.z, rhoi = fi.y, pori = fi.w;
     R irhoi = rcp(rhoi), prhoi = pori * rhoi;
     R pux = pori * uxi, puy = pori * uyi, puz = pori * uzi;
-    const bool kgc = P.kgc == 1;
+    const bool kgc = sw_on<SW>(SW_KGC, P.kgc == 1);
     Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
     int cnt = min(W.ncnt[i], P.nb_cap);
     R bx = 0, by = 0, bz = 0, A = 0, AP = 0;
@@ -2050,7 +2067,7 @@ __global__ void __launch_bounds__(128) k_ppe(DevParams P, SphState<R> S, SphWork
 // pass C: KERNEL_pressureforce3D_sph (functions_PPE2.cuh:2154-2335) and
 // KERNEL_time_update_projection_sph (functions_TIME_ISPH2.cuh:467-620).
 // ---------------------------------------------------------------------------
-template <typename R, int KT>
+template <typename R, int KT, int SW>
 __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWork<R> W) {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2065,13 +2082,13 @@ __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWo
     }
     R fx = 0, fy = 0, fz = 0;
     bool pf = !(P.open_bc > 0 && bt > 0) && pt < 1000 && pt > 0;
-    if (pf && P.fp) {
+    if (pf && sw_on<SW>(SW_FP, P.fp != 0)) {
         R th = (R)S.h[i];
         Knl<R, KT> K = knl_make<R, KT>(P, th);
         PosRec<R> qi = ldr(rec.pos + i);
         R pi = W.p_new[i], rhoi = W.rho_new[i], pori = rec.f1[i].w;
         R cpi = -pori * rcp(rhoi);
-        const bool kgc = P.kgc == 1;
+        const bool kgc = sw_on<SW>(SW_KGC, P.kgc == 1);
         Cm9<R> Cm = cm_load(W.Cm, n, i, kgc);
         int cnt = min(W.ncnt[i], P.nb_cap);
         const int* __restrict__ nb = W.nbr;
@@ -2119,14 +2136,14 @@ __global__ void __launch_bounds__(128) k_passC(DevParams P, SphState<R> S, SphWo
     if ((uxc * uxc + uyc * uyc + uzc * uzc) >= lim * lim) {
         uxc = ux0; uyc = uy0; uzc = uz0;
     }
-    if (!P.xsph && P.sph_lagrangian && pt > 0) {
+    if (!P.xsph && sw_on<SW>(SW_LAGR, P.sph_lagrangian != 0) && pt > 0) {
         S.x[i] += ((double)W.ux0[i] + (double)uxc) / 2.0 * P.sdt;
         S.y[i] += ((double)W.uy0[i] + (double)uyc) / 2.0 * P.sdt;
         S.z[i] += ((double)W.uz0[i] + (double)uzc) / 2.0 * P.sdt;
     }
     S.ux[i] = uxc; S.uy[i] = uyc; S.uz[i] = uzc;
     R tn = S.temp[i];
-    if (P.con && pt > 0) {
+    if (sw_on<SW>(SW_CON, P.con != 0) && pt > 0) {
         tn = W.temp0[i] + W.dtemp[i] * dt * (R)(pt != -1);
         S.temp[i] = tn;
     }
