@@ -128,6 +128,9 @@ struct EngineHost {
     // SPH list build: 1 = one thread per particle (k_build_list); 2, 4, 8 =
     // one warp per cell, that many cells per block (k_build_list_tiled, FP32)
     int list_mode = 1;
+    // SPH -> DEM list: false = a warp per cell (k_build_dlist), true = a
+    // thread per particle (k_build_dlist_pp); picked at commit by timing
+    bool dlist_pp = false;
     size_t list_elems = 0;
     MgWork mg{};             // two-level PCG preconditioner (ppe_precond TWO_LEVEL)
     bool has_mg = false;
@@ -595,6 +598,10 @@ cudaError_t launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState
     Engine<R>& E = EH->E;
     const DevParams& P = E.P;
     const int ncell = P.NI * P.NJ * P.NK;
+    if (EH->dlist_pp)
+        return launch_pdl(k_build_dlist_pp, nblocks(P.ns, TPB), TPB, 0, st, P, S.x, S.y, S.z, S.h,
+                          (const int*)S.itype, (const int4*)E.dw.rows, D.x, D.y, D.z, (const int*)D.ptype, E.sw.nbrd,
+                          E.sw.ncntd, P.nbd_cap, E.flags);
     if (cell_sort_sparse(E.cs_s, P.ns))   // the occupied cells, a warp each, grid-stride
         return launch_pdl(k_build_dlist<true>, (occ_warps(P) + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P,
                           S.x, S.y, S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd,
@@ -602,6 +609,38 @@ cudaError_t launch_dlist(EngineHost<R>* EH, const SphState<R>& S, const DemState
     return launch_pdl(k_build_dlist<false>, (ncell + DL_WARPS - 1) / DL_WARPS, DL_WARPS * 32, 0, st, P, S.x, S.y,
                       S.z, S.h, E.sw.g_str, E.sw.g_end, E.dw.rows, D.x, D.y, D.z, D.ptype, E.sw.nbrd, E.sw.ncntd,
                       P.nbd_cap, E.flags, (const int*)nullptr, (const int*)nullptr);
+}
+
+// The SPH -> DEM list build, picked at commit like the SPH list's: a thread
+// per particle against a warp per cell (each once untimed, three times
+// timed); both write the same list.  sphdem_set_list_build fixes it with
+// the SPH list's mode (1: per particle; 2, 4, 8: per cell).
+template <typename R>
+int tune_dlist(SphdemHandle* H, EngineHost<R>* EH, const SphState<R>& S, const DemState<double>& D) {
+    if (H->list_build_req != 0) {
+        EH->dlist_pp = H->list_build_req == 1;
+        return SPHDEM_OK;
+    }
+    cudaStream_t st = H->stream;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float ms[2] = {0, 0};
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < 2 && e == cudaSuccess; c++) {
+        EH->dlist_pp = c == 1;
+        if ((e = launch_dlist<R>(EH, S, D, st)) != cudaSuccess) break;
+        if ((e = cudaEventRecord(a, st)) != cudaSuccess) break;
+        for (int k = 0; k < 3 && e == cudaSuccess; k++) e = launch_dlist<R>(EH, S, D, st);
+        if (e != cudaSuccess || (e = cudaEventRecord(b, st)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(b)) != cudaSuccess) break;
+        e = cudaEventElapsedTime(&ms[c], a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return SPHDEM_E_CUDA;
+    EH->dlist_pp = ms[1] < ms[0];
+    return SPHDEM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1093,6 +1132,7 @@ static int commit_t(SphdemHandle* H) {
             P.nbd_cap = capd;
             W.nbrd = A.get<int>((size_t)capd * ns);
             if (!A.ok) return SPHDEM_E_NOMEM;
+            if ((r = tune_dlist<R>(H, EH, E.S[1], E.D[1]))) return r;
         }
         if (p.ppe_mode != SPHDEM_PPE_REFERENCE) {
             KryWork<R>& K = EH->K;

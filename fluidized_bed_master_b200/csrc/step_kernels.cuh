@@ -647,6 +647,46 @@ __device__ __forceinline__ void dlist_cell(int c, DevParams P, const double* __r
     }
 }
 
+// The same list with one thread per SPH particle over the DEM slots of its
+// stencil rows (the exact predicate for every candidate): the same entries
+// in the same order.  Picked per handle at commit where it is faster (2-D
+// beds, whose cells hold a few particles each); parked slots (i_type 3) keep
+// their count, as the warp-per-cell build leaves them.
+__global__ void __launch_bounds__(128) k_build_dlist_pp(DevParams P, const double* __restrict__ sx,
+                                                        const double* __restrict__ sy,
+                                                        const double* __restrict__ sz,
+                                                        const double* __restrict__ sh,
+                                                        const int* __restrict__ itype,
+                                                        const int4* __restrict__ drows,
+                                                        const double* __restrict__ dx,
+                                                        const double* __restrict__ dy,
+                                                        const double* __restrict__ dz,
+                                                        const int* __restrict__ dptype, int* __restrict__ nbrd,
+                                                        int* __restrict__ ncntd, int cap, DevFlags* F) {
+    grid_dep_wait();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P.ns;
+    const bool act = i < n && itype[i] != 3;
+    int cnt = 0;
+    if (act) {
+        const double xi = sx[i], yi = sy[i], zi = sz[i], Rr = P.kappa * sh[i];
+        int ic, jc, kc;
+        cell_ijk(P, xi, yi, zi, ic, jc, kc);
+        int* pw = nbrd ? nbrd + i : nullptr;   // entry cnt of row i at pw (pw += n per hit)
+        for_stencil_j(P, ic, jc, kc, drows, make_cull(xi, yi, zi, Rr), [&](int j) {
+            if (__ldg(dptype + j) <= 1000) return;
+            if (pair_dist(xi, yi, zi, dx[j], dy[j], dz[j]) < Rr) {
+                if (pw && cnt < cap) *pw = j;
+                pw += n;
+                cnt++;
+            }
+        });
+        ncntd[i] = cnt;
+    }
+    const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
+    if ((threadIdx.x & 31) == 0 && wmax > 0) atomicMax(&F->max_ncntd, wmax);
+}
+
 template <bool OCC>
 __global__ void __launch_bounds__(DL_WARPS * 32) k_build_dlist(DevParams P, const double* __restrict__ sx,
                                                                  const double* __restrict__ sy,

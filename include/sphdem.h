@@ -539,7 +539,10 @@ int sphdem_set_domain(SphdemHandle* h, const double* bbox6, double h0, double t_
  * build); 0 (the default) = timed at commit on the committed state, the
  * fastest kept.  Every mode writes the same lists in the same order, so the
  * choice changes only the speed.  FP64 handles build one thread per
- * particle.  Set before sphdem_commit_particles; read after it. */
+ * particle.  The SPH -> DEM list of the coupling passes is picked the same
+ * way (a thread per particle or a warp per cell); a fixed mode fixes it
+ * too (1: per particle, 2/4/8: per cell).  Set before
+ * sphdem_commit_particles; read after it. */
 int sphdem_set_list_build(SphdemHandle* h, int32_t mode);
 int sphdem_get_list_build(SphdemHandle* h, int32_t* mode);
 

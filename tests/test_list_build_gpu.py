@@ -1,6 +1,8 @@
 """The SPH list build's modes (sphdem_set_list_build / get): one thread per
 particle (1) and one warp per cell with 2, 4 or 8 cells per block, and the
-default (0) that times the four at commit and keeps the fastest.
+default (0) that times the four at commit and keeps the fastest.  A fixed
+mode also fixes the SPH -> DEM list build (1: a thread per particle, 2/4/8:
+a warp per cell), so the modes compare both of its kernels too.
 
 Bar: on the 3-D bed slice and on a 2-D bed (FP32 build), every mode gives
 the same neighbour lists and, after 5 steps, every field bit for bit equal
