@@ -877,6 +877,19 @@ def run_bed2d_batch(args, world, rank, local, pg):
         eng.collect_timing()
     kms = {k: (v[0] - b0.get(k, (0, 0))[0]) / (PROFILE_STEPS // 2) for k, v in eng.timing().items()}
     kms = {k: round(v, 4) for k, v in sorted(kms.items(), key=lambda kv: -kv[1]) if v > 0}
+    # the same with the DEM branch on the step stream: each kernel alone
+    eng.set_concurrency(False)
+    eng.step(2)
+    eng.collect_timing()
+    b1 = eng.timing()
+    for _ in range(PROFILE_STEPS // 2):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        eng.step(1)
+        eng.collect_timing()
+    kser = {k: (v[0] - b1.get(k, (0, 0))[0]) / (PROFILE_STEPS // 2) for k, v in eng.timing().items()}
+    kser = {k: round(v, 4) for k, v in sorted(kser.items(), key=lambda kv: -kv[1]) if v > 0}
+    eng.set_concurrency(True)
     eng.set_timing(False)
     eng.step(2)
     torch.cuda.synchronize()
@@ -948,6 +961,7 @@ def run_bed2d_batch(args, world, rank, local, pg):
         "state_finite": finite,
         "kernels_ms_per_step": kms,
         "kernels_ms_per_step_from": f"{PROFILE_STEPS // 2} steps with every kernel timed, before the timed region",
+        "kernels_ms_per_step_serialised": kser,
         "sequential": {"ms_per_step": seq_ms, "how": f"each bed alone in its own handle, {ks} timed steps each "
                        "after 3 warm-up steps, per-step device times summed over the beds",
                        "value": n * 1e3 / seq_ms if seq_ms else None, "unit": unit},
