@@ -702,7 +702,12 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     }
     CK(rec(1, sd));   // SPH -> DEM list built
     if (nd > 0) {
-        { KTIME_ON(KT_DEMCONTACT, sd); CK((launch_pdl(k_dem_contact<R>, bdw, TPB, 0, sd, P, D, DW, DW.rows, E.flags))); }
+        {
+            // a thread per sphere in two dimensions (a few candidates each), a warp in three
+            KTIME_ON(KT_DEMCONTACT, sd);
+            if (P.dim == 2) CK((launch_pdl(k_dem_contact<R, 1>, bd, TPB, 0, sd, P, D, DW, DW.rows, E.flags)));
+            else CK((launch_pdl(k_dem_contact<R, 32>, bdw, TPB, 0, sd, P, D, DW, DW.rows, E.flags)));
+        }
         { KTIME_ON(KT_DEMPREP, sd); CK((launch_pdl(k_dem_prep<R>, bdw, TPB, 0, sd, P, S, W.rec, D, DW, W.rows, DW.rows))); }
         *nl += 2;
     }

@@ -1170,20 +1170,27 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // start of the step (so two new partners in one step share a slot, as in
 // the reference).  Spring increments and overlap are FP64.
 // ---------------------------------------------------------------------------
-template <typename R>
+// G = 32: one warp per sphere (3-D beds: ~160 stencil candidates each);
+// G = 1: one thread per sphere over its candidates in visit order (2-D beds:
+// a few candidates, which a warp would leave mostly idle).  The launch picks
+// G from the bed's dimension, so a configuration always runs one form.
+template <typename R, int G>
 // 4 blocks of 128 per SM (128 registers, a few spilled): 0.145 -> 0.124 ms on
 // the bench bed against the unbounded 162-register build
 __global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<double> D, DemWork<double> DW,
                                                      const int4* __restrict__ drows,
                                                      DevFlags* F) {
+    static_assert(G == 32 || G == 1, "a warp or a thread per sphere");
     grid_dep_wait();
-    // one warp per sphere; lanes take candidates l, l+32, ... of the stencil
-    // in visit order (for_rows_warp) and the pair terms are reduced with
-    // shuffles.  History writes keep the sequential semantics: lookups use
-    // the start-of-step ids, a release clears only the partner's own slot,
-    // and every new contact targets the first slot free at the start of the
+    // G = 32: lanes take candidates l, l+32, ... of the stencil in visit
+    // order (for_rows_warp) and the pair terms are reduced with shuffles.
+    // History writes keep the sequential semantics: lookups use the
+    // start-of-step ids, a release clears only the partner's own slot, and
+    // every new contact targets the first slot free at the start of the
     // step, so the new contact visited last wins that slot.
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int i = G == 32 ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5)
+                          : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int lane = G == 32 ? (int)(threadIdx.x & 31) : 0;
     __shared__ int s_rows[4][20];
     int* sm = s_rows[threadIdx.x >> 5];
     const int n = P.nd;
@@ -1228,10 +1235,10 @@ __global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<do
     // this lane's last new contact (visit order t) and its spring
     int new_t = -1, new_id = 0;
     double new_dx = 0, new_dy = 0, new_dz = 0;
-    int t_visit = lane - 32;
+    int t_visit = lane - G;
     const Cull cu = make_cull(xi, yi, zi, P.r_search * radi);
-    for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, [&](int j) {
-        t_visit += 32;
+    auto pair = [&](int j) {
+        t_visit += G;
         if (D.ptype[j] <= 1000) return;
         double xj = D.x[j], yj = D.y[j], zj = D.z[j], radj = D.rad[j];
         double td = pair_dist(xi, yi, zi, xj, yj, zj);
@@ -1365,11 +1372,15 @@ __global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<do
             D.hds[(slot * 3 + 2) * n + i] = 0.0;
             D.hid[slot * n + i] = 0;
         }
-    });
+    };
+    if constexpr (G == 32) for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, pair);
+    else for_stencil_j(P, ic, jc, kc, drows, cu, pair);
     // the new contact visited last takes the first slot free at the start
     int last_t = new_t;
+    if constexpr (G == 32) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) last_t = max(last_t, __shfl_xor_sync(0xffffffffu, last_t, o));
+        for (int o = 16; o > 0; o >>= 1) last_t = max(last_t, __shfl_xor_sync(0xffffffffu, last_t, o));
+    }
     if (last_t >= 0 && new_t == last_t) {
         // no free slot (a 17th partner): flag it; the new contact acted this
         // step and is not recorded (the reference writes through an unset
@@ -1384,9 +1395,11 @@ __global__ void __launch_bounds__(128, 4) k_dem_contact(DevParams P, DemState<do
             D.hds[(slot * 3 + 2) * n + i] = new_dz;
         }
     }
-    tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
-    tqx = warp_sum(tqx); tqy = warp_sum(tqy); tqz = warp_sum(tqz);
-    dtr = warp_sum(dtr); dtc = warp_sum(dtc);
+    if constexpr (G == 32) {
+        tx = warp_sum(tx); ty = warp_sum(ty); tz = warp_sum(tz);
+        tqx = warp_sum(tqx); tqy = warp_sum(tqy); tqz = warp_sum(tqz);
+        dtr = warp_sum(dtr); dtc = warp_sum(dtc);
+    }
     if (lane != 0) return;
     if (P.fg) tz += -(Q)P.g_dem;
     if (P.con) {
