@@ -506,6 +506,14 @@ static int enqueue_krylov(SphdemHandle* H, EngineHost<R>* EH, SphState<R>& S, Sp
 }
 
 // SPH -> DEM list of the sorted sets S, D (W.nbrd may be null: count only)
+// The DEM contact, filter and coupling passes take a thread per sphere on
+// 2-D beds with many spheres (a sphere there has a few DEM and ~70 SPH
+// candidates, which a warp per sphere would leave mostly idle) and a warp
+// per sphere otherwise (3-D beds, ~160 DEM candidates; and few spheres,
+// where a warp each keeps more of the GPU busy).  A function of the
+// configuration, so a given bed always runs one form.
+inline bool dem_thread_per_sphere(const DevParams& P) { return P.dim == 2 && P.nd >= 65536; }
+
 // warps of a grid-stride pass over the occupied cells of a sparse grid: at
 // most one per SPH particle, at most 128 per SM
 inline int occ_warps(const DevParams& P) { return std::max(1, std::min(P.ns, 148 * 128)); }
@@ -703,12 +711,15 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     CK(rec(1, sd));   // SPH -> DEM list built
     if (nd > 0) {
         {
-            // a thread per sphere in two dimensions (a few candidates each), a warp in three
             KTIME_ON(KT_DEMCONTACT, sd);
-            if (P.dim == 2) CK((launch_pdl(k_dem_contact<R, 1>, bd, TPB, 0, sd, P, D, DW, DW.rows, E.flags)));
+            if (dem_thread_per_sphere(P)) CK((launch_pdl(k_dem_contact<R, 1>, bd, TPB, 0, sd, P, D, DW, DW.rows, E.flags)));
             else CK((launch_pdl(k_dem_contact<R, 32>, bdw, TPB, 0, sd, P, D, DW, DW.rows, E.flags)));
         }
-        { KTIME_ON(KT_DEMPREP, sd); CK((launch_pdl(k_dem_prep<R>, bdw, TPB, 0, sd, P, S, W.rec, D, DW, W.rows, DW.rows))); }
+        {
+            KTIME_ON(KT_DEMPREP, sd);   // see dem_thread_per_sphere
+            if (dem_thread_per_sphere(P)) CK((launch_pdl(k_dem_prep<R, 1>, bd, TPB, 0, sd, P, S, W.rec, D, DW, W.rows, DW.rows)));
+            else CK((launch_pdl(k_dem_prep<R, 32>, bdw, TPB, 0, sd, P, S, W.rec, D, DW, W.rows, DW.rows)));
+        }
         *nl += 2;
     }
     if (ns > 0) {
@@ -736,7 +747,10 @@ int enqueue_step(SphdemHandle* H, EngineHost<R>* EH, int flags, int64_t* nl) {
     if (nd > 0) {
         {
             KTIME(KT_DEMCOUPLING);
-            CK((launch_pdl(kt3 ? k_dem_coupling<R, 3> : k_dem_coupling<R, -1>, bdw, TPB, 0, st, P, S, W, D, DW, W.rows)));
+            if (dem_thread_per_sphere(P))   // see dem_thread_per_sphere
+                CK((launch_pdl(kt3 ? k_dem_coupling<R, 3, 1> : k_dem_coupling<R, -1, 1>, bd, TPB, 0, st, P, S, W, D, DW, W.rows)));
+            else
+                CK((launch_pdl(kt3 ? k_dem_coupling<R, 3, 32> : k_dem_coupling<R, -1, 32>, bdw, TPB, 0, st, P, S, W, D, DW, W.rows)));
             CK((launch_pdl(k_dem_finish<R>, bd, TPB, 0, st, P, D, DW)));
         }
         *nl += 2;

@@ -882,11 +882,16 @@ __global__ void k_gather_history(int n, const int* __restrict__ perm, const int*
 
 // KERNEL_clc_prep3D_coupling_dem: functions_PREP2.cuh:3367-3523.
 // One warp per DEM sphere; lanes stride over the candidate rows.
-template <typename R>
+// G = 32: a warp per sphere; G = 1: a thread per sphere (2-D beds with many
+// spheres); dem_thread_per_sphere in engine.cu.
+template <typename R, int G>
 __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, SphRec<R> rec, DemState<double> D,
                                                   DemWork<double> DW, const int4* __restrict__ srows, const int4* __restrict__ drows) {
+    static_assert(G == 32 || G == 1, "a warp or a thread per sphere");
     grid_dep_wait();
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int i = G == 32 ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5)
+                          : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int lane = G == 32 ? (int)(threadIdx.x & 31) : 0;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
     if (i >= P.nd) return;
@@ -909,6 +914,39 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
     // (p_type 1 or 3, the 1e-20 form)
     const unsigned lt = (1u << lane) - 1u;
     int cs = 0;
+    auto dem_por = [&](int j) {
+        if (D.ptype[j] <= 1000) return;
+        PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
+        if (!g.in) return;
+        R w = kw(K, g.r);
+        R rj = (R)D.rad[j];
+        por += w * dem_measure(P, rj);
+    };
+    if constexpr (G == 1) {
+        // in visit order, one candidate after another
+        for_stencil_j(P, ic, jc, kc, srows, cu, [&](int j) {
+            const PosRec<R> qj = ldr(rec.pos + j);
+            const int ptj = tag_ptype(qj.w);
+            if (ptj > 1000) return;
+            bool in = false, in20 = false;
+            Disp<R> d;
+            R r2 = 0;
+            test_pair2(P, qp, qj, xi, yi, zi, S.x, S.y, S.z, j, Rr, bd, d, r2, in, in20);
+            if (in) {
+                if (cs < DEM_SPH_CAP) DW.nbs[(size_t)i * DEM_SPH_CAP + cs] = j;
+                cs++;
+            }
+            if (!in20 || (ptj != 1 && ptj != 3)) return;
+            R r, rinv;
+            rdist(r2, r, rinv);
+            V2<R> mr = ldr(rec.mr0 + j);
+            R c = mr.x * rcp(mr.y) * kw(K, r);
+            if (ptj == 1) f1 += c;
+            else f3 += c;
+        });
+        DW.ncs[i] = cs;
+        for_stencil_j(P, ic, jc, kc, drows, cu, dem_por);
+    } else {
     for_rows_warp_all(P, ic, jc, kc, srows, cu, sm, lane, [&](int j) {
         bool in = false, in20 = false;
         int ptj = 0;
@@ -934,17 +972,11 @@ __global__ void __launch_bounds__(128) k_dem_prep(DevParams P, SphState<R> S, Sp
         else f3 += c;
     });
     if (lane == 0) DW.ncs[i] = cs;
-    for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, [&](int j) {
-        if (D.ptype[j] <= 1000) return;
-        PairT<R> g = pair_test<R>(xi, yi, zi, D.x[j], D.y[j], D.z[j], Rr, 1e-20, r2l, r2h);
-        if (!g.in) return;
-        R w = kw(K, g.r);
-        R rj = (R)D.rad[j];
-        por += w * dem_measure(P, rj);
-    });
+    for_rows_warp(P, ic, jc, kc, drows, cu, sm, lane, dem_por);
     f1 = warp_sum(f1);
     f3 = warp_sum(f3);
     por = warp_sum(por);
+    }
     if (lane == 0 && pti > 1000) {
         DW.flt_s[i] = f3;
         DW.flt_sd[i] = f1;
@@ -1171,9 +1203,10 @@ __global__ void __launch_bounds__(128) k_passB(DevParams P, SphState<R> S, SphWo
 // the reference).  Spring increments and overlap are FP64.
 // ---------------------------------------------------------------------------
 // G = 32: one warp per sphere (3-D beds: ~160 stencil candidates each);
-// G = 1: one thread per sphere over its candidates in visit order (2-D beds:
-// a few candidates, which a warp would leave mostly idle).  The launch picks
-// G from the bed's dimension, so a configuration always runs one form.
+// G = 1: one thread per sphere over its candidates in visit order (2-D beds
+// with many spheres: a few candidates, which a warp would leave mostly
+// idle).  The launch picks G from the configuration (dem_thread_per_sphere
+// in engine.cu), so a bed always runs one form.
 template <typename R, int G>
 // 4 blocks of 128 per SM (128 registers, a few spilled): 0.145 -> 0.124 ms on
 // the bench bed against the unbounded 162-register build
@@ -1593,11 +1626,16 @@ __device__ void dem_coupling_finish(const DevParams& P, DemState<double>& D, Dem
     if (P.con && pt > 0) DW.temp0[i] = D.temp[i];
 }
 
-template <typename R, int KT>
+// G = 32: a warp per sphere; G = 1: a thread per sphere (2-D beds with many
+// spheres, ~20 SPH neighbours each); dem_thread_per_sphere in engine.cu.
+template <typename R, int KT, int G>
 __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S, SphWork<R> W, DemState<double> D,
                                                       DemWork<double> DW, const int4* __restrict__ srows) {
+    static_assert(G == 32 || G == 1, "a warp or a thread per sphere");
     grid_dep_wait();
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int i = G == 32 ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5)
+                          : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int lane = G == 32 ? (int)(threadIdx.x & 31) : 0;
     __shared__ int s_rows[4][20];   // 128 threads = 4 warps
     int* sm = s_rows[threadIdx.x >> 5];
     if (i >= P.nd) return;
@@ -1638,12 +1676,13 @@ __global__ void __launch_bounds__(128) k_dem_coupling(DevParams P, SphState<R> S
         const int cs = DW.ncs[i];
         if (cs <= DEM_SPH_CAP) {
             const int* __restrict__ nbs = DW.nbs + (size_t)i * DEM_SPH_CAP;
-            for (int k = lane; k < cs; k += 32) pair(__ldg(nbs + k));
+            for (int k = lane; k < cs; k += G) pair(__ldg(nbs + k));
         } else {
             const Cull cu = make_cull(xi, yi, zi, Rr);
-            for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, pair);
+            if constexpr (G == 32) for_rows_warp(P, ic, jc, kc, srows, cu, sm, lane, pair);
+            else for_stencil_j(P, ic, jc, kc, srows, cu, pair);
         }
-        dc_warp_sum(a);
+        if constexpr (G == 32) dc_warp_sum(a);
     }
     if (lane != 0) return;
     // the closure and the predictor run in k_dem_finish (thread per sphere),

@@ -11,7 +11,9 @@ spheres, inlet velocities U(0.1, 0.3).  Bars (in each assert):
 * the FP64 batch against the oracle on the same beds (oracle_set_beds)
   after 20 steps: neighbour lists and contact partners exact, every field
   within rel. L2 1e-9;
-* planes closer than two cells are refused at commit (SPHDEM_E_INPUT).
+* planes closer than two cells are refused at commit (SPHDEM_E_INPUT);
+* the bench's 64-bed batch, FP64 against the oracle after 3 steps (its
+  sphere count selects the thread-per-sphere DEM passes).
 """
 import numpy as np
 import pytest
@@ -93,3 +95,20 @@ def test_close_planes_refused(batch):
     dem2 = {k: np.concatenate([d0[k], d1[k]]) for k in d0}
     with pytest.raises(SphdemError):
         _engine(p, sph2, dem2, 0, beds=r0 + r1)
+
+
+def test_large_batch_fp64_vs_oracle():
+    """The bench's 64-bed batch (1,029,448 SPH and 94,181 DEM): with more
+    than 65,536 spheres on 2-D beds the DEM contact, filter and coupling
+    passes take a thread per sphere; FP64 against the oracle after 3 steps,
+    lists and partners exact, every field within rel. L2 1e-9."""
+    p, sph, dem, rows, parts = bed2d_batch(seed=0)
+    assert len(dem["x"]) >= 65536
+    eng = _engine(p, sph, dem, 1, beds=rows)
+    orc = Oracle(p, sph, dem, threads=16, beds=rows)
+    eng.step(3)
+    orc.step(3)
+    _check_lists_and_partners(eng, orc, "step 3")
+    err = _field_errors(eng, orc, SPH_ALL, DEM_ALL)
+    bad = {k: v for k, v in err.items() if not v <= 1e-9}
+    assert not bad, sorted(bad.items(), key=lambda kv: -kv[1])
