@@ -11,7 +11,8 @@ spheres, inlet velocities U(0.1, 0.3).  Bars (in each assert):
 * the FP64 batch against the oracle on the same beds (oracle_set_beds)
   after 20 steps: neighbour lists and contact partners exact, every field
   within rel. L2 1e-9;
-* planes closer than two cells are refused at commit (SPHDEM_E_INPUT);
+* planes closer than two cells are refused at commit (SPHDEM_E_INPUT),
+  empty or non-finite rows and 3-D handles by sphdem_set_beds;
 * the bench's 64-bed batch, FP64 against the oracle after 3 steps (its
   sphere count selects the thread-per-sphere DEM passes).
 """
@@ -112,3 +113,23 @@ def test_large_batch_fp64_vs_oracle():
     err = _field_errors(eng, orc, SPH_ALL, DEM_ALL)
     bad = {k: v for k, v in err.items() if not v <= 1e-9}
     assert not bad, sorted(bad.items(), key=lambda kv: -kv[1])
+
+
+def test_set_beds_arguments(batch):
+    """sphdem_set_beds refuses what it cannot honour: no rows or a non-finite
+    row (SPHDEM_E_ARG), a 3-D handle (SPHDEM_E_UNSUPPORTED)."""
+    from fluidized_bed_master_b200.beds import box_bed
+    from fluidized_bed_master_b200.engine import SphdemError
+
+    p, sph, dem, rows, parts = batch
+    s0, d0, r0 = parts[0]
+    with pytest.raises(SphdemError) as e:
+        _engine(p, s0, d0, 0, beds=[])
+    assert e.value.status == -1
+    with pytest.raises(SphdemError) as e:
+        _engine(p, s0, d0, 0, beds=[dict(r0[0], inlet_uz=float("nan"))])
+    assert e.value.status == -1
+    p3, s3, d3 = box_bed(n_fluid=2_000, n_dem=100, dem_height=0.005, seed=1)
+    with pytest.raises(SphdemError) as e:
+        _engine(p3, s3, d3, 0, beds=r0)
+    assert e.value.status == -7
