@@ -47,11 +47,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="bed",
-                    choices=["bed", "dam2d", "dam2d-batch", "bed2d-batch", "ppe-profile", "column", "mlp", "slabs"],
+                    choices=["bed", "dam2d", "dam2d-batch", "bed2d-batch", "batch", "ppe-profile", "column", "mlp", "slabs"],
                     help="bed: the 3-D SPH-DEM fluidized bed (default); dam2d: the 2-D WCSPH dam break "
                          "(its protocol is --steps 1000); dam2d-batch: 64 uneven dam breaks in one handle "
                          "against the same beds run one after another; bed2d-batch: 64 uneven 2-D ISPH-DEM beds "
-                         "(per-bed inlet velocities) in one handle, against the same beds one after another; "
+                         "(per-bed inlet velocities) in one handle, against the same beds one after another (batch is "
+                         "the same workload); "
                          "ppe-profile: --steps steps of the bed with the "
                          "projected-start PCG and step graphs off, so that a kernel profiler sees the PPE "
                          "kernels (no timing); slabs: the bench bed cut into z slabs, one per rank (on one "
@@ -74,7 +75,10 @@ def parse():
                     help="--workload ppe-profile: the bench bed or the scaled bed")
     ap.add_argument("--ppe-bed", default="scaled", choices=["scaled", "bench"],
                     help="bed of the PPE comparison: the 2.2 M-particle scaled bed or the bench bed")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.workload == "batch":
+        args.workload = "bed2d-batch"
+    return args
 
 
 def dist_setup():
